@@ -1,0 +1,70 @@
+// Host-side context shared by all entry points (internal, not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <unordered_map>
+
+#include "bespoke_gpu.h"
+
+struct bo_ctx {
+  int device = 0;
+  int num_sms = 0;
+  size_t l2_bytes = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  std::atomic<int64_t> launches{0};
+
+  // Device error word (bo::kErr* bits) and per-operation scratch regions,
+  // allocated once and kept for the context's lifetime.  Named regions are
+  // grown on demand; kernels that accumulate into them leave them zeroed.
+  uint32_t* d_err = nullptr;
+  uint32_t* h_err = nullptr;  // pinned mirror for the single end-of-call read
+  struct Region {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+  };
+  std::unordered_map<std::string, Region> regions;
+  // Pinned staging used by the _host entry points.
+  void* h_stage = nullptr;
+  size_t h_stage_bytes = 0;
+};
+
+namespace bo {
+
+int set_error(bo_ctx* ctx, int code, const char* fmt, ...);
+int cuda_fail(bo_ctx* ctx, cudaError_t e, const char* what);
+
+#define BO_CUDA(ctx, call)                                  \
+  do {                                                      \
+    cudaError_t e__ = (call);                               \
+    if (e__ != cudaSuccess) return bo::cuda_fail((ctx), e__, #call); \
+  } while (0)
+
+#define BO_CHECK_CTX(ctx)                                   \
+  do {                                                      \
+    if (!(ctx)) return BO_ERR_INVALID;                      \
+  } while (0)
+
+// Returns a device region of at least `bytes`, zero-filled when first
+// allocated or grown (zeroing is ordered on the context's stream).
+int region(bo_ctx* ctx, const char* name, size_t bytes, void** out);
+// Pinned host staging buffer of at least `bytes`.
+int host_stage(bo_ctx* ctx, size_t bytes, void** out);
+// Records one kernel launch and checks the launch status.
+int after_launch(bo_ctx* ctx, const char* what);
+// Reads and clears the device error word (call only after a stream sync).
+int consume_device_errors(bo_ctx* ctx, uint32_t* bits_out);
+// Maps error bits to a status code with a message.
+int device_error_status(bo_ctx* ctx, uint32_t bits, const char* op);
+// Blocks per SM from the occupancy calculator, cached per kernel.
+int occupancy_blocks(const void* kernel, int block, size_t smem);
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace bo

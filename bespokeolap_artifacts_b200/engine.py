@@ -1,0 +1,153 @@
+"""Host-side mirror of the reference's per-query API over the GPU engine.
+
+The reference exposes ``run_qN(const Database&, const QNArgs&) -> vector<QNResultRow>``
+(bespoke_tpch/query_q1.hpp:22, query_q3.hpp:17, query_q6.hpp:15).  This module
+keeps those names, argument meanings and result fields; the work runs in
+``libbespoke_gpu.so`` through its C ABI (see ``native.py``).  Errors surface as
+:class:`native.BoError` with the engine's status code, the counterpart of the
+reference's ``std::runtime_error``.
+
+Inputs are device tensors (torch) or host numpy arrays; the ``*_host`` paths
+copy host buffers in and results out inside the call.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import native as N
+from .datagen import FLAG_A_LETTERS, FLAG_B_LETTERS, days_from_civil
+
+PRICE_SCALE = 100
+DISCOUNT_SCALE = 100
+
+
+@dataclass
+class Q1ResultRow:
+    """Fields of the reference's Q1ResultRow (bespoke_tpch/query_q1.hpp:9-20)."""
+    returnflag: str
+    linestatus: str
+    sum_qty: float
+    sum_base_price: float
+    sum_disc_price: float
+    sum_charge: float
+    avg_qty: float
+    avg_price: float
+    avg_disc: float
+    count_order: int
+
+
+def q1_rows_from_aggs(aggs: list[dict], returnflag_dict: list[str], linestatus_dict: list[str]) -> list[Q1ResultRow]:
+    """run_q1's finalisation (bespoke_tpch/query_q1.cpp:233-274): groups with a
+    non-zero count become rows, integer totals turn into doubles with the same
+    expressions (Python floats are IEEE doubles, int->float rounds to nearest as
+    the C++ conversion does), then rows are ordered by (returnflag, linestatus)."""
+    rows = []
+    ls_count = len(linestatus_dict)
+    for idx, a in enumerate(aggs):
+        if a["count"] == 0:
+            continue
+        count = float(a["count"])
+        sum_qty = float(a["sum_qty"]) / PRICE_SCALE
+        sum_base = float(a["sum_base_price"]) / PRICE_SCALE
+        rows.append(Q1ResultRow(
+            returnflag=returnflag_dict[idx // ls_count],
+            linestatus=linestatus_dict[idx % ls_count],
+            sum_qty=sum_qty,
+            sum_base_price=sum_base,
+            sum_disc_price=float(a["sum_disc_price"]) / PRICE_SCALE,
+            sum_charge=float(a["sum_charge"]) / (float(PRICE_SCALE) * DISCOUNT_SCALE),
+            avg_qty=sum_qty / count,
+            avg_price=sum_base / count,
+            avg_disc=float(a["sum_disc"]) / DISCOUNT_SCALE / count,
+            count_order=a["count"],
+        ))
+    rows.sort(key=lambda r: (r.returnflag, r.linestatus))
+    return rows
+
+
+def q1_cutoff(delta_days: int) -> int:
+    """Absolute-day cutoff of Q1: 1998-12-01 minus DELTA (query_q1.cpp:111-113)."""
+    return days_from_civil(1998, 12, 1) - int(delta_days)
+
+
+class Engine:
+    """One engine context (device, stream, scratch) with the pipeline entry points."""
+
+    def __init__(self, device: int = 0):
+        self.ctx = N.Context(device)
+
+    def close(self):
+        self.ctx.close()
+
+    @property
+    def launches(self) -> int:
+        return self.ctx.launches
+
+    def set_stream(self, stream_handle):
+        self.ctx.set_stream(stream_handle)
+
+    def synchronize(self):
+        self.ctx.synchronize()
+
+    # ------------------------------------------------------------ Q1 -------
+    @staticmethod
+    def fact_cols(cols, n_rows: int) -> N.FactCols:
+        """cols: (ship_date, quantity, ext_price, discount, tax, flag_a, flag_b)."""
+        return N.FactCols(*[N.ptr(c) for c in cols], n_rows)
+
+    def q1_fact_device(self, cols, n_rows: int, cutoff: int, n_flag_a: int, n_flag_b: int, out_dev) -> None:
+        """Launches the fused scan/filter/group-aggregate on device columns;
+        out_dev is a device buffer of >= n_flag_a*n_flag_b bo_q1_agg records."""
+        fc = self.fact_cols(cols, n_rows)
+        self.ctx.call("bo_q1_fact_device", C.byref(fc), cutoff, n_flag_a, n_flag_b, C.c_void_p(N.ptr(out_dev)))
+
+    def q1_fact_host(self, table, cutoff: int) -> list[dict]:
+        """Host arrays in, exact per-group totals out (copies inside the call)."""
+        cols = [np.ascontiguousarray(c) for c in table.columns()]
+        fc = self.fact_cols(cols, table.n_rows)
+        ng = table.n_flag_a * table.n_flag_b
+        out = (N.Q1Agg * ng)()
+        self.ctx.call("bo_q1_fact_host", C.byref(fc), cutoff, table.n_flag_a, table.n_flag_b, out)
+        return [out[g].as_dict() for g in range(ng)]
+
+    def run_q1_fact(self, table, delta_days: int = 90) -> list[Q1ResultRow]:
+        """run_q1 over the wide fact layout, flags mapped to order-preserving
+        returnflag / linestatus letters."""
+        aggs = self.q1_fact_host(table, q1_cutoff(delta_days))
+        return q1_rows_from_aggs(aggs, list(FLAG_A_LETTERS[:table.n_flag_a]), list(FLAG_B_LETTERS[:table.n_flag_b]))
+
+    @staticmethod
+    def lineitem_cols(li: dict) -> N.LineitemCols:
+        names = ["shipdate", "returnflag_linestatus", "extendedprice", "discounted_price", "discount", "tax",
+                 "quantity"]
+        return N.LineitemCols(*[N.ptr(li.get(k)) for k in names], int(li["n_rows"]))
+
+    def q1_lineitem_host(self, li: dict, cutoff_offset: int, n_groups: int) -> list[dict]:
+        lc = self.lineitem_cols(li)
+        out = (N.Q1Agg * n_groups)()
+        self.ctx.call("bo_q1_lineitem_host", C.byref(lc), cutoff_offset, n_groups, out)
+        return [out[g].as_dict() for g in range(n_groups)]
+
+    def q1_lineitem_device(self, li: dict, cutoff_offset: int, n_groups: int, out_dev) -> None:
+        lc = self.lineitem_cols(li)
+        self.ctx.call("bo_q1_lineitem_device", C.byref(lc), cutoff_offset, n_groups, C.c_void_p(N.ptr(out_dev)))
+
+    def run_q1(self, li: dict, delta_days: int = 90) -> list[Q1ResultRow]:
+        """run_q1 (bespoke_tpch/query_q1.cpp:104) over storage-plan lineitem
+        columns: ``li`` carries the columns, ``base_date_days`` and the
+        returnflag / linestatus dictionaries in code order."""
+        cutoff = q1_cutoff(delta_days) - int(li["base_date_days"])
+        rf = list(li["returnflag_dict"])
+        ls = list(li["linestatus_dict"])
+        aggs = self.q1_lineitem_host(li, cutoff, len(rf) * len(ls))
+        return q1_rows_from_aggs(aggs, rf, ls)
+
+    # ------------------------------------------------------------ Q6 -------
+    def q6_lineitem_host(self, li: dict, start: int, end: int, dmin: int, dmax: int, qlimit: int) -> tuple[int, int]:
+        lc = self.lineitem_cols(li)
+        out = N.Q6Result()
+        self.ctx.call("bo_q6_lineitem_host", C.byref(lc), start, end, dmin, dmax, qlimit, C.byref(out))
+        return out.revenue_raw, out.count

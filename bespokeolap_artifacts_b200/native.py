@@ -1,0 +1,222 @@
+"""ctypes binding of ``libbespoke_gpu.so`` (the C ABI in ``include/bespoke_gpu.h``).
+
+The library is the only compute path: if it is missing or was not built, every
+entry point raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libbespoke_gpu.so"
+
+BO_OK = 0
+STATUS_NAMES = {
+    0: "BO_OK",
+    -1: "BO_ERR_INVALID",
+    -2: "BO_ERR_OOM",
+    -3: "BO_ERR_OVERFLOW",
+    -4: "BO_ERR_TIMEOUT",
+    -5: "BO_ERR_CUDA",
+    -6: "BO_ERR_DATA",
+    -7: "BO_ERR_UNSUPPORTED",
+}
+
+Q1_MAX_GROUPS = 8
+
+
+class BoError(RuntimeError):
+    """A failed call into the engine; ``status`` is the BO_ERR_* code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+# ----------------------------------------------------------------- structs --
+class I128(C.Structure):
+    _fields_ = [("lo", C.c_uint64), ("hi", C.c_int64)]
+
+    def value(self) -> int:
+        return (self.hi << 64) | self.lo
+
+
+class Q1Agg(C.Structure):
+    _fields_ = [
+        ("count", C.c_int64),
+        ("sum_qty", C.c_int64),
+        ("sum_base_price", C.c_int64),
+        ("sum_disc", C.c_int64),
+        ("sum_disc_price", C.c_int64),
+        ("sum_disc_price_exact", C.c_int64),
+        ("sum_charge", I128),
+        ("sum_charge_exact", I128),
+    ]
+
+    def as_dict(self) -> dict:
+        return {
+            "count": self.count,
+            "sum_qty": self.sum_qty,
+            "sum_base_price": self.sum_base_price,
+            "sum_disc": self.sum_disc,
+            "sum_disc_price": self.sum_disc_price,
+            "sum_disc_price_exact": self.sum_disc_price_exact,
+            "sum_charge": self.sum_charge.value(),
+            "sum_charge_exact": self.sum_charge_exact.value(),
+        }
+
+
+class FactCols(C.Structure):
+    _fields_ = [
+        ("ship_date", C.c_void_p),
+        ("quantity", C.c_void_p),
+        ("ext_price", C.c_void_p),
+        ("discount", C.c_void_p),
+        ("tax", C.c_void_p),
+        ("flag_a", C.c_void_p),
+        ("flag_b", C.c_void_p),
+        ("n_rows", C.c_int64),
+    ]
+
+
+class LineitemCols(C.Structure):
+    _fields_ = [
+        ("shipdate", C.c_void_p),
+        ("returnflag_linestatus", C.c_void_p),
+        ("extendedprice", C.c_void_p),
+        ("discounted_price", C.c_void_p),
+        ("discount", C.c_void_p),
+        ("tax", C.c_void_p),
+        ("quantity", C.c_void_p),
+        ("n_rows", C.c_int64),
+    ]
+
+
+class Q6Result(C.Structure):
+    _fields_ = [("revenue_raw", C.c_int64), ("count", C.c_int64)]
+
+
+# --------------------------------------------------------------- prototypes --
+_P = C.c_void_p
+_SIGNATURES = {
+    "bo_create": (C.c_int, [C.POINTER(_P), C.c_int]),
+    "bo_destroy": (None, [_P]),
+    "bo_last_error": (C.c_char_p, [_P]),
+    "bo_set_stream": (C.c_int, [_P, _P]),
+    "bo_get_stream": (_P, [_P]),
+    "bo_synchronize": (C.c_int, [_P]),
+    "bo_num_sms": (C.c_int, [_P]),
+    "bo_build_info": (C.c_char_p, []),
+    "bo_device_alloc": (C.c_int, [_P, C.c_size_t, C.POINTER(_P)]),
+    "bo_device_free": (C.c_int, [_P, _P]),
+    "bo_host_alloc_pinned": (C.c_int, [_P, C.c_size_t, C.POINTER(_P)]),
+    "bo_host_free_pinned": (C.c_int, [_P, _P]),
+    "bo_copy_h2d": (C.c_int, [_P, _P, _P, C.c_size_t]),
+    "bo_copy_d2h": (C.c_int, [_P, _P, _P, C.c_size_t]),
+    "bo_launch_count": (C.c_int64, [_P]),
+    "bo_q1_fact_device": (C.c_int, [_P, C.POINTER(FactCols), C.c_int32, C.c_int32, C.c_int32, _P]),
+    "bo_q1_fact_host": (C.c_int, [_P, C.POINTER(FactCols), C.c_int32, C.c_int32, C.c_int32, C.POINTER(Q1Agg)]),
+    "bo_q1_lineitem_device": (C.c_int, [_P, C.POINTER(LineitemCols), C.c_int16, C.c_int32, _P]),
+    "bo_q1_lineitem_host": (C.c_int, [_P, C.POINTER(LineitemCols), C.c_int16, C.c_int32, C.POINTER(Q1Agg)]),
+    "bo_q6_lineitem_device": (
+        C.c_int, [_P, C.POINTER(LineitemCols), C.c_int16, C.c_int16, C.c_int32, C.c_int32, C.c_int32, _P]),
+    "bo_q6_lineitem_host": (
+        C.c_int,
+        [_P, C.POINTER(LineitemCols), C.c_int16, C.c_int16, C.c_int32, C.c_int32, C.c_int32, C.POINTER(Q6Result)]),
+}
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def register(name: str, restype, argtypes) -> None:
+    """Adds a prototype (used by the modules that bind later entry points)."""
+    _SIGNATURES[name] = (restype, argtypes)
+    if _lib is not None:
+        f = getattr(_lib, name)
+        f.restype, f.argtypes = restype, argtypes
+
+
+def lib() -> C.CDLL:
+    """Loads the engine library; raises if it has not been built."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m bespokeolap_artifacts_b200.build` "
+                    "(the engine has no CPU fallback)")
+            l = C.CDLL(str(LIB_PATH))
+            for name, (res, args) in _SIGNATURES.items():
+                f = getattr(l, name)
+                f.restype, f.argtypes = res, args
+            _lib = l
+    return _lib
+
+
+def ptr(a) -> int:
+    """Raw address of a numpy array or torch tensor (host or device)."""
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    if isinstance(a, int):
+        return a
+    raise TypeError(f"cannot take the address of {type(a)}")
+
+
+class Context:
+    """Owns one ``bo_ctx`` (one CUDA stream and its scratch state)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = lib()
+        h = C.c_void_p()
+        rc = self._lib.bo_create(C.byref(h), device)
+        if rc != BO_OK:
+            raise BoError(rc, f"bo_create(device={device}) failed (no sm_100 GPU visible?)")
+        self.handle = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.bo_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def check(self, rc: int, what: str = "") -> None:
+        if rc != BO_OK:
+            msg = self._lib.bo_last_error(self.handle)
+            raise BoError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def call(self, name: str, *args) -> None:
+        self.check(getattr(self._lib, name)(self.handle, *args), name)
+
+    @property
+    def num_sms(self) -> int:
+        return self._lib.bo_num_sms(self.handle)
+
+    @property
+    def launches(self) -> int:
+        return self._lib.bo_launch_count(self.handle)
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        self.call("bo_set_stream", C.c_void_p(stream_handle or 0))
+
+    def synchronize(self) -> None:
+        self.call("bo_synchronize")

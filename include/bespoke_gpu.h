@@ -1,0 +1,170 @@
+/*
+ * bespoke_gpu.h -- C ABI of the B200 execution engine for the data-parallel hot
+ * path of the bespoke OLAP pipelines (scan + filter, join build/probe, group-by
+ * aggregation, radix sort / top-k).
+ *
+ * Conventions
+ *  - Plain C: opaque context handle, plain pointers and sizes, int status codes.
+ *    No C++ exception and no torch type crosses this boundary.
+ *  - Every call returns BO_OK (0) or a negative BO_ERR_* code; the message of
+ *    the last failure is available from bo_last_error().
+ *  - "_device" entry points take DEVICE pointers and run asynchronously on the
+ *    context's stream (capturable in a CUDA graph); "_host" entry points take
+ *    HOST pointers, copy inputs in, run, copy results out and synchronise.
+ *  - One context per host thread.  All work of a context is ordered on its
+ *    stream; a context's scratch state is shared by its calls, so two calls of
+ *    the same context must not run concurrently on different streams.
+ *  - All aggregates are exact integer / fixed-point arithmetic (int64, with
+ *    128-bit totals where the reference uses __int128).
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths relative to the DataManagementLab/BespokeOLAP_Artifacts tree).
+ */
+#ifndef BESPOKE_GPU_H
+#define BESPOKE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+enum {
+  BO_OK = 0,
+  BO_ERR_INVALID = -1,     /* bad argument (null pointer, misalignment, bad size) */
+  BO_ERR_OOM = -2,         /* device or pinned-host allocation failed */
+  BO_ERR_OVERFLOW = -3,    /* a presized table/buffer overflowed and retries ran out */
+  BO_ERR_TIMEOUT = -4,     /* a bounded device-side wait gave up */
+  BO_ERR_CUDA = -5,        /* a CUDA runtime call failed */
+  BO_ERR_DATA = -6,        /* input data violates the layout contract (e.g. group code) */
+  BO_ERR_UNSUPPORTED = -7  /* no GPU / wrong architecture */
+};
+
+typedef struct bo_ctx bo_ctx;
+
+/* Signed 128-bit integer as two 64-bit words (value = hi * 2^64 + lo). */
+typedef struct bo_i128 {
+  uint64_t lo;
+  int64_t hi;
+} bo_i128;
+
+/* ------------------------------------------------------------- context ---- */
+/* Replaces the process-level set-up the reference's external driver does
+ * before query() (bespoke_tpch/query_impl.cpp:142-143: pin to one core). */
+int bo_create(bo_ctx** out, int device);
+void bo_destroy(bo_ctx* ctx);
+const char* bo_last_error(const bo_ctx* ctx);
+/* Use an external CUDA stream (cudaStream_t passed as void*); NULL restores the
+ * context's own stream. */
+int bo_set_stream(bo_ctx* ctx, void* cuda_stream);
+void* bo_get_stream(const bo_ctx* ctx);
+int bo_synchronize(bo_ctx* ctx);
+int bo_num_sms(const bo_ctx* ctx);
+/* Library version / build string (architecture it was compiled for). */
+const char* bo_build_info(void);
+
+/* Device / pinned memory helpers so C and C++ callers need no CUDA headers. */
+int bo_device_alloc(bo_ctx* ctx, size_t bytes, void** out);
+int bo_device_free(bo_ctx* ctx, void* ptr);
+int bo_host_alloc_pinned(bo_ctx* ctx, size_t bytes, void** out);
+int bo_host_free_pinned(bo_ctx* ctx, void* ptr);
+int bo_copy_h2d(bo_ctx* ctx, void* dst_device, const void* src_host, size_t bytes);
+int bo_copy_d2h(bo_ctx* ctx, void* dst_host, const void* src_device, size_t bytes);
+/* Kernels launched by this library since the context was created (counted on
+ * the host at each launch). */
+int64_t bo_launch_count(const bo_ctx* ctx);
+
+/* ===================================================================== Q1 ==
+ * Scan + filter + low-cardinality group-by aggregation.
+ * Replaces run_q1 (bespoke_tpch/query_q1.cpp:104-283, declared
+ * bespoke_tpch/query_q1.hpp:22) and its accumulator Q1Agg (query_q1.cpp:27-34).
+ */
+#define BO_Q1_MAX_GROUPS 8
+
+/* Per-group exact totals.  Scales: quantity/price x100, discount/tax x100.
+ *   sum_disc_price        = sum trunc(price*(100-disc)/100)        (x100)   reference form
+ *   sum_charge            = sum trunc(price*(100-disc)/100)*(100+tax) (x1e4) reference sum_charge_num
+ *   sum_disc_price_exact  = sum price*(100-disc)                   (x1e4)   exact form
+ *   sum_charge_exact      = sum price*(100-disc)*(100+tax)         (x1e6)   exact form
+ * In the storage-plan layout "trunc(price*(100-disc)/100)" is the stored
+ * discounted_price column (bespoke_tpch/builder_impl.cpp:522-532). */
+typedef struct bo_q1_agg {
+  int64_t count;
+  int64_t sum_qty;
+  int64_t sum_base_price;
+  int64_t sum_disc;
+  int64_t sum_disc_price;
+  int64_t sum_disc_price_exact;
+  bo_i128 sum_charge;
+  bo_i128 sum_charge_exact;
+} bo_q1_agg;
+
+/* Fact table in the declared wide layout (38 B/row): ship_date int32 days since
+ * 1970-01-01; quantity/ext_price int64 x100; discount/tax int64 x100 in
+ * [0,100]; flag_a/flag_b uint8 group flags.  Every pointer 16-byte aligned. */
+typedef struct bo_fact_cols {
+  const int32_t* ship_date;
+  const int64_t* quantity;
+  const int64_t* ext_price;
+  const int64_t* discount;
+  const int64_t* tax;
+  const uint8_t* flag_a;
+  const uint8_t* flag_b;
+  int64_t n_rows;
+} bo_fact_cols;
+
+/* Lineitem columns in the reference storage-plan layout (15 B/row,
+ * bespoke_tpch/builder_impl.hpp:39-66): shipdate int16 offset from 1992-01-01,
+ * returnflag_linestatus uint8 code, extendedprice int32 x100, discounted_price
+ * int32 x100, discount uint8, tax uint8, quantity int16 x100. */
+typedef struct bo_lineitem_cols {
+  const int16_t* shipdate;
+  const uint8_t* returnflag_linestatus;
+  const int32_t* extendedprice;
+  const int32_t* discounted_price;
+  const uint8_t* discount;
+  const uint8_t* tax;
+  const int16_t* quantity;
+  int64_t n_rows;
+} bo_lineitem_cols;
+
+/* Wide layout: keep rows with ship_date <= ship_cutoff; group code =
+ * flag_a * n_flag_b + flag_b (must be < n_flag_a*n_flag_b <= 8).
+ * out_device receives n_flag_a*n_flag_b bo_q1_agg entries indexed by code. */
+int bo_q1_fact_device(bo_ctx* ctx, const bo_fact_cols* cols, int32_t ship_cutoff,
+                      int32_t n_flag_a, int32_t n_flag_b, bo_q1_agg* out_device);
+int bo_q1_fact_host(bo_ctx* ctx, const bo_fact_cols* host_cols, int32_t ship_cutoff,
+                    int32_t n_flag_a, int32_t n_flag_b, bo_q1_agg* out_host);
+
+/* Storage-plan layout: keep rows with shipdate <= cutoff_offset (the int16
+ * cutoff run_q1 derives at query_q1.cpp:111-115); n_groups =
+ * returnflag_count * linestatus_count (<= 8). */
+int bo_q1_lineitem_device(bo_ctx* ctx, const bo_lineitem_cols* cols, int16_t cutoff_offset,
+                          int32_t n_groups, bo_q1_agg* out_device);
+int bo_q1_lineitem_host(bo_ctx* ctx, const bo_lineitem_cols* host_cols, int16_t cutoff_offset,
+                        int32_t n_groups, bo_q1_agg* out_host);
+
+/* ===================================================================== Q6 ==
+ * Range predicates + scalar sum.  Replaces run_q6
+ * (bespoke_tpch/query_q6.cpp:155-397, declared query_q6.hpp:15): keeps rows with
+ * start <= shipdate < end, disc_min <= discount <= disc_max, quantity < qty_limit
+ * and returns revenue_raw = sum extendedprice*discount (x1e4) and the row count. */
+typedef struct bo_q6_result {
+  int64_t revenue_raw;
+  int64_t count;
+} bo_q6_result;
+
+int bo_q6_lineitem_device(bo_ctx* ctx, const bo_lineitem_cols* cols, int16_t start_offset,
+                          int16_t end_offset, int32_t disc_min, int32_t disc_max,
+                          int32_t qty_limit, bo_q6_result* out_device);
+int bo_q6_lineitem_host(bo_ctx* ctx, const bo_lineitem_cols* host_cols, int16_t start_offset,
+                        int16_t end_offset, int32_t disc_min, int32_t disc_max,
+                        int32_t qty_limit, bo_q6_result* out_host);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BESPOKE_GPU_H */

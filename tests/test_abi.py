@@ -1,0 +1,67 @@
+"""The C ABI library loads and exports every entry point its headers declare
+(no compute calls: these run without a GPU)."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADERS = sorted((ROOT / "include").glob("*.h"))
+
+
+def declared_symbols():
+    names = set()
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b(bo_\w+)\s*\(", text, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_headers_declare_entry_points():
+    syms = declared_symbols()
+    assert "bo_create" in syms and "bo_q1_fact_device" in syms
+    assert len(syms) >= 20
+
+
+def test_library_exports_every_declared_symbol():
+    from bespokeolap_artifacts_b200 import native
+
+    lib = native.lib()
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_every_declared_symbol():
+    from bespokeolap_artifacts_b200 import native
+
+    native.lib()
+    missing = [s for s in declared_symbols() if s not in native._SIGNATURES]
+    assert not missing, missing
+
+
+def test_build_info_names_sm100a():
+    from bespokeolap_artifacts_b200 import native
+
+    assert b"sm_100a" in native.lib().bo_build_info()
+
+
+def test_create_without_gpu_reports_unsupported():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    from bespokeolap_artifacts_b200 import native
+
+    with pytest.raises(native.BoError) as e:
+        native.Context(0)
+    assert e.value.status == -7
+
+
+def test_null_context_is_rejected():
+    from bespokeolap_artifacts_b200 import native
+
+    lib = native.lib()
+    assert lib.bo_synchronize(None) == -1
+    assert lib.bo_q1_fact_device(None, None, 0, 3, 2, None) == -1
+    assert lib.bo_last_error(None) == b"null context"
