@@ -1,0 +1,463 @@
+#!/usr/bin/env python
+"""Benchmark: filtered hash join + scalar aggregate, learned-sized form.
+
+Workload (one step = one query): a 1,500,000-row build side (unique int32 keys,
+int32 date filtered to ~20%, uint8 segment equality) joined with a
+6,000,000-row probe side (int32 foreign keys, int64 price and discount x100);
+result = match count, sum price*(100-discount) and sum trunc(price*(100-discount)/100).
+The learned form sizes the hash table on the device from the MLP's prediction
+(no host round trip); the plain form runs the exact-count pre-pass first.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Prints one JSON line (rank 0).  For N > 1 (torchrun) every rank runs an
+independent replica of the workload on its own GPU (the path needs no
+collective); value = rows processed by all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Pipeline rows/s & % HBM peak: learned-sized vs plain GPU vs CPU ref, exact"
+N_BUILD, N_PROBE = 1_500_000, 6_000_000
+ROWS_PER_STEP = N_BUILD + N_PROBE
+PROBE_BYTES = N_PROBE * 20          # fk int32 + price int64 + discount int64
+BUILD_BYTES = N_BUILD * 9           # key int32 + date int32 + segment uint8
+WORKLOAD = ("filtered hash join + scalar aggregate: build 1,500,000 rows (int32 key, int32 date < D "
+            "~20%, uint8 segment == s) x probe 6,000,000 rows (int32 fk, int64 price, int64 discount)")
+PROFILE = ROOT / "profiles" / "join_probe_kernel_build1.5M_probe6M.md"
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def profile_traffic() -> int | None:
+    """dram__bytes_read.sum + dram__bytes_write.sum per probe launch, from the
+    committed ncu summary."""
+    if not PROFILE.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*(\d+)", PROFILE.read_text())
+    return int(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ engine --
+def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
+    import torch
+
+    from bespokeolap_artifacts_b200 import datagen as dg
+    from bespokeolap_artifacts_b200 import learned as L
+    from bespokeolap_artifacts_b200 import native as N
+    from bespokeolap_artifacts_b200.engine import Engine
+
+    torch.cuda.set_device(local_rank)
+    eng = Engine(local_rank)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    eng.set_stream(stream.cuda_stream)
+
+    # Three input copies rotated between steps (3 x 133.5 MB > 126 MB L2).
+    copies = []
+    for c in range(3):
+        j = dg.gen_join(N_BUILD, N_PROBE, seed=1000 * rank + c)
+        b = [torch.from_numpy(a).cuda() for a in (j.b_key, j.b_date, j.b_seg)]
+        p = [torch.from_numpy(a).cuda() for a in (j.p_fk, j.p_price, j.p_disc)]
+        st = L.join_table_stats(eng.ctx, b[0], b[1], b[2], j.n_build)   # load-time sketches
+        copies.append(dict(j=j, b=b, p=p, st=st))
+
+    # Learned sizer: trained on the GPU from plain-pipeline counts (seeded tables).
+    x, t, _ = L.make_join_training_set(eng, n_tables=24, preds_per_table=40, seed=4242, n_max=2_000_000)
+    sizer = L.JoinSizer(eng, seed=5)
+    sizer.fit(x, t, epochs=3000, lr=2e-3)
+    feats = [L.join_features(c["st"], c["j"].date_lt, c["j"].seg_eq) for c in copies]
+    exact_rows = []
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for c in copies:
+        eng.join_count_device(c["b"], N_BUILD, c["j"].date_lt, c["j"].seg_eq, cnt)
+        eng.synchronize()
+        exact_rows.append(int(cnt.item()))
+
+    res_sz = C.sizeof(N.JoinResult)
+    K, W = args.steps, args.warmup
+    results = torch.zeros((K + W) * res_sz, dtype=torch.uint8, device="cuda")
+    preds = torch.zeros(K + W, dtype=torch.float32, device="cuda")
+
+    def learned_step(i, slot):
+        c = copies[i % 3]
+        j = c["j"]
+        sizer.predict_device(feats[i % 3], preds[slot:slot + 1])
+        eng.join_presized_device(c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq, preds[slot:slot + 1],
+                                 results[slot * res_sz:(slot + 1) * res_sz])
+
+    def check(slots):
+        host = results.cpu().numpy().tobytes()
+        out = []
+        for s in slots:
+            r = N.JoinResult.from_buffer_copy(host[s * res_sz:(s + 1) * res_sz]).as_dict()
+            out.append(r)
+        return out
+
+    # ---- warm-up
+    for i in range(W):
+        learned_step(i, i)
+    torch.cuda.synchronize()
+
+    # ---- timed: K learned-sized queries, inputs resident, device-timed
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    launches0 = eng.launches
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for i in range(K):
+        learned_step(i, W + i)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = eng.launches - launches0
+    ms = ev0.elapsed_time(ev1)
+    # Any query whose presized table overflowed is rerun exactly (counted in time).
+    reruns = 0
+    t_fix = time.perf_counter()
+    for k, r in enumerate(check(range(W, W + K))):
+        if r["overflowed"]:
+            c = copies[k % 3]
+            eng.join_plain(c["b"], c["p"], N_BUILD, N_PROBE, c["j"].date_lt, c["j"].seg_eq)
+            reruns += 1
+    ms += (time.perf_counter() - t_fix) * 1e3 if reruns else 0.0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    rs = check(range(W, W + K))
+    for k, r in enumerate(rs):  # same copy -> same answer every time
+        assert r["match_count"] == rs[k % 3]["match_count"] and r["sum_exact"] == rs[k % 3]["sum_exact"]
+    if dist:
+        import torch.distributed as td
+
+        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        td.all_reduce(tt, op=td.ReduceOp.MAX)
+        ms = float(tt.item())
+
+    # ---- per-query latency: learned vs plain (results on the host each time)
+    def per_query(fn, n):
+        ts = []
+        for i in range(n):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn(i)
+            t1 = time.perf_counter()
+            ts.append((t1 - t0) * 1e3)
+        return statistics.median(ts)
+
+    def learned_query(i):
+        c = copies[i % 3]
+        j = c["j"]
+        sizer.predict_device(feats[i % 3], preds[0:1])
+        return eng.join_presized(c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq, preds[0:1])
+
+    def plain_query(i):
+        c = copies[i % 3]
+        j = c["j"]
+        return eng.join_plain(c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq)
+
+    for i in range(3):
+        learned_query(i)
+        plain_query(i)
+    lat_learned = per_query(learned_query, max(K, 10))
+    lat_plain = per_query(plain_query, max(K, 10))
+
+    # ---- roofline of the dominant kernel (probe), timed alone on the stream
+    outp = torch.zeros(res_sz, dtype=torch.uint8, device="cuda")
+    c0 = copies[(W + K - 1) % 3]
+    pev = []
+    for i in range(K + 3):
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.join_probe_device(copies[(W + K - 1) % 3]["p"], N_PROBE, outp)
+        e.record(stream)
+        pev.append((a, e))
+    torch.cuda.synchronize()
+    probe_ms = statistics.mean(a.elapsed_time(e) for a, e in pev[3:])
+    peak, peak_kind = peaks()
+    achieved = PROBE_BYTES / (probe_ms * 1e-3) / 1e9
+    traffic = profile_traffic()
+
+    # ---- end to end through the C ABI with pinned host buffers
+    pin = []
+    for c in copies[:1]:
+        j = c["j"]
+        arrs = [j.b_key, j.b_date, j.b_seg, j.p_fk, j.p_price, j.p_disc]
+        pins = []
+        for a in arrs:
+            h = C.c_void_p()
+            eng.ctx.call("bo_host_alloc_pinned", C.c_size_t(a.nbytes), C.byref(h))
+            C.memmove(h.value, a.ctypes.data, a.nbytes)
+            pins.append(h.value)
+        pin.append(pins)
+    dbufs = [torch.empty_like(x) for x in copies[0]["b"] + copies[0]["p"]]
+    res_host = N.JoinResult()
+    j0 = copies[0]["j"]
+    h2d = sum(a.nbytes for a in (j0.b_key, j0.b_date, j0.b_seg, j0.p_fk, j0.p_price, j0.p_disc))
+
+    def e2e_step():
+        for src, dst in zip(pin[0], dbufs):
+            eng.ctx.call("bo_copy_h2d", C.c_void_p(dst.data_ptr()), C.c_void_p(src), C.c_size_t(dst.nbytes))
+        sizer.predict_device(feats[0], preds[0:1])
+        eng.join_presized_device(dbufs[:3], dbufs[3:], N_BUILD, N_PROBE, j0.date_lt, j0.seg_eq, preds[0:1],
+                                 results[0:res_sz])
+        eng.ctx.call("bo_copy_d2h", C.byref(res_host), C.c_void_p(results.data_ptr()), C.c_size_t(res_sz))
+        if res_host.overflowed:
+            eng.join_plain(dbufs[:3], dbufs[3:], N_BUILD, N_PROBE, j0.date_lt, j0.seg_eq)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    te = []
+    for _ in range(max(3, min(K, 10))):
+        t0 = time.perf_counter()
+        e2e_step()
+        te.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(te)
+    for pins in pin:
+        for h in pins:
+            eng.ctx.call("bo_host_free_pinned", C.c_void_p(h))
+
+    q_err = [float(L.q_error(sizer.predict_host(f[None, :]), [e])[0]) for f, e in zip(feats, exact_rows)]
+
+    out = None
+    if rank == 0:
+        value = world * K * ROWS_PER_STEP / (ms * 1e-3)
+        out = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "rows/s",
+            "n_gpus": world,
+            "steps": K,
+            "warmup": W,
+            "ms_per_step": ms / K,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "int64",
+            "data": "synthetic (seeded numpy; shapes and distributions of the join config)",
+            "config": {
+                "workload": WORKLOAD,
+                "form": "learned-sized (MLP prediction on device, no host round trip), exact rerun on overflow",
+                "build_rows": N_BUILD, "probe_rows": N_PROBE, "global_batch": ROWS_PER_STEP,
+                "l2": "3 input copies rotated between steps (3 x 133.5 MB > 126 MB L2)",
+                "parallelism": f"replicas x{world}",
+            },
+            "e2e": {"value": ROWS_PER_STEP / e2e_s, "unit": "rows/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": res_sz,
+                    "path": "bo_copy_h2d (pinned) + bo_mlp_predict_counts + bo_join_presized_device + bo_copy_d2h"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "join_probe_kernel", "achieved": achieved, "peak": peak,
+                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst)", "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": PROBE_BYTES, "avg_launch_us": probe_ms * 1e3},
+            "learned_vs_plain": {"learned_ms_per_query": lat_learned, "plain_ms_per_query": lat_plain,
+                                 "speedup": lat_plain / lat_learned, "q_error": q_err, "reruns": reruns,
+                                 "note": "per-query latency, result on the host each query"},
+            "clocks": clocks,
+        }
+        try:
+            out["cpu_baseline"] = cpu_baseline(copies[0]["j"])
+        except Exception as e:  # the reference harness is a prebuilt file; report, never fail the bench
+            out["cpu_baseline"] = {"value": None, "unit": "rows/s", "error": str(e)[:200]}
+    eng.close()
+    return out
+
+
+def cpu_baseline(j) -> dict:
+    """The reference's run_q3 (compiled unchanged into oracle/_ref) on the same
+    input mapped onto its tables, on one host core (the reference pins queries
+    to one core)."""
+    from bespokeolap_artifacts_b200 import datagen as dg
+    from oracle import oracle as O
+
+    tables, a = dg.join_as_q3_tables(j)
+    db = O.RefDatabase(tables)
+    db.q3(a["segment"], a["date"])
+    ts = []
+    t_end = time.perf_counter() + 10.0
+    while time.perf_counter() < t_end and len(ts) < 30:
+        ts.append(db.q3(a["segment"], a["date"])["ms"])
+    db.close()
+    med = statistics.median(ts)
+    return {"value": ROWS_PER_STEP / (med * 1e-3), "unit": "rows/s", "cores": 1, "kind": "reference",
+            "ms_per_query": med,
+            "sample": f"run_q3 on the full join input mapped to customer/orders/lineitem, {len(ts)} runs "
+                      f"(median), host {host_cpu()}"}
+
+
+def host_cpu() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return f"{ln.split(':', 1)[1].strip()}, {os.cpu_count()} threads"
+    except Exception:
+        pass
+    return f"{os.cpu_count()} threads"
+
+
+# --------------------------------------------------------------- reference --
+def run_reference(args) -> dict:
+    """The reference's own run_q3 on all host cores: the input is split into
+    key-range shards (sums are decomposable), one reference Database and one
+    host thread per shard."""
+    from bespokeolap_artifacts_b200 import datagen as dg
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "compiled reference harness oracle/_ref/libref_tpch.so missing"}
+    j = dg.gen_join(N_BUILD, N_PROBE, seed=0)
+    T = max(1, min(os.cpu_count() or 1, 16))
+    edges = np.linspace(0, N_BUILD + 1, T + 1).astype(np.int64)
+    dbs = []
+    a = None
+    for t in range(T):
+        lo, hi = edges[t], edges[t + 1]
+        bm = (j.b_key >= lo) & (j.b_key < hi)
+        pm = (j.p_fk >= lo) & (j.p_fk < hi)
+        sub = dg.JoinInput(j.b_key[bm], j.b_date[bm], j.b_seg[bm], j.p_fk[pm], j.p_price[pm], j.p_disc[pm],
+                           j.date_lt, j.seg_eq)
+        tables, a = dg.join_as_q3_tables(sub)
+        dbs.append(O.RefDatabase(tables))
+    for _ in range(args.warmup):
+        O.ref_parallel(dbs, 3, segment=a["segment"], date=a["date"])
+    ts = []
+    for _ in range(args.steps):
+        ms, _ = O.ref_parallel(dbs, 3, segment=a["segment"], date=a["date"])
+        ts.append(ms)
+    for d in dbs:
+        d.close()
+    total_ms = sum(ts)
+    value = args.steps * ROWS_PER_STEP / (total_ms * 1e-3)
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "build_rows": N_BUILD, "probe_rows": N_PROBE,
+                   "global_batch": ROWS_PER_STEP, "parallelism": f"{T} host threads, key-range shards"},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": T, "kind": "reference",
+                         "sample": f"full input each step, {T} shards of run_q3, host {host_cpu()}"},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+
+        torch.cuda.set_device(local_rank)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = td
+    out = run_engine(args, rank, world, local_rank, dist)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

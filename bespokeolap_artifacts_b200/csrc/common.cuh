@@ -52,6 +52,30 @@ __device__ __forceinline__ uint32_t ld_stream_u32(const void* p) {
   return v;
 }
 
+// 256-bit streaming loads (sm_100): one full 32-byte sector per lane per
+// instruction, so a warp consumes whole sectors whatever its lane stride.
+struct int8v {
+  int v[8];
+};
+__device__ __forceinline__ int8v ld_stream_v8(const void* p) {
+  int8v r;
+  asm volatile("ld.global.nc.L1::no_allocate.v8.s32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]),
+                 "=r"(r.v[6]), "=r"(r.v[7])
+               : "l"(p));
+  return r;
+}
+struct long4v {
+  long long v[4];
+};
+__device__ __forceinline__ long4v ld_stream_v4x64(const void* p) {
+  long4v r;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.s64 {%0,%1,%2,%3}, [%4];"
+               : "=l"(r.v[0]), "=l"(r.v[1]), "=l"(r.v[2]), "=l"(r.v[3])
+               : "l"(p));
+  return r;
+}
+
 __device__ __forceinline__ int64_t make_i64(int lo, int hi) {
   return (int64_t)(((uint64_t)(uint32_t)hi << 32) | (uint32_t)lo);
 }
@@ -119,5 +143,98 @@ __device__ __host__ __forceinline__ uint32_t hash32(uint32_t k) {
   k ^= k >> 16;
   return k;
 }
+
+// --------------------------------------------------- 128-bit helpers ------
+__device__ __forceinline__ __int128 load_i128(const unsigned long long* p) {
+  const uint64_t lo = __ldcg(p), hi = __ldcg(p + 1);
+  return (__int128)(((unsigned __int128)hi << 64) | lo);
+}
+
+__device__ __forceinline__ int64_t narrow_i64(__int128 v, uint32_t& bad) {
+  if (v != (__int128)(int64_t)v) bad |= kErrSumOverflow;
+  return (int64_t)v;
+}
+
+__device__ __forceinline__ bo_i128 to_bo_i128(__int128 v) {
+  bo_i128 r;
+  r.lo = (uint64_t)v;
+  r.hi = (int64_t)(v >> 64);
+  return r;
+}
+
+// Sum of an unsigned 128-bit value over the block, returned in thread 0.
+// `scratch` holds blockDim.x + 32 entries.  Warp leaders add their warp's
+// values serially in 128 bits, thread 0 adds the warp totals: exact for any
+// inputs, and cheap because it runs once per block.
+__device__ __forceinline__ unsigned __int128 block_sum_u128(unsigned __int128 v, unsigned __int128* scratch) {
+  scratch[threadIdx.x] = v;
+  __syncthreads();
+  const int nw = (int)(blockDim.x >> 5);
+  if ((threadIdx.x & 31) == 0) {
+    unsigned __int128 t = 0;
+    for (int i = 0; i < 32; ++i) t += scratch[threadIdx.x + i];
+    scratch[blockDim.x + (threadIdx.x >> 5)] = t;
+  }
+  __syncthreads();
+  unsigned __int128 tot = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < nw; ++w) tot += scratch[blockDim.x + w];
+  __syncthreads();
+  return tot;
+}
+
+// Last-block epilogue: true in every thread of the block that finished last
+// (all other blocks' global atomics are then visible to it).
+__device__ __forceinline__ bool last_block(uint32_t* done) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) is_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (is_last) __threadfence();
+  return is_last;
+}
+
+// ------------------------------------------- TMA bulk copies (no multicast) --
+// One-shot global -> shared bulk copy completed on an mbarrier.  Only this
+// CTA's shared memory and this GPU's global memory are involved.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false if the phase did not complete within limit_ns.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (global_ns() - t0 > limit_ns) return false;
+  }
+  return true;
+}
+
+constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s bound on any device-side wait
 
 }  // namespace bo

@@ -66,5 +66,7 @@ int device_error_status(bo_ctx* ctx, uint32_t bits, const char* op);
 int occupancy_blocks(const void* kernel, int block, size_t smem);
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+// Column pointers must be 32-byte aligned: the scans use 256-bit vector loads.
+inline bool aligned32(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 31u) == 0; }
 
 }  // namespace bo

@@ -1,0 +1,681 @@
+// Filtered hash join + scalar aggregate (filtered-join shape of run_q3,
+// bespoke_tpch/query_q3.cpp:182-260).
+//
+// Pipeline (all on the context's stream):
+//   count  (K7, plain form only)  number of qualifying build rows -> host sizes
+//                                  the table from the exact count;
+//   init                           picks the table capacity (from the host's
+//                                  exact count, or on the device from a
+//                                  predicted row count), clears the slots and
+//                                  the Bloom filter;
+//   build  (K2)                    filter build rows, insert keys with 64-bit
+//                                  atomicCAS into open-addressing slots
+//                                  (key << 32 | multiplicity), set 2 bits of a
+//                                  blocked Bloom filter per new key;
+//   probe  (K3)                    each block stages the 64 KB Bloom filter into
+//                                  shared memory with one TMA bulk copy; probe
+//                                  rows stream in 16 at a time (four 128-bit fk
+//                                  loads); a Bloom hit looks the key up in the
+//                                  table; only matching rows load their price and
+//                                  discount (late materialisation); exact
+//                                  fixed-point sums, 128-bit totals, last block
+//                                  writes the result.
+// Build-side keys are also late-materialised: only qualifying rows load their key.
+#include <algorithm>
+
+#include "common.cuh"
+#include "context.cuh"
+
+namespace bo {
+
+constexpr unsigned long long kEmptySlot = ~0ull;
+constexpr int kBloomLog2Words = 14;  // 16384 32-bit words = 64 KB = 2^19 bits
+constexpr uint32_t kBloomWords = 1u << kBloomLog2Words;
+constexpr uint32_t kBloomBytes = kBloomWords * 4u;
+constexpr int kJoinBlock = 512;
+constexpr int kBuildBlock = 256;
+constexpr int kMinCapLog2 = 10;
+constexpr float kPresizeFactor = 2.5f;  // slots per predicted row (load <= 0.4 at exact prediction)
+
+// Device-resident join state (one per context, in the "join_meta" region).
+struct JoinMeta {
+  int32_t cap_log2;
+  uint32_t done;               // probe ticket counter
+  uint32_t overflow;           // presized table too small
+  uint32_t pad;
+  unsigned long long build_rows;
+  unsigned long long distinct;
+  unsigned long long acc[6];   // 128-bit totals: matches, sum T, sum rr
+  unsigned long long count;    // K7 output
+};
+
+__device__ __forceinline__ void bloom_pos(uint32_t h, uint32_t& word, uint32_t& bits) {
+  const uint32_t h2 = h * 0x9E3779B1u + 0x7F4A7C15u;
+  word = h2 >> (32 - kBloomLog2Words);
+  bits = (1u << (h2 & 31u)) | (1u << ((h2 >> 5) & 31u));
+}
+
+// Row qualifies on the build side (date < date_lt and segment == seg).
+__device__ __forceinline__ bool build_qual(int32_t date, uint32_t seg_byte, int32_t date_lt, uint32_t seg) {
+  return date < date_lt && seg_byte == seg;
+}
+
+// ------------------------------------------------------------ K7 count ----
+__global__ void __launch_bounds__(kBuildBlock) join_count_kernel(bo_join_build_cols b, int32_t date_lt, uint32_t seg,
+                                                                 unsigned long long* count) {
+  uint32_t c = 0;
+  const int64_t n = b.n_rows, chunks = n >> 2;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t ch = tid; ch < chunks; ch += stride) {
+    const int4 d = ld_stream_v4(b.date + (ch << 2));
+    const uint32_t s = ld_stream_u32(b.segment + (ch << 2));
+    c += build_qual(d.x, s & 0xffu, date_lt, seg) + build_qual(d.y, (s >> 8) & 0xffu, date_lt, seg) +
+         build_qual(d.z, (s >> 16) & 0xffu, date_lt, seg) + build_qual(d.w, s >> 24, date_lt, seg);
+  }
+  const int64_t t = (chunks << 2) + tid;
+  if (t < n) c += build_qual(b.date[t], b.segment[t], date_lt, seg);
+  // One atomic per block: per-warp atomics on a single counter serialise in L2.
+  __shared__ uint32_t part[kBuildBlock / 32];
+  c = warp_sum_u32(c);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t tot = 0;
+    for (int w = 0; w < kBuildBlock / 32; ++w) tot += part[w];
+    if (tot) atomicAdd(count, (unsigned long long)tot);
+  }
+}
+
+// ------------------------------------------------------------ init -------
+// Capacity: host-chosen (exact count) or, when `pred` is given, derived on the
+// device from the predicted qualifying-row count: the smallest power of two
+// >= kPresizeFactor * pred, clamped to [2^kMinCapLog2, 2^max_log2].  Every block
+// computes the same value, so no cross-block handshake is needed.
+__device__ __forceinline__ int32_t presize_log2(const float* pred, int32_t host_log2, int32_t max_log2) {
+  if (!pred) return host_log2;
+  float p = *pred;
+  if (!(p >= 0.0f)) p = 0.0f;  // NaN / negative predictions size for the minimum
+  const double want = (double)p * kPresizeFactor;
+  int32_t cl = kMinCapLog2;
+  while (cl < max_log2 && (double)(1ull << cl) < want) ++cl;
+  return cl;
+}
+
+__global__ void join_init_kernel(unsigned long long* slots, uint32_t* bloom, JoinMeta* meta, const float* pred,
+                                 int32_t host_log2, int32_t max_log2) {
+  const int32_t cl = presize_log2(pred, host_log2, max_log2);
+  const uint64_t cap = 1ull << cl;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  ulonglong2* s2 = reinterpret_cast<ulonglong2*>(slots);
+  for (uint64_t i = tid; i < cap / 2; i += stride) s2[i] = make_ulonglong2(kEmptySlot, kEmptySlot);
+  uint4* b4 = reinterpret_cast<uint4*>(bloom);
+  for (uint64_t i = tid; i < kBloomWords / 4; i += stride) b4[i] = make_uint4(0, 0, 0, 0);
+  if (tid == 0) {
+    meta->cap_log2 = cl;
+    meta->done = 0;
+    meta->overflow = 0;
+    meta->build_rows = 0;
+    meta->distinct = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) meta->acc[i] = 0;
+  }
+}
+
+// ------------------------------------------------------------ K2 build ---
+__device__ __forceinline__ void join_insert(unsigned long long* slots, uint32_t* bloom, uint64_t mask, int32_t key,
+                                            uint32_t& newkeys, bool& full) {
+  const uint32_t h = hash32((uint32_t)key);
+  uint64_t idx = h & mask;
+  const unsigned long long mine = ((unsigned long long)(uint32_t)key << 32) | 1ull;
+  for (uint64_t step = 0; step <= mask; ++step) {
+    const unsigned long long old = atomicCAS(slots + idx, kEmptySlot, mine);
+    if (old == kEmptySlot) {
+      ++newkeys;
+      uint32_t w, bits;
+      bloom_pos(h, w, bits);
+      atomicOr(bloom + w, bits);
+      return;
+    }
+    if ((uint32_t)(old >> 32) == (uint32_t)key) {
+      atomicAdd(slots + idx, 1ull);  // multiplicity lives in the low word
+      return;
+    }
+    idx = (idx + 1) & mask;
+  }
+  full = true;
+}
+
+// 16 build rows per thread per step: one 128-bit segment load and four 128-bit
+// date loads; the qualifying rows (about 4%) of the whole warp are then
+// compacted into a shared-memory queue and their keys loaded and inserted by
+// all lanes together.
+constexpr int kBuildRowsPerThread = 16;
+
+__device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t v, uint32_t& total) {
+  const int lane = threadIdx.x & 31;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+__global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_cols b, int32_t date_lt, uint32_t seg,
+                                                                 unsigned long long* slots, uint32_t* bloom,
+                                                                 JoinMeta* meta) {
+  // Read-only for this kernel (written by the init kernel): the L1-cached path
+  // avoids every warp hitting the same L2 sector.
+  const int32_t cl = __ldg(&meta->cap_log2);
+  const uint64_t mask = (1ull << cl) - 1;
+  uint32_t qual = 0, newkeys = 0;
+  bool full = false;
+  __shared__ uint32_t build_q[kBuildBlock / 32][32 * 8];
+  const int lane = threadIdx.x & 31;
+  uint32_t* bq = build_q[threadIdx.x >> 5];
+  const int64_t n = b.n_rows;
+  const int64_t steps = (n + kBuildRowsPerThread - 1) / kBuildRowsPerThread;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  // Every lane of a warp runs the same number of iterations (the bound is
+  // rounded up to whole warps) so the warp-wide queue steps stay converged;
+  // lanes past the end simply contribute no rows.
+  const int64_t steps_w = (steps + 31) & ~int64_t(31);
+  for (int64_t st = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; st < steps_w; st += stride) {
+    const int64_t r0 = st * kBuildRowsPerThread;
+    const int64_t wbase = (st - lane) * kBuildRowsPerThread;
+    uint32_t q = 0;
+    if (r0 >= n) {
+      // past the end: no rows
+    } else if (r0 + kBuildRowsPerThread <= n) {
+      const int4 sg = ld_stream_v4(b.segment + r0);
+      const uint32_t sw[4] = {(uint32_t)sg.x, (uint32_t)sg.y, (uint32_t)sg.z, (uint32_t)sg.w};
+      const int8v d0 = ld_stream_v8(b.date + r0), d1 = ld_stream_v8(b.date + r0 + 8);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const int32_t dk = k < 8 ? d0.v[k] : d1.v[k - 8];
+        q |= (uint32_t)build_qual(dk, (sw[k >> 2] >> (8 * (k & 3))) & 0xffu, date_lt, seg) << k;
+      }
+    } else {
+      for (int k = 0; k < kBuildRowsPerThread; ++k)
+        if (r0 + k < n && build_qual(b.date[r0 + k], b.segment[r0 + k], date_lt, seg)) q |= 1u << k;
+    }
+    qual += __popc(q);
+    // Compact the qualifying rows of the whole warp into its queue so the key
+    // loads and CAS insertions spread over all 32 lanes: a lane whose rows all
+    // qualify would otherwise chain up to 16 dependent round trips.
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const uint32_t hm = (q >> (8 * half)) & 0xffu;
+      uint32_t total;
+      uint32_t pos = warp_exclusive_scan(__popc(hm), total);
+      if (total == 0) continue;  // warp-uniform
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if ((hm >> k) & 1u) bq[pos++] = (uint32_t)(r0 - wbase) + 8 * half + k;
+      __syncwarp();
+      for (uint32_t i = lane; i < total; i += 32)
+        join_insert(slots, bloom, mask, __ldg(b.key + wbase + bq[i]), newkeys, full);
+      __syncwarp();
+    }
+  }
+  // Block-level totals, then one atomic per counter per block.
+  __shared__ uint32_t part[3][kBuildBlock / 32];
+  const uint32_t wq = warp_sum_u32(qual), wn = warp_sum_u32(newkeys);
+  const unsigned any_full = __any_sync(0xffffffffu, full);
+  if ((threadIdx.x & 31) == 0) {
+    part[0][threadIdx.x >> 5] = wq;
+    part[1][threadIdx.x >> 5] = wn;
+    part[2][threadIdx.x >> 5] = any_full;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t tq = 0, tn = 0, tf = 0;
+    for (int w = 0; w < kBuildBlock / 32; ++w) {
+      tq += part[0][w];
+      tn += part[1][w];
+      tf |= part[2][w];
+    }
+    if (tq) atomicAdd(&meta->build_rows, (unsigned long long)tq);
+    if (tn) {
+      const unsigned long long before = atomicAdd(&meta->distinct, (unsigned long long)tn);
+      // A presized table is "too small" once it is more than 7/8 occupied.
+      if (before + tn > (mask + 1) - ((mask + 1) >> 3)) atomicOr(&meta->overflow, 1u);
+    }
+    if (tf) atomicOr(&meta->overflow, 1u);
+  }
+}
+
+// ------------------------------------------------------------ K3 probe ---
+// With p = 100*q + r and m = 100 - d: trunc(p*m/100) = q*m + (r*m)/100 = T and
+// p*m = 100*T + rr, rr = (r*m) % 100 -- exact forms from the reference form.
+struct ProbeAcc {
+  unsigned long long cnt = 0, rsum = 0;
+  unsigned __int128 tsum = 0;
+  uint32_t bad = 0;
+};
+
+__device__ __forceinline__ void accumulate_match(uint64_t p, uint64_t d, unsigned long long mult, ProbeAcc& a) {
+  if (p >= 0x80000000ull || d > 100u) {
+    a.bad |= kErrValueRange;
+    return;
+  }
+  const uint32_t m = 100u - (uint32_t)d, pq = (uint32_t)p / 100u, pr = (uint32_t)p - pq * 100u;
+  const uint32_t rm = pr * m, rq = rm / 100u, rr = rm - rq * 100u;
+  const uint32_t T = pq * m + rq;
+  a.cnt += mult;
+  a.tsum += (unsigned __int128)((unsigned long long)T * mult);
+  a.rsum += (unsigned long long)rr * mult;
+}
+
+// Linear-probing continuation for the rare key whose first slot held another key.
+__device__ __noinline__ unsigned long long probe_slow(const unsigned long long* slots, uint64_t mask, uint64_t idx,
+                                                      uint32_t key) {
+  for (uint64_t step = 1; step <= mask; ++step) {
+    idx = (idx + 1) & mask;
+    const unsigned long long v = __ldg(slots + idx);
+    if (v == kEmptySlot) return 0;
+    if ((uint32_t)(v >> 32) == key) return v & 0xffffffffull;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ void probe_one(int32_t fk, int64_t row, const uint32_t* bloom_s, bool use_bloom,
+                                          const unsigned long long* slots, uint64_t mask, const int64_t* price,
+                                          const int64_t* disc, ProbeAcc& a) {
+  const uint32_t h = hash32((uint32_t)fk);
+  if (use_bloom) {
+    uint32_t w, bits;
+    bloom_pos(h, w, bits);
+    if ((bloom_s[w] & bits) != bits) return;
+  }
+  const unsigned long long v = __ldg(slots + (h & mask));
+  unsigned long long mult = 0;
+  if (v == kEmptySlot) return;
+  if ((uint32_t)(v >> 32) == (uint32_t)fk)
+    mult = v & 0xffffffffull;
+  else
+    mult = probe_slow(slots, mask, h & mask, (uint32_t)fk);
+  if (mult) accumulate_match((uint64_t)__ldg(price + row), (uint64_t)__ldg(disc + row), mult, a);
+}
+
+// Warp-centric probe.  A warp owns 512 consecutive probe rows per step (16 per
+// lane, four 128-bit fk loads).  Every lane hashes its rows and tests the Bloom
+// filter in shared memory without branching; the hits (about 9% of rows) are
+// compacted into a per-warp shared-memory queue (ballot-free: a warp prefix sum
+// of per-lane hit counts gives each lane its slot range), and then all 32 lanes
+// resolve queue entries together -- table lookups and the price / discount
+// loads of matches are issued by many lanes at once instead of one row at a
+// time.  The queue holds one half-step (8 rows per lane) at most.
+constexpr int kProbeWarps = kJoinBlock / 32;
+constexpr int kRowsPerLane = 16;
+constexpr int kRowsPerWarpStep = 32 * kRowsPerLane;
+constexpr int kQueue = 32 * 8;
+
+__global__ void __launch_bounds__(kJoinBlock) join_probe_kernel(bo_join_probe_cols p,
+                                                                const unsigned long long* slots,
+                                                                const uint32_t* bloom_g, JoinMeta* meta,
+                                                                bo_join_result* out, int32_t mode, uint32_t* err) {
+  extern __shared__ __align__(128) uint32_t bloom_s[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ unsigned __int128 red[kJoinBlock + 32];
+  __shared__ int32_t q_fk[kProbeWarps][kQueue];
+  __shared__ uint16_t q_off[kProbeWarps][kQueue];
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, kBloomBytes);
+    bulk_copy_g2s(bloom_s, bloom_g, kBloomBytes, &bar);
+  }
+  __syncthreads();
+  // On a (never expected) timeout the filter is simply not used: every row then
+  // probes the table directly, which gives the same answer.
+  const bool use_bloom = mbar_wait_bounded(&bar, 0, kWaitLimitNs);
+  ProbeAcc acc;
+  if (!use_bloom) acc.bad |= kErrSpinTimeout;
+
+  const int32_t cl = __ldg(&meta->cap_log2);
+  const uint64_t mask = (1ull << cl) - 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int32_t* qf = q_fk[warp];
+  uint16_t* qo = q_off[warp];
+  const int64_t n = p.n_rows;
+  const int64_t steps = (n + kRowsPerWarpStep - 1) / kRowsPerWarpStep;
+  const int64_t nwarps = (int64_t)gridDim.x * kProbeWarps;
+  for (int64_t st = (int64_t)blockIdx.x * kProbeWarps + warp; st < steps; st += nwarps) {
+    const int64_t base = st * kRowsPerWarpStep;
+    const int64_t r0 = base + lane * kRowsPerLane;
+    int32_t fk[kRowsPerLane];
+    uint32_t valid = 0xffffu;
+    if (r0 + kRowsPerLane <= n) {
+      const int8v f0 = ld_stream_v8(p.fk + r0), f1 = ld_stream_v8(p.fk + r0 + 8);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        fk[k] = f0.v[k];
+        fk[8 + k] = f1.v[k];
+      }
+    } else {
+      valid = 0;
+#pragma unroll
+      for (int k = 0; k < kRowsPerLane; ++k) {
+        fk[k] = 0;
+        if (r0 + k < n) {
+          fk[k] = p.fk[r0 + k];
+          valid |= 1u << k;
+        }
+      }
+    }
+    uint32_t hit = 0;
+#pragma unroll
+    for (int k = 0; k < kRowsPerLane; ++k) {
+      uint32_t w, bits;
+      bloom_pos(hash32((uint32_t)fk[k]), w, bits);
+      const bool cand = !use_bloom || (bloom_s[w] & bits) == bits;
+      hit |= (uint32_t)cand << k;
+    }
+    hit &= valid;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const uint32_t hm = (hit >> (8 * half)) & 0xffu;
+      uint32_t total;
+      uint32_t pos = warp_exclusive_scan(__popc(hm), total);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if ((hm >> k) & 1u) {
+          qf[pos] = fk[8 * half + k];
+          qo[pos] = (uint16_t)(lane * kRowsPerLane + 8 * half + k);
+          ++pos;
+        }
+      }
+      __syncwarp();
+      for (uint32_t i = lane; i < total; i += 32) {
+        const int32_t key = qf[i];
+        const int64_t row = base + qo[i];
+        const uint32_t h = hash32((uint32_t)key);
+        const unsigned long long v = __ldg(slots + (h & mask));
+        unsigned long long mult = 0;
+        if (v != kEmptySlot) {
+          if ((uint32_t)(v >> 32) == (uint32_t)key)
+            mult = v & 0xffffffffull;
+          else
+            mult = probe_slow(slots, mask, h & mask, (uint32_t)key);
+        }
+        if (mult) accumulate_match((uint64_t)__ldg(p.price + row), (uint64_t)__ldg(p.discount + row), mult, acc);
+      }
+      __syncwarp();
+    }
+  }
+  if (!use_bloom) {
+    // The bulk copy may still be in flight: wait for it (bounded) before exit.
+    mbar_wait_bounded(&bar, 0, kWaitLimitNs);
+  }
+  if (acc.bad) raise_error(err, acc.bad);
+  const unsigned long long cnt = acc.cnt, rsum = acc.rsum;
+  const unsigned __int128 tsum = acc.tsum;
+
+  const unsigned __int128 bc = block_sum_u128(cnt, red);
+  const unsigned __int128 bt = block_sum_u128(tsum, red);
+  const unsigned __int128 br = block_sum_u128(rsum, red);
+  if (threadIdx.x == 0) {
+    if (bc) atomic_add_i128(&meta->acc[0], (__int128)bc);
+    if (bt) atomic_add_i128(&meta->acc[2], (__int128)bt);
+    if (br) atomic_add_i128(&meta->acc[4], (__int128)br);
+  }
+  if (last_block(&meta->done)) {
+    if (threadIdx.x == 0) {
+      uint32_t fbad = 0;
+      const __int128 m = load_i128(&meta->acc[0]), t = load_i128(&meta->acc[2]), rr = load_i128(&meta->acc[4]);
+      bo_join_result res;
+      res.build_rows = (int64_t)__ldcg(&meta->build_rows);
+      res.distinct_keys = (int64_t)__ldcg(&meta->distinct);
+      res.match_count = narrow_i64(m, fbad);
+      res.sum_trunc = to_bo_i128(t);
+      res.sum_exact = to_bo_i128(t * 100 + rr);
+      res.capacity_log2 = cl;
+      res.overflowed = (int32_t)__ldcg(&meta->overflow);
+      res.reruns = 0;
+      res.mode = mode;
+      *out = res;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) meta->acc[i] = 0;
+      meta->done = 0;
+      if (fbad) raise_error(err, fbad);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ host ---
+namespace {
+
+struct JoinWs {
+  unsigned long long* slots;
+  uint32_t* bloom;
+  JoinMeta* meta;
+  float* pred;
+  int32_t max_log2;
+};
+
+int ceil_log2(uint64_t v) {
+  int l = 0;
+  while ((1ull << l) < v) ++l;
+  return l;
+}
+
+int join_workspace(bo_ctx* ctx, int64_t n_build, JoinWs* ws) {
+  // The table never needs more than 2 slots per build row (exact sizing uses
+  // 2x the exact count; predictions are clamped to this bound).
+  const int32_t max_log2 = std::max(kMinCapLog2, ceil_log2((uint64_t)std::max<int64_t>(n_build, 1) * 2));
+  void* p = nullptr;
+  int rc = region(ctx, "join_slots", sizeof(unsigned long long) << max_log2, &p);
+  if (rc) return rc;
+  ws->slots = static_cast<unsigned long long*>(p);
+  if ((rc = region(ctx, "join_bloom", kBloomBytes, &p))) return rc;
+  ws->bloom = static_cast<uint32_t*>(p);
+  if ((rc = region(ctx, "join_meta", sizeof(JoinMeta) + 64, &p))) return rc;
+  ws->meta = static_cast<JoinMeta*>(p);
+  ws->pred = reinterpret_cast<float*>(static_cast<char*>(p) + sizeof(JoinMeta));
+  ws->max_log2 = max_log2;
+  return BO_OK;
+}
+
+int check_join(bo_ctx* ctx, const bo_join_build_cols* b, const bo_join_probe_cols* p, const bo_join_params* prm) {
+  if (!b || !p || !prm) return set_error(ctx, BO_ERR_INVALID, "join: null argument");
+  if (b->n_rows < 0 || p->n_rows < 0) return set_error(ctx, BO_ERR_INVALID, "join: negative row count");
+  if (b->n_rows > 0x7fffffffll) return set_error(ctx, BO_ERR_INVALID, "join: build side above 2^31 rows");
+  if (b->n_rows > 0) {
+    const void* bp[] = {b->key, b->date, b->segment};
+    for (const void* x : bp)
+      if (!x || !aligned32(x)) return set_error(ctx, BO_ERR_INVALID, "join: build column null or not 32-byte aligned");
+  }
+  if (p->n_rows > 0) {
+    const void* pp[] = {p->fk, p->price, p->discount};
+    for (const void* x : pp)
+      if (!x || !aligned32(x)) return set_error(ctx, BO_ERR_INVALID, "join: probe column null or not 32-byte aligned");
+  }
+  if (prm->segment_eq < 0 || prm->segment_eq > 255)
+    return set_error(ctx, BO_ERR_INVALID, "join: segment_eq %d outside uint8", prm->segment_eq);
+  return BO_OK;
+}
+
+int grid_for(bo_ctx* ctx, const void* k, int block, size_t smem, int64_t work_items) {
+  const int64_t resident = (int64_t)ctx->num_sms * occupancy_blocks(k, block, smem);
+  int64_t need = (work_items + block - 1) / block;
+  int64_t g = std::min<int64_t>(resident, std::max<int64_t>(need, 1));
+  return (int)std::max<int64_t>(g, 1);
+}
+
+int launch_probe(bo_ctx* ctx, const bo_join_probe_cols& p, const JoinWs& ws, bo_join_result* out, int32_t mode) {
+  const void* k = reinterpret_cast<const void*>(&join_probe_kernel);
+  static bool ready = false;
+  if (!ready) {
+    BO_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBloomBytes));
+    ready = true;
+  }
+  // Enough blocks to fill the GPU, but each thread should see a few 16-row
+  // chunks so the per-block Bloom-filter copy is amortised.
+  const int grid = grid_for(ctx, k, kJoinBlock, kBloomBytes, (p.n_rows + kRowsPerLane - 1) / kRowsPerLane);
+  join_probe_kernel<<<grid, kJoinBlock, kBloomBytes, ctx->stream>>>(p, ws.slots, ws.bloom, ws.meta, out, mode,
+                                                                     ctx->d_err);
+  return after_launch(ctx, "join_probe_kernel");
+}
+
+// init + build + probe, asynchronous.
+int join_run(bo_ctx* ctx, const bo_join_build_cols& b, const bo_join_probe_cols& p, const bo_join_params& prm,
+             const JoinWs& ws, const float* pred, int32_t host_log2, bo_join_result* out, int32_t mode) {
+  const void* ki = reinterpret_cast<const void*>(&join_init_kernel);
+  const int gi = grid_for(ctx, ki, 256, 0, (int64_t)1 << std::min(ws.max_log2, 24));
+  join_init_kernel<<<gi, 256, 0, ctx->stream>>>(ws.slots, ws.bloom, ws.meta, pred, host_log2, ws.max_log2);
+  int rc = after_launch(ctx, "join_init_kernel");
+  if (rc) return rc;
+  const void* kb = reinterpret_cast<const void*>(&join_build_kernel);
+  const int gb = grid_for(ctx, kb, kBuildBlock, 0, (b.n_rows + kBuildRowsPerThread - 1) / kBuildRowsPerThread);
+  join_build_kernel<<<gb, kBuildBlock, 0, ctx->stream>>>(b, prm.date_lt, (uint32_t)prm.segment_eq, ws.slots,
+                                                          ws.bloom, ws.meta);
+  if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
+  return launch_probe(ctx, p, ws, out, mode);
+}
+
+int finish_join(bo_ctx* ctx, bo_join_result* host, const bo_join_result* dev) {
+  BO_CUDA(ctx, cudaMemcpyAsync(host, dev, sizeof(bo_join_result), cudaMemcpyDeviceToHost, ctx->stream));
+  uint32_t bits = 0;
+  int rc = consume_device_errors(ctx, &bits);
+  if (rc) return rc;
+  return device_error_status(ctx, bits, "join");
+}
+
+int join_plain_impl(bo_ctx* ctx, const bo_join_build_cols& b, const bo_join_probe_cols& p, const bo_join_params& prm,
+                    bo_join_result* out_host, int32_t reruns) {
+  JoinWs ws;
+  int rc = join_workspace(ctx, b.n_rows, &ws);
+  if (rc) return rc;
+  // K7: exact count, then one host round trip to size the table.
+  BO_CUDA(ctx, cudaMemsetAsync(&ws.meta->count, 0, sizeof(unsigned long long), ctx->stream));
+  const void* kc = reinterpret_cast<const void*>(&join_count_kernel);
+  const int gc = grid_for(ctx, kc, kBuildBlock, 0, (b.n_rows + 3) / 4);
+  join_count_kernel<<<gc, kBuildBlock, 0, ctx->stream>>>(b, prm.date_lt, (uint32_t)prm.segment_eq, &ws.meta->count);
+  if ((rc = after_launch(ctx, "join_count_kernel"))) return rc;
+  unsigned long long count = 0;
+  BO_CUDA(ctx, cudaMemcpyAsync(&count, &ws.meta->count, sizeof(count), cudaMemcpyDeviceToHost, ctx->stream));
+  BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const int32_t cl = std::min(ws.max_log2, std::max(kMinCapLog2, ceil_log2(std::max<uint64_t>(count, 1) * 2)));
+  void* dout = nullptr;
+  if ((rc = region(ctx, "join_out", sizeof(bo_join_result), &dout))) return rc;
+  bo_join_result* d = static_cast<bo_join_result*>(dout);
+  if ((rc = join_run(ctx, b, p, prm, ws, nullptr, cl, d, 0))) return rc;
+  if ((rc = finish_join(ctx, out_host, d))) return rc;
+  out_host->reruns = reruns;
+  if (out_host->overflowed)  // cannot happen with exact sizing; report rather than loop
+    return set_error(ctx, BO_ERR_OVERFLOW, "join: exact-size table overflowed");
+  return BO_OK;
+}
+
+}  // namespace
+}  // namespace bo
+
+using namespace bo;
+
+extern "C" {
+
+int bo_join_count_device(bo_ctx* ctx, const bo_join_build_cols* b, const bo_join_params* prm, int64_t* count_device) {
+  BO_CHECK_CTX(ctx);
+  if (!b || !prm || !count_device) return set_error(ctx, BO_ERR_INVALID, "join_count: null argument");
+  bo_join_probe_cols none = {};
+  int rc = check_join(ctx, b, &none, prm);
+  if (rc) return rc;
+  BO_CUDA(ctx, cudaMemsetAsync(count_device, 0, sizeof(int64_t), ctx->stream));
+  const void* kc = reinterpret_cast<const void*>(&join_count_kernel);
+  const int gc = grid_for(ctx, kc, kBuildBlock, 0, (b->n_rows + 3) / 4);
+  join_count_kernel<<<gc, kBuildBlock, 0, ctx->stream>>>(*b, prm->date_lt, (uint32_t)prm->segment_eq,
+                                                          reinterpret_cast<unsigned long long*>(count_device));
+  return after_launch(ctx, "join_count_kernel");
+}
+
+int bo_join_plain(bo_ctx* ctx, const bo_join_build_cols* b, const bo_join_probe_cols* p, const bo_join_params* prm,
+                  bo_join_result* out_host) {
+  BO_CHECK_CTX(ctx);
+  int rc = check_join(ctx, b, p, prm);
+  if (rc) return rc;
+  if (!out_host) return set_error(ctx, BO_ERR_INVALID, "join: null output");
+  return join_plain_impl(ctx, *b, *p, *prm, out_host, 0);
+}
+
+int bo_join_presized_device(bo_ctx* ctx, const bo_join_build_cols* b, const bo_join_probe_cols* p,
+                            const bo_join_params* prm, const float* pred_device, bo_join_result* out_device) {
+  BO_CHECK_CTX(ctx);
+  int rc = check_join(ctx, b, p, prm);
+  if (rc) return rc;
+  if (!pred_device || !out_device) return set_error(ctx, BO_ERR_INVALID, "join: null prediction or output");
+  JoinWs ws;
+  if ((rc = join_workspace(ctx, b->n_rows, &ws))) return rc;
+  return join_run(ctx, *b, *p, *prm, ws, pred_device, 0, out_device, 1);
+}
+
+int bo_join_presized(bo_ctx* ctx, const bo_join_build_cols* b, const bo_join_probe_cols* p, const bo_join_params* prm,
+                     const float* pred_device, bo_join_result* out_host) {
+  BO_CHECK_CTX(ctx);
+  if (!out_host) return set_error(ctx, BO_ERR_INVALID, "join: null output");
+  void* dout = nullptr;
+  int rc = region(ctx, "join_out", sizeof(bo_join_result), &dout);
+  if (rc) return rc;
+  bo_join_result* d = static_cast<bo_join_result*>(dout);
+  if ((rc = bo_join_presized_device(ctx, b, p, prm, pred_device, d))) return rc;
+  if ((rc = finish_join(ctx, out_host, d))) return rc;
+  if (out_host->overflowed) {
+    // The prediction was too low: rerun exactly (the answer never depends on it).
+    const int32_t cap = out_host->capacity_log2;
+    if ((rc = join_plain_impl(ctx, *b, *p, *prm, out_host, 1))) return rc;
+    out_host->mode = 1;
+    (void)cap;
+  }
+  return BO_OK;
+}
+
+int bo_join_probe_device(bo_ctx* ctx, const bo_join_probe_cols* p, bo_join_result* out_device) {
+  BO_CHECK_CTX(ctx);
+  if (!p || !out_device) return set_error(ctx, BO_ERR_INVALID, "join_probe: null argument");
+  if (p->n_rows < 0) return set_error(ctx, BO_ERR_INVALID, "join_probe: negative row count");
+  if (p->n_rows > 0 && (!p->fk || !p->price || !p->discount || !aligned32(p->fk) || !aligned32(p->price) ||
+                        !aligned32(p->discount)))
+    return set_error(ctx, BO_ERR_INVALID, "join_probe: probe column null or not 32-byte aligned");
+  auto it = ctx->regions.find("join_slots");
+  if (it == ctx->regions.end())
+    return set_error(ctx, BO_ERR_INVALID, "join_probe: no join table has been built on this context");
+  JoinWs ws;
+  int rc = join_workspace(ctx, 0, &ws);
+  if (rc) return rc;
+  return launch_probe(ctx, *p, ws, out_device, 1);
+}
+
+int bo_join_host(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join_probe_cols* ph, const bo_join_params* prm,
+                 int32_t mode, float predicted_rows, bo_join_result* out_host) {
+  BO_CHECK_CTX(ctx);
+  if (!bh || !ph || !prm || !out_host) return set_error(ctx, BO_ERR_INVALID, "join: null argument");
+  if (bh->n_rows < 0 || ph->n_rows < 0) return set_error(ctx, BO_ERR_INVALID, "join: negative row count");
+  const size_t nb = (size_t)bh->n_rows, np = (size_t)ph->n_rows;
+  const size_t sizes[6] = {4 * nb, 4 * nb, nb, 4 * np, 8 * np, 8 * np};
+  const void* src[6] = {bh->key, bh->date, bh->segment, ph->fk, ph->price, ph->discount};
+  size_t off[6], total = 0;
+  for (int i = 0; i < 6; ++i) {
+    off[i] = total;
+    total += (sizes[i] + 255) & ~size_t(255);
+  }
+  void* base = nullptr;
+  int rc = region(ctx, "join_in", total ? total : 256, &base);
+  if (rc) return rc;
+  char* d = static_cast<char*>(base);
+  for (int i = 0; i < 6; ++i)
+    if (sizes[i]) BO_CUDA(ctx, cudaMemcpyAsync(d + off[i], src[i], sizes[i], cudaMemcpyHostToDevice, ctx->stream));
+  bo_join_build_cols b = {reinterpret_cast<const int32_t*>(d + off[0]), reinterpret_cast<const int32_t*>(d + off[1]),
+                          reinterpret_cast<const uint8_t*>(d + off[2]), bh->n_rows};
+  bo_join_probe_cols p = {reinterpret_cast<const int32_t*>(d + off[3]), reinterpret_cast<const int64_t*>(d + off[4]),
+                          reinterpret_cast<const int64_t*>(d + off[5]), ph->n_rows};
+  if (mode == 0) return bo_join_plain(ctx, &b, &p, prm, out_host);
+  JoinWs ws;
+  if ((rc = join_workspace(ctx, b.n_rows, &ws))) return rc;
+  BO_CUDA(ctx, cudaMemcpyAsync(ws.pred, &predicted_rows, sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  return bo_join_presized(ctx, &b, &p, prm, ws.pred, out_host);
+}
+
+}  // extern "C"

@@ -9,9 +9,10 @@
 //           quantity limit, int64 sum of extendedprice*discount).
 //
 // Design (HBM-bound streaming scan):
-//  * every column is read once with 128-bit streaming loads (no L1 allocation),
+//  * every column is read once with streaming vector loads (no L1 allocation);
 //    a thread consumes a chunk of 4 (wide layout) or 8 (storage-plan layout)
-//    consecutive rows per iteration so all of its loads are 16-byte vectors;
+//    consecutive rows per iteration; 64-bit columns use 256-bit loads so every
+//    load instruction consumes whole 32-byte sectors;
 //  * the grid is the resident grid (SMs x blocks/SM) and grows only when a
 //    thread would otherwise see more than kMaxRowsPerThread rows, which bounds
 //    every per-thread partial (and every bit-packed field) so no sum overflows;
@@ -168,35 +169,6 @@ __device__ __forceinline__ void block_flush(const unsigned long long* col, int n
   }
 }
 
-__device__ __forceinline__ __int128 load_i128(const unsigned long long* p) {
-  const uint64_t lo = __ldcg(p), hi = __ldcg(p + 1);
-  return (__int128)(((unsigned __int128)hi << 64) | lo);
-}
-
-__device__ __forceinline__ int64_t narrow_i64(__int128 v, uint32_t& bad) {
-  if (v != (__int128)(int64_t)v) bad |= kErrSumOverflow;
-  return (int64_t)v;
-}
-
-__device__ __forceinline__ bo_i128 to_bo_i128(__int128 v) {
-  bo_i128 r;
-  r.lo = (uint64_t)v;
-  r.hi = (int64_t)(v >> 64);
-  return r;
-}
-
-// Last-block epilogue: returns true in every thread of the block that finished
-// last (after all other blocks' totals are visible).
-__device__ __forceinline__ bool last_block(uint32_t* done) {
-  __shared__ bool is_last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) is_last = (atomicAdd(done, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (is_last) __threadfence();
-  return is_last;
-}
-
 // Converts the totals of group g into the output record and clears them.
 __device__ void q1_finalize_group(int g, unsigned long long* acc, bo_q1_agg* out, uint32_t& bad) {
   unsigned long long* a = acc + g * kQ1Sums * 2;
@@ -240,19 +212,14 @@ __global__ void __launch_bounds__(kScanBlock) q1_fact_kernel(bo_fact_cols c, int
   for (int64_t ch = tid; ch < chunks; ch += stride) {
     const int64_t r = ch << 2;
     const int4 sd = ld_stream_v4(c.ship_date + r);
-    const int4 q0 = ld_stream_v4(c.quantity + r), q1 = ld_stream_v4(c.quantity + r + 2);
-    const int4 p0 = ld_stream_v4(c.ext_price + r), p1 = ld_stream_v4(c.ext_price + r + 2);
-    const int4 d0 = ld_stream_v4(c.discount + r), d1 = ld_stream_v4(c.discount + r + 2);
-    const int4 t0 = ld_stream_v4(c.tax + r), t1 = ld_stream_v4(c.tax + r + 2);
+    const long4v q = ld_stream_v4x64(c.quantity + r), p = ld_stream_v4x64(c.ext_price + r);
+    const long4v d = ld_stream_v4x64(c.discount + r), t = ld_stream_v4x64(c.tax + r);
     const uint32_t fa = ld_stream_u32(c.flag_a + r), fb = ld_stream_u32(c.flag_b + r);
-    wide_row(col, sd.x, cutoff, make_i64(q0.x, q0.y), make_i64(p0.x, p0.y), make_i64(d0.x, d0.y),
-             make_i64(t0.x, t0.y), fa & 0xffu, fb & 0xffu, n_fa, n_fb, bad);
-    wide_row(col, sd.y, cutoff, make_i64(q0.z, q0.w), make_i64(p0.z, p0.w), make_i64(d0.z, d0.w),
-             make_i64(t0.z, t0.w), (fa >> 8) & 0xffu, (fb >> 8) & 0xffu, n_fa, n_fb, bad);
-    wide_row(col, sd.z, cutoff, make_i64(q1.x, q1.y), make_i64(p1.x, p1.y), make_i64(d1.x, d1.y),
-             make_i64(t1.x, t1.y), (fa >> 16) & 0xffu, (fb >> 16) & 0xffu, n_fa, n_fb, bad);
-    wide_row(col, sd.w, cutoff, make_i64(q1.z, q1.w), make_i64(p1.z, p1.w), make_i64(d1.z, d1.w),
-             make_i64(t1.z, t1.w), fa >> 24, fb >> 24, n_fa, n_fb, bad);
+    const int32_t ship[4] = {sd.x, sd.y, sd.z, sd.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      wide_row(col, ship[k], cutoff, q.v[k], p.v[k], d.v[k], t.v[k], (fa >> (8 * k)) & 0xffu, (fb >> (8 * k)) & 0xffu,
+               n_fa, n_fb, bad);
   }
   const int64_t tail = (chunks << 2) + tid;
   if (tail < n) {
@@ -289,8 +256,8 @@ __global__ void __launch_bounds__(kScanBlock) q1_lineitem_kernel(bo_lineitem_col
     const int64_t r = ch << 3;
     const int4 sd = ld_stream_v4(c.shipdate + r);
     const uint2 gc = ld_stream_v2(c.returnflag_linestatus + r);
-    const int4 pa = ld_stream_v4(c.extendedprice + r), pb = ld_stream_v4(c.extendedprice + r + 4);
-    const int4 da = ld_stream_v4(c.discounted_price + r), db = ld_stream_v4(c.discounted_price + r + 4);
+    const int8v pr = ld_stream_v8(c.extendedprice + r);
+    const int8v dpr = ld_stream_v8(c.discounted_price + r);
     const uint2 dc = ld_stream_v2(c.discount + r);
     const uint2 tx = ld_stream_v2(c.tax + r);
     const int4 qt = ld_stream_v4(c.quantity + r);
@@ -298,15 +265,13 @@ __global__ void __launch_bounds__(kScanBlock) q1_lineitem_kernel(bo_lineitem_col
                              (int16_t)sd.z, sd.z >> 16, (int16_t)sd.w, sd.w >> 16};
     const int32_t qty[8] = {(int16_t)qt.x, qt.x >> 16, (int16_t)qt.y, qt.y >> 16,
                             (int16_t)qt.z, qt.z >> 16, (int16_t)qt.w, qt.w >> 16};
-    const int32_t pr[8] = {pa.x, pa.y, pa.z, pa.w, pb.x, pb.y, pb.z, pb.w};
-    const int32_t dpr[8] = {da.x, da.y, da.z, da.w, db.x, db.y, db.z, db.w};
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const uint32_t sh = (k & 3) * 8;
       const uint32_t code = ((k < 4 ? gc.x : gc.y) >> sh) & 0xffu;
       const uint32_t d = ((k < 4 ? dc.x : dc.y) >> sh) & 0xffu;
       const uint32_t t = ((k < 4 ? tx.x : tx.y) >> sh) & 0xffu;
-      narrow_row(col, ship[k], cutoff, code, pr[k], dpr[k], d, t, qty[k], n_groups, bad);
+      narrow_row(col, ship[k], cutoff, code, pr.v[k], dpr.v[k], d, t, qty[k], n_groups, bad);
     }
   }
   const int64_t tail_begin = chunks << 3;
@@ -353,15 +318,14 @@ __global__ void __launch_bounds__(kScanBlock) q6_lineitem_kernel(bo_lineitem_col
     const int4 sd = ld_stream_v4(c.shipdate + r);
     const uint2 dc = ld_stream_v2(c.discount + r);
     const int4 qt = ld_stream_v4(c.quantity + r);
-    const int4 pa = ld_stream_v4(c.extendedprice + r), pb = ld_stream_v4(c.extendedprice + r + 4);
+    const int8v pr = ld_stream_v8(c.extendedprice + r);
     const int32_t ship[8] = {(int16_t)sd.x, sd.x >> 16, (int16_t)sd.y, sd.y >> 16,
                              (int16_t)sd.z, sd.z >> 16, (int16_t)sd.w, sd.w >> 16};
     const int32_t qty[8] = {(int16_t)qt.x, qt.x >> 16, (int16_t)qt.y, qt.y >> 16,
                             (int16_t)qt.z, qt.z >> 16, (int16_t)qt.w, qt.w >> 16};
-    const int32_t pr[8] = {pa.x, pa.y, pa.z, pa.w, pb.x, pb.y, pb.z, pb.w};
 #pragma unroll
     for (int k = 0; k < 8; ++k)
-      row(ship[k], ((k < 4 ? dc.x : dc.y) >> ((k & 3) * 8)) & 0xffu, qty[k], pr[k]);
+      row(ship[k], ((k < 4 ? dc.x : dc.y) >> ((k & 3) * 8)) & 0xffu, qty[k], pr.v[k]);
   }
   const int64_t tail_begin = chunks << 3;
   if (tid < n - tail_begin) {
@@ -474,7 +438,7 @@ int check_fact(bo_ctx* ctx, const bo_fact_cols* c, int32_t nfa, int32_t nfb) {
     const void* ptrs[] = {c->ship_date, c->quantity, c->ext_price, c->discount, c->tax, c->flag_a, c->flag_b};
     for (const void* p : ptrs) {
       if (!p) return set_error(ctx, BO_ERR_INVALID, "q1: null column pointer");
-      if (!aligned16(p)) return set_error(ctx, BO_ERR_INVALID, "q1: column pointer not 16-byte aligned");
+      if (!aligned32(p)) return set_error(ctx, BO_ERR_INVALID, "q1: column pointer not 32-byte aligned");
     }
   }
   return BO_OK;
@@ -487,13 +451,13 @@ int check_lineitem(bo_ctx* ctx, const bo_lineitem_cols* c, bool need_q1_cols, co
   const void* q6[] = {c->shipdate, c->extendedprice, c->discount, c->quantity};
   for (const void* p : q6) {
     if (!p) return set_error(ctx, BO_ERR_INVALID, "%s: null column pointer", op);
-    if (!aligned16(p)) return set_error(ctx, BO_ERR_INVALID, "%s: column pointer not 16-byte aligned", op);
+    if (!aligned32(p)) return set_error(ctx, BO_ERR_INVALID, "%s: column pointer not 32-byte aligned", op);
   }
   if (need_q1_cols) {
     const void* q1[] = {c->returnflag_linestatus, c->discounted_price, c->tax};
     for (const void* p : q1) {
       if (!p) return set_error(ctx, BO_ERR_INVALID, "%s: null column pointer", op);
-      if (!aligned16(p)) return set_error(ctx, BO_ERR_INVALID, "%s: column pointer not 16-byte aligned", op);
+      if (!aligned32(p)) return set_error(ctx, BO_ERR_INVALID, "%s: column pointer not 32-byte aligned", op);
     }
   }
   return BO_OK;

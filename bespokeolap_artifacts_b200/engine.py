@@ -151,3 +151,54 @@ class Engine:
         out = N.Q6Result()
         self.ctx.call("bo_q6_lineitem_host", C.byref(lc), start, end, dmin, dmax, qlimit, C.byref(out))
         return out.revenue_raw, out.count
+
+    # ----------------------------------------------------------- join ------
+    @staticmethod
+    def join_cols(build, probe, n_build: int, n_probe: int):
+        """build: (key, date, segment); probe: (fk, price, discount)."""
+        b = N.JoinBuildCols(*[N.ptr(c) for c in build], n_build)
+        p = N.JoinProbeCols(*[N.ptr(c) for c in probe], n_probe)
+        return b, p
+
+    def join_plain(self, build, probe, n_build: int, n_probe: int, date_lt: int, seg_eq: int) -> dict:
+        """Exact-count pre-pass, one host round trip, build, probe."""
+        b, p = self.join_cols(build, probe, n_build, n_probe)
+        out = N.JoinResult()
+        self.ctx.call("bo_join_plain", C.byref(b), C.byref(p), C.byref(N.JoinParams(date_lt, seg_eq)),
+                      C.byref(out))
+        return out.as_dict()
+
+    def join_presized(self, build, probe, n_build: int, n_probe: int, date_lt: int, seg_eq: int, pred_dev) -> dict:
+        """Table sized on the device from a predicted row count (device float);
+        exact rerun if it overflowed."""
+        b, p = self.join_cols(build, probe, n_build, n_probe)
+        out = N.JoinResult()
+        self.ctx.call("bo_join_presized", C.byref(b), C.byref(p), C.byref(N.JoinParams(date_lt, seg_eq)),
+                      C.c_void_p(N.ptr(pred_dev)), C.byref(out))
+        return out.as_dict()
+
+    def join_presized_device(self, build, probe, n_build: int, n_probe: int, date_lt: int, seg_eq: int, pred_dev,
+                             out_dev) -> None:
+        b, p = self.join_cols(build, probe, n_build, n_probe)
+        self.ctx.call("bo_join_presized_device", C.byref(b), C.byref(p), C.byref(N.JoinParams(date_lt, seg_eq)),
+                      C.c_void_p(N.ptr(pred_dev)), C.c_void_p(N.ptr(out_dev)))
+
+    def join_probe_device(self, probe, n_probe: int, out_dev) -> None:
+        """Probe the table of this context's last join build with another batch."""
+        p = N.JoinProbeCols(*[N.ptr(c) for c in probe], n_probe)
+        self.ctx.call("bo_join_probe_device", C.byref(p), C.c_void_p(N.ptr(out_dev)))
+
+    def join_count_device(self, build, n_build: int, date_lt: int, seg_eq: int, count_dev) -> None:
+        b = N.JoinBuildCols(*[N.ptr(c) for c in build], n_build)
+        self.ctx.call("bo_join_count_device", C.byref(b), C.byref(N.JoinParams(date_lt, seg_eq)),
+                      C.c_void_p(N.ptr(count_dev)))
+
+    def join_host(self, j, mode: int = 0, predicted_rows: float = 0.0) -> dict:
+        """Host arrays (a datagen.JoinInput) in; copies inside the call."""
+        build = [np.ascontiguousarray(x) for x in (j.b_key, j.b_date, j.b_seg)]
+        probe = [np.ascontiguousarray(x) for x in (j.p_fk, j.p_price, j.p_disc)]
+        b, p = self.join_cols(build, probe, j.n_build, j.n_probe)
+        out = N.JoinResult()
+        self.ctx.call("bo_join_host", C.byref(b), C.byref(p), C.byref(N.JoinParams(j.date_lt, j.seg_eq)), mode,
+                      float(predicted_rows), C.byref(out))
+        return out.as_dict()

@@ -1,0 +1,250 @@
+"""Learned sizing: the MLP that presizes hash tables and output buffers.
+
+The network (``bo_mlp`` in ``csrc/mlp.cu``: n_features -> 64 -> 64 -> 64 ->
+n_outputs, FP32, ReLU) is trained on the GPU by the library's own forward /
+backward / Adam kernels, on (features, exact count) pairs that the plain GPU
+pipeline produces on seeded tables.  Features are predicate constants plus
+per-column sketches (``bo_sketch_i32`` / ``bo_histogram_small``: min, max, a
+64-bin equi-width histogram, HyperLogLog distinct estimates, exact histograms
+of small domains).  Targets are log1p(count).
+
+The prediction only sizes: the exact-count path stays the fallback (a presized
+table that overflows is rerun exactly) and the judge (q-error is reported), so
+no answer depends on it.  No reference counterpart exists -- the reference
+sizes its dense arrays exactly (bespoke_tpch/query_q3.cpp:178-180).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import native as N
+
+LOG_SCALE = 16.0
+
+
+class Mlp:
+    """One ``bo_mlp`` model bound to an engine context."""
+
+    def __init__(self, ctx: N.Context, n_features: int, n_outputs: int, seed: int = 0):
+        self.ctx = ctx
+        self.F, self.O = n_features, n_outputs
+        h = C.c_void_p()
+        ctx.check(ctx._lib.bo_mlp_create(ctx.handle, n_features, n_outputs, seed, C.byref(h)), "bo_mlp_create")
+        self.handle = h
+        self.P = ctx._lib.bo_mlp_num_params(h)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx._lib.bo_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.P, np.float32)
+        self.ctx.call("bo_mlp_get_params", self.handle, C.c_void_p(out.ctypes.data))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.shape == (self.P,)
+        self.ctx.call("bo_mlp_set_params", self.handle, C.c_void_p(p.ctypes.data))
+
+    def train(self, x: np.ndarray, t: np.ndarray, epochs: int = 2000, lr: float = 3e-3) -> float:
+        """Full-batch Adam on host arrays (copied to the device once)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = C.c_float()
+        self.ctx.call("bo_mlp_train_host", self.handle, C.c_void_p(x.ctypes.data), C.c_void_p(t.ctypes.data),
+                      x.shape[0], epochs, lr, C.byref(loss))
+        return float(loss.value)
+
+    def gradients(self, x_dev, t_dev, n: int, grad_dev, loss_dev) -> None:
+        self.ctx.call("bo_mlp_gradients_device", self.handle, C.c_void_p(N.ptr(x_dev)), C.c_void_p(N.ptr(t_dev)),
+                      n, C.c_void_p(N.ptr(grad_dev)), C.c_void_p(N.ptr(loss_dev)))
+
+    def infer_device(self, x_dev, n: int, y_dev) -> None:
+        self.ctx.call("bo_mlp_infer_device", self.handle, C.c_void_p(N.ptr(x_dev)), n, C.c_void_p(N.ptr(y_dev)))
+
+    def predict_counts_device(self, features: np.ndarray, counts_dev, log_dev=None) -> None:
+        """One feature vector (passed to the kernel by value) -> device counts."""
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        assert f.shape == (self.F,)
+        self.ctx.call("bo_mlp_predict_counts", self.handle, C.c_void_p(f.ctypes.data), C.c_void_p(N.ptr(counts_dev)),
+                      C.c_void_p(N.ptr(log_dev) if log_dev is not None else 0))
+
+
+# ------------------------------------------------------------------ sketches --
+@dataclass
+class IntSketch:
+    n: int
+    min: int
+    max: int
+    hist: np.ndarray       # 64 equi-width bins over [min, max]
+    distinct: float
+
+    def frac_below(self, v: int) -> float:
+        """Estimated fraction of rows with value < v (uniform within a bin)."""
+        if self.n == 0:
+            return 0.0
+        if v <= self.min:
+            return 0.0
+        if v > self.max:
+            return 1.0
+        span = self.max - self.min + 1
+        pos = (v - self.min) * len(self.hist) / span
+        b = int(pos)
+        below = float(self.hist[:b].sum()) + float(self.hist[b]) * (pos - b) if b < len(self.hist) else float(
+            self.hist.sum())
+        return below / self.n
+
+    def frac_between(self, lo: int, hi: int) -> float:
+        """Estimated fraction with lo <= value <= hi."""
+        return max(0.0, self.frac_below(hi + 1) - self.frac_below(lo))
+
+
+def sketch_i32(ctx: N.Context, col_dev, n: int) -> IntSketch:
+    s = N.Sketch()
+    ctx.call("bo_sketch_i32", C.c_void_p(N.ptr(col_dev)), n, C.byref(s))
+    return IntSketch(s.n, s.min, s.max, np.array(s.hist[:], dtype=np.int64), s.distinct_estimate)
+
+
+def histogram_small(ctx: N.Context, col_dev, elem_bytes: int, n: int, domain: int) -> np.ndarray:
+    out = np.zeros(domain, np.int64)
+    ctx.call("bo_histogram_small", C.c_void_p(N.ptr(col_dev)), elem_bytes, n, domain, C.c_void_p(out.ctypes.data))
+    return out
+
+
+# --------------------------------------------------------- join build sizing --
+JOIN_FEATURES = 8
+
+
+@dataclass
+class JoinTableStats:
+    """Load-time statistics of a join build side (computed once per table)."""
+    n: int
+    date: IntSketch
+    key: IntSketch
+    seg_hist: np.ndarray   # 256 counts
+
+
+def join_table_stats(ctx: N.Context, key_dev, date_dev, seg_dev, n: int) -> JoinTableStats:
+    return JoinTableStats(n, sketch_i32(ctx, date_dev, n), sketch_i32(ctx, key_dev, n),
+                          histogram_small(ctx, seg_dev, 1, n, 256))
+
+
+def join_independence_estimate(st: JoinTableStats, date_lt: int, seg_eq: int) -> float:
+    """The classic estimate: n * sel(date) * sel(segment), columns independent."""
+    if st.n == 0:
+        return 0.0
+    return st.n * st.date.frac_below(date_lt) * (st.seg_hist[seg_eq] / st.n)
+
+
+def join_features(st: JoinTableStats, date_lt: int, seg_eq: int) -> np.ndarray:
+    n = max(st.n, 1)
+    fd = st.date.frac_below(date_lt)
+    fs = st.seg_hist[seg_eq] / n
+    span = max(st.date.max - st.date.min + 1, 1)
+    return np.array([
+        math.log1p(st.n) / LOG_SCALE,
+        fd,
+        min(max((date_lt - st.date.min) / span, -0.5), 1.5),
+        fs,
+        math.log1p(st.n * fd * fs) / LOG_SCALE,
+        math.log1p(st.key.distinct) / LOG_SCALE,
+        fd * fs,
+        float(np.count_nonzero(st.seg_hist)) / 16.0,
+    ], dtype=np.float32)
+
+
+def gen_join_training_table(rng: np.random.Generator, n: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """A seeded build side with varied shape: uniform or skewed dates, uniform or
+    skewed segments, and (half the time) segments correlated with dates so the
+    independence estimate is wrong."""
+    from .datagen import DATE_HI, DATE_LO
+
+    key = rng.permutation(np.arange(1, n + 1, dtype=np.int32))
+    span = DATE_HI - DATE_LO
+    if rng.random() < 0.5:
+        date = rng.integers(DATE_LO, DATE_HI, size=n, endpoint=True, dtype=np.int32)
+    else:
+        date = (DATE_LO + span * rng.beta(rng.uniform(0.5, 3), rng.uniform(0.5, 3), size=n)).astype(np.int32)
+    k = int(rng.integers(2, 9))
+    if rng.random() < 0.5:
+        seg = rng.integers(0, k, size=n, dtype=np.uint8)
+    else:
+        w = np.arange(1, k + 1, dtype=np.float64) ** -rng.uniform(0.5, 2.0)
+        seg = rng.choice(k, size=n, p=w / w.sum()).astype(np.uint8)
+    if rng.random() < 0.5:  # correlate segment with date
+        bucket = ((date - DATE_LO) * k // (span + 1)).astype(np.int64)
+        noisy = rng.random(n) < rng.uniform(0.0, 0.5)
+        seg = np.where(noisy, seg, bucket % k).astype(np.uint8)
+    return key, date, seg
+
+
+def make_join_training_set(engine, n_tables: int = 24, preds_per_table: int = 40, seed: int = 1234,
+                           n_min: int = 20_000, n_max: int = 2_000_000):
+    """(features, log1p(exact qualifying rows), independence estimates): the
+    exact counts come from the plain GPU pipeline's count kernel (K7)."""
+    import torch
+
+    from .datagen import DATE_HI, DATE_LO
+
+    rng = np.random.default_rng(seed)
+    xs, ts, naive = [], [], []
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for _ in range(n_tables):
+        n = int(math.exp(rng.uniform(math.log(n_min), math.log(n_max))))
+        key, date, seg = gen_join_training_table(rng, n)
+        dk, dd, ds = (torch.from_numpy(a).cuda() for a in (key, date, seg))
+        st = join_table_stats(engine.ctx, dk, dd, ds, n)
+        for _ in range(preds_per_table):
+            d = int(rng.integers(DATE_LO, DATE_HI + 2))
+            s = int(rng.integers(0, 8))
+            engine.join_count_device((dk, dd, ds), n, d, s, cnt)
+            engine.synchronize()
+            c = int(cnt.item())
+            xs.append(join_features(st, d, s))
+            ts.append([math.log1p(c)])
+            naive.append(join_independence_estimate(st, d, s))
+    return np.stack(xs), np.array(ts, np.float32), np.array(naive)
+
+
+def q_error(pred, true) -> np.ndarray:
+    """max(p/t, t/p) with both counts floored at 1."""
+    p = np.maximum(np.asarray(pred, dtype=np.float64), 1.0)
+    t = np.maximum(np.asarray(true, dtype=np.float64), 1.0)
+    return np.maximum(p / t, t / p)
+
+
+class JoinSizer:
+    """Trained join-build sizer: features -> predicted qualifying build rows,
+    written on the device where the presized join reads it."""
+
+    def __init__(self, engine, seed: int = 7):
+        self.engine = engine
+        self.mlp = Mlp(engine.ctx, JOIN_FEATURES, 1, seed)
+
+    def fit(self, x, t, epochs: int = 3000, lr: float = 2e-3) -> float:
+        return self.mlp.train(x, t, epochs, lr)
+
+    def predict_host(self, x: np.ndarray) -> np.ndarray:
+        """Batch inference on the device (used for evaluation), counts on host."""
+        import torch
+
+        xd = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).cuda()
+        yd = torch.empty((x.shape[0], 1), dtype=torch.float32, device="cuda")
+        self.mlp.infer_device(xd, x.shape[0], yd)
+        self.engine.synchronize()
+        return np.expm1(yd.cpu().numpy()[:, 0].astype(np.float64)).clip(min=0)
+
+    def predict_device(self, features: np.ndarray, counts_dev) -> None:
+        self.mlp.predict_counts_device(features, counts_dev)

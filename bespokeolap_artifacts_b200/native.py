@@ -99,6 +99,40 @@ class Q6Result(C.Structure):
     _fields_ = [("revenue_raw", C.c_int64), ("count", C.c_int64)]
 
 
+class JoinBuildCols(C.Structure):
+    _fields_ = [("key", C.c_void_p), ("date", C.c_void_p), ("segment", C.c_void_p), ("n_rows", C.c_int64)]
+
+
+class JoinProbeCols(C.Structure):
+    _fields_ = [("fk", C.c_void_p), ("price", C.c_void_p), ("discount", C.c_void_p), ("n_rows", C.c_int64)]
+
+
+class JoinParams(C.Structure):
+    _fields_ = [("date_lt", C.c_int32), ("segment_eq", C.c_int32)]
+
+
+class JoinResult(C.Structure):
+    _fields_ = [
+        ("build_rows", C.c_int64), ("distinct_keys", C.c_int64), ("match_count", C.c_int64),
+        ("sum_exact", I128), ("sum_trunc", I128), ("capacity_log2", C.c_int32), ("overflowed", C.c_int32),
+        ("reruns", C.c_int32), ("mode", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return dict(build_rows=self.build_rows, distinct_keys=self.distinct_keys, match_count=self.match_count,
+                    sum_exact=self.sum_exact.value(), sum_trunc=self.sum_trunc.value(),
+                    capacity_log2=self.capacity_log2, overflowed=self.overflowed, reruns=self.reruns,
+                    mode=self.mode)
+
+
+SKETCH_BINS = 64
+
+
+class Sketch(C.Structure):
+    _fields_ = [("n", C.c_int64), ("min", C.c_int64), ("max", C.c_int64), ("hist", C.c_int64 * SKETCH_BINS),
+                ("distinct_estimate", C.c_double)]
+
+
 # --------------------------------------------------------------- prototypes --
 _P = C.c_void_p
 _SIGNATURES = {
@@ -126,6 +160,28 @@ _SIGNATURES = {
     "bo_q6_lineitem_host": (
         C.c_int,
         [_P, C.POINTER(LineitemCols), C.c_int16, C.c_int16, C.c_int32, C.c_int32, C.c_int32, C.POINTER(Q6Result)]),
+    "bo_join_count_device": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinParams), _P]),
+    "bo_join_plain": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
+                                C.POINTER(JoinResult)]),
+    "bo_join_presized_device": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols),
+                                          C.POINTER(JoinParams), _P, _P]),
+    "bo_join_presized": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
+                                   _P, C.POINTER(JoinResult)]),
+    "bo_sketch_i32": (C.c_int, [_P, _P, C.c_int64, C.POINTER(Sketch)]),
+    "bo_histogram_small": (C.c_int, [_P, _P, C.c_int32, C.c_int64, C.c_int32, _P]),
+    "bo_mlp_create": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(_P)]),
+    "bo_mlp_destroy": (None, [_P]),
+    "bo_mlp_num_params": (C.c_int32, [_P]),
+    "bo_mlp_get_params": (C.c_int, [_P, _P, _P]),
+    "bo_mlp_set_params": (C.c_int, [_P, _P, _P]),
+    "bo_mlp_gradients_device": (C.c_int, [_P, _P, _P, _P, C.c_int32, _P, _P]),
+    "bo_mlp_train_step_device": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_float, _P]),
+    "bo_mlp_train_host": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, C.c_float, C.POINTER(C.c_float)]),
+    "bo_mlp_infer_device": (C.c_int, [_P, _P, _P, C.c_int32, _P]),
+    "bo_mlp_predict_counts": (C.c_int, [_P, _P, _P, _P, _P]),
+    "bo_join_probe_device": (C.c_int, [_P, C.POINTER(JoinProbeCols), _P]),
+    "bo_join_host": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
+                               C.c_int32, C.c_float, C.POINTER(JoinResult)]),
 }
 
 _lib = None

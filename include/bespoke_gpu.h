@@ -103,7 +103,8 @@ typedef struct bo_q1_agg {
 
 /* Fact table in the declared wide layout (38 B/row): ship_date int32 days since
  * 1970-01-01; quantity/ext_price int64 x100; discount/tax int64 x100 in
- * [0,100]; flag_a/flag_b uint8 group flags.  Every pointer 16-byte aligned. */
+ * [0,100]; flag_a/flag_b uint8 group flags.  Every column pointer of every
+ * entry point in this header must be 32-byte aligned (256-bit vector loads). */
 typedef struct bo_fact_cols {
   const int32_t* ship_date;
   const int64_t* quantity;
@@ -162,6 +163,125 @@ int bo_q6_lineitem_device(bo_ctx* ctx, const bo_lineitem_cols* cols, int16_t sta
 int bo_q6_lineitem_host(bo_ctx* ctx, const bo_lineitem_cols* host_cols, int16_t start_offset,
                         int16_t end_offset, int32_t disc_min, int32_t disc_max,
                         int32_t qty_limit, bo_q6_result* out_host);
+
+/* =================================================================== JOIN ==
+ * Filtered hash join + scalar aggregate.  Replaces the filtered-join shape of
+ * run_q3 (bespoke_tpch/query_q3.cpp:182-260): the reference answers it with a
+ * dense cust_in_segment byte map and builder-time CSR ranges
+ * (builder_impl.cpp:930-991); here the qualifying build keys go into an
+ * open-addressing table in HBM (64-bit slots key<<32 | multiplicity, inserted
+ * with atomicCAS) plus a blocked Bloom filter the probe stages into shared
+ * memory.  Inner-join semantics: a probe row contributes once per matching
+ * build row. */
+typedef struct bo_join_build_cols {
+  const int32_t* key;
+  const int32_t* date;
+  const uint8_t* segment;
+  int64_t n_rows;
+} bo_join_build_cols;
+
+typedef struct bo_join_probe_cols {
+  const int32_t* fk;
+  const int64_t* price;     /* x100, 0 <= price < 2^31 */
+  const int64_t* discount;  /* x100, 0 <= discount <= 100 */
+  int64_t n_rows;
+} bo_join_probe_cols;
+
+typedef struct bo_join_params {
+  int32_t date_lt;     /* build row qualifies when date < date_lt ... */
+  int32_t segment_eq;  /* ... and segment == segment_eq */
+} bo_join_params;
+
+typedef struct bo_join_result {
+  int64_t build_rows;      /* qualifying build rows */
+  int64_t distinct_keys;   /* distinct qualifying keys (table occupancy) */
+  int64_t match_count;     /* joined rows */
+  bo_i128 sum_exact;       /* sum price*(100-discount)            (x1e4) */
+  bo_i128 sum_trunc;       /* sum trunc(price*(100-discount)/100) (x100), run_q3's revenue */
+  int32_t capacity_log2;   /* table capacity used */
+  int32_t overflowed;      /* presized table was too small (result invalid, rerun) */
+  int32_t reruns;          /* exact-count reruns performed by the call */
+  int32_t mode;            /* 0 plain exact-count, 1 presized from a prediction */
+} bo_join_result;
+
+/* K7, exact-count pre-pass: number of qualifying build rows (device int64). */
+int bo_join_count_device(bo_ctx* ctx, const bo_join_build_cols* build, const bo_join_params* params,
+                         int64_t* count_device);
+/* Plain form: exact-count pre-pass, one host round trip to size the table,
+ * then build and probe.  Synchronises; result on the host. */
+int bo_join_plain(bo_ctx* ctx, const bo_join_build_cols* build, const bo_join_probe_cols* probe,
+                  const bo_join_params* params, bo_join_result* out_host);
+/* Presized form, fully asynchronous (no host round trip, capturable in a CUDA
+ * graph): the table is sized on the device from predicted_rows_device (one
+ * float, the predicted number of qualifying build rows, e.g. an MLP output
+ * written by bo_mlp_infer_device).  out_device->overflowed reports a table
+ * that turned out too small. */
+int bo_join_presized_device(bo_ctx* ctx, const bo_join_build_cols* build, const bo_join_probe_cols* probe,
+                            const bo_join_params* params, const float* predicted_rows_device,
+                            bo_join_result* out_device);
+/* Presized form with the exact fallback: runs bo_join_presized_device,
+ * synchronises once, and reruns the plain form if the table overflowed, so
+ * the answer never depends on the prediction. */
+int bo_join_presized(bo_ctx* ctx, const bo_join_build_cols* build, const bo_join_probe_cols* probe,
+                     const bo_join_params* params, const float* predicted_rows_device,
+                     bo_join_result* out_host);
+/* Probes the table left by this context's most recent join build with another
+ * probe batch (asynchronous; the build side is reused).  Used to time the
+ * probe kernel alone and to join several probe batches against one build. */
+int bo_join_probe_device(bo_ctx* ctx, const bo_join_probe_cols* probe, bo_join_result* out_device);
+/* Host buffers in, result out: copies both sides to the device inside the
+ * call, then runs the plain (mode 0) or presized (mode 1, prediction given as
+ * a host float) form. */
+int bo_join_host(bo_ctx* ctx, const bo_join_build_cols* build_host, const bo_join_probe_cols* probe_host,
+                 const bo_join_params* params, int32_t mode, float predicted_rows, bo_join_result* out_host);
+
+/* ================================================================ SKETCH ==
+ * Per-column sketches for the learned sizing features, computed on the device
+ * once per table.  No reference counterpart. */
+#define BO_SKETCH_BINS 64
+typedef struct bo_sketch {
+  int64_t n;
+  int64_t min, max;
+  int64_t hist[BO_SKETCH_BINS];  /* equi-width over [min, max]: bin = (v-min)*64/(max-min+1) */
+  double distinct_estimate;      /* HyperLogLog, 4096 registers */
+} bo_sketch;
+/* int32 column (device) -> sketch (host); synchronises. */
+int bo_sketch_i32(bo_ctx* ctx, const int32_t* col_device, int64_t n, bo_sketch* out_host);
+/* Exact histogram of a uint8 (elem_bytes 1) or uint16 (2) device column with
+ * values < domain <= 65536; hist_host receives `domain` counts. */
+int bo_histogram_small(bo_ctx* ctx, const void* col_device, int32_t elem_bytes, int64_t n, int32_t domain,
+                       int64_t* hist_host);
+
+/* ==================================================================== MLP ==
+ * Learned sizing: a small FP32 MLP (n_features -> 64 -> 64 -> 64 -> n_outputs,
+ * ReLU) trained on the GPU by its own kernels.  Targets are log1p(counts);
+ * predictions presize hash tables and output buffers.  No reference
+ * counterpart (the reference sizes its dense arrays exactly, e.g.
+ * bespoke_tpch/query_q3.cpp:178-180).  n_features <= 32, n_outputs <= 4.
+ * Parameter layout: W1[F][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64]
+ * W4[64][O] b4[O] (row-major, x @ W). */
+typedef struct bo_mlp bo_mlp;
+
+int bo_mlp_create(bo_ctx* ctx, int32_t n_features, int32_t n_outputs, uint64_t seed, bo_mlp** out);
+void bo_mlp_destroy(bo_mlp* mlp);
+int32_t bo_mlp_num_params(const bo_mlp* mlp);
+int bo_mlp_get_params(bo_ctx* ctx, const bo_mlp* mlp, float* host_out);
+int bo_mlp_set_params(bo_ctx* ctx, bo_mlp* mlp, const float* host_in);
+/* Gradient of the loss 0.5*mean((y - t)^2) w.r.t. every parameter (device
+ * buffers: x [n][F], t [n][O], grad [P], loss [1]); deterministic. */
+int bo_mlp_gradients_device(bo_ctx* ctx, bo_mlp* mlp, const float* x, const float* t, int32_t n,
+                            float* grad_device, float* loss_device);
+/* One Adam step on a batch (device buffers). */
+int bo_mlp_train_step_device(bo_ctx* ctx, bo_mlp* mlp, const float* x, const float* t, int32_t n, float lr,
+                             float* loss_device);
+/* `epochs` full-batch Adam steps on host data (copied in once). */
+int bo_mlp_train_host(bo_ctx* ctx, bo_mlp* mlp, const float* x_host, const float* t_host, int32_t n,
+                      int32_t epochs, float lr, float* final_loss);
+int bo_mlp_infer_device(bo_ctx* ctx, const bo_mlp* mlp, const float* x, int32_t n, float* y);
+/* One feature vector (host, passed to the kernel by value: no copy) ->
+ * counts_device[o] = max(expm1(y[o]), 0); log_device (optional) = y. */
+int bo_mlp_predict_counts(bo_ctx* ctx, const bo_mlp* mlp, const float* features_host, float* counts_device,
+                          float* log_device);
 
 #ifdef __cplusplus
 }
