@@ -24,6 +24,9 @@
 //  * the last block to finish (ticket counter) converts the totals into the
 //    output records and re-zeroes the accumulators for the next call, so a
 //    query is a single launch with no memset.
+#include <algorithm>
+#include <mutex>
+
 #include "common.cuh"
 #include "context.cuh"
 
@@ -618,3 +621,116 @@ int bo_q6_lineitem_host(bo_ctx* ctx, const bo_lineitem_cols* h, int16_t start_of
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free variant of the wide-layout scan / group-aggregate.
+//
+// Some callers cannot allocate device memory at the moment they run a query:
+// code executing while another component owns every device allocation (a
+// host database's memory manager, a plugin sandbox), code running between
+// allocations it may not interleave with (inside a stream-ordered region whose
+// owner forbids cudaMalloc, or on a path that must not synchronise the device,
+// which cudaMalloc / cudaFree can do).  For them this entry point takes no
+// context and allocates nothing: the caller passes the stream, the inputs, the
+// output and an optional status word; the kernel's scratch (the 128-bit
+// per-group totals and the last-block ticket) lives in the file-scope device
+// array below, which every GPU that loads this library holds until exit.
+//
+// Limits and rules (also stated in include/bespoke_gpu.h):
+//  * at most BO_Q1_MAX_GROUPS groups (the size the array is laid out for);
+//    larger group domains are rejected with BO_ERR_INVALID;
+//  * every call shares the array: calls whose work overlaps on the GPU race
+//    and must be serialised by the caller (one stream, or events);
+//  * each call clears the array on its stream before the kernel, so a call
+//    never depends on what an earlier (possibly failed) call left behind;
+//  * the first call on a device resolves the array's device address
+//    (cudaGetSymbolAddress, with that device current) and sets the kernel's
+//    shared-memory attribute; make that first call before any stream capture.
+// ===========================================================================
+namespace bo {
+namespace {
+
+constexpr int kNoAllocAccWords = 2 * kQ1Sums * BO_Q1_MAX_GROUPS;  // 128-bit totals
+constexpr int kNoAllocWords = kNoAllocAccWords + 32;               // + ticket counter
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned long long g_q1_noalloc_scratch[kNoAllocWords];
+
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+int g_noalloc_sms[kNoAllocMaxDevices] = {};
+
+// Per-device set-up, done once with the device current: the array's device
+// address (a host-side use of the symbol would be a host stand-in, not a
+// device address) and the kernels' dynamic shared-memory opt-in.
+int noalloc_setup(int device, unsigned long long** scratch, int* sms) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_q1_noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return BO_ERR_CUDA;
+    }
+    int n_sms = 0;
+    if (cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || n_sms < 1)
+      return BO_ERR_CUDA;
+    if (cudaFuncSetAttribute(reinterpret_cast<const void*>(&q1_fact_kernel<6>),
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q1_smem_bytes<6>(true)) != cudaSuccess ||
+        cudaFuncSetAttribute(reinterpret_cast<const void*>(&q1_fact_kernel<8>),
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)q1_smem_bytes<8>(true)) != cudaSuccess)
+      return BO_ERR_CUDA;
+    g_noalloc_sms[device] = n_sms;
+    g_noalloc_ptr[device] = static_cast<unsigned long long*>(p);
+  }
+  *scratch = g_noalloc_ptr[device];
+  *sms = g_noalloc_sms[device];
+  return BO_OK;
+}
+
+template <int NG>
+int noalloc_launch(const bo_fact_cols& c, int32_t cutoff, uint32_t nfa, uint32_t nfb, unsigned long long* scratch,
+                   int sms, bo_q1_agg* out, uint32_t* status, cudaStream_t stream) {
+  const void* k = reinterpret_cast<const void*>(&q1_fact_kernel<NG>);
+  constexpr size_t smem = q1_smem_bytes<NG>(true);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kScanBlock, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int64_t chunks = c.n_rows >> 2;
+  const int64_t cap = (kMaxRowsPerThread - 1) / 4;
+  const int64_t need = (chunks + cap * kScanBlock - 1) / (cap * kScanBlock);
+  int64_t grid = std::max<int64_t>((int64_t)sms * per_sm, need);
+  grid = std::min<int64_t>(std::max<int64_t>(grid, 1), 0x7fffffff);
+  q1_fact_kernel<NG><<<(int)grid, kScanBlock, smem, stream>>>(
+      c, cutoff, nfa, nfb, scratch, reinterpret_cast<uint32_t*>(scratch + kNoAllocAccWords), out, status);
+  return cudaGetLastError() == cudaSuccess ? BO_OK : BO_ERR_CUDA;
+}
+
+}  // namespace
+}  // namespace bo
+
+extern "C" int bo_q1_fact_device_noalloc(const bo_fact_cols* cols, int32_t ship_cutoff, int32_t n_flag_a,
+                                         int32_t n_flag_b, bo_q1_agg* out_device, uint32_t* status_device,
+                                         void* cuda_stream) {
+  if (!cols || !out_device || cols->n_rows < 0) return BO_ERR_INVALID;
+  if (n_flag_a < 1 || n_flag_b < 1 || n_flag_a * n_flag_b > BO_Q1_MAX_GROUPS) return BO_ERR_INVALID;
+  if (cols->n_rows > 0) {
+    const void* ptrs[] = {cols->ship_date, cols->quantity, cols->ext_price, cols->discount,
+                          cols->tax,       cols->flag_a,   cols->flag_b};
+    for (const void* p : ptrs)
+      if (!p || !aligned32(p)) return BO_ERR_INVALID;
+  }
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kNoAllocMaxDevices) return BO_ERR_CUDA;
+  unsigned long long* scratch = nullptr;
+  int sms = 0;
+  int rc = noalloc_setup(device, &scratch, &sms);
+  if (rc) return rc;
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  if (cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * kNoAllocWords, stream) != cudaSuccess)
+    return BO_ERR_CUDA;
+  const int ng = n_flag_a * n_flag_b;
+  return ng <= 6 ? noalloc_launch<6>(*cols, ship_cutoff, n_flag_a, n_flag_b, scratch, sms, out_device,
+                                     status_device, stream)
+                 : noalloc_launch<8>(*cols, ship_cutoff, n_flag_a, n_flag_b, scratch, sms, out_device,
+                                     status_device, stream);
+}

@@ -153,6 +153,7 @@ _SIGNATURES = {
     "bo_launch_count": (C.c_int64, [_P]),
     "bo_q1_fact_device": (C.c_int, [_P, C.POINTER(FactCols), C.c_int32, C.c_int32, C.c_int32, _P]),
     "bo_q1_fact_host": (C.c_int, [_P, C.POINTER(FactCols), C.c_int32, C.c_int32, C.c_int32, C.POINTER(Q1Agg)]),
+    "bo_q1_fact_device_noalloc": (C.c_int, [C.POINTER(FactCols), C.c_int32, C.c_int32, C.c_int32, _P, _P, _P]),
     "bo_q1_lineitem_device": (C.c_int, [_P, C.POINTER(LineitemCols), C.c_int16, C.c_int32, _P]),
     "bo_q1_lineitem_host": (C.c_int, [_P, C.POINTER(LineitemCols), C.c_int16, C.c_int32, C.POINTER(Q1Agg)]),
     "bo_q6_lineitem_device": (

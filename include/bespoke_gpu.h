@@ -139,6 +139,28 @@ int bo_q1_fact_device(bo_ctx* ctx, const bo_fact_cols* cols, int32_t ship_cutoff
 int bo_q1_fact_host(bo_ctx* ctx, const bo_fact_cols* host_cols, int32_t ship_cutoff,
                     int32_t n_flag_a, int32_t n_flag_b, bo_q1_agg* out_host);
 
+/* Allocation-free variant of bo_q1_fact_device.  It has no counterpart in the
+ * reference.  It is for callers that cannot allocate device memory when they
+ * run the query -- a host process whose memory manager owns every device
+ * allocation, a plugin that may not call cudaMalloc, or a path that must not
+ * risk the device-wide synchronisation cudaMalloc / cudaFree can cause.  It
+ * takes no context and allocates nothing: the caller passes the CUDA stream
+ * (cudaStream_t as void*, NULL = legacy default stream), the device columns,
+ * out_device (n_flag_a*n_flag_b records) and an optional status_device word
+ * that the kernel ORs device-side error bits into (the caller zeroes it).
+ * The kernel's scratch -- 128-bit per-group totals and a ticket counter --
+ * is a fixed file-scope device array of (2*8*BO_Q1_MAX_GROUPS + 32) 64-bit
+ * words (1,280 bytes) that every GPU loading this library holds until exit;
+ * group domains above BO_Q1_MAX_GROUPS are rejected with BO_ERR_INVALID.
+ * Each call clears that array on its stream first; calls that overlap on the
+ * GPU share it and race, so the caller must serialise them.  The first call
+ * on a device resolves the array's device address and sets a kernel
+ * attribute: make it before any stream capture.  Returns BO_OK, BO_ERR_INVALID
+ * or BO_ERR_CUDA (no message: there is no context). */
+int bo_q1_fact_device_noalloc(const bo_fact_cols* cols, int32_t ship_cutoff, int32_t n_flag_a,
+                              int32_t n_flag_b, bo_q1_agg* out_device, uint32_t* status_device,
+                              void* cuda_stream);
+
 /* Storage-plan layout: keep rows with shipdate <= cutoff_offset (the int16
  * cutoff run_q1 derives at query_q1.cpp:111-115); n_groups =
  * returnflag_count * linestatus_count (<= 8). */
