@@ -65,6 +65,11 @@ int device_error_status(bo_ctx* ctx, uint32_t bits, const char* op);
 // Blocks per SM from the occupancy calculator, cached per kernel.
 int occupancy_blocks(const void* kernel, int block, size_t smem);
 
+// Stable LSD radix sort of (key, value) pairs by bits [begin_bit, end_bit)
+// (csrc/radix_sort.cu); n_dev, if given, is the actual count (<= n) on the device.
+int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsigned long long* tmp_keys,
+                     uint32_t* tmp_vals, int64_t n, int begin_bit, int end_bit, const unsigned long long* n_dev);
+
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 // Column pointers must be 32-byte aligned: the scans use 256-bit vector loads.
 inline bool aligned32(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 31u) == 0; }

@@ -1,0 +1,733 @@
+// Skewed three-way join + high-cardinality group-by + ordered top-k (K4, with
+// the K5 onesweep sort and K6 top-k of radix_sort.cu).
+//
+// Reference patterns this restates (no reference function computes the whole
+// pipeline verbatim):
+//   * dimension filters turned into dense masks and fact scans that count per
+//     id with bounds checks: bespoke_ceb/query_q1a.cpp (mask builders before
+//     :156, cast_info scan :503-601);
+//   * group-by with a min aggregate: bespoke_ceb/query_q10a.cpp:843-856;
+//   * order by count desc, id asc: bespoke_tpch/query_q10.cpp:318-372.
+//
+// Pipeline for  A(id)  B(a_id, c_id)  C(category, year; c_id = row index):
+//   init     capacity (host exact count, or device-side from a predicted group
+//            count), clear the group table, the Bloom filter and the A mask;
+//   cfilter  C rows -> exact pass bitmap (one 32-row word per thread, no
+//            atomics) and the passing ids into a 64 KB blocked Bloom filter;
+//   amask    A ids -> bitmap over [0, a_id_max];
+//   scan     B streamed 16 rows per lane (256-bit c_id loads); the Bloom filter
+//            (TMA-staged into shared memory) rejects ~97% of rows without
+//            leaving the SM; hits are compacted per warp, checked against the
+//            exact bitmap and the A mask, and only survivors load their a_id
+//            and the C year (late materialisation).  Survivors aggregate first
+//            into a per-block shared-memory table (count, min year) so Zipf
+//            heavy hitters cost one global update per block, then the block
+//            flushes into a global open-addressing table (key << 32 | count
+//            with 64-bit atomicCAS, min year by atomicMin).  The plain form's
+//            exact pre-pass runs the same scan setting bits of a distinct
+//            bitmap instead;
+//   compact  occupied slots -> packed sort keys ((cmax - count) << wa | a_id)
+//            with the min year as the value;
+//   sort     onesweep LSD radix sort over the key bits actually used, key
+//            count read from the device (no host round trip);
+//   topk     first k sorted entries decoded into the result record.
+#include <algorithm>
+
+#include "common.cuh"
+#include "context.cuh"
+
+namespace bo {
+
+constexpr unsigned long long kGbEmpty = ~0ull;
+constexpr int kGbBloomLog2Words = 14;
+constexpr uint32_t kGbBloomWords = 1u << kGbBloomLog2Words;
+constexpr uint32_t kGbBloomBytes = kGbBloomWords * 4u;
+constexpr int kGbBlock = 512;
+constexpr int kGbWarps = kGbBlock / 32;
+constexpr int kGbRowsPerLane = 16;
+constexpr int kGbRowsPerWarpStep = 32 * kGbRowsPerLane;
+constexpr int kGbQueue = 32 * 8;
+constexpr int kGbLocalSlots = 1024;  // per-block pre-aggregation table
+constexpr int kGbMinCapLog2 = 10;
+constexpr float kGbPresizeFactor = 2.5f;
+constexpr int kMaxCats = 64;
+
+struct GbMeta {
+  int32_t cap_log2;
+  uint32_t overflow;
+  uint32_t done;
+  uint32_t pad;
+  unsigned long long joined;          // joined (surviving) B rows
+  unsigned long long distinct;        // groups inserted into the global table
+  unsigned long long n_out;           // compacted groups (sort key count)
+  unsigned long long c_pass;          // qualifying C rows
+  unsigned long long exact_distinct;  // plain pre-pass result
+};
+
+struct CatSet {
+  uint16_t v[kMaxCats];
+  int32_t n;
+};
+
+__device__ __forceinline__ void gb_bloom_pos(uint32_t c, uint32_t& word, uint32_t& bits) {
+  const uint32_t h2 = (c * 0x9E3779B1u) ^ ((c >> 15) * 0x85EBCA6Bu);
+  const uint32_t h3 = h2 * 0xC2B2AE35u + 0x27D4EB2Fu;
+  word = h3 >> (32 - kGbBloomLog2Words);
+  bits = (1u << (h3 & 31u)) | (1u << ((h3 >> 5) & 31u));
+}
+
+__device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t& total) {
+  const int lane = threadIdx.x & 31;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+__device__ __forceinline__ int32_t gb_presize_log2(const float* pred, int32_t host_log2, int32_t max_log2) {
+  if (!pred) return host_log2;
+  float p = *pred;
+  if (!(p >= 0.0f)) p = 0.0f;
+  const double want = (double)p * kGbPresizeFactor;
+  int32_t cl = kGbMinCapLog2;
+  while (cl < max_log2 && (double)(1ull << cl) < want) ++cl;
+  return cl;
+}
+
+// ------------------------------------------------------------------ init --
+// clear_filters = 0 re-initialises only the group table (the plain form's
+// second phase keeps the C bitmap, Bloom filter, A mask and filter counters).
+__global__ void gb_init_kernel(unsigned long long* slots, int32_t* mins, uint32_t* bloom, uint32_t* amask,
+                               uint32_t* dbits, int64_t mask_words, GbMeta* meta, const float* pred, int32_t host_log2,
+                               int32_t max_log2, int clear_filters) {
+  const int32_t cl = gb_presize_log2(pred, host_log2, max_log2);
+  const uint64_t cap = 1ull << cl;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t i = tid; i < cap; i += stride) {
+    slots[i] = kGbEmpty;
+    mins[i] = 0x7fffffff;
+  }
+  if (clear_filters) {
+    for (uint64_t i = tid; i < kGbBloomWords; i += stride) bloom[i] = 0;
+    for (uint64_t i = tid; i < (uint64_t)mask_words; i += stride) {
+      amask[i] = 0;
+      if (dbits) dbits[i] = 0;
+    }
+  }
+  if (tid == 0) {
+    meta->cap_log2 = cl;
+    meta->overflow = 0;
+    meta->done = 0;
+    meta->joined = 0;
+    meta->distinct = 0;
+    meta->n_out = 0;
+    if (clear_filters) {
+      meta->c_pass = 0;
+      meta->exact_distinct = 0;
+    }
+  }
+}
+
+// --------------------------------------------------------------- cfilter --
+// Thread w owns C rows [32w, 32w+32): one full bitmap word, written with a
+// plain store.  The category set lives in a shared 65536-bit mask.
+__global__ void __launch_bounds__(256) gb_cfilter_kernel(bo_gb_c_cols c, CatSet cats, int32_t year_lo,
+                                                         int32_t year_hi, uint32_t* __restrict__ cbits,
+                                                         uint32_t* __restrict__ bloom, GbMeta* meta) {
+  __shared__ uint32_t catmask[2048];
+  for (int i = threadIdx.x; i < 2048; i += blockDim.x) catmask[i] = 0;
+  __syncthreads();
+  if (threadIdx.x < cats.n) atomicOr(&catmask[cats.v[threadIdx.x] >> 5], 1u << (cats.v[threadIdx.x] & 31u));
+  __syncthreads();
+  const int64_t n = c.n_rows;
+  const int64_t words = (n + 31) / 32;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  uint32_t passed = 0;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += stride) {
+    const int64_t r0 = w * 32;
+    uint32_t bits = 0;
+    if (r0 + 32 <= n) {
+      int8v cat[2];
+      cat[0] = ld_stream_v8(c.category + r0);
+      cat[1] = ld_stream_v8(c.category + r0 + 16);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int8v y = ld_stream_v8(c.year + r0 + 8 * q);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int row = 8 * q + k;
+          const uint32_t word = (uint32_t)cat[row >> 4].v[(row & 15) >> 1];
+          const uint32_t cv = (row & 1) ? (word >> 16) : (word & 0xffffu);
+          const bool ok = ((catmask[cv >> 5] >> (cv & 31u)) & 1u) && y.v[k] >= year_lo && y.v[k] <= year_hi;
+          bits |= (uint32_t)ok << row;
+        }
+      }
+    } else {
+      for (int k = 0; k < 32 && r0 + k < n; ++k) {
+        const uint32_t cv = c.category[r0 + k];
+        const int32_t y = c.year[r0 + k];
+        const bool ok = ((catmask[cv >> 5] >> (cv & 31u)) & 1u) && y >= year_lo && y <= year_hi;
+        bits |= (uint32_t)ok << k;
+      }
+    }
+    cbits[w] = bits;
+    passed += __popc(bits);
+    uint32_t b = bits;
+    while (b) {
+      const int k = __ffs(b) - 1;
+      b &= b - 1;
+      uint32_t bw, bb;
+      gb_bloom_pos((uint32_t)(r0 + k), bw, bb);
+      atomicOr(bloom + bw, bb);
+    }
+  }
+  __shared__ uint32_t part[8];
+  passed = warp_sum_u32(passed);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = passed;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += part[i];
+    if (t) atomicAdd(&meta->c_pass, (unsigned long long)t);
+  }
+}
+
+// ----------------------------------------------------------------- amask --
+__global__ void gb_amask_kernel(bo_gb_a_cols a, int32_t a_id_max, uint32_t* __restrict__ amask, uint32_t* err) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  uint32_t bad = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n_rows; i += stride) {
+    const int32_t id = a.id[i];
+    if (id < 0) continue;  // the reference's id masks skip negative ids
+    if (id > a_id_max) {
+      bad = 1;
+      continue;
+    }
+    atomicOr(amask + (id >> 5), 1u << (id & 31));
+  }
+  if (bad) raise_error(err, kErrValueRange);
+}
+
+// ------------------------------------------------------------------ scan --
+__device__ __forceinline__ bool gb_global_insert(unsigned long long* slots, int32_t* mins, uint64_t mask, uint32_t key,
+                                                 uint32_t cnt, int32_t mn, uint32_t& newkeys) {
+  uint64_t idx = hash32(key) & mask;
+  const unsigned long long claim = (unsigned long long)key << 32;
+  for (uint64_t step = 0; step <= mask; ++step) {
+    unsigned long long v = slots[idx];
+    if (v == kGbEmpty) {
+      v = atomicCAS(slots + idx, kGbEmpty, claim);
+      if (v == kGbEmpty) {
+        ++newkeys;
+        v = claim;
+      }
+    }
+    if ((uint32_t)(v >> 32) == key) {
+      atomicAdd(slots + idx, (unsigned long long)cnt);
+      atomicMin(mins + idx, mn);
+      return true;
+    }
+    idx = (idx + 1) & mask;
+  }
+  return false;
+}
+
+// kMode 0: exact distinct pre-pass (bits of a distinct bitmap); 1: aggregate.
+template <int kMode>
+__global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64_t n_c, int32_t a_id_max,
+                                                           const uint32_t* __restrict__ bloom_g,
+                                                           const uint32_t* __restrict__ cbits,
+                                                           const int32_t* __restrict__ c_year,
+                                                           const uint32_t* __restrict__ amask,
+                                                           unsigned long long* slots, int32_t* mins, uint32_t* dbits,
+                                                           GbMeta* meta, uint32_t* err) {
+  extern __shared__ __align__(128) uint32_t bloom_s[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int32_t q_c[kGbWarps][kGbQueue];
+  __shared__ uint16_t q_off[kGbWarps][kGbQueue];
+  __shared__ uint32_t l_key[kGbLocalSlots];
+  __shared__ uint32_t l_cnt[kGbLocalSlots];
+  __shared__ int32_t l_min[kGbLocalSlots];
+  __shared__ uint32_t red[3][kGbWarps];
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, kGbBloomBytes);
+    bulk_copy_g2s(bloom_s, bloom_g, kGbBloomBytes, &bar);
+  }
+  for (int i = threadIdx.x; i < kGbLocalSlots; i += blockDim.x) {
+    l_key[i] = 0xffffffffu;
+    l_cnt[i] = 0;
+    l_min[i] = 0x7fffffff;
+  }
+  __syncthreads();
+  // On a (never expected) timeout the filter is not used; the exact bitmap
+  // check below still decides, so the answer is unchanged.
+  const bool use_bloom = mbar_wait_bounded(&bar, 0, kWaitLimitNs);
+  uint32_t bad = use_bloom ? 0u : kErrSpinTimeout;
+  const int32_t cl = kMode ? __ldg(&meta->cap_log2) : 0;
+  const uint64_t mask = (1ull << cl) - 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int32_t* qc = q_c[warp];
+  uint16_t* qo = q_off[warp];
+  uint32_t joined = 0, newkeys = 0, full = 0;
+  const int64_t n = b.n_rows;
+  const int64_t steps = (n + kGbRowsPerWarpStep - 1) / kGbRowsPerWarpStep;
+  const int64_t nwarps = (int64_t)gridDim.x * kGbWarps;
+  for (int64_t st = (int64_t)blockIdx.x * kGbWarps + warp; st < steps; st += nwarps) {
+    const int64_t base = st * kGbRowsPerWarpStep;
+    const int64_t r0 = base + lane * kGbRowsPerLane;
+    int32_t cid[kGbRowsPerLane];
+    uint32_t valid = 0xffffu;
+    if (r0 + kGbRowsPerLane <= n) {
+      const int8v c0 = ld_stream_v8(b.c_id + r0), c1 = ld_stream_v8(b.c_id + r0 + 8);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        cid[k] = c0.v[k];
+        cid[8 + k] = c1.v[k];
+      }
+    } else {
+      valid = 0;
+#pragma unroll
+      for (int k = 0; k < kGbRowsPerLane; ++k) {
+        cid[k] = -1;
+        if (r0 + k < n) {
+          cid[k] = b.c_id[r0 + k];
+          valid |= 1u << k;
+        }
+      }
+    }
+    uint32_t hit = 0;
+#pragma unroll
+    for (int k = 0; k < kGbRowsPerLane; ++k) {
+      const uint32_t cv = (uint32_t)cid[k];
+      bool cand = cid[k] >= 0 && (int64_t)cid[k] < n_c;
+      if (use_bloom) {
+        uint32_t w, bits;
+        gb_bloom_pos(cv, w, bits);
+        cand = cand && (bloom_s[w] & bits) == bits;
+      }
+      hit |= (uint32_t)cand << k;
+    }
+    hit &= valid;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const uint32_t hm = (hit >> (8 * half)) & 0xffu;
+      uint32_t total;
+      uint32_t pos = warp_excl_scan(__popc(hm), total);
+      if (total == 0) continue;  // warp-uniform
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if ((hm >> k) & 1u) {
+          qc[pos] = cid[8 * half + k];
+          qo[pos] = (uint16_t)(lane * kGbRowsPerLane + 8 * half + k);
+          ++pos;
+        }
+      }
+      __syncwarp();
+      for (uint32_t i = lane; i < total; i += 32) {
+        const int32_t c = qc[i];
+        if (!((__ldg(cbits + (c >> 5)) >> (c & 31)) & 1u)) continue;
+        const int64_t row = base + qo[i];
+        const int32_t a = __ldg(b.a_id + row);
+        if (a < 0 || a > a_id_max || !((__ldg(amask + (a >> 5)) >> (a & 31)) & 1u)) continue;
+        ++joined;
+        if (kMode == 0) {
+          atomicOr(dbits + (a >> 5), 1u << (a & 31));
+        } else {
+          const int32_t y = __ldg(c_year + c);
+          const uint32_t h = hash32((uint32_t)a);
+          bool done = false;
+#pragma unroll 1
+          for (int p = 0; p < 8 && !done; ++p) {
+            const int s = (int)((h + p) & (kGbLocalSlots - 1));
+            const uint32_t old = atomicCAS(&l_key[s], 0xffffffffu, (uint32_t)a);
+            if (old == 0xffffffffu || old == (uint32_t)a) {
+              atomicAdd(&l_cnt[s], 1u);
+              atomicMin(&l_min[s], y);
+              done = true;
+            }
+          }
+          if (!done && !gb_global_insert(slots, mins, mask, (uint32_t)a, 1u, y, newkeys)) full = 1;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  if (kMode == 1) {
+    // Flush the block's pre-aggregated groups into the global table.
+    for (int i = threadIdx.x; i < kGbLocalSlots; i += blockDim.x) {
+      if (l_key[i] != 0xffffffffu)
+        if (!gb_global_insert(slots, mins, mask, l_key[i], l_cnt[i], l_min[i], newkeys)) full = 1;
+    }
+  }
+  if (!use_bloom) mbar_wait_bounded(&bar, 0, kWaitLimitNs);
+  if (bad) raise_error(err, bad);
+  const uint32_t wj = warp_sum_u32(joined), wn = warp_sum_u32(newkeys);
+  const unsigned wf = __any_sync(0xffffffffu, full != 0);
+  if (lane == 0) {
+    red[0][warp] = wj;
+    red[1][warp] = wn;
+    red[2][warp] = wf;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t tj = 0, tn = 0, tf = 0;
+    for (int w = 0; w < kGbWarps; ++w) {
+      tj += red[0][w];
+      tn += red[1][w];
+      tf |= red[2][w];
+    }
+    if (tj) atomicAdd(&meta->joined, (unsigned long long)tj);
+    if (tn) {
+      const unsigned long long before = atomicAdd(&meta->distinct, (unsigned long long)tn);
+      if (kMode == 1 && before + tn > (mask + 1) - ((mask + 1) >> 3)) atomicOr(&meta->overflow, 1u);
+    }
+    if (tf) atomicOr(&meta->overflow, 1u);
+  }
+}
+
+__global__ void gb_popcount_kernel(const uint32_t* __restrict__ dbits, int64_t words, GbMeta* meta) {
+  uint32_t c = 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) c += __popc(dbits[i]);
+  c = warp_sum_u32(c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&meta->exact_distinct, (unsigned long long)c);
+}
+
+// --------------------------------------------------------------- compact --
+__global__ void gb_compact_kernel(const unsigned long long* __restrict__ slots, const int32_t* __restrict__ mins,
+                                  GbMeta* meta, int wa, unsigned long long cmax, unsigned long long* __restrict__ keys,
+                                  uint32_t* __restrict__ vals) {
+  const int32_t cl = __ldg(&meta->cap_log2);
+  const uint64_t cap = 1ull << cl;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  // Uniform trip count per warp so the warp-aggregated slot reservation stays converged.
+  const uint64_t cap_w = (cap + 31) & ~31ull;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap_w; i += stride) {
+    const unsigned long long v = i < cap ? slots[i] : kGbEmpty;
+    const bool occ = v != kGbEmpty;
+    const uint32_t ballot = __ballot_sync(0xffffffffu, occ);
+    if (!ballot) continue;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(&meta->n_out, (unsigned long long)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (occ) {
+      const unsigned long long pos = base + __popc(ballot & ((1u << lane) - 1u));
+      const unsigned long long cnt = v & 0xffffffffull;
+      const unsigned long long key = v >> 32;
+      keys[pos] = ((cmax - cnt) << wa) | key;
+      vals[pos] = (uint32_t)mins[i];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ topk --
+__global__ void gb_topk_kernel(const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ vals,
+                               GbMeta* meta, int k, int wa, unsigned long long cmax, int mode,
+                               bo_gb_result* __restrict__ out) {
+  const unsigned long long n = __ldcg(&meta->n_out);
+  const int t = threadIdx.x;
+  if (t < k && (unsigned long long)t < n) {
+    const unsigned long long key = keys[t];
+    bo_gb_row r;
+    r.a_id = (int32_t)(key & ((1ull << wa) - 1ull));
+    r.min_year = (int32_t)vals[t];
+    r.count = (int64_t)(cmax - (key >> wa));
+    out->rows[t] = r;
+  }
+  if (t == 0) {
+    out->n_groups = (int64_t)n;
+    out->joined_rows = (int64_t)__ldcg(&meta->joined);
+    out->c_qualifying = (int64_t)__ldcg(&meta->c_pass);
+    out->capacity_log2 = __ldcg(&meta->cap_log2);
+    out->overflowed = (int32_t)__ldcg(&meta->overflow);
+    out->reruns = 0;
+    out->mode = mode;
+    out->n_rows_out = (int32_t)(n < (unsigned long long)k ? n : (unsigned long long)k);
+    out->exact_distinct = (int64_t)__ldcg(&meta->exact_distinct);
+  }
+}
+
+// ------------------------------------------------------------------ host --
+namespace {
+
+int bit_length(uint64_t v) {
+  int b = 0;
+  while (v) {
+    ++b;
+    v >>= 1;
+  }
+  return b;
+}
+
+struct GbWs {
+  unsigned long long* slots;
+  int32_t* mins;
+  uint32_t* bloom;
+  uint32_t* cbits;
+  uint32_t* amask;
+  uint32_t* dbits;
+  GbMeta* meta;
+  float* pred;
+  unsigned long long* keys;
+  uint32_t* vals;
+  unsigned long long* tkeys;
+  uint32_t* tvals;
+  int32_t max_log2;
+  int64_t mask_words;
+};
+
+template <class T>
+T* carve(char*& p, size_t count) {
+  T* r = reinterpret_cast<T*>(p);
+  p += (sizeof(T) * count + 255) & ~size_t(255);
+  return r;
+}
+
+int gb_workspace(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, int32_t a_id_max, GbWs* ws) {
+  const uint64_t groups_max = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)a_id_max + 1, (uint64_t)b.n_rows));
+  const int32_t max_log2 = std::max(kGbMinCapLog2, bit_length(groups_max * 2 - 1));
+  const uint64_t cap = 1ull << max_log2;
+  const int64_t mask_words = ((int64_t)a_id_max + 1 + 31) / 32;
+  const int64_t cwords = (c.n_rows + 31) / 32;
+  size_t total = 0;
+  auto add = [&](size_t bytes) { total += (bytes + 255) & ~size_t(255); };
+  add(8 * cap);                       // slots
+  add(4 * cap);                       // mins
+  add(kGbBloomBytes);                 // bloom
+  add(4 * (size_t)std::max<int64_t>(cwords, 1));
+  add(4 * (size_t)mask_words);        // amask
+  add(4 * (size_t)mask_words);        // dbits
+  add(sizeof(GbMeta) + 64);
+  add(8 * cap);                       // keys
+  add(4 * cap);                       // vals
+  add(8 * cap);                       // tmp keys
+  add(4 * cap);                       // tmp vals
+  void* base = nullptr;
+  int rc = region(ctx, "gb_ws", total, &base);
+  if (rc) return rc;
+  char* p = static_cast<char*>(base);
+  ws->slots = carve<unsigned long long>(p, cap);
+  ws->mins = carve<int32_t>(p, cap);
+  ws->bloom = carve<uint32_t>(p, kGbBloomWords);
+  ws->cbits = carve<uint32_t>(p, (size_t)std::max<int64_t>(cwords, 1));
+  ws->amask = carve<uint32_t>(p, (size_t)mask_words);
+  ws->dbits = carve<uint32_t>(p, (size_t)mask_words);
+  char* meta_p = p;
+  p += (sizeof(GbMeta) + 64 + 255) & ~size_t(255);
+  ws->meta = reinterpret_cast<GbMeta*>(meta_p);
+  ws->pred = reinterpret_cast<float*>(meta_p + sizeof(GbMeta));
+  ws->keys = carve<unsigned long long>(p, cap);
+  ws->vals = carve<uint32_t>(p, cap);
+  ws->tkeys = carve<unsigned long long>(p, cap);
+  ws->tvals = carve<uint32_t>(p, cap);
+  ws->max_log2 = max_log2;
+  ws->mask_words = mask_words;
+  return BO_OK;
+}
+
+int check_gb(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
+             const bo_gb_params* prm) {
+  if (!a || !b || !c || !prm) return set_error(ctx, BO_ERR_INVALID, "groupby: null argument");
+  if (a->n_rows < 0 || b->n_rows < 0 || c->n_rows < 0) return set_error(ctx, BO_ERR_INVALID, "groupby: negative rows");
+  if (c->n_rows > 0x7fffffffll || b->n_rows > 0xffffffffll)
+    return set_error(ctx, BO_ERR_INVALID, "groupby: C above 2^31 rows or B above 2^32 rows");
+  if (prm->a_id_max < 0) return set_error(ctx, BO_ERR_INVALID, "groupby: a_id_max must be >= 0");
+  if (prm->k < 0 || prm->k > BO_GB_MAX_K) return set_error(ctx, BO_ERR_INVALID, "groupby: k outside [0, %d]", BO_GB_MAX_K);
+  if (prm->n_categories < 0 || prm->n_categories > kMaxCats || (prm->n_categories > 0 && !prm->categories))
+    return set_error(ctx, BO_ERR_INVALID, "groupby: at most %d categories", kMaxCats);
+  if (b->n_rows > 0 && (!b->a_id || !b->c_id || !aligned32(b->a_id) || !aligned32(b->c_id)))
+    return set_error(ctx, BO_ERR_INVALID, "groupby: B columns null or not 32-byte aligned");
+  if (c->n_rows > 0 && (!c->category || !c->year || !aligned32(c->category) || !aligned32(c->year)))
+    return set_error(ctx, BO_ERR_INVALID, "groupby: C columns null or not 32-byte aligned");
+  if (a->n_rows > 0 && !a->id) return set_error(ctx, BO_ERR_INVALID, "groupby: A column null");
+  return BO_OK;
+}
+
+int grid_res(bo_ctx* ctx, const void* k, int block, size_t smem, int64_t items) {
+  const int64_t resident = (int64_t)ctx->num_sms * occupancy_blocks(k, block, smem);
+  const int64_t need = (items + block - 1) / block;
+  return (int)std::max<int64_t>(1, std::min(resident, need));
+}
+
+// Filters (init, C filter, A mask): common to both forms.
+int gb_prepare(bo_ctx* ctx, const bo_gb_a_cols& a, const bo_gb_c_cols& c, const bo_gb_params& prm, const GbWs& ws,
+               const float* pred, int32_t host_log2) {
+  const void* ki = reinterpret_cast<const void*>(&gb_init_kernel);
+  const int gi = grid_res(ctx, ki, 256, 0, std::max<int64_t>((int64_t)1 << std::min(ws.max_log2, 24), ws.mask_words));
+  gb_init_kernel<<<gi, 256, 0, ctx->stream>>>(ws.slots, ws.mins, ws.bloom, ws.amask, ws.dbits, ws.mask_words, ws.meta,
+                                              pred, host_log2, ws.max_log2, 1);
+  int rc = after_launch(ctx, "gb_init_kernel");
+  if (rc) return rc;
+  CatSet cs{};
+  cs.n = prm.n_categories;
+  for (int i = 0; i < prm.n_categories; ++i) cs.v[i] = prm.categories[i];
+  const int64_t cwords = (c.n_rows + 31) / 32;
+  if (cwords > 0) {
+    const void* kc = reinterpret_cast<const void*>(&gb_cfilter_kernel);
+    const int gc = grid_res(ctx, kc, 256, 0, cwords);
+    gb_cfilter_kernel<<<gc, 256, 0, ctx->stream>>>(c, cs, prm.year_lo, prm.year_hi, ws.cbits, ws.bloom, ws.meta);
+    if ((rc = after_launch(ctx, "gb_cfilter_kernel"))) return rc;
+  }
+  if (a.n_rows > 0) {
+    const void* ka = reinterpret_cast<const void*>(&gb_amask_kernel);
+    const int ga = grid_res(ctx, ka, 256, 0, a.n_rows);
+    gb_amask_kernel<<<ga, 256, 0, ctx->stream>>>(a, prm.a_id_max, ws.amask, ctx->d_err);
+    if ((rc = after_launch(ctx, "gb_amask_kernel"))) return rc;
+  }
+  return BO_OK;
+}
+
+template <int kMode>
+int gb_launch_scan(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, const bo_gb_params& prm,
+                   const GbWs& ws) {
+  const void* k = reinterpret_cast<const void*>(&gb_scan_kernel<kMode>);
+  static bool ready = false;
+  if (!ready) {
+    BO_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGbBloomBytes));
+    ready = true;
+  }
+  const int grid = grid_res(ctx, k, kGbBlock, kGbBloomBytes, (b.n_rows + kGbRowsPerLane - 1) / kGbRowsPerLane);
+  gb_scan_kernel<kMode><<<grid, kGbBlock, kGbBloomBytes, ctx->stream>>>(b, c.n_rows, prm.a_id_max, ws.bloom, ws.cbits,
+                                                                        c.year, ws.amask, ws.slots, ws.mins, ws.dbits,
+                                                                        ws.meta, ctx->d_err);
+  return after_launch(ctx, "gb_scan_kernel");
+}
+
+// Aggregate + compact + sort + top-k, asynchronous.
+int gb_aggregate_order(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, const bo_gb_params& prm,
+                       const GbWs& ws, bo_gb_result* out, int32_t mode) {
+  int rc = gb_launch_scan<1>(ctx, b, c, prm, ws);
+  if (rc) return rc;
+  const int wa = std::max(1, bit_length((uint64_t)prm.a_id_max));
+  const int wc = std::max(1, bit_length((uint64_t)b.n_rows));
+  const unsigned long long cmax = (wc >= 64) ? ~0ull : ((1ull << wc) - 1ull);
+  const uint64_t cap_max = 1ull << ws.max_log2;
+  const void* kc = reinterpret_cast<const void*>(&gb_compact_kernel);
+  const int gc = grid_res(ctx, kc, 256, 0, (int64_t)cap_max);
+  gb_compact_kernel<<<gc, 256, 0, ctx->stream>>>(ws.slots, ws.mins, ws.meta, wa, cmax, ws.keys, ws.vals);
+  if ((rc = after_launch(ctx, "gb_compact_kernel"))) return rc;
+  if ((rc = radix_sort_pairs(ctx, ws.keys, ws.vals, ws.tkeys, ws.tvals, (int64_t)cap_max, 0, wa + wc, &ws.meta->n_out)))
+    return rc;
+  gb_topk_kernel<<<1, BO_GB_MAX_K, 0, ctx->stream>>>(ws.keys, ws.vals, ws.meta, prm.k, wa, cmax, mode, out);
+  return after_launch(ctx, "gb_topk_kernel");
+}
+
+int gb_finish(bo_ctx* ctx, bo_gb_result* host, const bo_gb_result* dev) {
+  BO_CUDA(ctx, cudaMemcpyAsync(host, dev, sizeof(bo_gb_result), cudaMemcpyDeviceToHost, ctx->stream));
+  uint32_t bits = 0;
+  int rc = consume_device_errors(ctx, &bits);
+  if (rc) return rc;
+  return device_error_status(ctx, bits, "groupby");
+}
+
+int gb_plain_impl(bo_ctx* ctx, const bo_gb_a_cols& a, const bo_gb_b_cols& b, const bo_gb_c_cols& c,
+                  const bo_gb_params& prm, bo_gb_result* out_host, int32_t reruns) {
+  GbWs ws;
+  int rc = gb_workspace(ctx, b, c, prm.a_id_max, &ws);
+  if (rc) return rc;
+  if ((rc = gb_prepare(ctx, a, c, prm, ws, nullptr, kGbMinCapLog2))) return rc;
+  // Exact pre-pass: distinct qualifying groups, then one host round trip.
+  if ((rc = gb_launch_scan<0>(ctx, b, c, prm, ws))) return rc;
+  const void* kp = reinterpret_cast<const void*>(&gb_popcount_kernel);
+  const int gp = grid_res(ctx, kp, 256, 0, ws.mask_words);
+  gb_popcount_kernel<<<gp, 256, 0, ctx->stream>>>(ws.dbits, ws.mask_words, ws.meta);
+  if ((rc = after_launch(ctx, "gb_popcount_kernel"))) return rc;
+  unsigned long long distinct = 0;
+  BO_CUDA(ctx, cudaMemcpyAsync(&distinct, &ws.meta->exact_distinct, sizeof(distinct), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const int32_t cl = std::min(ws.max_log2, std::max(kGbMinCapLog2, bit_length(std::max<uint64_t>(distinct, 1) * 2 - 1)));
+  // Re-initialise only the group table at the exact size; the filters stay.
+  const void* ki = reinterpret_cast<const void*>(&gb_init_kernel);
+  const int gi = grid_res(ctx, ki, 256, 0, (int64_t)1 << std::min(ws.max_log2, 24));
+  gb_init_kernel<<<gi, 256, 0, ctx->stream>>>(ws.slots, ws.mins, ws.bloom, ws.amask, ws.dbits, ws.mask_words, ws.meta,
+                                              nullptr, cl, ws.max_log2, 0);
+  if ((rc = after_launch(ctx, "gb_init_kernel"))) return rc;
+  void* dout = nullptr;
+  if ((rc = region(ctx, "gb_out", sizeof(bo_gb_result), &dout))) return rc;
+  bo_gb_result* d = static_cast<bo_gb_result*>(dout);
+  if ((rc = gb_aggregate_order(ctx, b, c, prm, ws, d, 0))) return rc;
+  if ((rc = gb_finish(ctx, out_host, d))) return rc;
+  out_host->reruns = reruns;
+  out_host->exact_distinct = (int64_t)distinct;
+  if (out_host->overflowed) return set_error(ctx, BO_ERR_OVERFLOW, "groupby: exact-size table overflowed");
+  return BO_OK;
+}
+
+}  // namespace
+}  // namespace bo
+
+using namespace bo;
+
+extern "C" {
+
+int bo_groupby_topk_plain(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
+                          const bo_gb_params* prm, bo_gb_result* out_host) {
+  BO_CHECK_CTX(ctx);
+  int rc = check_gb(ctx, a, b, c, prm);
+  if (rc) return rc;
+  if (!out_host) return set_error(ctx, BO_ERR_INVALID, "groupby: null output");
+  return gb_plain_impl(ctx, *a, *b, *c, *prm, out_host, 0);
+}
+
+int bo_groupby_topk_presized_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b,
+                                    const bo_gb_c_cols* c, const bo_gb_params* prm, const float* pred_groups_device,
+                                    bo_gb_result* out_device) {
+  BO_CHECK_CTX(ctx);
+  int rc = check_gb(ctx, a, b, c, prm);
+  if (rc) return rc;
+  if (!pred_groups_device || !out_device) return set_error(ctx, BO_ERR_INVALID, "groupby: null prediction/output");
+  GbWs ws;
+  if ((rc = gb_workspace(ctx, *b, *c, prm->a_id_max, &ws))) return rc;
+  if ((rc = gb_prepare(ctx, *a, *c, *prm, ws, pred_groups_device, 0))) return rc;
+  return gb_aggregate_order(ctx, *b, *c, *prm, ws, out_device, 1);
+}
+
+int bo_groupby_topk_presized(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
+                             const bo_gb_params* prm, const float* pred_groups_device, bo_gb_result* out_host) {
+  BO_CHECK_CTX(ctx);
+  if (!out_host) return set_error(ctx, BO_ERR_INVALID, "groupby: null output");
+  void* dout = nullptr;
+  int rc = region(ctx, "gb_out", sizeof(bo_gb_result), &dout);
+  if (rc) return rc;
+  bo_gb_result* d = static_cast<bo_gb_result*>(dout);
+  if ((rc = bo_groupby_topk_presized_device(ctx, a, b, c, prm, pred_groups_device, d))) return rc;
+  if ((rc = gb_finish(ctx, out_host, d))) return rc;
+  if (out_host->overflowed) {
+    if ((rc = gb_plain_impl(ctx, *a, *b, *c, *prm, out_host, 1))) return rc;
+    out_host->mode = 1;
+  }
+  return BO_OK;
+}
+
+int bo_groupby_distinct_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
+                               const bo_gb_params* prm, int64_t* out_device) {
+  BO_CHECK_CTX(ctx);
+  int rc = check_gb(ctx, a, b, c, prm);
+  if (rc) return rc;
+  if (!out_device) return set_error(ctx, BO_ERR_INVALID, "groupby: null output");
+  GbWs ws;
+  if ((rc = gb_workspace(ctx, *b, *c, prm->a_id_max, &ws))) return rc;
+  if ((rc = gb_prepare(ctx, *a, *c, *prm, ws, nullptr, kGbMinCapLog2))) return rc;
+  if ((rc = gb_launch_scan<0>(ctx, *b, *c, *prm, ws))) return rc;
+  const void* kp = reinterpret_cast<const void*>(&gb_popcount_kernel);
+  gb_popcount_kernel<<<grid_res(ctx, kp, 256, 0, ws.mask_words), 256, 0, ctx->stream>>>(ws.dbits, ws.mask_words,
+                                                                                          ws.meta);
+  if ((rc = after_launch(ctx, "gb_popcount_kernel"))) return rc;
+  // out[0] = exact distinct groups, out[1] = joined rows
+  BO_CUDA(ctx, cudaMemcpyAsync(out_device, &ws.meta->exact_distinct, sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+  BO_CUDA(ctx, cudaMemcpyAsync(out_device + 1, &ws.meta->joined, sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+  return BO_OK;
+}
+
+}  // extern "C"

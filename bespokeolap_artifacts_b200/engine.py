@@ -202,3 +202,63 @@ class Engine:
         self.ctx.call("bo_join_host", C.byref(b), C.byref(p), C.byref(N.JoinParams(j.date_lt, j.seg_eq)), mode,
                       float(predicted_rows), C.byref(out))
         return out.as_dict()
+
+    # ------------------------------------------------------- group-by ------
+    @staticmethod
+    def gb_args(a_id, b_a, b_c, c_cat, c_year, n_a, n_b, n_c, cat_set, year_lo, year_hi, k, a_id_max):
+        cats = np.ascontiguousarray(cat_set, dtype=np.uint16)
+        a = N.GbACols(N.ptr(a_id), n_a)
+        b = N.GbBCols(N.ptr(b_a), N.ptr(b_c), n_b)
+        c = N.GbCCols(N.ptr(c_cat), N.ptr(c_year), n_c)
+        prm = N.GbParams(cats.ctypes.data, len(cats), year_lo, year_hi, k, a_id_max)
+        return a, b, c, prm, cats
+
+    def groupby_plain(self, dev: dict, g) -> dict:
+        """Exact distinct pre-pass, one host round trip, aggregation, sort, top-k.
+        ``dev`` holds device columns a_ids, b_a, b_c, c_cat, c_year."""
+        a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
+                                          len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
+                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)))
+        out = N.GbResult()
+        self.ctx.call("bo_groupby_topk_plain", C.byref(a), C.byref(b), C.byref(c), C.byref(prm), C.byref(out))
+        return out.as_dict()
+
+    def groupby_presized(self, dev: dict, g, pred_dev) -> dict:
+        a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
+                                          len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
+                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)))
+        out = N.GbResult()
+        self.ctx.call("bo_groupby_topk_presized", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
+                      C.c_void_p(N.ptr(pred_dev)), C.byref(out))
+        return out.as_dict()
+
+    def groupby_presized_device(self, dev: dict, g, pred_dev, out_dev) -> None:
+        a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
+                                          len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
+                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)))
+        self.ctx.call("bo_groupby_topk_presized_device", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
+                      C.c_void_p(N.ptr(pred_dev)), C.c_void_p(N.ptr(out_dev)))
+
+    def groupby_distinct_device(self, dev: dict, g, out_dev) -> None:
+        a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
+                                          len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
+                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)))
+        self.ctx.call("bo_groupby_distinct_device", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
+                      C.c_void_p(N.ptr(out_dev)))
+
+    @staticmethod
+    def groupby_to_device(g) -> dict:
+        import torch
+
+        d = {k: torch.from_numpy(np.ascontiguousarray(getattr(g, k))).cuda()
+             for k in ("a_ids", "b_a", "b_c", "c_cat", "c_year")}
+        d["a_id_max"] = int(g.a_ids.max()) if len(g.a_ids) else 0
+        return d
+
+    # ---------------------------------------------------------- sort -------
+    def radix_sort_pairs_host(self, keys: np.ndarray, vals: np.ndarray, begin_bit: int = 0, end_bit: int = 64):
+        k = np.ascontiguousarray(keys, dtype=np.uint64).copy()
+        v = np.ascontiguousarray(vals, dtype=np.uint32).copy()
+        self.ctx.call("bo_radix_sort_pairs_host", C.c_void_p(k.ctypes.data), C.c_void_p(v.ctypes.data), len(k),
+                      begin_bit, end_bit)
+        return k, v

@@ -125,6 +125,45 @@ class JoinResult(C.Structure):
                     mode=self.mode)
 
 
+GB_MAX_K = 64
+
+
+class GbACols(C.Structure):
+    _fields_ = [("id", C.c_void_p), ("n_rows", C.c_int64)]
+
+
+class GbBCols(C.Structure):
+    _fields_ = [("a_id", C.c_void_p), ("c_id", C.c_void_p), ("n_rows", C.c_int64)]
+
+
+class GbCCols(C.Structure):
+    _fields_ = [("category", C.c_void_p), ("year", C.c_void_p), ("n_rows", C.c_int64)]
+
+
+class GbParams(C.Structure):
+    _fields_ = [("categories", C.c_void_p), ("n_categories", C.c_int32), ("year_lo", C.c_int32),
+                ("year_hi", C.c_int32), ("k", C.c_int32), ("a_id_max", C.c_int32)]
+
+
+class GbRow(C.Structure):
+    _fields_ = [("a_id", C.c_int32), ("min_year", C.c_int32), ("count", C.c_int64)]
+
+
+class GbResult(C.Structure):
+    _fields_ = [("n_groups", C.c_int64), ("joined_rows", C.c_int64), ("c_qualifying", C.c_int64),
+                ("exact_distinct", C.c_int64), ("capacity_log2", C.c_int32), ("overflowed", C.c_int32),
+                ("reruns", C.c_int32), ("mode", C.c_int32), ("n_rows_out", C.c_int32), ("pad", C.c_int32),
+                ("rows", GbRow * GB_MAX_K)]
+
+    def as_dict(self) -> dict:
+        n = self.n_rows_out
+        return dict(n_groups=self.n_groups, joined_rows=self.joined_rows, c_qualifying=self.c_qualifying,
+                    exact_distinct=self.exact_distinct, capacity_log2=self.capacity_log2,
+                    overflowed=self.overflowed, reruns=self.reruns, mode=self.mode,
+                    keys=[self.rows[i].a_id for i in range(n)], counts=[self.rows[i].count for i in range(n)],
+                    min_years=[self.rows[i].min_year for i in range(n)])
+
+
 SKETCH_BINS = 64
 
 
@@ -168,6 +207,16 @@ _SIGNATURES = {
                                           C.POINTER(JoinParams), _P, _P]),
     "bo_join_presized": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
                                    _P, C.POINTER(JoinResult)]),
+    "bo_groupby_topk_plain": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),
+                                         C.POINTER(GbParams), C.POINTER(GbResult)]),
+    "bo_groupby_topk_presized_device": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),
+                                                   C.POINTER(GbParams), _P, _P]),
+    "bo_groupby_topk_presized": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),
+                                            C.POINTER(GbParams), _P, C.POINTER(GbResult)]),
+    "bo_groupby_distinct_device": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),
+                                              C.POINTER(GbParams), _P]),
+    "bo_radix_sort_pairs_device": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, C.c_int32]),
+    "bo_radix_sort_pairs_host": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, C.c_int32]),
     "bo_sketch_i32": (C.c_int, [_P, _P, C.c_int64, C.POINTER(Sketch)]),
     "bo_histogram_small": (C.c_int, [_P, _P, C.c_int32, C.c_int64, C.c_int32, _P]),
     "bo_mlp_create": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(_P)]),

@@ -257,6 +257,85 @@ int bo_join_probe_device(bo_ctx* ctx, const bo_join_probe_cols* probe, bo_join_r
 int bo_join_host(bo_ctx* ctx, const bo_join_build_cols* build_host, const bo_join_probe_cols* probe_host,
                  const bo_join_params* params, int32_t mode, float predicted_rows, bo_join_result* out_host);
 
+/* =============================================================== GROUP-BY ==
+ * Skewed three-way join + high-cardinality group-by + ordered top-k.  Restates
+ * the dense-mask / per-id count pattern of run_q1a
+ * (bespoke_ceb/query_q1a.cpp:503-601), the min aggregate of run_q10a
+ * (bespoke_ceb/query_q10a.cpp:843-856) and the (count desc, id asc) ordering of
+ * radix_sort_groups (bespoke_tpch/query_q10.cpp:318-372):
+ *   C row (c_id = row index) qualifies when category is in the set and
+ *   year_lo <= year <= year_hi; B row (a_id, c_id) joins when 0 <= c_id <
+ *   n_C, C[c_id] qualifies and a_id is an id of A; group by a_id: count,
+ *   min(C.year); order by count desc, a_id asc; first k. */
+#define BO_GB_MAX_K 64
+typedef struct bo_gb_a_cols {
+  const int32_t* id;
+  int64_t n_rows;
+} bo_gb_a_cols;
+typedef struct bo_gb_b_cols {
+  const int32_t* a_id;
+  const int32_t* c_id;
+  int64_t n_rows;
+} bo_gb_b_cols;
+typedef struct bo_gb_c_cols {
+  const uint16_t* category;
+  const int32_t* year;
+  int64_t n_rows;
+} bo_gb_c_cols;
+typedef struct bo_gb_params {
+  const uint16_t* categories;  /* host array, at most 64 values */
+  int32_t n_categories;
+  int32_t year_lo, year_hi;
+  int32_t k;                   /* <= BO_GB_MAX_K */
+  int32_t a_id_max;            /* every id of A lies in [0, a_id_max] (negative ids are skipped) */
+} bo_gb_params;
+typedef struct bo_gb_row {
+  int32_t a_id;
+  int32_t min_year;
+  int64_t count;
+} bo_gb_row;
+typedef struct bo_gb_result {
+  int64_t n_groups;        /* groups (distinct qualifying a_id) */
+  int64_t joined_rows;     /* B rows that joined */
+  int64_t c_qualifying;    /* qualifying C rows */
+  int64_t exact_distinct;  /* plain form: the exact pre-pass count */
+  int32_t capacity_log2;
+  int32_t overflowed;      /* presized table too small (result invalid, rerun) */
+  int32_t reruns;
+  int32_t mode;            /* 0 plain exact-count, 1 presized */
+  int32_t n_rows_out;      /* min(k, n_groups) */
+  int32_t pad;
+  bo_gb_row rows[BO_GB_MAX_K];
+} bo_gb_result;
+
+/* Plain form: exact distinct-group pre-pass (a full scan of B), one host
+ * round trip to size the group table, then the aggregation scan, compaction,
+ * onesweep sort and top-k.  Synchronises. */
+int bo_groupby_topk_plain(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
+                          const bo_gb_params* params, bo_gb_result* out_host);
+/* Presized form, asynchronous: the group table is sized on the device from a
+ * predicted group count (device float, e.g. an MLP output); one scan of B. */
+int bo_groupby_topk_presized_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b,
+                                    const bo_gb_c_cols* c, const bo_gb_params* params,
+                                    const float* predicted_groups_device, bo_gb_result* out_device);
+/* Presized form with the exact fallback (rerun in the plain form on overflow). */
+int bo_groupby_topk_presized(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
+                             const bo_gb_params* params, const float* predicted_groups_device,
+                             bo_gb_result* out_host);
+/* The exact pre-pass alone: out_device[0] = distinct qualifying groups,
+ * out_device[1] = joined rows (device int64[2]); asynchronous. */
+int bo_groupby_distinct_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
+                               const bo_gb_params* params, int64_t* out_device);
+
+/* ================================================================== SORT ==
+ * Stable LSD onesweep radix sort (decoupled look-back) of (uint64 key, uint32
+ * value) pairs ascending by key bits [begin_bit, end_bit).  Replaces the LSD
+ * counting sorts of bespoke_tpch/query_q10.cpp:134-168, 285-316, 318-372. */
+int bo_radix_sort_pairs_device(bo_ctx* ctx, uint64_t* keys, uint32_t* vals, int64_t n, int32_t begin_bit,
+                               int32_t end_bit);
+int bo_radix_sort_pairs_host(bo_ctx* ctx, uint64_t* keys, uint32_t* vals, int64_t n, int32_t begin_bit,
+                             int32_t end_bit);
+
 /* ================================================================ SKETCH ==
  * Per-column sketches for the learned sizing features, computed on the device
  * once per table.  No reference counterpart. */
