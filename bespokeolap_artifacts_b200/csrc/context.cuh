@@ -70,6 +70,15 @@ int occupancy_blocks(const void* kernel, int block, size_t smem);
 int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsigned long long* tmp_keys,
                      uint32_t* tmp_vals, int64_t n, int begin_bit, int end_bit, const unsigned long long* n_dev);
 
+// The k smallest keys (ascending) of (keys, vals) into the front of
+// (cand_keys, cand_vals): radix select + small sort (csrc/radix_sort.cu).
+// lo_bits / hi_max_dev (optional): keys are (hi << lo_bits) | lo with all hi
+// equal above the highest bit of *hi_max_dev; the select digit sits there.
+int radix_topk_pairs(bo_ctx* ctx, const unsigned long long* keys, const uint32_t* vals, int64_t n_max,
+                     const unsigned long long* n_dev, int key_bits, int k, unsigned long long* cand_keys,
+                     uint32_t* cand_vals, unsigned long long* tmp_keys, uint32_t* tmp_vals, int lo_bits,
+                     const unsigned long long* hi_max_dev);
+
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 // Column pointers must be 32-byte aligned: the scans use 256-bit vector loads.
 inline bool aligned32(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 31u) == 0; }

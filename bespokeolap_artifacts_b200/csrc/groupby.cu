@@ -42,12 +42,18 @@ constexpr unsigned long long kGbEmpty = ~0ull;
 constexpr int kGbBloomLog2Words = 14;
 constexpr uint32_t kGbBloomWords = 1u << kGbBloomLog2Words;
 constexpr uint32_t kGbBloomBytes = kGbBloomWords * 4u;
-constexpr int kGbBlock = 512;
+constexpr int kGbBlock = 256;
 constexpr int kGbWarps = kGbBlock / 32;
 constexpr int kGbRowsPerLane = 16;
 constexpr int kGbRowsPerWarpStep = 32 * kGbRowsPerLane;
-constexpr int kGbQueue = 32 * 8;
-constexpr int kGbLocalSlots = 1024;  // per-block pre-aggregation table
+constexpr int kGbQueue = 384;        // per-warp candidate queue (entries)
+constexpr int kGbFlushAt = 128;      // resolve once this many candidates are queued
+constexpr int kGbResolveR = 4;       // independent candidates per lane per resolve round
+// Per-block pre-aggregation table for Zipf heavy hitters: small (tail keys go
+// straight to the global table, where they do not contend) and probed at most
+// kGbLocalProbes times, so a full table costs a tail key two shared CAS.
+constexpr int kGbLocalSlots = 256;
+constexpr int kGbLocalProbes = 2;
 constexpr int kGbMinCapLog2 = 10;
 constexpr float kGbPresizeFactor = 2.5f;
 constexpr int kMaxCats = 64;
@@ -62,6 +68,7 @@ struct GbMeta {
   unsigned long long n_out;           // compacted groups (sort key count)
   unsigned long long c_pass;          // qualifying C rows
   unsigned long long exact_distinct;  // plain pre-pass result
+  unsigned long long inv_max;         // largest packed (cmax - count): the smallest count's
 };
 
 struct CatSet {
@@ -69,11 +76,13 @@ struct CatSet {
   int32_t n;
 };
 
+// Multiplicative (Fibonacci) hashing: one multiply gives the word from the
+// high bits and two bit positions from the low bits -- cheap enough to run on
+// every B row.
 __device__ __forceinline__ void gb_bloom_pos(uint32_t c, uint32_t& word, uint32_t& bits) {
-  const uint32_t h2 = (c * 0x9E3779B1u) ^ ((c >> 15) * 0x85EBCA6Bu);
-  const uint32_t h3 = h2 * 0xC2B2AE35u + 0x27D4EB2Fu;
-  word = h3 >> (32 - kGbBloomLog2Words);
-  bits = (1u << (h3 & 31u)) | (1u << ((h3 >> 5) & 31u));
+  const uint32_t h = c * 0x9E3779B1u;
+  word = h >> (32 - kGbBloomLog2Words);
+  bits = (1u << (h & 31u)) | (1u << ((h >> 5) & 31u));
 }
 
 __device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t& total) {
@@ -126,6 +135,7 @@ __global__ void gb_init_kernel(unsigned long long* slots, int32_t* mins, uint32_
     meta->joined = 0;
     meta->distinct = 0;
     meta->n_out = 0;
+    meta->inv_max = 0;
     if (clear_filters) {
       meta->c_pass = 0;
       meta->exact_distinct = 0;
@@ -215,17 +225,16 @@ __global__ void gb_amask_kernel(bo_gb_a_cols a, int32_t a_id_max, uint32_t* __re
 
 // ------------------------------------------------------------------ scan --
 __device__ __forceinline__ bool gb_global_insert(unsigned long long* slots, int32_t* mins, uint64_t mask, uint32_t key,
-                                                 uint32_t cnt, int32_t mn, uint32_t& newkeys) {
-  uint64_t idx = hash32(key) & mask;
+                                                 uint32_t cnt, int32_t mn, uint32_t& newkeys,
+                                                 uint64_t start = ~0ull) {
+  uint64_t idx = start == ~0ull ? (hash32(key) & mask) : start;
   const unsigned long long claim = (unsigned long long)key << 32;
   for (uint64_t step = 0; step <= mask; ++step) {
-    unsigned long long v = slots[idx];
+    // CAS first: one round trip claims an empty slot or returns its owner.
+    unsigned long long v = atomicCAS(slots + idx, kGbEmpty, claim);
     if (v == kGbEmpty) {
-      v = atomicCAS(slots + idx, kGbEmpty, claim);
-      if (v == kGbEmpty) {
-        ++newkeys;
-        v = claim;
-      }
+      ++newkeys;
+      v = claim;
     }
     if ((uint32_t)(v >> 32) == key) {
       atomicAdd(slots + idx, (unsigned long long)cnt);
@@ -249,7 +258,7 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
   extern __shared__ __align__(128) uint32_t bloom_s[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int32_t q_c[kGbWarps][kGbQueue];
-  __shared__ uint16_t q_off[kGbWarps][kGbQueue];
+  __shared__ uint32_t q_row[kGbWarps][kGbQueue];
   __shared__ uint32_t l_key[kGbLocalSlots];
   __shared__ uint32_t l_cnt[kGbLocalSlots];
   __shared__ int32_t l_min[kGbLocalSlots];
@@ -269,49 +278,143 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
   // check below still decides, so the answer is unchanged.
   const bool use_bloom = mbar_wait_bounded(&bar, 0, kWaitLimitNs);
   uint32_t bad = use_bloom ? 0u : kErrSpinTimeout;
+  __shared__ uint32_t all_ones;
+  if (threadIdx.x == 0) all_ones = 0xffffffffu;
+  __syncthreads();
+  const uint32_t* bl = use_bloom ? bloom_s : &all_ones;
+  const uint32_t wmask = use_bloom ? (kGbBloomWords - 1u) : 0u;
   const int32_t cl = kMode ? __ldg(&meta->cap_log2) : 0;
   const uint64_t mask = (1ull << cl) - 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int32_t* qc = q_c[warp];
-  uint16_t* qo = q_off[warp];
+  uint32_t* qr = q_row[warp];
+  uint32_t qn = 0;  // queued candidates (warp-uniform)
   uint32_t joined = 0, newkeys = 0, full = 0;
   const int64_t n = b.n_rows;
   const int64_t steps = (n + kGbRowsPerWarpStep - 1) / kGbRowsPerWarpStep;
   const int64_t nwarps = (int64_t)gridDim.x * kGbWarps;
-  for (int64_t st = (int64_t)blockIdx.x * kGbWarps + warp; st < steps; st += nwarps) {
-    const int64_t base = st * kGbRowsPerWarpStep;
-    const int64_t r0 = base + lane * kGbRowsPerLane;
-    int32_t cid[kGbRowsPerLane];
-    uint32_t valid = 0xffffu;
+  // One step of software prefetch: the next step's c_ids are in flight while
+  // the current step is tested and resolved.
+  auto load_step = [&](int64_t st, int32_t (&out)[kGbRowsPerLane], uint32_t& vmask) {
+    const int64_t r0 = st * kGbRowsPerWarpStep + lane * kGbRowsPerLane;
+    vmask = 0;
+    if (st >= steps) return;
     if (r0 + kGbRowsPerLane <= n) {
       const int8v c0 = ld_stream_v8(b.c_id + r0), c1 = ld_stream_v8(b.c_id + r0 + 8);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        cid[k] = c0.v[k];
-        cid[8 + k] = c1.v[k];
+        out[k] = c0.v[k];
+        out[8 + k] = c1.v[k];
       }
+      vmask = 0xffffu;
     } else {
-      valid = 0;
 #pragma unroll
       for (int k = 0; k < kGbRowsPerLane; ++k) {
-        cid[k] = -1;
+        out[k] = -1;
         if (r0 + k < n) {
-          cid[k] = b.c_id[r0 + k];
-          valid |= 1u << k;
+          out[k] = b.c_id[r0 + k];
+          vmask |= 1u << k;
         }
       }
     }
+  };
+  // Resolves the warp's queued candidates: lanes take up to kGbResolveR
+  // entries each and every round issues its loads for all of them at once
+  // (exact C bitmap; then a_id and the C year of the passing ones; then the A
+  // mask), so a warp has many independent memory chains in flight.
+  auto resolve = [&](uint32_t cnt) {
+    __syncwarp();
+    for (uint32_t i0 = 0; i0 < cnt; i0 += 32 * kGbResolveR) {
+      int32_t c[kGbResolveR];
+      uint32_t row[kGbResolveR], w[kGbResolveR];
+      int32_t a[kGbResolveR], y[kGbResolveR];
+#pragma unroll
+      for (int r = 0; r < kGbResolveR; ++r) {
+        const uint32_t i = i0 + r * 32 + lane;
+        c[r] = i < cnt ? qc[i] : -1;
+        row[r] = i < cnt ? qr[i] : 0u;
+        const bool in = (uint32_t)c[r] < (uint32_t)n_c;  // negative or past C: no partner
+        w[r] = in ? __ldg(cbits + (c[r] >> 5)) : 0u;
+      }
+#pragma unroll
+      for (int r = 0; r < kGbResolveR; ++r) {
+        const bool pass = (w[r] >> (c[r] & 31)) & 1u;
+        a[r] = pass ? __ldg(b.a_id + row[r]) : -1;
+        y[r] = (pass && kMode == 1) ? __ldg(c_year + c[r]) : 0;
+      }
+      // Survivors: A-mask test, then the heavy-hitter table in shared memory;
+      // the rest try their first global slot with one CAS each, all issued
+      // before any result is used (collisions continue out of line).
+      bool pend[kGbResolveR];
+#pragma unroll
+      for (int r = 0; r < kGbResolveR; ++r) {
+        const bool in_a = a[r] >= 0 && a[r] <= a_id_max;
+        const uint32_t m = in_a ? __ldg(amask + (a[r] >> 5)) : 0u;
+        pend[r] = false;
+        if (!in_a || !((m >> (a[r] & 31)) & 1u)) continue;
+        ++joined;
+        if (kMode == 0) {
+          atomicOr(dbits + (a[r] >> 5), 1u << (a[r] & 31));
+          continue;
+        }
+        const uint32_t h = hash32((uint32_t)a[r]);
+        bool done = false;
+#pragma unroll 1
+        for (int p = 0; p < kGbLocalProbes && !done; ++p) {
+          const int sl = (int)((h + p) & (kGbLocalSlots - 1));
+          const uint32_t old = atomicCAS(&l_key[sl], 0xffffffffu, (uint32_t)a[r]);
+          if (old == 0xffffffffu || old == (uint32_t)a[r]) {
+            atomicAdd(&l_cnt[sl], 1u);
+            atomicMin(&l_min[sl], y[r]);
+            done = true;
+          }
+        }
+        pend[r] = !done;
+      }
+      if (kMode == 1) {
+        unsigned long long got[kGbResolveR];
+        uint64_t first[kGbResolveR];
+#pragma unroll
+        for (int r = 0; r < kGbResolveR; ++r) {
+          first[r] = pend[r] ? (hash32((uint32_t)a[r]) & mask) : 0;
+          got[r] = pend[r] ? atomicCAS(slots + first[r], kGbEmpty, (unsigned long long)(uint32_t)a[r] << 32)
+                           : 0ull;
+        }
+#pragma unroll
+        for (int r = 0; r < kGbResolveR; ++r) {
+          if (!pend[r]) continue;
+          if (got[r] == kGbEmpty) ++newkeys;
+          if (got[r] == kGbEmpty || (uint32_t)(got[r] >> 32) == (uint32_t)a[r]) {
+            atomicAdd(slots + first[r], 1ull);
+            atomicMin(mins + first[r], y[r]);
+          } else if (!gb_global_insert(slots, mins, mask, (uint32_t)a[r], 1u, y[r], newkeys, (first[r] + 1) & mask)) {
+            full = 1;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  };
+  int32_t nxt[kGbRowsPerLane];
+  uint32_t nxt_valid;
+  int64_t st = (int64_t)blockIdx.x * kGbWarps + warp;
+  load_step(st, nxt, nxt_valid);
+  for (; st < steps; st += nwarps) {
+    const int64_t base = st * kGbRowsPerWarpStep;
+    int32_t cid[kGbRowsPerLane];
+#pragma unroll
+    for (int k = 0; k < kGbRowsPerLane; ++k) cid[k] = nxt[k];
+    const uint32_t valid = nxt_valid;
+    load_step(st + nwarps, nxt, nxt_valid);
+    // Branch-free Bloom test of all 16 rows (every lookup is issued; without
+    // the filter every word reads as all ones).
+    // (The c_id range check happens in the rare resolve path below.)
     uint32_t hit = 0;
 #pragma unroll
-    for (int k = 0; k < kGbRowsPerLane; ++k) {
-      const uint32_t cv = (uint32_t)cid[k];
-      bool cand = cid[k] >= 0 && (int64_t)cid[k] < n_c;
-      if (use_bloom) {
-        uint32_t w, bits;
-        gb_bloom_pos(cv, w, bits);
-        cand = cand && (bloom_s[w] & bits) == bits;
-      }
-      hit |= (uint32_t)cand << k;
+    for (int k = kGbRowsPerLane - 1; k >= 0; --k) {
+      const uint32_t h = (uint32_t)cid[k] * 0x9E3779B1u;
+      const uint32_t x = bl[(h >> (32 - kGbBloomLog2Words)) & wmask];
+      hit = (hit << 1) | (__funnelshift_r(x, x, h) & __funnelshift_r(x, x, h >> 5) & 1u);
     }
     hit &= valid;
 #pragma unroll
@@ -320,44 +423,28 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
       uint32_t total;
       uint32_t pos = warp_excl_scan(__popc(hm), total);
       if (total == 0) continue;  // warp-uniform
+      if (qn + total > kGbQueue) {  // keep room: resolve what is queued first
+        resolve(qn);
+        qn = 0;
+      }
+      pos += qn;
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         if ((hm >> k) & 1u) {
           qc[pos] = cid[8 * half + k];
-          qo[pos] = (uint16_t)(lane * kGbRowsPerLane + 8 * half + k);
+          qr[pos] = (uint32_t)(base + lane * kGbRowsPerLane + 8 * half + k);
           ++pos;
         }
       }
+      qn += total;
       __syncwarp();
-      for (uint32_t i = lane; i < total; i += 32) {
-        const int32_t c = qc[i];
-        if (!((__ldg(cbits + (c >> 5)) >> (c & 31)) & 1u)) continue;
-        const int64_t row = base + qo[i];
-        const int32_t a = __ldg(b.a_id + row);
-        if (a < 0 || a > a_id_max || !((__ldg(amask + (a >> 5)) >> (a & 31)) & 1u)) continue;
-        ++joined;
-        if (kMode == 0) {
-          atomicOr(dbits + (a >> 5), 1u << (a & 31));
-        } else {
-          const int32_t y = __ldg(c_year + c);
-          const uint32_t h = hash32((uint32_t)a);
-          bool done = false;
-#pragma unroll 1
-          for (int p = 0; p < 8 && !done; ++p) {
-            const int s = (int)((h + p) & (kGbLocalSlots - 1));
-            const uint32_t old = atomicCAS(&l_key[s], 0xffffffffu, (uint32_t)a);
-            if (old == 0xffffffffu || old == (uint32_t)a) {
-              atomicAdd(&l_cnt[s], 1u);
-              atomicMin(&l_min[s], y);
-              done = true;
-            }
-          }
-          if (!done && !gb_global_insert(slots, mins, mask, (uint32_t)a, 1u, y, newkeys)) full = 1;
-        }
+      if (qn >= kGbFlushAt) {
+        resolve(qn);
+        qn = 0;
       }
-      __syncwarp();
     }
   }
+  if (qn) resolve(qn);
   __syncthreads();
   if (kMode == 1) {
     // Flush the block's pre-aggregated groups into the global table.
@@ -401,30 +488,67 @@ __global__ void gb_popcount_kernel(const uint32_t* __restrict__ dbits, int64_t w
 }
 
 // --------------------------------------------------------------- compact --
-__global__ void gb_compact_kernel(const unsigned long long* __restrict__ slots, const int32_t* __restrict__ mins,
-                                  GbMeta* meta, int wa, unsigned long long cmax, unsigned long long* __restrict__ keys,
-                                  uint32_t* __restrict__ vals) {
+// Each block compacts a contiguous range of slots: warps count their occupied
+// slots, one atomic per block reserves the block's output range (per-warp
+// atomics on the single counter would serialise in L2).
+constexpr int kCompactBlock = 256;
+constexpr int kCompactPerThread = 8;
+
+__global__ void __launch_bounds__(kCompactBlock) gb_compact_kernel(const unsigned long long* __restrict__ slots,
+                                                                   const int32_t* __restrict__ mins, GbMeta* meta,
+                                                                   int wa, unsigned long long cmax,
+                                                                   unsigned long long* __restrict__ keys,
+                                                                   uint32_t* __restrict__ vals) {
+  __shared__ uint32_t warp_off[kCompactBlock / 32 + 1];
+  __shared__ unsigned long long block_base;
   const int32_t cl = __ldg(&meta->cap_log2);
   const uint64_t cap = 1ull << cl;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const int lane = threadIdx.x & 31;
-  // Uniform trip count per warp so the warp-aggregated slot reservation stays converged.
-  const uint64_t cap_w = (cap + 31) & ~31ull;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap_w; i += stride) {
-    const unsigned long long v = i < cap ? slots[i] : kGbEmpty;
-    const bool occ = v != kGbEmpty;
-    const uint32_t ballot = __ballot_sync(0xffffffffu, occ);
-    if (!ballot) continue;
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(&meta->n_out, (unsigned long long)__popc(ballot));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (occ) {
-      const unsigned long long pos = base + __popc(ballot & ((1u << lane) - 1u));
-      const unsigned long long cnt = v & 0xffffffffull;
-      const unsigned long long key = v >> 32;
-      keys[pos] = ((cmax - cnt) << wa) | key;
-      vals[pos] = (uint32_t)mins[i];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t span = (uint64_t)kCompactBlock * kCompactPerThread;
+  for (uint64_t b0 = (uint64_t)blockIdx.x * span; b0 < cap; b0 += (uint64_t)gridDim.x * span) {
+    uint32_t occ = 0;
+    unsigned long long v[kCompactPerThread];
+#pragma unroll
+    for (int j = 0; j < kCompactPerThread; ++j) {
+      const uint64_t i = b0 + (uint64_t)j * kCompactBlock + threadIdx.x;
+      v[j] = i < cap ? slots[i] : kGbEmpty;
+      occ += v[j] != kGbEmpty;
     }
+    uint32_t wtot;
+    const uint32_t mine = warp_excl_scan(occ, wtot);
+    if (lane == 0) warp_off[warp] = wtot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < kCompactBlock / 32; ++w) {
+        const uint32_t c = warp_off[w];
+        warp_off[w] = t;
+        t += c;
+      }
+      block_base = t ? atomicAdd(&meta->n_out, (unsigned long long)t) : 0ull;
+    }
+    __syncthreads();
+    unsigned long long pos = block_base + warp_off[warp] + mine;
+    unsigned long long cmaxc = 0;  // largest count seen by this thread
+#pragma unroll
+    for (int j = 0; j < kCompactPerThread; ++j) {
+      if (v[j] != kGbEmpty) {
+        const uint64_t i = b0 + (uint64_t)j * kCompactBlock + threadIdx.x;
+        const unsigned long long cnt = v[j] & 0xffffffffull;
+        cmaxc = cnt > cmaxc ? cnt : cmaxc;
+        keys[pos] = ((cmax - cnt) << wa) | (v[j] >> 32);
+        vals[pos] = (uint32_t)mins[i];
+        ++pos;
+      }
+    }
+    // The select digit of the top-k must sit below the highest bit that
+    // differs among the packed counts: track the largest count.
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long other = __shfl_xor_sync(0xffffffffu, cmaxc, o);
+      cmaxc = other > cmaxc ? other : cmaxc;
+    }
+    if (lane == 0 && cmaxc) atomicMax(&meta->inv_max, cmaxc);
+    __syncthreads();
   }
 }
 
@@ -576,7 +700,7 @@ int gb_prepare(bo_ctx* ctx, const bo_gb_a_cols& a, const bo_gb_c_cols& c, const 
     gb_cfilter_kernel<<<gc, 256, 0, ctx->stream>>>(c, cs, prm.year_lo, prm.year_hi, ws.cbits, ws.bloom, ws.meta);
     if ((rc = after_launch(ctx, "gb_cfilter_kernel"))) return rc;
   }
-  if (a.n_rows > 0) {
+  if (a.n_rows > 0 && !prm.a_mask) {
     const void* ka = reinterpret_cast<const void*>(&gb_amask_kernel);
     const int ga = grid_res(ctx, ka, 256, 0, a.n_rows);
     gb_amask_kernel<<<ga, 256, 0, ctx->stream>>>(a, prm.a_id_max, ws.amask, ctx->d_err);
@@ -595,9 +719,9 @@ int gb_launch_scan(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, co
     ready = true;
   }
   const int grid = grid_res(ctx, k, kGbBlock, kGbBloomBytes, (b.n_rows + kGbRowsPerLane - 1) / kGbRowsPerLane);
-  gb_scan_kernel<kMode><<<grid, kGbBlock, kGbBloomBytes, ctx->stream>>>(b, c.n_rows, prm.a_id_max, ws.bloom, ws.cbits,
-                                                                        c.year, ws.amask, ws.slots, ws.mins, ws.dbits,
-                                                                        ws.meta, ctx->d_err);
+  gb_scan_kernel<kMode><<<grid, kGbBlock, kGbBloomBytes, ctx->stream>>>(
+      b, c.n_rows, prm.a_id_max, ws.bloom, ws.cbits, c.year, prm.a_mask ? prm.a_mask : ws.amask, ws.slots, ws.mins,
+      ws.dbits, ws.meta, ctx->d_err);
   return after_launch(ctx, "gb_scan_kernel");
 }
 
@@ -611,12 +735,20 @@ int gb_aggregate_order(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c
   const unsigned long long cmax = (wc >= 64) ? ~0ull : ((1ull << wc) - 1ull);
   const uint64_t cap_max = 1ull << ws.max_log2;
   const void* kc = reinterpret_cast<const void*>(&gb_compact_kernel);
-  const int gc = grid_res(ctx, kc, 256, 0, (int64_t)cap_max);
-  gb_compact_kernel<<<gc, 256, 0, ctx->stream>>>(ws.slots, ws.mins, ws.meta, wa, cmax, ws.keys, ws.vals);
+  const int gc = grid_res(ctx, kc, kCompactBlock, 0, (int64_t)cap_max / kCompactPerThread);
+  gb_compact_kernel<<<gc, kCompactBlock, 0, ctx->stream>>>(ws.slots, ws.mins, ws.meta, wa, cmax, ws.keys, ws.vals);
   if ((rc = after_launch(ctx, "gb_compact_kernel"))) return rc;
-  if ((rc = radix_sort_pairs(ctx, ws.keys, ws.vals, ws.tkeys, ws.tvals, (int64_t)cap_max, 0, wa + wc, &ws.meta->n_out)))
+  // ORDER BY count desc, a_id asc LIMIT k: radix select of the k smallest
+  // packed keys, then the onesweep / in-CTA LSD sort of the candidates.
+  // The candidates go to the temporary buffers; the sort uses the key
+  // buffers (no longer needed) as its scratch.
+  // (cmax - count) for counts in [1, max_count] shares every bit above the
+  // highest bit of max_count with cmax: the select digit goes just below it
+  // (inv_max holds the largest count; topk_shift takes its bit length).
+  if ((rc = radix_topk_pairs(ctx, ws.keys, ws.vals, (int64_t)cap_max, &ws.meta->n_out, wa + wc, prm.k, ws.tkeys,
+                             ws.tvals, ws.keys, ws.vals, wa, &ws.meta->inv_max)))
     return rc;
-  gb_topk_kernel<<<1, BO_GB_MAX_K, 0, ctx->stream>>>(ws.keys, ws.vals, ws.meta, prm.k, wa, cmax, mode, out);
+  gb_topk_kernel<<<1, BO_GB_MAX_K, 0, ctx->stream>>>(ws.tkeys, ws.tvals, ws.meta, prm.k, wa, cmax, mode, out);
   return after_launch(ctx, "gb_topk_kernel");
 }
 
@@ -706,6 +838,19 @@ int bo_groupby_topk_presized(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_c
     out_host->mode = 1;
   }
   return BO_OK;
+}
+
+int bo_groupby_a_mask_device(bo_ctx* ctx, const bo_gb_a_cols* a, int32_t a_id_max, uint32_t* mask_device) {
+  BO_CHECK_CTX(ctx);
+  if (!a || !mask_device || a_id_max < 0 || a->n_rows < 0 || (a->n_rows > 0 && !a->id))
+    return set_error(ctx, BO_ERR_INVALID, "groupby_a_mask: bad argument");
+  const int64_t words = ((int64_t)a_id_max + 1 + 31) / 32;
+  BO_CUDA(ctx, cudaMemsetAsync(mask_device, 0, sizeof(uint32_t) * (size_t)words, ctx->stream));
+  if (a->n_rows == 0) return BO_OK;
+  const void* ka = reinterpret_cast<const void*>(&gb_amask_kernel);
+  gb_amask_kernel<<<grid_res(ctx, ka, 256, 0, a->n_rows), 256, 0, ctx->stream>>>(*a, a_id_max, mask_device,
+                                                                                   ctx->d_err);
+  return after_launch(ctx, "gb_amask_kernel");
 }
 
 int bo_groupby_distinct_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,

@@ -49,10 +49,23 @@ struct JoinMeta {
   unsigned long long count;    // K7 output
 };
 
-__device__ __forceinline__ void bloom_pos(uint32_t h, uint32_t& word, uint32_t& bits) {
-  const uint32_t h2 = h * 0x9E3779B1u + 0x7F4A7C15u;
+// Bloom positions from the key with one multiply (Fibonacci hashing): the word
+// from the high bits, two bit positions from the low bits.  Cheap enough for
+// every probe row; the table uses the stronger hash32 only for the ~9% that
+// pass.
+__device__ __forceinline__ void bloom_pos(uint32_t key, uint32_t& word, uint32_t& bits) {
+  const uint32_t h2 = key * 0x9E3779B1u;
   word = h2 >> (32 - kBloomLog2Words);
   bits = (1u << (h2 & 31u)) | (1u << ((h2 >> 5) & 31u));
+}
+
+// The same test as (word & bits) == bits with two funnel-shift rotates (the
+// rotate amount uses the low 5 bits, so no masking): 1 if the key may be in
+// the filter.
+__device__ __forceinline__ uint32_t bloom_test(const uint32_t* bl, uint32_t wmask, uint32_t key) {
+  const uint32_t h2 = key * 0x9E3779B1u;
+  const uint32_t x = bl[(h2 >> (32 - kBloomLog2Words)) & wmask];
+  return __funnelshift_r(x, x, h2) & __funnelshift_r(x, x, h2 >> 5) & 1u;
 }
 
 // Row qualifies on the build side (date < date_lt and segment == seg).
@@ -134,7 +147,7 @@ __device__ __forceinline__ void join_insert(unsigned long long* slots, uint32_t*
     if (old == kEmptySlot) {
       ++newkeys;
       uint32_t w, bits;
-      bloom_pos(h, w, bits);
+      bloom_pos((uint32_t)key, w, bits);
       atomicOr(bloom + w, bits);
       return;
     }
@@ -289,7 +302,7 @@ __device__ __forceinline__ void probe_one(int32_t fk, int64_t row, const uint32_
   const uint32_t h = hash32((uint32_t)fk);
   if (use_bloom) {
     uint32_t w, bits;
-    bloom_pos(h, w, bits);
+    bloom_pos((uint32_t)fk, w, bits);
     if ((bloom_s[w] & bits) != bits) return;
   }
   const unsigned long long v = __ldg(slots + (h & mask));
@@ -335,6 +348,11 @@ __global__ void __launch_bounds__(kJoinBlock) join_probe_kernel(bo_join_probe_co
   const bool use_bloom = mbar_wait_bounded(&bar, 0, kWaitLimitNs);
   ProbeAcc acc;
   if (!use_bloom) acc.bad |= kErrSpinTimeout;
+  __shared__ uint32_t all_ones;
+  if (threadIdx.x == 0) all_ones = 0xffffffffu;
+  __syncthreads();
+  const uint32_t* bl = use_bloom ? bloom_s : &all_ones;
+  const uint32_t wmask = use_bloom ? (kBloomWords - 1u) : 0u;
 
   const int32_t cl = __ldg(&meta->cap_log2);
   const uint64_t mask = (1ull << cl) - 1;
@@ -367,14 +385,10 @@ __global__ void __launch_bounds__(kJoinBlock) join_probe_kernel(bo_join_probe_co
         }
       }
     }
+    // Branch-free Bloom test (without the filter every word reads as all ones).
     uint32_t hit = 0;
 #pragma unroll
-    for (int k = 0; k < kRowsPerLane; ++k) {
-      uint32_t w, bits;
-      bloom_pos(hash32((uint32_t)fk[k]), w, bits);
-      const bool cand = !use_bloom || (bloom_s[w] & bits) == bits;
-      hit |= (uint32_t)cand << k;
-    }
+    for (int k = kRowsPerLane - 1; k >= 0; --k) hit = (hit << 1) | bloom_test(bl, wmask, (uint32_t)fk[k]);
     hit &= valid;
 #pragma unroll
     for (int half = 0; half < 2; ++half) {

@@ -34,6 +34,7 @@ struct bo_mlp {
   int partial_blocks = 0;
   float* loss = nullptr;     // device scalar
   int64_t step = 0;
+  mutable bool predict_ready = false;
 };
 
 namespace bo {
@@ -226,31 +227,61 @@ struct FeatureVec {
 };
 
 // One feature vector passed by value (no host-to-device copy): predicted
-// counts = max(expm1(y), 0), written to counts[0..O).
-__global__ void __launch_bounds__(kH) mlp_predict_counts(const float* __restrict__ params, FeatureVec xv, int F,
-                                                         int O, float* __restrict__ counts, float* __restrict__ y_log) {
+// counts = max(expm1(y), 0), written to counts[0..O).  256 threads: the
+// parameters are staged into shared memory with coalesced loads, each of the
+// 64 units of a layer is computed by 4 threads over a quarter of its inputs
+// and combined with two shuffles.
+constexpr int kPredThreads = 256;
+
+__global__ void __launch_bounds__(kPredThreads) mlp_predict_counts(const float* __restrict__ params, FeatureVec xv,
+                                                                   int F, int O, float* __restrict__ counts,
+                                                                   float* __restrict__ y_log) {
+  extern __shared__ float W[];
   __shared__ float a[2][kH];
   const MlpLayout L = mlp_layout(F, O);
-  const int j = threadIdx.x;
-  float z = params[L.b1 + j];
-  for (int i = 0; i < F; ++i) z = fmaf(xv.f[i], params[L.w1 + i * kH + j], z);
-  a[0][j] = z > 0.0f ? z : 0.0f;
+  for (int i = threadIdx.x; i < L.P; i += kPredThreads) W[i] = params[i];
+  if (threadIdx.x < kMaxF) a[1][threadIdx.x] = threadIdx.x < F ? xv.f[threadIdx.x] : 0.0f;
   __syncthreads();
-  z = params[L.b2 + j];
-  for (int i = 0; i < kH; ++i) z = fmaf(a[0][i], params[L.w2 + i * kH + j], z);
-  a[1][j] = z > 0.0f ? z : 0.0f;
-  __syncthreads();
-  z = params[L.b3 + j];
-  for (int i = 0; i < kH; ++i) z = fmaf(a[1][i], params[L.w3 + i * kH + j], z);
-  __syncthreads();
-  a[0][j] = z > 0.0f ? z : 0.0f;
-  __syncthreads();
-  if (j < O) {
-    float y = params[L.b4 + j];
-    for (int i = 0; i < kH; ++i) y = fmaf(a[0][i], params[L.w4 + i * O + j], y);
-    if (y_log) y_log[j] = y;
-    const float c = expm1f(y);
-    counts[j] = c > 0.0f ? c : 0.0f;
+  const int j = threadIdx.x >> 2, part = threadIdx.x & 3;
+  // layer 1: inputs a[1][0..F)
+  {
+    float z = 0.0f;
+    for (int i = part; i < F; i += 4) z = fmaf(a[1][i], W[L.w1 + i * kH + j], z);
+    z += __shfl_xor_sync(0xffffffffu, z, 1);
+    z += __shfl_xor_sync(0xffffffffu, z, 2);
+    z += W[L.b1 + j];
+    __syncthreads();
+    if (part == 0) a[0][j] = z > 0.0f ? z : 0.0f;
+    __syncthreads();
+  }
+  const int wofs[2] = {L.w2, L.w3}, bofs[2] = {L.b2, L.b3};
+#pragma unroll
+  for (int l = 0; l < 2; ++l) {
+    const float* in = a[l & 1 ? 1 : 0];
+    float z = 0.0f;
+#pragma unroll 4
+    for (int i = part; i < kH; i += 4) z = fmaf(in[i], W[wofs[l] + i * kH + j], z);
+    z += __shfl_xor_sync(0xffffffffu, z, 1);
+    z += __shfl_xor_sync(0xffffffffu, z, 2);
+    z += W[bofs[l] + j];
+    __syncthreads();
+    if (part == 0) a[l & 1 ? 0 : 1][j] = z > 0.0f ? z : 0.0f;
+    __syncthreads();
+  }
+  // after two hidden layers the third activation is in a[0]
+  if (threadIdx.x < 32) {
+    for (int o = 0; o < O; ++o) {
+      float y = fmaf(a[0][threadIdx.x], W[L.w4 + threadIdx.x * O + o], 0.0f);
+      y = fmaf(a[0][threadIdx.x + 32], W[L.w4 + (threadIdx.x + 32) * O + o], y);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) y += __shfl_xor_sync(0xffffffffu, y, off);
+      if (threadIdx.x == 0) {
+        y += W[L.b4 + o];
+        if (y_log) y_log[o] = y;
+        const float c = expm1f(y);
+        counts[o] = c > 0.0f ? c : 0.0f;
+      }
+    }
   }
 }
 
@@ -445,7 +476,13 @@ int bo_mlp_predict_counts(bo_ctx* ctx, const bo_mlp* m, const float* features_ho
   if (!features_host || !counts_device) return set_error(ctx, BO_ERR_INVALID, "mlp_predict: bad argument");
   FeatureVec fv;
   for (int i = 0; i < kMaxF; ++i) fv.f[i] = i < m->F ? features_host[i] : 0.0f;
-  mlp_predict_counts<<<1, kH, 0, ctx->stream>>>(m->params, fv, m->F, m->O, counts_device, log_device);
+  const size_t smem = sizeof(float) * (size_t)m->P;
+  if (!m->predict_ready) {
+    BO_CUDA(ctx, cudaFuncSetAttribute(reinterpret_cast<const void*>(&mlp_predict_counts),
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    m->predict_ready = true;
+  }
+  mlp_predict_counts<<<1, kPredThreads, smem, ctx->stream>>>(m->params, fv, m->F, m->O, counts_device, log_device);
   return after_launch(ctx, "mlp_predict_counts");
 }
 

@@ -10,14 +10,15 @@
 // Design (8-bit digits, only the passes covering [begin_bit, end_bit)):
 //  * radix_hist_kernel -- one read of the keys builds every pass's 256-bin
 //    histogram (shared-memory counters, one global atomic per bin per block);
-//    radix_scan_kernel turns them into exclusive digit bases;
-//  * radix_pass_kernel -- tiles of 4096 keys, tile ids taken from an atomic
-//    counter so every predecessor tile has started.  A warp ranks its 512 keys
+//    its last block turns them into exclusive digit bases;
+//  * radix_pass_kernel -- persistent blocks (at most the resident grid) take
+//    tiles of 4096 keys in order from an atomic counter, so every predecessor
+//    tile belongs to a running block.  A warp ranks its 512 keys
 //    stably in 16 rounds of 32 (match_any on the digit, per-warp digit counters
 //    in shared memory), the block sums its warps into tile counts, publishes
 //    them, and each of the 256 threads does the decoupled look-back for one
 //    digit over predecessor tiles' 64-bit status words
-//    (flag:2 | epoch:30 | count:32).  The epoch (unique per pass launch) makes
+//    (flag:2 | epoch:30 | count:32), 16 predecessors per round trip.  The epoch (unique per pass launch) makes
 //    stale words from earlier passes read as "not ready", so status arrays are
 //    never cleared.  Every spin is bounded by the global timer; a timeout sets
 //    an error bit instead of hanging.
@@ -44,11 +45,15 @@ __device__ __forceinline__ int64_t sort_n(int64_t n, const unsigned long long* n
   return v < (unsigned long long)n ? (int64_t)v : n;
 }
 
+// Histograms of every pass; the last block to finish turns them into
+// exclusive digit bases in place (no separate scan launch).
 __global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(const unsigned long long* __restrict__ keys, int64_t n_max,
                                                                 const unsigned long long* __restrict__ n_dev,
                                                                 int begin_bit, int n_passes,
-                                                                unsigned long long* __restrict__ hist) {
+                                                                unsigned long long* __restrict__ hist,
+                                                                uint32_t* __restrict__ done) {
   const int64_t n = sort_n(n_max, n_dev);
+  if (n == 0) return;  // nothing to sort: no histogram, no ticket
   __shared__ uint32_t h[kMaxPasses][kRadix];
   for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
@@ -60,22 +65,19 @@ __global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(const unsigned l
   __syncthreads();
   for (int i = threadIdx.x; i < n_passes * kRadix; i += blockDim.x)
     if ((&h[0][0])[i]) atomicAdd(&hist[i], (unsigned long long)(&h[0][0])[i]);
-}
-
-// One block: exclusive scan of each pass's 256 bins (hist -> bases, in place).
-__global__ void __launch_bounds__(kRadix) radix_scan_kernel(unsigned long long* hist, int n_passes) {
-  __shared__ unsigned long long s[kRadix];
+  if (!last_block(done)) return;
+  __shared__ unsigned long long sc[kRadix];
   for (int p = 0; p < n_passes; ++p) {
-    const unsigned long long v = hist[p * kRadix + threadIdx.x];
-    s[threadIdx.x] = v;
+    const unsigned long long v = __ldcg(&hist[p * kRadix + threadIdx.x]);
+    sc[threadIdx.x] = v;
     __syncthreads();
     for (int o = 1; o < kRadix; o <<= 1) {
-      const unsigned long long add = threadIdx.x >= o ? s[threadIdx.x - o] : 0ull;
+      const unsigned long long add = threadIdx.x >= o ? sc[threadIdx.x - o] : 0ull;
       __syncthreads();
-      s[threadIdx.x] += add;
+      sc[threadIdx.x] += add;
       __syncthreads();
     }
-    hist[p * kRadix + threadIdx.x] = s[threadIdx.x] - v;
+    hist[p * kRadix + threadIdx.x] = sc[threadIdx.x] - v;
     __syncthreads();
   }
 }
@@ -89,92 +91,320 @@ __global__ void __launch_bounds__(kSortBlock) radix_pass_kernel(
   // tiles past the actual count retire at once (tile ids are handed out in
   // order, so no live tile ever looks back at them).
   const int64_t n = sort_n(n_max, n_dev);
+  if (n == 0) return;  // nothing to sort: retire before touching the tile counter
   __shared__ uint32_t warp_cnt[kSortWarps][kRadix];
   __shared__ unsigned long long tile_base[kRadix];
   __shared__ uint32_t tile_s;
-  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&warp_cnt[0][0])[i] = 0;
-  if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
-  __syncthreads();
-  const uint32_t tile = tile_s;
-  if ((int64_t)tile * kSortTile >= n && tile != 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t seg = (int64_t)tile * kSortTile + (int64_t)warp * (32 * kSortRounds);
   const uint32_t lt_mask = (1u << lane) - 1u;
+  // Persistent blocks take tiles in order from the counter until the keys run
+  // out (the grid is at most the resident grid, so every tile a block waits
+  // on belongs to a running block that has already published its counts).
+  for (;;) {
+    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&warp_cnt[0][0])[i] = 0;
+    if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint32_t tile = tile_s;
+    if ((int64_t)tile * kSortTile >= n) break;
+    const int64_t seg = (int64_t)tile * kSortTile + (int64_t)warp * (32 * kSortRounds);
 
-  unsigned long long key[kSortRounds];
-  uint32_t val[kSortRounds];
-  uint32_t rank[kSortRounds];
-  uint32_t dig[kSortRounds];
-  // Stable per-warp ranking: rounds in input order, lanes in input order.
+    unsigned long long key[kSortRounds];
+    uint32_t val[kSortRounds];
+    uint32_t rank[kSortRounds];
+    uint32_t dig[kSortRounds];
+    // Stable per-warp ranking: rounds in input order, lanes in input order.
 #pragma unroll
-  for (int r = 0; r < kSortRounds; ++r) {
-    const int64_t idx = seg + r * 32 + lane;
-    const bool valid = idx < n;
-    key[r] = valid ? kin[idx] : 0ull;
-    val[r] = valid ? vin[idx] : 0u;
-    const uint32_t d = valid ? (uint32_t)((key[r] >> shift) & 0xffu) : 0x100u;
-    dig[r] = d;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    const uint32_t before = valid ? warp_cnt[warp][d] : 0u;
-    __syncwarp();
-    if (valid && lane == __ffs(peers) - 1) warp_cnt[warp][d] = before + __popc(peers);
-    __syncwarp();
-    rank[r] = before + __popc(peers & lt_mask);
-  }
-  __syncthreads();
-  // Thread t owns digit t: tile count, warp offsets (in place), look-back.
-  {
-    const int d = threadIdx.x;
-    uint32_t tot = 0;
-#pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) {
-      const uint32_t c = warp_cnt[w][d];
-      warp_cnt[w][d] = tot;
-      tot += c;
+    for (int r = 0; r < kSortRounds; ++r) {
+      const int64_t idx = seg + r * 32 + lane;
+      const bool valid = idx < n;
+      key[r] = valid ? kin[idx] : 0ull;
+      val[r] = valid ? vin[idx] : 0u;
+      const uint32_t d = valid ? (uint32_t)((key[r] >> shift) & 0xffu) : 0x100u;
+      dig[r] = d;
+      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      const uint32_t before = valid ? warp_cnt[warp][d] : 0u;
+      __syncwarp();
+      if (valid && lane == __ffs(peers) - 1) warp_cnt[warp][d] = before + __popc(peers);
+      __syncwarp();
+      rank[r] = before + __popc(peers & lt_mask);
     }
-    unsigned long long* my = status + (size_t)tile * kRadix + d;
-    const unsigned long long ep = (unsigned long long)(epoch & 0x3fffffffu) << 32;
-    unsigned long long excl = 0;
-    if (tile == 0) {
-      st_release_u64(my, kFlagPrefix | ep | tot);
-    } else {
-      st_release_u64(my, kFlagAgg | ep | tot);
-      int64_t j = (int64_t)tile - 1;
-      const uint64_t t0 = global_ns();
-      bool timed_out = false;
-      while (j >= 0) {
-        const unsigned long long s = ld_acquire_u64(status + (size_t)j * kRadix + d);
-        const bool ready = (s & (3ull << 62)) != 0 && ((s >> 32) & 0x3fffffffull) == (epoch & 0x3fffffffu);
-        if (!ready) {
-          if (global_ns() - t0 > kWaitLimitNs) {
+    __syncthreads();
+    // Thread t owns digit t: tile count, warp offsets (in place), look-back.
+    {
+      const int d = threadIdx.x;
+      uint32_t tot = 0;
+#pragma unroll
+      for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = warp_cnt[w][d];
+        warp_cnt[w][d] = tot;
+        tot += c;
+      }
+      unsigned long long* my = status + (size_t)tile * kRadix + d;
+      const unsigned long long ep = (unsigned long long)(epoch & 0x3fffffffu) << 32;
+      unsigned long long excl = 0;
+      if (tile == 0) {
+        st_release_u64(my, kFlagPrefix | ep | tot);
+      } else {
+        st_release_u64(my, kFlagAgg | ep | tot);
+        // Batched look-back: the status words of up to kLookback predecessors
+        // are loaded together (one round trip), then consumed nearest first
+        // until a published prefix; a not-yet-published predecessor restarts
+        // the batch from it.
+        constexpr int kLookback = 16;
+        int64_t j = (int64_t)tile - 1;
+        const uint64_t t0 = global_ns();
+        bool timed_out = false;
+        while (j >= 0) {
+          unsigned long long sw[kLookback];
+#pragma unroll
+          for (int q = 0; q < kLookback; ++q)
+            sw[q] = (j - q >= 0) ? ld_acquire_u64(status + (size_t)(j - q) * kRadix + d) : 0ull;
+          int q = 0;
+          bool found = false;
+          for (; q < kLookback && j - q >= 0; ++q) {
+            const unsigned long long s = sw[q];
+            const bool ready = (s & (3ull << 62)) != 0 && ((s >> 32) & 0x3fffffffull) == (epoch & 0x3fffffffu);
+            if (!ready) break;
+            excl += s & 0xffffffffull;
+            if (s & kFlagPrefix) {
+              found = true;
+              break;
+            }
+          }
+          if (found) break;
+          j -= q;
+          if (q == 0 && global_ns() - t0 > kWaitLimitNs) {
             timed_out = true;
             break;
           }
-          continue;
         }
-        excl += s & 0xffffffffull;
-        if (s & kFlagPrefix) break;
-        --j;
+        if (timed_out) raise_error(err, kErrSpinTimeout);
+        st_release_u64(my, kFlagPrefix | ep | (excl + tot));
       }
-      if (timed_out) raise_error(err, kErrSpinTimeout);
-      st_release_u64(my, kFlagPrefix | ep | (excl + tot));
+      tile_base[d] = digit_base[d] + excl;
     }
-    tile_base[d] = digit_base[d] + excl;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+      const uint32_t d = dig[r];
+      if (d < 0x100u) {
+        const unsigned long long pos = tile_base[d] + warp_cnt[warp][d] + rank[r];
+        if (pos < (unsigned long long)n) {
+          kout[pos] = key[r];
+          vout[pos] = val[r];
+        } else {
+          raise_error(err, kErrOutputOverflow);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------ top-k (K6) --
+// Radix select: the k smallest keys all have a top digit <= d*, the smallest
+// digit whose cumulative count reaches k.  One histogram pass over the top
+// digit (its last block finds d* and the threshold), one filter pass that
+// compacts the candidates (keys below the threshold), then the candidates --
+// usually a few hundred -- are sorted: inside one CTA when they fit in a tile
+// (a stable 8-bit LSD counting sort in shared memory), otherwise by the
+// onesweep passes.  Keys are unique (packed count and id), so the first k of
+// the sorted candidates are exactly the first k of the full order.
+constexpr int kTopkBlock = 256;
+
+struct TopkState {
+  unsigned long long threshold;  // candidates: select digit <= threshold
+  unsigned long long shift;      // bit position of the select digit
+  unsigned long long n_cand;     // compacted candidates
+  unsigned long long small;      // 1 when the candidates fit one CTA tile
+  uint32_t done;                 // ticket for the histogram's last block
+  uint32_t pad;
+  unsigned long long hist[kRadix];
+};
+
+// The select digit: by default the top digit of the key; with (lo_bits,
+// hi_max_dev) the key is (hi << lo_bits) | lo where every hi has the same bits
+// above the highest bit of *hi_max_dev (keys packed as (cmax - count) << wa |
+// id), and the digit just below that bit is the first one that orders them.
+__device__ __forceinline__ int topk_shift(int top_shift, int lo_bits, const unsigned long long* hi_max_dev) {
+  if (!hi_max_dev) return top_shift;
+  const unsigned long long m = *hi_max_dev;
+  const int L = m ? 64 - __clzll((long long)m) : 0;
+  const int s = lo_bits + (L > 8 ? L - 8 : 0);
+  return s < top_shift ? s : top_shift;
+}
+
+__global__ void __launch_bounds__(kTopkBlock) topk_hist_kernel(const unsigned long long* __restrict__ keys,
+                                                              int64_t n_max, const unsigned long long* __restrict__ n_dev,
+                                                              int top_shift_default, int lo_bits,
+                                                              const unsigned long long* __restrict__ hi_max_dev, int k,
+                                                              TopkState* st) {
+  const int64_t n = sort_n(n_max, n_dev);
+  const int top_shift = topk_shift(top_shift_default, lo_bits, hi_max_dev);
+  __shared__ uint32_t h[kRadix];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  const int64_t n_w = (n + 31) & ~int64_t(31);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_w; i += stride) {
+    // Warp-aggregated increments: most keys share a few top digits.
+    const uint32_t d = i < n ? (uint32_t)((keys[i] >> top_shift) & 0xffu) : 0x100u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    if (d < 0x100u && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
   }
   __syncthreads();
-#pragma unroll
-  for (int r = 0; r < kSortRounds; ++r) {
-    const uint32_t d = dig[r];
-    if (d < 0x100u) {
-      const unsigned long long pos = tile_base[d] + warp_cnt[warp][d] + rank[r];
-      if (pos < (unsigned long long)n) {
-        kout[pos] = key[r];
-        vout[pos] = val[r];
-      } else {
-        raise_error(err, kErrOutputOverflow);
+  if (h[threadIdx.x]) atomicAdd(&st->hist[threadIdx.x], (unsigned long long)h[threadIdx.x]);
+  if (!last_block(&st->done)) return;
+  // Inclusive scan of the 256 bins (one per thread), then the first digit
+  // whose cumulative count reaches k.
+  __shared__ unsigned long long cum[kRadix];
+  __shared__ int first;
+  unsigned long long x = __ldcg(&st->hist[threadIdx.x]);
+  cum[threadIdx.x] = x;
+  if (threadIdx.x == 0) first = kRadix;
+  __syncthreads();
+  for (int o = 1; o < kRadix; o <<= 1) {
+    const unsigned long long y = threadIdx.x >= o ? cum[threadIdx.x - o] : 0ull;
+    __syncthreads();
+    x += y;
+    cum[threadIdx.x] = x;
+    __syncthreads();
+  }
+  if (x >= (unsigned long long)k) atomicMin(&first, (int)threadIdx.x);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // keys whose select digit is <= first (all keys when the count never reaches k)
+    st->threshold = (unsigned long long)(first >= kRadix ? kRadix - 1 : first);
+    st->shift = (unsigned long long)top_shift;
+    st->n_cand = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kTopkBlock) topk_filter_kernel(const unsigned long long* __restrict__ keys,
+                                                                const uint32_t* __restrict__ vals, int64_t n_max,
+                                                                const unsigned long long* __restrict__ n_dev,
+                                                                TopkState* st, unsigned long long* __restrict__ ck,
+                                                                uint32_t* __restrict__ cv) {
+  const int64_t n = sort_n(n_max, n_dev);
+  const unsigned long long thr = __ldcg(&st->threshold);
+  const int shift = (int)__ldcg(&st->shift);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  const int64_t n_w = (n + 31) & ~int64_t(31);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_w; i += stride) {
+    const unsigned long long key = i < n ? keys[i] : ~0ull;
+    const bool take = i < n && ((key >> shift) & 0xffull) <= thr;
+    const uint32_t ballot = __ballot_sync(0xffffffffu, take);
+    if (!ballot) continue;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(&st->n_cand, (unsigned long long)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (take) {
+      const unsigned long long pos = base + __popc(ballot & ((1u << lane) - 1u));
+      if (pos < (unsigned long long)n_max) {
+        ck[pos] = key;
+        cv[pos] = vals[i];
       }
     }
   }
+}
+
+// Stable LSD radix sort of <= kBlockSortMax pairs inside one CTA (8-bit digits
+// over [begin_bit, end_bit)), with the same warp ranking as the onesweep pass
+// (each warp owns a contiguous segment, rounds and lanes in input order).
+// Sets st->small = 0 and leaves the data alone if there are more candidates
+// (the onesweep passes then sort them).
+constexpr int kBlockSortMax = 2048;
+constexpr int kBlockSortRounds = kBlockSortMax / kSortBlock;  // keys per lane
+
+__global__ void __launch_bounds__(kSortBlock) block_sort_kernel(unsigned long long* __restrict__ ck,
+                                                                uint32_t* __restrict__ cv, TopkState* st,
+                                                                int begin_bit, int end_bit) {
+  extern __shared__ __align__(16) unsigned char bs_smem[];
+  unsigned long long* sk = reinterpret_cast<unsigned long long*>(bs_smem);       // [2][kBlockSortMax]
+  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + 2 * kBlockSortMax);           // [2][kBlockSortMax]
+  __shared__ uint32_t warp_cnt[kSortWarps][kRadix];
+  __shared__ uint32_t dig_base[kRadix];
+  const unsigned long long n = __ldcg(&st->n_cand);
+  if (n > (unsigned long long)kBlockSortMax) {
+    if (threadIdx.x == 0) st->small = 0;
+    return;
+  }
+  if (threadIdx.x == 0) st->small = 1;
+  for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) {
+    sk[i] = ck[i];
+    sv[i] = cv[i];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  int src = 0;
+  for (int shift = begin_bit; shift < end_bit; shift += 8) {
+    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&warp_cnt[0][0])[i] = 0;
+    __syncthreads();
+    const unsigned long long* ks = sk + src * kBlockSortMax;
+    const uint32_t* vs = sv + src * kBlockSortMax;
+    uint32_t rank[kBlockSortRounds], dig[kBlockSortRounds];
+#pragma unroll
+    for (int r = 0; r < kBlockSortRounds; ++r) {
+      const unsigned long long idx = (unsigned long long)warp * (32 * kBlockSortRounds) + r * 32 + lane;
+      const bool valid = idx < n;
+      const uint32_t d = valid ? (uint32_t)((ks[idx] >> shift) & 0xffu) : 0x100u;
+      dig[r] = d;
+      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      const uint32_t before = valid ? warp_cnt[warp][d] : 0u;
+      __syncwarp();
+      if (valid && lane == __ffs(peers) - 1) warp_cnt[warp][d] = before + __popc(peers);
+      __syncwarp();
+      rank[r] = before + __popc(peers & lt_mask);
+    }
+    __syncthreads();
+    {
+      const int d = threadIdx.x;  // one digit per thread
+      uint32_t tot = 0;
+      for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = warp_cnt[w][d];
+        warp_cnt[w][d] = tot;
+        tot += c;
+      }
+      // exclusive scan of the digit totals across the 256 threads
+      dig_base[d] = tot;
+      __syncthreads();
+      uint32_t x = tot;
+      for (int o = 1; o < kRadix; o <<= 1) {
+        const uint32_t y = d >= o ? dig_base[d - o] : 0u;
+        __syncthreads();
+        x += y;
+        dig_base[d] = x;
+        __syncthreads();
+      }
+      dig_base[d] = x - tot;
+    }
+    __syncthreads();
+    unsigned long long* kd = sk + (src ^ 1) * kBlockSortMax;
+    uint32_t* vd = sv + (src ^ 1) * kBlockSortMax;
+#pragma unroll
+    for (int r = 0; r < kBlockSortRounds; ++r) {
+      const uint32_t d = dig[r];
+      if (d < 0x100u) {
+        const unsigned long long idx = (unsigned long long)warp * (32 * kBlockSortRounds) + r * 32 + lane;
+        const uint32_t pos = dig_base[d] + warp_cnt[warp][d] + rank[r];
+        kd[pos] = ks[idx];
+        vd[pos] = vs[idx];
+      }
+    }
+    __syncthreads();
+    src ^= 1;
+  }
+  for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) {
+    ck[i] = sk[src * kBlockSortMax + i];
+    cv[i] = sv[src * kBlockSortMax + i];
+  }
+}
+
+// Key count for the onesweep fallback: 0 when the CTA sort already handled it.
+__global__ void topk_big_count_kernel(const TopkState* st, unsigned long long* big) {
+  if (threadIdx.x == 0) *big = __ldcg(&st->small) ? 0ull : __ldcg(&st->n_cand);
 }
 
 }  // namespace bo
@@ -208,16 +438,18 @@ int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsi
   uint32_t* ctr = reinterpret_cast<uint32_t*>(static_cast<char*>(p) + hist_bytes);
   unsigned long long* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(p) + hist_bytes + ctr_bytes);
   BO_CUDA(ctx, cudaMemsetAsync(p, 0, hist_bytes + ctr_bytes, ctx->stream));
-  const int hg = (int)std::min<int64_t>((n + kSortBlock - 1) / kSortBlock, (int64_t)ctx->num_sms * 4);
-  radix_hist_kernel<<<std::max(hg, 1), kSortBlock, 0, ctx->stream>>>(keys, n, n_dev, begin_bit, n_passes, hist);
+  const int hg = (int)std::min<int64_t>((n + kSortBlock - 1) / kSortBlock, (int64_t)ctx->num_sms);
+  radix_hist_kernel<<<std::max(hg, 1), kSortBlock, 0, ctx->stream>>>(keys, n, n_dev, begin_bit, n_passes, hist,
+                                                                      ctr + kMaxPasses);
   if ((rc = after_launch(ctx, "radix_hist_kernel"))) return rc;
-  radix_scan_kernel<<<1, kRadix, 0, ctx->stream>>>(hist, n_passes);
-  if ((rc = after_launch(ctx, "radix_scan_kernel"))) return rc;
+  const int64_t resident = (int64_t)ctx->num_sms *
+                           occupancy_blocks(reinterpret_cast<const void*>(&radix_pass_kernel), kSortBlock, 0);
+  const int pass_grid = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, resident));
   unsigned long long *src_k = keys, *dst_k = tmp_keys;
   uint32_t *src_v = vals, *dst_v = tmp_vals;
   for (int pass = 0; pass < n_passes; ++pass) {
     const uint32_t epoch = g_sort_epoch.fetch_add(1);
-    radix_pass_kernel<<<(int)tiles, kSortBlock, 0, ctx->stream>>>(src_k, src_v, dst_k, dst_v, n, n_dev,
+    radix_pass_kernel<<<pass_grid, kSortBlock, 0, ctx->stream>>>(src_k, src_v, dst_k, dst_v, n, n_dev,
                                                                     begin_bit + 8 * pass, hist + pass * kRadix, status,
                                                                     ctr + pass, epoch, ctx->d_err);
     if ((rc = after_launch(ctx, "radix_pass_kernel"))) return rc;
@@ -229,6 +461,47 @@ int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsi
     BO_CUDA(ctx, cudaMemcpyAsync(vals, src_v, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, ctx->stream));
   }
   return BO_OK;
+}
+}  // namespace bo
+
+namespace bo {
+// The k smallest keys in ascending order, written to the front of
+// (cand_keys, cand_vals) (capacity n_max each); the count of keys comes from
+// n_dev.  Asynchronous; no host round trip.
+int radix_topk_pairs(bo_ctx* ctx, const unsigned long long* keys, const uint32_t* vals, int64_t n_max,
+                     const unsigned long long* n_dev, int key_bits, int k, unsigned long long* cand_keys,
+                     uint32_t* cand_vals, unsigned long long* tmp_keys, uint32_t* tmp_vals, int lo_bits,
+                     const unsigned long long* hi_max_dev) {
+  void* p = nullptr;
+  int rc = region(ctx, "topk_state", sizeof(TopkState), &p);
+  if (rc) return rc;
+  TopkState* st = static_cast<TopkState*>(p);
+  BO_CUDA(ctx, cudaMemsetAsync(st, 0, sizeof(TopkState), ctx->stream));
+  const int bits = std::max(8, ((key_bits + 7) / 8) * 8);
+  const int top_shift = bits - 8;
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>((n_max + kTopkBlock - 1) / kTopkBlock, ctx->num_sms));
+  topk_hist_kernel<<<g, kTopkBlock, 0, ctx->stream>>>(keys, n_max, n_dev, top_shift, lo_bits, hi_max_dev,
+                                                       std::max(k, 1), st);
+  if ((rc = after_launch(ctx, "topk_hist_kernel"))) return rc;
+  topk_filter_kernel<<<g, kTopkBlock, 0, ctx->stream>>>(keys, vals, n_max, n_dev, st, cand_keys, cand_vals);
+  if ((rc = after_launch(ctx, "topk_filter_kernel"))) return rc;
+  const size_t bs_smem = (sizeof(unsigned long long) + sizeof(uint32_t)) * 2 * kBlockSortMax;
+  static bool bs_ready = false;
+  if (!bs_ready) {
+    BO_CUDA(ctx, cudaFuncSetAttribute(reinterpret_cast<const void*>(&block_sort_kernel),
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bs_smem));
+    bs_ready = true;
+  }
+  block_sort_kernel<<<1, kSortBlock, bs_smem, ctx->stream>>>(cand_keys, cand_vals, st, 0, bits);
+  if ((rc = after_launch(ctx, "block_sort_kernel"))) return rc;
+  // Large candidate sets (heavy ties in the top digit): the onesweep passes.
+  // With a small set they see a zero count and retire immediately.
+  void* q = nullptr;
+  if ((rc = region(ctx, "topk_bigcount", 64, &q))) return rc;
+  unsigned long long* big = static_cast<unsigned long long*>(q);
+  topk_big_count_kernel<<<1, 32, 0, ctx->stream>>>(st, big);
+  if ((rc = after_launch(ctx, "topk_big_count_kernel"))) return rc;
+  return radix_sort_pairs(ctx, cand_keys, cand_vals, tmp_keys, tmp_vals, n_max, 0, bits, big);
 }
 }  // namespace bo
 

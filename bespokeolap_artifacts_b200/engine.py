@@ -205,12 +205,12 @@ class Engine:
 
     # ------------------------------------------------------- group-by ------
     @staticmethod
-    def gb_args(a_id, b_a, b_c, c_cat, c_year, n_a, n_b, n_c, cat_set, year_lo, year_hi, k, a_id_max):
+    def gb_args(a_id, b_a, b_c, c_cat, c_year, n_a, n_b, n_c, cat_set, year_lo, year_hi, k, a_id_max, a_mask=None):
         cats = np.ascontiguousarray(cat_set, dtype=np.uint16)
         a = N.GbACols(N.ptr(a_id), n_a)
         b = N.GbBCols(N.ptr(b_a), N.ptr(b_c), n_b)
         c = N.GbCCols(N.ptr(c_cat), N.ptr(c_year), n_c)
-        prm = N.GbParams(cats.ctypes.data, len(cats), year_lo, year_hi, k, a_id_max)
+        prm = N.GbParams(cats.ctypes.data, len(cats), year_lo, year_hi, k, a_id_max, N.ptr(a_mask))
         return a, b, c, prm, cats
 
     def groupby_plain(self, dev: dict, g) -> dict:
@@ -218,7 +218,8 @@ class Engine:
         ``dev`` holds device columns a_ids, b_a, b_c, c_cat, c_year."""
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
                                           len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
-                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)))
+                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
+                                          dev.get("a_mask"))
         out = N.GbResult()
         self.ctx.call("bo_groupby_topk_plain", C.byref(a), C.byref(b), C.byref(c), C.byref(prm), C.byref(out))
         return out.as_dict()
@@ -226,7 +227,8 @@ class Engine:
     def groupby_presized(self, dev: dict, g, pred_dev) -> dict:
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
                                           len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
-                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)))
+                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
+                                          dev.get("a_mask"))
         out = N.GbResult()
         self.ctx.call("bo_groupby_topk_presized", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
                       C.c_void_p(N.ptr(pred_dev)), C.byref(out))
@@ -235,24 +237,32 @@ class Engine:
     def groupby_presized_device(self, dev: dict, g, pred_dev, out_dev) -> None:
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
                                           len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
-                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)))
+                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
+                                          dev.get("a_mask"))
         self.ctx.call("bo_groupby_topk_presized_device", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
                       C.c_void_p(N.ptr(pred_dev)), C.c_void_p(N.ptr(out_dev)))
 
     def groupby_distinct_device(self, dev: dict, g, out_dev) -> None:
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
                                           len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
-                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)))
+                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
+                                          dev.get("a_mask"))
         self.ctx.call("bo_groupby_distinct_device", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
                       C.c_void_p(N.ptr(out_dev)))
 
-    @staticmethod
-    def groupby_to_device(g) -> dict:
+    def groupby_to_device(self, g, prebuild_a_mask: bool = False) -> dict:
+        """Uploads the three tables; optionally builds A's id mask once (a
+        per-table structure, like the sketches)."""
         import torch
 
         d = {k: torch.from_numpy(np.ascontiguousarray(getattr(g, k))).cuda()
              for k in ("a_ids", "b_a", "b_c", "c_cat", "c_year")}
         d["a_id_max"] = int(g.a_ids.max()) if len(g.a_ids) else 0
+        if prebuild_a_mask:
+            m = torch.zeros((d["a_id_max"] + 32) // 32, dtype=torch.int32, device="cuda")
+            a = N.GbACols(N.ptr(d["a_ids"]), len(g.a_ids))
+            self.ctx.call("bo_groupby_a_mask_device", C.byref(a), d["a_id_max"], C.c_void_p(m.data_ptr()))
+            d["a_mask"] = m
         return d
 
     # ---------------------------------------------------------- sort -------

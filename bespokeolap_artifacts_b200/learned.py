@@ -248,3 +248,112 @@ class JoinSizer:
 
     def predict_device(self, features: np.ndarray, counts_dev) -> None:
         self.mlp.predict_counts_device(features, counts_dev)
+
+
+# ------------------------------------------------------ group-by sizing -----
+GB_FEATURES = 12
+CAT_DOMAIN = 4096
+
+
+@dataclass
+class GroupByTableStats:
+    """Load-time statistics of the three group-by inputs."""
+    n_a: int
+    n_b: int
+    n_c: int
+    year: IntSketch
+    cat_hist: np.ndarray   # exact counts of category codes < CAT_DOMAIN
+    b_a: IntSketch         # HLL distinct of B.a_id
+    b_c: IntSketch         # HLL distinct of B.c_id
+
+
+def groupby_table_stats(ctx: N.Context, dev: dict, n_a: int, n_b: int, n_c: int) -> GroupByTableStats:
+    return GroupByTableStats(
+        n_a, n_b, n_c, sketch_i32(ctx, dev["c_year"], n_c), histogram_small(ctx, dev["c_cat"], 2, n_c, CAT_DOMAIN),
+        sketch_i32(ctx, dev["b_a"], n_b), sketch_i32(ctx, dev["b_c"], n_b))
+
+
+def groupby_naive(st: GroupByTableStats, cat_set, year_lo: int, year_hi: int) -> tuple[float, float]:
+    """Independence / uniformity estimates: joined rows = n_b * sel(C), groups =
+    distinct a_ids that see at least one joining row (rows spread evenly)."""
+    if st.n_c == 0 or st.n_b == 0:
+        return 0.0, 0.0
+    f_cat = float(st.cat_hist[np.asarray(cat_set, dtype=np.int64)].sum()) / st.n_c
+    f_c = f_cat * st.year.frac_between(year_lo, year_hi)
+    joined = st.n_b * f_c
+    d_a = max(st.b_a.distinct, 1.0)
+    per_a = st.n_b / d_a
+    groups = d_a * (1.0 - (1.0 - min(f_c, 1.0)) ** per_a)
+    return groups, joined
+
+
+def groupby_features(st: GroupByTableStats, cat_set, year_lo: int, year_hi: int) -> np.ndarray:
+    f_cat = float(st.cat_hist[np.asarray(cat_set, dtype=np.int64)].sum()) / max(st.n_c, 1)
+    f_year = st.year.frac_between(year_lo, year_hi)
+    groups, joined = groupby_naive(st, cat_set, year_lo, year_hi)
+    lg = lambda v: math.log1p(max(v, 0.0)) / LOG_SCALE  # noqa: E731
+    return np.array([
+        lg(st.n_a), lg(st.n_b), lg(st.n_c), f_cat, f_year, f_cat * f_year,
+        lg(st.b_a.distinct), lg(st.b_c.distinct), st.b_a.distinct / max(st.n_b, 1),
+        st.b_c.distinct / max(st.n_b, 1), lg(groups), lg(joined),
+    ], dtype=np.float32)
+
+
+def make_groupby_training_set(engine, n_tables: int = 16, preds_per_table: int = 30, seed: int = 77,
+                              nb_min: int = 100_000, nb_max: int = 4_000_000):
+    """(features, [log1p(groups), log1p(joined)], naive estimates): exact targets
+    from the plain GPU pipeline's pre-pass (bo_groupby_distinct_device)."""
+    import torch
+
+    from .datagen import GroupByInput, gen_groupby
+
+    rng = np.random.default_rng(seed)
+    xs, ts, naive = [], [], []
+    out = torch.zeros(2, dtype=torch.int64, device="cuda")
+    for _ in range(n_tables):
+        n_b = int(math.exp(rng.uniform(math.log(nb_min), math.log(nb_max))))
+        n_a = max(1000, int(n_b * rng.uniform(0.02, 0.2)))
+        n_c = max(1000, int(n_b * rng.uniform(0.05, 0.3)))
+        g = gen_groupby(n_a, n_b, n_c, seed=int(rng.integers(1 << 30)), s_a=float(rng.uniform(0.7, 1.4)),
+                        s_c=float(rng.uniform(0.5, 1.2)))
+        dev = engine.groupby_to_device(g)
+        st = groupby_table_stats(engine.ctx, dev, n_a, n_b, n_c)
+        for _ in range(preds_per_table):
+            k = int(rng.integers(1, 17))
+            cats = np.sort(rng.choice(113, size=k, replace=False)).astype(np.uint16)
+            lo = int(rng.integers(1900, 2021))
+            hi = int(min(2020, lo + rng.integers(0, 60)))
+            q = GroupByInput(g.a_ids, g.b_a, g.b_c, g.c_cat, g.c_year, cats, lo, hi, 10, g.seed)
+            engine.groupby_distinct_device(dev, q, out)
+            engine.synchronize()
+            groups, joined = (int(v) for v in out.tolist())
+            xs.append(groupby_features(st, cats, lo, hi))
+            ts.append([math.log1p(groups), math.log1p(joined)])
+            naive.append(groupby_naive(st, cats, lo, hi))
+        del dev
+    return np.stack(xs), np.array(ts, np.float32), np.array(naive)
+
+
+class GroupBySizer:
+    """Trained group-table sizer: features -> predicted (groups, joined rows);
+    the group count is written on the device for the presized group-by."""
+
+    def __init__(self, engine, seed: int = 9):
+        self.engine = engine
+        self.mlp = Mlp(engine.ctx, GB_FEATURES, 2, seed)
+
+    def fit(self, x, t, epochs: int = 3000, lr: float = 2e-3) -> float:
+        return self.mlp.train(x, t, epochs, lr)
+
+    def predict_host(self, x: np.ndarray) -> np.ndarray:
+        import torch
+
+        xd = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).cuda()
+        yd = torch.empty((x.shape[0], 2), dtype=torch.float32, device="cuda")
+        self.mlp.infer_device(xd, x.shape[0], yd)
+        self.engine.synchronize()
+        return np.expm1(yd.cpu().numpy().astype(np.float64)).clip(min=0)
+
+    def predict_device(self, features: np.ndarray, counts_dev) -> None:
+        """counts_dev[0] = predicted groups, counts_dev[1] = predicted joined rows."""
+        self.mlp.predict_counts_device(features, counts_dev)

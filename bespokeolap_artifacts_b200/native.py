@@ -142,7 +142,7 @@ class GbCCols(C.Structure):
 
 class GbParams(C.Structure):
     _fields_ = [("categories", C.c_void_p), ("n_categories", C.c_int32), ("year_lo", C.c_int32),
-                ("year_hi", C.c_int32), ("k", C.c_int32), ("a_id_max", C.c_int32)]
+                ("year_hi", C.c_int32), ("k", C.c_int32), ("a_id_max", C.c_int32), ("a_mask", C.c_void_p)]
 
 
 class GbRow(C.Structure):
@@ -215,6 +215,7 @@ _SIGNATURES = {
                                             C.POINTER(GbParams), _P, C.POINTER(GbResult)]),
     "bo_groupby_distinct_device": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),
                                               C.POINTER(GbParams), _P]),
+    "bo_groupby_a_mask_device": (C.c_int, [_P, C.POINTER(GbACols), C.c_int32, _P]),
     "bo_radix_sort_pairs_device": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, C.c_int32]),
     "bo_radix_sort_pairs_host": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, C.c_int32]),
     "bo_sketch_i32": (C.c_int, [_P, _P, C.c_int64, C.POINTER(Sketch)]),

@@ -288,6 +288,8 @@ typedef struct bo_gb_params {
   int32_t year_lo, year_hi;
   int32_t k;                   /* <= BO_GB_MAX_K */
   int32_t a_id_max;            /* every id of A lies in [0, a_id_max] (negative ids are skipped) */
+  const uint32_t* a_mask;      /* optional device bitmap of A's ids over [0, a_id_max], built once per
+                                  table by bo_groupby_a_mask_device; NULL builds it inside the call */
 } bo_gb_params;
 typedef struct bo_gb_row {
   int32_t a_id;
@@ -322,6 +324,11 @@ int bo_groupby_topk_presized_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo
 int bo_groupby_topk_presized(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
                              const bo_gb_params* params, const float* predicted_groups_device,
                              bo_gb_result* out_host);
+/* Bitmap of A's ids over [0, a_id_max] ((a_id_max + 32) / 32 words, device),
+ * the semi-join mask of the group-by (the reference rebuilds such masks per
+ * query, e.g. build_id_mask in bespoke_ceb/query_q1a.cpp); it depends only on
+ * A, so it can be built once when the table is loaded.  Asynchronous. */
+int bo_groupby_a_mask_device(bo_ctx* ctx, const bo_gb_a_cols* a, int32_t a_id_max, uint32_t* mask_device);
 /* The exact pre-pass alone: out_device[0] = distinct qualifying groups,
  * out_device[1] = joined rows (device int64[2]); asynchronous. */
 int bo_groupby_distinct_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,

@@ -98,3 +98,13 @@ def test_groupby_distinct_prepass(engine, torch_cuda):
     engine.groupby_distinct_device(engine.groupby_to_device(g), g, out)
     engine.synchronize()
     assert out.tolist() == [o["n_groups"], o["joined_rows"]]
+
+
+def test_groupby_prebuilt_a_mask(engine, torch_cuda):
+    torch = torch_cuda
+    g = dg.gen_groupby(100_000, 1_500_000, 200_000, seed=9)
+    o = O.groupby_topk(g)
+    dev = engine.groupby_to_device(g, prebuild_a_mask=True)
+    assert same(engine.groupby_plain(dev, g), o)
+    pred = torch.tensor([float(o["n_groups"])], dtype=torch.float32, device="cuda")
+    assert same(engine.groupby_presized(dev, g, pred), o)
