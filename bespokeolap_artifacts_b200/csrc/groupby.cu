@@ -34,14 +34,17 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "rows.cuh"
 #include "context.cuh"
 
 namespace bo {
 
-constexpr unsigned long long kGbEmpty = ~0ull;
-constexpr int kGbBloomLog2Words = 14;
-constexpr uint32_t kGbBloomWords = 1u << kGbBloomLog2Words;
-constexpr uint32_t kGbBloomBytes = kGbBloomWords * 4u;
+// The group table and the C-id Bloom filter use the join's slot and filter
+// formats (rows.cuh).
+constexpr unsigned long long kGbEmpty = kEmptySlot;
+constexpr int kGbBloomLog2Words = kBloomLog2Words;
+constexpr uint32_t kGbBloomWords = kBloomWords;
+constexpr uint32_t kGbBloomBytes = kBloomBytes;
 constexpr int kGbBlock = 256;
 constexpr int kGbWarps = kGbBlock / 32;
 constexpr int kGbRowsPerLane = 16;
@@ -75,27 +78,6 @@ struct CatSet {
   uint16_t v[kMaxCats];
   int32_t n;
 };
-
-// Multiplicative (Fibonacci) hashing: one multiply gives the word from the
-// high bits and two bit positions from the low bits -- cheap enough to run on
-// every B row.
-__device__ __forceinline__ void gb_bloom_pos(uint32_t c, uint32_t& word, uint32_t& bits) {
-  const uint32_t h = c * 0x9E3779B1u;
-  word = h >> (32 - kGbBloomLog2Words);
-  bits = (1u << (h & 31u)) | (1u << ((h >> 5) & 31u));
-}
-
-__device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t& total) {
-  const int lane = threadIdx.x & 31;
-  uint32_t x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  total = __shfl_sync(0xffffffffu, x, 31);
-  return x - v;
-}
 
 __device__ __forceinline__ int32_t gb_presize_log2(const float* pred, int32_t host_log2, int32_t max_log2) {
   if (!pred) return host_log2;
@@ -192,7 +174,7 @@ __global__ void __launch_bounds__(256) gb_cfilter_kernel(bo_gb_c_cols c, CatSet 
       const int k = __ffs(b) - 1;
       b &= b - 1;
       uint32_t bw, bb;
-      gb_bloom_pos((uint32_t)(r0 + k), bw, bb);
+      bloom_pos((uint32_t)(r0 + k), bw, bb);
       atomicOr(bloom + bw, bb);
     }
   }
@@ -224,27 +206,6 @@ __global__ void gb_amask_kernel(bo_gb_a_cols a, int32_t a_id_max, uint32_t* __re
 }
 
 // ------------------------------------------------------------------ scan --
-__device__ __forceinline__ bool gb_global_insert(unsigned long long* slots, int32_t* mins, uint64_t mask, uint32_t key,
-                                                 uint32_t cnt, int32_t mn, uint32_t& newkeys,
-                                                 uint64_t start = ~0ull) {
-  uint64_t idx = start == ~0ull ? (hash32(key) & mask) : start;
-  const unsigned long long claim = (unsigned long long)key << 32;
-  for (uint64_t step = 0; step <= mask; ++step) {
-    // CAS first: one round trip claims an empty slot or returns its owner.
-    unsigned long long v = atomicCAS(slots + idx, kGbEmpty, claim);
-    if (v == kGbEmpty) {
-      ++newkeys;
-      v = claim;
-    }
-    if ((uint32_t)(v >> 32) == key) {
-      atomicAdd(slots + idx, (unsigned long long)cnt);
-      atomicMin(mins + idx, mn);
-      return true;
-    }
-    idx = (idx + 1) & mask;
-  }
-  return false;
-}
 
 // kMode 0: exact distinct pre-pass (bits of a distinct bitmap); 1: aggregate.
 template <int kMode>
@@ -421,7 +382,7 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
     for (int half = 0; half < 2; ++half) {
       const uint32_t hm = (hit >> (8 * half)) & 0xffu;
       uint32_t total;
-      uint32_t pos = warp_excl_scan(__popc(hm), total);
+      uint32_t pos = warp_exclusive_scan(__popc(hm), total);
       if (total == 0) continue;  // warp-uniform
       if (qn + total > kGbQueue) {  // keep room: resolve what is queued first
         resolve(qn);
@@ -515,7 +476,7 @@ __global__ void __launch_bounds__(kCompactBlock) gb_compact_kernel(const unsigne
       occ += v[j] != kGbEmpty;
     }
     uint32_t wtot;
-    const uint32_t mine = warp_excl_scan(occ, wtot);
+    const uint32_t mine = warp_exclusive_scan(occ, wtot);
     if (lane == 0) warp_off[warp] = wtot;
     __syncthreads();
     if (threadIdx.x == 0) {

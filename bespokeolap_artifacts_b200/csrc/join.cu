@@ -24,14 +24,11 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "rows.cuh"
 #include "context.cuh"
 
 namespace bo {
 
-constexpr unsigned long long kEmptySlot = ~0ull;
-constexpr int kBloomLog2Words = 14;  // 16384 32-bit words = 64 KB = 2^19 bits
-constexpr uint32_t kBloomWords = 1u << kBloomLog2Words;
-constexpr uint32_t kBloomBytes = kBloomWords * 4u;
 constexpr int kJoinBlock = 512;
 constexpr int kBuildBlock = 256;
 constexpr int kMinCapLog2 = 10;
@@ -49,29 +46,6 @@ struct JoinMeta {
   unsigned long long count;    // K7 output
 };
 
-// Bloom positions from the key with one multiply (Fibonacci hashing): the word
-// from the high bits, two bit positions from the low bits.  Cheap enough for
-// every probe row; the table uses the stronger hash32 only for the ~9% that
-// pass.
-__device__ __forceinline__ void bloom_pos(uint32_t key, uint32_t& word, uint32_t& bits) {
-  const uint32_t h2 = key * 0x9E3779B1u;
-  word = h2 >> (32 - kBloomLog2Words);
-  bits = (1u << (h2 & 31u)) | (1u << ((h2 >> 5) & 31u));
-}
-
-// The same test as (word & bits) == bits with two funnel-shift rotates (the
-// rotate amount uses the low 5 bits, so no masking): 1 if the key may be in
-// the filter.
-__device__ __forceinline__ uint32_t bloom_test(const uint32_t* bl, uint32_t wmask, uint32_t key) {
-  const uint32_t h2 = key * 0x9E3779B1u;
-  const uint32_t x = bl[(h2 >> (32 - kBloomLog2Words)) & wmask];
-  return __funnelshift_r(x, x, h2) & __funnelshift_r(x, x, h2 >> 5) & 1u;
-}
-
-// Row qualifies on the build side (date < date_lt and segment == seg).
-__device__ __forceinline__ bool build_qual(int32_t date, uint32_t seg_byte, int32_t date_lt, uint32_t seg) {
-  return date < date_lt && seg_byte == seg;
-}
 
 // ------------------------------------------------------------ K7 count ----
 __global__ void __launch_bounds__(kBuildBlock) join_count_kernel(bo_join_build_cols b, int32_t date_lt, uint32_t seg,
@@ -137,28 +111,6 @@ __global__ void join_init_kernel(unsigned long long* slots, uint32_t* bloom, Joi
 }
 
 // ------------------------------------------------------------ K2 build ---
-__device__ __forceinline__ void join_insert(unsigned long long* slots, uint32_t* bloom, uint64_t mask, int32_t key,
-                                            uint32_t& newkeys, bool& full) {
-  const uint32_t h = hash32((uint32_t)key);
-  uint64_t idx = h & mask;
-  const unsigned long long mine = ((unsigned long long)(uint32_t)key << 32) | 1ull;
-  for (uint64_t step = 0; step <= mask; ++step) {
-    const unsigned long long old = atomicCAS(slots + idx, kEmptySlot, mine);
-    if (old == kEmptySlot) {
-      ++newkeys;
-      uint32_t w, bits;
-      bloom_pos((uint32_t)key, w, bits);
-      atomicOr(bloom + w, bits);
-      return;
-    }
-    if ((uint32_t)(old >> 32) == (uint32_t)key) {
-      atomicAdd(slots + idx, 1ull);  // multiplicity lives in the low word
-      return;
-    }
-    idx = (idx + 1) & mask;
-  }
-  full = true;
-}
 
 // 16 build rows per thread per step: one 128-bit segment load and four 128-bit
 // date loads; the qualifying rows (about 4%) of the whole warp are then
@@ -166,17 +118,6 @@ __device__ __forceinline__ void join_insert(unsigned long long* slots, uint32_t*
 // all lanes together.
 constexpr int kBuildRowsPerThread = 16;
 
-__device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t v, uint32_t& total) {
-  const int lane = threadIdx.x & 31;
-  uint32_t x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  total = __shfl_sync(0xffffffffu, x, 31);
-  return x - v;
-}
 
 __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_cols b, int32_t date_lt, uint32_t seg,
                                                                  unsigned long long* slots, uint32_t* bloom,
@@ -263,57 +204,6 @@ __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_c
 }
 
 // ------------------------------------------------------------ K3 probe ---
-// With p = 100*q + r and m = 100 - d: trunc(p*m/100) = q*m + (r*m)/100 = T and
-// p*m = 100*T + rr, rr = (r*m) % 100 -- exact forms from the reference form.
-struct ProbeAcc {
-  unsigned long long cnt = 0, rsum = 0;
-  unsigned __int128 tsum = 0;
-  uint32_t bad = 0;
-};
-
-__device__ __forceinline__ void accumulate_match(uint64_t p, uint64_t d, unsigned long long mult, ProbeAcc& a) {
-  if (p >= 0x80000000ull || d > 100u) {
-    a.bad |= kErrValueRange;
-    return;
-  }
-  const uint32_t m = 100u - (uint32_t)d, pq = (uint32_t)p / 100u, pr = (uint32_t)p - pq * 100u;
-  const uint32_t rm = pr * m, rq = rm / 100u, rr = rm - rq * 100u;
-  const uint32_t T = pq * m + rq;
-  a.cnt += mult;
-  a.tsum += (unsigned __int128)((unsigned long long)T * mult);
-  a.rsum += (unsigned long long)rr * mult;
-}
-
-// Linear-probing continuation for the rare key whose first slot held another key.
-__device__ __noinline__ unsigned long long probe_slow(const unsigned long long* slots, uint64_t mask, uint64_t idx,
-                                                      uint32_t key) {
-  for (uint64_t step = 1; step <= mask; ++step) {
-    idx = (idx + 1) & mask;
-    const unsigned long long v = __ldg(slots + idx);
-    if (v == kEmptySlot) return 0;
-    if ((uint32_t)(v >> 32) == key) return v & 0xffffffffull;
-  }
-  return 0;
-}
-
-__device__ __forceinline__ void probe_one(int32_t fk, int64_t row, const uint32_t* bloom_s, bool use_bloom,
-                                          const unsigned long long* slots, uint64_t mask, const int64_t* price,
-                                          const int64_t* disc, ProbeAcc& a) {
-  const uint32_t h = hash32((uint32_t)fk);
-  if (use_bloom) {
-    uint32_t w, bits;
-    bloom_pos((uint32_t)fk, w, bits);
-    if ((bloom_s[w] & bits) != bits) return;
-  }
-  const unsigned long long v = __ldg(slots + (h & mask));
-  unsigned long long mult = 0;
-  if (v == kEmptySlot) return;
-  if ((uint32_t)(v >> 32) == (uint32_t)fk)
-    mult = v & 0xffffffffull;
-  else
-    mult = probe_slow(slots, mask, h & mask, (uint32_t)fk);
-  if (mult) accumulate_match((uint64_t)__ldg(price + row), (uint64_t)__ldg(disc + row), mult, a);
-}
 
 // Warp-centric probe.  A warp owns 512 consecutive probe rows per step (16 per
 // lane, four 128-bit fk loads).  Every lane hashes its rows and tests the Bloom
@@ -414,7 +304,7 @@ __global__ void __launch_bounds__(kJoinBlock) join_probe_kernel(bo_join_probe_co
           if ((uint32_t)(v >> 32) == (uint32_t)key)
             mult = v & 0xffffffffull;
           else
-            mult = probe_slow(slots, mask, h & mask, (uint32_t)key);
+            mult = probe_slow<false>(slots, mask, h & mask, (uint32_t)key);
         }
         if (mult) accumulate_match((uint64_t)__ldg(p.price + row), (uint64_t)__ldg(p.discount + row), mult, acc);
       }

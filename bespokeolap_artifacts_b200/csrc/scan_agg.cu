@@ -28,80 +28,10 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "rows.cuh"
 #include "context.cuh"
 
 namespace bo {
-
-constexpr int kScanBlock = 256;
-constexpr int kMaxRowsPerThread = 256;
-constexpr int kQ1Sums = 8;  // canonical totals per group, bo_q1_agg order without the doubles
-
-// ------------------------------------------------------------ accumulators --
-// Canonical per-group totals (global 128-bit accumulators, index s):
-//   0 count  1 qty  2 price  3 disc  4 dp = sum trunc(p*(100-d)/100)
-//   5 dpe = sum p*(100-d)  6 ch = sum dp*(100+t)  7 che = sum p*(100-d)*(100+t)
-//
-// Per-thread partials live in shared memory, one private column per thread
-// (layout [group][word][thread], 8-byte words): a row adds into its own group's
-// words with a load-add-store, so the update is branch-free, conflict-free
-// (a warp touches 32 consecutive words whatever its lanes' groups) and costs a
-// handful of instructions instead of one predicated update per group.
-// Small sums are bit-packed into one word; kMaxRowsPerThread = 256 bounds
-// every field so no packed field can carry into the next.
-// The column is private to its thread, so a plain load-add-store suffices (a
-// shared-memory atomic would serialise in the atomic unit for nothing).
-__device__ __forceinline__ void red_shared_u64(unsigned long long* p, unsigned long long v) {
-  *p += v;
-}
-
-// Wide layout (0 <= qty, price < 2^31; 0 <= disc, tax <= 100).  With
-// p = 100*q + r and m = 100 - d:
-//   trunc(p*m/100) = q*m + (r*m)/100 =: T,   p*m = 100*T + rr,  rr = (r*m) % 100
-// so the exact forms follow from the reference forms plus the small residues:
-//   dpe = 100*sum T + sum rr,   che = 100*sum T*(100+t) + sum rr*(100+t).
-// Words per group: 0 qty  1 price  2 T  3 T*(100+t)  4 packed
-//   packed = count | disc << 9 | rr << 24 | rr*(100+t) << 39
-// (<= 256 rows: count < 2^9, disc sum < 2^15, rr sum < 2^15, rr*(100+t) sum < 2^23).
-constexpr int kWideWords = 5;
-
-__device__ __forceinline__ void wide_row(unsigned long long* col, int32_t ship, int32_t cutoff, uint64_t q,
-                                         uint64_t p, uint64_t d, uint64_t t, uint32_t fa, uint32_t fb,
-                                         uint32_t n_fa, uint32_t n_fb, uint32_t& bad) {
-  if (ship > cutoff) return;
-  const bool in_range = q < 0x80000000ull && p < 0x80000000ull && d <= 100u && t <= 100u;
-  const bool code_ok = fa < n_fa && fb < n_fb;
-  if (!(in_range && code_ok)) {
-    bad |= (in_range ? 0u : kErrValueRange) | (code_ok ? 0u : kErrBadGroupCode);
-    return;
-  }
-  const uint32_t p32 = (uint32_t)p, m = 100u - (uint32_t)d, tm = 100u + (uint32_t)t;
-  const uint32_t pq = p32 / 100u, pr = p32 - pq * 100u;
-  const uint32_t rm = pr * m;
-  const uint32_t rq = rm / 100u, rr = rm - rq * 100u;
-  const uint32_t T = pq * m + rq;
-  unsigned long long* w = col + (fa * n_fb + fb) * (kWideWords * kScanBlock);
-  red_shared_u64(w, q);
-  red_shared_u64(w + kScanBlock, p);
-  red_shared_u64(w + 2 * kScanBlock, T);
-  red_shared_u64(w + 3 * kScanBlock, (unsigned long long)T * tm);
-  red_shared_u64(w + 4 * kScanBlock, 1ull | ((unsigned long long)d << 9) | ((unsigned long long)rr << 24) |
-                                         ((unsigned long long)(rr * tm) << 39));
-}
-
-// Expands one thread's wide-layout words of group g into the canonical sums.
-__device__ __forceinline__ void wide_canon(const unsigned long long* col, int g, int64_t v[kQ1Sums]) {
-  const unsigned long long* w = col + g * (kWideWords * kScanBlock);
-  const uint64_t pk = w[4 * kScanBlock];
-  const int64_t T = (int64_t)w[2 * kScanBlock], TT = (int64_t)w[3 * kScanBlock];
-  v[0] = (int64_t)(pk & 0x1ffu);
-  v[1] = (int64_t)w[0];
-  v[2] = (int64_t)w[kScanBlock];
-  v[3] = (int64_t)((pk >> 9) & 0x7fffu);
-  v[4] = T;
-  v[5] = 100 * T + (int64_t)((pk >> 24) & 0x7fffu);
-  v[6] = TT;
-  v[7] = 100 * TT + (int64_t)(pk >> 39);
-}
 
 // Storage-plan layout: words per group
 //   0 price  1 dp  2 dp*(100+t)  3 p*(100-d)  4 p*(100-d)*(100+t)
@@ -178,16 +108,7 @@ __device__ void q1_finalize_group(int g, unsigned long long* acc, bo_q1_agg* out
   __int128 t[kQ1Sums];
 #pragma unroll
   for (int s = 0; s < kQ1Sums; ++s) t[s] = load_i128(a + 2 * s);
-  bo_q1_agg r;
-  r.count = narrow_i64(t[0], bad);
-  r.sum_qty = narrow_i64(t[1], bad);
-  r.sum_base_price = narrow_i64(t[2], bad);
-  r.sum_disc = narrow_i64(t[3], bad);
-  r.sum_disc_price = narrow_i64(t[4], bad);
-  r.sum_disc_price_exact = narrow_i64(t[5], bad);
-  r.sum_charge = to_bo_i128(t[6]);
-  r.sum_charge_exact = to_bo_i128(t[7]);
-  out[g] = r;
+  out[g] = q1_record(t, bad);
 #pragma unroll
   for (int s = 0; s < 2 * kQ1Sums; ++s) a[s] = 0ull;
 }

@@ -164,6 +164,26 @@ class GbResult(C.Structure):
                     min_years=[self.rows[i].min_year for i in range(n)])
 
 
+BATCH_SCAN_AGG, BATCH_JOIN, BATCH_GROUPBY = 0, 1, 2
+BATCH_MAX_CATS = 64
+
+
+class BatchInstance(C.Structure):
+    """``bo_batch_instance``: one pipeline of a batch (fields per kind)."""
+    _fields_ = [("kind", C.c_int32), ("tile_rows", C.c_int32), ("predicted", C.c_float),
+                ("presize_factor", C.c_float), ("fact", FactCols), ("ship_cutoff", C.c_int32),
+                ("n_flag_a", C.c_int32), ("n_flag_b", C.c_int32), ("pad0", C.c_int32),
+                ("build", JoinBuildCols), ("probe", JoinProbeCols), ("join", JoinParams),
+                ("a", GbACols), ("b", GbBCols), ("c", GbCCols), ("categories", C.c_uint16 * BATCH_MAX_CATS),
+                ("n_categories", C.c_int32), ("year_lo", C.c_int32), ("year_hi", C.c_int32), ("k", C.c_int32),
+                ("a_id_max", C.c_int32), ("pad1", C.c_int32)]
+
+
+class BatchResult(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("overflowed", C.c_int32), ("reruns", C.c_int32), ("pad", C.c_int32),
+                ("q1", Q1Agg * Q1_MAX_GROUPS), ("join", JoinResult), ("groupby", GbResult)]
+
+
 SKETCH_BINS = 64
 
 
@@ -230,6 +250,15 @@ _SIGNATURES = {
     "bo_mlp_train_host": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, C.c_float, C.POINTER(C.c_float)]),
     "bo_mlp_infer_device": (C.c_int, [_P, _P, _P, C.c_int32, _P]),
     "bo_mlp_predict_counts": (C.c_int, [_P, _P, _P, _P, _P]),
+    "bo_batch_create": (C.c_int, [_P, C.POINTER(BatchInstance), C.c_int32, C.c_int32, C.POINTER(_P)]),
+    "bo_batch_create_pool": (C.c_int, [_P, C.c_int32, C.c_int64, C.c_int64, C.c_int32, C.POINTER(_P)]),
+    "bo_batch_update": (C.c_int, [_P, _P, C.POINTER(BatchInstance), C.c_int32]),
+    "bo_batch_footprint": (C.c_int, [C.POINTER(BatchInstance), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "bo_batch_launch": (C.c_int, [_P, _P]),
+    "bo_batch_results": (C.c_int, [_P, _P, C.POINTER(BatchResult)]),
+    "bo_batch_last_ms": (C.c_float, [_P]),
+    "bo_batch_num_items": (C.c_int32, [_P]),
+    "bo_batch_destroy": (None, [_P]),
     "bo_join_probe_device": (C.c_int, [_P, C.POINTER(JoinProbeCols), _P]),
     "bo_join_host": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
                                C.c_int32, C.c_float, C.POINTER(JoinResult)]),

@@ -343,6 +343,78 @@ int bo_radix_sort_pairs_device(bo_ctx* ctx, uint64_t* keys, uint32_t* vals, int6
 int bo_radix_sort_pairs_host(bo_ctx* ctx, uint64_t* keys, uint32_t* vals, int64_t n, int32_t begin_bit,
                              int32_t end_bit);
 
+/* ================================================================= BATCH ==
+ * Many pipelines of uneven sizes in ONE persistent kernel fed by a device work
+ * queue of (instance, stage, tile) items, captured in a CUDA graph.  Stages of
+ * one instance are ordered by per-instance completion counters (bounded waits);
+ * work of different instances overlaps.  Tables are sized from each instance's
+ * predicted count (e.g. an MLP prediction); an instance whose table overflowed
+ * is rerun alone in the exact form when its results are read, so every result
+ * equals the solo run.  No reference counterpart (the reference runs one query
+ * at a time, bespoke_tpch/query_impl.cpp:159-388). */
+#define BO_BATCH_SCAN_AGG 0
+#define BO_BATCH_JOIN 1
+#define BO_BATCH_GROUPBY 2
+#define BO_BATCH_MAX_CATS 64
+
+typedef struct bo_batch_instance {
+  int32_t kind;            /* BO_BATCH_* */
+  int32_t tile_rows;       /* rows per work item; 0 = library default */
+  float predicted;         /* join: qualifying build rows; group-by: groups; <= 0 sizes for the upper bound */
+  float presize_factor;    /* slots per predicted row; 0 = 2.5 */
+  /* scan-agg (wide layout) */
+  bo_fact_cols fact;
+  int32_t ship_cutoff, n_flag_a, n_flag_b, pad0;
+  /* join */
+  bo_join_build_cols build;
+  bo_join_probe_cols probe;
+  bo_join_params join;
+  /* group-by */
+  bo_gb_a_cols a;
+  bo_gb_b_cols b;
+  bo_gb_c_cols c;
+  uint16_t categories[BO_BATCH_MAX_CATS];
+  int32_t n_categories, year_lo, year_hi, k, a_id_max, pad1;
+} bo_batch_instance;
+
+typedef struct bo_batch_result {
+  int32_t kind;
+  int32_t overflowed;   /* the batch's presized table overflowed (the result below is the exact rerun) */
+  int32_t reruns;
+  int32_t pad;
+  bo_q1_agg q1[BO_Q1_MAX_GROUPS];
+  bo_join_result join;
+  bo_gb_result groupby;
+} bo_batch_result;
+
+typedef struct bo_batch bo_batch;
+
+/* Plans a batch sized exactly for these instances: validates them, allocates
+ * their tables, builds the work queue (level-major, larger instances first
+ * inside a level) and captures the launch (queue reset + the persistent
+ * kernel) into a CUDA graph.  workers_per_sm = 0 uses the library default. */
+int bo_batch_create(bo_ctx* ctx, const bo_batch_instance* instances, int32_t n, int32_t workers_per_sm,
+                    bo_batch** out);
+/* An empty batch with room for max_instances instances, max_items work items
+ * and pool_bytes of tables; fill it with bo_batch_update. */
+int bo_batch_create_pool(bo_ctx* ctx, int32_t max_instances, int64_t max_items, int64_t pool_bytes,
+                         int32_t workers_per_sm, bo_batch** out);
+/* Re-plans the batch with a new set of instances inside its pool (BO_ERR_OVERFLOW
+ * if their tables or items do not fit): one asynchronous copy on the
+ * context's stream, no re-capture.  Read the previous launch's results first. */
+int bo_batch_update(bo_ctx* ctx, bo_batch* batch, const bo_batch_instance* instances, int32_t n);
+/* Table bytes and work items one instance needs (admission by footprint). */
+int bo_batch_footprint(const bo_batch_instance* instance, int64_t* table_bytes, int64_t* items);
+/* Launches the captured graph on the context's stream (asynchronous). */
+int bo_batch_launch(bo_ctx* ctx, bo_batch* batch);
+/* Waits, copies every instance's result to the host and reruns any instance
+ * whose presized table overflowed alone in the exact form. */
+int bo_batch_results(bo_ctx* ctx, bo_batch* batch, bo_batch_result* out_host);
+/* Device time (ms) of the last launch, from events around the graph. */
+float bo_batch_last_ms(const bo_batch* batch);
+int32_t bo_batch_num_items(const bo_batch* batch);
+void bo_batch_destroy(bo_batch* batch);
+
 /* ================================================================ SKETCH ==
  * Per-column sketches for the learned sizing features, computed on the device
  * once per table.  No reference counterpart. */
