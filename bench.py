@@ -187,8 +187,10 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
+    torch.cuda.nvtx.range_push("timed")  # lets a profiler select exactly the timed launches
     for i in range(K):
         learned_step(i, W + i)
+    torch.cuda.nvtx.range_pop()
     ev1.record(stream)
     torch.cuda.synchronize()
     launches = eng.launches - launches0
@@ -303,6 +305,25 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
 
     q_err = [float(L.q_error(sizer.predict_host(f[None, :]), [e])[0]) for f, e in zip(feats, exact_rows)]
 
+    # ---- the other configurations (rank 0; extra keys of the same line)
+    extra = {}
+    if rank == 0 and args.sections != "none":
+        wanted = ["scan_agg", "groupby", "batch"] if args.sections == "all" else args.sections.split(",")
+        peak_gbs, _ = peaks()
+        for name in wanted:
+            t_sec = time.perf_counter()
+            try:
+                if name == "scan_agg":
+                    extra[name] = scan_agg_section(eng, stream, peak_gbs)
+                elif name == "groupby":
+                    extra[name] = groupby_section(eng, stream)
+                elif name == "batch":
+                    extra[name] = batch_section(eng, stream, K, sizer)
+            except Exception as e:  # report, never lose the headline line
+                extra[name] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
+            if name in extra:
+                extra[name]["section_s"] = round(time.perf_counter() - t_sec, 1)
+
     out = None
     if rank == 0:
         value = world * K * ROWS_PER_STEP / (ms * 1e-3)
@@ -338,12 +359,214 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
                                  "speedup": lat_plain / lat_learned, "q_error": q_err, "reruns": reruns,
                                  "note": "per-query latency, result on the host each query"},
             "clocks": clocks,
+            "configs": extra,
         }
         try:
             out["cpu_baseline"] = cpu_baseline(copies[0]["j"])
         except Exception as e:  # the reference harness is a prebuilt file; report, never fail the bench
             out["cpu_baseline"] = {"value": None, "unit": "rows/s", "error": str(e)[:200]}
     eng.close()
+    return out
+
+
+# ------------------------------------------------------ other configs ------
+def _median_wall_ms(fn, n: int) -> float:
+    import torch
+
+    ts = []
+    for i in range(n):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn(i)
+        ts.append((time.perf_counter() - t0) * 1e3)
+    return statistics.median(ts)
+
+
+def scan_agg_section(eng, stream, peak: float) -> dict:
+    """Scan-filter-group-aggregate (wide fact layout, 38 B/row): 6M rows (two
+    copies alternated, 2 x 228 MB > L2) and a 60M-row table; device time per
+    launch from CUDA events on the launching stream."""
+    import torch
+
+    from bespokeolap_artifacts_b200 import batching as B
+    from bespokeolap_artifacts_b200 import native as N
+    from bespokeolap_artifacts_b200.datagen import Q1_CUTOFF
+
+    out = torch.zeros(8 * C.sizeof(N.Q1Agg), dtype=torch.uint8, device="cuda")
+    res = {}
+    for n, copies in ((6_000_000, 2), (60_000_000, 1)):
+        insts = [B.fact_instance(n, seed=70 + c, cutoff=Q1_CUTOFF) for c in range(copies)]
+        cols = [[i.cols[k] for k in ("ship_date", "quantity", "ext_price", "discount", "tax", "flag_a", "flag_b")]
+                for i in insts]
+        for r in range(3):
+            eng.q1_fact_device(cols[r % copies], n, Q1_CUTOFF, 3, 2, out)
+        torch.cuda.synchronize()
+        evs = []
+        for r in range(20):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            eng.q1_fact_device(cols[r % copies], n, Q1_CUTOFF, 3, 2, out)
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        us = statistics.median(a.elapsed_time(b) for a, b in evs) * 1e3
+        gbs = n * 38 / (us * 1e-6) / 1e9
+        res[f"rows_{n}"] = {"us_per_launch": us, "rows_per_s": n / (us * 1e-6), "achieved_gbs": gbs,
+                            "frac_of_measured_hbm": gbs / peak, "kernel": "q1_fact_kernel",
+                            "algorithmic_bytes_per_launch": n * 38}
+        del insts, cols
+    torch.cuda.empty_cache()
+    return res
+
+
+def groupby_section(eng, stream, n_queries: int = 10) -> dict:
+    """Skewed three-way join + group-by + top-k at full size (A 2.5M, B 36M, C
+    4M): per-query latency (result on the host) of the plain exact-count form,
+    the learned-presized multi-kernel form and the learned-presized form as one
+    graph launch of the persistent kernel (MLP output read on the device)."""
+    import torch
+
+    from bespokeolap_artifacts_b200 import batching as B
+    from bespokeolap_artifacts_b200 import learned as L
+    from bespokeolap_artifacts_b200 import native as N
+
+    t_setup = time.perf_counter()
+    base = B.groupby_instance(36_000_000, seed=2)
+    c = base.cols
+    n_a, n_b, n_c = int(c["a_ids"].numel()), int(c["b_a"].numel()), int(c["c_cat"].numel())
+    st = L.groupby_table_stats(eng.ctx, c, n_a, n_b, n_c)
+    x, t, _ = L.make_groupby_training_set(eng, n_tables=12, preds_per_table=30, seed=3, nb_max=2_000_000)
+    sizer = L.GroupBySizer(eng, seed=2)
+    sizer.fit(x, t, epochs=3000, lr=2e-3)
+    rng = np.random.default_rng(11)
+    queries = [sorted(int(v) for v in rng.choice(113, size=8, replace=False)) for _ in range(3)]
+    insts = []
+    for cats in queries:
+        q = B.Instance(N.BATCH_GROUPBY, n_b, c, dict(base.params, cat_set=cats, year_lo=1990, year_hi=2010))
+        insts.append(q)
+    feats = [L.groupby_features(st, q.params["cat_set"], 1990, 2010) for q in insts]
+    pred = torch.zeros(2, dtype=torch.float32, device="cuda")
+    args = [eng.gb_args(c["a_ids"], c["b_a"], c["b_c"], c["c_cat"], c["c_year"], n_a, n_b, n_c,
+                        q.params["cat_set"], 1990, 2010, 10, q.params["a_id_max"]) for q in insts]
+
+    def plain(i):
+        a, b, cc, prm, _ = args[i % 3]
+        out = N.GbResult()
+        eng.ctx.call("bo_groupby_topk_plain", C.byref(a), C.byref(b), C.byref(cc), C.byref(prm), C.byref(out))
+        return out.as_dict()
+
+    def learned_kernels(i):
+        a, b, cc, prm, _ = args[i % 3]
+        sizer.predict_device(feats[i % 3], pred)
+        out = N.GbResult()
+        eng.ctx.call("bo_groupby_topk_presized", C.byref(a), C.byref(b), C.byref(cc), C.byref(prm),
+                     C.c_void_p(pred.data_ptr()), C.byref(out))
+        return out.as_dict()
+
+    for q in insts:
+        q.predicted_device = pred[0:1]
+    tb = max(B.footprint(q)[0] for q in insts)
+    it = max(B.footprint(q)[1] for q in insts)
+    batch = B.Batch.pool(eng, 1, it, tb)
+
+    def learned_graph(i):
+        sizer.predict_device(feats[i % 3], pred)
+        batch.update([insts[i % 3]])
+        batch.launch()
+        return batch.results()[0]
+
+    exact = [plain(i) for i in range(3)]
+    same = True
+    for fn in (learned_kernels, learned_graph):
+        for i in range(3):
+            r = fn(i)
+            same &= all(r[f] == exact[i][f] for f in B.ANSWER_FIELDS["groupby"])
+    setup_s = time.perf_counter() - t_setup
+    n = max(n_queries, 6)
+    ms_plain = _median_wall_ms(plain, n)
+    ms_kern = _median_wall_ms(learned_kernels, n)
+    ms_graph = _median_wall_ms(learned_graph, n)
+    pg = [float(sizer.predict_host(f[None, :])[0, 0]) for f in feats]
+    batch.close()
+    return {
+        "workload": "A 2,500,000 ids; B 36,000,000 (a_id Zipf 1.1, c_id Zipf 0.9); C 4,000,000 (category 0..112, "
+                    "year 1900..2020); category in a seeded 8-value set, year in [1990, 2010]; group by a_id, "
+                    "count + min(year), order by count desc, a_id asc, limit 10",
+        "groups": [e["n_groups"] for e in exact],
+        "plain_ms_per_query": ms_plain,
+        "learned_multikernel_ms_per_query": ms_kern,
+        "learned_graph_ms_per_query": ms_graph,
+        "speedup_learned_graph_vs_plain": ms_plain / ms_graph,
+        "speedup_learned_multikernel_vs_plain": ms_plain / ms_kern,
+        "q_error_groups": [float(L.q_error([p], [e["n_groups"]])[0]) for p, e in zip(pg, exact)],
+        "answers_identical": bool(same),
+        "note": "host-visible latency per query; same 3 queries rotated; setup (data, sketches, MLP training) "
+                f"{setup_s:.1f} s outside the timing",
+    }
+
+
+def batch_section(eng, stream, K: int, join_sizer=None) -> dict:
+    """64 instances of the three pipeline shapes, rows log-uniform in [1e4,
+    6e7] (seeded), predicate constants redrawn, tile sizes from the shipped
+    autotuner table: one graph launch of the persistent kernel against
+    one-pipeline-per-launch plain execution of the same instances."""
+    import torch
+
+    from bespokeolap_artifacts_b200 import batching as B
+    from bespokeolap_artifacts_b200 import learned as L
+    from bespokeolap_artifacts_b200 import native as N
+
+    insts = B.mixed_workload(64, 1e4, 6e7, seed=2024)
+    table = B.load_tile_table()
+    table.apply(insts)
+    if join_sizer is not None:  # learned presizing of the join tables
+        for q in insts:
+            if q.kind == N.BATCH_JOIN:
+                c = q.cols
+                st = L.join_table_stats(eng.ctx, c["b_key"], c["b_date"], c["b_seg"], int(c["b_key"].numel()))
+                f = L.join_features(st, q.params["date_lt"], q.params["seg_eq"])
+                q.predicted = float(join_sizer.predict_host(f[None, :])[0])
+    total_bytes = sum(q.algorithmic_bytes() for q in insts)
+    total_rows = sum(sum(t.numel() for t in q.cols.values()) // len(q.cols) for q in insts)
+    b = B.Batch(eng, insts, table.workers_per_sm)
+    res = b.run()
+    solo = [B.solo_result(eng, q) for q in insts]  # warms the solo paths too
+    exact = sum(B.same_answer(r, s) for r, s in zip(res, solo))
+    reruns = sum(r.get("reruns", 0) for r in res)
+    dev_ms = []
+    for _ in range(max(K, 3)):
+        b.launch()
+        eng.synchronize()
+        dev_ms.append(b.last_ms())
+    wall_batch = _median_wall_ms(lambda i: b.run(), 3)
+    # One pipeline per launch: each instance alone, plain exact-count form.
+    fin = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for q in insts:
+        B.solo_result(eng, q)
+        fin.append((time.perf_counter() - t0) * 1e3)
+    seq_ms = fin[-1]
+    n_items = b.num_items
+    b.close()
+    bm = statistics.median(dev_ms)
+    out = {
+        "instances": len(insts), "work_items": n_items,
+        "kinds": {B.KINDS[k]: sum(q.kind == k for q in insts) for k in B.KINDS},
+        "rows_total": int(total_rows), "algorithmic_bytes": int(total_bytes),
+        "batch_device_ms": bm, "batch_wall_ms": wall_batch,
+        "batch_gbs": total_bytes / (bm * 1e-3) / 1e9,
+        "one_pipeline_per_launch_ms": seq_ms,
+        "speedup_vs_one_per_launch": seq_ms / wall_batch,
+        "latency_ms": {"batch_p50": wall_batch, "batch_p99": wall_batch,
+                       "one_per_launch_p50": float(np.percentile(fin, 50)),
+                       "one_per_launch_p99": float(np.percentile(fin, 99))},
+        "bit_exact_vs_solo": f"{exact}/{len(insts)}", "reruns": int(reruns),
+        "tile_table": "bespokeolap_artifacts_b200/tile_table.json" if B.TILE_TABLE_PATH.exists() else "defaults",
+        "workers_per_sm": table.workers_per_sm,
+    }
+    del insts, res, solo
+    torch.cuda.empty_cache()
     return out
 
 
@@ -430,6 +653,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--sections", default="all",
+                    help="other configurations reported beside the headline: all, none, or a comma list of "
+                         "scan_agg,groupby,batch")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))

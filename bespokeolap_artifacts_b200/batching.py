@@ -36,6 +36,7 @@ class Instance:
     params: dict
     predicted: float = 0.0         # presizing prediction (<= 0: size for the upper bound)
     tile_rows: int = 0
+    predicted_device: object = None  # device float tensor read at launch (overrides predicted)
     keep: list = field(default_factory=list)
 
     def to_c(self) -> N.BatchInstance:
@@ -44,6 +45,7 @@ class Instance:
         x.tile_rows = int(self.tile_rows)
         x.predicted = float(self.predicted)
         x.presize_factor = 0.0
+        x.predicted_device = N.ptr(self.predicted_device) if self.predicted_device is not None else None
         p, c = self.params, self.cols
         if self.kind == N.BATCH_SCAN_AGG:
             x.fact = N.FactCols(*[N.ptr(c[k]) for k in ("ship_date", "quantity", "ext_price", "discount", "tax",
@@ -414,3 +416,40 @@ def autotune(engine, instances: list[Instance], candidates=TILE_CANDIDATES, work
             best_w, best_ms = w, ms
     table.workers_per_sm = best_w
     return table
+
+
+# ------------------------------------------------------------------ CLI ----
+TILE_TABLE_PATH = Path(__file__).resolve().parent / "tile_table.json"
+
+
+def load_tile_table() -> TileTable:
+    """The autotuned table shipped with the package (defaults if absent)."""
+    return TileTable.load(TILE_TABLE_PATH) if TILE_TABLE_PATH.exists() else TileTable()
+
+
+def main(argv=None) -> None:
+    """``python -m bespokeolap_artifacts_b200.batching --autotune OUT.json``:
+    tunes the tile table on the 64-instance mixed workload (seeded) on cuda:0."""
+    import argparse
+
+    import torch
+
+    from .engine import Engine
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--autotune", required=True, help="output JSON path")
+    ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args(argv)
+    torch.cuda.set_device(0)
+    eng = Engine(0)
+    insts = mixed_workload(a.instances, seed=a.seed)
+    table = autotune(eng, insts, reps=a.reps)
+    table.save(Path(a.autotune))
+    print(table.to_json())
+    eng.close()
+
+
+if __name__ == "__main__":
+    main()

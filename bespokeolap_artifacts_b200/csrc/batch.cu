@@ -85,7 +85,9 @@ constexpr int kGbLocalProbesB = 2;
 
 struct InstDesc {
   int32_t kind;
-  int32_t cap_log2;
+  int32_t cap_log2;          // table capacity (the upper bound when pred_dev is set)
+  const float* pred_dev;     // optional device prediction read at launch time
+  float factor;              // slots per predicted row
   uint32_t level_items[kLevels];
   int64_t tile[kNumStages];      // rows / slots / words per tile
   uint32_t n_tiles[kNumStages];
@@ -415,9 +417,23 @@ __device__ __forceinline__ void split_range(int64_t total, uint32_t t, uint32_t 
   hi = (int64_t)((__int128)total * (t + 1) / n);
 }
 
+// Capacity of this launch: planned on the host, or derived on the device from
+// a prediction in device memory by the solo presized forms' rule (smallest
+// power of two >= factor * prediction, at least 2^10, at most the planned
+// upper bound).  Every tile computes the same value from the same float.
+__device__ __forceinline__ int32_t cap_log2_of(const InstDesc& d) {
+  if (!d.pred_dev) return d.cap_log2;
+  float p = __ldcg(d.pred_dev);
+  if (!(p >= 0.0f)) p = 0.0f;
+  const double want = (double)p * d.factor;
+  int32_t cl = 10;
+  while (cl < d.cap_log2 && (double)(1ull << cl) < want) ++cl;
+  return cl;
+}
+
 __device__ void stage_join_init(const InstDesc& d, uint32_t tile) {
   int64_t lo, hi;
-  split_range((int64_t)1 << d.cap_log2, tile, d.n_tiles[kSJInit], lo, hi);
+  split_range((int64_t)1 << cap_log2_of(d), tile, d.n_tiles[kSJInit], lo, hi);
   for (int64_t i = lo + threadIdx.x; i < hi; i += kBB) d.slots[i] = kEmptySlot;
   if (tile == 0) {
     uint4* b4 = reinterpret_cast<uint4*>(d.bloom);
@@ -430,7 +446,8 @@ __device__ void stage_join_build(const InstDesc& d, InstState* st, uint32_t tile
   const bo_join_build_cols& b = d.build;
   const int64_t lo = (int64_t)tile * d.tile[kSJBuild];
   const int64_t hi = min(b.n_rows, lo + d.tile[kSJBuild]);
-  const uint64_t mask = (1ull << d.cap_log2) - 1;
+  const int32_t cl = cap_log2_of(d);
+  const uint64_t mask = (1ull << cl) - 1;
   const int lane = threadIdx.x & 31;
   uint32_t* bq = reinterpret_cast<uint32_t*>(sm.b) + (threadIdx.x >> 5) * 256;
   uint32_t qual = 0, newkeys = 0;
@@ -489,7 +506,8 @@ __device__ void stage_join_probe(const InstDesc& d, InstState* st, uint32_t tile
   const bo_join_probe_cols& p = d.probe;
   const int64_t lo = (int64_t)tile * d.tile[kSJProbe];
   const int64_t hi = min(p.n_rows, lo + d.tile[kSJProbe]);
-  const uint64_t mask = (1ull << d.cap_log2) - 1;
+  const int32_t cl = cap_log2_of(d);
+  const uint64_t mask = (1ull << cl) - 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int32_t* qf = reinterpret_cast<int32_t*>(sm.b) + warp * 256;
   uint16_t* qo = reinterpret_cast<uint16_t*>(sm.b + kBW * 256 * 4) + warp * 256;
@@ -573,7 +591,7 @@ __device__ void stage_join_probe(const InstDesc& d, InstState* st, uint32_t tile
     r.match_count = narrow_i64(m, fbad);
     r.sum_trunc = to_bo_i128(t);
     r.sum_exact = to_bo_i128(t * 100 + rr);
-    r.capacity_log2 = d.cap_log2;
+    r.capacity_log2 = cl;
     r.overflowed = (int32_t)__ldcg(&st->overflow);
     r.reruns = 0;
     r.mode = 1;
@@ -588,7 +606,7 @@ __device__ void stage_join_probe(const InstDesc& d, InstState* st, uint32_t tile
 __device__ void stage_gb_init(const InstDesc& d, uint32_t tile) {
   const uint32_t nt = d.n_tiles[kSGInit];
   int64_t lo, hi;
-  split_range((int64_t)1 << d.cap_log2, tile, nt, lo, hi);
+  split_range((int64_t)1 << cap_log2_of(d), tile, nt, lo, hi);
   for (int64_t i = lo + threadIdx.x; i < hi; i += kBB) {
     d.slots[i] = kEmptySlot;
     d.mins[i] = 0x7fffffff;
@@ -691,7 +709,8 @@ __device__ void stage_gb_scan(const InstDesc& d, InstState* st, uint32_t tile, c
   const uint32_t* amask = d.amask;
   unsigned long long* slots = d.slots;
   int32_t* mins = d.mins;
-  const uint64_t mask = (1ull << d.cap_log2) - 1;
+  const int32_t cl = cap_log2_of(d);
+  const uint64_t mask = (1ull << cl) - 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int32_t* qc = q_c + warp * kGbQueueB;
   uint32_t* qr = q_row + warp * kGbQueueB;
@@ -843,7 +862,8 @@ __device__ void stage_gb_select(const InstDesc& d, InstState* st, uint32_t tile,
   const int wa = d.wa;
   const unsigned long long cmax = d.cmax;
   int64_t lo, hi;
-  split_range((int64_t)1 << d.cap_log2, tile, d.n_tiles[kSGSelect], lo, hi);
+  const int32_t cl = cap_log2_of(d);
+  split_range((int64_t)1 << cl, tile, d.n_tiles[kSGSelect], lo, hi);
   sel_reset(sb);
   uint32_t occ = 0;
   for (int64_t base = lo; base < hi; base += kSelChunk) {
@@ -918,7 +938,7 @@ __device__ void stage_gb_select(const InstDesc& d, InstState* st, uint32_t tile,
     g.joined_rows = (int64_t)__ldcg(&st->cnt[0]);
     g.c_qualifying = (int64_t)__ldcg(&st->cnt[2]);
     g.exact_distinct = 0;
-    g.capacity_log2 = d.cap_log2;
+    g.capacity_log2 = cl;
     g.overflowed = (int32_t)__ldcg(&st->overflow);
     g.reruns = 0;
     g.mode = 1;
@@ -1213,8 +1233,10 @@ Plan plan_instance(const bo_batch_instance& x) {
   std::memset(&p.d, 0, sizeof(p.d));
   InstDesc& d = p.d;
   d.kind = x.kind;
+  d.pred_dev = x.kind == BO_BATCH_SCAN_AGG ? nullptr : x.predicted_device;
   const int64_t t = x.tile_rows > 0 ? ((int64_t)x.tile_rows + 4095) / 4096 * 4096 : 131072;
   const float factor = x.presize_factor > 0.0f ? x.presize_factor : 2.5f;
+  d.factor = factor;
   p.table_bytes = 0;
   p.weight = 0.0;
   for (int s = 0; s < kNumStages; ++s) d.tile[s] = 1;
@@ -1232,7 +1254,7 @@ Plan plan_instance(const bo_batch_instance& x) {
     d.date_lt = x.join.date_lt;
     d.seg = (uint32_t)x.join.segment_eq;
     const int32_t max_log2 = std::max(10, ceil_log2_u64((uint64_t)std::max<int64_t>(x.build.n_rows, 1) * 2));
-    d.cap_log2 = presize(x.predicted, factor, max_log2);
+    d.cap_log2 = x.predicted_device ? max_log2 : presize(x.predicted, factor, max_log2);
     const int64_t cap = (int64_t)1 << d.cap_log2;
     d.tile[kSJInit] = kInitSlotsPerTile;
     d.n_tiles[kSJInit] = (uint32_t)std::max<int64_t>(1, ceil_div(cap, kInitSlotsPerTile));
@@ -1258,7 +1280,7 @@ Plan plan_instance(const bo_batch_instance& x) {
     const uint64_t groups_max =
         std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)x.a_id_max + 1, (uint64_t)x.b.n_rows));
     const int32_t max_log2 = std::max(10, bit_len(groups_max * 2 - 1));
-    d.cap_log2 = presize(x.predicted, factor, max_log2);
+    d.cap_log2 = x.predicted_device ? max_log2 : presize(x.predicted, factor, max_log2);
     const int64_t cap = (int64_t)1 << d.cap_log2;
     d.mask_words = ((int64_t)x.a_id_max + 1 + 31) / 32;
     d.c_words = (x.c.n_rows + 31) / 32;

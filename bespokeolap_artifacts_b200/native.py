@@ -176,7 +176,7 @@ class BatchInstance(C.Structure):
                 ("build", JoinBuildCols), ("probe", JoinProbeCols), ("join", JoinParams),
                 ("a", GbACols), ("b", GbBCols), ("c", GbCCols), ("categories", C.c_uint16 * BATCH_MAX_CATS),
                 ("n_categories", C.c_int32), ("year_lo", C.c_int32), ("year_hi", C.c_int32), ("k", C.c_int32),
-                ("a_id_max", C.c_int32), ("pad1", C.c_int32)]
+                ("a_id_max", C.c_int32), ("pad1", C.c_int32), ("predicted_device", C.c_void_p)]
 
 
 class BatchResult(C.Structure):

@@ -375,6 +375,11 @@ typedef struct bo_batch_instance {
   bo_gb_c_cols c;
   uint16_t categories[BO_BATCH_MAX_CATS];
   int32_t n_categories, year_lo, year_hi, k, a_id_max, pad1;
+  /* join / group-by, optional: device float read when the batch runs (e.g. an
+   * MLP prediction left on the device); overrides `predicted`.  The pool then
+   * holds tables of the upper-bound size and the launch uses the capacity the
+   * device value gives. */
+  const float* predicted_device;
 } bo_batch_instance;
 
 typedef struct bo_batch_result {

@@ -127,3 +127,31 @@ def test_batch_pool_replans_in_place(engine, torch_cuda):
     b.update(sets[1])
     check_against_solo(engine, sets[1], b.run())
     b.close()
+
+
+def test_batch_device_prediction(engine, torch_cuda):
+    """Capacity taken from a device float at launch time (an MLP output left on
+    the device): same capacity as the solo presized form, same answer; the
+    same graph re-run with a too-low value overflows and is rerun exactly."""
+    torch = torch_cuda
+    g = B.groupby_instance(300_000, 41)
+    g.params.update({"year_lo": 1900, "year_hi": 2020})
+    j = B.join_instance(200_000, 42)
+    exact_g, exact_j = B.solo_result(engine, g), B.solo_result(engine, j)
+    pred = torch.tensor([float(exact_g["n_groups"]), float(exact_j["build_rows"])], dtype=torch.float32,
+                        device="cuda")
+    g.predicted_device, j.predicted_device = pred[0:1], pred[1:2]
+    g.predicted, j.predicted = float(exact_g["n_groups"]), float(exact_j["build_rows"])
+    torch.cuda.synchronize()  # the engine's stream reads what torch's stream wrote
+    b = B.Batch(engine, [g, j])
+    res = b.run()
+    check_against_solo(engine, [g, j], res)
+    solo_g, solo_j = B.solo_result(engine, g, presized=True), B.solo_result(engine, j, presized=True)
+    assert res[0]["capacity_log2"] == solo_g["capacity_log2"] and res[0]["reruns"] == 0
+    assert res[1]["capacity_log2"] == solo_j["capacity_log2"] and res[1]["reruns"] == 0
+    pred.fill_(1.0)
+    torch.cuda.synchronize()
+    res = b.run()
+    check_against_solo(engine, [g, j], res)
+    assert res[0]["reruns"] == 1 and res[1]["reruns"] == 1
+    b.close()
