@@ -141,9 +141,13 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
         copies.append(dict(j=j, b=b, p=p, st=st))
 
     # Learned sizer: trained on the GPU from plain-pipeline counts (seeded tables).
-    x, t, _ = L.make_join_training_set(eng, n_tables=24, preds_per_table=40, seed=4242, n_max=2_000_000)
+    # Seeded build sides of 20K..2M rows; 80% to train, 20% to calibrate the
+    # sizing margin.
+    x, t, _ = L.make_join_training_set(eng, n_tables=30, preds_per_table=40, seed=4242, n_max=2_000_000)
+    tr, ho = L.split_holdout(len(x), 0.2, seed=1)
     sizer = L.JoinSizer(eng, seed=5)
-    sizer.fit(x, t, epochs=3000, lr=2e-3)
+    sizer.fit(x[tr], t[tr], epochs=3000, lr=2e-3)
+    sizer.calibrate(x[ho], t[ho], quantile=0.9)
     feats = [L.join_features(c["st"], c["j"].date_lt, c["j"].seg_eq) for c in copies]
     exact_rows = []
     cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
@@ -246,6 +250,78 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     lat_learned = per_query(learned_query, max(K, 10))
     lat_plain = per_query(plain_query, max(K, 10))
 
+    # ---- CUDA-graph forms.  The learned query has no host round trip, so the
+    # whole query (MLP prediction + init + build + probe) replays as one graph.
+    # The plain query keeps its exact-count round trip, then replays the same
+    # presized pipeline as a graph with the table sized from the exact count.
+    res_pin = C.c_void_p()
+    eng.ctx.call("bo_host_alloc_pinned", C.c_size_t(res_sz + 64), C.byref(res_pin))
+    cnt_host = C.c_int64()
+    g_learned, g_sized, g_pred, g_out = [], [], [], []
+    for i in range(3):
+        c = copies[i]
+        j = c["j"]
+        pl = torch.zeros(2, dtype=torch.float32, device="cuda")
+        ob = torch.zeros(res_sz, dtype=torch.uint8, device="cuda")
+
+        def lseq(c=c, j=j, pl=pl, ob=ob, i=i):
+            sizer.predict_device(feats[i], pl[0:1])
+            eng.join_presized_device(c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq, pl[0:1], ob)
+
+        def sseq(c=c, j=j, pl=pl, ob=ob):
+            eng.join_presized_device(c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq, pl[1:2], ob)
+
+        pl[1] = float(exact_rows[i]) * 0.8
+        for fn in (lseq, sseq):
+            fn()
+            torch.cuda.synchronize()
+        gl, gs = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gl, stream=stream):
+            lseq()
+        with torch.cuda.graph(gs, stream=stream):
+            sseq()
+        g_learned.append(gl)
+        g_sized.append(gs)
+        g_pred.append(pl)
+        g_out.append(ob)
+
+    def read_result(i):
+        eng.ctx.call("bo_copy_d2h", res_pin, C.c_void_p(g_out[i].data_ptr()), C.c_size_t(res_sz))
+        return N.JoinResult.from_address(res_pin.value)
+
+    def learned_graph_query(i):
+        k = i % 3
+        g_learned[k].replay()
+        r = read_result(k)
+        if r.overflowed:
+            c = copies[k]
+            return eng.join_plain(c["b"], c["p"], N_BUILD, N_PROBE, c["j"].date_lt, c["j"].seg_eq)
+        return r.as_dict()
+
+    pred_pin = C.c_void_p()
+    eng.ctx.call("bo_host_alloc_pinned", C.c_size_t(64), C.byref(pred_pin))
+
+    def plain_graph_query(i):
+        k = i % 3
+        c = copies[k]
+        eng.join_count_device(c["b"], N_BUILD, c["j"].date_lt, c["j"].seg_eq, cnt)
+        eng.ctx.call("bo_copy_d2h", C.byref(cnt_host), C.c_void_p(cnt.data_ptr()), C.c_size_t(8))
+        # exact sizing: 2 slots per qualifying row (the plain rule) = 2.5 x (0.8 x count)
+        C.c_float.from_address(pred_pin.value).value = 0.8 * cnt_host.value
+        eng.ctx.call("bo_copy_h2d", C.c_void_p(g_pred[k].data_ptr() + 4), pred_pin, C.c_size_t(4))
+        g_sized[k].replay()
+        return read_result(k).as_dict()
+
+    same_graph = True
+    for i in range(3):
+        a, b = learned_graph_query(i), plain_graph_query(i)
+        same_graph &= a["match_count"] == b["match_count"] and a["sum_exact"] == b["sum_exact"]
+    lat_learned_graph = per_query(learned_graph_query, max(K, 10))
+    lat_plain_graph = per_query(plain_graph_query, max(K, 10))
+    del g_learned, g_sized
+    eng.ctx.call("bo_host_free_pinned", res_pin)
+    eng.ctx.call("bo_host_free_pinned", pred_pin)
+
     # ---- roofline of the dominant kernel (probe), timed alone on the stream
     outp = torch.zeros(res_sz, dtype=torch.uint8, device="cuda")
     c0 = copies[(W + K - 1) % 3]
@@ -310,15 +386,16 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     if rank == 0 and args.sections != "none":
         wanted = ["scan_agg", "groupby", "batch"] if args.sections == "all" else args.sections.split(",")
         peak_gbs, _ = peaks()
+        keep = {}
         for name in wanted:
             t_sec = time.perf_counter()
             try:
                 if name == "scan_agg":
                     extra[name] = scan_agg_section(eng, stream, peak_gbs)
                 elif name == "groupby":
-                    extra[name] = groupby_section(eng, stream)
+                    extra[name] = groupby_section(eng, stream, keep=keep)
                 elif name == "batch":
-                    extra[name] = batch_section(eng, stream, K, sizer)
+                    extra[name] = batch_section(eng, stream, K, sizer, keep.get("gb_sizer"))
             except Exception as e:  # report, never lose the headline line
                 extra[name] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
             if name in extra:
@@ -355,8 +432,14 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst)", "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": PROBE_BYTES, "avg_launch_us": probe_ms * 1e3},
-            "learned_vs_plain": {"learned_ms_per_query": lat_learned, "plain_ms_per_query": lat_plain,
-                                 "speedup": lat_plain / lat_learned, "q_error": q_err, "reruns": reruns,
+            "learned_vs_plain": {"learned_ms_per_query": lat_learned_graph, "plain_ms_per_query": lat_plain_graph,
+                                 "speedup": lat_plain_graph / lat_learned_graph,
+                                 "form": "CUDA graphs: learned = one graph (MLP prediction + presized init/build/"
+                                         "probe); plain = count kernel + host round trip + the same presized "
+                                         "pipeline graph sized from the exact count",
+                                 "eager_learned_ms_per_query": lat_learned, "eager_plain_ms_per_query": lat_plain,
+                                 "eager_speedup": lat_plain / lat_learned, "answers_identical": bool(same_graph),
+                                 "q_error": q_err, "sizing_margin": sizer.margin, "reruns": reruns,
                                  "note": "per-query latency, result on the host each query"},
             "clocks": clocks,
             "configs": extra,
@@ -419,7 +502,7 @@ def scan_agg_section(eng, stream, peak: float) -> dict:
     return res
 
 
-def groupby_section(eng, stream, n_queries: int = 10) -> dict:
+def groupby_section(eng, stream, n_queries: int = 10, keep: dict | None = None) -> dict:
     """Skewed three-way join + group-by + top-k at full size (A 2.5M, B 36M, C
     4M): per-query latency (result on the host) of the plain exact-count form,
     the learned-presized multi-kernel form and the learned-presized form as one
@@ -435,9 +518,12 @@ def groupby_section(eng, stream, n_queries: int = 10) -> dict:
     c = base.cols
     n_a, n_b, n_c = int(c["a_ids"].numel()), int(c["b_a"].numel()), int(c["c_cat"].numel())
     st = L.groupby_table_stats(eng.ctx, c, n_a, n_b, n_c)
-    x, t, _ = L.make_groupby_training_set(eng, n_tables=12, preds_per_table=30, seed=3, nb_max=2_000_000)
+    x, t, _ = L.make_groupby_training_set(eng, n_tables=24, preds_per_table=30, seed=3, nb_min=100_000,
+                                          nb_max=60_000_000, device_gen=True)
+    tr, ho = L.split_holdout(len(x), 0.2, seed=1)
     sizer = L.GroupBySizer(eng, seed=2)
-    sizer.fit(x, t, epochs=3000, lr=2e-3)
+    sizer.fit(x[tr], t[tr], epochs=3000, lr=2e-3)
+    sizer.calibrate(x[ho], t[ho], quantile=0.9)
     rng = np.random.default_rng(11)
     queries = [sorted(int(v) for v in rng.choice(113, size=8, replace=False)) for _ in range(3)]
     insts = []
@@ -488,6 +574,8 @@ def groupby_section(eng, stream, n_queries: int = 10) -> dict:
     ms_graph = _median_wall_ms(learned_graph, n)
     pg = [float(sizer.predict_host(f[None, :])[0, 0]) for f in feats]
     batch.close()
+    if keep is not None:
+        keep["gb_sizer"] = sizer
     return {
         "workload": "A 2,500,000 ids; B 36,000,000 (a_id Zipf 1.1, c_id Zipf 0.9); C 4,000,000 (category 0..112, "
                     "year 1900..2020); category in a seeded 8-value set, year in [1990, 2010]; group by a_id, "
@@ -495,17 +583,18 @@ def groupby_section(eng, stream, n_queries: int = 10) -> dict:
         "groups": [e["n_groups"] for e in exact],
         "plain_ms_per_query": ms_plain,
         "learned_multikernel_ms_per_query": ms_kern,
-        "learned_graph_ms_per_query": ms_graph,
-        "speedup_learned_graph_vs_plain": ms_plain / ms_graph,
+        "learned_persistent_ms_per_query": ms_graph,
+        "speedup_learned_persistent_vs_plain": ms_plain / ms_graph,
         "speedup_learned_multikernel_vs_plain": ms_plain / ms_kern,
         "q_error_groups": [float(L.q_error([p], [e["n_groups"]])[0]) for p, e in zip(pg, exact)],
+        "sizing_margin": sizer.margin,
         "answers_identical": bool(same),
         "note": "host-visible latency per query; same 3 queries rotated; setup (data, sketches, MLP training) "
                 f"{setup_s:.1f} s outside the timing",
     }
 
 
-def batch_section(eng, stream, K: int, join_sizer=None) -> dict:
+def batch_section(eng, stream, K: int, join_sizer=None, gb_sizer=None) -> dict:
     """64 instances of the three pipeline shapes, rows log-uniform in [1e4,
     6e7] (seeded), predicate constants redrawn, tile sizes from the shipped
     autotuner table: one graph launch of the persistent kernel against
@@ -526,12 +615,26 @@ def batch_section(eng, stream, K: int, join_sizer=None) -> dict:
                 st = L.join_table_stats(eng.ctx, c["b_key"], c["b_date"], c["b_seg"], int(c["b_key"].numel()))
                 f = L.join_features(st, q.params["date_lt"], q.params["seg_eq"])
                 q.predicted = float(join_sizer.predict_host(f[None, :])[0])
+    if gb_sizer is not None:  # learned presizing of the group tables
+        for q in insts:
+            if q.kind == N.BATCH_GROUPBY:
+                c = q.cols
+                st = L.groupby_table_stats(eng.ctx, c, int(c["a_ids"].numel()), int(c["b_a"].numel()),
+                                           int(c["c_cat"].numel()))
+                f = L.groupby_features(st, q.params["cat_set"], q.params["year_lo"], q.params["year_hi"])
+                q.predicted = float(gb_sizer.predict_host(f[None, :])[0, 0])
     total_bytes = sum(q.algorithmic_bytes() for q in insts)
     total_rows = sum(sum(t.numel() for t in q.cols.values()) // len(q.cols) for q in insts)
     b = B.Batch(eng, insts, table.workers_per_sm)
     res = b.run()
     solo = [B.solo_result(eng, q) for q in insts]  # warms the solo paths too
     exact = sum(B.same_answer(r, s) for r, s in zip(res, solo))
+    ratio = {"join": [], "groupby": []}  # predicted / exact (calibrated predictions)
+    for q, s_ in zip(insts, solo):
+        if q.predicted > 0 and q.kind == N.BATCH_JOIN:
+            ratio["join"].append(q.predicted / max(s_["build_rows"], 1))
+        elif q.predicted > 0 and q.kind == N.BATCH_GROUPBY:
+            ratio["groupby"].append(q.predicted / max(s_["n_groups"], 1))
     reruns = sum(r.get("reruns", 0) for r in res)
     dev_ms = []
     for _ in range(max(K, 3)):
@@ -564,6 +667,10 @@ def batch_section(eng, stream, K: int, join_sizer=None) -> dict:
         "bit_exact_vs_solo": f"{exact}/{len(insts)}", "reruns": int(reruns),
         "tile_table": "bespokeolap_artifacts_b200/tile_table.json" if B.TILE_TABLE_PATH.exists() else "defaults",
         "workers_per_sm": table.workers_per_sm,
+        "presizing": {"join": "MLP" if join_sizer is not None else "upper bound",
+                      "groupby": "MLP" if gb_sizer is not None else "upper bound",
+                      "pred_over_exact": {k: {"min": min(v), "median": float(np.median(v)), "max": max(v),
+                                              "under": sum(x < 1 for x in v)} for k, v in ratio.items() if v}},
     }
     del insts, res, solo
     torch.cuda.empty_cache()

@@ -284,29 +284,36 @@ def _zipf_device(g, n: int, n_ranks: int, s: float):
     return torch.clamp(torch.searchsorted(cdf, u, right=True), max=n_ranks - 1)
 
 
+def groupby_tables_device(n_a: int, n_b: int, n_c: int, seed: int, s_a: float = 1.1, s_c: float = 0.9) -> dict:
+    """Device tables of the skewed three-way join: A ids 1..n_a shuffled, B
+    (a_id Zipf s_a over A, c_id Zipf s_c over C rows; ranks mapped to ids by
+    seeded permutations), C (category 0..112, year 1900..2020)."""
+    import torch
+
+    g = _gen(seed)
+    a_ids = (torch.randperm(n_a, generator=g, device="cuda") + 1).to(torch.int32)
+    rank_to_a = (torch.randperm(n_a, generator=g, device="cuda") + 1).to(torch.int32)
+    rank_to_c = torch.randperm(n_c, generator=g, device="cuda").to(torch.int32)
+    return {
+        "a_ids": a_ids,
+        "b_a": rank_to_a[_zipf_device(g, n_b, n_a, s_a)].contiguous(),
+        "b_c": rank_to_c[_zipf_device(g, n_b, n_c, s_c)].contiguous(),
+        "c_cat": _randint(g, 0, 112, n_c, torch.int16),  # uint16 values 0..112, same bits
+        "c_year": _randint(g, 1900, 2020, n_c, torch.int32),
+        "a_id_max": n_a,
+    }
+
+
 def groupby_instance(n_b: int, seed: int, k: int = 10) -> Instance:
     """Skewed three-way join + group-by + top-k instance: A, B, C in the
     2.5M : 36M : 4M proportions of the full workload scaled to n_b B rows,
     a_id Zipf s=1.1 over A, c_id Zipf s=0.9 over C, category 0..112, year
     1900..2020; the category set (8 values) and the year range are redrawn."""
-    import torch
-
     n_a = max(16, int(round(n_b * 2.5 / 36)))
     n_c = max(16, int(round(n_b * 4 / 36)))
-    g = _gen(seed)
     rng = np.random.default_rng(seed + 104729)
-    a_ids = (torch.randperm(n_a, generator=g, device="cuda") + 1).to(torch.int32)
-    rank_to_a = (torch.randperm(n_a, generator=g, device="cuda") + 1).to(torch.int32)
-    rank_to_c = torch.randperm(n_c, generator=g, device="cuda").to(torch.int32)
-    b_a = rank_to_a[_zipf_device(g, n_b, n_a, 1.1)]
-    b_c = rank_to_c[_zipf_device(g, n_b, n_c, 0.9)]
-    cols = {
-        "a_ids": a_ids,
-        "b_a": b_a.contiguous(),
-        "b_c": b_c.contiguous(),
-        "c_cat": _randint(g, 0, 112, n_c, torch.int16),  # uint16 values 0..112, same bits
-        "c_year": _randint(g, 1900, 2020, n_c, torch.int32),
-    }
+    cols = groupby_tables_device(n_a, n_b, n_c, seed)
+    del cols["a_id_max"]
     cat_set = sorted(int(v) for v in rng.choice(113, size=8, replace=False))
     y0 = int(rng.integers(1900, 2010))
     y1 = int(min(2020, y0 + int(rng.integers(5, 30))))

@@ -71,12 +71,20 @@ constexpr int kStageLevel[kNumStages] = {0, 0, 1, 2, 0, 1, 1, 2, 3};
 // Rows of one scan-agg flush period: <= 63 four-row chunks per thread plus one
 // tail row keeps every per-thread packed field inside its bits.
 constexpr int64_t kQ1SubRows = (int64_t)((kMaxRowsPerThread - 1) / 4) * 4 * kBB;
-constexpr int64_t kInitSlotsPerTile = 1 << 16;
-constexpr int64_t kSelectSlotsPerTile = 1 << 14;
+// Tile sizing: a stage of n units is cut into about kTargetTiles tiles (two per
+// worker block of a 148-SM B200 at two blocks per SM), so that even a lone large
+// instance spreads every stage over the whole GPU, but never into tiles below
+// the stage's minimum (per-item overhead) nor above the autotuned maximum.
+constexpr int64_t kTargetTiles = 2 * 148 * 2;
+constexpr int64_t kPoolMaxParticipants = 2 * 148;     // one per worker block
+constexpr int64_t kPoolWarps = kPoolMaxParticipants * 8;
+constexpr int64_t kPoolChunksPerWarp = 4;
+constexpr int64_t kPoolChunksPerBlock = 16;
 constexpr int kSelChunk = 1024;   // slots (or candidates) added per select round
 constexpr int kSelBuf = 2048;     // select buffer entries
 constexpr int kQ1ColBytes = BO_Q1_MAX_GROUPS * kWideWords * kBB * 8;
 static_assert(kQ1ColBytes + kBW * BO_Q1_MAX_GROUPS * kQ1Sums * 8 <= (int)kSmemBytes, "scan-agg columns fit");
+constexpr int kProbeResolveB = 4;  // join candidates per lane per resolve round
 constexpr int kGbQueueB = 384;
 constexpr int kGbFlushAtB = 128;
 constexpr int kGbResolveB = 4;
@@ -89,8 +97,9 @@ struct InstDesc {
   const float* pred_dev;     // optional device prediction read at launch time
   float factor;              // slots per predicted row
   uint32_t level_items[kLevels];
-  int64_t tile[kNumStages];      // rows / slots / words per tile
-  uint32_t n_tiles[kNumStages];
+  int64_t unit[kNumStages];       // rows / slots / words per tile (fixed stages) or chunk (pooled stages)
+  uint32_t n_chunks[kNumStages];  // chunks of a pooled stage (= tiles of a fixed stage)
+  uint32_t n_tiles[kNumStages];   // work items: tiles of a fixed stage, participants of a pooled one
   // scan-agg
   bo_fact_cols fact;
   int32_t cutoff;
@@ -123,11 +132,12 @@ struct InstState {
   uint32_t done[kLevels];  // completed items per level
   uint32_t ticket;         // finishing ticket of the last stage
   uint32_t overflow;
-  uint32_t pad[2];
+  uint32_t cursor[kNumStages];  // next chunk of each pooled stage
+  uint32_t pad[1];
   // join: 0 build rows, 1 distinct keys; group-by: 0 joined, 1 distinct, 2 C passing, 3 groups
   unsigned long long cnt[4];
   unsigned long long n_cand;
-  unsigned long long pad2[7];
+  unsigned long long pad2[3];
   unsigned long long acc[BO_Q1_MAX_GROUPS * kQ1Sums * 2];  // scan-agg 128-bit totals; join uses [0, 6)
 };
 static_assert(sizeof(InstState) % 64 == 0, "state alignment");
@@ -349,8 +359,8 @@ __device__ void stage_q1(const InstDesc& d, InstState* st, uint32_t tile, const 
   const int ng = (int)(d.n_fa * d.n_fb);
   const bo_fact_cols& c = d.fact;
   const int64_t n = c.n_rows;
-  const int64_t lo = (int64_t)tile * d.tile[kSQ1];
-  const int64_t hi = min(n, lo + d.tile[kSQ1]);
+  const int64_t lo = (int64_t)tile * d.unit[kSQ1];
+  const int64_t hi = min(n, lo + d.unit[kSQ1]);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t bad = 0;
   for (int64_t r = lo; r < hi; r += kQ1SubRows) {
@@ -431,61 +441,96 @@ __device__ __forceinline__ int32_t cap_log2_of(const InstDesc& d) {
   return cl;
 }
 
-__device__ void stage_join_init(const InstDesc& d, uint32_t tile) {
-  int64_t lo, hi;
-  split_range((int64_t)1 << cap_log2_of(d), tile, d.n_tiles[kSJInit], lo, hi);
-  for (int64_t i = lo + threadIdx.x; i < hi; i += kBB) d.slots[i] = kEmptySlot;
-  if (tile == 0) {
+// Streaming stages run as chunk pools: an instance's stage has a few
+// participant items (blocks); each warp of a participant takes the stage's
+// next chunk from a per-instance cursor until none are left, so work spreads
+// evenly over warps and blocks whatever the stage's size, and the block-level
+// totals are flushed once per participant rather than once per chunk.
+__device__ __forceinline__ bool next_chunk(uint32_t* cursor, uint32_t n_chunks, uint32_t& c) {
+  uint32_t v = 0;
+  if ((threadIdx.x & 31) == 0) v = atomicAdd(cursor, 1u);
+  c = __shfl_sync(0xffffffffu, v, 0);
+  return c < n_chunks;
+}
+
+// Units [lo, hi) of chunk c, clipped to n.
+__device__ __forceinline__ void chunk_range(uint32_t c, int64_t unit, int64_t n, int64_t& lo, int64_t& hi) {
+  lo = (int64_t)c * unit;
+  hi = min(n, lo + unit);
+}
+
+__device__ __forceinline__ unsigned __int128 warp_sum_u128(unsigned __int128 v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long lo = __shfl_xor_sync(0xffffffffu, (unsigned long long)v, o);
+    const unsigned long long hi = __shfl_xor_sync(0xffffffffu, (unsigned long long)(v >> 64), o);
+    v += ((unsigned __int128)hi << 64) | lo;
+  }
+  return v;
+}
+
+__device__ void stage_join_init(const InstDesc& d, InstState* st, uint32_t part) {
+  const int64_t cap = (int64_t)1 << cap_log2_of(d);
+  if (part == 0) {
     uint4* b4 = reinterpret_cast<uint4*>(d.bloom);
     for (uint32_t i = threadIdx.x; i < kBloomWords / 4; i += kBB) b4[i] = make_uint4(0, 0, 0, 0);
   }
+  ulonglong2* s2 = reinterpret_cast<ulonglong2*>(d.slots);
+  const int lane = threadIdx.x & 31;
+  uint32_t c;
+  while (next_chunk(&st->cursor[kSJInit], d.n_chunks[kSJInit], c)) {
+    int64_t lo, hi;
+    chunk_range(c, d.unit[kSJInit], cap, lo, hi);  // even bounds: unit and cap are even
+    for (int64_t i = lo / 2 + lane; i < hi / 2; i += 32) s2[i] = make_ulonglong2(kEmptySlot, kEmptySlot);
+  }
 }
 
-__device__ void stage_join_build(const InstDesc& d, InstState* st, uint32_t tile, const Smem& sm,
-                                 uint32_t (*red)[kBW]) {
-  const bo_join_build_cols& b = d.build;
-  const int64_t lo = (int64_t)tile * d.tile[kSJBuild];
-  const int64_t hi = min(b.n_rows, lo + d.tile[kSJBuild]);
-  const int32_t cl = cap_log2_of(d);
-  const uint64_t mask = (1ull << cl) - 1;
+__device__ void stage_join_build(const InstDesc& d, InstState* st, const Smem& sm, uint32_t (*red)[kBW]) {
+  const bo_join_build_cols b = d.build;
+  const int32_t date_lt = d.date_lt;
+  const uint32_t seg = d.seg;
+  unsigned long long* slots = d.slots;
+  uint32_t* bloom = d.bloom;
+  const uint64_t mask = (1ull << cap_log2_of(d)) - 1;
   const int lane = threadIdx.x & 31;
   uint32_t* bq = reinterpret_cast<uint32_t*>(sm.b) + (threadIdx.x >> 5) * 256;
   uint32_t qual = 0, newkeys = 0;
   bool full = false;
-  const int64_t steps = hi > lo ? (hi - lo + 15) / 16 : 0;
-  const int64_t steps_w = (steps + 31) & ~int64_t(31);
-  for (int64_t s = threadIdx.x; s < steps_w; s += kBB) {
-    const int64_t r0 = lo + s * 16;
-    const int64_t wbase = lo + (s - lane) * 16;
-    uint32_t q = 0;
-    if (r0 >= hi) {
-    } else if (r0 + 16 <= hi) {
-      const int4 sg = ld_stream_v4(b.segment + r0);
-      const uint32_t sw[4] = {(uint32_t)sg.x, (uint32_t)sg.y, (uint32_t)sg.z, (uint32_t)sg.w};
-      const int8v d0 = ld_stream_v8(b.date + r0), d1 = ld_stream_v8(b.date + r0 + 8);
+  uint32_t c;
+  while (next_chunk(&st->cursor[kSJBuild], d.n_chunks[kSJBuild], c)) {
+    int64_t lo, hi;
+    chunk_range(c, d.unit[kSJBuild], b.n_rows, lo, hi);
+    for (int64_t base = lo; base < hi; base += 512) {  // warp-uniform: 16 rows per lane
+      const int64_t r0 = base + lane * 16;
+      uint32_t q = 0;
+      if (r0 + 16 <= hi) {
+        const int4 sg = ld_stream_v4(b.segment + r0);
+        const uint32_t sw[4] = {(uint32_t)sg.x, (uint32_t)sg.y, (uint32_t)sg.z, (uint32_t)sg.w};
+        const int8v d0 = ld_stream_v8(b.date + r0), d1 = ld_stream_v8(b.date + r0 + 8);
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        const int32_t dk = k < 8 ? d0.v[k] : d1.v[k - 8];
-        q |= (uint32_t)build_qual(dk, (sw[k >> 2] >> (8 * (k & 3))) & 0xffu, d.date_lt, d.seg) << k;
+        for (int k = 0; k < 16; ++k) {
+          const int32_t dk = k < 8 ? d0.v[k] : d1.v[k - 8];
+          q |= (uint32_t)build_qual(dk, (sw[k >> 2] >> (8 * (k & 3))) & 0xffu, date_lt, seg) << k;
+        }
+      } else {
+        for (int k = 0; k < 16; ++k)
+          if (r0 + k < hi && build_qual(b.date[r0 + k], b.segment[r0 + k], date_lt, seg)) q |= 1u << k;
       }
-    } else {
-      for (int k = 0; k < 16; ++k)
-        if (r0 + k < hi && build_qual(b.date[r0 + k], b.segment[r0 + k], d.date_lt, d.seg)) q |= 1u << k;
-    }
-    qual += __popc(q);
+      qual += __popc(q);
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const uint32_t hm = (q >> (8 * half)) & 0xffu;
-      uint32_t total;
-      uint32_t pos = warp_exclusive_scan(__popc(hm), total);
-      if (total == 0) continue;
+      for (int half = 0; half < 2; ++half) {
+        const uint32_t hm = (q >> (8 * half)) & 0xffu;
+        uint32_t total;
+        uint32_t pos = warp_exclusive_scan(__popc(hm), total);
+        if (total == 0) continue;
 #pragma unroll
-      for (int k = 0; k < 8; ++k)
-        if ((hm >> k) & 1u) bq[pos++] = (uint32_t)(r0 - wbase) + 8 * half + k;
-      __syncwarp();
-      for (uint32_t i = lane; i < total; i += 32)
-        join_insert(d.slots, d.bloom, mask, __ldg(b.key + wbase + bq[i]), newkeys, full);
-      __syncwarp();
+        for (int k = 0; k < 8; ++k)
+          if ((hm >> k) & 1u) bq[pos++] = (uint32_t)(lane * 16 + 8 * half + k);
+        __syncwarp();
+        for (uint32_t i = lane; i < total; i += 32)
+          join_insert(slots, bloom, mask, __ldg(b.key + base + bq[i]), newkeys, full, kPresizedProbeLimit);
+        __syncwarp();
+      }
     }
   }
   uint32_t tot[4];
@@ -500,84 +545,84 @@ __device__ void stage_join_build(const InstDesc& d, InstState* st, uint32_t tile
   }
 }
 
-__device__ void stage_join_probe(const InstDesc& d, InstState* st, uint32_t tile, const Smem& sm,
-                                 const uint32_t* bl, uint32_t wmask, bo_batch_result* res, uint32_t* flag,
-                                 uint32_t* err) {
-  const bo_join_probe_cols& p = d.probe;
-  const int64_t lo = (int64_t)tile * d.tile[kSJProbe];
-  const int64_t hi = min(p.n_rows, lo + d.tile[kSJProbe]);
+__device__ void stage_join_probe(const InstDesc& d, InstState* st, const Smem& sm, const uint32_t* bl, uint32_t wmask,
+                                 bo_batch_result* res, uint32_t* flag, uint32_t* err) {
+  const bo_join_probe_cols p = d.probe;
   const int32_t cl = cap_log2_of(d);
   const uint64_t mask = (1ull << cl) - 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int32_t* qf = reinterpret_cast<int32_t*>(sm.b) + warp * 256;
   uint16_t* qo = reinterpret_cast<uint16_t*>(sm.b + kBW * 256 * 4) + warp * 256;
-  unsigned __int128* red = reinterpret_cast<unsigned __int128*>(sm.b + kBW * 256 * 6);
+  unsigned __int128* red = reinterpret_cast<unsigned __int128*>(sm.b + kBW * 256 * 6);  // [3][kBW]
   const unsigned long long* slots = d.slots;
   ProbeAcc acc;
-  const int64_t nsteps = hi > lo ? (hi - lo + 511) / 512 : 0;
-  for (int64_t s = warp; s < nsteps; s += kBW) {
-    const int64_t base = lo + s * 512;
-    const int64_t r0 = base + lane * 16;
-    int32_t fk[16];
-    uint32_t valid = 0xffffu;
-    if (r0 + 16 <= hi) {
-      const int8v f0 = ld_stream_v8(p.fk + r0), f1 = ld_stream_v8(p.fk + r0 + 8);
+  uint32_t c;
+  while (next_chunk(&st->cursor[kSJProbe], d.n_chunks[kSJProbe], c)) {
+    int64_t lo, hi;
+    chunk_range(c, d.unit[kSJProbe], p.n_rows, lo, hi);
+    for (int64_t base = lo; base < hi; base += 512) {
+      const int64_t r0 = base + lane * 16;
+      int32_t fk[16];
+      uint32_t valid = 0xffffu;
+      if (r0 + 16 <= hi) {
+        const int8v f0 = ld_stream_v8(p.fk + r0), f1 = ld_stream_v8(p.fk + r0 + 8);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        fk[k] = f0.v[k];
-        fk[8 + k] = f1.v[k];
-      }
-    } else {
-      valid = 0;
+        for (int k = 0; k < 8; ++k) {
+          fk[k] = f0.v[k];
+          fk[8 + k] = f1.v[k];
+        }
+      } else {
+        valid = 0;
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        fk[k] = 0;
-        if (r0 + k < hi) {
-          fk[k] = p.fk[r0 + k];
-          valid |= 1u << k;
+        for (int k = 0; k < 16; ++k) {
+          fk[k] = 0;
+          if (r0 + k < hi) {
+            fk[k] = p.fk[r0 + k];
+            valid |= 1u << k;
+          }
         }
       }
-    }
-    uint32_t hit = 0;
+      uint32_t hit = 0;
 #pragma unroll
-    for (int k = 15; k >= 0; --k) hit = (hit << 1) | bloom_test(bl, wmask, (uint32_t)fk[k]);
-    hit &= valid;
+      for (int k = 15; k >= 0; --k) hit = (hit << 1) | bloom_test(bl, wmask, (uint32_t)fk[k]);
+      hit &= valid;
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const uint32_t hm = (hit >> (8 * half)) & 0xffu;
-      uint32_t total;
-      uint32_t pos = warp_exclusive_scan(__popc(hm), total);
+      for (int half = 0; half < 2; ++half) {
+        const uint32_t hm = (hit >> (8 * half)) & 0xffu;
+        uint32_t total;
+        uint32_t pos = warp_exclusive_scan(__popc(hm), total);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if ((hm >> k) & 1u) {
-          qf[pos] = fk[8 * half + k];
-          qo[pos] = (uint16_t)(lane * 16 + 8 * half + k);
-          ++pos;
+        for (int k = 0; k < 8; ++k) {
+          if ((hm >> k) & 1u) {
+            qf[pos] = fk[8 * half + k];
+            qo[pos] = (uint16_t)(lane * 16 + 8 * half + k);
+            ++pos;
+          }
         }
+        __syncwarp();
+        probe_resolve<kProbeResolveB, true>(qf, qo, total, base, slots, mask, kPresizedProbeLimit, p.price, p.discount,
+                                            acc);
+        __syncwarp();
       }
-      __syncwarp();
-      for (uint32_t i = lane; i < total; i += 32) {
-        const int32_t key = qf[i];
-        const int64_t row = base + qo[i];
-        const uint32_t h = hash32((uint32_t)key);
-        const unsigned long long v = __ldcg(slots + (h & mask));
-        unsigned long long mult = 0;
-        if (v != kEmptySlot) {
-          if ((uint32_t)(v >> 32) == (uint32_t)key)
-            mult = v & 0xffffffffull;
-          else
-            mult = probe_slow<true>(slots, mask, h & mask, (uint32_t)key);
-        }
-        if (mult) accumulate_match((uint64_t)__ldg(p.price + row), (uint64_t)__ldg(p.discount + row), mult, acc);
-      }
-      __syncwarp();
     }
   }
   if (acc.bad) raise_error(err, acc.bad);
-  const unsigned __int128 bc = block_sum_u128(acc.cnt, red);
-  const unsigned __int128 bt = block_sum_u128(acc.tsum, red);
-  const unsigned __int128 br = block_sum_u128(acc.rsum, red);
+  // Participant totals: warp sums in registers, one pass through shared memory.
+  const unsigned __int128 wc = warp_sum_u128(acc.cnt), wt = warp_sum_u128(acc.tsum),
+                          wr = warp_sum_u128(acc.rsum);
+  if (lane == 0) {
+    red[warp] = wc;
+    red[kBW + warp] = wt;
+    red[2 * kBW + warp] = wr;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
+    unsigned __int128 bc = 0, bt = 0, br = 0;
+    for (int w = 0; w < kBW; ++w) {
+      bc += red[w];
+      bt += red[kBW + w];
+      br += red[2 * kBW + w];
+    }
     if (bc) atomic_add_i128(&st->acc[0], (__int128)bc);
     if (bt) atomic_add_i128(&st->acc[2], (__int128)bt);
     if (br) atomic_add_i128(&st->acc[4], (__int128)br);
@@ -603,68 +648,82 @@ __device__ void stage_join_probe(const InstDesc& d, InstState* st, uint32_t tile
   }
 }
 
-__device__ void stage_gb_init(const InstDesc& d, uint32_t tile) {
-  const uint32_t nt = d.n_tiles[kSGInit];
-  int64_t lo, hi;
-  split_range((int64_t)1 << cap_log2_of(d), tile, nt, lo, hi);
-  for (int64_t i = lo + threadIdx.x; i < hi; i += kBB) {
-    d.slots[i] = kEmptySlot;
-    d.mins[i] = 0x7fffffff;
-  }
-  split_range(d.mask_words, tile, nt, lo, hi);
-  for (int64_t i = lo + threadIdx.x; i < hi; i += kBB) d.amask[i] = 0u;
-  if (tile == 0)
+// Group-by init: one index space of the group slots [0, cap) followed by the
+// A-mask words; participant 0 also clears the Bloom filter.
+__device__ void stage_gb_init(const InstDesc& d, InstState* st, uint32_t part) {
+  const int64_t cap = (int64_t)1 << cap_log2_of(d);
+  const int64_t total = cap + d.mask_words;
+  if (part == 0)
     for (uint32_t i = threadIdx.x; i < kBloomWords; i += kBB) d.bloom[i] = 0u;
+  const int lane = threadIdx.x & 31;
+  uint32_t c;
+  while (next_chunk(&st->cursor[kSGInit], d.n_chunks[kSGInit], c)) {
+    int64_t lo, hi;
+    chunk_range(c, d.unit[kSGInit], total, lo, hi);
+    for (int64_t i = lo + lane; i < hi; i += 32) {
+      if (i < cap) {
+        d.slots[i] = kEmptySlot;
+        d.mins[i] = 0x7fffffff;
+      } else {
+        d.amask[i - cap] = 0u;
+      }
+    }
+  }
 }
 
-__device__ void stage_gb_cfilter(const InstDesc& d, InstState* st, uint32_t tile, const Smem& sm,
-                                 uint32_t (*red)[kBW]) {
+__device__ void stage_gb_cfilter(const InstDesc& d, InstState* st, const Smem& sm, uint32_t (*red)[kBW]) {
   uint32_t* catmask = reinterpret_cast<uint32_t*>(sm.b);
   for (int i = threadIdx.x; i < 2048; i += kBB) catmask[i] = 0u;
   __syncthreads();
   if (threadIdx.x < d.n_cats) atomicOr(&catmask[d.cats[threadIdx.x] >> 5], 1u << (d.cats[threadIdx.x] & 31u));
   __syncthreads();
-  const bo_gb_c_cols& c = d.c;
-  const int64_t n = c.n_rows;
-  const int64_t w0 = (int64_t)tile * d.tile[kSGCFilter];
-  const int64_t w1 = min(d.c_words, w0 + d.tile[kSGCFilter]);
-  uint32_t passed = 0;
-  for (int64_t w = w0 + threadIdx.x; w < w1; w += kBB) {
-    const int64_t r0 = w * 32;
-    uint32_t bits = 0;
-    if (r0 + 32 <= n) {
-      int8v cat[2];
-      cat[0] = ld_stream_v8(c.category + r0);
-      cat[1] = ld_stream_v8(c.category + r0 + 16);
+  const bo_gb_c_cols cc = d.c;
+  const int64_t n = cc.n_rows;
+  const int32_t year_lo = d.year_lo, year_hi = d.year_hi;
+  uint32_t* cbits = d.cbits;
+  uint32_t* bloom = d.bloom;
+  const int lane = threadIdx.x & 31;
+  uint32_t passed = 0, c;
+  while (next_chunk(&st->cursor[kSGCFilter], d.n_chunks[kSGCFilter], c)) {
+    int64_t w0, w1;
+    chunk_range(c, d.unit[kSGCFilter], d.c_words, w0, w1);
+    for (int64_t w = w0 + lane; w < w1; w += 32) {
+      const int64_t r0 = w * 32;
+      uint32_t bits = 0;
+      if (r0 + 32 <= n) {
+        int8v cat[2];
+        cat[0] = ld_stream_v8(cc.category + r0);
+        cat[1] = ld_stream_v8(cc.category + r0 + 16);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int8v y = ld_stream_v8(c.year + r0 + 8 * q);
+        for (int q = 0; q < 4; ++q) {
+          const int8v y = ld_stream_v8(cc.year + r0 + 8 * q);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const int row = 8 * q + k;
-          const uint32_t word = (uint32_t)cat[row >> 4].v[(row & 15) >> 1];
-          const uint32_t cv = (row & 1) ? (word >> 16) : (word & 0xffffu);
-          const bool ok = ((catmask[cv >> 5] >> (cv & 31u)) & 1u) && y.v[k] >= d.year_lo && y.v[k] <= d.year_hi;
-          bits |= (uint32_t)ok << row;
+          for (int k = 0; k < 8; ++k) {
+            const int row = 8 * q + k;
+            const uint32_t word = (uint32_t)cat[row >> 4].v[(row & 15) >> 1];
+            const uint32_t cv = (row & 1) ? (word >> 16) : (word & 0xffffu);
+            const bool ok = ((catmask[cv >> 5] >> (cv & 31u)) & 1u) && y.v[k] >= year_lo && y.v[k] <= year_hi;
+            bits |= (uint32_t)ok << row;
+          }
+        }
+      } else {
+        for (int k = 0; k < 32 && r0 + k < n; ++k) {
+          const uint32_t cv = cc.category[r0 + k];
+          const int32_t y = cc.year[r0 + k];
+          const bool ok = ((catmask[cv >> 5] >> (cv & 31u)) & 1u) && y >= year_lo && y <= year_hi;
+          bits |= (uint32_t)ok << k;
         }
       }
-    } else {
-      for (int k = 0; k < 32 && r0 + k < n; ++k) {
-        const uint32_t cv = c.category[r0 + k];
-        const int32_t y = c.year[r0 + k];
-        const bool ok = ((catmask[cv >> 5] >> (cv & 31u)) & 1u) && y >= d.year_lo && y <= d.year_hi;
-        bits |= (uint32_t)ok << k;
+      cbits[w] = bits;
+      passed += __popc(bits);
+      uint32_t bb = bits;
+      while (bb) {
+        const int k = __ffs(bb) - 1;
+        bb &= bb - 1;
+        uint32_t bw, bm;
+        bloom_pos((uint32_t)(r0 + k), bw, bm);
+        atomicOr(bloom + bw, bm);
       }
-    }
-    d.cbits[w] = bits;
-    passed += __popc(bits);
-    uint32_t bb = bits;
-    while (bb) {
-      const int k = __ffs(bb) - 1;
-      bb &= bb - 1;
-      uint32_t bw, bm;
-      bloom_pos((uint32_t)(r0 + k), bw, bm);
-      atomicOr(d.bloom + bw, bm);
     }
   }
   uint32_t tot[4];
@@ -672,24 +731,30 @@ __device__ void stage_gb_cfilter(const InstDesc& d, InstState* st, uint32_t tile
   if (threadIdx.x == 0 && tot[0]) atomicAdd(&st->cnt[2], (unsigned long long)tot[0]);
 }
 
-__device__ void stage_gb_amask(const InstDesc& d, uint32_t tile, uint32_t* err) {
-  const int64_t lo = (int64_t)tile * d.tile[kSGAMask];
-  const int64_t hi = min(d.a.n_rows, lo + d.tile[kSGAMask]);
-  uint32_t bad = 0;
-  for (int64_t i = lo + threadIdx.x; i < hi; i += kBB) {
-    const int32_t id = d.a.id[i];
-    if (id < 0) continue;  // negative ids are skipped, as by the reference's id masks
-    if (id > d.a_id_max) {
-      bad = 1;
-      continue;
+__device__ void stage_gb_amask(const InstDesc& d, InstState* st, uint32_t* err) {
+  const int32_t* ids = d.a.id;
+  const int32_t a_id_max = d.a_id_max;
+  uint32_t* amask = d.amask;
+  const int lane = threadIdx.x & 31;
+  uint32_t bad = 0, c;
+  while (next_chunk(&st->cursor[kSGAMask], d.n_chunks[kSGAMask], c)) {
+    int64_t lo, hi;
+    chunk_range(c, d.unit[kSGAMask], d.a.n_rows, lo, hi);
+    for (int64_t i = lo + lane; i < hi; i += 32) {
+      const int32_t id = ids[i];
+      if (id < 0) continue;  // negative ids are skipped, as by the reference's id masks
+      if (id > a_id_max) {
+        bad = 1;
+        continue;
+      }
+      atomicOr(amask + (id >> 5), 1u << (id & 31));
     }
-    atomicOr(d.amask + (id >> 5), 1u << (id & 31));
   }
   if (bad) raise_error(err, kErrValueRange);
 }
 
-__device__ void stage_gb_scan(const InstDesc& d, InstState* st, uint32_t tile, const Smem& sm, const uint32_t* bl,
-                              uint32_t wmask, uint32_t (*red)[kBW]) {
+__device__ void stage_gb_scan(const InstDesc& d, InstState* st, const Smem& sm, const uint32_t* bl, uint32_t wmask,
+                              uint32_t (*red)[kBW]) {
   int32_t* q_c = reinterpret_cast<int32_t*>(sm.b);
   uint32_t* q_row = reinterpret_cast<uint32_t*>(sm.b + kBW * kGbQueueB * 4);
   uint32_t* l_key = reinterpret_cast<uint32_t*>(sm.b + 2 * kBW * kGbQueueB * 4);
@@ -701,7 +766,7 @@ __device__ void stage_gb_scan(const InstDesc& d, InstState* st, uint32_t tile, c
     l_min[i] = 0x7fffffff;
   }
   __syncthreads();
-  const bo_gb_b_cols& b = d.b;
+  const bo_gb_b_cols b = d.b;
   const int64_t n_c = d.c.n_rows;
   const int32_t* c_year = d.c.year;
   const int32_t a_id_max = d.a_id_max;
@@ -709,32 +774,29 @@ __device__ void stage_gb_scan(const InstDesc& d, InstState* st, uint32_t tile, c
   const uint32_t* amask = d.amask;
   unsigned long long* slots = d.slots;
   int32_t* mins = d.mins;
-  const int32_t cl = cap_log2_of(d);
-  const uint64_t mask = (1ull << cl) - 1;
+  const uint64_t mask = (1ull << cap_log2_of(d)) - 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int32_t* qc = q_c + warp * kGbQueueB;
   uint32_t* qr = q_row + warp * kGbQueueB;
   uint32_t qn = 0, joined = 0, newkeys = 0, full = 0;
-  const int64_t lo = (int64_t)tile * d.tile[kSGScan];
-  const int64_t hi = min(b.n_rows, lo + d.tile[kSGScan]);
   auto resolve = [&](uint32_t cnt) {
     __syncwarp();
     for (uint32_t i0 = 0; i0 < cnt; i0 += 32 * kGbResolveB) {
-      int32_t c[kGbResolveB], a[kGbResolveB], y[kGbResolveB];
+      int32_t cc[kGbResolveB], a[kGbResolveB], y[kGbResolveB];
       uint32_t row[kGbResolveB], w[kGbResolveB];
 #pragma unroll
       for (int r = 0; r < kGbResolveB; ++r) {
         const uint32_t i = i0 + r * 32 + lane;
-        c[r] = i < cnt ? qc[i] : -1;
+        cc[r] = i < cnt ? qc[i] : -1;
         row[r] = i < cnt ? qr[i] : 0u;
-        const bool in = (uint32_t)c[r] < (uint32_t)n_c;
-        w[r] = in ? __ldcg(cbits + (c[r] >> 5)) : 0u;
+        const bool in = (uint32_t)cc[r] < (uint32_t)n_c;
+        w[r] = in ? __ldcg(cbits + (cc[r] >> 5)) : 0u;
       }
 #pragma unroll
       for (int r = 0; r < kGbResolveB; ++r) {
-        const bool pass = (w[r] >> (c[r] & 31)) & 1u;
+        const bool pass = (w[r] >> (cc[r] & 31)) & 1u;
         a[r] = pass ? __ldg(b.a_id + row[r]) : -1;
-        y[r] = pass ? __ldg(c_year + c[r]) : 0;
+        y[r] = pass ? __ldg(c_year + cc[r]) : 0;
       }
       bool pend[kGbResolveB];
 #pragma unroll
@@ -772,65 +834,69 @@ __device__ void stage_gb_scan(const InstDesc& d, InstState* st, uint32_t tile, c
         if (got[r] == kEmptySlot || (uint32_t)(got[r] >> 32) == (uint32_t)a[r]) {
           atomicAdd(slots + first[r], 1ull);
           atomicMin(mins + first[r], y[r]);
-        } else if (!gb_global_insert(slots, mins, mask, (uint32_t)a[r], 1u, y[r], newkeys, (first[r] + 1) & mask)) {
+        } else if (!gb_global_insert(slots, mins, mask, (uint32_t)a[r], 1u, y[r], newkeys, (first[r] + 1) & mask,
+                                       kPresizedProbeLimit)) {
           full = 1;
         }
       }
     }
     __syncwarp();
   };
-  const int64_t nsteps = hi > lo ? (hi - lo + 511) / 512 : 0;
-  for (int64_t s = warp; s < nsteps; s += kBW) {
-    const int64_t base = lo + s * 512;
-    const int64_t r0 = base + lane * 16;
-    int32_t cid[16];
-    uint32_t valid = 0;
-    if (r0 + 16 <= hi) {
-      const int8v c0 = ld_stream_v8(b.c_id + r0), c1 = ld_stream_v8(b.c_id + r0 + 8);
+  uint32_t c;
+  while (next_chunk(&st->cursor[kSGScan], d.n_chunks[kSGScan], c)) {
+    int64_t lo, hi;
+    chunk_range(c, d.unit[kSGScan], b.n_rows, lo, hi);
+    for (int64_t base = lo; base < hi; base += 512) {
+      const int64_t r0 = base + lane * 16;
+      int32_t cid[16];
+      uint32_t valid = 0;
+      if (r0 + 16 <= hi) {
+        const int8v c0 = ld_stream_v8(b.c_id + r0), c1 = ld_stream_v8(b.c_id + r0 + 8);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        cid[k] = c0.v[k];
-        cid[8 + k] = c1.v[k];
-      }
-      valid = 0xffffu;
-    } else {
+        for (int k = 0; k < 8; ++k) {
+          cid[k] = c0.v[k];
+          cid[8 + k] = c1.v[k];
+        }
+        valid = 0xffffu;
+      } else {
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        cid[k] = -1;
-        if (r0 + k < hi) {
-          cid[k] = b.c_id[r0 + k];
-          valid |= 1u << k;
+        for (int k = 0; k < 16; ++k) {
+          cid[k] = -1;
+          if (r0 + k < hi) {
+            cid[k] = b.c_id[r0 + k];
+            valid |= 1u << k;
+          }
         }
       }
-    }
-    uint32_t hit = 0;
+      uint32_t hit = 0;
 #pragma unroll
-    for (int k = 15; k >= 0; --k) hit = (hit << 1) | bloom_test(bl, wmask, (uint32_t)cid[k]);
-    hit &= valid;
+      for (int k = 15; k >= 0; --k) hit = (hit << 1) | bloom_test(bl, wmask, (uint32_t)cid[k]);
+      hit &= valid;
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const uint32_t hm = (hit >> (8 * half)) & 0xffu;
-      uint32_t total;
-      uint32_t pos = warp_exclusive_scan(__popc(hm), total);
-      if (total == 0) continue;
-      if (qn + total > kGbQueueB) {
-        resolve(qn);
-        qn = 0;
-      }
-      pos += qn;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if ((hm >> k) & 1u) {
-          qc[pos] = cid[8 * half + k];
-          qr[pos] = (uint32_t)(r0 + 8 * half + k);
-          ++pos;
+      for (int half = 0; half < 2; ++half) {
+        const uint32_t hm = (hit >> (8 * half)) & 0xffu;
+        uint32_t total;
+        uint32_t pos = warp_exclusive_scan(__popc(hm), total);
+        if (total == 0) continue;
+        if (qn + total > kGbQueueB) {
+          resolve(qn);
+          qn = 0;
         }
-      }
-      qn += total;
-      __syncwarp();
-      if (qn >= kGbFlushAtB) {
-        resolve(qn);
-        qn = 0;
+        pos += qn;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          if ((hm >> k) & 1u) {
+            qc[pos] = cid[8 * half + k];
+            qr[pos] = (uint32_t)(r0 + 8 * half + k);
+            ++pos;
+          }
+        }
+        qn += total;
+        __syncwarp();
+        if (qn >= kGbFlushAtB) {
+          resolve(qn);
+          qn = 0;
+        }
       }
     }
   }
@@ -838,7 +904,8 @@ __device__ void stage_gb_scan(const InstDesc& d, InstState* st, uint32_t tile, c
   __syncthreads();
   for (int i = threadIdx.x; i < kGbLocalB; i += kBB)
     if (l_key[i] != 0xffffffffu)
-      if (!gb_global_insert(slots, mins, mask, l_key[i], l_cnt[i], l_min[i], newkeys)) full = 1;
+      if (!gb_global_insert(slots, mins, mask, l_key[i], l_cnt[i], l_min[i], newkeys, ~0ull, kPresizedProbeLimit))
+        full = 1;
   uint32_t tot[4];
   block_counts(joined, newkeys, 0, full, red, tot);
   if (threadIdx.x == 0) {
@@ -1055,25 +1122,25 @@ __global__ void __launch_bounds__(kBB, 2)
         stage_q1(d, st, tile, sm, res, &flag, err);
         break;
       case kSJInit:
-        stage_join_init(d, tile);
+        stage_join_init(d, st, tile);
         break;
       case kSJBuild:
-        stage_join_build(d, st, tile, sm, red);
+        stage_join_build(d, st, sm, red);
         break;
       case kSJProbe:
-        stage_join_probe(d, st, tile, sm, bl, wmask, res, &flag, err);
+        stage_join_probe(d, st, sm, bl, wmask, res, &flag, err);
         break;
       case kSGInit:
-        stage_gb_init(d, tile);
+        stage_gb_init(d, st, tile);
         break;
       case kSGCFilter:
-        stage_gb_cfilter(d, st, tile, sm, red);
+        stage_gb_cfilter(d, st, sm, red);
         break;
       case kSGAMask:
-        stage_gb_amask(d, tile, err);
+        stage_gb_amask(d, st, err);
         break;
       case kSGScan:
-        stage_gb_scan(d, st, tile, sm, bl, wmask, red);
+        stage_gb_scan(d, st, sm, bl, wmask, red);
         break;
       case kSGSelect:
         stage_gb_select(d, st, tile, sm, &selctl, red, res, &flag);
@@ -1111,6 +1178,26 @@ int32_t presize(float pred, float factor, int32_t max_log2) {
   return cl;
 }
 int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+// Units per tile for a stage of n units: about n / kTargetTiles, clamped to
+// [lo, hi] and rounded up to a multiple of `align`.
+int64_t tile_size(int64_t n, int64_t lo, int64_t hi, int64_t align) {
+  int64_t t = ceil_div(std::max<int64_t>(n, 1), kTargetTiles);
+  t = std::min(std::max(t, lo), std::max(hi, lo));
+  return ceil_div(t, align) * align;
+}
+
+// A pooled stage of n units: chunks of about n / (kPoolChunksPerWarp x the
+// warps of a full GPU) units, clamped to [lo, hi] and a multiple of `align`;
+// one participant block per kPoolChunksPerBlock chunks, at most one per worker.
+void pool_stage(InstDesc& d, int s, int64_t n, int64_t lo, int64_t hi, int64_t align) {
+  int64_t u = ceil_div(std::max<int64_t>(n, 1), kPoolWarps * kPoolChunksPerWarp);
+  u = std::min(std::max(u, lo), std::max(hi, lo));
+  u = ceil_div(u, align) * align;
+  d.unit[s] = u;
+  const int64_t chunks = std::max<int64_t>(1, ceil_div(n, u));
+  d.n_chunks[s] = (uint32_t)chunks;
+  d.n_tiles[s] = (uint32_t)std::min<int64_t>(kPoolMaxParticipants, ceil_div(chunks, kPoolChunksPerBlock));
+}
 
 bool cols_ok(std::initializer_list<const void*> ps) {
   for (const void* p : ps)
@@ -1239,14 +1326,14 @@ Plan plan_instance(const bo_batch_instance& x) {
   d.factor = factor;
   p.table_bytes = 0;
   p.weight = 0.0;
-  for (int s = 0; s < kNumStages; ++s) d.tile[s] = 1;
+  for (int s = 0; s < kNumStages; ++s) d.unit[s] = 1;
   if (x.kind == BO_BATCH_SCAN_AGG) {
     d.fact = x.fact;
     d.cutoff = x.ship_cutoff;
     d.n_fa = (uint32_t)x.n_flag_a;
     d.n_fb = (uint32_t)x.n_flag_b;
-    d.tile[kSQ1] = t;
-    d.n_tiles[kSQ1] = (uint32_t)std::max<int64_t>(1, ceil_div(x.fact.n_rows, t));
+    d.unit[kSQ1] = tile_size(x.fact.n_rows, 16384, t, 1024);
+    d.n_chunks[kSQ1] = d.n_tiles[kSQ1] = (uint32_t)std::max<int64_t>(1, ceil_div(x.fact.n_rows, d.unit[kSQ1]));
     p.weight = 38.0 * (double)x.fact.n_rows;
   } else if (x.kind == BO_BATCH_JOIN) {
     d.build = x.build;
@@ -1256,12 +1343,9 @@ Plan plan_instance(const bo_batch_instance& x) {
     const int32_t max_log2 = std::max(10, ceil_log2_u64((uint64_t)std::max<int64_t>(x.build.n_rows, 1) * 2));
     d.cap_log2 = x.predicted_device ? max_log2 : presize(x.predicted, factor, max_log2);
     const int64_t cap = (int64_t)1 << d.cap_log2;
-    d.tile[kSJInit] = kInitSlotsPerTile;
-    d.n_tiles[kSJInit] = (uint32_t)std::max<int64_t>(1, ceil_div(cap, kInitSlotsPerTile));
-    d.tile[kSJBuild] = 2 * t;
-    d.n_tiles[kSJBuild] = (uint32_t)std::max<int64_t>(1, ceil_div(x.build.n_rows, 2 * t));
-    d.tile[kSJProbe] = t;
-    d.n_tiles[kSJProbe] = (uint32_t)std::max<int64_t>(1, ceil_div(x.probe.n_rows, t));
+    pool_stage(d, kSJInit, cap, 2048, 1 << 16, 2048);
+    pool_stage(d, kSJBuild, x.build.n_rows, 512, 2 * t, 512);
+    pool_stage(d, kSJProbe, x.probe.n_rows, 512, t, 512);
     p.table_bytes = al256(8 * (size_t)cap) + al256(kBloomBytes);
     p.weight = 9.0 * (double)x.build.n_rows + 20.0 * (double)x.probe.n_rows;
   } else {
@@ -1284,17 +1368,13 @@ Plan plan_instance(const bo_batch_instance& x) {
     const int64_t cap = (int64_t)1 << d.cap_log2;
     d.mask_words = ((int64_t)x.a_id_max + 1 + 31) / 32;
     d.c_words = (x.c.n_rows + 31) / 32;
-    d.tile[kSGInit] = kInitSlotsPerTile;
-    d.n_tiles[kSGInit] =
-        (uint32_t)std::max<int64_t>(1, ceil_div(std::max<int64_t>(cap, d.mask_words), kInitSlotsPerTile));
-    d.tile[kSGCFilter] = std::max<int64_t>(1, t / 32);
-    d.n_tiles[kSGCFilter] = (uint32_t)std::max<int64_t>(1, ceil_div(d.c_words, d.tile[kSGCFilter]));
-    d.tile[kSGAMask] = t;
-    d.n_tiles[kSGAMask] = (uint32_t)std::max<int64_t>(1, ceil_div(x.a.n_rows, t));
-    d.tile[kSGScan] = t;
-    d.n_tiles[kSGScan] = (uint32_t)std::max<int64_t>(1, ceil_div(x.b.n_rows, t));
-    d.tile[kSGSelect] = kSelectSlotsPerTile;
-    d.n_tiles[kSGSelect] = (uint32_t)std::max<int64_t>(1, ceil_div(cap, kSelectSlotsPerTile));
+    pool_stage(d, kSGInit, cap + d.mask_words, 2048, 1 << 16, 1024);
+    pool_stage(d, kSGCFilter, d.c_words, 32, std::max<int64_t>(32, t / 32), 32);  // bitmap words
+    pool_stage(d, kSGAMask, x.a.n_rows, 1024, t, 1024);
+    pool_stage(d, kSGScan, x.b.n_rows, 512, t, 512);
+    // Select tiles split the slot range of this launch's capacity evenly.
+    d.unit[kSGSelect] = tile_size(cap, 2048, 65536, 1024);
+    d.n_chunks[kSGSelect] = d.n_tiles[kSGSelect] = (uint32_t)std::max<int64_t>(1, ceil_div(cap, d.unit[kSGSelect]));
     const size_t n_cand = (size_t)d.n_tiles[kSGSelect] * (size_t)std::max(1, x.k);
     p.table_bytes = al256(8 * (size_t)cap) + al256(4 * (size_t)cap) + al256(kBloomBytes) +
                     al256(4 * (size_t)std::max<int64_t>(d.c_words, 1)) + al256(4 * (size_t)d.mask_words) +

@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
                                                            const int32_t* __restrict__ c_year,
                                                            const uint32_t* __restrict__ amask,
                                                            unsigned long long* slots, int32_t* mins, uint32_t* dbits,
-                                                           GbMeta* meta, uint32_t* err) {
+                                                           GbMeta* meta, uint64_t probe_limit, uint32_t* err) {
   extern __shared__ __align__(128) uint32_t bloom_s[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int32_t q_c[kGbWarps][kGbQueue];
@@ -348,7 +348,8 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
           if (got[r] == kGbEmpty || (uint32_t)(got[r] >> 32) == (uint32_t)a[r]) {
             atomicAdd(slots + first[r], 1ull);
             atomicMin(mins + first[r], y[r]);
-          } else if (!gb_global_insert(slots, mins, mask, (uint32_t)a[r], 1u, y[r], newkeys, (first[r] + 1) & mask)) {
+          } else if (!gb_global_insert(slots, mins, mask, (uint32_t)a[r], 1u, y[r], newkeys, (first[r] + 1) & mask,
+                                              probe_limit)) {
             full = 1;
           }
         }
@@ -411,7 +412,8 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
     // Flush the block's pre-aggregated groups into the global table.
     for (int i = threadIdx.x; i < kGbLocalSlots; i += blockDim.x) {
       if (l_key[i] != 0xffffffffu)
-        if (!gb_global_insert(slots, mins, mask, l_key[i], l_cnt[i], l_min[i], newkeys)) full = 1;
+        if (!gb_global_insert(slots, mins, mask, l_key[i], l_cnt[i], l_min[i], newkeys, ~0ull, probe_limit))
+          full = 1;
     }
   }
   if (!use_bloom) mbar_wait_bounded(&bar, 0, kWaitLimitNs);
@@ -672,7 +674,7 @@ int gb_prepare(bo_ctx* ctx, const bo_gb_a_cols& a, const bo_gb_c_cols& c, const 
 
 template <int kMode>
 int gb_launch_scan(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, const bo_gb_params& prm,
-                   const GbWs& ws) {
+                   const GbWs& ws, uint64_t probe_limit = ~0ull) {
   const void* k = reinterpret_cast<const void*>(&gb_scan_kernel<kMode>);
   static bool ready = false;
   if (!ready) {
@@ -682,14 +684,15 @@ int gb_launch_scan(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, co
   const int grid = grid_res(ctx, k, kGbBlock, kGbBloomBytes, (b.n_rows + kGbRowsPerLane - 1) / kGbRowsPerLane);
   gb_scan_kernel<kMode><<<grid, kGbBlock, kGbBloomBytes, ctx->stream>>>(
       b, c.n_rows, prm.a_id_max, ws.bloom, ws.cbits, c.year, prm.a_mask ? prm.a_mask : ws.amask, ws.slots, ws.mins,
-      ws.dbits, ws.meta, ctx->d_err);
+      ws.dbits, ws.meta, probe_limit, ctx->d_err);
   return after_launch(ctx, "gb_scan_kernel");
 }
 
 // Aggregate + compact + sort + top-k, asynchronous.
 int gb_aggregate_order(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, const bo_gb_params& prm,
                        const GbWs& ws, bo_gb_result* out, int32_t mode) {
-  int rc = gb_launch_scan<1>(ctx, b, c, prm, ws);
+  // Exact-size tables (mode 0) probe without a bound; presized ones fail fast.
+  int rc = gb_launch_scan<1>(ctx, b, c, prm, ws, mode == 0 ? ~0ull : kPresizedProbeLimit);
   if (rc) return rc;
   const int wa = std::max(1, bit_length((uint64_t)prm.a_id_max));
   const int wc = std::max(1, bit_length((uint64_t)b.n_rows));

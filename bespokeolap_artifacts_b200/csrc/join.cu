@@ -121,7 +121,7 @@ constexpr int kBuildRowsPerThread = 16;
 
 __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_cols b, int32_t date_lt, uint32_t seg,
                                                                  unsigned long long* slots, uint32_t* bloom,
-                                                                 JoinMeta* meta) {
+                                                                 JoinMeta* meta, uint64_t probe_limit) {
   // Read-only for this kernel (written by the init kernel): the L1-cached path
   // avoids every warp hitting the same L2 sector.
   const int32_t cl = __ldg(&meta->cap_log2);
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_c
         if ((hm >> k) & 1u) bq[pos++] = (uint32_t)(r0 - wbase) + 8 * half + k;
       __syncwarp();
       for (uint32_t i = lane; i < total; i += 32)
-        join_insert(slots, bloom, mask, __ldg(b.key + wbase + bq[i]), newkeys, full);
+        join_insert(slots, bloom, mask, __ldg(b.key + wbase + bq[i]), newkeys, full, probe_limit);
       __syncwarp();
     }
   }
@@ -217,11 +217,13 @@ constexpr int kProbeWarps = kJoinBlock / 32;
 constexpr int kRowsPerLane = 16;
 constexpr int kRowsPerWarpStep = 32 * kRowsPerLane;
 constexpr int kQueue = 32 * 8;
+constexpr int kJoinResolveR = 2;  // candidates per lane per resolve round
 
-__global__ void __launch_bounds__(kJoinBlock) join_probe_kernel(bo_join_probe_cols p,
+__global__ void __launch_bounds__(kJoinBlock, 2) join_probe_kernel(bo_join_probe_cols p,
                                                                 const unsigned long long* slots,
                                                                 const uint32_t* bloom_g, JoinMeta* meta,
-                                                                bo_join_result* out, int32_t mode, uint32_t* err) {
+                                                                bo_join_result* out, int32_t mode, uint64_t probe_limit,
+                                                                uint32_t* err) {
   extern __shared__ __align__(128) uint32_t bloom_s[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ unsigned __int128 red[kJoinBlock + 32];
@@ -294,20 +296,7 @@ __global__ void __launch_bounds__(kJoinBlock) join_probe_kernel(bo_join_probe_co
         }
       }
       __syncwarp();
-      for (uint32_t i = lane; i < total; i += 32) {
-        const int32_t key = qf[i];
-        const int64_t row = base + qo[i];
-        const uint32_t h = hash32((uint32_t)key);
-        const unsigned long long v = __ldg(slots + (h & mask));
-        unsigned long long mult = 0;
-        if (v != kEmptySlot) {
-          if ((uint32_t)(v >> 32) == (uint32_t)key)
-            mult = v & 0xffffffffull;
-          else
-            mult = probe_slow<false>(slots, mask, h & mask, (uint32_t)key);
-        }
-        if (mult) accumulate_match((uint64_t)__ldg(p.price + row), (uint64_t)__ldg(p.discount + row), mult, acc);
-      }
+      probe_resolve<kJoinResolveR, false>(qf, qo, total, base, slots, mask, probe_limit, p.price, p.discount, acc);
       __syncwarp();
     }
   }
@@ -410,7 +399,8 @@ int grid_for(bo_ctx* ctx, const void* k, int block, size_t smem, int64_t work_it
   return (int)std::max<int64_t>(g, 1);
 }
 
-int launch_probe(bo_ctx* ctx, const bo_join_probe_cols& p, const JoinWs& ws, bo_join_result* out, int32_t mode) {
+int launch_probe(bo_ctx* ctx, const bo_join_probe_cols& p, const JoinWs& ws, bo_join_result* out, int32_t mode,
+                 uint64_t probe_limit) {
   const void* k = reinterpret_cast<const void*>(&join_probe_kernel);
   static bool ready = false;
   if (!ready) {
@@ -421,7 +411,7 @@ int launch_probe(bo_ctx* ctx, const bo_join_probe_cols& p, const JoinWs& ws, bo_
   // chunks so the per-block Bloom-filter copy is amortised.
   const int grid = grid_for(ctx, k, kJoinBlock, kBloomBytes, (p.n_rows + kRowsPerLane - 1) / kRowsPerLane);
   join_probe_kernel<<<grid, kJoinBlock, kBloomBytes, ctx->stream>>>(p, ws.slots, ws.bloom, ws.meta, out, mode,
-                                                                     ctx->d_err);
+                                                                     probe_limit, ctx->d_err);
   return after_launch(ctx, "join_probe_kernel");
 }
 
@@ -435,10 +425,12 @@ int join_run(bo_ctx* ctx, const bo_join_build_cols& b, const bo_join_probe_cols&
   if (rc) return rc;
   const void* kb = reinterpret_cast<const void*>(&join_build_kernel);
   const int gb = grid_for(ctx, kb, kBuildBlock, 0, (b.n_rows + kBuildRowsPerThread - 1) / kBuildRowsPerThread);
+  // Exact-size tables (mode 0) probe without a bound; presized ones fail fast.
+  const uint64_t limit = mode == 0 ? ~0ull : kPresizedProbeLimit;
   join_build_kernel<<<gb, kBuildBlock, 0, ctx->stream>>>(b, prm.date_lt, (uint32_t)prm.segment_eq, ws.slots,
-                                                          ws.bloom, ws.meta);
+                                                          ws.bloom, ws.meta, limit);
   if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
-  return launch_probe(ctx, p, ws, out, mode);
+  return launch_probe(ctx, p, ws, out, mode, limit);
 }
 
 int finish_join(bo_ctx* ctx, bo_join_result* host, const bo_join_result* dev) {
@@ -549,7 +541,7 @@ int bo_join_probe_device(bo_ctx* ctx, const bo_join_probe_cols* p, bo_join_resul
   JoinWs ws;
   int rc = join_workspace(ctx, 0, &ws);
   if (rc) return rc;
-  return launch_probe(ctx, *p, ws, out_device, 1);
+  return launch_probe(ctx, *p, ws, out_device, 1, ~0ull);  // the table's build bound is not known here
 }
 
 int bo_join_host(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join_probe_cols* ph, const bo_join_params* prm,

@@ -140,12 +140,21 @@ __device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t v, uint32_t& to
 
 // Inserts one qualifying build key: a new key claims a slot and sets its two
 // Bloom bits; a repeated key adds to the multiplicity in the low word.
+// Probe-chain bound of presized tables: a table sized from a prediction that
+// turns out too low must fail fast (the caller reruns exactly) instead of
+// walking ever longer chains; at the loads a presized table is built for
+// (<= 0.4 at an exact prediction) chains stay far below it.  Exact-size tables
+// pass their capacity as the bound (no limit), and a lookup may stop at the
+// bound because a key that needed a longer chain would have flagged overflow.
+constexpr uint64_t kPresizedProbeLimit = 256;
+
 __device__ __forceinline__ void join_insert(unsigned long long* slots, uint32_t* bloom, uint64_t mask, int32_t key,
-                                            uint32_t& newkeys, bool& full) {
+                                            uint32_t& newkeys, bool& full, uint64_t limit) {
   const uint32_t h = hash32((uint32_t)key);
   uint64_t idx = h & mask;
   const unsigned long long mine = ((unsigned long long)(uint32_t)key << 32) | 1ull;
-  for (uint64_t step = 0; step <= mask; ++step) {
+  const uint64_t steps = mask < limit ? mask : limit;
+  for (uint64_t step = 0; step <= steps; ++step) {
     const unsigned long long old = atomicCAS(slots + idx, kEmptySlot, mine);
     if (old == kEmptySlot) {
       ++newkeys;
@@ -188,8 +197,9 @@ __device__ __forceinline__ void accumulate_match(uint64_t p, uint64_t d, unsigne
 // kCoherent reads through L2 only (for a table written earlier in the same launch).
 template <bool kCoherent>
 static __device__ __noinline__ unsigned long long probe_slow(const unsigned long long* slots, uint64_t mask, uint64_t idx,
-                                                      uint32_t key) {
-  for (uint64_t step = 1; step <= mask; ++step) {
+                                                      uint32_t key, uint64_t limit) {
+  const uint64_t steps = mask < limit ? mask : limit;
+  for (uint64_t step = 1; step <= steps; ++step) {
     idx = (idx + 1) & mask;
     const unsigned long long v = kCoherent ? __ldcg(slots + idx) : __ldg(slots + idx);
     if (v == kEmptySlot) return 0;
@@ -198,15 +208,64 @@ static __device__ __noinline__ unsigned long long probe_slow(const unsigned long
   return 0;
 }
 
+// Resolves a warp's queued probe candidates: keys qf[i] of rows base + qo[i],
+// i < total (all lanes call it together).  Each lane takes R entries per round
+// and issues their table loads together, then the price / discount loads of
+// the matches together, so a warp keeps up to 32 x R lookups in flight instead
+// of one dependent chain per lane.  kCoherent reads the table through L2 only
+// (for a table written earlier in the same launch).
+template <int R, bool kCoherent>
+__device__ __forceinline__ void probe_resolve(const int32_t* qf, const uint16_t* qo, uint32_t total, int64_t base,
+                                              const unsigned long long* slots, uint64_t mask, uint64_t limit,
+                                              const int64_t* price, const int64_t* disc, ProbeAcc& acc) {
+  const int lane = threadIdx.x & 31;
+  for (uint32_t i0 = 0; i0 < total; i0 += 32 * R) {
+    int32_t key[R];
+    int64_t row[R];
+    uint64_t idx[R];
+    unsigned long long v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const uint32_t i = i0 + r * 32 + lane;
+      const bool ok = i < total;
+      key[r] = ok ? qf[i] : 0;
+      row[r] = ok ? base + qo[i] : 0;
+      idx[r] = hash32((uint32_t)key[r]) & mask;
+      v[r] = ok ? (kCoherent ? __ldcg(slots + idx[r]) : __ldg(slots + idx[r])) : kEmptySlot;
+    }
+    unsigned long long mult[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      mult[r] = 0;
+      if (v[r] != kEmptySlot) {
+        if ((uint32_t)(v[r] >> 32) == (uint32_t)key[r])
+          mult[r] = v[r] & 0xffffffffull;
+        else
+          mult[r] = probe_slow<kCoherent>(slots, mask, idx[r], (uint32_t)key[r], limit);
+      }
+    }
+    uint64_t pr[R], dc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      pr[r] = mult[r] ? (uint64_t)__ldg(price + row[r]) : 0;
+      dc[r] = mult[r] ? (uint64_t)__ldg(disc + row[r]) : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (mult[r]) accumulate_match(pr[r], dc[r], mult[r], acc);
+  }
+}
+
 // Group-table insert of a (key, count, min) partial, starting at `start` or at
 // the key's hash slot: key << 32 | count words claimed with one CAS, the
 // minimum kept beside the slot with atomicMin.
 __device__ __forceinline__ bool gb_global_insert(unsigned long long* slots, int32_t* mins, uint64_t mask, uint32_t key,
                                                  uint32_t cnt, int32_t mn, uint32_t& newkeys,
-                                                 uint64_t start = ~0ull) {
+                                                 uint64_t start = ~0ull, uint64_t limit = ~0ull) {
   uint64_t idx = start == ~0ull ? (hash32(key) & mask) : start;
   const unsigned long long claim = (unsigned long long)key << 32;
-  for (uint64_t step = 0; step <= mask; ++step) {
+  const uint64_t steps = mask < limit ? mask : limit;
+  for (uint64_t step = 0; step <= steps; ++step) {
     // CAS first: one round trip claims an empty slot or returns its owner.
     unsigned long long v = atomicCAS(slots + idx, kEmptySlot, claim);
     if (v == kEmptySlot) {

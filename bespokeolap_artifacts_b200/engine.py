@@ -73,6 +73,11 @@ def q1_cutoff(delta_days: int) -> int:
     return days_from_civil(1998, 12, 1) - int(delta_days)
 
 
+def _rows(dev: dict, name: str) -> int:
+    """Row count of a device column (torch tensor) of a group-by table set."""
+    return int(dev[name].numel())
+
+
 class Engine:
     """One engine context (device, stream, scratch) with the pipeline entry points."""
 
@@ -217,7 +222,7 @@ class Engine:
         """Exact distinct pre-pass, one host round trip, aggregation, sort, top-k.
         ``dev`` holds device columns a_ids, b_a, b_c, c_cat, c_year."""
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
-                                          len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
+                                          _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,
                                           g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
                                           dev.get("a_mask"))
         out = N.GbResult()
@@ -226,7 +231,7 @@ class Engine:
 
     def groupby_presized(self, dev: dict, g, pred_dev) -> dict:
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
-                                          len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
+                                          _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,
                                           g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
                                           dev.get("a_mask"))
         out = N.GbResult()
@@ -236,7 +241,7 @@ class Engine:
 
     def groupby_presized_device(self, dev: dict, g, pred_dev, out_dev) -> None:
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
-                                          len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
+                                          _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,
                                           g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
                                           dev.get("a_mask"))
         self.ctx.call("bo_groupby_topk_presized_device", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
@@ -244,7 +249,7 @@ class Engine:
 
     def groupby_distinct_device(self, dev: dict, g, out_dev) -> None:
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
-                                          len(g.a_ids), len(g.b_a), len(g.c_cat), g.cat_set, g.year_lo, g.year_hi,
+                                          _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,
                                           g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
                                           dev.get("a_mask"))
         self.ctx.call("bo_groupby_distinct_device", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),

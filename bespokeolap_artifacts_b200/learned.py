@@ -190,10 +190,47 @@ def gen_join_training_table(rng: np.random.Generator, n: int) -> tuple[np.ndarra
     return key, date, seg
 
 
+def gen_join_training_table_device(rng: np.random.Generator, n: int):
+    """The same family of build sides as gen_join_training_table, generated on
+    the device (seeded from `rng`) so that tables of tens of millions of rows
+    cost milliseconds."""
+    import torch
+
+    from .datagen import DATE_HI, DATE_LO
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(int(rng.integers(1 << 62)))
+    key = (torch.randperm(n, generator=g, device="cuda") + 1).to(torch.int32)
+    span = DATE_HI - DATE_LO
+    if rng.random() < 0.5:
+        date = torch.randint(DATE_LO, DATE_HI + 1, (n,), generator=g, device="cuda", dtype=torch.int32)
+    else:
+        a, b = float(rng.uniform(0.5, 3)), float(rng.uniform(0.5, 3))
+        # Beta(a, b) as X / (X + Y) with X ~ Gamma(a), Y ~ Gamma(b) (torch's gamma sampler takes no generator,
+        # so the uniform draws are transformed instead: inverse-CDF of the beta is not closed-form, the
+        # gamma route is seeded through the global device generator below).
+        torch.cuda.manual_seed(int(rng.integers(1 << 62)))
+        x = torch._standard_gamma(torch.full((n,), a, device="cuda"))
+        y = torch._standard_gamma(torch.full((n,), b, device="cuda"))
+        date = (DATE_LO + span * (x / (x + y))).to(torch.int32)
+    k = int(rng.integers(2, 9))
+    if rng.random() < 0.5:
+        seg = torch.randint(0, k, (n,), generator=g, device="cuda", dtype=torch.int32)
+    else:
+        w = torch.arange(1, k + 1, dtype=torch.float64, device="cuda").pow(-float(rng.uniform(0.5, 2.0)))
+        seg = torch.multinomial(w, n, replacement=True, generator=g).to(torch.int32)
+    if rng.random() < 0.5:  # correlate segment with date
+        bucket = ((date.to(torch.int64) - DATE_LO) * k // (span + 1)) % k
+        noisy = torch.rand(n, generator=g, device="cuda") < float(rng.uniform(0.0, 0.5))
+        seg = torch.where(noisy, seg, bucket.to(torch.int32))
+    return key, date, seg.to(torch.uint8)
+
+
 def make_join_training_set(engine, n_tables: int = 24, preds_per_table: int = 40, seed: int = 1234,
-                           n_min: int = 20_000, n_max: int = 2_000_000):
+                           n_min: int = 20_000, n_max: int = 2_000_000, device_gen: bool = False):
     """(features, log1p(exact qualifying rows), independence estimates): the
-    exact counts come from the plain GPU pipeline's count kernel (K7)."""
+    exact counts come from the plain GPU pipeline's count kernel (K7).
+    device_gen draws the tables on the device (for large n_max)."""
     import torch
 
     from .datagen import DATE_HI, DATE_LO
@@ -203,8 +240,11 @@ def make_join_training_set(engine, n_tables: int = 24, preds_per_table: int = 40
     cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
     for _ in range(n_tables):
         n = int(math.exp(rng.uniform(math.log(n_min), math.log(n_max))))
-        key, date, seg = gen_join_training_table(rng, n)
-        dk, dd, ds = (torch.from_numpy(a).cuda() for a in (key, date, seg))
+        if device_gen:
+            dk, dd, ds = gen_join_training_table_device(rng, n)
+        else:
+            key, date, seg = gen_join_training_table(rng, n)
+            dk, dd, ds = (torch.from_numpy(a).cuda() for a in (key, date, seg))
         st = join_table_stats(engine.ctx, dk, dd, ds, n)
         for _ in range(preds_per_table):
             d = int(rng.integers(DATE_LO, DATE_HI + 2))
@@ -225,6 +265,30 @@ def q_error(pred, true) -> np.ndarray:
     return np.maximum(p / t, t / p)
 
 
+def split_holdout(n: int, frac: float = 0.2, seed: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Seeded (train, holdout) index split."""
+    idx = np.random.default_rng(seed).permutation(n)
+    k = int(round(n * (1.0 - frac)))
+    return idx[:k], idx[k:]
+
+
+def calibrate_margin(mlp: Mlp, pred_counts: np.ndarray, exact_counts: np.ndarray, quantile: float = 0.9,
+                     output: int = 0) -> float:
+    """Safety margin from held-out data: the `quantile` of exact / predicted
+    (at least 1).  The margin is folded into the network itself -- log(margin)
+    is added to the output's final bias, so every later prediction (host or
+    device) comes out about `margin` times larger.  A table sized from an
+    under-prediction runs at high load (long probe chains) or overflows and is
+    rerun, while an over-prediction only costs memory, so sizing from an upper
+    quantile is the cheaper side to err on."""
+    ratio = np.maximum(np.asarray(exact_counts, np.float64), 1.0) / np.maximum(np.asarray(pred_counts, np.float64), 1.0)
+    m = float(max(1.0, np.quantile(ratio, quantile))) if len(ratio) else 1.0
+    p = mlp.get_params()
+    p[len(p) - mlp.O + output] += math.log(m)
+    mlp.set_params(p)
+    return m
+
+
 class JoinSizer:
     """Trained join-build sizer: features -> predicted qualifying build rows,
     written on the device where the presized join reads it."""
@@ -232,6 +296,12 @@ class JoinSizer:
     def __init__(self, engine, seed: int = 7):
         self.engine = engine
         self.mlp = Mlp(engine.ctx, JOIN_FEATURES, 1, seed)
+        self.margin = 1.0
+
+    def calibrate(self, x, t, quantile: float = 0.9) -> float:
+        """Scales later predictions by the held-out quantile of exact / predicted."""
+        self.margin = calibrate_margin(self.mlp, self.predict_host(x), np.expm1(np.asarray(t)[:, 0]), quantile)
+        return self.margin
 
     def fit(self, x, t, epochs: int = 3000, lr: float = 2e-3) -> float:
         return self.mlp.train(x, t, epochs, lr)
@@ -300,9 +370,10 @@ def groupby_features(st: GroupByTableStats, cat_set, year_lo: int, year_hi: int)
 
 
 def make_groupby_training_set(engine, n_tables: int = 16, preds_per_table: int = 30, seed: int = 77,
-                              nb_min: int = 100_000, nb_max: int = 4_000_000):
+                              nb_min: int = 100_000, nb_max: int = 4_000_000, device_gen: bool = False):
     """(features, [log1p(groups), log1p(joined)], naive estimates): exact targets
-    from the plain GPU pipeline's pre-pass (bo_groupby_distinct_device)."""
+    from the plain GPU pipeline's pre-pass (bo_groupby_distinct_device).
+    device_gen draws the tables on the device (for large nb_max)."""
     import torch
 
     from .datagen import GroupByInput, gen_groupby
@@ -314,9 +385,17 @@ def make_groupby_training_set(engine, n_tables: int = 16, preds_per_table: int =
         n_b = int(math.exp(rng.uniform(math.log(nb_min), math.log(nb_max))))
         n_a = max(1000, int(n_b * rng.uniform(0.02, 0.2)))
         n_c = max(1000, int(n_b * rng.uniform(0.05, 0.3)))
-        g = gen_groupby(n_a, n_b, n_c, seed=int(rng.integers(1 << 30)), s_a=float(rng.uniform(0.7, 1.4)),
-                        s_c=float(rng.uniform(0.5, 1.2)))
-        dev = engine.groupby_to_device(g)
+        s_a, s_c = float(rng.uniform(0.7, 1.4)), float(rng.uniform(0.5, 1.2))
+        tseed = int(rng.integers(1 << 30))
+        if device_gen:
+            from .batching import groupby_tables_device
+
+            dev = groupby_tables_device(n_a, n_b, n_c, tseed, s_a, s_c)
+            g = GroupByInput(np.zeros(n_a, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32),
+                             np.zeros(0, np.uint16), np.zeros(0, np.int32), np.zeros(0, np.uint16), 0, 0)
+        else:
+            g = gen_groupby(n_a, n_b, n_c, seed=tseed, s_a=s_a, s_c=s_c)
+            dev = engine.groupby_to_device(g)
         st = groupby_table_stats(engine.ctx, dev, n_a, n_b, n_c)
         for _ in range(preds_per_table):
             k = int(rng.integers(1, 17))
@@ -341,6 +420,13 @@ class GroupBySizer:
     def __init__(self, engine, seed: int = 9):
         self.engine = engine
         self.mlp = Mlp(engine.ctx, GB_FEATURES, 2, seed)
+        self.margin = 1.0
+
+    def calibrate(self, x, t, quantile: float = 0.9) -> float:
+        """Scales later group-count predictions by the held-out quantile of
+        exact / predicted."""
+        self.margin = calibrate_margin(self.mlp, self.predict_host(x)[:, 0], np.expm1(np.asarray(t)[:, 0]), quantile)
+        return self.margin
 
     def fit(self, x, t, epochs: int = 3000, lr: float = 2e-3) -> float:
         return self.mlp.train(x, t, epochs, lr)

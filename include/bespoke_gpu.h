@@ -359,7 +359,7 @@ int bo_radix_sort_pairs_host(bo_ctx* ctx, uint64_t* keys, uint32_t* vals, int64_
 
 typedef struct bo_batch_instance {
   int32_t kind;            /* BO_BATCH_* */
-  int32_t tile_rows;       /* rows per work item; 0 = library default */
+  int32_t tile_rows;       /* largest rows per work item (tiles are smaller for small stages); 0 = default */
   float predicted;         /* join: qualifying build rows; group-by: groups; <= 0 sizes for the upper bound */
   float presize_factor;    /* slots per predicted row; 0 = 2.5 */
   /* scan-agg (wide layout) */
