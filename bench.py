@@ -384,7 +384,8 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     # ---- the other configurations (rank 0; extra keys of the same line)
     extra = {}
     if rank == 0 and args.sections != "none":
-        wanted = ["scan_agg", "groupby", "batch"] if args.sections == "all" else args.sections.split(",")
+        wanted = (["scan_agg", "groupby", "batch", "serving"] if args.sections == "all"
+                  else args.sections.split(","))
         peak_gbs, _ = peaks()
         keep = {}
         for name in wanted:
@@ -396,6 +397,8 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
                     extra[name] = groupby_section(eng, stream, keep=keep)
                 elif name == "batch":
                     extra[name] = batch_section(eng, stream, K, sizer, keep.get("gb_sizer"))
+                elif name == "serving":
+                    extra[name] = serving_section(eng, stream, sizer, keep.get("gb_sizer"))
             except Exception as e:  # report, never lose the headline line
                 extra[name] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
             if name in extra:
@@ -677,6 +680,47 @@ def batch_section(eng, stream, K: int, join_sizer=None, gb_sizer=None) -> dict:
     return out
 
 
+def serving_section(eng, stream, join_sizer=None, gb_sizer=None, rates=(50, 500, 2000)) -> dict:
+    """Serving over device-resident tables scaled to a 60M-row fact table: a
+    Poisson stream per rate, served by continuous batching (2 concurrent batch
+    slots, admission by MLP-estimated HBM footprint) and by one pipeline per
+    launch (plain exact-count form); latency = completion - arrival."""
+    import torch
+
+    from bespokeolap_artifacts_b200 import batching as B
+    from bespokeolap_artifacts_b200 import serving as S
+
+    t_load = time.perf_counter()
+    tables = S.ServingTables.load(eng, 60_000_000, seed=11)
+    load_s = time.perf_counter() - t_load
+    tile = B.load_tile_table()
+    srv = S.BatchedServer(tables, n_slots=2, max_batch=16, pool_bytes=2 << 30, max_items=65536, workers_per_sm=1,
+                          join_sizer=join_sizer, gb_sizer=gb_sizer, tile_table=tile)
+    srv.serve(S.poisson_requests(1000.0, 24, seed=1))  # warm-up: plans, graphs, solo paths
+    S.serve_one_per_launch(eng, tables, S.poisson_requests(1000.0, 6, seed=2))
+    out = {"tables": "fact 60M rows; join build 15M x probe 60M; group-by A 25M, B 60M, C 40M (device-resident)",
+           "load_s": round(load_s, 2), "slots": 2, "max_batch": 16, "pool_bytes_per_slot": 2 << 30,
+           "rates": {}}
+    for rate in rates:
+        n = int(min(2000, max(100, rate)))
+        rb = S.poisson_requests(float(rate), n, seed=rate)
+        rp = S.poisson_requests(float(rate), n, seed=rate)
+        l0 = srv.launches
+        srv.serve(rb)
+        launches = srv.launches - l0
+        S.serve_one_per_launch(eng, tables, rp)
+        same = sum(B.same_answer(a.result, b.result) for a, b in zip(rb, rp))
+        sb, sp = S.latency_stats(rb), S.latency_stats(rp)
+        out["rates"][str(rate)] = {
+            "batched": sb, "one_per_launch": sp, "p99_cut": sp["p99_ms"] / sb["p99_ms"],
+            "batch_launches": launches, "reruns": sum(r.result.get("reruns", 0) for r in rb),
+            "answers_identical": f"{same}/{n}"}
+    srv.close()
+    del tables
+    torch.cuda.empty_cache()
+    return out
+
+
 def cpu_baseline(j) -> dict:
     """The reference's run_q3 (compiled unchanged into oracle/_ref) on the same
     input mapped onto its tables, on one host core (the reference pins queries
@@ -762,7 +806,7 @@ def main():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--sections", default="all",
                     help="other configurations reported beside the headline: all, none, or a comma list of "
-                         "scan_agg,groupby,batch")
+                         "scan_agg,groupby,batch,serving")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))

@@ -147,6 +147,13 @@ class Batch:
     def launch(self) -> None:
         self.engine.ctx.call("bo_batch_launch", self.handle)
 
+    def done(self) -> bool:
+        """Non-blocking: has the last launch finished?"""
+        rc = int(self._lib.bo_batch_done(self.handle))
+        if rc < 0:
+            raise N.BoError(rc, "bo_batch_done")
+        return rc == 1
+
     def last_ms(self) -> float:
         return float(self._lib.bo_batch_last_ms(self.handle))
 

@@ -1638,6 +1638,17 @@ int bo_batch_results(bo_ctx* ctx, bo_batch* b, bo_batch_result* out_host) {
   return BO_OK;
 }
 
+int bo_batch_done(const bo_batch* b) {
+  if (!b || !b->launched) return BO_ERR_INVALID;
+  const cudaError_t e = cudaEventQuery(b->ev1);
+  if (e == cudaSuccess) return 1;
+  if (e == cudaErrorNotReady) {
+    cudaGetLastError();  // not an error: clear it
+    return 0;
+  }
+  return BO_ERR_CUDA;
+}
+
 float bo_batch_last_ms(const bo_batch* b) {
   if (!b || !b->launched) return -1.0f;
   float ms = -1.0f;

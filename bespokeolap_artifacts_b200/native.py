@@ -257,6 +257,7 @@ _SIGNATURES = {
     "bo_batch_launch": (C.c_int, [_P, _P]),
     "bo_batch_results": (C.c_int, [_P, _P, C.POINTER(BatchResult)]),
     "bo_batch_last_ms": (C.c_float, [_P]),
+    "bo_batch_done": (C.c_int, [_P]),
     "bo_batch_num_items": (C.c_int32, [_P]),
     "bo_batch_destroy": (None, [_P]),
     "bo_join_probe_device": (C.c_int, [_P, C.POINTER(JoinProbeCols), _P]),

@@ -1,0 +1,253 @@
+"""Serving loop over device-resident tables with continuous batching.
+
+Requests (scan-agg, join or group-by queries with their own predicate
+constants) arrive as a Poisson stream.  The server keeps a FIFO of arrived
+requests and several batch slots -- each its own engine context (CUDA stream)
+and a re-plannable persistent-kernel batch with a fixed table pool.  Whenever a
+slot is free and requests are waiting, it admits requests in arrival order
+while their tables, sized from the MLP predictions (the calibrated sizers),
+fit the slot's HBM pool and work-item budget, re-plans the batch in place and
+launches it; slots run concurrently on the device, so requests that arrive
+while others are on the GPU start as soon as a slot and memory free up.  A
+finished slot's results are read (an instance whose presized table overflowed
+is rerun exactly) and the slot takes the next requests.
+
+The baseline runs the same arrival stream one pipeline per launch: each
+request alone, in arrival order, through the plain exact-count entry points.
+
+The reference serves one query per call (bespoke_tpch/query_impl.cpp:159-388);
+this layer has no reference counterpart.  Every served answer must equal the
+request's solo answer (tests/test_serving_gpu.py).
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import batching as B
+from . import native as N
+from .datagen import DATE_HI, DATE_LO
+
+KIND_NAMES = B.KINDS
+
+
+# ----------------------------------------------------------------- tables ---
+@dataclass
+class ServingTables:
+    """The device-resident tables every request reads, plus their load-time
+    statistics (sketches) for the sizers."""
+    fact: dict
+    join: dict
+    gb: dict
+    join_stats: object = None
+    gb_stats: object = None
+
+    @classmethod
+    def load(cls, engine, fact_rows: int = 60_000_000, seed: int = 0) -> "ServingTables":
+        """fact_rows fact rows (scan-agg distributions); a join with a build
+        side of fact_rows / 4 rows (ten times the 1.5M build of the join
+        workload at 60M) and a probe side of fact_rows rows; a group-by with B
+        = fact_rows rows and A, C ten times the 2.5M / 4M of the group-by
+        workload at 60M (scaled down proportionally for smaller fact_rows)."""
+        from . import learned as L
+
+        f = B.fact_instance(fact_rows, seed + 1).cols
+        j = B.join_instance(fact_rows, seed + 2, n_build=max(1, fact_rows // 4)).cols
+        scale = fact_rows / 60_000_000
+        n_a, n_c = max(16, int(25_000_000 * scale)), max(16, int(40_000_000 * scale))
+        g = B.groupby_tables_device(n_a, fact_rows, n_c, seed + 3)
+        t = cls(f, j, g)
+        t.join_stats = L.join_table_stats(engine.ctx, j["b_key"], j["b_date"], j["b_seg"], int(j["b_key"].numel()))
+        t.gb_stats = L.groupby_table_stats(engine.ctx, g, n_a, fact_rows, n_c)
+        return t
+
+
+# --------------------------------------------------------------- requests ---
+@dataclass
+class Request:
+    rid: int
+    kind: int
+    params: dict
+    arrival: float                      # seconds from the start of the stream
+    predicted: float = 0.0              # sizing prediction (join rows / groups)
+    result: dict | None = None
+    done: float = math.nan              # completion time, same clock as arrival
+
+    @property
+    def latency_ms(self) -> float:
+        return (self.done - self.arrival) * 1e3
+
+
+def poisson_requests(rate_qps: float, n: int, seed: int = 0, mix=(1, 1, 1)) -> list[Request]:
+    """n requests with exponential inter-arrival times at rate_qps, the three
+    pipeline shapes drawn with weights `mix`, predicate constants seeded."""
+    rng = np.random.default_rng(seed)
+    kinds = (N.BATCH_SCAN_AGG, N.BATCH_JOIN, N.BATCH_GROUPBY)
+    w = np.asarray(mix, np.float64) / float(sum(mix))
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += float(rng.exponential(1.0 / rate_qps))
+        kind = int(kinds[int(rng.choice(3, p=w))])
+        if kind == N.BATCH_SCAN_AGG:
+            p = {"cutoff": int(rng.integers(DATE_LO + 365, DATE_HI + 1)), "n_flag_a": 3, "n_flag_b": 2}
+        elif kind == N.BATCH_JOIN:
+            p = {"date_lt": int(rng.integers(DATE_LO + 100, DATE_HI + 1)), "seg_eq": int(rng.integers(0, 5))}
+        else:
+            y0 = int(rng.integers(1900, 2010))
+            p = {"cat_set": sorted(int(v) for v in rng.choice(113, size=8, replace=False)), "year_lo": y0,
+                 "year_hi": int(min(2020, y0 + int(rng.integers(5, 30)))), "k": 10}
+        out.append(Request(i, kind, p, t))
+    return out
+
+
+def instance_of(tables: ServingTables, r: Request, tile_table: B.TileTable | None = None) -> B.Instance:
+    """The batch instance of a request over the shared device tables."""
+    if r.kind == N.BATCH_SCAN_AGG:
+        cols, rows = tables.fact, int(tables.fact["ship_date"].numel())
+        params = dict(r.params)
+    elif r.kind == N.BATCH_JOIN:
+        cols, rows = tables.join, int(tables.join["p_fk"].numel())
+        params = dict(r.params)
+    else:
+        cols = {k: v for k, v in tables.gb.items() if k != "a_id_max"}
+        rows = int(cols["b_a"].numel())
+        params = dict(r.params, a_id_max=int(tables.gb["a_id_max"]))
+    inst = B.Instance(r.kind, rows, cols, params, predicted=r.predicted)
+    if tile_table is not None:
+        inst.tile_rows = tile_table.tile_for(r.kind, rows)
+    return inst
+
+
+def predict_requests(tables: ServingTables, reqs: list[Request], join_sizer=None, gb_sizer=None) -> None:
+    """Fills r.predicted from the sizers (one device inference per kind)."""
+    from . import learned as L
+
+    js = [r for r in reqs if r.kind == N.BATCH_JOIN]
+    gs = [r for r in reqs if r.kind == N.BATCH_GROUPBY]
+    if js and join_sizer is not None:
+        x = np.stack([L.join_features(tables.join_stats, r.params["date_lt"], r.params["seg_eq"]) for r in js])
+        for r, p in zip(js, join_sizer.predict_host(x)):
+            r.predicted = float(p)
+    if gs and gb_sizer is not None:
+        x = np.stack([L.groupby_features(tables.gb_stats, r.params["cat_set"], r.params["year_lo"],
+                                         r.params["year_hi"]) for r in gs])
+        for r, p in zip(gs, gb_sizer.predict_host(x)[:, 0]):
+            r.predicted = float(p)
+
+
+def admit(pending: deque, footprints: dict, max_batch: int, pool_bytes: int, max_items: int) -> list:
+    """Takes requests from the head of `pending` (arrival order) while the
+    batch stays within max_batch requests, pool_bytes of tables and max_items
+    work items.  footprints[rid] = (table bytes, items).  A request whose
+    footprint alone exceeds the slot is admitted alone (its tables are then
+    sized for the upper bound by the caller) so nothing starves."""
+    out, tb, it = [], 0, 0
+    while pending and len(out) < max_batch:
+        r = pending[0]
+        b, i = footprints[r.rid]
+        if out and (tb + b > pool_bytes or it + i > max_items):
+            break
+        out.append(pending.popleft())
+        tb += b
+        it += i
+    return out
+
+
+# ----------------------------------------------------------------- server ---
+@dataclass
+class Slot:
+    engine: object
+    batch: B.Batch
+    reqs: list = field(default_factory=list)
+    busy: bool = False
+
+
+class BatchedServer:
+    """Continuous batching over `n_slots` concurrently running batch slots."""
+
+    def __init__(self, tables: ServingTables, n_slots: int = 2, max_batch: int = 16,
+                 pool_bytes: int = 2 << 30, max_items: int = 65536, workers_per_sm: int = 1,
+                 join_sizer=None, gb_sizer=None, tile_table: B.TileTable | None = None):
+        from .engine import Engine
+
+        self.tables = tables
+        self.max_batch, self.pool_bytes, self.max_items = max_batch, pool_bytes, max_items
+        self.join_sizer, self.gb_sizer = join_sizer, gb_sizer
+        self.tile_table = tile_table
+        self.slots = []
+        for _ in range(n_slots):
+            e = Engine(0)
+            self.slots.append(Slot(e, B.Batch.pool(e, max_batch, max_items, pool_bytes, workers_per_sm)))
+        self.launches = 0
+
+    def close(self):
+        for s in self.slots:
+            s.batch.close()
+            s.engine.close()
+
+    def _footprint(self, r: Request) -> tuple[int, int]:
+        return B.footprint(instance_of(self.tables, r, self.tile_table))
+
+    def serve(self, requests: list[Request]) -> list[Request]:
+        """Runs the arrival stream in real time; fills each request's result
+        and completion time."""
+        pending: deque = deque()
+        foot: dict = {}
+        n, i, finished = len(requests), 0, 0
+        t0 = time.perf_counter()
+        while finished < n:
+            now = time.perf_counter() - t0
+            arrived = []
+            while i < n and requests[i].arrival <= now:
+                arrived.append(requests[i])
+                i += 1
+            if arrived:
+                predict_requests(self.tables, arrived, self.join_sizer, self.gb_sizer)
+                for r in arrived:
+                    foot[r.rid] = self._footprint(r)
+                    pending.append(r)
+            for s in self.slots:
+                if s.busy and s.batch.done():
+                    res = s.batch.results()
+                    t_done = time.perf_counter() - t0
+                    for r, x in zip(s.reqs, res):
+                        r.result, r.done = x, t_done
+                    finished += len(s.reqs)
+                    s.reqs, s.busy = [], False
+            for s in self.slots:
+                if not s.busy and pending:
+                    reqs = admit(pending, foot, self.max_batch, self.pool_bytes, self.max_items)
+                    insts = [instance_of(self.tables, r, self.tile_table) for r in reqs]
+                    tb = sum(foot[r.rid][0] for r in reqs)
+                    if tb > self.pool_bytes:  # a single request above the pool: upper-bound tables do not fit
+                        raise RuntimeError(f"request {reqs[0].rid} needs {tb} bytes of tables, slot holds "
+                                           f"{self.pool_bytes}")
+                    s.batch.update(insts)
+                    s.batch.launch()
+                    s.reqs, s.busy = reqs, True
+                    self.launches += 1
+        return requests
+
+
+def serve_one_per_launch(engine, tables: ServingTables, requests: list[Request]) -> list[Request]:
+    """Baseline: each request alone, in arrival order, plain exact-count form."""
+    t0 = time.perf_counter()
+    for r in requests:
+        while time.perf_counter() - t0 < r.arrival:
+            pass
+        r.result = B.solo_result(engine, instance_of(tables, r))
+        r.done = time.perf_counter() - t0
+    return requests
+
+
+def latency_stats(requests: list[Request]) -> dict:
+    lat = np.array([r.latency_ms for r in requests])
+    span = max(r.done for r in requests) - min(r.arrival for r in requests)
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "p99_9_ms": float(np.percentile(lat, 99.9)), "mean_ms": float(lat.mean()),
+            "qps": len(requests) / span if span > 0 else math.inf, "requests": len(requests)}

@@ -415,6 +415,9 @@ int bo_batch_launch(bo_ctx* ctx, bo_batch* batch);
 /* Waits, copies every instance's result to the host and reruns any instance
  * whose presized table overflowed alone in the exact form. */
 int bo_batch_results(bo_ctx* ctx, bo_batch* batch, bo_batch_result* out_host);
+/* Non-blocking: 1 if the last launch has finished, 0 if it is still running,
+ * a negative status on error. */
+int bo_batch_done(const bo_batch* batch);
 /* Device time (ms) of the last launch, from events around the graph. */
 float bo_batch_last_ms(const bo_batch* batch);
 int32_t bo_batch_num_items(const bo_batch* batch);
