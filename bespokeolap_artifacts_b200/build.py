@@ -87,6 +87,34 @@ def build_gpu_lib(force: bool = False, verbose: bool = False, ptxas_info: bool =
     return LIB_PATH
 
 
+HOST = PKG / "host"
+HOST_LIB = HOST / "libbespoke_tpch_gpu.so"
+HOST_DRIVER = HOST / "bespoke_tpch_gpu"
+
+
+def build_host(force: bool = False) -> Path | None:
+    """The drop-in C++ host (load / build / query over the C ABI) and a stand-in
+    driver executable, against the Arrow / Parquet C++ libraries that come
+    with pyarrow.  Skipped (None) when pyarrow is not importable."""
+    try:
+        import pyarrow as pa
+    except ImportError:
+        return None
+    inc, libdir = pa.get_include(), pa.get_library_dirs()[0]
+    srcs = [HOST / "tpch_gpu.cpp"]
+    deps = srcs + [HOST / "tpch_gpu.hpp", INCLUDE / "bespoke_gpu.h", LIB_PATH]
+    arrow = [f"-L{libdir}", "-l:libarrow.so.2400", "-l:libparquet.so.2400", f"-Wl,-rpath,{libdir}"]
+    if force or _stale(HOST_LIB, deps):
+        subprocess.run(["g++", "-std=c++20", "-O2", "-fPIC", "-shared", f"-I{INCLUDE}", f"-I{inc}", *map(str, srcs),
+                        f"-L{PKG}", "-lbespoke_gpu", f"-Wl,-rpath,{PKG}", *arrow, "-o", str(HOST_LIB)], check=True)
+    main = HOST / "driver_main.cpp"
+    if force or _stale(HOST_DRIVER, [main, HOST_LIB, HOST / "tpch_gpu.hpp"]):
+        subprocess.run(["g++", "-std=c++20", "-O2", f"-I{INCLUDE}", f"-I{inc}", str(main), f"-L{HOST}",
+                        "-lbespoke_tpch_gpu", f"-Wl,-rpath,{HOST}", f"-L{PKG}", "-lbespoke_gpu", f"-Wl,-rpath,{PKG}",
+                        *arrow, "-o", str(HOST_DRIVER)], check=True)
+    return HOST_LIB
+
+
 def build_oracle(force: bool = False) -> None:
     """Builds the CPU checker under ``oracle/`` (C restatement and, when the
     reference sources are present on this machine, the compiled reference)."""
@@ -97,6 +125,7 @@ def build_oracle(force: bool = False) -> None:
 
 def build_all(force: bool = False) -> None:
     build_gpu_lib(force=force)
+    build_host(force=force)
     build_oracle(force=force)
 
 

@@ -222,4 +222,12 @@ int bo_copy_d2h(bo_ctx* ctx, void* dst, const void* src, size_t bytes) {
 
 int64_t bo_launch_count(const bo_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
 
+int bo_check_errors(bo_ctx* ctx) {
+  BO_CHECK_CTX(ctx);
+  uint32_t bits = 0;
+  int rc = bo::consume_device_errors(ctx, &bits);
+  if (rc) return rc;
+  return bo::device_error_status(ctx, bits, "device");
+}
+
 }  // extern "C"

@@ -1,0 +1,247 @@
+// TPC-H Q3 over the storage-plan layout: run_q3 of bespoke_tpch/query_q3.cpp:153-365.
+//
+// The reference walks the orders sorted by date, takes the qualifying ones
+// (orderdate < D, customer in the segment; :207-322) and sums each one's
+// lineitems with shipdate > D through its CSR range (:219-260), then sorts all
+// resulting orders by revenue desc, orderdate asc (:348-355).  On the GPU the
+// same result comes from four data-parallel passes and a sort:
+//   cust   segment membership as a bitmap over custkey (:182-204);
+//   orders one 32-row bitmap word per warp iteration: orderdate < D and the
+//          customer's bit (:311-322); no atomics;
+//   lines  every lineitem with shipdate > D finds its order row through
+//          orderkey_to_row (the map the reference's CSR ranges are built from,
+//          bespoke_tpch/builder_impl.cpp:930-990) and, if that order
+//          qualifies, adds its discounted price and a count with 64-bit
+//          atomics (only the ~2% of lineitems that pass both filters do);
+//   compact orders with at least one such lineitem (`has_lineitem`, :248);
+//   sort   the onesweep radix sort twice, stable: by orderkey, then by
+//          (revenue desc, orderdate asc).  The reference's std::sort leaves
+//          rows equal in both keys in unspecified order; here they come out in
+//          orderkey order, a canonical form of the same result.
+#include <algorithm>
+
+#include "common.cuh"
+#include "context.cuh"
+
+namespace bo {
+namespace {
+
+constexpr int kQ3Block = 256;
+constexpr unsigned long long kRevBits = 47;  // revenue < 2^47 (checked) so (rev, date) packs into 63 bits
+
+__global__ void q3_cust_kernel(const int32_t* __restrict__ custkey, const uint16_t* __restrict__ seg, int64_t n,
+                               int32_t segment_code, int32_t bound, uint32_t* __restrict__ mask) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if ((int32_t)seg[i] != segment_code) continue;
+    const int32_t k = custkey[i];
+    if (k >= 0 && k < bound) atomicOr(mask + (k >> 5), 1u << (k & 31));
+  }
+}
+
+// Warp w of the grid owns order rows [32w, 32w + 32): one qualification word.
+__global__ void q3_orders_kernel(const int32_t* __restrict__ o_custkey, const int16_t* __restrict__ o_orderdate,
+                                 int64_t n, int16_t date_offset, int32_t bound, const uint32_t* __restrict__ mask,
+                                 uint32_t* __restrict__ qual) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 < n; w += warps) {
+    const int64_t i = w * 32 + lane;
+    bool q = false;
+    if (i < n && o_orderdate[i] < date_offset) {
+      const int32_t c = o_custkey[i];
+      q = c >= 0 && c < bound && ((mask[c >> 5] >> (c & 31)) & 1u);
+    }
+    const uint32_t word = __ballot_sync(0xffffffffu, q);
+    if (lane == 0) qual[w] = word;
+  }
+}
+
+__global__ void q3_lineitem_kernel(const int32_t* __restrict__ l_orderkey, const int16_t* __restrict__ l_shipdate,
+                                   const int32_t* __restrict__ l_dprice, int64_t n, int16_t date_offset,
+                                   const int32_t* __restrict__ key_to_row, int64_t n_map, int64_t n_orders,
+                                   const uint32_t* __restrict__ qual, unsigned long long* __restrict__ rev,
+                                   uint32_t* __restrict__ cnt) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (l_shipdate[i] <= date_offset) continue;
+    const int32_t key = l_orderkey[i];
+    if (key < 0 || (int64_t)key >= n_map) continue;
+    const int32_t row = key_to_row[key];
+    if (row < 0 || (int64_t)row >= n_orders) continue;
+    if (!((qual[row >> 5] >> (row & 31)) & 1u)) continue;
+    atomicAdd(rev + row, (unsigned long long)(int64_t)l_dprice[i]);
+    atomicAdd(cnt + row, 1u);
+  }
+}
+
+// Orders with a counted lineitem -> (orderkey, row) pairs; one reservation per block.
+__global__ void __launch_bounds__(kQ3Block) q3_compact_kernel(const uint32_t* __restrict__ cnt,
+                                                              const int32_t* __restrict__ o_orderkey, int64_t n,
+                                                              unsigned long long* __restrict__ keys,
+                                                              uint32_t* __restrict__ vals,
+                                                              unsigned long long* n_out) {
+  __shared__ uint32_t warp_off[kQ3Block / 32];
+  __shared__ unsigned long long base;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t b0 = (int64_t)blockIdx.x * kQ3Block; b0 < n; b0 += (int64_t)gridDim.x * kQ3Block) {
+    const int64_t i = b0 + threadIdx.x;
+    const bool keep = i < n && cnt[i] > 0u;
+    const uint32_t m = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) warp_off[warp] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < kQ3Block / 32; ++w) {
+        const uint32_t c = warp_off[w];
+        warp_off[w] = t;
+        t += c;
+      }
+      base = t ? atomicAdd(n_out, (unsigned long long)t) : 0ull;
+    }
+    __syncthreads();
+    if (keep) {
+      const unsigned long long pos = base + warp_off[warp] + __popc(m & ((1u << lane) - 1u));
+      keys[pos] = (unsigned long long)(uint32_t)o_orderkey[i];  // orderkey >= 0: it indexed the map
+      vals[pos] = (uint32_t)i;
+    }
+    __syncthreads();
+  }
+}
+
+// Second sort key in orderkey order: (2^47 - 1 - revenue) << 16 | (orderdate + 32768).
+__global__ void q3_key2_kernel(const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ rev,
+                               const int16_t* __restrict__ o_orderdate, const unsigned long long* n_out,
+                               unsigned long long* __restrict__ keys, uint32_t* err) {
+  const unsigned long long n = *n_out;
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t row = vals[i];
+    const unsigned long long r = rev[row];
+    if (r >> kRevBits) raise_error(err, kErrValueRange);
+    const unsigned long long inv = ((1ull << kRevBits) - 1ull) - (r & ((1ull << kRevBits) - 1ull));
+    keys[i] = (inv << 16) | (unsigned long long)(uint16_t)(o_orderdate[row] + 32768);
+  }
+}
+
+__global__ void q3_gather_kernel(const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ rev,
+                                 const int32_t* __restrict__ o_orderkey, const int16_t* __restrict__ o_orderdate,
+                                 const int32_t* __restrict__ o_shippriority, const unsigned long long* n_out,
+                                 bo_tpch_q3_row* __restrict__ out) {
+  const unsigned long long n = *n_out;
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t row = vals[i];
+    bo_tpch_q3_row r;
+    r.revenue_raw = (int64_t)rev[row];
+    r.orderkey = o_orderkey[row];
+    r.shippriority = o_shippriority ? o_shippriority[row] : 0;
+    r.orderdate_offset = o_orderdate[row];
+    r.pad0 = 0;
+    r.pad1 = 0;
+    out[i] = r;
+  }
+}
+
+template <class T>
+T* carve(char*& p, size_t count) {
+  T* r = reinterpret_cast<T*>(p);
+  p += (sizeof(T) * count + 255) & ~size_t(255);
+  return r;
+}
+
+int grid_of(bo_ctx* ctx, int64_t items) {
+  const int64_t need = (items + kQ3Block - 1) / kQ3Block;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)ctx->num_sms * 8));
+}
+
+}  // namespace
+}  // namespace bo
+
+using namespace bo;
+
+extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_offset, int32_t segment_code,
+                          bo_tpch_q3_row* out_host, int64_t max_rows, int64_t* n_rows) {
+  BO_CHECK_CTX(ctx);
+  if (!t || !n_rows || max_rows < 0 || (max_rows > 0 && !out_host))
+    return set_error(ctx, BO_ERR_INVALID, "q3: null argument");
+  if (t->n_customer < 0 || t->n_orders < 0 || t->n_lineitem < 0 || t->n_orderkey_map < 0 || t->custkey_bound < 0)
+    return set_error(ctx, BO_ERR_INVALID, "q3: negative size");
+  if (t->n_orders > 0xffffffffll) return set_error(ctx, BO_ERR_INVALID, "q3: more than 2^32 orders");
+  if ((t->n_customer > 0 && (!t->c_custkey || !t->c_mktsegment)) ||
+      (t->n_orders > 0 && (!t->o_orderkey || !t->o_custkey || !t->o_orderdate)) ||
+      (t->n_orderkey_map > 0 && !t->orderkey_to_row) ||
+      (t->n_lineitem > 0 && (!t->l_orderkey || !t->l_shipdate || !t->l_discounted_price)))
+    return set_error(ctx, BO_ERR_INVALID, "q3: null column");
+  *n_rows = 0;
+  const int64_t no = t->n_orders;
+  if (no == 0 || segment_code < 0) return BO_OK;  // no order can qualify (unknown segment: none, :176-183)
+  const int64_t mask_words = ((int64_t)t->custkey_bound + 31) / 32 + 1;
+  const int64_t qual_words = (no + 31) / 32;
+  size_t total = 0;
+  auto add = [&](size_t b) { total += (b + 255) & ~size_t(255); };
+  add(4 * (size_t)mask_words);
+  add(4 * (size_t)qual_words);
+  add(8 * (size_t)no);  // revenue
+  add(4 * (size_t)no);  // count
+  add(8 * (size_t)no);  // keys
+  add(4 * (size_t)no);  // vals
+  add(8 * (size_t)no);  // tmp keys
+  add(4 * (size_t)no);  // tmp vals
+  add(sizeof(bo_tpch_q3_row) * (size_t)no);
+  add(64);
+  void* base = nullptr;
+  int rc = region(ctx, "q3_ws", total, &base);
+  if (rc) return rc;
+  char* p = static_cast<char*>(base);
+  uint32_t* mask = carve<uint32_t>(p, (size_t)mask_words);
+  uint32_t* qual = carve<uint32_t>(p, (size_t)qual_words);
+  unsigned long long* rev = carve<unsigned long long>(p, (size_t)no);
+  uint32_t* cnt = carve<uint32_t>(p, (size_t)no);
+  unsigned long long* keys = carve<unsigned long long>(p, (size_t)no);
+  uint32_t* vals = carve<uint32_t>(p, (size_t)no);
+  unsigned long long* tkeys = carve<unsigned long long>(p, (size_t)no);
+  uint32_t* tvals = carve<uint32_t>(p, (size_t)no);
+  bo_tpch_q3_row* rows = carve<bo_tpch_q3_row>(p, (size_t)no);
+  unsigned long long* n_out = carve<unsigned long long>(p, 8);
+  // Scratch that accumulates starts at zero (the bitmaps are written whole or by atomicOr).
+  BO_CUDA(ctx, cudaMemsetAsync(mask, 0, 4 * (size_t)mask_words, ctx->stream));
+  BO_CUDA(ctx, cudaMemsetAsync(rev, 0, 8 * (size_t)no, ctx->stream));
+  BO_CUDA(ctx, cudaMemsetAsync(cnt, 0, 4 * (size_t)no, ctx->stream));
+  BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, 8, ctx->stream));
+  if (t->n_customer > 0) {
+    q3_cust_kernel<<<grid_of(ctx, t->n_customer), kQ3Block, 0, ctx->stream>>>(
+        t->c_custkey, t->c_mktsegment, t->n_customer, segment_code, t->custkey_bound, mask);
+    if ((rc = after_launch(ctx, "q3_cust_kernel"))) return rc;
+  }
+  q3_orders_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(t->o_custkey, t->o_orderdate, no, date_offset,
+                                                                     t->custkey_bound, mask, qual);
+  if ((rc = after_launch(ctx, "q3_orders_kernel"))) return rc;
+  if (t->n_lineitem > 0 && t->n_orderkey_map > 0) {
+    q3_lineitem_kernel<<<grid_of(ctx, t->n_lineitem), kQ3Block, 0, ctx->stream>>>(
+        t->l_orderkey, t->l_shipdate, t->l_discounted_price, t->n_lineitem, date_offset, t->orderkey_to_row,
+        t->n_orderkey_map, no, qual, rev, cnt);
+    if ((rc = after_launch(ctx, "q3_lineitem_kernel"))) return rc;
+  }
+  q3_compact_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(cnt, t->o_orderkey, no, keys, vals, n_out);
+  if ((rc = after_launch(ctx, "q3_compact_kernel"))) return rc;
+  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, no, 0, 32, n_out))) return rc;
+  q3_key2_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(vals, rev, t->o_orderdate, n_out, keys,
+                                                                   ctx->d_err);
+  if ((rc = after_launch(ctx, "q3_key2_kernel"))) return rc;
+  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, no, 0, 64, n_out))) return rc;
+  q3_gather_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(vals, rev, t->o_orderkey, t->o_orderdate,
+                                                                     t->o_shippriority, n_out, rows);
+  if ((rc = after_launch(ctx, "q3_gather_kernel"))) return rc;
+  unsigned long long n = 0;
+  BO_CUDA(ctx, cudaMemcpyAsync(&n, n_out, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  uint32_t bits = 0;
+  if ((rc = consume_device_errors(ctx, &bits))) return rc;  // synchronises the stream
+  if ((rc = device_error_status(ctx, bits, "q3"))) return rc;
+  *n_rows = (int64_t)n;
+  const int64_t m = std::min<int64_t>((int64_t)n, max_rows);
+  if (m > 0) {
+    BO_CUDA(ctx, cudaMemcpyAsync(out_host, rows, sizeof(bo_tpch_q3_row) * (size_t)m, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return BO_OK;
+}

@@ -1,0 +1,576 @@
+// Drop-in GPU host for the reference's TPC-H engine: load / build / query.
+// See tpch_gpu.hpp for the contract.
+#include "tpch_gpu.hpp"
+
+#include <arrow/api.h>
+#include <arrow/io/file.h>
+#include <parquet/arrow/reader.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <numeric>
+#include <sstream>
+#include <stdexcept>
+#include <unordered_map>
+
+namespace bo_tpch {
+
+// Days since 1970-01-01 of a proleptic Gregorian date (H. Hinnant's
+// days_from_civil algorithm) and its inverse.
+int64_t days_from_civil(int64_t y, unsigned m, unsigned d) {
+  y -= m <= 2;
+  const int64_t era = (y >= 0 ? y : y - 399) / 400;
+  const unsigned yoe = static_cast<unsigned>(y - era * 400);
+  const unsigned doy = (153 * (m > 2 ? m - 3 : m + 9) + 2) / 5 + d - 1;
+  const unsigned doe = yoe * 365 + yoe / 4 - yoe / 100 + doy;
+  return era * 146097 + static_cast<int64_t>(doe) - 719468;
+}
+
+void civil_from_days(int64_t z, int& y, unsigned& m, unsigned& d) {
+  z += 719468;
+  const int64_t era = (z >= 0 ? z : z - 146096) / 146097;
+  const unsigned doe = static_cast<unsigned>(z - era * 146097);
+  const unsigned yoe = (doe - doe / 1460 + doe / 36524 - doe / 146096) / 365;
+  const int64_t yy = static_cast<int64_t>(yoe) + era * 400;
+  const unsigned doy = doe - (365 * yoe + yoe / 4 - yoe / 100);
+  const unsigned mp = (5 * doy + 2) / 153;
+  d = doy - (153 * mp + 2) / 5 + 1;
+  m = mp < 10 ? mp + 3 : mp - 9;
+  y = static_cast<int>(yy + (m <= 2));
+}
+
+namespace {
+
+constexpr int32_t kPriceScale = 100;
+constexpr int32_t kDiscountScale = 100;
+
+void check(bo_ctx* ctx, int rc, const char* what) {
+  if (rc != BO_OK) {
+    throw std::runtime_error(std::string(what) + ": " + (ctx ? bo_last_error(ctx) : "no context") + " (status " +
+                             std::to_string(rc) + ")");
+  }
+}
+
+// ------------------------------------------------------------- arrow input --
+std::shared_ptr<arrow::Table> read_parquet(const std::string& path) {
+  auto file = arrow::io::ReadableFile::Open(path);
+  if (!file.ok()) throw std::runtime_error("cannot open " + path + ": " + file.status().ToString());
+  auto reader = parquet::arrow::OpenFile(*file, arrow::default_memory_pool());
+  if (!reader.ok()) throw std::runtime_error("cannot read parquet " + path + ": " + reader.status().ToString());
+  auto table = (*reader)->ReadTable();
+  if (!table.ok()) throw std::runtime_error("cannot read table " + path + ": " + table.status().ToString());
+  return *table;
+}
+
+std::shared_ptr<arrow::ChunkedArray> column(const ParquetTables::ArrowTable& t, const char* name) {
+  auto c = t ? t->GetColumnByName(name) : nullptr;
+  if (!c) throw std::runtime_error(std::string("Missing column: ") + name);
+  return c;
+}
+
+template <class ArrayT, class T, class F>
+void each(const std::shared_ptr<arrow::ChunkedArray>& c, std::vector<T>& out, F conv) {
+  for (const auto& chunk : c->chunks()) {
+    const auto a = std::static_pointer_cast<ArrayT>(chunk);
+    for (int64_t i = 0; i < a->length(); ++i) out.push_back(a->IsNull(i) ? T{} : conv(a->Value(i)));
+  }
+}
+
+// Integer keys (int32 / int64 columns), nulls as 0.
+std::vector<int32_t> int_values(const std::shared_ptr<arrow::ChunkedArray>& c) {
+  std::vector<int32_t> out;
+  out.reserve(c->length());
+  switch (c->type()->id()) {
+    case arrow::Type::INT32:
+      each<arrow::Int32Array>(c, out, [](int32_t v) { return v; });
+      break;
+    case arrow::Type::INT64:
+      each<arrow::Int64Array>(c, out, [](int64_t v) { return static_cast<int32_t>(v); });
+      break;
+    default:
+      throw std::runtime_error("Unsupported integer column type: " + c->type()->ToString());
+  }
+  return out;
+}
+
+// Decimal values scaled to integers: llround(value * scale); a decimal column
+// goes through its text form and a double, as the reference's builder converts
+// it (bespoke_tpch/builder_impl.cpp:287-338), so both round identically.
+std::vector<int32_t> scaled_values(const std::shared_ptr<arrow::ChunkedArray>& c, int32_t scale) {
+  std::vector<int32_t> out;
+  out.reserve(c->length());
+  const double s = static_cast<double>(scale);
+  auto r = [s](double v) { return static_cast<int32_t>(std::llround(v * s)); };
+  switch (c->type()->id()) {
+    case arrow::Type::DOUBLE:
+      each<arrow::DoubleArray>(c, out, [&](double v) { return r(v); });
+      break;
+    case arrow::Type::FLOAT:
+      each<arrow::FloatArray>(c, out, [&](float v) { return r(static_cast<double>(v)); });
+      break;
+    case arrow::Type::INT32:
+      each<arrow::Int32Array>(c, out, [&](int32_t v) { return r(static_cast<double>(v)); });
+      break;
+    case arrow::Type::INT64:
+      each<arrow::Int64Array>(c, out, [&](int64_t v) { return r(static_cast<double>(v)); });
+      break;
+    case arrow::Type::DECIMAL128:
+      for (const auto& chunk : c->chunks()) {
+        const auto a = std::static_pointer_cast<arrow::Decimal128Array>(chunk);
+        for (int64_t i = 0; i < a->length(); ++i) out.push_back(a->IsNull(i) ? 0 : r(std::stod(a->FormatValue(i))));
+      }
+      break;
+    case arrow::Type::DECIMAL256:
+      for (const auto& chunk : c->chunks()) {
+        const auto a = std::static_pointer_cast<arrow::Decimal256Array>(chunk);
+        for (int64_t i = 0; i < a->length(); ++i) out.push_back(a->IsNull(i) ? 0 : r(std::stod(a->FormatValue(i))));
+      }
+      break;
+    default:
+      throw std::runtime_error("Unsupported numeric column type: " + c->type()->ToString());
+  }
+  return out;
+}
+
+// Dates as int16 day offsets from base_days (DATE32 / DATE64; nulls as 0).
+std::vector<int16_t> date_offsets(const std::shared_ptr<arrow::ChunkedArray>& c, int32_t base_days) {
+  std::vector<int16_t> out;
+  out.reserve(c->length());
+  for (const auto& chunk : c->chunks()) {
+    if (chunk->type_id() == arrow::Type::DATE32) {
+      const auto a = std::static_pointer_cast<arrow::Date32Array>(chunk);
+      for (int64_t i = 0; i < a->length(); ++i)
+        out.push_back(a->IsNull(i) ? int16_t(0) : static_cast<int16_t>(a->Value(i) - base_days));
+    } else if (chunk->type_id() == arrow::Type::DATE64) {
+      const auto a = std::static_pointer_cast<arrow::Date64Array>(chunk);
+      for (int64_t i = 0; i < a->length(); ++i)
+        out.push_back(a->IsNull(i) ? int16_t(0)
+                                   : static_cast<int16_t>(static_cast<int32_t>(a->Value(i) / 86400000) - base_days));
+    } else {
+      throw std::runtime_error("Unsupported date type: " + chunk->type()->ToString());
+    }
+  }
+  return out;
+}
+
+// Dictionary codes in first-appearance order (strings, large strings or
+// dictionary-encoded strings; nulls as the empty string).
+std::vector<uint16_t> dictionary_codes(const std::shared_ptr<arrow::ChunkedArray>& c, Dictionary& dict) {
+  std::vector<uint16_t> codes;
+  codes.reserve(c->length());
+  std::unordered_map<std::string, uint16_t> ids;
+  auto add = [&](const std::string& v) {
+    auto it = ids.find(v);
+    if (it != ids.end()) {
+      codes.push_back(it->second);
+      return;
+    }
+    if (dict.values.size() > 0xffff) throw std::runtime_error("Dictionary column exceeds uint16_t capacity");
+    const uint16_t id = static_cast<uint16_t>(dict.values.size());
+    ids.emplace(v, id);
+    dict.values.push_back(v);
+    codes.push_back(id);
+  };
+  for (const auto& chunk : c->chunks()) {
+    switch (chunk->type_id()) {
+      case arrow::Type::STRING: {
+        const auto a = std::static_pointer_cast<arrow::StringArray>(chunk);
+        for (int64_t i = 0; i < a->length(); ++i) add(a->IsNull(i) ? std::string() : a->GetString(i));
+        break;
+      }
+      case arrow::Type::LARGE_STRING: {
+        const auto a = std::static_pointer_cast<arrow::LargeStringArray>(chunk);
+        for (int64_t i = 0; i < a->length(); ++i) add(a->IsNull(i) ? std::string() : a->GetString(i));
+        break;
+      }
+      case arrow::Type::DICTIONARY: {
+        const auto a = std::static_pointer_cast<arrow::DictionaryArray>(chunk);
+        const auto values = std::static_pointer_cast<arrow::StringArray>(a->dictionary());
+        for (int64_t i = 0; i < a->length(); ++i)
+          add(a->IsNull(i) ? std::string() : values->GetString(a->GetValueIndex(i)));
+        break;
+      }
+      default:
+        throw std::runtime_error("Unsupported string column type: " + chunk->type()->ToString());
+    }
+  }
+  return codes;
+}
+
+template <class T>
+DeviceColumn upload(bo_ctx* ctx, const std::vector<T>& v) {
+  DeviceColumn c;
+  c.rows = static_cast<int64_t>(v.size());
+  check(ctx, bo_device_alloc(ctx, std::max<size_t>(sizeof(T) * v.size(), 256), &c.ptr), "device alloc");
+  if (!v.empty()) check(ctx, bo_copy_h2d(ctx, c.ptr, v.data(), sizeof(T) * v.size()), "upload");
+  return c;
+}
+
+template <class T>
+std::vector<T> permute(const std::vector<T>& v, const std::vector<uint32_t>& order) {
+  std::vector<T> out(v.size());
+  for (size_t i = 0; i < order.size(); ++i) out[i] = v[order[i]];
+  return out;
+}
+
+std::string escape_csv(const std::string& v) {
+  std::string out = "\"";
+  for (char ch : v) {
+    if (ch == '"') out.push_back('\\');
+    out.push_back(ch);
+  }
+  out.push_back('"');
+  return out;
+}
+
+int16_t date_offset_of(const std::string& text, int32_t base_days, int add_years = 0) {
+  int y = std::stoi(text.substr(0, 4)) + add_years;
+  const int m = std::stoi(text.substr(5, 2));
+  int d = std::stoi(text.substr(8, 2));
+  if (add_years) {  // the same day of month, clamped to the target month's length
+    static const int kDays[] = {31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
+    const bool leap = (y % 4 == 0 && y % 100 != 0) || y % 400 == 0;
+    const int dim = (m == 2 && leap) ? 29 : kDays[m - 1];
+    d = std::min(d, dim);
+  }
+  return static_cast<int16_t>(static_cast<int32_t>(days_from_civil(y, (unsigned)m, (unsigned)d)) - base_days);
+}
+
+int32_t scaled_arg(const std::string& text, int32_t scale) {
+  return static_cast<int32_t>(std::llround(std::stod(text) * static_cast<double>(scale)));
+}
+
+template <class T>
+const T* col(const DeviceColumn& c) {
+  return static_cast<const T*>(c.ptr);
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------- queries --
+std::vector<Q1ResultRow> run_q1(const Database& db, const std::string& delta) {
+  const int32_t delta_days = static_cast<int32_t>(std::stoi(delta));
+  const int32_t cutoff = static_cast<int32_t>(days_from_civil(1998, 12, 1)) - delta_days - db.base_date_days;
+  const size_t rf = db.returnflag.values.size(), ls = db.linestatus.values.size();
+  const size_t groups = rf * ls;
+  std::vector<Q1ResultRow> rows;
+  if (groups == 0) return rows;
+  if (groups > BO_Q1_MAX_GROUPS)
+    throw std::runtime_error("Q1: " + std::to_string(groups) + " returnflag x linestatus groups, the GPU path holds " +
+                             std::to_string(BO_Q1_MAX_GROUPS));
+  bo_lineitem_cols c{col<int16_t>(db.l_shipdate), col<uint8_t>(db.l_returnflag_linestatus),
+                     col<int32_t>(db.l_extendedprice), col<int32_t>(db.l_discounted_price),
+                     col<uint8_t>(db.l_discount), col<uint8_t>(db.l_tax), col<int16_t>(db.l_quantity), db.n_lineitem};
+  void* dev = db.scratch.ptr;
+  check(db.ctx, bo_q1_lineitem_device(db.ctx, &c, static_cast<int16_t>(cutoff), static_cast<int32_t>(groups),
+                                      static_cast<bo_q1_agg*>(dev)),
+        "q1");
+  std::vector<bo_q1_agg> agg(groups);
+  check(db.ctx, bo_copy_d2h(db.ctx, agg.data(), dev, sizeof(bo_q1_agg) * groups), "q1 result");
+  check(db.ctx, bo_check_errors(db.ctx), "q1");
+  // Finalisation of bespoke_tpch/query_q1.cpp:233-274: integer totals to
+  // doubles by the same expressions, non-empty groups, (returnflag, linestatus) order.
+  for (size_t g = 0; g < groups; ++g) {
+    const bo_q1_agg& a = agg[g];
+    if (a.count == 0) continue;
+    const __int128 charge = (static_cast<__int128>(a.sum_charge.hi) << 64) | a.sum_charge.lo;
+    const double count = static_cast<double>(a.count);
+    Q1ResultRow r;
+    r.returnflag = db.returnflag.values[g / ls];
+    r.linestatus = db.linestatus.values[g % ls];
+    r.sum_qty = static_cast<double>(a.sum_qty) / kPriceScale;
+    r.sum_base_price = static_cast<double>(a.sum_base_price) / kPriceScale;
+    r.sum_disc_price = static_cast<double>(a.sum_disc_price) / kPriceScale;
+    r.sum_charge = static_cast<double>(charge) / (static_cast<double>(kPriceScale) * kDiscountScale);
+    r.avg_qty = r.sum_qty / count;
+    r.avg_price = r.sum_base_price / count;
+    r.avg_disc = static_cast<double>(a.sum_disc) / kDiscountScale / count;
+    r.count_order = a.count;
+    rows.push_back(std::move(r));
+  }
+  std::sort(rows.begin(), rows.end(), [](const Q1ResultRow& x, const Q1ResultRow& y) {
+    return x.returnflag == y.returnflag ? x.linestatus < y.linestatus : x.returnflag < y.returnflag;
+  });
+  return rows;
+}
+
+std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, const std::string& discount,
+                                const std::string& quantity) {
+  const int16_t start = date_offset_of(date, db.base_date_days);
+  const int16_t end = date_offset_of(date, db.base_date_days, 1);
+  const int32_t d = scaled_arg(discount, kDiscountScale);
+  const int32_t q = scaled_arg(quantity, kPriceScale);
+  bo_lineitem_cols c{};
+  c.shipdate = col<int16_t>(db.l_shipdate);
+  c.extendedprice = col<int32_t>(db.l_extendedprice);
+  c.discount = col<uint8_t>(db.l_discount);
+  c.quantity = col<int16_t>(db.l_quantity);
+  c.n_rows = db.n_lineitem;
+  void* dev = db.scratch.ptr;
+  check(db.ctx, bo_q6_lineitem_device(db.ctx, &c, start, end, d - 1, d + 1, q, static_cast<bo_q6_result*>(dev)),
+        "q6");
+  bo_q6_result r{};
+  check(db.ctx, bo_copy_d2h(db.ctx, &r, dev, sizeof(r)), "q6 result");
+  check(db.ctx, bo_check_errors(db.ctx), "q6");
+  return {Q6ResultRow{r.revenue_raw}};
+}
+
+std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, const std::string& date) {
+  const int16_t d = date_offset_of(date, db.base_date_days);
+  int32_t code = -1;
+  for (size_t i = 0; i < db.mktsegment.values.size(); ++i)
+    if (db.mktsegment.values[i] == segment) {
+      code = static_cast<int32_t>(i);
+      break;
+    }
+  bo_tpch_q3_tables t{};
+  t.c_custkey = col<int32_t>(db.c_custkey);
+  t.c_mktsegment = col<uint16_t>(db.c_mktsegment);
+  t.n_customer = db.n_customer;
+  t.custkey_bound = db.custkey_bound;
+  t.o_orderkey = col<int32_t>(db.o_orderkey);
+  t.o_custkey = col<int32_t>(db.o_custkey);
+  t.o_orderdate = col<int16_t>(db.o_orderdate);
+  t.o_shippriority = col<int32_t>(db.o_shippriority);
+  t.n_orders = db.n_orders;
+  t.orderkey_to_row = col<int32_t>(db.orderkey_to_row);
+  t.n_orderkey_map = db.n_orderkey_map;
+  t.l_orderkey = col<int32_t>(db.l_orderkey);
+  t.l_shipdate = col<int16_t>(db.l_shipdate);
+  t.l_discounted_price = col<int32_t>(db.l_discounted_price);
+  t.n_lineitem = db.n_lineitem;
+  std::vector<bo_tpch_q3_row> out(static_cast<size_t>(std::max<int64_t>(db.n_orders, 1)));
+  int64_t n = 0;
+  check(db.ctx, bo_tpch_q3(db.ctx, &t, d, code, out.data(), db.n_orders, &n), "q3");
+  std::vector<Q3ResultRow> rows(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    rows[i].orderkey = out[i].orderkey;
+    rows[i].revenue_raw = out[i].revenue_raw;
+    rows[i].orderdate_offset = out[i].orderdate_offset;
+    rows[i].shippriority = out[i].shippriority;
+  }
+  return rows;
+}
+
+// ------------------------------------------------------------------ output --
+void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& rows) {
+  std::ofstream out(filename);
+  out << "l_returnflag,l_linestatus,sum_qty,sum_base_price,sum_disc_price,sum_charge,avg_qty,avg_price,avg_disc,"
+         "count_order\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows) {
+    out << r.returnflag << ',' << r.linestatus << ',' << r.sum_qty << ',' << r.sum_base_price << ','
+        << r.sum_disc_price << ',' << r.sum_charge << ',' << r.avg_qty << ',' << r.avg_price << ','
+        << std::setprecision(4) << r.avg_disc << std::setprecision(2) << ',' << r.count_order << "\n";
+  }
+}
+
+void write_q3_csv(const Database& db, const std::string& filename, const std::vector<Q3ResultRow>& rows) {
+  std::ofstream out(filename);
+  out << "l_orderkey,revenue,o_orderdate,o_shippriority\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows) {
+    int y = 0;
+    unsigned m = 0, d = 0;
+    civil_from_days(db.base_date_days + r.orderdate_offset, y, m, d);
+    std::ostringstream date;
+    date << std::setw(4) << std::setfill('0') << y << '-' << std::setw(2) << std::setfill('0') << m << '-'
+         << std::setw(2) << std::setfill('0') << d;
+    out << r.orderkey << ',' << static_cast<double>(r.revenue_raw) / kPriceScale << ',' << date.str() << ','
+        << r.shippriority << "\n";
+  }
+}
+
+void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& rows) {
+  std::ofstream out(filename);
+  out << "revenue\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows)
+    out << static_cast<double>(r.revenue_raw) / (static_cast<double>(kPriceScale) * kDiscountScale) << "\n";
+}
+
+}  // namespace bo_tpch
+
+using namespace bo_tpch;
+
+Database::~Database() {
+  if (!ctx) return;
+  DeviceColumn* cols[] = {&l_orderkey, &l_shipdate, &l_returnflag_linestatus, &l_extendedprice, &l_discounted_price,
+                          &l_discount, &l_tax, &l_quantity, &o_orderkey, &o_custkey, &o_orderdate,
+                          &o_shippriority, &orderkey_to_row, &c_custkey, &c_mktsegment, &scratch};
+  for (auto* c : cols)
+    if (c->ptr) bo_device_free(ctx, c->ptr);
+  bo_destroy(ctx);
+}
+
+// ---------------------------------------------------------- entry points --
+ParquetTables* load(std::string path) {
+  auto* t = new ParquetTables{};
+  t->customer = read_parquet(path + "customer.parquet");
+  t->lineitem = read_parquet(path + "lineitem.parquet");
+  t->nation = read_parquet(path + "nation.parquet");
+  t->orders = read_parquet(path + "orders.parquet");
+  t->part = read_parquet(path + "part.parquet");
+  t->partsupp = read_parquet(path + "partsupp.parquet");
+  t->region = read_parquet(path + "region.parquet");
+  t->supplier = read_parquet(path + "supplier.parquet");
+  return t;
+}
+
+Database* build(ParquetTables* tables) {
+  const auto t0 = std::chrono::steady_clock::now();
+  auto* db = new Database();
+  db->base_date_days = static_cast<int32_t>(days_from_civil(1992, 1, 1));
+  const char* dev_env = std::getenv("BO_DEVICE");
+  const int rc = bo_create(&db->ctx, dev_env ? std::atoi(dev_env) : 0);
+  if (rc != BO_OK) {
+    delete db;
+    throw std::runtime_error("bo_create failed (status " + std::to_string(rc) + "): an sm_100 GPU is required");
+  }
+  bo_ctx* ctx = db->ctx;
+  // lineitem: the storage-plan columns of bespoke_tpch/builder_impl.cpp:456-567.
+  {
+    const auto& L = tables->lineitem;
+    const auto orderkey = int_values(column(L, "l_orderkey"));
+    const auto quantity = scaled_values(column(L, "l_quantity"), kPriceScale);
+    const auto price = scaled_values(column(L, "l_extendedprice"), kPriceScale);
+    const auto discount = scaled_values(column(L, "l_discount"), kDiscountScale);
+    const auto tax = scaled_values(column(L, "l_tax"), kDiscountScale);
+    const auto ship = date_offsets(column(L, "l_shipdate"), db->base_date_days);
+    const auto rf = dictionary_codes(column(L, "l_returnflag"), db->returnflag);
+    const auto ls = dictionary_codes(column(L, "l_linestatus"), db->linestatus);
+    const size_t n = orderkey.size();
+    const size_t ls_count = db->linestatus.values.size();
+    if (db->returnflag.values.size() * ls_count > 255)
+      throw std::runtime_error("Lineitem returnflag/linestatus exceeds uint8 capacity");
+    std::vector<uint8_t> d8(n), t8(n), code(n);
+    std::vector<int16_t> q16(n);
+    std::vector<int32_t> dprice(n);
+    for (size_t i = 0; i < n; ++i) {
+      d8[i] = static_cast<uint8_t>(discount[i]);
+      t8[i] = static_cast<uint8_t>(tax[i]);
+      q16[i] = static_cast<int16_t>(quantity[i]);
+      dprice[i] = static_cast<int32_t>(static_cast<int64_t>(price[i]) * (kDiscountScale - static_cast<int32_t>(d8[i])) /
+                                       kDiscountScale);
+      code[i] = static_cast<uint8_t>(rf[i] * ls_count + ls[i]);
+    }
+    db->n_lineitem = static_cast<int64_t>(n);
+    db->l_orderkey = upload(ctx, orderkey);
+    db->l_shipdate = upload(ctx, ship);
+    db->l_returnflag_linestatus = upload(ctx, code);
+    db->l_extendedprice = upload(ctx, price);
+    db->l_discounted_price = upload(ctx, dprice);
+    db->l_discount = upload(ctx, d8);
+    db->l_tax = upload(ctx, t8);
+    db->l_quantity = upload(ctx, q16);
+  }
+  // orders, stably sorted by orderdate, and the orderkey -> row map
+  // (bespoke_tpch/builder_impl.cpp:580-642).
+  {
+    const auto& O = tables->orders;
+    const auto okey = int_values(column(O, "o_orderkey"));
+    const auto ckey = int_values(column(O, "o_custkey"));
+    const auto odate = date_offsets(column(O, "o_orderdate"), db->base_date_days);
+    const auto prio = int_values(column(O, "o_shippriority"));
+    std::vector<uint32_t> order(okey.size());
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return odate[a] < odate[b]; });
+    const auto sk = permute(okey, order), sc = permute(ckey, order), sp = permute(prio, order);
+    const auto sd = permute(odate, order);
+    int32_t max_key = -1;
+    for (int32_t k : sk) max_key = std::max(max_key, k);
+    std::vector<int32_t> map(max_key >= 0 ? static_cast<size_t>(max_key) + 1 : 0, -1);
+    for (size_t i = 0; i < sk.size(); ++i)
+      if (sk[i] >= 0 && static_cast<size_t>(sk[i]) < map.size()) map[static_cast<size_t>(sk[i])] = static_cast<int32_t>(i);
+    db->n_orders = static_cast<int64_t>(sk.size());
+    db->n_orderkey_map = static_cast<int64_t>(map.size());
+    db->o_orderkey = upload(ctx, sk);
+    db->o_custkey = upload(ctx, sc);
+    db->o_orderdate = upload(ctx, sd);
+    db->o_shippriority = upload(ctx, sp);
+    db->orderkey_to_row = upload(ctx, map);
+  }
+  // customer: keys and market-segment codes (bespoke_tpch/builder_impl.cpp:670-700).
+  {
+    const auto& C = tables->customer;
+    const auto ckey = int_values(column(C, "c_custkey"));
+    const auto seg = dictionary_codes(column(C, "c_mktsegment"), db->mktsegment);
+    int32_t max_key = 0;
+    for (int32_t k : ckey) max_key = std::max(max_key, k);
+    db->n_customer = static_cast<int64_t>(ckey.size());
+    db->custkey_bound = ckey.empty() ? 0 : max_key + 1;
+    db->c_custkey = upload(ctx, ckey);
+    db->c_mktsegment = upload(ctx, seg);
+  }
+  check(ctx, bo_device_alloc(ctx, sizeof(bo_q1_agg) * BO_Q1_MAX_GROUPS + 256, &db->scratch.ptr), "scratch alloc");
+  check(ctx, bo_synchronize(ctx), "build");
+  const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+  std::cout << "Build ms: " << ms << "\n";
+  return db;
+}
+
+void query(Database* db) {
+  struct Request {
+    std::string id, line;
+  };
+  std::vector<Request> requests;
+  std::string line;
+  while (std::getline(std::cin, line)) {
+    if (line.empty()) break;
+    std::istringstream iss(line);
+    std::string id = "0";
+    iss >> id;
+    if (!iss) continue;
+    requests.push_back(Request{id, line});
+  }
+  for (size_t idx = 0; idx < requests.size(); ++idx) {
+    const auto& r = requests[idx];
+    const auto start = std::chrono::steady_clock::now();
+    const std::string file = "result" + std::to_string(idx + 1) + ".csv";
+    std::istringstream iss(r.line);
+    std::string qid;
+    iss >> qid;
+    auto arg = [&](const char* name) {
+      std::string v;
+      if (!(iss >> std::quoted(v))) throw std::runtime_error("Q" + r.id + ": failed to parse " + name);
+      return v;
+    };
+    if (r.id == "1") {
+      const std::string delta = arg("DELTA");
+      const auto rows = run_q1(*db, delta);
+      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      write_q1_csv(file, rows);
+      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+    } else if (r.id == "3") {
+      const std::string segment = arg("SEGMENT");
+      const std::string date = arg("DATE");
+      const auto rows = run_q3(*db, segment, date);
+      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      write_q3_csv(*db, file, rows);
+      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+    } else if (r.id == "6") {
+      const std::string date = arg("DATE");
+      const std::string discount = arg("DISCOUNT");
+      const std::string quantity = arg("QUANTITY");
+      const auto rows = run_q6(*db, date, discount, quantity);
+      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      write_q6_csv(file, rows);
+      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+    } else {
+      // Not on the GPU path: the reference's stub record.
+      std::ofstream out(file);
+      out << "query_id,params\n" << escape_csv(r.id) << "," << escape_csv(r.line) << "\n";
+      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+    }
+  }
+}

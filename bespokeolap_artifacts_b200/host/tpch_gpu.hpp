@@ -1,0 +1,124 @@
+// Drop-in GPU host for the reference's TPC-H engine.
+//
+// The reference's external driver links three C++ entry points
+// (bespoke_tpch/loader_impl.hpp:20, builder_impl.hpp:173, query_impl.hpp:6):
+//     ParquetTables* load(std::string);   Database* build(ParquetTables*);   void query(Database*);
+// This library exports the same three signatures, so that driver links
+// unchanged.  load() reads the same eight Parquet files; build() derives the
+// storage-plan columns the hot path reads (the reference builder's rules,
+// bespoke_tpch/builder_impl.cpp:447-999, restated) and uploads them once;
+// query() speaks the same stdin / result<idx>.csv / "Execution ms" protocol
+// (bespoke_tpch/query_impl.cpp:142-389) and runs Q1, Q3 and Q6 on the GPU
+// through the C ABI of include/bespoke_gpu.h.  Result structs and CSV formats
+// are the reference's (query_q1.hpp:9-20, query_q3.hpp:10-15, query_q6.hpp).
+// Requests for other query ids get the reference's stub CSV
+// (query_impl.cpp:98-103): this library has no CPU implementation of them.
+#pragma once
+
+#include <arrow/table.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "bespoke_gpu.h"
+
+struct ParquetTables {
+  using ArrowTable = std::shared_ptr<arrow::Table>;
+
+  ArrowTable customer;
+  ArrowTable lineitem;
+  ArrowTable nation;
+  ArrowTable orders;
+  ArrowTable part;
+  ArrowTable partsupp;
+  ArrowTable region;
+  ArrowTable supplier;
+};
+
+namespace bo_tpch {
+
+// One device allocation per column, freed with the database.
+struct DeviceColumn {
+  void* ptr = nullptr;
+  int64_t rows = 0;
+};
+
+struct Dictionary {
+  std::vector<std::string> values;  // first-appearance order
+};
+
+}  // namespace bo_tpch
+
+// GPU-resident database: the storage-plan columns of the three tables the
+// hot path reads, on the device; dictionaries and sizes on the host.
+struct Database {
+  int32_t base_date_days = 0;
+  bo_ctx* ctx = nullptr;
+  // lineitem (row order of the input)
+  int64_t n_lineitem = 0;
+  bo_tpch::DeviceColumn l_orderkey, l_shipdate, l_returnflag_linestatus, l_extendedprice, l_discounted_price,
+      l_discount, l_tax, l_quantity;
+  bo_tpch::Dictionary returnflag, linestatus;
+  // orders, sorted by orderdate (stable)
+  int64_t n_orders = 0;
+  bo_tpch::DeviceColumn o_orderkey, o_custkey, o_orderdate, o_shippriority, orderkey_to_row;
+  int64_t n_orderkey_map = 0;
+  // customer
+  int64_t n_customer = 0;
+  int32_t custkey_bound = 0;
+  bo_tpch::DeviceColumn c_custkey, c_mktsegment;
+  bo_tpch::Dictionary mktsegment;
+  // Result record of the last scan-agg / Q6 query.  Queries on one Database
+  // run one at a time (as the reference's single-threaded query()).
+  bo_tpch::DeviceColumn scratch;
+  ~Database();
+};
+
+ParquetTables* load(std::string);
+Database* build(ParquetTables*);
+void query(Database*);
+
+// ---------------------------------------------------------------- queries --
+struct Q1ResultRow {
+  std::string returnflag;
+  std::string linestatus;
+  double sum_qty = 0.0;
+  double sum_base_price = 0.0;
+  double sum_disc_price = 0.0;
+  double sum_charge = 0.0;
+  double avg_qty = 0.0;
+  double avg_price = 0.0;
+  double avg_disc = 0.0;
+  int64_t count_order = 0;
+};
+
+struct Q3ResultRow {
+  int32_t orderkey = 0;
+  int64_t revenue_raw = 0;
+  int16_t orderdate_offset = 0;
+  int32_t shippriority = 0;
+};
+
+struct Q6ResultRow {
+  int64_t revenue_raw = 0;
+};
+
+namespace bo_tpch {
+
+int64_t days_from_civil(int64_t y, unsigned m, unsigned d);
+void civil_from_days(int64_t z, int& y, unsigned& m, unsigned& d);
+
+// Run on the GPU; the arguments are the request's strings (DELTA; SEGMENT,
+// DATE; DATE, DISCOUNT, QUANTITY), parsed as the reference parses them.
+std::vector<Q1ResultRow> run_q1(const Database& db, const std::string& delta);
+std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, const std::string& date);
+std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, const std::string& discount,
+                                const std::string& quantity);
+
+void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& rows);
+void write_q3_csv(const Database& db, const std::string& filename, const std::vector<Q3ResultRow>& rows);
+void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& rows);
+
+}  // namespace bo_tpch

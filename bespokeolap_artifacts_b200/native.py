@@ -210,6 +210,7 @@ _SIGNATURES = {
     "bo_copy_h2d": (C.c_int, [_P, _P, _P, C.c_size_t]),
     "bo_copy_d2h": (C.c_int, [_P, _P, _P, C.c_size_t]),
     "bo_launch_count": (C.c_int64, [_P]),
+    "bo_check_errors": (C.c_int, [_P]),
     "bo_q1_fact_device": (C.c_int, [_P, C.POINTER(FactCols), C.c_int32, C.c_int32, C.c_int32, _P]),
     "bo_q1_fact_host": (C.c_int, [_P, C.POINTER(FactCols), C.c_int32, C.c_int32, C.c_int32, C.POINTER(Q1Agg)]),
     "bo_q1_fact_device_noalloc": (C.c_int, [C.POINTER(FactCols), C.c_int32, C.c_int32, C.c_int32, _P, _P, _P]),

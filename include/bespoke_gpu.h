@@ -75,6 +75,9 @@ int bo_copy_d2h(bo_ctx* ctx, void* dst_host, const void* src_device, size_t byte
 /* Kernels launched by this library since the context was created (counted on
  * the host at each launch). */
 int64_t bo_launch_count(const bo_ctx* ctx);
+/* Waits for the context's stream and turns the device error word (set by the
+ * _device entry points' kernels) into a status; clears it. */
+int bo_check_errors(bo_ctx* ctx);
 
 /* ===================================================================== Q1 ==
  * Scan + filter + low-cardinality group-by aggregation.
@@ -342,6 +345,49 @@ int bo_radix_sort_pairs_device(bo_ctx* ctx, uint64_t* keys, uint32_t* vals, int6
                                int32_t end_bit);
 int bo_radix_sort_pairs_host(bo_ctx* ctx, uint64_t* keys, uint32_t* vals, int64_t n, int32_t begin_bit,
                              int32_t end_bit);
+
+/* ================================================================ TPC-H Q3 ==
+ * run_q3 over the storage-plan layout (bespoke_tpch/query_q3.cpp:153-365):
+ * customers of one market segment, their orders dated before D, each order's
+ * revenue = sum of discounted_price over its lineitems shipped after D; every
+ * order with such a lineitem, sorted by revenue desc, orderdate asc (rows equal
+ * in both come in orderkey order).  Columns as the reference builder lays them
+ * out (bespoke_tpch/builder_impl.hpp:39-97): dates are int16 day offsets from
+ * the database's base date, orders sorted by orderdate, orderkey_to_row maps an
+ * orderkey to its orders row (-1 if none; builder_impl.cpp:610-642). */
+typedef struct bo_tpch_q3_tables {
+  const int32_t* c_custkey;
+  const uint16_t* c_mktsegment;   /* dictionary codes */
+  int64_t n_customer;
+  int32_t custkey_bound;          /* max custkey + 1 (0 if none) */
+  int32_t pad0;
+  const int32_t* o_orderkey;
+  const int32_t* o_custkey;
+  const int16_t* o_orderdate;
+  const int32_t* o_shippriority;  /* may be NULL (reported as 0) */
+  int64_t n_orders;
+  const int32_t* orderkey_to_row;
+  int64_t n_orderkey_map;
+  const int32_t* l_orderkey;
+  const int16_t* l_shipdate;
+  const int32_t* l_discounted_price;
+  int64_t n_lineitem;
+} bo_tpch_q3_tables;
+
+typedef struct bo_tpch_q3_row {   /* Q3ResultRow fields (bespoke_tpch/query_q3.hpp:10-15) */
+  int64_t revenue_raw;            /* x100 */
+  int32_t orderkey;
+  int32_t shippriority;
+  int16_t orderdate_offset;
+  int16_t pad0;
+  int32_t pad1;
+} bo_tpch_q3_row;
+
+/* Device columns in, rows on the host: the first min(n, max_rows) rows are
+ * copied to out_host and *n_rows = n.  segment_code < 0 (segment not in the
+ * dictionary) gives no rows. */
+int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* tables, int16_t date_offset, int32_t segment_code,
+               bo_tpch_q3_row* out_host, int64_t max_rows, int64_t* n_rows);
 
 /* ================================================================= BATCH ==
  * Many pipelines of uneven sizes in ONE persistent kernel fed by a device work

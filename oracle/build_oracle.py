@@ -67,6 +67,15 @@ def build_reference(force: bool = False) -> list[Path]:
             f"-Wl,-rpath,{libdir}", "-lpthread", "-o", str(out),
         ]
         jobs.append(subprocess.Popen(cmd))
+    # The reference's own load / build / query behind a stand-in driver main.
+    drv = OUT_REF / "ref_tpch_driver"
+    outs.append(drv)
+    dsrcs = [HERE / "ref_driver_main.cpp", tpch / "query_impl.cpp", tpch / "builder_impl.cpp", tpch / "loader_impl.cpp"]
+    if force or _stale(drv, dsrcs + deps):
+        jobs.append(subprocess.Popen([
+            "g++", "-std=c++20", "-O2", f"-I{tpch}", f"-I{HERE / 'ref_stubs'}", f"-I{inc}", *map(str, dsrcs),
+            f"-L{libdir}", "-l:libarrow.so.2400", "-l:libparquet.so.2400", f"-Wl,-rpath,{libdir}", "-lpthread",
+            "-o", str(drv)]))
     for j in jobs:
         if j.wait() != 0:
             raise RuntimeError("building the reference harness failed")
