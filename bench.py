@@ -44,6 +44,25 @@ WORKLOAD = ("filtered hash join + scalar aggregate: build 1,500,000 rows (int32 
 PROFILE = ROOT / "profiles" / "join_probe_kernel_build1.5M_probe6M.md"
 
 
+def max_over_ranks(value: float, dist) -> float:
+    """The largest value over all ranks (device time of the slowest rank); the
+    value itself without a process group."""
+    if dist is None:
+        return value
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rows_per_s(world: int, steps: int, rows_per_step: int, ms: float) -> float:
+    """Whole-job throughput: rows processed by all ranks over the slowest
+    rank's time (every rank runs an independent replica)."""
+    return world * steps * rows_per_step / (ms * 1e-3)
+
+
 def peaks() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -215,12 +234,7 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     rs = check(range(W, W + K))
     for k, r in enumerate(rs):  # same copy -> same answer every time
         assert r["match_count"] == rs[k % 3]["match_count"] and r["sum_exact"] == rs[k % 3]["sum_exact"]
-    if dist:
-        import torch.distributed as td
-
-        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        td.all_reduce(tt, op=td.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, dist)
 
     # ---- per-query latency: learned vs plain (results on the host each time)
     def per_query(fn, n):
@@ -406,7 +420,7 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
 
     out = None
     if rank == 0:
-        value = world * K * ROWS_PER_STEP / (ms * 1e-3)
+        value = job_rows_per_s(world, K, ROWS_PER_STEP, ms)
         out = {
             "metric": METRIC,
             "value": value,
