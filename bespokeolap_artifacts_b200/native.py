@@ -164,6 +164,21 @@ class GbResult(C.Structure):
                     min_years=[self.rows[i].min_year for i in range(n)])
 
 
+class TpchQ3Tables(C.Structure):
+    """``bo_tpch_q3_tables``: storage-plan columns of customer, orders, lineitem."""
+    _fields_ = [("c_custkey", C.c_void_p), ("c_mktsegment", C.c_void_p), ("n_customer", C.c_int64),
+                ("custkey_bound", C.c_int32), ("pad0", C.c_int32), ("o_orderkey", C.c_void_p),
+                ("o_custkey", C.c_void_p), ("o_orderdate", C.c_void_p), ("o_shippriority", C.c_void_p),
+                ("n_orders", C.c_int64), ("orderkey_to_row", C.c_void_p), ("n_orderkey_map", C.c_int64),
+                ("l_orderkey", C.c_void_p), ("l_shipdate", C.c_void_p), ("l_discounted_price", C.c_void_p),
+                ("n_lineitem", C.c_int64)]
+
+
+class TpchQ3Row(C.Structure):
+    _fields_ = [("revenue_raw", C.c_int64), ("orderkey", C.c_int32), ("shippriority", C.c_int32),
+                ("orderdate_offset", C.c_int16), ("pad0", C.c_int16), ("pad1", C.c_int32)]
+
+
 BATCH_SCAN_AGG, BATCH_JOIN, BATCH_GROUPBY = 0, 1, 2
 BATCH_MAX_CATS = 64
 
@@ -251,6 +266,8 @@ _SIGNATURES = {
     "bo_mlp_train_host": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, C.c_float, C.POINTER(C.c_float)]),
     "bo_mlp_infer_device": (C.c_int, [_P, _P, _P, C.c_int32, _P]),
     "bo_mlp_predict_counts": (C.c_int, [_P, _P, _P, _P, _P]),
+    "bo_tpch_q3": (C.c_int, [_P, C.POINTER(TpchQ3Tables), C.c_int16, C.c_int32, C.POINTER(TpchQ3Row), C.c_int64,
+                             C.POINTER(C.c_int64)]),
     "bo_batch_create": (C.c_int, [_P, C.POINTER(BatchInstance), C.c_int32, C.c_int32, C.POINTER(_P)]),
     "bo_batch_create_pool": (C.c_int, [_P, C.c_int32, C.c_int64, C.c_int64, C.c_int32, C.POINTER(_P)]),
     "bo_batch_update": (C.c_int, [_P, _P, C.POINTER(BatchInstance), C.c_int32]),

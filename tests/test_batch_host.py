@@ -60,3 +60,19 @@ def test_batch_struct_layout_matches_header(tmp_path):
             N.BatchInstance.build.offset, N.BatchInstance.a.offset, N.BatchInstance.categories.offset,
             N.BatchInstance.n_categories.offset, N.BatchResult.join.offset, N.BatchResult.groupby.offset]
     assert got == want
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="needs gcc")
+def test_q3_struct_layout_matches_header(tmp_path):
+    src = tmp_path / "q3layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "bespoke_gpu.h"\n'
+        'int main(void){printf("%zu %zu %zu %zu %zu\\n", sizeof(bo_tpch_q3_tables), sizeof(bo_tpch_q3_row),'
+        ' offsetof(bo_tpch_q3_tables, o_orderkey), offsetof(bo_tpch_q3_tables, l_orderkey),'
+        ' offsetof(bo_tpch_q3_row, orderdate_offset)); return 0;}\n')
+    exe = tmp_path / "q3layout"
+    subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = [C.sizeof(N.TpchQ3Tables), C.sizeof(N.TpchQ3Row), N.TpchQ3Tables.o_orderkey.offset,
+            N.TpchQ3Tables.l_orderkey.offset, N.TpchQ3Row.orderdate_offset.offset]
+    assert got == want
