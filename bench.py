@@ -353,45 +353,58 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     achieved = PROBE_BYTES / (probe_ms * 1e-3) / 1e9
     traffic = profile_traffic()
 
-    # ---- end to end through the C ABI with pinned host buffers
-    pin = []
-    for c in copies[:1]:
-        j = c["j"]
-        arrs = [j.b_key, j.b_date, j.b_seg, j.p_fk, j.p_price, j.p_disc]
-        pins = []
-        for a in arrs:
-            h = C.c_void_p()
-            eng.ctx.call("bo_host_alloc_pinned", C.c_size_t(a.nbytes), C.byref(h))
-            C.memmove(h.value, a.ctypes.data, a.nbytes)
-            pins.append(h.value)
-        pin.append(pins)
-    dbufs = [torch.empty_like(x) for x in copies[0]["b"] + copies[0]["p"]]
-    res_host = N.JoinResult()
+    # ---- end to end through the C ABI: inputs in pinned host memory, the
+    # streamed join (dense columns copied in chunks overlapped with the probe,
+    # keys / price / discount of qualifying rows read in place)
+    from bespokeolap_artifacts_b200.engine import PinnedColumns, join_stream
+
     j0 = copies[0]["j"]
-    h2d = sum(a.nbytes for a in (j0.b_key, j0.b_date, j0.b_seg, j0.p_fk, j0.p_price, j0.p_disc))
+    pc = PinnedColumns(eng, {"b_key": j0.b_key, "b_date": j0.b_date, "b_seg": j0.b_seg, "p_fk": j0.p_fk,
+                             "p_price": j0.p_price, "p_disc": j0.p_disc})
+    h2d = j0.b_date.nbytes + j0.b_seg.nbytes + j0.p_fk.nbytes
+    e2e_res = {}
 
-    def e2e_step():
-        for src, dst in zip(pin[0], dbufs):
-            eng.ctx.call("bo_copy_h2d", C.c_void_p(dst.data_ptr()), C.c_void_p(src), C.c_size_t(dst.nbytes))
-        sizer.predict_device(feats[0], preds[0:1])
-        eng.join_presized_device(dbufs[:3], dbufs[3:], N_BUILD, N_PROBE, j0.date_lt, j0.seg_eq, preds[0:1],
-                                 results[0:res_sz])
-        eng.ctx.call("bo_copy_d2h", C.byref(res_host), C.c_void_p(results.data_ptr()), C.c_size_t(res_sz))
-        if res_host.overflowed:
-            eng.join_plain(dbufs[:3], dbufs[3:], N_BUILD, N_PROBE, j0.date_lt, j0.seg_eq)
+    # Learned queries need no host round trip, so consecutive queries pipeline:
+    # query i+1's copies overlap query i's kernels (two buffer sets); each
+    # query's copies, prediction, kernels and result read are inside the
+    # timed region, results are checked after the single synchronise.
+    from bespokeolap_artifacts_b200.engine import join_stream_async
 
-    for _ in range(2):
-        e2e_step()
+    n_e2e = max(10, K)
+    res_sz_b = C.sizeof(N.JoinResult)
+    res_pin = C.c_void_p()
+    eng.ctx.call("bo_host_alloc_pinned", C.c_size_t(n_e2e * res_sz_b), C.byref(res_pin))
+
+    def e2e_run(n):
+        for i in range(n):
+            sizer.predict_device(feats[0], preds[0:1])
+            join_stream_async(eng, pc, N_BUILD, N_PROBE, j0.date_lt, j0.seg_eq, preds[0:1],
+                              res_pin.value + i * res_sz_b)
+        eng.ctx.call("bo_check_errors")
+        out_e = []
+        for i in range(n):
+            r = N.JoinResult.from_address(res_pin.value + i * res_sz_b).as_dict()
+            if r["overflowed"]:  # invalid: rerun exactly (inside the timed region)
+                r = join_stream(eng, pc, N_BUILD, N_PROBE, j0.date_lt, j0.seg_eq)
+            out_e.append(r)
+        return out_e
+
+    e2e_run(3)
     torch.cuda.synchronize()
-    te = []
-    for _ in range(max(3, min(K, 10))):
-        t0 = time.perf_counter()
-        e2e_step()
-        te.append(time.perf_counter() - t0)
-    e2e_s = statistics.median(te)
-    for pins in pin:
-        for h in pins:
-            eng.ctx.call("bo_host_free_pinned", C.c_void_p(h))
+    t0 = time.perf_counter()
+    outs_e2e = e2e_run(n_e2e)
+    e2e_s = (time.perf_counter() - t0) / n_e2e
+    e2e_res.update(outs_e2e[-1])
+    assert all(o["match_count"] == outs_e2e[0]["match_count"] for o in outs_e2e)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        sizer.predict_device(feats[0], preds[0:1])
+        join_stream(eng, pc, N_BUILD, N_PROBE, j0.date_lt, j0.seg_eq, preds[0:1])
+    e2e_serial_ms = (time.perf_counter() - t0) / 5 * 1e3
+    eng.ctx.call("bo_host_free_pinned", res_pin)
+    zero_copy = 4 * e2e_res["build_rows"] + 16 * e2e_res["match_count"]
+    assert e2e_res["match_count"] == rs[0]["match_count"] and e2e_res["sum_exact"] == rs[0]["sum_exact"]
+    pc.close()
 
     q_err = [float(L.q_error(sizer.predict_host(f[None, :]), [e])[0]) for f, e in zip(feats, exact_rows)]
 
@@ -442,8 +455,13 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
                 "parallelism": f"replicas x{world}",
             },
             "e2e": {"value": ROWS_PER_STEP / e2e_s, "unit": "rows/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": res_sz,
-                    "path": "bo_copy_h2d (pinned) + bo_mlp_predict_counts + bo_join_presized_device + bo_copy_d2h"},
+                    "d2h_bytes_per_step": res_sz, "zero_copy_read_bytes_per_step": zero_copy,
+                    "ms_per_step": e2e_s * 1e3, "ms_one_query_alone": e2e_serial_ms,
+                    "path": "inputs in pinned host memory; per query bo_mlp_predict_counts + "
+                            "bo_join_stream_host_async (build date/segment and probe fk copied, fk in 1M-row chunks "
+                            "overlapped with the probe; keys of qualifying build rows and price/discount of matching "
+                            "probe rows read in place over PCIe, counted in zero_copy_read_bytes_per_step; result "
+                            "copied to pinned host memory); queries pipelined, one synchronise per run"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": "join_probe_kernel", "achieved": achieved, "peak": peak,
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst)", "unit": "GB/s",

@@ -155,7 +155,7 @@ __device__ __forceinline__ int64_t narrow_i64(__int128 v, uint32_t& bad) {
   return (int64_t)v;
 }
 
-__device__ __forceinline__ bo_i128 to_bo_i128(__int128 v) {
+__host__ __device__ __forceinline__ bo_i128 to_bo_i128(__int128 v) {
   bo_i128 r;
   r.lo = (uint64_t)v;
   r.hi = (int64_t)(v >> 64);

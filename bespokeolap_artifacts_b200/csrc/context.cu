@@ -153,6 +153,11 @@ void bo_destroy(bo_ctx* ctx) {
   if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->h_err) cudaFreeHost(ctx->h_err);
   if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
+  for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -195,7 +200,8 @@ int bo_device_free(bo_ctx* ctx, void* ptr) {
 int bo_host_alloc_pinned(bo_ctx* ctx, size_t bytes, void** out) {
   BO_CHECK_CTX(ctx);
   if (!out) return bo::set_error(ctx, BO_ERR_INVALID, "bo_host_alloc_pinned: null out");
-  BO_CUDA(ctx, cudaHostAlloc(out, bytes ? bytes : 16, cudaHostAllocDefault));
+  // Mapped: kernels may also read it in place (zero-copy), e.g. the streamed join.
+  BO_CUDA(ctx, cudaHostAlloc(out, bytes ? bytes : 16, cudaHostAllocMapped | cudaHostAllocPortable));
   return BO_OK;
 }
 

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "bespoke_gpu.h"
 
@@ -33,6 +34,11 @@ struct bo_ctx {
   // Pinned staging used by the _host entry points.
   void* h_stage = nullptr;
   size_t h_stage_bytes = 0;
+  // Second stream for host->device copies that overlap with kernels, and the
+  // events that order the two (created on first use).
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> events;
+  int stream_set = 0;  // buffer set of the streamed join's next query
 };
 
 namespace bo {

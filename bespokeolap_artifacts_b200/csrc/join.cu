@@ -467,6 +467,165 @@ int join_plain_impl(bo_ctx* ctx, const bo_join_build_cols& b, const bo_join_prob
   return BO_OK;
 }
 
+// ------------------------------------------------------ streamed join ---
+// Inputs in pinned host memory: the dense columns (build date and segment,
+// probe fk) are copied on the context's copy stream, fk in chunks; the kernels
+// read the build keys of qualifying rows and the price / discount of matching
+// rows in place.  Two buffer sets alternate so that a query's copies overlap
+// the previous query's kernels; a set is reused only after the compute stream
+// has finished with it (its "done" event).
+constexpr int64_t kStreamChunkRows = 1 << 20;  // probe rows per copy / probe step
+
+__global__ void join_combine_kernel(const bo_join_result* __restrict__ part, int64_t n, bo_join_result* out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  bo_join_result r = part[0];
+  __int128 se = 0, st = 0;
+  int64_t mc = 0;
+  int32_t of = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    se += ((__int128)part[i].sum_exact.hi << 64) | part[i].sum_exact.lo;
+    st += ((__int128)part[i].sum_trunc.hi << 64) | part[i].sum_trunc.lo;
+    mc += part[i].match_count;
+    of |= part[i].overflowed;
+  }
+  r.match_count = mc;
+  r.sum_exact = to_bo_i128(se);
+  r.sum_trunc = to_bo_i128(st);
+  r.overflowed = of;
+  r.reruns = 0;
+  *out = r;
+}
+
+// Device pointer of a pinned (mapped) host buffer, or null if it is not one.
+const void* mapped_device_pointer(const void* host) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+  return a.devicePointer;
+}
+
+struct StreamIn {
+  const int32_t* key = nullptr;    // device views of pinned host columns
+  const int64_t* price = nullptr;
+  const int64_t* disc = nullptr;
+  int64_t chunks = 1;
+};
+
+int stream_check(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join_probe_cols* ph, const bo_join_params* prm,
+                 StreamIn* in) {
+  if (!bh || !ph || !prm) return set_error(ctx, BO_ERR_INVALID, "join_stream: null argument");
+  if (bh->n_rows < 0 || ph->n_rows < 0 || bh->n_rows > 0x7fffffffll)
+    return set_error(ctx, BO_ERR_INVALID, "join_stream: row counts");
+  if (prm->segment_eq < 0 || prm->segment_eq > 255)
+    return set_error(ctx, BO_ERR_INVALID, "join_stream: segment_eq %d outside uint8", prm->segment_eq);
+  if (bh->n_rows > 0) {
+    in->key = static_cast<const int32_t*>(mapped_device_pointer(bh->key));
+    if (!in->key || !mapped_device_pointer(bh->date) || !mapped_device_pointer(bh->segment))
+      return set_error(ctx, BO_ERR_INVALID, "join_stream: build columns must be pinned host memory");
+  }
+  if (ph->n_rows > 0) {
+    in->price = static_cast<const int64_t*>(mapped_device_pointer(ph->price));
+    in->disc = static_cast<const int64_t*>(mapped_device_pointer(ph->discount));
+    if (!in->price || !in->disc || !mapped_device_pointer(ph->fk))
+      return set_error(ctx, BO_ERR_INVALID, "join_stream: probe columns must be pinned host memory");
+  }
+  in->chunks = std::max<int64_t>(1, (ph->n_rows + kStreamChunkRows - 1) / kStreamChunkRows);
+  return BO_OK;
+}
+
+struct StreamSet {
+  int32_t* date;
+  uint8_t* seg;
+  int32_t* fk;
+  bo_join_result* part;
+  bo_join_result* combined;
+};
+
+size_t al256(size_t v) { return (v + 255) & ~size_t(255); }
+
+int stream_set(bo_ctx* ctx, int64_t nb, int64_t np, int64_t chunks, int set, StreamSet* s) {
+  const size_t b_date = al256(4 * (size_t)nb), b_seg = al256((size_t)nb), b_fk = al256(4 * (size_t)np);
+  const size_t b_part = al256(sizeof(bo_join_result) * (size_t)(chunks + 1));
+  const size_t per = b_date + b_seg + b_fk + b_part;
+  void* base = nullptr;
+  int rc = region(ctx, "join_stream", 2 * per, &base);
+  if (rc) return rc;
+  char* p = static_cast<char*>(base) + (size_t)set * per;
+  s->date = reinterpret_cast<int32_t*>(p);
+  s->seg = reinterpret_cast<uint8_t*>(p + b_date);
+  s->fk = reinterpret_cast<int32_t*>(p + b_date + b_seg);
+  s->part = reinterpret_cast<bo_join_result*>(p + b_date + b_seg + b_fk);
+  s->combined = s->part + chunks;
+  return BO_OK;
+}
+
+// Events: [0], [1] "set done"; [2] build columns copied; [3 + c] probe chunk c copied.
+int stream_events(bo_ctx* ctx, int64_t chunks) {
+  while (ctx->events.size() < (size_t)(chunks + 3)) {
+    cudaEvent_t e;
+    BO_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->events.push_back(e);
+  }
+  return BO_OK;
+}
+
+int stream_copies(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join_probe_cols* ph, const StreamIn& in,
+                  const StreamSet& s, int set) {
+  if (!ctx->copy_stream) BO_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  cudaStream_t cs = ctx->copy_stream;
+  cudaEvent_t* ev = ctx->events.data();
+  BO_CUDA(ctx, cudaStreamWaitEvent(cs, ev[set], 0));  // the set's previous query has finished with it
+  const int64_t nb = bh->n_rows, np = ph->n_rows;
+  if (nb > 0) {
+    BO_CUDA(ctx, cudaMemcpyAsync(s.date, bh->date, 4 * (size_t)nb, cudaMemcpyHostToDevice, cs));
+    BO_CUDA(ctx, cudaMemcpyAsync(s.seg, bh->segment, (size_t)nb, cudaMemcpyHostToDevice, cs));
+  }
+  BO_CUDA(ctx, cudaEventRecord(ev[2], cs));
+  for (int64_t c = 0; c < in.chunks; ++c) {
+    const int64_t lo = c * kStreamChunkRows, n = std::min(np - lo, kStreamChunkRows);
+    if (n > 0) BO_CUDA(ctx, cudaMemcpyAsync(s.fk + lo, ph->fk + lo, 4 * (size_t)n, cudaMemcpyHostToDevice, cs));
+    BO_CUDA(ctx, cudaEventRecord(ev[3 + c], cs));
+  }
+  return BO_OK;
+}
+
+// init + build + chunked probe + combine on the compute stream; the caller
+// made the compute stream wait for ev[2] already when it sized the table from
+// an exact count (pred == nullptr).
+int stream_compute(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join_probe_cols* ph, const bo_join_params* prm,
+                   const float* pred, int32_t host_log2, const JoinWs& ws, const StreamIn& in, const StreamSet& s,
+                   int set) {
+  cudaEvent_t* ev = ctx->events.data();
+  BO_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ev[2], 0));
+  const int64_t nb = bh->n_rows, np = ph->n_rows;
+  const int32_t mode = pred ? 1 : 0;
+  const uint64_t limit = mode == 0 ? ~0ull : kPresizedProbeLimit;
+  const bo_join_build_cols b = {in.key, s.date, s.seg, nb};
+  const void* ki = reinterpret_cast<const void*>(&join_init_kernel);
+  join_init_kernel<<<grid_for(ctx, ki, 256, 0, (int64_t)1 << std::min(ws.max_log2, 24)), 256, 0, ctx->stream>>>(
+      ws.slots, ws.bloom, ws.meta, pred, host_log2, ws.max_log2);
+  int rc = after_launch(ctx, "join_init_kernel");
+  if (rc) return rc;
+  const void* kb = reinterpret_cast<const void*>(&join_build_kernel);
+  join_build_kernel<<<grid_for(ctx, kb, kBuildBlock, 0, (nb + kBuildRowsPerThread - 1) / kBuildRowsPerThread),
+                      kBuildBlock, 0, ctx->stream>>>(b, prm->date_lt, (uint32_t)prm->segment_eq, ws.slots, ws.bloom,
+                                                     ws.meta, limit);
+  if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
+  for (int64_t c = 0; c < in.chunks; ++c) {
+    const int64_t lo = c * kStreamChunkRows, n = std::max<int64_t>(0, std::min(np - lo, kStreamChunkRows));
+    BO_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ev[3 + c], 0));
+    const bo_join_probe_cols pc = {s.fk + lo, in.price ? in.price + lo : nullptr, in.disc ? in.disc + lo : nullptr, n};
+    if ((rc = launch_probe(ctx, pc, ws, s.part + c, mode, limit))) return rc;
+  }
+  join_combine_kernel<<<1, 32, 0, ctx->stream>>>(s.part, in.chunks, s.combined);
+  if ((rc = after_launch(ctx, "join_combine_kernel"))) return rc;
+  BO_CUDA(ctx, cudaEventRecord(ev[set], ctx->stream));
+  return BO_OK;
+}
+
 }  // namespace
 }  // namespace bo
 
@@ -572,6 +731,70 @@ int bo_join_host(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join_probe_
   if ((rc = join_workspace(ctx, b.n_rows, &ws))) return rc;
   BO_CUDA(ctx, cudaMemcpyAsync(ws.pred, &predicted_rows, sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   return bo_join_presized(ctx, &b, &p, prm, ws.pred, out_host);
+}
+
+// Streamed join over pinned host columns (see include/bespoke_gpu.h).
+int bo_join_stream_host(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join_probe_cols* ph,
+                        const bo_join_params* prm, const float* pred_device, bo_join_result* out_host) {
+  BO_CHECK_CTX(ctx);
+  if (!out_host) return set_error(ctx, BO_ERR_INVALID, "join_stream: null output");
+  StreamIn in;
+  int rc = stream_check(ctx, bh, ph, prm, &in);
+  if (rc) return rc;
+  JoinWs ws;
+  StreamSet s;
+  const int set = ctx->stream_set ^= 1;
+  if ((rc = join_workspace(ctx, bh->n_rows, &ws)) || (rc = stream_set(ctx, bh->n_rows, ph->n_rows, in.chunks, set, &s)) ||
+      (rc = stream_events(ctx, in.chunks)) || (rc = stream_copies(ctx, bh, ph, in, s, set)))
+    return rc;
+  int32_t cl = 0;
+  if (!pred_device) {  // exact-count form: one host round trip, as bo_join_plain
+    BO_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->events[2], 0));
+    const bo_join_build_cols b = {in.key, s.date, s.seg, bh->n_rows};
+    BO_CUDA(ctx, cudaMemsetAsync(&ws.meta->count, 0, sizeof(unsigned long long), ctx->stream));
+    const void* kc = reinterpret_cast<const void*>(&join_count_kernel);
+    join_count_kernel<<<grid_for(ctx, kc, kBuildBlock, 0, (bh->n_rows + 3) / 4), kBuildBlock, 0, ctx->stream>>>(
+        b, prm->date_lt, (uint32_t)prm->segment_eq, &ws.meta->count);
+    if ((rc = after_launch(ctx, "join_count_kernel"))) return rc;
+    unsigned long long count = 0;
+    BO_CUDA(ctx, cudaMemcpyAsync(&count, &ws.meta->count, sizeof(count), cudaMemcpyDeviceToHost, ctx->stream));
+    BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    cl = std::min(ws.max_log2, std::max(kMinCapLog2, ceil_log2(std::max<uint64_t>(count, 1) * 2)));
+  }
+  if ((rc = stream_compute(ctx, bh, ph, prm, pred_device, cl, ws, in, s, set))) return rc;
+  BO_CUDA(ctx, cudaMemcpyAsync(out_host, s.combined, sizeof(bo_join_result), cudaMemcpyDeviceToHost, ctx->stream));
+  uint32_t bits = 0;
+  if ((rc = consume_device_errors(ctx, &bits))) return rc;  // synchronises the stream
+  if ((rc = device_error_status(ctx, bits, "join_stream"))) return rc;
+  out_host->mode = pred_device ? 1 : 0;
+  if (out_host->overflowed && pred_device) {  // the prediction was too low: rerun with the exact count
+    if ((rc = bo_join_stream_host(ctx, bh, ph, prm, nullptr, out_host))) return rc;
+    out_host->reruns = 1;
+    out_host->mode = 1;
+    return BO_OK;
+  }
+  if (out_host->overflowed) return set_error(ctx, BO_ERR_OVERFLOW, "join_stream: exact-size table overflowed");
+  return BO_OK;
+}
+
+int bo_join_stream_host_async(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join_probe_cols* ph,
+                              const bo_join_params* prm, const float* pred_device, bo_join_result* out_pinned) {
+  BO_CHECK_CTX(ctx);
+  if (!pred_device || !out_pinned) return set_error(ctx, BO_ERR_INVALID, "join_stream_async: null prediction/output");
+  if (!mapped_device_pointer(out_pinned))
+    return set_error(ctx, BO_ERR_INVALID, "join_stream_async: the result must be pinned host memory");
+  StreamIn in;
+  int rc = stream_check(ctx, bh, ph, prm, &in);
+  if (rc) return rc;
+  JoinWs ws;
+  StreamSet s;
+  const int set = ctx->stream_set ^= 1;
+  if ((rc = join_workspace(ctx, bh->n_rows, &ws)) || (rc = stream_set(ctx, bh->n_rows, ph->n_rows, in.chunks, set, &s)) ||
+      (rc = stream_events(ctx, in.chunks)) || (rc = stream_copies(ctx, bh, ph, in, s, set)) ||
+      (rc = stream_compute(ctx, bh, ph, prm, pred_device, 0, ws, in, s, set)))
+    return rc;
+  BO_CUDA(ctx, cudaMemcpyAsync(out_pinned, s.combined, sizeof(bo_join_result), cudaMemcpyDeviceToHost, ctx->stream));
+  return BO_OK;
 }
 
 }  // extern "C"

@@ -277,3 +277,48 @@ class Engine:
         self.ctx.call("bo_radix_sort_pairs_host", C.c_void_p(k.ctypes.data), C.c_void_p(v.ctypes.data), len(k),
                       begin_bit, end_bit)
         return k, v
+
+
+class PinnedColumns:
+    """numpy arrays copied into pinned, mapped host buffers (the inputs of the
+    streamed entry points); freed with close()."""
+
+    def __init__(self, engine: Engine, arrays: dict):
+        self.engine = engine
+        self.ptrs = {}
+        for name, a in arrays.items():
+            a = np.ascontiguousarray(a)
+            h = C.c_void_p()
+            engine.ctx.call("bo_host_alloc_pinned", C.c_size_t(max(a.nbytes, 64)), C.byref(h))
+            if a.nbytes:
+                C.memmove(h.value, a.ctypes.data, a.nbytes)
+            self.ptrs[name] = h.value
+
+    def close(self):
+        for p in self.ptrs.values():
+            self.engine.ctx.call("bo_host_free_pinned", C.c_void_p(p))
+        self.ptrs.clear()
+
+
+def join_stream(engine: Engine, pc: PinnedColumns, n_build: int, n_probe: int, date_lt: int, seg_eq: int,
+                pred_dev=None) -> dict:
+    """bo_join_stream_host over pinned columns named b_key, b_date, b_seg,
+    p_fk, p_price, p_disc."""
+    p = pc.ptrs
+    b = N.JoinBuildCols(p["b_key"], p["b_date"], p["b_seg"], n_build)
+    pr = N.JoinProbeCols(p["p_fk"], p["p_price"], p["p_disc"], n_probe)
+    out = N.JoinResult()
+    engine.ctx.call("bo_join_stream_host", C.byref(b), C.byref(pr), C.byref(N.JoinParams(date_lt, seg_eq)),
+                    C.c_void_p(N.ptr(pred_dev)), C.byref(out))
+    return out.as_dict()
+
+
+def join_stream_async(engine: Engine, pc: PinnedColumns, n_build: int, n_probe: int, date_lt: int, seg_eq: int,
+                      pred_dev, out_pinned_addr: int) -> None:
+    """bo_join_stream_host_async: enqueue one presized streamed join whose
+    result lands at out_pinned_addr (pinned host memory) after a synchronize."""
+    p = pc.ptrs
+    b = N.JoinBuildCols(p["b_key"], p["b_date"], p["b_seg"], n_build)
+    pr = N.JoinProbeCols(p["p_fk"], p["p_price"], p["p_disc"], n_probe)
+    engine.ctx.call("bo_join_stream_host_async", C.byref(b), C.byref(pr), C.byref(N.JoinParams(date_lt, seg_eq)),
+                    C.c_void_p(N.ptr(pred_dev)), C.c_void_p(out_pinned_addr))

@@ -279,6 +279,10 @@ _SIGNATURES = {
     "bo_batch_num_items": (C.c_int32, [_P]),
     "bo_batch_destroy": (None, [_P]),
     "bo_join_probe_device": (C.c_int, [_P, C.POINTER(JoinProbeCols), _P]),
+    "bo_join_stream_host": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
+                                      _P, C.POINTER(JoinResult)]),
+    "bo_join_stream_host_async": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols),
+                                            C.POINTER(JoinParams), _P, _P]),
     "bo_join_host": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
                                C.c_int32, C.c_float, C.POINTER(JoinResult)]),
 }

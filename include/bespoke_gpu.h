@@ -260,6 +260,23 @@ int bo_join_probe_device(bo_ctx* ctx, const bo_join_probe_cols* probe, bo_join_r
 int bo_join_host(bo_ctx* ctx, const bo_join_build_cols* build_host, const bo_join_probe_cols* probe_host,
                  const bo_join_params* params, int32_t mode, float predicted_rows, bo_join_result* out_host);
 
+/* Streamed form for inputs in pinned host memory (bo_host_alloc_pinned or
+ * cudaHostRegister'd): only the columns every row needs cross PCIe as copies
+ * (build date and segment, probe fk, the latter in 1M-row chunks overlapped
+ * with the probe of the previous chunks); the build keys of qualifying rows
+ * and the price / discount of matching rows are read in place by the kernels
+ * (zero-copy).  pred_device = NULL runs the exact-count form; otherwise the
+ * table is presized from the device prediction and rerun exactly on overflow. */
+int bo_join_stream_host(bo_ctx* ctx, const bo_join_build_cols* build_host, const bo_join_probe_cols* probe_host,
+                        const bo_join_params* prm, const float* pred_device, bo_join_result* out_host);
+/* The presized streamed form without waiting: the result lands in out_pinned
+ * (pinned host memory) once the context's stream reaches it (bo_synchronize /
+ * bo_check_errors).  Consecutive calls overlap one query's copies with the
+ * previous query's kernels (two buffer sets).  A result with `overflowed` set
+ * is invalid: rerun that query with bo_join_stream_host. */
+int bo_join_stream_host_async(bo_ctx* ctx, const bo_join_build_cols* build_host, const bo_join_probe_cols* probe_host,
+                              const bo_join_params* prm, const float* pred_device, bo_join_result* out_pinned);
+
 /* =============================================================== GROUP-BY ==
  * Skewed three-way join + high-cardinality group-by + ordered top-k.  Restates
  * the dense-mask / per-id count pattern of run_q1a
