@@ -71,6 +71,14 @@ int device_error_status(bo_ctx* ctx, uint32_t bits, const char* op);
 // Blocks per SM from the occupancy calculator, cached per kernel.
 int occupancy_blocks(const void* kernel, int block, size_t smem);
 
+// Next `count` elements of a workspace carved from one region, 256-byte aligned.
+template <class T>
+T* carve(char*& p, size_t count) {
+  T* r = reinterpret_cast<T*>(p);
+  p += (sizeof(T) * count + 255) & ~size_t(255);
+  return r;
+}
+
 // Stable LSD radix sort of (key, value) pairs by bits [begin_bit, end_bit)
 // (csrc/radix_sort.cu); n_dev, if given, is the actual count (<= n) on the device.
 int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsigned long long* tmp_keys,

@@ -571,13 +571,6 @@ struct GbWs {
   int64_t mask_words;
 };
 
-template <class T>
-T* carve(char*& p, size_t count) {
-  T* r = reinterpret_cast<T*>(p);
-  p += (sizeof(T) * count + 255) & ~size_t(255);
-  return r;
-}
-
 int gb_workspace(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, int32_t a_id_max, GbWs* ws) {
   const uint64_t groups_max = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)a_id_max + 1, (uint64_t)b.n_rows));
   const int32_t max_log2 = std::max(kGbMinCapLog2, bit_length(groups_max * 2 - 1));

@@ -141,13 +141,6 @@ __global__ void q3_gather_kernel(const uint32_t* __restrict__ vals, const unsign
   }
 }
 
-template <class T>
-T* carve(char*& p, size_t count) {
-  T* r = reinterpret_cast<T*>(p);
-  p += (sizeof(T) * count + 255) & ~size_t(255);
-  return r;
-}
-
 int grid_of(bo_ctx* ctx, int64_t items) {
   const int64_t need = (items + kQ3Block - 1) / kQ3Block;
   return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)ctx->num_sms * 8));

@@ -7,6 +7,7 @@
 #include <parquet/arrow/reader.h>
 
 #include <algorithm>
+#include <charconv>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -159,13 +160,42 @@ std::vector<int16_t> date_offsets(const std::shared_ptr<arrow::ChunkedArray>& c,
   return out;
 }
 
-// Dictionary codes in first-appearance order (strings, large strings or
-// dictionary-encoded strings; nulls as the empty string).
+// Calls fn(value) for each value of a string column (strings, large strings
+// or dictionary-encoded strings; nulls as the empty string).
+template <class F>
+void for_each_string(const std::shared_ptr<arrow::ChunkedArray>& c, F fn) {
+  for (const auto& chunk : c->chunks()) {
+    switch (chunk->type_id()) {
+      case arrow::Type::STRING: {
+        const auto a = std::static_pointer_cast<arrow::StringArray>(chunk);
+        for (int64_t i = 0; i < a->length(); ++i) fn(a->IsNull(i) ? std::string_view() : a->GetView(i));
+        break;
+      }
+      case arrow::Type::LARGE_STRING: {
+        const auto a = std::static_pointer_cast<arrow::LargeStringArray>(chunk);
+        for (int64_t i = 0; i < a->length(); ++i) fn(a->IsNull(i) ? std::string_view() : a->GetView(i));
+        break;
+      }
+      case arrow::Type::DICTIONARY: {
+        const auto a = std::static_pointer_cast<arrow::DictionaryArray>(chunk);
+        const auto values = std::static_pointer_cast<arrow::StringArray>(a->dictionary());
+        for (int64_t i = 0; i < a->length(); ++i)
+          fn(a->IsNull(i) ? std::string_view() : values->GetView(a->GetValueIndex(i)));
+        break;
+      }
+      default:
+        throw std::runtime_error("Unsupported string column type: " + chunk->type()->ToString());
+    }
+  }
+}
+
+// Dictionary codes in first-appearance order.
 std::vector<uint16_t> dictionary_codes(const std::shared_ptr<arrow::ChunkedArray>& c, Dictionary& dict) {
   std::vector<uint16_t> codes;
   codes.reserve(c->length());
   std::unordered_map<std::string, uint16_t> ids;
-  auto add = [&](const std::string& v) {
+  for_each_string(c, [&](std::string_view sv) {
+    std::string v(sv);
     auto it = ids.find(v);
     if (it != ids.end()) {
       codes.push_back(it->second);
@@ -174,33 +204,23 @@ std::vector<uint16_t> dictionary_codes(const std::shared_ptr<arrow::ChunkedArray
     if (dict.values.size() > 0xffff) throw std::runtime_error("Dictionary column exceeds uint16_t capacity");
     const uint16_t id = static_cast<uint16_t>(dict.values.size());
     ids.emplace(v, id);
-    dict.values.push_back(v);
+    dict.values.push_back(std::move(v));
     codes.push_back(id);
-  };
-  for (const auto& chunk : c->chunks()) {
-    switch (chunk->type_id()) {
-      case arrow::Type::STRING: {
-        const auto a = std::static_pointer_cast<arrow::StringArray>(chunk);
-        for (int64_t i = 0; i < a->length(); ++i) add(a->IsNull(i) ? std::string() : a->GetString(i));
-        break;
-      }
-      case arrow::Type::LARGE_STRING: {
-        const auto a = std::static_pointer_cast<arrow::LargeStringArray>(chunk);
-        for (int64_t i = 0; i < a->length(); ++i) add(a->IsNull(i) ? std::string() : a->GetString(i));
-        break;
-      }
-      case arrow::Type::DICTIONARY: {
-        const auto a = std::static_pointer_cast<arrow::DictionaryArray>(chunk);
-        const auto values = std::static_pointer_cast<arrow::StringArray>(a->dictionary());
-        for (int64_t i = 0; i < a->length(); ++i)
-          add(a->IsNull(i) ? std::string() : values->GetString(a->GetValueIndex(i)));
-        break;
-      }
-      default:
-        throw std::runtime_error("Unsupported string column type: " + chunk->type()->ToString());
-    }
-  }
+  });
   return codes;
+}
+
+// Concatenated values with offsets (the reference's StringColumn layout).
+StringColumn string_column(const std::shared_ptr<arrow::ChunkedArray>& c) {
+  StringColumn out;
+  out.offsets.reserve(c->length() + 1);
+  out.offsets.push_back(0);
+  for_each_string(c, [&](std::string_view v) {
+    out.data.append(v);
+    if (out.data.size() > 0xffffffffull) throw std::runtime_error("String column exceeds 4 GiB");
+    out.offsets.push_back(static_cast<uint32_t>(out.data.size()));
+  });
+  return out;
 }
 
 template <class T>
@@ -229,11 +249,22 @@ std::string escape_csv(const std::string& v) {
   return out;
 }
 
-int16_t date_offset_of(const std::string& text, int32_t base_days, int add_years = 0) {
-  int y = std::stoi(text.substr(0, 4)) + add_years;
-  const int m = std::stoi(text.substr(5, 2));
+// "YYYY-MM-DD" plus add_months, the day clamped to the target month's length
+// (the reference's parse_date_offset(_add_*) helpers, e.g.
+// bespoke_tpch/query_q10.cpp:47-75), as a day offset from base_days.
+int16_t date_offset_of(const std::string& text, int32_t base_days, int add_months = 0) {
+  int y = std::stoi(text.substr(0, 4));
+  int m = std::stoi(text.substr(5, 2));
   int d = std::stoi(text.substr(8, 2));
-  if (add_years) {  // the same day of month, clamped to the target month's length
+  if (add_months) {
+    int index = m - 1 + add_months;
+    y += index / 12;
+    index %= 12;
+    if (index < 0) {
+      index += 12;
+      y -= 1;
+    }
+    m = index + 1;
     static const int kDays[] = {31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
     const bool leap = (y % 4 == 0 && y % 100 != 0) || y % 400 == 0;
     const int dim = (m == 2 && leap) ? 29 : kDays[m - 1];
@@ -303,7 +334,7 @@ std::vector<Q1ResultRow> run_q1(const Database& db, const std::string& delta) {
 std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, const std::string& discount,
                                 const std::string& quantity) {
   const int16_t start = date_offset_of(date, db.base_date_days);
-  const int16_t end = date_offset_of(date, db.base_date_days, 1);
+  const int16_t end = date_offset_of(date, db.base_date_days, 12);
   const int32_t d = scaled_arg(discount, kDiscountScale);
   const int32_t q = scaled_arg(quantity, kPriceScale);
   bo_lineitem_cols c{};
@@ -358,7 +389,130 @@ std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, 
   return rows;
 }
 
+std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date) {
+  const int16_t start = date_offset_of(date, db.base_date_days);
+  const int16_t end = date_offset_of(date, db.base_date_days, 3);
+  int32_t rf = -1;
+  for (size_t i = 0; i < db.returnflag.values.size(); ++i)
+    if (db.returnflag.values[i] == "R") {
+      rf = static_cast<int32_t>(i);
+      break;
+    }
+  if (rf < 0) return {};
+  const int32_t ls_count = static_cast<int32_t>(db.linestatus.values.size());
+  bo_tpch_q10_tables t{};
+  t.o_orderkey = col<int32_t>(db.o_orderkey);
+  t.o_custkey = col<int32_t>(db.o_custkey);
+  t.o_orderdate = col<int16_t>(db.o_orderdate);
+  t.o_li_begin = col<uint32_t>(db.o_li_begin);
+  t.o_li_end = col<uint32_t>(db.o_li_end);
+  t.n_orders = db.n_orders;
+  t.l_orderkey = col<int32_t>(db.l_orderkey);
+  t.l_returnflag_linestatus = col<uint8_t>(db.l_returnflag_linestatus);
+  t.l_discounted_price = col<int32_t>(db.l_discounted_price);
+  t.n_lineitem = db.n_lineitem;
+  t.lineitem_orderkey_sorted = db.lineitem_orderkey_sorted ? 1 : 0;
+  t.nation_bound = db.nation_bound;
+  t.custkey_to_row = col<int32_t>(db.custkey_to_row);
+  t.n_custkey_map = db.n_custkey_map;
+  t.c_nationkey = col<int32_t>(db.c_nationkey);
+  t.n_customer = db.n_customer;
+  std::vector<bo_tpch_q10_row> out(static_cast<size_t>(std::max<int64_t>(db.n_custkey_map, 1)));
+  int64_t n = 0;
+  check(db.ctx, bo_tpch_q10(db.ctx, &t, start, end, rf * ls_count, ls_count, out.data(), db.n_custkey_map, &n),
+        "q10");
+  std::vector<Q10ResultRow> rows(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    const auto& g = out[i];
+    const size_t r = static_cast<size_t>(g.cust_row);
+    auto& row = rows[i];
+    row.custkey = g.custkey;
+    row.name = db.c_name.view(r);
+    row.revenue_raw = g.revenue_raw;
+    row.acctbal_raw = db.c_acctbal[r];
+    row.nation_name = db.nation_name[static_cast<size_t>(g.nationkey)];
+    row.address = db.c_address.view(r);
+    row.phone = db.c_phone.view(r);
+    row.comment = db.c_comment.view(r);
+  }
+  return rows;
+}
+
+std::vector<Q18ResultRow> run_q18(const Database& db, const std::string& quantity) {
+  if (quantity == "<<NULL>>") return {};
+  const int32_t threshold = scaled_arg(quantity, kPriceScale);
+  int32_t max_key = db.max_lineitem_orderkey;
+  if (db.n_orderkey_map > 0) max_key = std::max(max_key, static_cast<int32_t>(db.n_orderkey_map - 1));
+  bo_tpch_q18_tables t{};
+  t.o_orderkey = col<int32_t>(db.o_orderkey);
+  t.o_custkey = col<int32_t>(db.o_custkey);
+  t.o_orderdate = col<int16_t>(db.o_orderdate);
+  t.o_totalprice = col<int32_t>(db.o_totalprice);
+  t.n_orders = db.n_orders;
+  t.l_orderkey = col<int32_t>(db.l_orderkey);
+  t.l_quantity = col<int16_t>(db.l_quantity);
+  t.n_lineitem = db.n_lineitem;
+  t.custkey_to_row = col<int32_t>(db.custkey_to_row);
+  t.n_custkey_map = db.n_custkey_map;
+  t.n_customer = db.n_customer;
+  t.orderkey_bound = max_key >= 0 ? static_cast<int64_t>(max_key) + 1 : 0;
+  t.dense_orderkeys = db.dense_orderkeys ? 1 : 0;
+  t.dense_custkeys = db.dense_custkeys ? 1 : 0;
+  std::vector<bo_tpch_q18_row> out(static_cast<size_t>(std::max<int64_t>(db.n_orders, 1)));
+  int64_t n = 0;
+  check(db.ctx, bo_tpch_q18(db.ctx, &t, threshold, out.data(), db.n_orders, &n), "q18");
+  std::vector<Q18ResultRow> rows(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    const auto& g = out[i];
+    auto& row = rows[i];
+    row.c_name = std::string(db.c_name.view(static_cast<size_t>(g.cust_row)));
+    row.c_custkey = g.custkey;
+    row.o_orderkey = g.orderkey;
+    row.o_orderdate_offset = g.orderdate_offset;
+    row.o_totalprice_raw = g.totalprice_raw;
+    row.sum_qty_raw = g.sum_qty_raw;
+  }
+  return rows;
+}
+
 // ------------------------------------------------------------------ output --
+namespace {
+
+std::string format_date(int32_t base_days, int16_t offset) {
+  int y = 0;
+  unsigned m = 0, d = 0;
+  civil_from_days(base_days + offset, y, m, d);
+  std::ostringstream date;
+  date << std::setw(4) << std::setfill('0') << y << '-' << std::setw(2) << std::setfill('0') << m << '-'
+       << std::setw(2) << std::setfill('0') << d;
+  return date.str();
+}
+
+void append_csv_field(std::string& out, std::string_view v) {
+  out.push_back('"');
+  for (char ch : v) {
+    if (ch == '"') out.push_back('\\');
+    out.push_back(ch);
+  }
+  out.push_back('"');
+}
+
+// Sign, integer part and two decimals of a x100 value (query_q10.cpp:110-123).
+void append_fixed_2(std::string& out, int64_t v) {
+  if (v < 0) {
+    out.push_back('-');
+    v = -v;
+  }
+  char buf[32];
+  const auto res = std::to_chars(std::begin(buf), std::end(buf), v / kPriceScale);
+  out.append(buf, res.ptr);
+  out.push_back('.');
+  out.push_back(static_cast<char>('0' + (v % kPriceScale) / 10));
+  out.push_back(static_cast<char>('0' + (v % kPriceScale) % 10));
+}
+
+}  // namespace
+
 void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& rows) {
   std::ofstream out(filename);
   out << "l_returnflag,l_linestatus,sum_qty,sum_base_price,sum_disc_price,sum_charge,avg_qty,avg_price,avg_disc,"
@@ -378,14 +532,54 @@ void write_q3_csv(const Database& db, const std::string& filename, const std::ve
   out.setf(std::ios::fixed);
   out << std::setprecision(2);
   for (const auto& r : rows) {
-    int y = 0;
-    unsigned m = 0, d = 0;
-    civil_from_days(db.base_date_days + r.orderdate_offset, y, m, d);
-    std::ostringstream date;
-    date << std::setw(4) << std::setfill('0') << y << '-' << std::setw(2) << std::setfill('0') << m << '-'
-         << std::setw(2) << std::setfill('0') << d;
-    out << r.orderkey << ',' << static_cast<double>(r.revenue_raw) / kPriceScale << ',' << date.str() << ','
-        << r.shippriority << "\n";
+    out << r.orderkey << ',' << static_cast<double>(r.revenue_raw) / kPriceScale << ','
+        << format_date(db.base_date_days, r.orderdate_offset) << ',' << r.shippriority << "\n";
+  }
+}
+
+
+void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows) {
+  std::ofstream out(filename, std::ios::binary);
+  std::string buf;
+  buf.reserve(1 << 20);
+  buf.append("c_custkey,c_name,revenue,c_acctbal,n_name,c_address,c_phone,c_comment\n");
+  for (const auto& r : rows) {
+    char ib[32];
+    const auto res = std::to_chars(std::begin(ib), std::end(ib), r.custkey);
+    buf.append(ib, res.ptr);
+    buf.push_back(',');
+    append_csv_field(buf, r.name);
+    buf.push_back(',');
+    append_fixed_2(buf, r.revenue_raw);
+    buf.push_back(',');
+    append_fixed_2(buf, r.acctbal_raw);
+    buf.push_back(',');
+    append_csv_field(buf, r.nation_name);
+    buf.push_back(',');
+    append_csv_field(buf, r.address);
+    buf.push_back(',');
+    append_csv_field(buf, r.phone);
+    buf.push_back(',');
+    append_csv_field(buf, r.comment);
+    buf.push_back('\n');
+    if (buf.size() >= (1u << 20)) {
+      out.write(buf.data(), static_cast<std::streamsize>(buf.size()));
+      buf.clear();
+    }
+  }
+  out.write(buf.data(), static_cast<std::streamsize>(buf.size()));
+}
+
+void write_q18_csv(const Database& db, const std::string& filename, const std::vector<Q18ResultRow>& rows) {
+  std::ofstream out(filename);
+  out << "c_name,c_custkey,o_orderkey,o_orderdate,o_totalprice,sum(l_quantity)\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows) {
+    out << escape_csv(r.c_name) << ',' << r.c_custkey << ',' << r.o_orderkey << ','
+        << format_date(db.base_date_days, r.o_orderdate_offset) << ','
+        << static_cast<double>(r.o_totalprice_raw) / kPriceScale << ','
+        << static_cast<double>(r.sum_qty_raw) / kPriceScale << "\n";
   }
 }
 
@@ -406,7 +600,8 @@ Database::~Database() {
   if (!ctx) return;
   DeviceColumn* cols[] = {&l_orderkey, &l_shipdate, &l_returnflag_linestatus, &l_extendedprice, &l_discounted_price,
                           &l_discount, &l_tax, &l_quantity, &o_orderkey, &o_custkey, &o_orderdate,
-                          &o_shippriority, &orderkey_to_row, &c_custkey, &c_mktsegment, &scratch};
+                          &o_shippriority, &o_totalprice, &orderkey_to_row, &o_li_begin, &o_li_end,
+                          &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
   bo_destroy(ctx);
@@ -464,6 +659,10 @@ Database* build(ParquetTables* tables) {
       code[i] = static_cast<uint8_t>(rf[i] * ls_count + ls[i]);
     }
     db->n_lineitem = static_cast<int64_t>(n);
+    for (size_t i = 0; i < n; ++i) {  // builder_impl.cpp:569-577
+      if (i > 0 && orderkey[i] < orderkey[i - 1]) db->lineitem_orderkey_sorted = false;
+      db->max_lineitem_orderkey = std::max(db->max_lineitem_orderkey, orderkey[i]);
+    }
     db->l_orderkey = upload(ctx, orderkey);
     db->l_shipdate = upload(ctx, ship);
     db->l_returnflag_linestatus = upload(ctx, code);
@@ -481,11 +680,13 @@ Database* build(ParquetTables* tables) {
     const auto ckey = int_values(column(O, "o_custkey"));
     const auto odate = date_offsets(column(O, "o_orderdate"), db->base_date_days);
     const auto prio = int_values(column(O, "o_shippriority"));
+    const auto total = scaled_values(column(O, "o_totalprice"), kPriceScale);
     std::vector<uint32_t> order(okey.size());
     std::iota(order.begin(), order.end(), 0u);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return odate[a] < odate[b]; });
     const auto sk = permute(okey, order), sc = permute(ckey, order), sp = permute(prio, order);
     const auto sd = permute(odate, order);
+    const auto st = permute(total, order);
     int32_t max_key = -1;
     for (int32_t k : sk) max_key = std::max(max_key, k);
     std::vector<int32_t> map(max_key >= 0 ? static_cast<size_t>(max_key) + 1 : 0, -1);
@@ -497,19 +698,57 @@ Database* build(ParquetTables* tables) {
     db->o_custkey = upload(ctx, sc);
     db->o_orderdate = upload(ctx, sd);
     db->o_shippriority = upload(ctx, sp);
+    db->o_totalprice = upload(ctx, st);
     db->orderkey_to_row = upload(ctx, map);
+    db->dense_orderkeys = !sk.empty() && sk.front() == 1 && sk.back() == static_cast<int32_t>(sk.size());
+    // Per-order lineitem ranges (builder_impl.cpp:930-990), built on the device.
+    check(ctx, bo_device_alloc(ctx, std::max<size_t>(4 * sk.size(), 256), &db->o_li_begin.ptr), "device alloc");
+    check(ctx, bo_device_alloc(ctx, std::max<size_t>(4 * sk.size(), 256), &db->o_li_end.ptr), "device alloc");
+    db->o_li_begin.rows = db->o_li_end.rows = db->n_orders;
+    check(ctx,
+          bo_tpch_order_ranges(ctx, col<int32_t>(db->l_orderkey), db->n_lineitem, col<int32_t>(db->orderkey_to_row),
+                               db->n_orderkey_map, db->n_orders, static_cast<uint32_t*>(db->o_li_begin.ptr),
+                               static_cast<uint32_t*>(db->o_li_end.ptr)),
+          "order ranges");
   }
-  // customer: keys and market-segment codes (bespoke_tpch/builder_impl.cpp:670-700).
+  // customer: keys, market-segment codes, nationkeys, the custkey -> row map
+  // and the strings of result rows (bespoke_tpch/builder_impl.cpp:670-700).
   {
     const auto& C = tables->customer;
     const auto ckey = int_values(column(C, "c_custkey"));
     const auto seg = dictionary_codes(column(C, "c_mktsegment"), db->mktsegment);
+    const auto nkey = int_values(column(C, "c_nationkey"));
     int32_t max_key = 0;
     for (int32_t k : ckey) max_key = std::max(max_key, k);
     db->n_customer = static_cast<int64_t>(ckey.size());
     db->custkey_bound = ckey.empty() ? 0 : max_key + 1;
+    db->dense_custkeys =
+        !ckey.empty() && ckey.front() == 1 && ckey.back() == static_cast<int32_t>(ckey.size());
+    std::vector<int32_t> map(ckey.empty() ? 0 : static_cast<size_t>(max_key) + 1, -1);
+    for (size_t i = 0; i < ckey.size(); ++i)
+      if (ckey[i] >= 0) map[static_cast<size_t>(ckey[i])] = static_cast<int32_t>(i);
+    db->n_custkey_map = static_cast<int64_t>(map.size());
     db->c_custkey = upload(ctx, ckey);
     db->c_mktsegment = upload(ctx, seg);
+    db->c_nationkey = upload(ctx, nkey);
+    db->custkey_to_row = upload(ctx, map);
+    db->c_acctbal = scaled_values(column(C, "c_acctbal"), kPriceScale);
+    db->c_name = string_column(column(C, "c_name"));
+    db->c_address = string_column(column(C, "c_address"));
+    db->c_phone = string_column(column(C, "c_phone"));
+    db->c_comment = string_column(column(C, "c_comment"));
+  }
+  // nation names by key (bespoke_tpch/builder_impl.cpp:780-803; query_q10.cpp:497-515)
+  {
+    const auto& N = tables->nation;
+    const auto key = int_values(column(N, "n_nationkey"));
+    const auto name = string_column(column(N, "n_name"));
+    int32_t max_key = 0;
+    for (int32_t k : key) max_key = std::max(max_key, k);
+    db->nation_bound = max_key + 1;
+    db->nation_name.assign(static_cast<size_t>(db->nation_bound), std::string());
+    for (size_t i = 0; i < key.size(); ++i)
+      if (key[i] >= 0) db->nation_name[static_cast<size_t>(key[i])] = std::string(name.view(i));
   }
   check(ctx, bo_device_alloc(ctx, sizeof(bo_q1_agg) * BO_Q1_MAX_GROUPS + 256, &db->scratch.ptr), "scratch alloc");
   check(ctx, bo_synchronize(ctx), "build");
@@ -556,6 +795,18 @@ void query(Database* db) {
       const auto rows = run_q3(*db, segment, date);
       const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
       write_q3_csv(*db, file, rows);
+      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+    } else if (r.id == "10") {
+      const std::string date = arg("DATE");
+      const auto rows = run_q10(*db, date);
+      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      write_q10_csv(file, rows);
+      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+    } else if (r.id == "18") {
+      const std::string quantity = arg("QUANTITY");
+      const auto rows = run_q18(*db, quantity);
+      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      write_q18_csv(*db, file, rows);
       std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
     } else if (r.id == "6") {
       const std::string date = arg("DATE");

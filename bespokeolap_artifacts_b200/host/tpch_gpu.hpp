@@ -8,9 +8,10 @@
 // storage-plan columns the hot path reads (the reference builder's rules,
 // bespoke_tpch/builder_impl.cpp:447-999, restated) and uploads them once;
 // query() speaks the same stdin / result<idx>.csv / "Execution ms" protocol
-// (bespoke_tpch/query_impl.cpp:142-389) and runs Q1, Q3 and Q6 on the GPU
-// through the C ABI of include/bespoke_gpu.h.  Result structs and CSV formats
-// are the reference's (query_q1.hpp:9-20, query_q3.hpp:10-15, query_q6.hpp).
+// (bespoke_tpch/query_impl.cpp:142-389) and runs Q1, Q3, Q6, Q10 and Q18 on
+// the GPU through the C ABI of include/bespoke_gpu.h.  Result structs and CSV
+// formats are the reference's (query_q1.hpp:9-20, query_q3.hpp:10-15,
+// query_q6.hpp, query_q10.hpp:10-19, query_q18.hpp:10-17).
 // Requests for other query ids get the reference's stub CSV
 // (query_impl.cpp:98-103): this library has no CPU implementation of them.
 #pragma once
@@ -20,6 +21,7 @@
 #include <cstdint>
 #include <memory>
 #include <string>
+#include <string_view>
 #include <vector>
 
 #include "bespoke_gpu.h"
@@ -49,10 +51,20 @@ struct Dictionary {
   std::vector<std::string> values;  // first-appearance order
 };
 
+// Host strings the result rows carry: values concatenated, row i at
+// [offsets[i], offsets[i + 1]) (bespoke_tpch/builder_impl.hpp StringColumn).
+struct StringColumn {
+  std::string data;
+  std::vector<uint32_t> offsets;
+  std::string_view view(size_t row) const {
+    return std::string_view(data.data() + offsets[row], offsets[row + 1] - offsets[row]);
+  }
+};
+
 }  // namespace bo_tpch
 
-// GPU-resident database: the storage-plan columns of the three tables the
-// hot path reads, on the device; dictionaries and sizes on the host.
+// GPU-resident database: the storage-plan columns the GPU queries read, on
+// the device; dictionaries, sizes and the strings of result rows on the host.
 struct Database {
   int32_t base_date_days = 0;
   bo_ctx* ctx = nullptr;
@@ -61,15 +73,26 @@ struct Database {
   bo_tpch::DeviceColumn l_orderkey, l_shipdate, l_returnflag_linestatus, l_extendedprice, l_discounted_price,
       l_discount, l_tax, l_quantity;
   bo_tpch::Dictionary returnflag, linestatus;
-  // orders, sorted by orderdate (stable)
+  bool lineitem_orderkey_sorted = true;
+  int32_t max_lineitem_orderkey = -1;
+  // orders, sorted by orderdate (stable); each row's lineitem range
   int64_t n_orders = 0;
-  bo_tpch::DeviceColumn o_orderkey, o_custkey, o_orderdate, o_shippriority, orderkey_to_row;
+  bo_tpch::DeviceColumn o_orderkey, o_custkey, o_orderdate, o_shippriority, o_totalprice, orderkey_to_row,
+      o_li_begin, o_li_end;
   int64_t n_orderkey_map = 0;
-  // customer
+  bool dense_orderkeys = false;  // first orderkey 1, last n_orders (date order)
+  // customer; custkey_to_row keeps the last row of each custkey >= 0
   int64_t n_customer = 0;
   int32_t custkey_bound = 0;
-  bo_tpch::DeviceColumn c_custkey, c_mktsegment;
+  bool dense_custkeys = false;  // first custkey 1, last n_customer
+  bo_tpch::DeviceColumn c_custkey, c_mktsegment, c_nationkey, custkey_to_row;
+  int64_t n_custkey_map = 0;
   bo_tpch::Dictionary mktsegment;
+  std::vector<int32_t> c_acctbal;
+  bo_tpch::StringColumn c_name, c_address, c_phone, c_comment;
+  // nation names by nationkey in [0, nation_bound) (last row of each key)
+  int32_t nation_bound = 1;
+  std::vector<std::string> nation_name;
   // Result record of the last scan-agg / Q6 query.  Queries on one Database
   // run one at a time (as the reference's single-threaded query()).
   bo_tpch::DeviceColumn scratch;
@@ -105,20 +128,45 @@ struct Q6ResultRow {
   int64_t revenue_raw = 0;
 };
 
+struct Q10ResultRow {
+  int32_t custkey = 0;
+  std::string_view name;
+  int64_t revenue_raw = 0;
+  int32_t acctbal_raw = 0;
+  std::string_view nation_name;
+  std::string_view address;
+  std::string_view phone;
+  std::string_view comment;
+};
+
+struct Q18ResultRow {
+  std::string c_name;
+  int32_t c_custkey = 0;
+  int32_t o_orderkey = 0;
+  int16_t o_orderdate_offset = 0;
+  int32_t o_totalprice_raw = 0;
+  int64_t sum_qty_raw = 0;
+};
+
 namespace bo_tpch {
 
 int64_t days_from_civil(int64_t y, unsigned m, unsigned d);
 void civil_from_days(int64_t z, int& y, unsigned& m, unsigned& d);
 
 // Run on the GPU; the arguments are the request's strings (DELTA; SEGMENT,
-// DATE; DATE, DISCOUNT, QUANTITY), parsed as the reference parses them.
+// DATE; DATE, DISCOUNT, QUANTITY; DATE; QUANTITY), parsed as the reference
+// parses them.
 std::vector<Q1ResultRow> run_q1(const Database& db, const std::string& delta);
 std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, const std::string& date);
 std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, const std::string& discount,
                                 const std::string& quantity);
+std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date);
+std::vector<Q18ResultRow> run_q18(const Database& db, const std::string& quantity);
 
 void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& rows);
 void write_q3_csv(const Database& db, const std::string& filename, const std::vector<Q3ResultRow>& rows);
 void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& rows);
+void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows);
+void write_q18_csv(const Database& db, const std::string& filename, const std::vector<Q18ResultRow>& rows);
 
 }  // namespace bo_tpch

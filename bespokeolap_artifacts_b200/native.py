@@ -179,6 +179,37 @@ class TpchQ3Row(C.Structure):
                 ("orderdate_offset", C.c_int16), ("pad0", C.c_int16), ("pad1", C.c_int32)]
 
 
+class TpchQ10Tables(C.Structure):
+    """``bo_tpch_q10_tables``: orders with lineitem ranges, lineitem, customer map and nations."""
+    _fields_ = [("o_orderkey", C.c_void_p), ("o_custkey", C.c_void_p), ("o_orderdate", C.c_void_p),
+                ("o_li_begin", C.c_void_p), ("o_li_end", C.c_void_p), ("n_orders", C.c_int64),
+                ("l_orderkey", C.c_void_p), ("l_returnflag_linestatus", C.c_void_p),
+                ("l_discounted_price", C.c_void_p), ("n_lineitem", C.c_int64),
+                ("lineitem_orderkey_sorted", C.c_int32), ("nation_bound", C.c_int32),
+                ("custkey_to_row", C.c_void_p), ("n_custkey_map", C.c_int64), ("c_nationkey", C.c_void_p),
+                ("n_customer", C.c_int64)]
+
+
+class TpchQ10Row(C.Structure):
+    _fields_ = [("revenue_raw", C.c_int64), ("custkey", C.c_int32), ("cust_row", C.c_int32),
+                ("nationkey", C.c_int32), ("pad0", C.c_int32)]
+
+
+class TpchQ18Tables(C.Structure):
+    """``bo_tpch_q18_tables``: orders, lineitem quantities, customer map, key-layout flags."""
+    _fields_ = [("o_orderkey", C.c_void_p), ("o_custkey", C.c_void_p), ("o_orderdate", C.c_void_p),
+                ("o_totalprice", C.c_void_p), ("n_orders", C.c_int64), ("l_orderkey", C.c_void_p),
+                ("l_quantity", C.c_void_p), ("n_lineitem", C.c_int64), ("custkey_to_row", C.c_void_p),
+                ("n_custkey_map", C.c_int64), ("n_customer", C.c_int64), ("orderkey_bound", C.c_int64),
+                ("dense_orderkeys", C.c_int32), ("dense_custkeys", C.c_int32)]
+
+
+class TpchQ18Row(C.Structure):
+    _fields_ = [("sum_qty_raw", C.c_int64), ("custkey", C.c_int32), ("cust_row", C.c_int32),
+                ("orderkey", C.c_int32), ("totalprice_raw", C.c_int32), ("orderdate_offset", C.c_int16),
+                ("pad0", C.c_int16), ("pad1", C.c_int32)]
+
+
 BATCH_SCAN_AGG, BATCH_JOIN, BATCH_GROUPBY = 0, 1, 2
 BATCH_MAX_CATS = 64
 
@@ -268,6 +299,11 @@ _SIGNATURES = {
     "bo_mlp_predict_counts": (C.c_int, [_P, _P, _P, _P, _P]),
     "bo_tpch_q3": (C.c_int, [_P, C.POINTER(TpchQ3Tables), C.c_int16, C.c_int32, C.POINTER(TpchQ3Row), C.c_int64,
                              C.POINTER(C.c_int64)]),
+    "bo_tpch_order_ranges": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, C.c_int64, _P, _P]),
+    "bo_tpch_q10": (C.c_int, [_P, C.POINTER(TpchQ10Tables), C.c_int16, C.c_int16, C.c_int32, C.c_int32,
+                              C.POINTER(TpchQ10Row), C.c_int64, C.POINTER(C.c_int64)]),
+    "bo_tpch_q18": (C.c_int, [_P, C.POINTER(TpchQ18Tables), C.c_int32, C.POINTER(TpchQ18Row), C.c_int64,
+                              C.POINTER(C.c_int64)]),
     "bo_batch_create": (C.c_int, [_P, C.POINTER(BatchInstance), C.c_int32, C.c_int32, C.POINTER(_P)]),
     "bo_batch_create_pool": (C.c_int, [_P, C.c_int32, C.c_int64, C.c_int64, C.c_int32, C.POINTER(_P)]),
     "bo_batch_update": (C.c_int, [_P, _P, C.POINTER(BatchInstance), C.c_int32]),

@@ -406,6 +406,112 @@ typedef struct bo_tpch_q3_row {   /* Q3ResultRow fields (bespoke_tpch/query_q3.h
 int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* tables, int16_t date_offset, int32_t segment_code,
                bo_tpch_q3_row* out_host, int64_t max_rows, int64_t* n_rows);
 
+/* ===================================================== TPC-H order ranges ==
+ * Build step of the reference's per-order lineitem ranges
+ * (bespoke_tpch/builder_impl.cpp:930-990): for each orders row r,
+ * [begin[r], end[r]) spans the first to the last lineitem whose orderkey maps
+ * to r through orderkey_to_row; end[r] == 0 when none does.  For lineitems
+ * sorted by orderkey that is the orderkey's run, as in the reference's sorted
+ * branch; otherwise the same min / max bounds as its unsorted branch.  Device
+ * pointers; n_lineitem < 2^32. */
+int bo_tpch_order_ranges(bo_ctx* ctx, const int32_t* l_orderkey, int64_t n_lineitem, const int32_t* orderkey_to_row,
+                         int64_t n_orderkey_map, int64_t n_orders, uint32_t* begin, uint32_t* end);
+
+/* =============================================================== TPC-H Q10 ==
+ * run_q10 over the storage-plan layout (bespoke_tpch/query_q10.cpp:375-585):
+ * orders dated in [start, end) (orders sorted by orderdate, so these are the
+ * reference's lower_bound range, :411-424) whose custkey is in
+ * [0, n_custkey_map); each order's revenue = sum of discounted_price over the
+ * lineitems of its range with a group code in [group_lo, group_lo +
+ * group_count) (returnflag 'R' x every linestatus, :396-405), checking the
+ * lineitem's orderkey unless lineitem_orderkey_sorted (:450-476); orders with
+ * revenue != 0 add it to their customer; every such customer that has a row
+ * (custkey_to_row >= 0) and a nationkey in [0, nation_bound), sorted by
+ * revenue descending as an unsigned 64-bit value (:352-371), then custkey
+ * ascending. */
+typedef struct bo_tpch_q10_tables {
+  const int32_t* o_orderkey;
+  const int32_t* o_custkey;
+  const int16_t* o_orderdate;         /* ascending */
+  const uint32_t* o_li_begin;         /* bo_tpch_order_ranges */
+  const uint32_t* o_li_end;
+  int64_t n_orders;
+  const int32_t* l_orderkey;
+  const uint8_t* l_returnflag_linestatus;
+  const int32_t* l_discounted_price;  /* x100 */
+  int64_t n_lineitem;
+  int32_t lineitem_orderkey_sorted;   /* l_orderkey non-decreasing (builder_impl.cpp:569-577) */
+  int32_t nation_bound;               /* max(0, max n_nationkey) + 1 */
+  const int32_t* custkey_to_row;      /* last customer row of each custkey >= 0; -1 if none */
+  int64_t n_custkey_map;              /* max custkey + 1 (0 if no customer) */
+  const int32_t* c_nationkey;         /* per customer row */
+  int64_t n_customer;
+} bo_tpch_q10_tables;
+
+typedef struct bo_tpch_q10_row {      /* Q10ResultRow keys (bespoke_tpch/query_q10.hpp:10-19) */
+  int64_t revenue_raw;                /* x100 */
+  int32_t custkey;
+  int32_t cust_row;                   /* customer row: name, acctbal, address, phone, comment */
+  int32_t nationkey;
+  int32_t pad0;
+} bo_tpch_q10_row;
+
+/* Device columns in, rows on the host (first min(n, max_rows); *n_rows = n).
+ * group_lo < 0 ('R' not in the returnflag dictionary) gives no rows. */
+int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* tables, int16_t start_offset, int16_t end_offset,
+                int32_t group_lo, int32_t group_count, bo_tpch_q10_row* out_host, int64_t max_rows,
+                int64_t* n_rows);
+
+/* =============================================================== TPC-H Q18 ==
+ * run_q18 over the storage-plan layout (bespoke_tpch/query_q18.cpp:183-455):
+ * sum_qty[k] = sum of l_quantity over the lineitems of orderkey k; orders
+ * whose sum exceeds the threshold, with their customer, sorted by totalprice
+ * desc, orderdate asc, orderkey asc.  The reference's two paths:
+ *   dense_orderkeys (the date-sorted orders start with orderkey 1 and end with
+ *   orderkey n_orders, :204-206): lineitem orderkeys index [0, n_orders]
+ *   (others are an error here); orderkey k in [1, n_orders] qualifies and
+ *   reads orders row k - 1 (:207-290); its customer row is custkey - 1 when
+ *   dense_custkeys, else custkey_to_row;
+ *   otherwise: sums over [0, orderkey_bound); every orders row whose
+ *   orderkey's sum exceeds the threshold, customer row from custkey_to_row
+ *   (:292-434).
+ * The dense path qualifies an order when its running sum first exceeds the
+ * threshold (:232-238); with negative quantities that differs from the final
+ * sum, so a negative quantity there is an error.  A custkey outside the map
+ * has no customer row (the reference reads past its map there). */
+typedef struct bo_tpch_q18_tables {
+  const int32_t* o_orderkey;          /* date-sorted orders */
+  const int32_t* o_custkey;
+  const int16_t* o_orderdate;
+  const int32_t* o_totalprice;        /* x100 */
+  int64_t n_orders;
+  const int32_t* l_orderkey;          /* 16-byte aligned */
+  const int16_t* l_quantity;          /* x100, 16-byte aligned */
+  int64_t n_lineitem;
+  const int32_t* custkey_to_row;      /* last customer row of each custkey >= 0; -1 if none */
+  int64_t n_custkey_map;              /* max custkey + 1 (0 if no customer) */
+  int64_t n_customer;
+  int64_t orderkey_bound;             /* max(max o_orderkey, max l_orderkey) + 1 */
+  int32_t dense_orderkeys;
+  int32_t dense_custkeys;             /* customer keys start at 1 and end at n_customer */
+} bo_tpch_q18_tables;
+
+typedef struct bo_tpch_q18_row {      /* Q18ResultRow fields (bespoke_tpch/query_q18.hpp:10-17) */
+  int64_t sum_qty_raw;                /* x100 */
+  int32_t custkey;
+  int32_t cust_row;                   /* customer row: c_name */
+  int32_t orderkey;
+  int32_t totalprice_raw;             /* x100 */
+  int16_t orderdate_offset;
+  int16_t pad0;
+  int32_t pad1;
+} bo_tpch_q18_row;
+
+/* quantity_threshold x100 (llround of QUANTITY * 100, :198-199).  Rows as in
+ * bo_tpch_q10. */
+int bo_tpch_q18(bo_ctx* ctx, const bo_tpch_q18_tables* tables, int32_t quantity_threshold,
+                bo_tpch_q18_row* out_host, int64_t max_rows, int64_t* n_rows);
+
 /* ================================================================= BATCH ==
  * Many pipelines of uneven sizes in ONE persistent kernel fed by a device work
  * queue of (instance, stage, tile) items, captured in a CUDA graph.  Stages of

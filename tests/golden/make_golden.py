@@ -26,7 +26,7 @@ Q1_CASES = [(1, 100_000), (2, 4_099), (3, 1), (4, 7)]
 Q1_DELTAS = [90, 60, 3000]
 Q3_CASES = [(5, 20_000, 80_000), (6, 1_000, 4_003), (7, 3, 10)]
 Q6_CASES = [(8, 50_000)]
-Q6_PARAMS = [("1994-01-01", "0.06", "24"), ("1996-01-01", "0.02", "40"), ("1992-03-15", "0.09", "10")]
+Q6_PARAMS = [("1994-02-01", "0.07", "23"), ("1996-01-01", "0.02", "40"), ("1992-03-15", "0.09", "10")]
 
 
 def q1_fixture():

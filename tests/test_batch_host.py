@@ -76,3 +76,23 @@ def test_q3_struct_layout_matches_header(tmp_path):
     want = [C.sizeof(N.TpchQ3Tables), C.sizeof(N.TpchQ3Row), N.TpchQ3Tables.o_orderkey.offset,
             N.TpchQ3Tables.l_orderkey.offset, N.TpchQ3Row.orderdate_offset.offset]
     assert got == want
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="needs gcc")
+def test_q10_q18_struct_layouts_match_header(tmp_path):
+    src = tmp_path / "q10layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "bespoke_gpu.h"\n'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
+        ' sizeof(bo_tpch_q10_tables), sizeof(bo_tpch_q10_row), sizeof(bo_tpch_q18_tables), sizeof(bo_tpch_q18_row),'
+        ' offsetof(bo_tpch_q10_tables, lineitem_orderkey_sorted), offsetof(bo_tpch_q10_tables, n_customer),'
+        ' offsetof(bo_tpch_q10_row, nationkey), offsetof(bo_tpch_q18_tables, orderkey_bound),'
+        ' offsetof(bo_tpch_q18_tables, dense_custkeys), offsetof(bo_tpch_q18_row, orderdate_offset)); return 0;}\n')
+    exe = tmp_path / "q10layout"
+    subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = [C.sizeof(N.TpchQ10Tables), C.sizeof(N.TpchQ10Row), C.sizeof(N.TpchQ18Tables), C.sizeof(N.TpchQ18Row),
+            N.TpchQ10Tables.lineitem_orderkey_sorted.offset, N.TpchQ10Tables.n_customer.offset,
+            N.TpchQ10Row.nationkey.offset, N.TpchQ18Tables.orderkey_bound.offset,
+            N.TpchQ18Tables.dense_custkeys.offset, N.TpchQ18Row.orderdate_offset.offset]
+    assert got == want

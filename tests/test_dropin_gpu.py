@@ -2,9 +2,12 @@
 query (bespokeolap_artifacts_b200/host) and the reference's own load / build /
 query (compiled unchanged into oracle/_ref/ref_tpch_driver) read the same
 Parquet files and the same stdin requests; their result<idx>.csv files must
-agree: Q1 and Q6 byte for byte, Q3 row for row (the reference's std::sort
-leaves rows equal in revenue and orderdate in unspecified order; the GPU
-emits them in orderkey order)."""
+agree: Q1, Q6, Q10 and Q18 byte for byte, Q3 row for row (the reference's
+std::sort leaves rows equal in revenue and orderdate in unspecified order;
+the GPU emits them in orderkey order).  The key layouts select each of the
+reference's paths: dense and sparse orderkeys (Q18's two scans), dense,
+partly shuffled and sparse custkeys (its customer lookups), lineitems sorted
+by orderkey or not (Q10's two range loops)."""
 import csv
 import re
 import subprocess
@@ -22,8 +25,19 @@ REF_DRIVER = ROOT / "oracle" / "_ref" / "ref_tpch_driver"
 
 REQUESTS = [
     '1 "90"', '1 "60"', '1 "3"',
-    '3 "BUILDING" "1995-03-15"', '3 "AUTOMOBILE" "1993-06-30"', '3 "MACHINERY" "1997-12-31"', '3 "NOSUCH" "1995-03-15"',
-    '6 "1994-01-01" "0.06" "24"', '6 "1996-02-29" "0.05" "25"', '6 "1992-01-01" "0.10" "50"',
+    '3 "SEG_B" "1995-03-17"', '3 "SEG_A" "1993-06-30"', '3 "SEG_E" "1997-12-31"', '3 "NOSUCH" "1995-03-17"',
+    '6 "1994-02-01" "0.07" "23"', '6 "1996-02-29" "0.05" "25"', '6 "1992-01-01" "0.10" "50"',
+    '10 "1993-10-01"', '10 "1995-01-31"', '10 "1992-11-30"', '10 "1998-07-01"', '10 "1999-01-01"',
+    '18 "250"', '18 "150.5"', '18 "0"', '18 "-1"', '18 "400"', '18 "<<NULL>>"',
+]
+
+LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem)
+    (4, False, "sparse", "dense", False),
+    (3, True, "sparse", "dense", False),
+    (5, False, "dense", "inner", False),
+    (6, False, "dense", "sparse", False),
+    (7, False, "sparse", "sparse", True),
+    (8, False, "dense", "dense", True),
 ]
 
 
@@ -40,11 +54,13 @@ def q3_rows(path: Path):
     return rows[0], [(int(r[0]), r[1], r[2], r[3]) for r in rows[1:]]
 
 
-@pytest.mark.parametrize("decimal", [False, True])
-def test_dropin_matches_reference_driver(tmp_path, decimal):
+@pytest.mark.parametrize("layout", LAYOUTS, ids=lambda l: "-".join(map(str, l)))
+def test_dropin_matches_reference_driver(tmp_path, layout):
     if not REF_DRIVER.exists() or not GPU_DRIVER.exists():
         pytest.skip("drivers not built")
-    data = write_tpch(tmp_path / "data", seed=3 if decimal else 4, decimal=decimal)
+    seed, decimal, order_keys, customer_keys, shuffle = layout
+    data = write_tpch(tmp_path / "data", seed=seed, decimal=decimal, order_keys=order_keys,
+                      customer_keys=customer_keys, shuffle_lineitem=shuffle)
     out_gpu = run(GPU_DRIVER, data, tmp_path / "gpu", REQUESTS)
     out_ref = run(REF_DRIVER, data, tmp_path / "ref", REQUESTS)
     for out in (out_gpu, out_ref):
@@ -68,7 +84,7 @@ def test_dropin_stub_for_queries_off_the_gpu_path(tmp_path):
     if not GPU_DRIVER.exists():
         pytest.skip("driver not built")
     data = write_tpch(tmp_path / "data", n_customer=50, n_orders=200, seed=5)
-    run(GPU_DRIVER, data, tmp_path / "gpu", ['2 "15" "BRASS" "EUROPE"', '1 "90"'])
+    run(GPU_DRIVER, data, tmp_path / "gpu", ['2 "15" "PART_T" "REGION0"', '1 "90"'])
     assert (tmp_path / "gpu" / "result1.csv").read_text() == \
-        'query_id,params\n"2","2 \\"15\\" \\"BRASS\\" \\"EUROPE\\""\n'
+        'query_id,params\n"2","2 \\"15\\" \\"PART_T\\" \\"REGION0\\""\n'
     assert (tmp_path / "gpu" / "result2.csv").read_text().startswith("l_returnflag,")

@@ -1,0 +1,193 @@
+"""Q10, Q18 and the per-order lineitem ranges through the C ABI at sizes the
+drop-in files do not reach (millions of lineitems), against numpy
+restatements of run_q10 (bespoke_tpch/query_q10.cpp:375-585), run_q18
+(bespoke_tpch/query_q18.cpp:183-455) and the builder's ranges
+(bespoke_tpch/builder_impl.cpp:930-990); plus the entry points' error
+contract.  Byte-level parity with the reference itself is in
+test_dropin_gpu.py."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from bespokeolap_artifacts_b200 import native as N
+
+pytestmark = pytest.mark.gpu
+
+
+def tables(n_orders: int, seed: int, shuffle: bool = False, n_customer: int = 150_000):
+    rng = np.random.default_rng(seed)
+    okey = (np.arange(n_orders, dtype=np.int64) // 8 * 32 + np.arange(n_orders) % 8 + 1).astype(np.int32)
+    ocust = rng.integers(0, n_customer + 20, n_orders).astype(np.int32)  # some without a customer
+    odate = rng.integers(0, 2405, n_orders).astype(np.int16)
+    ototal = rng.integers(100_000, 50_000_000, n_orders).astype(np.int32)
+    order = np.argsort(odate, kind="stable")
+    okey, ocust, odate, ototal = okey[order], ocust[order], odate[order], ototal[order]
+    lines = rng.integers(1, 8, n_orders)
+    lkey = np.repeat(np.sort(okey), lines)
+    n = len(lkey)
+    if shuffle:
+        lkey = lkey[rng.permutation(n)]
+    lqty = (rng.integers(1, 51, n) * 100).astype(np.int16)
+    lcode = rng.integers(0, 6, n).astype(np.uint8)  # returnflag (3) x linestatus (2)
+    ldp = rng.integers(90_000, 10_500_000, n).astype(np.int32)
+    ckey = rng.permutation(np.arange(1, n_customer + 1, dtype=np.int32) * 2)[: n_customer]
+    cmap = np.full(int(ckey.max()) + 1, -1, np.int32)
+    cmap[ckey] = np.arange(n_customer, dtype=np.int32)
+    cnation = rng.integers(-1, 27, n_customer).astype(np.int32)
+    omap = np.full(int(okey.max()) + 1, -1, np.int32)
+    omap[okey] = np.arange(n_orders, dtype=np.int32)
+    return dict(okey=okey, ocust=ocust, odate=odate, ototal=ototal, lkey=lkey, lqty=lqty, lcode=lcode, ldp=ldp,
+                cmap=cmap, cnation=cnation, omap=omap, sorted=not shuffle)
+
+
+def dev(torch, d):
+    return {k: (torch.from_numpy(v).cuda() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
+
+
+def ranges(engine, torch, g, n_orders):
+    begin = torch.empty(n_orders, dtype=torch.int32, device="cuda")
+    end = torch.empty(n_orders, dtype=torch.int32, device="cuda")
+    engine.ctx.call("bo_tpch_order_ranges", C.c_void_p(g["lkey"].data_ptr()), g["lkey"].numel(),
+                    C.c_void_p(g["omap"].data_ptr()), g["omap"].numel(), n_orders, C.c_void_p(begin.data_ptr()),
+                    C.c_void_p(end.data_ptr()))
+    torch.cuda.synchronize()
+    return begin, end
+
+
+@pytest.mark.parametrize("shuffle", [False, True])
+def test_order_ranges(engine, torch_cuda, shuffle):
+    torch = torch_cuda
+    t = tables(200_000, 1, shuffle)
+    g = dev(torch, t)
+    begin, end = ranges(engine, torch, g, len(t["okey"]))
+    rows = t["omap"][t["lkey"]]
+    idx = np.arange(len(rows), dtype=np.int64)
+    want_b = np.full(len(t["okey"]), 0xFFFFFFFF, np.int64)
+    want_e = np.zeros(len(t["okey"]), np.int64)
+    np.minimum.at(want_b, rows, idx)
+    np.maximum.at(want_e, rows, idx + 1)
+    assert np.array_equal(begin.cpu().numpy().view(np.uint32).astype(np.int64), want_b)
+    assert np.array_equal(end.cpu().numpy().view(np.uint32).astype(np.int64), want_e)
+
+
+def q18_oracle(t, thr):
+    """Non-dense path (:292-434): every orders row whose orderkey's quantity
+    sum exceeds thr and whose customer has a row."""
+    sums = np.zeros(max(int(t["okey"].max()), int(t["lkey"].max())) + 1, np.int64)
+    np.add.at(sums, t["lkey"], t["lqty"].astype(np.int64))
+    s = sums[t["okey"]]
+    c = t["ocust"]
+    crow = np.where(c < len(t["cmap"]), t["cmap"][np.minimum(c, len(t["cmap"]) - 1)], -1)
+    keep = (s > thr) & (crow >= 0)
+    rows = np.nonzero(keep)[0]
+    order = np.lexsort((t["okey"][rows], t["odate"][rows], -t["ototal"][rows].astype(np.int64)))
+    rows = rows[order]
+    return s[rows], c[rows], crow[rows], t["okey"][rows], t["ototal"][rows], t["odate"][rows]
+
+
+@pytest.mark.parametrize("thr", [25_000, 30_000, 0])
+def test_q18_matches_numpy(engine, torch_cuda, thr):
+    torch = torch_cuda
+    t = tables(1_500_000, 2)
+    g = dev(torch, t)
+    tb = N.TpchQ18Tables()
+    tb.o_orderkey, tb.o_custkey = g["okey"].data_ptr(), g["ocust"].data_ptr()
+    tb.o_orderdate, tb.o_totalprice = g["odate"].data_ptr(), g["ototal"].data_ptr()
+    tb.n_orders = len(t["okey"])
+    tb.l_orderkey, tb.l_quantity, tb.n_lineitem = g["lkey"].data_ptr(), g["lqty"].data_ptr(), len(t["lkey"])
+    tb.custkey_to_row, tb.n_custkey_map = g["cmap"].data_ptr(), len(t["cmap"])
+    tb.n_customer = 150_000
+    tb.orderkey_bound = max(int(t["okey"].max()), int(t["lkey"].max())) + 1
+    out = (N.TpchQ18Row * len(t["okey"]))()
+    n = C.c_int64()
+    engine.ctx.call("bo_tpch_q18", C.byref(tb), thr, out, len(t["okey"]), C.byref(n))
+    want = q18_oracle(t, thr)
+    assert n.value == len(want[0]) and n.value > 0
+    got = np.frombuffer(out, dtype=np.dtype([("sum", "<i8"), ("cust", "<i4"), ("crow", "<i4"), ("okey", "<i4"),
+                                            ("total", "<i4"), ("date", "<i2"), ("p0", "<i2"), ("p1", "<i4")]))[: n.value]
+    for name, w in zip(("sum", "cust", "crow", "okey", "total", "date"), want):
+        assert np.array_equal(got[name], w), name
+
+
+def q10_oracle(t, start, end, glo, gcount, nation_bound):
+    n_map = len(t["cmap"])
+    rows = np.nonzero((t["odate"] >= start) & (t["odate"] < end) & (t["ocust"] >= 0) & (t["ocust"] < n_map))[0]
+    lrow = t["omap"][t["lkey"]]
+    ok = ((t["lcode"].astype(np.int64) - glo) >= 0) & ((t["lcode"].astype(np.int64) - glo) < gcount)
+    rev = np.zeros(len(t["okey"]), np.int64)
+    np.add.at(rev, lrow[ok], t["ldp"][ok].astype(np.int64))
+    rows = rows[rev[rows] != 0]
+    cust = np.zeros(n_map, np.int64)
+    hit = np.zeros(n_map, bool)
+    np.add.at(cust, t["ocust"][rows], rev[rows])
+    hit[t["ocust"][rows]] = True
+    ck = np.nonzero(hit)[0]
+    crow = t["cmap"][ck]
+    ck, crow = ck[crow >= 0], crow[crow >= 0]
+    nk = t["cnation"][crow]
+    sel = (nk >= 0) & (nk < nation_bound)
+    ck, crow, nk = ck[sel], crow[sel], nk[sel]
+    r = cust[ck]
+    order = np.lexsort((ck, ~r.view(np.uint64)))
+    return r[order], ck[order], crow[order], nk[order]
+
+
+@pytest.mark.parametrize("shuffle", [False, True])
+def test_q10_matches_numpy(engine, torch_cuda, shuffle):
+    torch = torch_cuda
+    t = tables(1_500_000, 3, shuffle)
+    g = dev(torch, t)
+    no = len(t["okey"])
+    begin, end = ranges(engine, torch, g, no)
+    tb = N.TpchQ10Tables()
+    tb.o_orderkey, tb.o_custkey, tb.o_orderdate = g["okey"].data_ptr(), g["ocust"].data_ptr(), g["odate"].data_ptr()
+    tb.o_li_begin, tb.o_li_end, tb.n_orders = begin.data_ptr(), end.data_ptr(), no
+    tb.l_orderkey, tb.l_returnflag_linestatus = g["lkey"].data_ptr(), g["lcode"].data_ptr()
+    tb.l_discounted_price, tb.n_lineitem = g["ldp"].data_ptr(), len(t["lkey"])
+    tb.lineitem_orderkey_sorted = 1 if t["sorted"] else 0
+    tb.nation_bound = 25
+    tb.custkey_to_row, tb.n_custkey_map = g["cmap"].data_ptr(), len(t["cmap"])
+    tb.c_nationkey, tb.n_customer = g["cnation"].data_ptr(), len(t["cnation"])
+    for start, end_ in [(640, 730), (0, 2405), (100, 100)]:
+        out = (N.TpchQ10Row * len(t["cmap"]))()
+        n = C.c_int64()
+        engine.ctx.call("bo_tpch_q10", C.byref(tb), start, end_, 2, 2, out, len(t["cmap"]), C.byref(n))
+        want = q10_oracle(t, start, end_, 2, 2, 25)
+        assert n.value == len(want[0])
+        got = np.frombuffer(out, dtype=np.dtype([("rev", "<i8"), ("cust", "<i4"), ("crow", "<i4"), ("nk", "<i4"),
+                                                ("p0", "<i4")]))[: n.value]
+        for name, w in zip(("rev", "cust", "crow", "nk"), want):
+            assert np.array_equal(got[name], w), (name, start, end_)
+    out = (N.TpchQ10Row * 1)()
+    n = C.c_int64(-1)
+    engine.ctx.call("bo_tpch_q10", C.byref(tb), 0, 2405, -1, 2, out, 1, C.byref(n))  # no 'R' in the dictionary
+    assert n.value == 0
+
+
+def test_q18_error_contract(engine, torch_cuda):
+    torch = torch_cuda
+    okey = torch.arange(1, 1001, dtype=torch.int32, device="cuda")
+    zeros16 = torch.zeros(1000, dtype=torch.int16, device="cuda")
+    ones32 = torch.ones(1000, dtype=torch.int32, device="cuda")
+    lkey = torch.arange(0, 1000, dtype=torch.int32, device="cuda")
+    lkey[500] = 1001  # beyond the dense sum array
+    qty = torch.full((1000,), 100, dtype=torch.int16, device="cuda")
+    tb = N.TpchQ18Tables()
+    tb.o_orderkey, tb.o_custkey, tb.o_orderdate, tb.o_totalprice = (okey.data_ptr(), ones32.data_ptr(),
+                                                                     zeros16.data_ptr(), ones32.data_ptr())
+    tb.n_orders, tb.l_orderkey, tb.l_quantity, tb.n_lineitem = 1000, lkey.data_ptr(), qty.data_ptr(), 1000
+    tb.n_customer, tb.dense_orderkeys, tb.dense_custkeys = 1, 1, 1
+    out = (N.TpchQ18Row * 1000)()
+    n = C.c_int64()
+    with pytest.raises(N.BoError) as e:
+        engine.ctx.call("bo_tpch_q18", C.byref(tb), 50, out, 1000, C.byref(n))
+    assert e.value.status == -6
+    lkey[500] = 500
+    engine.ctx.call("bo_tpch_q18", C.byref(tb), 50, out, 1000, C.byref(n))  # the context stays usable
+    assert n.value == 999  # orderkeys 1..999 have one lineitem each; every order maps to customer row 0
+    tb.l_orderkey = lkey.data_ptr() + 4
+    tb.n_lineitem = 999
+    with pytest.raises(N.BoError) as e:
+        engine.ctx.call("bo_tpch_q18", C.byref(tb), 50, out, 1000, C.byref(n))
+    assert e.value.status == -1
