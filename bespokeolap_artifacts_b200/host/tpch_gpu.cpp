@@ -438,6 +438,27 @@ std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date) {
   return rows;
 }
 
+std::vector<Q13ResultRow> run_q13(const Database& db, const std::string& word1, const std::string& word2) {
+  bo_tpch_q13_tables t{};
+  t.o_comment = col<uint8_t>(db.o_comment);
+  t.o_comment_offsets = col<uint32_t>(db.o_comment_offsets);
+  t.o_custkey = col<int32_t>(db.o_custkey);
+  t.n_orders = db.n_orders;
+  t.c_custkey = col<int32_t>(db.c_custkey);
+  t.n_customer = db.n_customer;
+  t.n_count_map = std::max<int64_t>(db.custkey_bound, 1);
+  const int64_t cap = db.n_orders + 1;  // distinct order counts
+  std::vector<bo_tpch_q13_row> out(static_cast<size_t>(cap));
+  int64_t n = 0;
+  check(db.ctx,
+        bo_tpch_q13(db.ctx, &t, word1.data(), static_cast<int64_t>(word1.size()), word2.data(),
+                    static_cast<int64_t>(word2.size()), out.data(), cap, &n),
+        "q13");
+  std::vector<Q13ResultRow> rows(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) rows[i] = Q13ResultRow{out[i].c_count, out[i].custdist};
+  return rows;
+}
+
 std::vector<Q18ResultRow> run_q18(const Database& db, const std::string& quantity) {
   if (quantity == "<<NULL>>") return {};
   const int32_t threshold = scaled_arg(quantity, kPriceScale);
@@ -570,6 +591,12 @@ void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>&
   out.write(buf.data(), static_cast<std::streamsize>(buf.size()));
 }
 
+void write_q13_csv(const std::string& filename, const std::vector<Q13ResultRow>& rows) {
+  std::ofstream out(filename);
+  out << "c_count,custdist\n";
+  for (const auto& r : rows) out << r.c_count << ',' << r.custdist << "\n";
+}
+
 void write_q18_csv(const Database& db, const std::string& filename, const std::vector<Q18ResultRow>& rows) {
   std::ofstream out(filename);
   out << "c_name,c_custkey,o_orderkey,o_orderdate,o_totalprice,sum(l_quantity)\n";
@@ -601,6 +628,7 @@ Database::~Database() {
   DeviceColumn* cols[] = {&l_orderkey, &l_shipdate, &l_returnflag_linestatus, &l_extendedprice, &l_discounted_price,
                           &l_discount, &l_tax, &l_quantity, &o_orderkey, &o_custkey, &o_orderdate,
                           &o_shippriority, &o_totalprice, &orderkey_to_row, &o_li_begin, &o_li_end,
+                          &o_comment, &o_comment_offsets,
                           &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
@@ -681,6 +709,7 @@ Database* build(ParquetTables* tables) {
     const auto odate = date_offsets(column(O, "o_orderdate"), db->base_date_days);
     const auto prio = int_values(column(O, "o_shippriority"));
     const auto total = scaled_values(column(O, "o_totalprice"), kPriceScale);
+    const auto comment = string_column(column(O, "o_comment"));
     std::vector<uint32_t> order(okey.size());
     std::iota(order.begin(), order.end(), 0u);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return odate[a] < odate[b]; });
@@ -701,6 +730,20 @@ Database* build(ParquetTables* tables) {
     db->o_totalprice = upload(ctx, st);
     db->orderkey_to_row = upload(ctx, map);
     db->dense_orderkeys = !sk.empty() && sk.front() == 1 && sk.back() == static_cast<int32_t>(sk.size());
+    {  // comments in the same date order (builder_impl.cpp:350-371, 607)
+      std::vector<uint8_t> bytes;
+      bytes.reserve(comment.data.size());
+      std::vector<uint32_t> offs;
+      offs.reserve(order.size() + 1);
+      offs.push_back(0);
+      for (const uint32_t i : order) {
+        const auto v = comment.view(i);
+        bytes.insert(bytes.end(), v.begin(), v.end());
+        offs.push_back(static_cast<uint32_t>(bytes.size()));
+      }
+      db->o_comment = upload(ctx, bytes);
+      db->o_comment_offsets = upload(ctx, offs);
+    }
     // Per-order lineitem ranges (builder_impl.cpp:930-990), built on the device.
     check(ctx, bo_device_alloc(ctx, std::max<size_t>(4 * sk.size(), 256), &db->o_li_begin.ptr), "device alloc");
     check(ctx, bo_device_alloc(ctx, std::max<size_t>(4 * sk.size(), 256), &db->o_li_end.ptr), "device alloc");
@@ -801,6 +844,13 @@ void query(Database* db) {
       const auto rows = run_q10(*db, date);
       const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
       write_q10_csv(file, rows);
+      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+    } else if (r.id == "13") {
+      const std::string word1 = arg("WORD1");
+      const std::string word2 = arg("WORD2");
+      const auto rows = run_q13(*db, word1, word2);
+      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      write_q13_csv(file, rows);
       std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
     } else if (r.id == "18") {
       const std::string quantity = arg("QUANTITY");

@@ -8,10 +8,10 @@
 // storage-plan columns the hot path reads (the reference builder's rules,
 // bespoke_tpch/builder_impl.cpp:447-999, restated) and uploads them once;
 // query() speaks the same stdin / result<idx>.csv / "Execution ms" protocol
-// (bespoke_tpch/query_impl.cpp:142-389) and runs Q1, Q3, Q6, Q10 and Q18 on
-// the GPU through the C ABI of include/bespoke_gpu.h.  Result structs and CSV
-// formats are the reference's (query_q1.hpp:9-20, query_q3.hpp:10-15,
-// query_q6.hpp, query_q10.hpp:10-19, query_q18.hpp:10-17).
+// (bespoke_tpch/query_impl.cpp:142-389) and runs Q1, Q3, Q6, Q10, Q13 and Q18
+// on the GPU through the C ABI of include/bespoke_gpu.h.  Result structs and
+// CSV formats are the reference's (query_q1.hpp:9-20, query_q3.hpp:10-15,
+// query_q6.hpp, query_q10.hpp:10-19, query_q13.hpp:9-12, query_q18.hpp:10-17).
 // Requests for other query ids get the reference's stub CSV
 // (query_impl.cpp:98-103): this library has no CPU implementation of them.
 #pragma once
@@ -78,7 +78,7 @@ struct Database {
   // orders, sorted by orderdate (stable); each row's lineitem range
   int64_t n_orders = 0;
   bo_tpch::DeviceColumn o_orderkey, o_custkey, o_orderdate, o_shippriority, o_totalprice, orderkey_to_row,
-      o_li_begin, o_li_end;
+      o_li_begin, o_li_end, o_comment, o_comment_offsets;
   int64_t n_orderkey_map = 0;
   bool dense_orderkeys = false;  // first orderkey 1, last n_orders (date order)
   // customer; custkey_to_row keeps the last row of each custkey >= 0
@@ -128,6 +128,11 @@ struct Q6ResultRow {
   int64_t revenue_raw = 0;
 };
 
+struct Q13ResultRow {
+  int64_t c_count = 0;
+  int64_t custdist = 0;
+};
+
 struct Q10ResultRow {
   int32_t custkey = 0;
   std::string_view name;
@@ -154,19 +159,21 @@ int64_t days_from_civil(int64_t y, unsigned m, unsigned d);
 void civil_from_days(int64_t z, int& y, unsigned& m, unsigned& d);
 
 // Run on the GPU; the arguments are the request's strings (DELTA; SEGMENT,
-// DATE; DATE, DISCOUNT, QUANTITY; DATE; QUANTITY), parsed as the reference
-// parses them.
+// DATE; DATE, DISCOUNT, QUANTITY; DATE; WORD1, WORD2; QUANTITY), parsed as the
+// reference parses them.
 std::vector<Q1ResultRow> run_q1(const Database& db, const std::string& delta);
 std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, const std::string& date);
 std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, const std::string& discount,
                                 const std::string& quantity);
 std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date);
+std::vector<Q13ResultRow> run_q13(const Database& db, const std::string& word1, const std::string& word2);
 std::vector<Q18ResultRow> run_q18(const Database& db, const std::string& quantity);
 
 void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& rows);
 void write_q3_csv(const Database& db, const std::string& filename, const std::vector<Q3ResultRow>& rows);
 void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& rows);
 void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows);
+void write_q13_csv(const std::string& filename, const std::vector<Q13ResultRow>& rows);
 void write_q18_csv(const Database& db, const std::string& filename, const std::vector<Q18ResultRow>& rows);
 
 }  // namespace bo_tpch

@@ -210,6 +210,17 @@ class TpchQ18Row(C.Structure):
                 ("pad0", C.c_int16), ("pad1", C.c_int32)]
 
 
+class TpchQ13Tables(C.Structure):
+    """``bo_tpch_q13_tables``: order comments (bytes + offsets), custkeys, customer keys."""
+    _fields_ = [("o_comment", C.c_void_p), ("o_comment_offsets", C.c_void_p), ("o_custkey", C.c_void_p),
+                ("n_orders", C.c_int64), ("c_custkey", C.c_void_p), ("n_customer", C.c_int64),
+                ("n_count_map", C.c_int64)]
+
+
+class TpchQ13Row(C.Structure):
+    _fields_ = [("c_count", C.c_int64), ("custdist", C.c_int64)]
+
+
 BATCH_SCAN_AGG, BATCH_JOIN, BATCH_GROUPBY = 0, 1, 2
 BATCH_MAX_CATS = 64
 
@@ -302,6 +313,8 @@ _SIGNATURES = {
     "bo_tpch_order_ranges": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, C.c_int64, _P, _P]),
     "bo_tpch_q10": (C.c_int, [_P, C.POINTER(TpchQ10Tables), C.c_int16, C.c_int16, C.c_int32, C.c_int32,
                               C.POINTER(TpchQ10Row), C.c_int64, C.POINTER(C.c_int64)]),
+    "bo_tpch_q13": (C.c_int, [_P, C.POINTER(TpchQ13Tables), C.c_char_p, C.c_int64, C.c_char_p, C.c_int64,
+                              C.POINTER(TpchQ13Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q18": (C.c_int, [_P, C.POINTER(TpchQ18Tables), C.c_int32, C.POINTER(TpchQ18Row), C.c_int64,
                               C.POINTER(C.c_int64)]),
     "bo_batch_create": (C.c_int, [_P, C.POINTER(BatchInstance), C.c_int32, C.c_int32, C.POINTER(_P)]),

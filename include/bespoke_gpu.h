@@ -512,6 +512,35 @@ typedef struct bo_tpch_q18_row {      /* Q18ResultRow fields (bespoke_tpch/query
 int bo_tpch_q18(bo_ctx* ctx, const bo_tpch_q18_tables* tables, int32_t quantity_threshold,
                 bo_tpch_q18_row* out_host, int64_t max_rows, int64_t* n_rows);
 
+/* =============================================================== TPC-H Q13 ==
+ * run_q13 (bespoke_tpch/query_q13.cpp:166-270): per custkey, the orders whose
+ * comment does NOT match word1 ... word2; then, per customer row, how many
+ * customers have each order count (c_count -> custdist), sorted by custdist
+ * desc, c_count desc.  The match is the reference's (:44-83): word1's first
+ * occurrence p, then word2 at or after p + len1; an empty word matches at the
+ * search start, but a search that starts at the comment's end finds nothing.
+ * (The reference's alpha / bigram masks only skip rows that cannot match.)
+ * An order whose custkey is outside [0, n_count_map) is an error (the
+ * reference indexes past its array there). */
+typedef struct bo_tpch_q13_tables {
+  const uint8_t* o_comment;           /* concatenated comment bytes, 16-byte aligned */
+  const uint32_t* o_comment_offsets;  /* n_orders + 1; comment i is [off[i], off[i + 1]) */
+  const int32_t* o_custkey;
+  int64_t n_orders;
+  const int32_t* c_custkey;
+  int64_t n_customer;
+  int64_t n_count_map;                /* max custkey + 1 */
+} bo_tpch_q13_tables;
+
+typedef struct bo_tpch_q13_row {      /* Q13ResultRow (bespoke_tpch/query_q13.hpp:9-12) */
+  int64_t c_count;
+  int64_t custdist;
+} bo_tpch_q13_row;
+
+/* word1 / word2: host bytes (not NUL-terminated).  Rows as in bo_tpch_q10. */
+int bo_tpch_q13(bo_ctx* ctx, const bo_tpch_q13_tables* tables, const char* word1, int64_t len1, const char* word2,
+                int64_t len2, bo_tpch_q13_row* out_host, int64_t max_rows, int64_t* n_rows);
+
 /* ================================================================= BATCH ==
  * Many pipelines of uneven sizes in ONE persistent kernel fed by a device work
  * queue of (instance, stage, tile) items, captured in a CUDA graph.  Stages of

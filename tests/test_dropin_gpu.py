@@ -2,7 +2,7 @@
 query (bespokeolap_artifacts_b200/host) and the reference's own load / build /
 query (compiled unchanged into oracle/_ref/ref_tpch_driver) read the same
 Parquet files and the same stdin requests; their result<idx>.csv files must
-agree: Q1, Q6, Q10 and Q18 byte for byte, Q3 row for row (the reference's
+agree: Q1, Q6, Q10, Q13 and Q18 byte for byte, Q3 row for row (the reference's
 std::sort leaves rows equal in revenue and orderdate in unspecified order;
 the GPU emits them in orderkey order).  The key layouts select each of the
 reference's paths: dense and sparse orderkeys (Q18's two scans), dense,
@@ -29,6 +29,8 @@ REQUESTS = [
     '6 "1994-02-01" "0.07" "23"', '6 "1996-02-29" "0.05" "25"', '6 "1992-01-01" "0.10" "50"',
     '10 "1993-10-01"', '10 "1995-01-31"', '10 "1992-11-30"', '10 "1998-07-01"', '10 "1999-01-01"',
     '18 "250"', '18 "150.5"', '18 "0"', '18 "-1"', '18 "400"', '18 "<<NULL>>"',
+    '13 "pending" "deposits"', '13 "quick" "quick"', '13 "" ""', '13 "bold" ""', '13 "" "final"',
+    '13 "x\\"y" "a,b"', '13 "ironic quick pending bold deposits final final" "x"', '13 "zzz" "ironic"',
 ]
 
 LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem)

@@ -191,3 +191,47 @@ def test_q18_error_contract(engine, torch_cuda):
     with pytest.raises(N.BoError) as e:
         engine.ctx.call("bo_tpch_q18", C.byref(tb), 50, out, 1000, C.byref(n))
     assert e.value.status == -1
+
+
+def q13_match(s: bytes, w1: bytes, w2: bytes) -> bool:
+    """matches_pattern of bespoke_tpch/query_q13.cpp:68-83 (first word1, then word2 after it)."""
+    n = len(s)
+    p1 = s.find(w1) if w1 else 0
+    if p1 < 0 or p1 == n:
+        return False
+    start = p1 + len(w1)
+    p2 = s.find(w2, start) if w2 else start
+    return p2 >= 0 and p2 != n
+
+
+@pytest.mark.parametrize("words", [(b"ab", b"ba"), (b"", b""), (b"a", b""), (b"", b"\x00\xff"), (b"abcab", b"c")])
+def test_q13_matches_python(engine, torch_cuda, words):
+    torch = torch_cuda
+    rng = np.random.default_rng(11)
+    n_orders, n_customer = 300_000, 20_000
+    lens = rng.integers(0, 40, n_orders)
+    lens[rng.integers(0, n_orders, 200)] = rng.integers(3000, 9000, 200)  # warps whose comments overflow the slice
+    alphabet = np.frombuffer(b"abc \x00\xff", np.uint8)
+    data = alphabet[rng.integers(0, len(alphabet), int(lens.sum()))]
+    offs = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint32)
+    ocust = rng.integers(0, n_customer + 1, n_orders).astype(np.int32)
+    ckey = rng.permutation(np.arange(1, n_customer + 1, dtype=np.int32))
+    ckey[-3:] = ckey[:3]  # repeated customer rows count twice
+    w1, w2 = words
+    raw = data.tobytes()
+    counts = np.zeros(n_customer + 1, np.int64)
+    for i in range(n_orders):
+        if not q13_match(raw[offs[i]:offs[i + 1]], w1, w2):
+            counts[ocust[i]] += 1
+    dist = np.bincount(counts[ckey])
+    want = sorted(((c, d) for c, d in enumerate(dist) if d), key=lambda r: (-r[1], -r[0]))
+    g = dev(torch, dict(data=data if len(data) else np.zeros(16, np.uint8), offs=offs.view(np.int32), ocust=ocust,
+                        ckey=ckey))
+    tb = N.TpchQ13Tables()
+    tb.o_comment, tb.o_comment_offsets, tb.o_custkey = g["data"].data_ptr(), g["offs"].data_ptr(), g["ocust"].data_ptr()
+    tb.n_orders, tb.c_custkey, tb.n_customer, tb.n_count_map = n_orders, g["ckey"].data_ptr(), n_customer, n_customer + 1
+    out = (N.TpchQ13Row * (n_orders + 1))()
+    n = C.c_int64()
+    for _ in range(2):  # the histogram is left clear for the next call
+        engine.ctx.call("bo_tpch_q13", C.byref(tb), w1, len(w1), w2, len(w2), out, n_orders + 1, C.byref(n))
+        assert [(out[i].c_count, out[i].custdist) for i in range(n.value)] == want

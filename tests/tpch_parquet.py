@@ -46,6 +46,11 @@ def _text(rng, n: int, words: int) -> list[str]:
     return [" ".join(WORDS[i] for i in row) for row in picks]
 
 
+def _ragged_text(rng, n: int, max_words: int) -> list[str]:
+    counts = rng.integers(0, max_words + 1, n)
+    return [" ".join(WORDS[i] for i in rng.integers(0, len(WORDS), c)) for c in counts]
+
+
 def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: int = 0,
                decimal: bool = False, order_keys: str = "sparse", customer_keys: str = "dense",
                shuffle_lineitem: bool = False) -> Path:
@@ -87,7 +92,7 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
         "o_totalprice": _dec(rng.integers(100000, 50000000, n_orders) / 100.0, decimal),
         "o_orderdate": pa.array(o_date, pa.date32()), "o_orderpriority": ["1-URGENT"] * n_orders,
         "o_clerk": ["Clerk#000000001"] * n_orders, "o_shippriority": np.zeros(n_orders, np.int32),
-        "o_comment": [""] * n_orders,
+        "o_comment": _ragged_text(rng, n_orders, 8),
     }), out / "orders.parquet")
     lines = rng.integers(1, 8, n_orders)
     lk = np.repeat(orderkey, lines)
