@@ -195,34 +195,61 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
             out.append(r)
         return out
 
-    # ---- warm-up
-    for i in range(W):
+    # ---- the step as the product runs it: one learned query (MLP prediction +
+    # init + build + probe, no host round trip) is one CUDA graph; one graph
+    # per input copy, each writing its own result record.
+    for i in range(3):
         learned_step(i, i)
     torch.cuda.synchronize()
+    step_graphs = []
+    kernels_per_step = 0
+    for k in range(3):
+        g = torch.cuda.CUDAGraph()
+        n0 = eng.launches
+        with torch.cuda.graph(g, stream=stream):
+            learned_step(k, k)
+        kernels_per_step = eng.launches - n0
+        step_graphs.append(g)
 
-    # ---- timed: K learned-sized queries, inputs resident, device-timed
+    # ---- warm-up
+    for i in range(W):
+        step_graphs[i % 3].replay()
+    torch.cuda.synchronize()
+
+    # ---- timed: K learned-sized queries (graph replays, copies rotated),
+    # inputs resident, device-timed
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    # The timed region lasts about a millisecond, shorter than nvidia-smi's
+    # sampling period, so the clocks are sampled over a window of ~0.6 s of
+    # the same step replays that ends with the timed region.
     sampler = ClockSampler(local_rank)
     sampler.start()
-    launches0 = eng.launches
+    t_win = time.perf_counter()
+    while time.perf_counter() - t_win < 0.6:
+        for i in range(64):
+            step_graphs[i % 3].replay()
+        torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     torch.cuda.nvtx.range_push("timed")  # lets a profiler select exactly the timed launches
     for i in range(K):
-        learned_step(i, W + i)
+        step_graphs[i % 3].replay()
     torch.cuda.nvtx.range_pop()
     ev1.record(stream)
     torch.cuda.synchronize()
-    launches = eng.launches - launches0
+    launches = K * kernels_per_step
     ms = ev0.elapsed_time(ev1)
-    # Any query whose presized table overflowed is rerun exactly (counted in time).
+    # Every replay of copy k's graph gives the same answer (checked against the
+    # eager warm-up runs); a query whose presized table overflowed is rerun
+    # exactly, and the rerun is counted in the time.
     reruns = 0
     t_fix = time.perf_counter()
-    for k, r in enumerate(check(range(W, W + K))):
-        if r["overflowed"]:
+    rs_last = check(range(3))
+    for k in range(K):
+        if rs_last[k % 3]["overflowed"]:
             c = copies[k % 3]
             eng.join_plain(c["b"], c["p"], N_BUILD, N_PROBE, c["j"].date_lt, c["j"].seg_eq)
             reruns += 1
@@ -231,9 +258,12 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
         dist.barrier()
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    rs = check(range(W, W + K))
-    for k, r in enumerate(rs):  # same copy -> same answer every time
-        assert r["match_count"] == rs[k % 3]["match_count"] and r["sum_exact"] == rs[k % 3]["sum_exact"]
+    clocks["window"] = "0.6 s of the same step replays, then the timed region"
+    rs = [rs_last[k % 3] for k in range(K)]
+    for k in range(3):  # graph replays agree with the eager runs of the same copy
+        c = copies[k]
+        ref = eng.join_plain(c["b"], c["p"], N_BUILD, N_PROBE, c["j"].date_lt, c["j"].seg_eq)
+        assert (rs_last[k]["match_count"], rs_last[k]["sum_exact"]) == (ref["match_count"], ref["sum_exact"])
     ms = max_over_ranks(ms, dist)
 
     # ---- per-query latency: learned vs plain (results on the host each time)
@@ -336,19 +366,29 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     eng.ctx.call("bo_host_free_pinned", res_pin)
     eng.ctx.call("bo_host_free_pinned", pred_pin)
 
-    # ---- roofline of the dominant kernel (probe), timed alone on the stream
+    # ---- roofline of the dominant kernel (probe), timed alone on the stream:
+    # one graph per probe copy (against the table of the last build), K
+    # replays back to back with the copies rotated, average per launch.
     outp = torch.zeros(res_sz, dtype=torch.uint8, device="cuda")
-    c0 = copies[(W + K - 1) % 3]
-    pev = []
-    for i in range(K + 3):
-        a = torch.cuda.Event(enable_timing=True)
-        e = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        eng.join_probe_device(copies[(W + K - 1) % 3]["p"], N_PROBE, outp)
-        e.record(stream)
-        pev.append((a, e))
+    probe_graphs = []
+    for k in range(3):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            eng.join_probe_device(copies[k]["p"], N_PROBE, outp)
+        probe_graphs.append(g)
+    for i in range(3):
+        probe_graphs[i % 3].replay()
     torch.cuda.synchronize()
-    probe_ms = statistics.mean(a.elapsed_time(e) for a, e in pev[3:])
+    pa = torch.cuda.Event(enable_timing=True)
+    pe = torch.cuda.Event(enable_timing=True)
+    n_probe_launches = max(K, 30)
+    pa.record(stream)
+    for i in range(n_probe_launches):
+        probe_graphs[i % 3].replay()
+    pe.record(stream)
+    torch.cuda.synchronize()
+    probe_ms = pa.elapsed_time(pe) / n_probe_launches
+    del probe_graphs
     peak, peak_kind = peaks()
     achieved = PROBE_BYTES / (probe_ms * 1e-3) / 1e9
     traffic = profile_traffic()

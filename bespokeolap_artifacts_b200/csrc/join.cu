@@ -14,13 +14,13 @@
 //                                  blocked Bloom filter per new key;
 //   probe  (K3)                    each block stages the 64 KB Bloom filter into
 //                                  shared memory with one TMA bulk copy; probe
-//                                  rows stream in 16 at a time (four 128-bit fk
-//                                  loads); a Bloom hit looks the key up in the
+//                                  rows stream in 8 per lane (one 256-bit fk
+//                                  load); a Bloom hit looks the key up in the
 //                                  table; only matching rows load their price and
 //                                  discount (late materialisation); exact
 //                                  fixed-point sums, 128-bit totals, last block
 //                                  writes the result.
-// Build-side keys are also late-materialised: only qualifying rows load their key.
+// Build-side keys are read densely with the filter columns (one streaming pass).
 #include <algorithm>
 
 #include "common.cuh"
@@ -112,10 +112,12 @@ __global__ void join_init_kernel(unsigned long long* slots, uint32_t* bloom, Joi
 
 // ------------------------------------------------------------ K2 build ---
 
-// 16 build rows per thread per step: one 128-bit segment load and four 128-bit
-// date loads; the qualifying rows (about 4%) of the whole warp are then
-// compacted into a shared-memory queue and their keys loaded and inserted by
-// all lanes together.
+// 16 build rows per thread per step: one 128-bit segment load and two 256-bit
+// loads each of dates and keys (the keys are read densely with the filter
+// columns: loading only the ~4% qualifying keys afterwards put one more
+// dependent DRAM round trip on every warp's path, 2 us per 1.5M-row build on
+// B200); the qualifying keys of the whole warp are then compacted into a
+// shared-memory queue and inserted by all lanes together.
 constexpr int kBuildRowsPerThread = 16;
 
 
@@ -128,7 +130,7 @@ __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_c
   const uint64_t mask = (1ull << cl) - 1;
   uint32_t qual = 0, newkeys = 0;
   bool full = false;
-  __shared__ uint32_t build_q[kBuildBlock / 32][32 * 8];
+  __shared__ uint32_t build_q[kBuildBlock / 32][32 * kBuildRowsPerThread];
   const int lane = threadIdx.x & 31;
   uint32_t* bq = build_q[threadIdx.x >> 5];
   const int64_t n = b.n_rows;
@@ -140,41 +142,44 @@ __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_c
   const int64_t steps_w = (steps + 31) & ~int64_t(31);
   for (int64_t st = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; st < steps_w; st += stride) {
     const int64_t r0 = st * kBuildRowsPerThread;
-    const int64_t wbase = (st - lane) * kBuildRowsPerThread;
     uint32_t q = 0;
+    int32_t keys[kBuildRowsPerThread];
     if (r0 >= n) {
-      // past the end: no rows
+#pragma unroll
+      for (int k = 0; k < kBuildRowsPerThread; ++k) keys[k] = 0;
     } else if (r0 + kBuildRowsPerThread <= n) {
       const int4 sg = ld_stream_v4(b.segment + r0);
       const uint32_t sw[4] = {(uint32_t)sg.x, (uint32_t)sg.y, (uint32_t)sg.z, (uint32_t)sg.w};
       const int8v d0 = ld_stream_v8(b.date + r0), d1 = ld_stream_v8(b.date + r0 + 8);
+      const int8v k0 = ld_stream_v8(b.key + r0), k1 = ld_stream_v8(b.key + r0 + 8);
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
+      for (int k = 0; k < kBuildRowsPerThread; ++k) {
         const int32_t dk = k < 8 ? d0.v[k] : d1.v[k - 8];
         q |= (uint32_t)build_qual(dk, (sw[k >> 2] >> (8 * (k & 3))) & 0xffu, date_lt, seg) << k;
+        keys[k] = k < 8 ? k0.v[k] : k1.v[k - 8];
       }
     } else {
-      for (int k = 0; k < kBuildRowsPerThread; ++k)
-        if (r0 + k < n && build_qual(b.date[r0 + k], b.segment[r0 + k], date_lt, seg)) q |= 1u << k;
+#pragma unroll
+      for (int k = 0; k < kBuildRowsPerThread; ++k) {
+        keys[k] = 0;
+        if (r0 + k < n && build_qual(b.date[r0 + k], b.segment[r0 + k], date_lt, seg)) {
+          q |= 1u << k;
+          keys[k] = b.key[r0 + k];
+        }
+      }
     }
     qual += __popc(q);
-    // Compact the qualifying rows of the whole warp into its queue so the key
-    // loads and CAS insertions spread over all 32 lanes: a lane whose rows all
-    // qualify would otherwise chain up to 16 dependent round trips.
+    // Compact the qualifying keys of the whole warp into its queue so the CAS
+    // insertions spread over all 32 lanes.
+    uint32_t total;
+    uint32_t pos = warp_exclusive_scan(__popc(q), total);
+    if (total == 0) continue;  // warp-uniform
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const uint32_t hm = (q >> (8 * half)) & 0xffu;
-      uint32_t total;
-      uint32_t pos = warp_exclusive_scan(__popc(hm), total);
-      if (total == 0) continue;  // warp-uniform
-#pragma unroll
-      for (int k = 0; k < 8; ++k)
-        if ((hm >> k) & 1u) bq[pos++] = (uint32_t)(r0 - wbase) + 8 * half + k;
-      __syncwarp();
-      for (uint32_t i = lane; i < total; i += 32)
-        join_insert(slots, bloom, mask, __ldg(b.key + wbase + bq[i]), newkeys, full, probe_limit);
-      __syncwarp();
-    }
+    for (int k = 0; k < kBuildRowsPerThread; ++k)
+      if ((q >> k) & 1u) bq[pos++] = (uint32_t)keys[k];
+    __syncwarp();
+    for (uint32_t i = lane; i < total; i += 32) join_insert(slots, bloom, mask, (int32_t)bq[i], newkeys, full, probe_limit);
+    __syncwarp();
   }
   // Block-level totals, then one atomic per counter per block.
   __shared__ uint32_t part[3][kBuildBlock / 32];
@@ -205,18 +210,20 @@ __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_c
 
 // ------------------------------------------------------------ K3 probe ---
 
-// Warp-centric probe.  A warp owns 512 consecutive probe rows per step (16 per
-// lane, four 128-bit fk loads).  Every lane hashes its rows and tests the Bloom
+// Warp-centric probe.  A warp owns 256 consecutive probe rows per step (8 per
+// lane, one 256-bit fk load).  Every lane hashes its rows and tests the Bloom
 // filter in shared memory without branching; the hits (about 9% of rows) are
 // compacted into a per-warp shared-memory queue (ballot-free: a warp prefix sum
 // of per-lane hit counts gives each lane its slot range), and then all 32 lanes
 // resolve queue entries together -- table lookups and the price / discount
 // loads of matches are issued by many lanes at once instead of one row at a
-// time.  The queue holds one half-step (8 rows per lane) at most.
+// time.  The queue holds a whole step.  (Steps of 512 rows resolved in two
+// halves took 32 us per 6M-row launch on B200, steps of 256 rows 27.5 us:
+// more, shorter dependent chains in flight per SM.)
 constexpr int kProbeWarps = kJoinBlock / 32;
-constexpr int kRowsPerLane = 16;
+constexpr int kRowsPerLane = 8;
 constexpr int kRowsPerWarpStep = 32 * kRowsPerLane;
-constexpr int kQueue = 32 * 8;
+constexpr int kQueue = 32 * kRowsPerLane;
 constexpr int kJoinResolveR = 2;  // candidates per lane per resolve round
 
 __global__ void __launch_bounds__(kJoinBlock, 2) join_probe_kernel(bo_join_probe_cols p,
@@ -258,14 +265,11 @@ __global__ void __launch_bounds__(kJoinBlock, 2) join_probe_kernel(bo_join_probe
     const int64_t base = st * kRowsPerWarpStep;
     const int64_t r0 = base + lane * kRowsPerLane;
     int32_t fk[kRowsPerLane];
-    uint32_t valid = 0xffffu;
+    uint32_t valid = 0xffu;
     if (r0 + kRowsPerLane <= n) {
-      const int8v f0 = ld_stream_v8(p.fk + r0), f1 = ld_stream_v8(p.fk + r0 + 8);
+      const int8v f0 = ld_stream_v8(p.fk + r0);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        fk[k] = f0.v[k];
-        fk[8 + k] = f1.v[k];
-      }
+      for (int k = 0; k < kRowsPerLane; ++k) fk[k] = f0.v[k];
     } else {
       valid = 0;
 #pragma unroll
@@ -282,23 +286,19 @@ __global__ void __launch_bounds__(kJoinBlock, 2) join_probe_kernel(bo_join_probe
 #pragma unroll
     for (int k = kRowsPerLane - 1; k >= 0; --k) hit = (hit << 1) | bloom_test(bl, wmask, (uint32_t)fk[k]);
     hit &= valid;
+    uint32_t total;
+    uint32_t pos = warp_exclusive_scan(__popc(hit), total);
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const uint32_t hm = (hit >> (8 * half)) & 0xffu;
-      uint32_t total;
-      uint32_t pos = warp_exclusive_scan(__popc(hm), total);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        if ((hm >> k) & 1u) {
-          qf[pos] = fk[8 * half + k];
-          qo[pos] = (uint16_t)(lane * kRowsPerLane + 8 * half + k);
-          ++pos;
-        }
+    for (int k = 0; k < kRowsPerLane; ++k) {
+      if ((hit >> k) & 1u) {
+        qf[pos] = fk[k];
+        qo[pos] = (uint16_t)(lane * kRowsPerLane + k);
+        ++pos;
       }
-      __syncwarp();
-      probe_resolve<kJoinResolveR, false>(qf, qo, total, base, slots, mask, probe_limit, p.price, p.discount, acc);
-      __syncwarp();
     }
+    __syncwarp();
+    probe_resolve<kJoinResolveR, false>(qf, qo, total, base, slots, mask, probe_limit, p.price, p.discount, acc);
+    __syncwarp();
   }
   if (!use_bloom) {
     // The bulk copy may still be in flight: wait for it (bounded) before exit.
@@ -407,7 +407,7 @@ int launch_probe(bo_ctx* ctx, const bo_join_probe_cols& p, const JoinWs& ws, bo_
     BO_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBloomBytes));
     ready = true;
   }
-  // Enough blocks to fill the GPU, but each thread should see a few 16-row
+  // Enough blocks to fill the GPU, but each thread should see a few 8-row
   // chunks so the per-block Bloom-filter copy is amortised.
   const int grid = grid_for(ctx, k, kJoinBlock, kBloomBytes, (p.n_rows + kRowsPerLane - 1) / kRowsPerLane);
   join_probe_kernel<<<grid, kJoinBlock, kBloomBytes, ctx->stream>>>(p, ws.slots, ws.bloom, ws.meta, out, mode,

@@ -34,7 +34,6 @@ struct bo_mlp {
   int partial_blocks = 0;
   float* loss = nullptr;     // device scalar
   int64_t step = 0;
-  mutable bool predict_ready = false;
 };
 
 namespace bo {
@@ -233,50 +232,77 @@ struct FeatureVec {
 // and combined with two shuffles.
 constexpr int kPredThreads = 256;
 
+// One feature vector through the MLP in one CTA.  Thread (j, part) owns hidden
+// unit j's partial dot products over inputs i = part (mod 4); every weight the
+// thread will use is loaded into registers up front (all loads independent,
+// one memory latency for the whole kernel), and only the 64-wide activations
+// move through shared memory between layers.
 __global__ void __launch_bounds__(kPredThreads) mlp_predict_counts(const float* __restrict__ params, FeatureVec xv,
                                                                    int F, int O, float* __restrict__ counts,
                                                                    float* __restrict__ y_log) {
-  extern __shared__ float W[];
   __shared__ float a[2][kH];
   const MlpLayout L = mlp_layout(F, O);
-  for (int i = threadIdx.x; i < L.P; i += kPredThreads) W[i] = params[i];
-  if (threadIdx.x < kMaxF) a[1][threadIdx.x] = threadIdx.x < F ? xv.f[threadIdx.x] : 0.0f;
-  __syncthreads();
   const int j = threadIdx.x >> 2, part = threadIdx.x & 3;
-  // layer 1: inputs a[1][0..F)
-  {
-    float z = 0.0f;
-    for (int i = part; i < F; i += 4) z = fmaf(a[1][i], W[L.w1 + i * kH + j], z);
-    z += __shfl_xor_sync(0xffffffffu, z, 1);
-    z += __shfl_xor_sync(0xffffffffu, z, 2);
-    z += W[L.b1 + j];
-    __syncthreads();
-    if (part == 0) a[0][j] = z > 0.0f ? z : 0.0f;
-    __syncthreads();
-  }
-  const int wofs[2] = {L.w2, L.w3}, bofs[2] = {L.b2, L.b3};
+  float w1[kMaxF / 4], w2[kH / 4], w3[kH / 4], w4[2 * kMaxO];
 #pragma unroll
-  for (int l = 0; l < 2; ++l) {
-    const float* in = a[l & 1 ? 1 : 0];
-    float z = 0.0f;
-#pragma unroll 4
-    for (int i = part; i < kH; i += 4) z = fmaf(in[i], W[wofs[l] + i * kH + j], z);
-    z += __shfl_xor_sync(0xffffffffu, z, 1);
-    z += __shfl_xor_sync(0xffffffffu, z, 2);
-    z += W[bofs[l] + j];
-    __syncthreads();
-    if (part == 0) a[l & 1 ? 0 : 1][j] = z > 0.0f ? z : 0.0f;
-    __syncthreads();
+  for (int k = 0; k < kMaxF / 4; ++k) {
+    const int i = part + 4 * k;
+    w1[k] = i < F ? __ldg(params + L.w1 + i * kH + j) : 0.0f;
   }
-  // after two hidden layers the third activation is in a[0]
-  if (threadIdx.x < 32) {
-    for (int o = 0; o < O; ++o) {
-      float y = fmaf(a[0][threadIdx.x], W[L.w4 + threadIdx.x * O + o], 0.0f);
-      y = fmaf(a[0][threadIdx.x + 32], W[L.w4 + (threadIdx.x + 32) * O + o], y);
+#pragma unroll
+  for (int k = 0; k < kH / 4; ++k) {
+    w2[k] = __ldg(params + L.w2 + (part + 4 * k) * kH + j);
+    w3[k] = __ldg(params + L.w3 + (part + 4 * k) * kH + j);
+  }
+  const float b1 = __ldg(params + L.b1 + j), b2 = __ldg(params + L.b2 + j), b3 = __ldg(params + L.b3 + j);
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int o = 0; o < kMaxO; ++o) {
+    w4[2 * o] = (t < 32 && o < O) ? __ldg(params + L.w4 + t * O + o) : 0.0f;
+    w4[2 * o + 1] = (t < 32 && o < O) ? __ldg(params + L.w4 + (t + 32) * O + o) : 0.0f;
+  }
+  const float b4 = t < O ? __ldg(params + L.b4 + t) : 0.0f;
+  if (t < kMaxF) a[1][t] = t < F ? xv.f[t] : 0.0f;
+  __syncthreads();
+  // layer 1: inputs a[1][0..F)
+  float z = 0.0f;
+#pragma unroll
+  for (int k = 0; k < kMaxF / 4; ++k) z = fmaf(a[1][part + 4 * k], w1[k], z);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  z += __shfl_xor_sync(0xffffffffu, z, 2);
+  z += b1;
+  __syncthreads();
+  if (part == 0) a[0][j] = z > 0.0f ? z : 0.0f;
+  __syncthreads();
+  // layer 2: a[0] -> a[1]
+  z = 0.0f;
+#pragma unroll
+  for (int k = 0; k < kH / 4; ++k) z = fmaf(a[0][part + 4 * k], w2[k], z);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  z += __shfl_xor_sync(0xffffffffu, z, 2);
+  z += b2;
+  if (part == 0) a[1][j] = z > 0.0f ? z : 0.0f;
+  __syncthreads();
+  // layer 3: a[1] -> a[0]
+  z = 0.0f;
+#pragma unroll
+  for (int k = 0; k < kH / 4; ++k) z = fmaf(a[1][part + 4 * k], w3[k], z);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  z += __shfl_xor_sync(0xffffffffu, z, 2);
+  z += b3;
+  if (part == 0) a[0][j] = z > 0.0f ? z : 0.0f;
+  __syncthreads();
+  if (t < 32) {
+#pragma unroll
+    for (int o = 0; o < kMaxO; ++o) {
+      if (o >= O) break;
+      float y = fmaf(a[0][t], w4[2 * o], 0.0f);
+      y = fmaf(a[0][t + 32], w4[2 * o + 1], y);
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) y += __shfl_xor_sync(0xffffffffu, y, off);
-      if (threadIdx.x == 0) {
-        y += W[L.b4 + o];
+      const float bo = __shfl_sync(0xffffffffu, b4, o);
+      if (t == 0) {
+        y += bo;
         if (y_log) y_log[o] = y;
         const float c = expm1f(y);
         counts[o] = c > 0.0f ? c : 0.0f;
@@ -476,13 +502,7 @@ int bo_mlp_predict_counts(bo_ctx* ctx, const bo_mlp* m, const float* features_ho
   if (!features_host || !counts_device) return set_error(ctx, BO_ERR_INVALID, "mlp_predict: bad argument");
   FeatureVec fv;
   for (int i = 0; i < kMaxF; ++i) fv.f[i] = i < m->F ? features_host[i] : 0.0f;
-  const size_t smem = sizeof(float) * (size_t)m->P;
-  if (!m->predict_ready) {
-    BO_CUDA(ctx, cudaFuncSetAttribute(reinterpret_cast<const void*>(&mlp_predict_counts),
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    m->predict_ready = true;
-  }
-  mlp_predict_counts<<<1, kPredThreads, smem, ctx->stream>>>(m->params, fv, m->F, m->O, counts_device, log_device);
+  mlp_predict_counts<<<1, kPredThreads, 0, ctx->stream>>>(m->params, fv, m->F, m->O, counts_device, log_device);
   return after_launch(ctx, "mlp_predict_counts");
 }
 
