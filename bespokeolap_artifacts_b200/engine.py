@@ -198,6 +198,30 @@ class Engine:
         self.ctx.call("bo_join_count_device", C.byref(b), C.byref(N.JoinParams(date_lt, seg_eq)),
                       C.c_void_p(N.ptr(count_dev)))
 
+    @staticmethod
+    def join_params(params) -> "C.Array":
+        """[(date_lt, seg_eq), ...] -> bo_join_params[]."""
+        arr = (N.JoinParams * len(params))()
+        for i, (d, s) in enumerate(params):
+            arr[i] = N.JoinParams(int(d), int(s))
+        return arr
+
+    def join_multi(self, build, probe, n_build: int, n_probe: int, params) -> list[dict]:
+        """Shared joins over device columns: one count / build / probe pass for
+        all (date_lt, seg_eq) pairs in `params`; exact solo reruns if the build
+        keys repeat.  Synchronises; one result per pair."""
+        b, p = self.join_cols(build, probe, n_build, n_probe)
+        prm = self.join_params(params)
+        out = (N.JoinResult * len(params))()
+        self.ctx.call("bo_join_multi_host", C.byref(b), C.byref(p), prm, len(params), out)
+        return [out[i].as_dict() for i in range(len(params))]
+
+    def join_multi_device(self, build, probe, n_build: int, n_probe: int, params, out_dev) -> None:
+        """Asynchronous shared joins; out_dev receives len(params) bo_join_result records."""
+        b, p = self.join_cols(build, probe, n_build, n_probe)
+        self.ctx.call("bo_join_multi_device", C.byref(b), C.byref(p), self.join_params(params), len(params),
+                      C.c_void_p(N.ptr(out_dev)))
+
     def join_host(self, j, mode: int = 0, predicted_rows: float = 0.0) -> dict:
         """Host arrays (a datagen.JoinInput) in; copies inside the call."""
         build = [np.ascontiguousarray(x) for x in (j.b_key, j.b_date, j.b_seg)]

@@ -111,6 +111,9 @@ class JoinParams(C.Structure):
     _fields_ = [("date_lt", C.c_int32), ("segment_eq", C.c_int32)]
 
 
+JOIN_MULTI_MAX = 32
+
+
 class JoinResult(C.Structure):
     _fields_ = [
         ("build_rows", C.c_int64), ("distinct_keys", C.c_int64), ("match_count", C.c_int64),
@@ -332,6 +335,10 @@ _SIGNATURES = {
                                       _P, C.POINTER(JoinResult)]),
     "bo_join_stream_host_async": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols),
                                             C.POINTER(JoinParams), _P, _P]),
+    "bo_join_multi_device": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
+                                       C.c_int32, _P]),
+    "bo_join_multi_host": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
+                                     C.c_int32, C.POINTER(JoinResult)]),
     "bo_join_host": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
                                C.c_int32, C.c_float, C.POINTER(JoinResult)]),
 }

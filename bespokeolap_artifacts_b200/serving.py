@@ -21,6 +21,7 @@ request's solo answer (tests/test_serving_gpu.py).
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 import time
 from collections import deque
@@ -163,26 +164,44 @@ def admit(pending: deque, footprints: dict, max_batch: int, pool_bytes: int, max
 class Slot:
     engine: object
     batch: B.Batch
+    stream: object = None               # torch stream the slot's engine runs on
+    join_out: object = None             # device records of the slot's shared joins
+    event: object = None                # recorded after the slot's last launch
     reqs: list = field(default_factory=list)
+    joins: list = field(default_factory=list)
+    others: list = field(default_factory=list)
     busy: bool = False
 
 
 class BatchedServer:
-    """Continuous batching over `n_slots` concurrently running batch slots."""
+    """Continuous batching over `n_slots` concurrently running batch slots.
+
+    The join requests a slot admits share one pass over the join tables
+    (bo_join_multi_device: one build and one probe pass whatever their number,
+    since they differ only in predicate constants); the scan-agg and group-by
+    requests run as instances of the slot's persistent batch kernel behind
+    them on the same stream.  With shared=False every request is a batch
+    instance."""
 
     def __init__(self, tables: ServingTables, n_slots: int = 2, max_batch: int = 16,
                  pool_bytes: int = 2 << 30, max_items: int = 65536, workers_per_sm: int = 1,
-                 join_sizer=None, gb_sizer=None, tile_table: B.TileTable | None = None):
+                 join_sizer=None, gb_sizer=None, tile_table: B.TileTable | None = None, shared: bool = True):
+        import torch
+
         from .engine import Engine
 
         self.tables = tables
         self.max_batch, self.pool_bytes, self.max_items = max_batch, pool_bytes, max_items
         self.join_sizer, self.gb_sizer = join_sizer, gb_sizer
         self.tile_table = tile_table
+        self.shared = shared
         self.slots = []
         for _ in range(n_slots):
             e = Engine(0)
-            self.slots.append(Slot(e, B.Batch.pool(e, max_batch, max_items, pool_bytes, workers_per_sm)))
+            st = torch.cuda.Stream()
+            e.set_stream(st.cuda_stream)
+            out = torch.zeros(N.JOIN_MULTI_MAX * C.sizeof(N.JoinResult), dtype=torch.uint8, device="cuda")
+            self.slots.append(Slot(e, B.Batch.pool(e, max_batch, max_items, pool_bytes, workers_per_sm), st, out))
         self.launches = 0
 
     def close(self):
@@ -191,7 +210,47 @@ class BatchedServer:
             s.engine.close()
 
     def _footprint(self, r: Request) -> tuple[int, int]:
+        if self.shared and r.kind == N.BATCH_JOIN:
+            return 0, 0  # shared joins use the slot's own table, not the batch pool
         return B.footprint(instance_of(self.tables, r, self.tile_table))
+
+    def _launch(self, s: Slot, reqs: list) -> None:
+        """Enqueues one slot's requests on its stream: the shared joins, then
+        the batch kernel over the rest; an event marks the end."""
+        import torch
+
+        s.joins = [r for r in reqs if self.shared and r.kind == N.BATCH_JOIN]
+        s.others = [r for r in reqs if not (self.shared and r.kind == N.BATCH_JOIN)]
+        if s.joins:
+            j = self.tables.join
+            s.engine.join_multi_device((j["b_key"], j["b_date"], j["b_seg"]), (j["p_fk"], j["p_price"], j["p_disc"]),
+                                       int(j["b_key"].numel()), int(j["p_fk"].numel()),
+                                       [(r.params["date_lt"], r.params["seg_eq"]) for r in s.joins], s.join_out)
+        if s.others:
+            insts = [instance_of(self.tables, r, self.tile_table) for r in s.others]
+            s.batch.update(insts)
+            s.batch.launch()
+        s.event = torch.cuda.Event()
+        s.event.record(s.stream)
+        s.reqs, s.busy = reqs, True
+        self.launches += 1
+
+    def _results(self, s: Slot) -> None:
+        """Fills the results of a finished slot's requests (an overflowed
+        instance or a shared join over repeated keys is rerun exactly)."""
+        if s.others:
+            for r, x in zip(s.others, s.batch.results()):
+                r.result = x
+        if s.joins:
+            s.engine.ctx.call("bo_check_errors")  # device errors of the shared joins (the batch's are read above)
+            host = s.join_out[: len(s.joins) * C.sizeof(N.JoinResult)].cpu().numpy().tobytes()
+            for i, r in enumerate(s.joins):
+                d = N.JoinResult.from_buffer_copy(host[i * C.sizeof(N.JoinResult):]).as_dict()
+                if d["overflowed"]:
+                    d = B.solo_result(s.engine, instance_of(self.tables, r))
+                    d["reruns"] = 1
+                d["kind"] = "join"
+                r.result = d
 
     def serve(self, requests: list[Request]) -> list[Request]:
         """Runs the arrival stream in real time; fills each request's result
@@ -212,25 +271,21 @@ class BatchedServer:
                     foot[r.rid] = self._footprint(r)
                     pending.append(r)
             for s in self.slots:
-                if s.busy and s.batch.done():
-                    res = s.batch.results()
+                if s.busy and s.event.query():
+                    self._results(s)
                     t_done = time.perf_counter() - t0
-                    for r, x in zip(s.reqs, res):
-                        r.result, r.done = x, t_done
+                    for r in s.reqs:
+                        r.done = t_done
                     finished += len(s.reqs)
                     s.reqs, s.busy = [], False
             for s in self.slots:
                 if not s.busy and pending:
                     reqs = admit(pending, foot, self.max_batch, self.pool_bytes, self.max_items)
-                    insts = [instance_of(self.tables, r, self.tile_table) for r in reqs]
                     tb = sum(foot[r.rid][0] for r in reqs)
                     if tb > self.pool_bytes:  # a single request above the pool: upper-bound tables do not fit
                         raise RuntimeError(f"request {reqs[0].rid} needs {tb} bytes of tables, slot holds "
                                            f"{self.pool_bytes}")
-                    s.batch.update(insts)
-                    s.batch.launch()
-                    s.reqs, s.busy = reqs, True
-                    self.launches += 1
+                    self._launch(s, reqs)
         return requests
 
 

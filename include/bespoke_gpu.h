@@ -260,6 +260,23 @@ int bo_join_probe_device(bo_ctx* ctx, const bo_join_probe_cols* probe, bo_join_r
 int bo_join_host(bo_ctx* ctx, const bo_join_build_cols* build_host, const bo_join_probe_cols* probe_host,
                  const bo_join_params* params, int32_t mode, float predicted_rows, bo_join_result* out_host);
 
+/* Shared joins: n_queries (1..BO_JOIN_MULTI_MAX) filtered joins of the same
+ * build and probe tables that differ only in their predicate constants, in
+ * one count, one build and one probe pass (the table maps a key to the mask
+ * of the queries it qualifies for).  out[i] is the result bo_join_plain
+ * returns for params[i] (capacity_log2 is the shared table's).  No reference
+ * counterpart: it serves concurrent requests (the reference runs one query
+ * per call, bespoke_tpch/query_impl.cpp:159-388).  A key that qualifies
+ * through two build rows cannot carry per-query multiplicities in the shared
+ * table: then every record has overflowed = 1 and the queries must run alone
+ * -- bo_join_multi_host does that itself (reruns = 1).  The _device form is
+ * asynchronous (out_device: n_queries records), the _host form synchronises. */
+#define BO_JOIN_MULTI_MAX 32
+int bo_join_multi_device(bo_ctx* ctx, const bo_join_build_cols* build, const bo_join_probe_cols* probe,
+                         const bo_join_params* params_host, int32_t n_queries, bo_join_result* out_device);
+int bo_join_multi_host(bo_ctx* ctx, const bo_join_build_cols* build, const bo_join_probe_cols* probe,
+                       const bo_join_params* params_host, int32_t n_queries, bo_join_result* out_host);
+
 /* Streamed form for inputs in pinned host memory (bo_host_alloc_pinned or
  * cudaHostRegister'd): only the columns every row needs cross PCIe as copies
  * (build date and segment, probe fk, the latter in 1M-row chunks overlapped

@@ -55,3 +55,21 @@ def test_one_per_launch_baseline(engine, tables):
     reqs = S.poisson_requests(5000.0, 12, seed=9)
     S.serve_one_per_launch(engine, tables, reqs)
     check(engine, tables, reqs)
+
+
+def test_served_joins_share_one_pass(engine, tables):
+    reqs = S.poisson_requests(50000.0, 40, seed=10, mix=(0, 1, 0))
+    srv = S.BatchedServer(tables, n_slots=2, max_batch=16, pool_bytes=512 << 20, max_items=32768)
+    srv.serve(reqs)
+    assert srv.launches < len(reqs)
+    assert all(r.result.get("reruns", 0) == 0 for r in reqs)
+    check(engine, tables, reqs)
+    srv.close()
+
+
+def test_served_without_sharing(engine, tables):
+    reqs = S.poisson_requests(20000.0, 24, seed=11)
+    srv = S.BatchedServer(tables, n_slots=2, max_batch=8, pool_bytes=512 << 20, max_items=32768, shared=False)
+    srv.serve(reqs)
+    check(engine, tables, reqs)
+    srv.close()
