@@ -78,6 +78,14 @@ def _rows(dev: dict, name: str) -> int:
     return int(dev[name].numel())
 
 
+def _a_id_max(dev: dict, g) -> int:
+    """Largest A id: from the device table set when it records it, else from
+    the host arrays of ``g``."""
+    if "a_id_max" in dev:
+        return int(dev["a_id_max"])
+    return int(g.a_ids.max()) if len(g.a_ids) else 0
+
+
 class Engine:
     """One engine context (device, stream, scratch) with the pipeline entry points."""
 
@@ -247,7 +255,7 @@ class Engine:
         ``dev`` holds device columns a_ids, b_a, b_c, c_cat, c_year."""
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
                                           _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,
-                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
+                                          g.k, _a_id_max(dev, g),
                                           dev.get("a_mask"))
         out = N.GbResult()
         self.ctx.call("bo_groupby_topk_plain", C.byref(a), C.byref(b), C.byref(c), C.byref(prm), C.byref(out))
@@ -256,7 +264,7 @@ class Engine:
     def groupby_presized(self, dev: dict, g, pred_dev) -> dict:
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
                                           _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,
-                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
+                                          g.k, _a_id_max(dev, g),
                                           dev.get("a_mask"))
         out = N.GbResult()
         self.ctx.call("bo_groupby_topk_presized", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
@@ -266,7 +274,7 @@ class Engine:
     def groupby_presized_device(self, dev: dict, g, pred_dev, out_dev) -> None:
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
                                           _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,
-                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
+                                          g.k, _a_id_max(dev, g),
                                           dev.get("a_mask"))
         self.ctx.call("bo_groupby_topk_presized_device", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
                       C.c_void_p(N.ptr(pred_dev)), C.c_void_p(N.ptr(out_dev)))
@@ -274,7 +282,7 @@ class Engine:
     def groupby_distinct_device(self, dev: dict, g, out_dev) -> None:
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
                                           _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,
-                                          g.k, int(dev.get("a_id_max", g.a_ids.max() if len(g.a_ids) else 0)),
+                                          g.k, _a_id_max(dev, g),
                                           dev.get("a_mask"))
         self.ctx.call("bo_groupby_distinct_device", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
                       C.c_void_p(N.ptr(out_dev)))

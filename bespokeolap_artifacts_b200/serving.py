@@ -26,6 +26,7 @@ import math
 import time
 from collections import deque
 from dataclasses import dataclass, field
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -54,6 +55,8 @@ class ServingTables:
         workload at 60M) and a probe side of fact_rows rows; a group-by with B
         = fact_rows rows and A, C ten times the 2.5M / 4M of the group-by
         workload at 60M (scaled down proportionally for smaller fact_rows)."""
+        import torch
+
         from . import learned as L
 
         f = B.fact_instance(fact_rows, seed + 1).cols
@@ -61,6 +64,11 @@ class ServingTables:
         scale = fact_rows / 60_000_000
         n_a, n_c = max(16, int(25_000_000 * scale)), max(16, int(40_000_000 * scale))
         g = B.groupby_tables_device(n_a, fact_rows, n_c, seed + 3)
+        # A's id mask depends on table A alone: built once at load (an index,
+        # like the sketches) for the slots' group-by pipelines.
+        g["a_mask"] = torch.zeros((int(g["a_id_max"]) + 32) // 32, dtype=torch.int32, device="cuda")
+        engine.ctx.call("bo_groupby_a_mask_device", C.byref(N.GbACols(N.ptr(g["a_ids"]), int(g["a_ids"].numel()))),
+                        int(g["a_id_max"]), C.c_void_p(g["a_mask"].data_ptr()))
         t = cls(f, j, g)
         t.join_stats = L.join_table_stats(engine.ctx, j["b_key"], j["b_date"], j["b_seg"], int(j["b_key"].numel()))
         t.gb_stats = L.groupby_table_stats(engine.ctx, g, n_a, fact_rows, n_c)
@@ -115,7 +123,7 @@ def instance_of(tables: ServingTables, r: Request, tile_table: B.TileTable | Non
         cols, rows = tables.join, int(tables.join["p_fk"].numel())
         params = dict(r.params)
     else:
-        cols = {k: v for k, v in tables.gb.items() if k != "a_id_max"}
+        cols = {k: v for k, v in tables.gb.items() if k not in ("a_id_max", "a_mask")}
         rows = int(cols["b_a"].numel())
         params = dict(r.params, a_id_max=int(tables.gb["a_id_max"]))
     inst = B.Instance(r.kind, rows, cols, params, predicted=r.predicted)
@@ -166,9 +174,13 @@ class Slot:
     batch: B.Batch
     stream: object = None               # torch stream the slot's engine runs on
     join_out: object = None             # device records of the slot's shared joins
+    gb_out: object = None               # device records of the slot's group-by pipelines
+    gb_pred_h: object = None            # their predicted group counts (pinned host, device)
+    gb_pred_d: object = None
     event: object = None                # recorded after the slot's last launch
     reqs: list = field(default_factory=list)
     joins: list = field(default_factory=list)
+    gbs: list = field(default_factory=list)
     others: list = field(default_factory=list)
     busy: bool = False
 
@@ -178,10 +190,12 @@ class BatchedServer:
 
     The join requests a slot admits share one pass over the join tables
     (bo_join_multi_device: one build and one probe pass whatever their number,
-    since they differ only in predicate constants); the scan-agg and group-by
-    requests run as instances of the slot's persistent batch kernel behind
-    them on the same stream.  With shared=False every request is a batch
-    instance."""
+    since they differ only in predicate constants); each group-by request runs
+    the presized multi-kernel pipeline (table sized on the device from its MLP
+    prediction, A's id mask built once at load; an overflowed table is rerun
+    exactly), and the scan-agg requests run as instances of the slot's
+    persistent batch kernel -- all on the slot's stream, one event at the
+    end.  With shared=False every request is a batch instance."""
 
     def __init__(self, tables: ServingTables, n_slots: int = 2, max_batch: int = 16,
                  pool_bytes: int = 2 << 30, max_items: int = 65536, workers_per_sm: int = 1,
@@ -201,7 +215,11 @@ class BatchedServer:
             st = torch.cuda.Stream()
             e.set_stream(st.cuda_stream)
             out = torch.zeros(N.JOIN_MULTI_MAX * C.sizeof(N.JoinResult), dtype=torch.uint8, device="cuda")
-            self.slots.append(Slot(e, B.Batch.pool(e, max_batch, max_items, pool_bytes, workers_per_sm), st, out))
+            slot = Slot(e, B.Batch.pool(e, max_batch, max_items, pool_bytes, workers_per_sm), st, out)
+            slot.gb_out = torch.zeros(max_batch * C.sizeof(N.GbResult), dtype=torch.uint8, device="cuda")
+            slot.gb_pred_h = torch.zeros(max_batch, dtype=torch.float32).pin_memory()
+            slot.gb_pred_d = torch.zeros(max_batch, dtype=torch.float32, device="cuda")
+            self.slots.append(slot)
         self.launches = 0
 
     def close(self):
@@ -212,7 +230,10 @@ class BatchedServer:
     def _footprint(self, r: Request) -> tuple[int, int]:
         if self.shared and r.kind == N.BATCH_JOIN:
             return 0, 0  # shared joins use the slot's own table, not the batch pool
-        return B.footprint(instance_of(self.tables, r, self.tile_table))
+        tb, items = B.footprint(instance_of(self.tables, r, self.tile_table))
+        if self.shared and r.kind == N.BATCH_GROUPBY:
+            return tb, 0  # its own pipeline: HBM footprint from the prediction, no batch work items
+        return tb, items
 
     def _launch(self, s: Slot, reqs: list) -> None:
         """Enqueues one slot's requests on its stream: the shared joins, then
@@ -220,7 +241,19 @@ class BatchedServer:
         import torch
 
         s.joins = [r for r in reqs if self.shared and r.kind == N.BATCH_JOIN]
-        s.others = [r for r in reqs if not (self.shared and r.kind == N.BATCH_JOIN)]
+        s.gbs = [r for r in reqs if self.shared and r.kind == N.BATCH_GROUPBY]
+        s.others = [r for r in reqs if not (self.shared and r.kind in (N.BATCH_JOIN, N.BATCH_GROUPBY))]
+        if s.gbs:
+            for i, r in enumerate(s.gbs):
+                s.gb_pred_h[i] = float(r.predicted)
+            with torch.cuda.stream(s.stream):
+                s.gb_pred_d[: len(s.gbs)].copy_(s.gb_pred_h[: len(s.gbs)], non_blocking=True)
+            g = self.tables.gb
+            for i, r in enumerate(s.gbs):
+                prm = SimpleNamespace(cat_set=r.params["cat_set"], year_lo=r.params["year_lo"],
+                                      year_hi=r.params["year_hi"], k=r.params["k"])
+                s.engine.groupby_presized_device(g, prm, s.gb_pred_d[i:i + 1],
+                                                 s.gb_out[i * C.sizeof(N.GbResult):(i + 1) * C.sizeof(N.GbResult)])
         if s.joins:
             j = self.tables.join
             s.engine.join_multi_device((j["b_key"], j["b_date"], j["b_seg"]), (j["p_fk"], j["p_price"], j["p_disc"]),
@@ -241,6 +274,16 @@ class BatchedServer:
         if s.others:
             for r, x in zip(s.others, s.batch.results()):
                 r.result = x
+        if s.gbs:
+            s.engine.ctx.call("bo_check_errors")  # device errors of the slot's pipelines (the batch's are read above)
+            host = s.gb_out[: len(s.gbs) * C.sizeof(N.GbResult)].cpu().numpy().tobytes()
+            for i, r in enumerate(s.gbs):
+                d = N.GbResult.from_buffer_copy(host[i * C.sizeof(N.GbResult):]).as_dict()
+                if d["overflowed"]:  # predicted too few groups: the exact form
+                    d = B.solo_result(s.engine, instance_of(self.tables, r))
+                    d["reruns"] = 1
+                d["kind"] = "groupby"
+                r.result = d
         if s.joins:
             s.engine.ctx.call("bo_check_errors")  # device errors of the shared joins (the batch's are read above)
             host = s.join_out[: len(s.joins) * C.sizeof(N.JoinResult)].cpu().numpy().tobytes()
