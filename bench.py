@@ -27,6 +27,7 @@ import subprocess
 import sys
 import threading
 import time
+import types
 from pathlib import Path
 
 import numpy as np
@@ -651,6 +652,55 @@ def groupby_section(eng, stream, n_queries: int = 10, keep: dict | None = None) 
     batch.close()
     if keep is not None:
         keep["gb_sizer"] = sizer
+
+    # ---- radix-partitioned form: the MLP's predicted group count picks the
+    # fan-out (single pass while the table stays in L2); here and on a
+    # high-cardinality case (flat keys, broad filter) where it partitions.
+    dev2 = {"a_ids": c["a_ids"], "b_a": c["b_a"], "b_c": c["b_c"], "c_cat": c["c_cat"], "c_year": c["c_year"],
+            "a_id_max": insts[0].params["a_id_max"]}
+    pj = [float(sizer.predict_host(f[None, :])[0, 1]) for f in feats]
+
+    def qobj(cats, lo, hi):
+        return types.SimpleNamespace(cat_set=cats, year_lo=lo, year_hi=hi, k=10)
+
+    def partitioned(i, log2p):
+        return eng.groupby_partitioned(dev2, qobj(queries[i % 3], 1990, 2010), log2p, pj[i % 3])
+
+    fan2 = [L.GroupBySizer.fanout(p) for p in pg]
+    same_p = all(all(partitioned(i, 6)[f] == exact[i][f] for f in B.ANSWER_FIELDS["groupby"]) for i in range(3))
+    ms_part6 = _median_wall_ms(lambda i: partitioned(i, 6), n)
+    hc = B.groupby_tables_device(25_000_000, 60_000_000, 4_000_000, seed=21, s_a=0.3, s_c=0.3)
+    hc_cats = list(range(0, 113, 2))[:64]
+    hq = qobj(hc_cats, 1900, 2020)
+    st_hc = L.groupby_table_stats(eng.ctx, hc, 25_000_000, 60_000_000, 4_000_000)
+    f_hc = L.groupby_features(st_hc, hc_cats, 1900, 2020)
+    p_hc = sizer.predict_host(f_hc[None, :])[0]
+    fan_hc = L.GroupBySizer.fanout(float(p_hc[0]))
+    hc_plain = eng.groupby_plain(hc, hq)
+    pred_hc = torch.tensor([float(p_hc[0])], dtype=torch.float32, device="cuda")
+    hc_single = eng.groupby_presized(hc, hq, pred_hc)
+    hc_part = eng.groupby_partitioned(hc, hq, fan_hc, float(p_hc[1]))
+    same_hc = all(hc_single[f] == hc_plain[f] and hc_part[f] == hc_plain[f] for f in B.ANSWER_FIELDS["groupby"])
+    ms_hc_plain = _median_wall_ms(lambda i: eng.groupby_plain(hc, hq), 5)
+    ms_hc_single = _median_wall_ms(lambda i: eng.groupby_presized(hc, hq, pred_hc), 5)
+    ms_hc_part = _median_wall_ms(lambda i: eng.groupby_partitioned(hc, hq, fan_hc, float(p_hc[1])), 5)
+    partition_out = {
+        "fanout_log2_chosen": fan2, "partitioned_log2_6_ms_per_query": ms_part6,
+        "answers_identical_partitioned": bool(same_p),
+        "high_cardinality": {
+            "workload": "A 25,000,000 ids; B 60,000,000 (a_id Zipf 0.3, c_id Zipf 0.3); C 4,000,000; 64 "
+                        "categories, years 1900..2020; group by a_id, count + min(year), top 10",
+            "groups": hc_plain["n_groups"], "joined_rows": hc_plain["joined_rows"],
+            "predicted_groups": float(p_hc[0]), "predicted_joined_rows": float(p_hc[1]),
+            "fanout_log2_chosen": fan_hc,
+            "plain_ms_per_query": ms_hc_plain, "learned_single_pass_ms_per_query": ms_hc_single,
+            "learned_partitioned_ms_per_query": ms_hc_part,
+            "speedup_partitioned_vs_single_pass": ms_hc_single / ms_hc_part,
+            "speedup_partitioned_vs_plain": ms_hc_plain / ms_hc_part,
+            "reruns": [hc_single["reruns"], hc_part["reruns"]],
+            "answers_identical": bool(same_hc)},
+    }
+    del hc
     return {
         "workload": "A 2,500,000 ids; B 36,000,000 (a_id Zipf 1.1, c_id Zipf 0.9); C 4,000,000 (category 0..112, "
                     "year 1900..2020); category in a seeded 8-value set, year in [1990, 2010]; group by a_id, "
@@ -666,6 +716,7 @@ def groupby_section(eng, stream, n_queries: int = 10, keep: dict | None = None) 
         "answers_identical": bool(same),
         "note": "host-visible latency per query; same 3 queries rotated; setup (data, sketches, MLP training) "
                 f"{setup_s:.1f} s outside the timing",
+        "partitioned": partition_out,
     }
 
 

@@ -208,6 +208,24 @@ __global__ void gb_amask_kernel(bo_gb_a_cols a, int32_t a_id_max, uint32_t* __re
 // ------------------------------------------------------------------ scan --
 
 // kMode 0: exact distinct pre-pass (bits of a distinct bitmap); 1: aggregate.
+// Records of the radix-partitioned form: the scan appends (key, count, min
+// year, partition) records to one array through a warp-aggregated cursor (so
+// skewed keys cannot overflow a partition's share), and a counting scatter
+// then groups them by partition; the partition of a key is the top bits of
+// hash32(key) (shift = 32 - log2 partitions; 32 for one partition).
+struct GbParts {
+  uint4* records = nullptr;
+  uint32_t* cursor = nullptr;
+  uint32_t cap = 0;
+  uint32_t shift = 32;
+  __device__ __forceinline__ uint32_t of(uint32_t key) const { return shift >= 32 ? 0u : hash32(key) >> shift; }
+  __device__ __forceinline__ bool put(uint32_t pos, uint32_t key, uint32_t cnt, int32_t mn) const {
+    if (pos >= cap) return false;  // more records than the prediction allowed for: the call reruns exactly
+    records[pos] = make_uint4(key, cnt, (uint32_t)mn, of(key));
+    return true;
+  }
+};
+
 template <int kMode>
 __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64_t n_c, int32_t a_id_max,
                                                            const uint32_t* __restrict__ bloom_g,
@@ -215,7 +233,8 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
                                                            const int32_t* __restrict__ c_year,
                                                            const uint32_t* __restrict__ amask,
                                                            unsigned long long* slots, int32_t* mins, uint32_t* dbits,
-                                                           GbMeta* meta, uint64_t probe_limit, uint32_t* err) {
+                                                           GbMeta* meta, uint64_t probe_limit, GbParts parts,
+                                                           uint32_t* err) {
   extern __shared__ __align__(128) uint32_t bloom_s[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int32_t q_c[kGbWarps][kGbQueue];
@@ -301,7 +320,7 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
       for (int r = 0; r < kGbResolveR; ++r) {
         const bool pass = (w[r] >> (c[r] & 31)) & 1u;
         a[r] = pass ? __ldg(b.a_id + row[r]) : -1;
-        y[r] = (pass && kMode == 1) ? __ldg(c_year + c[r]) : 0;
+        y[r] = (pass && kMode >= 1) ? __ldg(c_year + c[r]) : 0;
       }
       // Survivors: A-mask test, then the heavy-hitter table in shared memory;
       // the rest try their first global slot with one CAS each, all issued
@@ -331,6 +350,21 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
           }
         }
         pend[r] = !done;
+      }
+      if (kMode == 2) {
+        // Partitioned form: each survivor appends a (key, 1, year) record;
+        // the warp reserves its records with one atomic per round.
+#pragma unroll
+        for (int r = 0; r < kGbResolveR; ++r) {
+          const uint32_t pm = __ballot_sync(0xffffffffu, pend[r]);
+          if (!pm) continue;  // warp-uniform
+          const int leader = __ffs(pm) - 1;
+          uint32_t first_pos = 0;
+          if (lane == leader) first_pos = atomicAdd(parts.cursor, (uint32_t)__popc(pm));
+          first_pos = __shfl_sync(0xffffffffu, first_pos, leader);
+          if (pend[r] && !parts.put(first_pos + __popc(pm & ((1u << lane) - 1u)), (uint32_t)a[r], 1u, y[r]))
+            full = 1;
+        }
       }
       if (kMode == 1) {
         unsigned long long got[kGbResolveR];
@@ -414,6 +448,12 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
       if (l_key[i] != 0xffffffffu)
         if (!gb_global_insert(slots, mins, mask, l_key[i], l_cnt[i], l_min[i], newkeys, ~0ull, probe_limit))
           full = 1;
+    }
+  } else if (kMode == 2) {
+    // ... or as records, one per pre-aggregated group.
+    for (int i = threadIdx.x; i < kGbLocalSlots; i += blockDim.x) {
+      if (l_key[i] != 0xffffffffu)
+        if (!parts.put(atomicAdd(parts.cursor, 1u), l_key[i], l_cnt[i], l_min[i])) full = 1;
     }
   }
   if (!use_bloom) mbar_wait_bounded(&bar, 0, kWaitLimitNs);
@@ -513,6 +553,168 @@ __global__ void __launch_bounds__(kCompactBlock) gb_compact_kernel(const unsigne
     if (lane == 0 && cmaxc) atomicMax(&meta->inv_max, cmaxc);
     __syncthreads();
   }
+}
+
+// ------------------------------------------------- partitioned aggregate --
+// Counting scatter of the records by partition (histogram, exclusive scan,
+// scatter), then one block per partition (grid-stride over partitions): the
+// partition's records aggregate in a shared-memory table (key, count, min
+// year) and its groups are written as packed sort keys like
+// gb_compact_kernel's.  A partition with more groups than the table holds
+// sets the overflow flag (the caller reruns exactly).
+constexpr int kPartBlock = 512;
+constexpr int kPartSlots = 8192;  // slots of a partition's shared table
+constexpr uint32_t kPartMaxGroups = kPartSlots / 8 * 7;  // fuller counts as overflow
+constexpr int kPartProbes = 256;  // probe-chain bound: a longer chain counts as overflow
+constexpr size_t kPartSmem = (size_t)kPartSlots * 12;
+constexpr int kPartScanBlock = 1024;
+
+__global__ void __launch_bounds__(kPartBlock) gb_part_hist_kernel(GbParts parts, uint32_t n_parts,
+                                                                  uint32_t* __restrict__ counts) {
+  extern __shared__ uint32_t hist[];
+  for (uint32_t i = threadIdx.x; i < n_parts; i += kPartBlock) hist[i] = 0;
+  __syncthreads();
+  const uint32_t n = min(__ldcg(parts.cursor), parts.cap);
+  for (uint32_t i = blockIdx.x * kPartBlock + threadIdx.x; i < n; i += gridDim.x * kPartBlock)
+    atomicAdd(hist + parts.records[i].w, 1u);
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n_parts; i += kPartBlock)
+    if (hist[i]) atomicAdd(counts + i, hist[i]);
+}
+
+// offsets[p] = records before partition p (offsets[n_parts] = all); fill = offsets.
+__global__ void __launch_bounds__(kPartScanBlock) gb_part_scan_kernel(const uint32_t* __restrict__ counts,
+                                                                      uint32_t n_parts, uint32_t* __restrict__ offsets,
+                                                                      uint32_t* __restrict__ fill) {
+  __shared__ uint32_t warp_tot[kPartScanBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t per = (n_parts + kPartScanBlock - 1) / kPartScanBlock;
+  const uint32_t lo = threadIdx.x * per, hi = min(lo + per, n_parts);
+  uint32_t local = 0;
+  for (uint32_t i = lo; i < hi; ++i) local += counts[i];
+  uint32_t wt;
+  const uint32_t wex = warp_exclusive_scan(local, wt);
+  if (lane == 0) warp_tot[warp] = wt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kPartScanBlock / 32; ++w) {
+      const uint32_t x = warp_tot[w];
+      warp_tot[w] = t;
+      t += x;
+    }
+    offsets[n_parts] = t;
+  }
+  __syncthreads();
+  uint32_t run = warp_tot[warp] + wex;
+  for (uint32_t i = lo; i < hi; ++i) {
+    offsets[i] = run;
+    fill[i] = run;
+    run += counts[i];
+  }
+}
+
+// Records -> their partition's range; the lanes of one partition reserve
+// their slots with one atomic (match_any groups them).
+__global__ void __launch_bounds__(kPartBlock) gb_part_scatter_kernel(GbParts parts, uint32_t* __restrict__ fill,
+                                                                     uint4* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t n = min(__ldcg(parts.cursor), parts.cap);
+  const uint32_t warps = gridDim.x * (kPartBlock / 32);
+  for (uint32_t i0 = (blockIdx.x * kPartBlock + threadIdx.x) & ~31u; i0 < n; i0 += warps * 32) {
+    const uint32_t i = i0 + lane;
+    const bool valid = i < n;
+    const uint4 r = valid ? parts.records[i] : make_uint4(0, 0, 0, 0xffffffffu);
+    const uint32_t peers = __match_any_sync(0xffffffffu, r.w);
+    const int leader = __ffs(peers) - 1;
+    uint32_t first_pos = 0;
+    if (valid && lane == leader) first_pos = atomicAdd(fill + r.w, (uint32_t)__popc(peers));
+    first_pos = __shfl_sync(0xffffffffu, first_pos, leader);
+    if (valid) out[first_pos + __popc(peers & ((1u << lane) - 1u))] = r;
+  }
+}
+
+__global__ void __launch_bounds__(kPartBlock) gb_part_agg_kernel(const uint4* __restrict__ recs,
+                                                                 const uint32_t* __restrict__ offsets, int n_parts,
+                                                                 GbMeta* meta, int wa, unsigned long long cmax,
+                                                                 unsigned long long* __restrict__ keys,
+                                                                 uint32_t* __restrict__ vals) {
+  extern __shared__ __align__(16) uint32_t part_smem[];
+  uint32_t* t_key = part_smem;
+  uint32_t* t_cnt = part_smem + kPartSlots;
+  int32_t* t_min = reinterpret_cast<int32_t*>(part_smem + 2 * kPartSlots);
+  __shared__ uint32_t warp_off[kPartBlock / 32];
+  __shared__ unsigned long long base;
+  __shared__ uint32_t full_s, used_s;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kPer = kPartSlots / kPartBlock;
+  unsigned long long cmaxc = 0;
+  for (int p = blockIdx.x; p < n_parts; p += gridDim.x) {
+    for (int i = threadIdx.x; i < kPartSlots; i += kPartBlock) {
+      t_key[i] = 0xffffffffu;
+      t_cnt[i] = 0;
+      t_min[i] = 0x7fffffff;
+    }
+    if (threadIdx.x == 0) full_s = used_s = 0;
+    __syncthreads();
+    const uint32_t b0 = offsets[p], b1 = offsets[p + 1];
+    for (uint32_t i = b0 + threadIdx.x; i < b1; i += kPartBlock) {
+      if (*reinterpret_cast<volatile uint32_t*>(&full_s)) break;  // the call reruns: stop early
+      const uint4 r = recs[i];
+      uint32_t sl = hash32(r.x) & (kPartSlots - 1);
+      bool done = false;
+      for (int step = 0; step < kPartProbes && !done; ++step) {
+        const uint32_t old = atomicCAS(t_key + sl, 0xffffffffu, r.x);
+        if (old == 0xffffffffu || old == r.x) {
+          if (old == 0xffffffffu && atomicAdd(&used_s, 1u) + 1u > kPartMaxGroups) full_s = 1;
+          atomicAdd(t_cnt + sl, r.y);
+          atomicMin(t_min + sl, (int32_t)r.z);
+          done = true;
+        }
+        sl = (sl + 1) & (kPartSlots - 1);
+      }
+      if (!done) full_s = 1;
+    }
+    __syncthreads();
+    // Emit the partition's groups: one reservation per block.
+    uint32_t occ = 0;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) occ += t_key[j * kPartBlock + threadIdx.x] != 0xffffffffu;
+    uint32_t wtot;
+    const uint32_t mine = warp_exclusive_scan(occ, wtot);
+    if (lane == 0) warp_off[warp] = wtot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < kPartBlock / 32; ++w) {
+        const uint32_t x = warp_off[w];
+        warp_off[w] = t;
+        t += x;
+      }
+      base = t ? atomicAdd(&meta->n_out, (unsigned long long)t) : 0ull;
+      if (t) atomicAdd(&meta->distinct, (unsigned long long)t);
+      if (full_s) atomicOr(&meta->overflow, 1u);
+    }
+    __syncthreads();
+    unsigned long long pos = base + warp_off[warp] + mine;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int i = j * kPartBlock + threadIdx.x;
+      if (t_key[i] != 0xffffffffu) {
+        const unsigned long long cnt = t_cnt[i];
+        cmaxc = cnt > cmaxc ? cnt : cmaxc;
+        keys[pos] = ((cmax - cnt) << wa) | t_key[i];
+        vals[pos] = (uint32_t)t_min[i];
+        ++pos;
+      }
+    }
+    __syncthreads();
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, cmaxc, o);
+    cmaxc = other > cmaxc ? other : cmaxc;
+  }
+  if (lane == 0 && cmaxc) atomicMax(&meta->inv_max, cmaxc);
 }
 
 // ------------------------------------------------------------------ topk --
@@ -667,7 +869,7 @@ int gb_prepare(bo_ctx* ctx, const bo_gb_a_cols& a, const bo_gb_c_cols& c, const 
 
 template <int kMode>
 int gb_launch_scan(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, const bo_gb_params& prm,
-                   const GbWs& ws, uint64_t probe_limit = ~0ull) {
+                   const GbWs& ws, uint64_t probe_limit = ~0ull, GbParts parts = GbParts{}) {
   const void* k = reinterpret_cast<const void*>(&gb_scan_kernel<kMode>);
   static bool ready = false;
   if (!ready) {
@@ -677,7 +879,7 @@ int gb_launch_scan(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, co
   const int grid = grid_res(ctx, k, kGbBlock, kGbBloomBytes, (b.n_rows + kGbRowsPerLane - 1) / kGbRowsPerLane);
   gb_scan_kernel<kMode><<<grid, kGbBlock, kGbBloomBytes, ctx->stream>>>(
       b, c.n_rows, prm.a_id_max, ws.bloom, ws.cbits, c.year, prm.a_mask ? prm.a_mask : ws.amask, ws.slots, ws.mins,
-      ws.dbits, ws.meta, probe_limit, ctx->d_err);
+      ws.dbits, ws.meta, probe_limit, parts, ctx->d_err);
   return after_launch(ctx, "gb_scan_kernel");
 }
 
@@ -793,6 +995,93 @@ int bo_groupby_topk_presized(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_c
   if (out_host->overflowed) {
     if ((rc = gb_plain_impl(ctx, *a, *b, *c, *prm, out_host, 1))) return rc;
     out_host->mode = 1;
+  }
+  return BO_OK;
+}
+
+int bo_groupby_topk_partitioned_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b,
+                                       const bo_gb_c_cols* c, const bo_gb_params* prm, int32_t log2_partitions,
+                                       float predicted_joined_rows, bo_gb_result* out_device) {
+  BO_CHECK_CTX(ctx);
+  int rc = check_gb(ctx, a, b, c, prm);
+  if (rc) return rc;
+  if (!out_device) return set_error(ctx, BO_ERR_INVALID, "groupby: null output");
+  if (log2_partitions < 0 || log2_partitions > BO_GB_MAX_LOG2_PARTITIONS)
+    return set_error(ctx, BO_ERR_INVALID, "groupby: log2_partitions %d outside [0, %d]", log2_partitions,
+                     BO_GB_MAX_LOG2_PARTITIONS);
+  GbWs ws;
+  if ((rc = gb_workspace(ctx, *b, *c, prm->a_id_max, &ws))) return rc;
+  // The global group table is not used: initialise the smallest one.
+  if ((rc = gb_prepare(ctx, *a, *c, *prm, ws, nullptr, kGbMinCapLog2))) return rc;
+  const uint32_t n_parts = 1u << log2_partitions;
+  // Records: at most one per joined row (fewer after the per-block
+  // pre-aggregation); sized from the prediction with a margin and slack.
+  const double want = std::max(0.0, (double)predicted_joined_rows) * 1.25 + 65536.0;
+  if (want * 2 * sizeof(uint4) > (double)(64ull << 30))
+    return set_error(ctx, BO_ERR_INVALID, "groupby: predicted partition records above 64 GiB");
+  GbParts parts;
+  parts.cap = (uint32_t)std::min(want, (double)0xfffffff0u);
+  parts.shift = log2_partitions == 0 ? 32u : (uint32_t)(32 - log2_partitions);
+  const size_t rec_bytes = ((size_t)parts.cap * sizeof(uint4) + 255) & ~size_t(255);
+  const size_t ctr_bytes = 4 * (3 * (size_t)n_parts + 2) + 256;
+  void* pbase = nullptr;
+  if ((rc = region(ctx, "gb_parts", 2 * rec_bytes + ctr_bytes, &pbase))) return rc;
+  char* pp = static_cast<char*>(pbase);
+  parts.records = reinterpret_cast<uint4*>(pp);
+  uint4* scattered = reinterpret_cast<uint4*>(pp + rec_bytes);
+  uint32_t* ctr = reinterpret_cast<uint32_t*>(pp + 2 * rec_bytes);
+  parts.cursor = ctr;                   // [0]
+  uint32_t* counts = ctr + 1;           // [1, 1 + n_parts)
+  uint32_t* offsets = counts + n_parts; // n_parts + 1
+  uint32_t* fill = offsets + n_parts + 1;
+  BO_CUDA(ctx, cudaMemsetAsync(ctr, 0, 4 * (1 + (size_t)n_parts), ctx->stream));
+  if ((rc = gb_launch_scan<2>(ctx, *b, *c, *prm, ws, ~0ull, parts))) return rc;
+  const int wa = std::max(1, bit_length((uint64_t)prm->a_id_max));
+  const int wc = std::max(1, bit_length((uint64_t)b->n_rows));
+  const unsigned long long cmax = (wc >= 64) ? ~0ull : ((1ull << wc) - 1ull);
+  static bool ready = false;
+  const void* kh = reinterpret_cast<const void*>(&gb_part_hist_kernel);
+  const void* kp = reinterpret_cast<const void*>(&gb_part_agg_kernel);
+  if (!ready) {
+    BO_CUDA(ctx, cudaFuncSetAttribute(kh, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(4u << BO_GB_MAX_LOG2_PARTITIONS)));
+    BO_CUDA(ctx, cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPartSmem));
+    ready = true;
+  }
+  const size_t hsmem = 4 * (size_t)n_parts;
+  gb_part_hist_kernel<<<ctx->num_sms * 2, kPartBlock, hsmem, ctx->stream>>>(parts, n_parts, counts);
+  if ((rc = after_launch(ctx, "gb_part_hist_kernel"))) return rc;
+  gb_part_scan_kernel<<<1, kPartScanBlock, 0, ctx->stream>>>(counts, n_parts, offsets, fill);
+  if ((rc = after_launch(ctx, "gb_part_scan_kernel"))) return rc;
+  gb_part_scatter_kernel<<<ctx->num_sms * 4, kPartBlock, 0, ctx->stream>>>(parts, fill, scattered);
+  if ((rc = after_launch(ctx, "gb_part_scatter_kernel"))) return rc;
+  const int gp = (int)std::min<int64_t>(n_parts, (int64_t)ctx->num_sms * occupancy_blocks(kp, kPartBlock, kPartSmem));
+  gb_part_agg_kernel<<<std::max(gp, 1), kPartBlock, kPartSmem, ctx->stream>>>(scattered, offsets, (int)n_parts,
+                                                                              ws.meta, wa, cmax, ws.keys, ws.vals);
+  if ((rc = after_launch(ctx, "gb_part_agg_kernel"))) return rc;
+  const uint64_t cap_max = 1ull << ws.max_log2;
+  if ((rc = radix_topk_pairs(ctx, ws.keys, ws.vals, (int64_t)cap_max, &ws.meta->n_out, wa + wc, prm->k, ws.tkeys,
+                             ws.tvals, ws.keys, ws.vals, wa, &ws.meta->inv_max)))
+    return rc;
+  gb_topk_kernel<<<1, BO_GB_MAX_K, 0, ctx->stream>>>(ws.tkeys, ws.tvals, ws.meta, prm->k, wa, cmax, 2, out_device);
+  return after_launch(ctx, "gb_topk_kernel");
+}
+
+int bo_groupby_topk_partitioned(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
+                                const bo_gb_params* prm, int32_t log2_partitions, float predicted_joined_rows,
+                                bo_gb_result* out_host) {
+  BO_CHECK_CTX(ctx);
+  if (!out_host) return set_error(ctx, BO_ERR_INVALID, "groupby: null output");
+  void* dout = nullptr;
+  int rc = region(ctx, "gb_out", sizeof(bo_gb_result), &dout);
+  if (rc) return rc;
+  bo_gb_result* d = static_cast<bo_gb_result*>(dout);
+  if ((rc = bo_groupby_topk_partitioned_device(ctx, a, b, c, prm, log2_partitions, predicted_joined_rows, d)))
+    return rc;
+  if ((rc = gb_finish(ctx, out_host, d))) return rc;
+  if (out_host->overflowed) {
+    if ((rc = gb_plain_impl(ctx, *a, *b, *c, *prm, out_host, 1))) return rc;
+    out_host->mode = 2;
   }
   return BO_OK;
 }

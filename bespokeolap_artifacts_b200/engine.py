@@ -279,6 +279,25 @@ class Engine:
         self.ctx.call("bo_groupby_topk_presized_device", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
                       C.c_void_p(N.ptr(pred_dev)), C.c_void_p(N.ptr(out_dev)))
 
+    def groupby_partitioned(self, dev: dict, g, log2_partitions: int, predicted_joined_rows: float) -> dict:
+        """Radix-partitioned form: 2^log2_partitions partitions sized from the
+        predicted joined rows; plain rerun if a partition was too small."""
+        a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
+                                          _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,
+                                          g.k, _a_id_max(dev, g), dev.get("a_mask"))
+        out = N.GbResult()
+        self.ctx.call("bo_groupby_topk_partitioned", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
+                      int(log2_partitions), float(predicted_joined_rows), C.byref(out))
+        return out.as_dict()
+
+    def groupby_partitioned_device(self, dev: dict, g, log2_partitions: int, predicted_joined_rows: float,
+                                   out_dev) -> None:
+        a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
+                                          _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,
+                                          g.k, _a_id_max(dev, g), dev.get("a_mask"))
+        self.ctx.call("bo_groupby_topk_partitioned_device", C.byref(a), C.byref(b), C.byref(c), C.byref(prm),
+                      int(log2_partitions), float(predicted_joined_rows), C.c_void_p(N.ptr(out_dev)))
+
     def groupby_distinct_device(self, dev: dict, g, out_dev) -> None:
         a, b, c, prm, keep = self.gb_args(dev["a_ids"], dev["b_a"], dev["b_c"], dev["c_cat"], dev["c_year"],
                                           _rows(dev, "a_ids"), _rows(dev, "b_a"), _rows(dev, "c_cat"), g.cat_set, g.year_lo, g.year_hi,

@@ -443,3 +443,17 @@ class GroupBySizer:
     def predict_device(self, features: np.ndarray, counts_dev) -> None:
         """counts_dev[0] = predicted groups, counts_dev[1] = predicted joined rows."""
         self.mlp.predict_counts_device(features, counts_dev)
+
+    # Fan-out of the radix-partitioned group-by from the predicted group count:
+    # one pass while the single-pass table (2.5 slots of 12 bytes per group)
+    # fits in half the L2, else partitions of about 4096 groups (half of a
+    # partition's 8192-slot shared-memory table).
+    PART_GROUPS = 4096
+
+    @classmethod
+    def fanout(cls, predicted_groups: float, l2_bytes: int = 126 << 20) -> int:
+        """log2 of the partition count for a predicted group count (0 = single pass)."""
+        g = max(0.0, float(predicted_groups))
+        if g * 2.5 * 12 <= l2_bytes / 2:
+            return 0
+        return int(min(N.GB_MAX_LOG2_PARTITIONS, max(1, math.ceil(math.log2(g / cls.PART_GROUPS)))))

@@ -112,6 +112,7 @@ class JoinParams(C.Structure):
 
 
 JOIN_MULTI_MAX = 32
+GB_MAX_LOG2_PARTITIONS = 14
 
 
 class JoinResult(C.Structure):
@@ -335,6 +336,10 @@ _SIGNATURES = {
                                       _P, C.POINTER(JoinResult)]),
     "bo_join_stream_host_async": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols),
                                             C.POINTER(JoinParams), _P, _P]),
+    "bo_groupby_topk_partitioned_device": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),
+                                                     C.POINTER(GbParams), C.c_int32, C.c_float, _P]),
+    "bo_groupby_topk_partitioned": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),
+                                              C.POINTER(GbParams), C.c_int32, C.c_float, C.POINTER(GbResult)]),
     "bo_join_multi_device": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
                                        C.c_int32, _P]),
     "bo_join_multi_host": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),

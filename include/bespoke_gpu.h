@@ -341,7 +341,7 @@ typedef struct bo_gb_result {
   int32_t capacity_log2;
   int32_t overflowed;      /* presized table too small (result invalid, rerun) */
   int32_t reruns;
-  int32_t mode;            /* 0 plain exact-count, 1 presized */
+  int32_t mode;            /* 0 plain exact-count, 1 presized, 2 radix-partitioned */
   int32_t n_rows_out;      /* min(k, n_groups) */
   int32_t pad;
   bo_gb_row rows[BO_GB_MAX_K];
@@ -361,6 +361,24 @@ int bo_groupby_topk_presized_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo
 int bo_groupby_topk_presized(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
                              const bo_gb_params* params, const float* predicted_groups_device,
                              bo_gb_result* out_host);
+/* Radix-partitioned form (2^log2_partitions partitions, 0..BO_GB_MAX_LOG2_PARTITIONS):
+ * the scan of B writes each surviving row -- or, for keys the block
+ * pre-aggregated in shared memory, one (key, count, min year) record per
+ * block -- into the partition of the top bits of its key's hash; one block
+ * per partition then aggregates the partition in a shared-memory table, so
+ * the group table never leaves the SM however many groups there are.  The
+ * caller picks the fan-out (the MLP's predicted group count: one partition
+ * while the single-pass table stays in L2, else enough partitions for a few
+ * thousand groups each) and sizes the partition buffers from the predicted
+ * joined rows.  A partition buffer or table that turns out too small sets
+ * overflowed; bo_groupby_topk_partitioned then reruns the plain form. */
+#define BO_GB_MAX_LOG2_PARTITIONS 14
+int bo_groupby_topk_partitioned_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b,
+                                       const bo_gb_c_cols* c, const bo_gb_params* params, int32_t log2_partitions,
+                                       float predicted_joined_rows, bo_gb_result* out_device);
+int bo_groupby_topk_partitioned(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b, const bo_gb_c_cols* c,
+                                const bo_gb_params* params, int32_t log2_partitions, float predicted_joined_rows,
+                                bo_gb_result* out_host);
 /* Bitmap of A's ids over [0, a_id_max] ((a_id_max + 32) / 32 words, device),
  * the semi-join mask of the group-by (the reference rebuilds such masks per
  * query, e.g. build_id_mask in bespoke_ceb/query_q1a.cpp); it depends only on
