@@ -1014,9 +1014,15 @@ int bo_groupby_topk_partitioned_device(bo_ctx* ctx, const bo_gb_a_cols* a, const
   // The global group table is not used: initialise the smallest one.
   if ((rc = gb_prepare(ctx, *a, *c, *prm, ws, nullptr, kGbMinCapLog2))) return rc;
   const uint32_t n_parts = 1u << log2_partitions;
-  // Records: at most one per joined row (fewer after the per-block
-  // pre-aggregation); sized from the prediction with a margin and slack.
-  const double want = std::max(0.0, (double)predicted_joined_rows) * 1.25 + 65536.0;
+  // Records: at most one per joined row, so at most one per B row.  The
+  // buffers take that bound while it stays within kRecordBoundBytes (HBM is
+  // plentiful: 60M B rows need 1.9 GB for the two record arrays); beyond it
+  // they are sized from the predicted joined rows with a margin and slack.
+  constexpr double kRecordBoundBytes = 16.0 * (1ull << 30);
+  const double bound = (double)b->n_rows + 65536.0;
+  double want = bound;
+  if (bound * 2 * sizeof(uint4) > kRecordBoundBytes)
+    want = std::min(bound, std::max(0.0, (double)predicted_joined_rows) * 1.25 + 65536.0);
   if (want * 2 * sizeof(uint4) > (double)(64ull << 30))
     return set_error(ctx, BO_ERR_INVALID, "groupby: predicted partition records above 64 GiB");
   GbParts parts;

@@ -369,9 +369,11 @@ int bo_groupby_topk_presized(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_c
  * the group table never leaves the SM however many groups there are.  The
  * caller picks the fan-out (the MLP's predicted group count: one partition
  * while the single-pass table stays in L2, else enough partitions for a few
- * thousand groups each) and sizes the partition buffers from the predicted
- * joined rows.  A partition buffer or table that turns out too small sets
- * overflowed; bo_groupby_topk_partitioned then reruns the plain form. */
+ * thousand groups each).  The record buffers hold one record per B row (a
+ * survivor makes at most one) while that stays within 16 GiB, else they are
+ * sized from predicted_joined_rows.  A record buffer or partition table that
+ * turns out too small sets overflowed; bo_groupby_topk_partitioned then
+ * reruns the plain form. */
 #define BO_GB_MAX_LOG2_PARTITIONS 14
 int bo_groupby_topk_partitioned_device(bo_ctx* ctx, const bo_gb_a_cols* a, const bo_gb_b_cols* b,
                                        const bo_gb_c_cols* c, const bo_gb_params* params, int32_t log2_partitions,
