@@ -452,7 +452,7 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     # ---- the other configurations (rank 0; extra keys of the same line)
     extra = {}
     if rank == 0 and args.sections != "none":
-        wanted = (["scan_agg", "groupby", "batch", "serving"] if args.sections == "all"
+        wanted = (["scan_agg", "groupby", "join_large", "batch", "serving"] if args.sections == "all"
                   else args.sections.split(","))
         peak_gbs, _ = peaks()
         keep = {}
@@ -463,6 +463,8 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
                     extra[name] = scan_agg_section(eng, stream, peak_gbs)
                 elif name == "groupby":
                     extra[name] = groupby_section(eng, stream, keep=keep)
+                elif name == "join_large":
+                    extra[name] = join_large_section(eng, sizer, feats)
                 elif name == "batch":
                     extra[name] = batch_section(eng, stream, K, sizer, keep.get("gb_sizer"))
                 elif name == "serving":
@@ -718,6 +720,54 @@ def groupby_section(eng, stream, n_queries: int = 10, keep: dict | None = None) 
                 f"{setup_s:.1f} s outside the timing",
         "partitioned": partition_out,
     }
+
+
+def join_large_section(eng, sizer, headline_feats) -> dict:
+    """Single pass vs radix-partitioned join where the qualifying build keys
+    make a table far beyond L2 (build 150M rows, 30M qualifying; probe 150M
+    rows), with the fan-out picked from the MLP's predicted qualifying rows;
+    and the fan-out the same rule picks for the headline workload."""
+    import torch
+
+    from bespokeolap_artifacts_b200 import learned as L
+    from bespokeolap_artifacts_b200.datagen import DATE_HI, DATE_LO
+
+    nb = npr = 150_000_000
+    g = torch.Generator(device="cuda")
+    g.manual_seed(31)
+    key = (torch.randperm(nb, generator=g, device="cuda") + 1).to(torch.int32)
+    date = torch.randint(DATE_LO, DATE_HI + 1, (nb,), generator=g, device="cuda", dtype=torch.int32)
+    seg = torch.randint(0, 5, (nb,), generator=g, device="cuda", dtype=torch.uint8)
+    fk = torch.randint(1, nb + 1, (npr,), generator=g, device="cuda", dtype=torch.int32)
+    price = torch.randint(90_000, 10_500_001, (npr,), generator=g, device="cuda", dtype=torch.int64)
+    disc = torch.randint(0, 11, (npr,), generator=g, device="cuda", dtype=torch.int64)
+    date_lt, seg_eq = DATE_HI + 1, 2
+    build, probe = (key, date, seg), (fk, price, disc)
+    st = L.join_table_stats(eng.ctx, key, date, seg, nb)
+    pred = float(sizer.predict_host(L.join_features(st, date_lt, seg_eq)[None, :])[0])
+    fan = L.JoinSizer.fanout(pred)
+    plain = eng.join_plain(build, probe, nb, npr, date_lt, seg_eq)
+    part = eng.join_partitioned(build, probe, nb, npr, date_lt, seg_eq, fan)
+    fields = ("build_rows", "distinct_keys", "match_count", "sum_exact", "sum_trunc")
+    same = all(plain[f] == part[f] for f in fields)
+    ms_plain = _median_wall_ms(lambda i: eng.join_plain(build, probe, nb, npr, date_lt, seg_eq), 5)
+    ms_part = _median_wall_ms(lambda i: eng.join_partitioned(build, probe, nb, npr, date_lt, seg_eq, fan), 5)
+    head = [L.JoinSizer.fanout(float(sizer.predict_host(f[None, :])[0])) for f in headline_feats]
+    out = {
+        "workload": "build 150,000,000 rows (unique int32 keys, all dates, segment == 2: ~20% qualify), probe "
+                    "150,000,000 rows (fk uniform over the keys), sum price*(100-discount)",
+        "qualifying_build_rows": plain["build_rows"], "predicted_qualifying_rows": pred,
+        "fanout_log2_chosen": fan,
+        "single_pass_ms_per_query": ms_plain, "partitioned_ms_per_query": ms_part,
+        "speedup_partitioned_vs_single_pass": ms_plain / ms_part,
+        "rows_per_s_partitioned": (nb + npr) / (ms_part * 1e-3),
+        "reruns": part["reruns"], "answers_identical": bool(same),
+        "headline_fanout_log2_chosen": head,
+        "note": "single pass = the plain form (exact count, table sized 2 slots per key); host-visible latency",
+    }
+    del key, date, seg, fk, price, disc
+    torch.cuda.empty_cache()
+    return out
 
 
 def batch_section(eng, stream, K: int, join_sizer=None, gb_sizer=None) -> dict:

@@ -206,6 +206,16 @@ class Engine:
         self.ctx.call("bo_join_count_device", C.byref(b), C.byref(N.JoinParams(date_lt, seg_eq)),
                       C.c_void_p(N.ptr(count_dev)))
 
+    def join_partitioned(self, build, probe, n_build: int, n_probe: int, date_lt: int, seg_eq: int,
+                         log2_partitions: int) -> dict:
+        """Radix-partitioned filtered join (2^log2_partitions partitions); the
+        plain single pass reruns it if a partition's table was too small."""
+        b, p = self.join_cols(build, probe, n_build, n_probe)
+        out = N.JoinResult()
+        self.ctx.call("bo_join_partitioned", C.byref(b), C.byref(p), C.byref(N.JoinParams(date_lt, seg_eq)),
+                      int(log2_partitions), C.byref(out))
+        return out.as_dict()
+
     @staticmethod
     def join_params(params) -> "C.Array":
         """[(date_lt, seg_eq), ...] -> bo_join_params[]."""

@@ -113,6 +113,7 @@ class JoinParams(C.Structure):
 
 JOIN_MULTI_MAX = 32
 GB_MAX_LOG2_PARTITIONS = 14
+JOIN_MAX_LOG2_PARTITIONS = 14
 
 
 class JoinResult(C.Structure):
@@ -340,6 +341,10 @@ _SIGNATURES = {
                                                      C.POINTER(GbParams), C.c_int32, C.c_float, _P]),
     "bo_groupby_topk_partitioned": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),
                                               C.POINTER(GbParams), C.c_int32, C.c_float, C.POINTER(GbResult)]),
+    "bo_join_partitioned_device": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols),
+                                             C.POINTER(JoinParams), C.c_int32, _P]),
+    "bo_join_partitioned": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
+                                      C.c_int32, C.POINTER(JoinResult)]),
     "bo_join_multi_device": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),
                                        C.c_int32, _P]),
     "bo_join_multi_host": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),

@@ -226,7 +226,7 @@ typedef struct bo_join_result {
   int32_t capacity_log2;   /* table capacity used */
   int32_t overflowed;      /* presized table was too small (result invalid, rerun) */
   int32_t reruns;          /* exact-count reruns performed by the call */
-  int32_t mode;            /* 0 plain exact-count, 1 presized from a prediction */
+  int32_t mode;            /* 0 plain exact-count, 1 presized from a prediction, 2 radix-partitioned */
 } bo_join_result;
 
 /* K7, exact-count pre-pass: number of qualifying build rows (device int64). */
@@ -259,6 +259,22 @@ int bo_join_probe_device(bo_ctx* ctx, const bo_join_probe_cols* probe, bo_join_r
  * a host float) form. */
 int bo_join_host(bo_ctx* ctx, const bo_join_build_cols* build_host, const bo_join_probe_cols* probe_host,
                  const bo_join_params* params, int32_t mode, float predicted_rows, bo_join_result* out_host);
+
+/* Radix-partitioned form (2^log2_partitions partitions, 0..BO_JOIN_MAX_LOG2_PARTITIONS)
+ * for qualifying build keys far beyond L2: qualifying build keys and the probe
+ * rows that pass a global Bloom filter of them are split by the top bits of
+ * their key's hash (record arrays sized by the row counts, counting scatter),
+ * then one block per partition joins the partition in a shared-memory table
+ * (8192 slots), so no lookup leaves the SM.  The caller picks the fan-out
+ * (learned.JoinSizer.fanout on the predicted qualifying rows: a single pass
+ * while its table stays in L2, else partitions of about 4096 keys).  A
+ * partition with more distinct keys than its table holds sets overflowed;
+ * bo_join_partitioned then reruns the plain single pass (reruns = 1). */
+#define BO_JOIN_MAX_LOG2_PARTITIONS 14
+int bo_join_partitioned_device(bo_ctx* ctx, const bo_join_build_cols* build, const bo_join_probe_cols* probe,
+                               const bo_join_params* params, int32_t log2_partitions, bo_join_result* out_device);
+int bo_join_partitioned(bo_ctx* ctx, const bo_join_build_cols* build, const bo_join_probe_cols* probe,
+                        const bo_join_params* params, int32_t log2_partitions, bo_join_result* out_host);
 
 /* Shared joins: n_queries (1..BO_JOIN_MULTI_MAX) filtered joins of the same
  * build and probe tables that differ only in their predicate constants, in
