@@ -182,11 +182,11 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     preds = torch.zeros(K + W, dtype=torch.float32, device="cuda")
 
     def learned_step(i, slot):
+        # MLP prediction folded into the table's init kernel (bo_join_learned_device)
         c = copies[i % 3]
         j = c["j"]
-        sizer.predict_device(feats[i % 3], preds[slot:slot + 1])
-        eng.join_presized_device(c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq, preds[slot:slot + 1],
-                                 results[slot * res_sz:(slot + 1) * res_sz])
+        sizer.join_device(feats[i % 3], c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq,
+                          results[slot * res_sz:(slot + 1) * res_sz], preds[slot:slot + 1])
 
     def check(slots):
         host = results.cpu().numpy().tobytes()
@@ -281,8 +281,7 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     def learned_query(i):
         c = copies[i % 3]
         j = c["j"]
-        sizer.predict_device(feats[i % 3], preds[0:1])
-        return eng.join_presized(c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq, preds[0:1])
+        return sizer.join(feats[i % 3], c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq)
 
     def plain_query(i):
         c = copies[i % 3]
@@ -310,8 +309,7 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
         ob = torch.zeros(res_sz, dtype=torch.uint8, device="cuda")
 
         def lseq(c=c, j=j, pl=pl, ob=ob, i=i):
-            sizer.predict_device(feats[i], pl[0:1])
-            eng.join_presized_device(c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq, pl[0:1], ob)
+            sizer.join_device(feats[i], c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq, ob, pl[0:1])
 
         def sseq(c=c, j=j, pl=pl, ob=ob):
             eng.join_presized_device(c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq, pl[1:2], ob)
@@ -512,9 +510,10 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
                          "algorithmic_bytes_per_launch": PROBE_BYTES, "avg_launch_us": probe_ms * 1e3},
             "learned_vs_plain": {"learned_ms_per_query": lat_learned_graph, "plain_ms_per_query": lat_plain_graph,
                                  "speedup": lat_plain_graph / lat_learned_graph,
-                                 "form": "CUDA graphs: learned = one graph (MLP prediction + presized init/build/"
-                                         "probe); plain = count kernel + host round trip + the same presized "
-                                         "pipeline graph sized from the exact count",
+                                 "form": "CUDA graphs: learned = one graph of bo_join_learned_device (MLP "
+                                         "prediction fused into the table init, build, probe); plain = count "
+                                         "kernel + host round trip + the presized pipeline graph sized from the "
+                                         "exact count",
                                  "eager_learned_ms_per_query": lat_learned, "eager_plain_ms_per_query": lat_plain,
                                  "eager_speedup": lat_plain / lat_learned, "answers_identical": bool(same_graph),
                                  "q_error": q_err, "sizing_margin": sizer.margin, "reruns": reruns,

@@ -26,6 +26,7 @@
 #include "common.cuh"
 #include "rows.cuh"
 #include "context.cuh"
+#include "mlp.cuh"
 
 namespace bo {
 
@@ -79,14 +80,17 @@ __global__ void __launch_bounds__(kBuildBlock) join_count_kernel(bo_join_build_c
 // device from the predicted qualifying-row count: the smallest power of two
 // >= kPresizeFactor * pred, clamped to [2^kMinCapLog2, 2^max_log2].  Every block
 // computes the same value, so no cross-block handshake is needed.
-__device__ __forceinline__ int32_t presize_log2(const float* pred, int32_t host_log2, int32_t max_log2) {
-  if (!pred) return host_log2;
-  float p = *pred;
+__device__ __forceinline__ int32_t presize_log2_of(float p, int32_t max_log2) {
   if (!(p >= 0.0f)) p = 0.0f;  // NaN / negative predictions size for the minimum
   const double want = (double)p * kPresizeFactor;
   int32_t cl = kMinCapLog2;
   while (cl < max_log2 && (double)(1ull << cl) < want) ++cl;
   return cl;
+}
+
+__device__ __forceinline__ int32_t presize_log2(const float* pred, int32_t host_log2, int32_t max_log2) {
+  if (!pred) return host_log2;
+  return presize_log2_of(*pred, max_log2);
 }
 
 __global__ void join_init_kernel(unsigned long long* slots, uint32_t* bloom, JoinMeta* meta, const float* pred,
@@ -107,6 +111,41 @@ __global__ void join_init_kernel(unsigned long long* slots, uint32_t* bloom, Joi
     meta->distinct = 0;
 #pragma unroll
     for (int i = 0; i < 6; ++i) meta->acc[i] = 0;
+  }
+}
+
+// The learned form's first kernel: every block evaluates the sizing MLP for
+// the query's feature vector (the same instructions on the same inputs, so
+// every block derives the same capacity as mlp_predict_counts followed by
+// join_init_kernel would), then clears its share of the table and the Bloom
+// filter; block 0 resets the join state and records the prediction.  One
+// launch instead of two on the query's critical path.
+__global__ void __launch_bounds__(kPredThreads) join_learned_init_kernel(const float* __restrict__ params,
+                                                                         FeatureVec xv, int F, int O,
+                                                                         unsigned long long* slots, uint32_t* bloom,
+                                                                         JoinMeta* meta, int32_t max_log2,
+                                                                         float* pred_out) {
+  __shared__ float y[kMaxO];
+  mlp_predict_block(params, xv, F, O, y);
+  const float c = expm1f(y[0]);
+  const float pred = c > 0.0f ? c : 0.0f;
+  const int32_t cl = presize_log2_of(pred, max_log2);
+  const uint64_t cap = 1ull << cl;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  ulonglong2* s2 = reinterpret_cast<ulonglong2*>(slots);
+  for (uint64_t i = tid; i < cap / 2; i += stride) s2[i] = make_ulonglong2(kEmptySlot, kEmptySlot);
+  uint4* b4 = reinterpret_cast<uint4*>(bloom);
+  for (uint64_t i = tid; i < kBloomWords / 4; i += stride) b4[i] = make_uint4(0, 0, 0, 0);
+  if (tid == 0) {
+    meta->cap_log2 = cl;
+    meta->done = 0;
+    meta->overflow = 0;
+    meta->build_rows = 0;
+    meta->distinct = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) meta->acc[i] = 0;
+    if (pred_out) *pred_out = pred;
   }
 }
 
@@ -665,6 +704,49 @@ int bo_join_presized_device(bo_ctx* ctx, const bo_join_build_cols* b, const bo_j
   JoinWs ws;
   if ((rc = join_workspace(ctx, b->n_rows, &ws))) return rc;
   return join_run(ctx, *b, *p, *prm, ws, pred_device, 0, out_device, 1);
+}
+
+int bo_join_learned_device(bo_ctx* ctx, const bo_mlp* m, const float* features_host, const bo_join_build_cols* b,
+                           const bo_join_probe_cols* p, const bo_join_params* prm, bo_join_result* out_device,
+                           float* pred_device) {
+  BO_CHECK_CTX(ctx);
+  int rc = check_join(ctx, b, p, prm);
+  if (rc) return rc;
+  const float* params = nullptr;
+  int F = 0, O = 0;
+  if (!features_host || !out_device || mlp_view(m, &params, &F, &O) != BO_OK || F < 1 || F > kMaxF || O < 1 ||
+      O > kMaxO)
+    return set_error(ctx, BO_ERR_INVALID, "join_learned: null argument or bad model");
+  FeatureVec fv;
+  for (int i = 0; i < kMaxF; ++i) fv.f[i] = i < F ? features_host[i] : 0.0f;
+  JoinWs ws;
+  if ((rc = join_workspace(ctx, b->n_rows, &ws))) return rc;
+  join_learned_init_kernel<<<ctx->num_sms * 2, kPredThreads, 0, ctx->stream>>>(params, fv, F, O, ws.slots, ws.bloom,
+                                                                             ws.meta, ws.max_log2, pred_device);
+  if ((rc = after_launch(ctx, "join_learned_init_kernel"))) return rc;
+  const void* kb = reinterpret_cast<const void*>(&join_build_kernel);
+  const int gb = grid_for(ctx, kb, kBuildBlock, 0, (b->n_rows + kBuildRowsPerThread - 1) / kBuildRowsPerThread);
+  join_build_kernel<<<gb, kBuildBlock, 0, ctx->stream>>>(*b, prm->date_lt, (uint32_t)prm->segment_eq, ws.slots,
+                                                          ws.bloom, ws.meta, kPresizedProbeLimit);
+  if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
+  return launch_probe(ctx, *p, ws, out_device, 1, kPresizedProbeLimit);
+}
+
+int bo_join_learned(bo_ctx* ctx, const bo_mlp* m, const float* features_host, const bo_join_build_cols* b,
+                    const bo_join_probe_cols* p, const bo_join_params* prm, bo_join_result* out_host) {
+  BO_CHECK_CTX(ctx);
+  if (!out_host) return set_error(ctx, BO_ERR_INVALID, "join: null output");
+  void* dout = nullptr;
+  int rc = region(ctx, "join_out", sizeof(bo_join_result), &dout);
+  if (rc) return rc;
+  bo_join_result* d = static_cast<bo_join_result*>(dout);
+  if ((rc = bo_join_learned_device(ctx, m, features_host, b, p, prm, d, nullptr))) return rc;
+  if ((rc = finish_join(ctx, out_host, d))) return rc;
+  if (out_host->overflowed) {  // the prediction was too low: the exact form
+    if ((rc = join_plain_impl(ctx, *b, *p, *prm, out_host, 1))) return rc;
+    out_host->mode = 1;
+  }
+  return BO_OK;
 }
 
 int bo_join_presized(bo_ctx* ctx, const bo_join_build_cols* b, const bo_join_probe_cols* p, const bo_join_params* prm,

@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "context.cuh"
+#include "mlp.cuh"
 
 struct bo_mlp {
   int F = 0, O = 0, P = 0;
@@ -38,32 +39,8 @@ struct bo_mlp {
 
 namespace bo {
 
-constexpr int kH = 64;
 constexpr int kTB = 64;            // samples per CTA
 constexpr int kPad = kTB + 1;      // column stride of per-sample tables in shared memory
-constexpr int kMaxF = 32;
-constexpr int kMaxO = 4;
-
-struct MlpLayout {
-  int F, O;
-  int w1, b1, w2, b2, w3, b3, w4, b4, P;
-};
-
-__host__ __device__ inline MlpLayout mlp_layout(int F, int O) {
-  MlpLayout L;
-  L.F = F;
-  L.O = O;
-  L.w1 = 0;
-  L.b1 = L.w1 + F * kH;
-  L.w2 = L.b1 + kH;
-  L.b2 = L.w2 + kH * kH;
-  L.w3 = L.b2 + kH;
-  L.b3 = L.w3 + kH * kH;
-  L.w4 = L.b3 + kH;
-  L.b4 = L.w4 + kH * O;
-  L.P = L.b4 + O;
-  return L;
-}
 
 __host__ __device__ inline size_t mlp_smem_floats(int F, int O) {
   const MlpLayout L = mlp_layout(F, O);
@@ -221,94 +198,28 @@ __global__ void mlp_reduce_adam(float* __restrict__ params, float* __restrict__ 
   params[p] -= lr * (mm / bc1) / (sqrtf(vv / bc2) + eps);
 }
 
-struct FeatureVec {
-  float f[kMaxF];
-};
-
 // One feature vector passed by value (no host-to-device copy): predicted
-// counts = max(expm1(y), 0), written to counts[0..O).  256 threads: the
-// parameters are staged into shared memory with coalesced loads, each of the
-// 64 units of a layer is computed by 4 threads over a quarter of its inputs
-// and combined with two shuffles.
-constexpr int kPredThreads = 256;
-
-// One feature vector through the MLP in one CTA.  Thread (j, part) owns hidden
-// unit j's partial dot products over inputs i = part (mod 4); every weight the
-// thread will use is loaded into registers up front (all loads independent,
-// one memory latency for the whole kernel), and only the 64-wide activations
-// move through shared memory between layers.
+// counts = max(expm1(y), 0), written to counts[0..O) (mlp_predict_block in
+// mlp.cuh does the forward pass).
 __global__ void __launch_bounds__(kPredThreads) mlp_predict_counts(const float* __restrict__ params, FeatureVec xv,
                                                                    int F, int O, float* __restrict__ counts,
                                                                    float* __restrict__ y_log) {
-  __shared__ float a[2][kH];
-  const MlpLayout L = mlp_layout(F, O);
-  const int j = threadIdx.x >> 2, part = threadIdx.x & 3;
-  float w1[kMaxF / 4], w2[kH / 4], w3[kH / 4], w4[2 * kMaxO];
-#pragma unroll
-  for (int k = 0; k < kMaxF / 4; ++k) {
-    const int i = part + 4 * k;
-    w1[k] = i < F ? __ldg(params + L.w1 + i * kH + j) : 0.0f;
-  }
-#pragma unroll
-  for (int k = 0; k < kH / 4; ++k) {
-    w2[k] = __ldg(params + L.w2 + (part + 4 * k) * kH + j);
-    w3[k] = __ldg(params + L.w3 + (part + 4 * k) * kH + j);
-  }
-  const float b1 = __ldg(params + L.b1 + j), b2 = __ldg(params + L.b2 + j), b3 = __ldg(params + L.b3 + j);
+  __shared__ float y[kMaxO];
+  mlp_predict_block(params, xv, F, O, y);
   const int t = threadIdx.x;
-#pragma unroll
-  for (int o = 0; o < kMaxO; ++o) {
-    w4[2 * o] = (t < 32 && o < O) ? __ldg(params + L.w4 + t * O + o) : 0.0f;
-    w4[2 * o + 1] = (t < 32 && o < O) ? __ldg(params + L.w4 + (t + 32) * O + o) : 0.0f;
+  if (t < O) {
+    if (y_log) y_log[t] = y[t];
+    const float c = expm1f(y[t]);
+    counts[t] = c > 0.0f ? c : 0.0f;
   }
-  const float b4 = t < O ? __ldg(params + L.b4 + t) : 0.0f;
-  if (t < kMaxF) a[1][t] = t < F ? xv.f[t] : 0.0f;
-  __syncthreads();
-  // layer 1: inputs a[1][0..F)
-  float z = 0.0f;
-#pragma unroll
-  for (int k = 0; k < kMaxF / 4; ++k) z = fmaf(a[1][part + 4 * k], w1[k], z);
-  z += __shfl_xor_sync(0xffffffffu, z, 1);
-  z += __shfl_xor_sync(0xffffffffu, z, 2);
-  z += b1;
-  __syncthreads();
-  if (part == 0) a[0][j] = z > 0.0f ? z : 0.0f;
-  __syncthreads();
-  // layer 2: a[0] -> a[1]
-  z = 0.0f;
-#pragma unroll
-  for (int k = 0; k < kH / 4; ++k) z = fmaf(a[0][part + 4 * k], w2[k], z);
-  z += __shfl_xor_sync(0xffffffffu, z, 1);
-  z += __shfl_xor_sync(0xffffffffu, z, 2);
-  z += b2;
-  if (part == 0) a[1][j] = z > 0.0f ? z : 0.0f;
-  __syncthreads();
-  // layer 3: a[1] -> a[0]
-  z = 0.0f;
-#pragma unroll
-  for (int k = 0; k < kH / 4; ++k) z = fmaf(a[1][part + 4 * k], w3[k], z);
-  z += __shfl_xor_sync(0xffffffffu, z, 1);
-  z += __shfl_xor_sync(0xffffffffu, z, 2);
-  z += b3;
-  if (part == 0) a[0][j] = z > 0.0f ? z : 0.0f;
-  __syncthreads();
-  if (t < 32) {
-#pragma unroll
-    for (int o = 0; o < kMaxO; ++o) {
-      if (o >= O) break;
-      float y = fmaf(a[0][t], w4[2 * o], 0.0f);
-      y = fmaf(a[0][t + 32], w4[2 * o + 1], y);
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) y += __shfl_xor_sync(0xffffffffu, y, off);
-      const float bo = __shfl_sync(0xffffffffu, b4, o);
-      if (t == 0) {
-        y += bo;
-        if (y_log) y_log[o] = y;
-        const float c = expm1f(y);
-        counts[o] = c > 0.0f ? c : 0.0f;
-      }
-    }
-  }
+}
+
+int mlp_view(const bo_mlp* m, const float** params, int* F, int* O) {
+  if (!m || !m->params) return BO_ERR_INVALID;
+  *params = m->params;
+  *F = m->F;
+  *O = m->O;
+  return BO_OK;
 }
 
 }  // namespace bo

@@ -319,6 +319,28 @@ class JoinSizer:
     def predict_device(self, features: np.ndarray, counts_dev) -> None:
         self.mlp.predict_counts_device(features, counts_dev)
 
+    def join_device(self, features: np.ndarray, build, probe, n_build: int, n_probe: int, date_lt: int,
+                    seg_eq: int, out_dev, pred_dev=None) -> None:
+        """The learned join in one call (bo_join_learned_device): the MLP
+        prediction is folded into the table's init kernel."""
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        b = N.JoinBuildCols(*[N.ptr(c) for c in build], n_build)
+        p = N.JoinProbeCols(*[N.ptr(c) for c in probe], n_probe)
+        self.engine.ctx.call("bo_join_learned_device", self.mlp.handle, C.c_void_p(f.ctypes.data), C.byref(b),
+                             C.byref(p), C.byref(N.JoinParams(date_lt, seg_eq)), C.c_void_p(N.ptr(out_dev)),
+                             C.c_void_p(N.ptr(pred_dev) if pred_dev is not None else 0))
+
+    def join(self, features: np.ndarray, build, probe, n_build: int, n_probe: int, date_lt: int,
+             seg_eq: int) -> dict:
+        """bo_join_learned: synchronous, exact rerun if the table overflowed."""
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        b = N.JoinBuildCols(*[N.ptr(c) for c in build], n_build)
+        p = N.JoinProbeCols(*[N.ptr(c) for c in probe], n_probe)
+        out = N.JoinResult()
+        self.engine.ctx.call("bo_join_learned", self.mlp.handle, C.c_void_p(f.ctypes.data), C.byref(b), C.byref(p),
+                             C.byref(N.JoinParams(date_lt, seg_eq)), C.byref(out))
+        return out.as_dict()
+
     # Fan-out of the radix-partitioned join from the predicted qualifying build
     # rows: one pass while the single-pass table (2.5 slots of 8 bytes per
     # row) fits in half the L2, else partitions of about 4096 keys (half of a

@@ -341,6 +341,10 @@ _SIGNATURES = {
                                                      C.POINTER(GbParams), C.c_int32, C.c_float, _P]),
     "bo_groupby_topk_partitioned": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),
                                               C.POINTER(GbParams), C.c_int32, C.c_float, C.POINTER(GbResult)]),
+    "bo_join_learned_device": (C.c_int, [_P, _P, _P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols),
+                                         C.POINTER(JoinParams), _P, _P]),
+    "bo_join_learned": (C.c_int, [_P, _P, _P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols),
+                                  C.POINTER(JoinParams), C.POINTER(JoinResult)]),
     "bo_join_partitioned_device": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols),
                                              C.POINTER(JoinParams), C.c_int32, _P]),
     "bo_join_partitioned": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols), C.POINTER(JoinParams),

@@ -722,6 +722,21 @@ int bo_mlp_infer_device(bo_ctx* ctx, const bo_mlp* mlp, const float* x, int32_t 
 int bo_mlp_predict_counts(bo_ctx* ctx, const bo_mlp* mlp, const float* features_host, float* counts_device,
                           float* log_device);
 
+/* Learned join in three launches (no counterpart in the reference; the
+ * presized form of the filtered join of run_q3, bespoke_tpch/query_q3.cpp:
+ * 182-260): the first kernel evaluates `mlp` (output 0 = predicted qualifying
+ * build rows) for the host feature vector in every block and clears the
+ * table sized from it -- the result bo_mlp_predict_counts followed by
+ * bo_join_presized_device gives, in one launch fewer -- then build and
+ * probe.  pred_device (optional) receives the prediction.  The _device form
+ * is asynchronous (out_device->overflowed reports a too-small table); the
+ * host form reruns the plain form on overflow. */
+int bo_join_learned_device(bo_ctx* ctx, const bo_mlp* mlp, const float* features_host,
+                           const bo_join_build_cols* build, const bo_join_probe_cols* probe,
+                           const bo_join_params* params, bo_join_result* out_device, float* pred_device);
+int bo_join_learned(bo_ctx* ctx, const bo_mlp* mlp, const float* features_host, const bo_join_build_cols* build,
+                    const bo_join_probe_cols* probe, const bo_join_params* params, bo_join_result* out_host);
+
 #ifdef __cplusplus
 }
 #endif
