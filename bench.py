@@ -314,7 +314,7 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
         def sseq(c=c, j=j, pl=pl, ob=ob):
             eng.join_presized_device(c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq, pl[1:2], ob)
 
-        pl[1] = float(exact_rows[i]) * 0.8
+        pl[1] = float(exact_rows[i])
         for fn in (lseq, sseq):
             fn()
             torch.cuda.synchronize()
@@ -349,8 +349,8 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
         c = copies[k]
         eng.join_count_device(c["b"], N_BUILD, c["j"].date_lt, c["j"].seg_eq, cnt)
         eng.ctx.call("bo_copy_d2h", C.byref(cnt_host), C.c_void_p(cnt.data_ptr()), C.c_size_t(8))
-        # exact sizing: 2 slots per qualifying row (the plain rule) = 2.5 x (0.8 x count)
-        C.c_float.from_address(pred_pin.value).value = 0.8 * cnt_host.value
+        # exact sizing: the plain form's slots per qualifying row (4, as the presize factor)
+        C.c_float.from_address(pred_pin.value).value = float(cnt_host.value)
         eng.ctx.call("bo_copy_h2d", C.c_void_p(g_pred[k].data_ptr() + 4), pred_pin, C.c_size_t(4))
         g_sized[k].replay()
         return read_result(k).as_dict()
@@ -366,9 +366,12 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     eng.ctx.call("bo_host_free_pinned", pred_pin)
 
     # ---- roofline of the dominant kernel (probe), timed alone on the stream:
-    # one graph per probe copy (against the table of the last build), K
-    # replays back to back with the copies rotated, average per launch.
+    # one graph per probe copy (against the learned-sized table of a timed
+    # step's build), K replays back to back with the copies rotated, average
+    # per launch.
     outp = torch.zeros(res_sz, dtype=torch.uint8, device="cuda")
+    step_graphs[2].replay()  # the table the timed steps probe: learned-sized (copy 2's build)
+    torch.cuda.synchronize()
     probe_graphs = []
     for k in range(3):
         g = torch.cuda.CUDAGraph()

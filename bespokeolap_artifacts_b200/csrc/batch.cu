@@ -1322,7 +1322,9 @@ Plan plan_instance(const bo_batch_instance& x) {
   d.kind = x.kind;
   d.pred_dev = x.kind == BO_BATCH_SCAN_AGG ? nullptr : x.predicted_device;
   const int64_t t = x.tile_rows > 0 ? ((int64_t)x.tile_rows + 4095) / 4096 * 4096 : 131072;
-  const float factor = x.presize_factor > 0.0f ? x.presize_factor : 2.5f;
+  // Default slots per predicted row: the solo presized forms' (join 4,
+  // group-by 2.5), so an instance's table matches its solo run's.
+  const float factor = x.presize_factor > 0.0f ? x.presize_factor : (x.kind == BO_BATCH_JOIN ? 4.0f : 2.5f);
   d.factor = factor;
   p.table_bytes = 0;
   p.weight = 0.0;

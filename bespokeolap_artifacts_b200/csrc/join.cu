@@ -33,7 +33,13 @@ namespace bo {
 constexpr int kJoinBlock = 512;
 constexpr int kBuildBlock = 256;
 constexpr int kMinCapLog2 = 10;
-constexpr float kPresizeFactor = 2.5f;  // slots per predicted row (load <= 0.4 at exact prediction)
+// Slots per qualifying build row: a predicted count (presized forms) or the
+// exact count (plain form).  Load <= 0.25 at an exact count: measured on B200
+// (6M-row probe, 60K keys), a table at load 0.46 probed in 33.0 us, at 0.23 in
+// 28.4 us (fewer collisions leave the first slot); sparser tables gain
+// little more (26.7 us at 0.06).
+constexpr float kPresizeFactor = 4.0f;
+constexpr uint64_t kPlainSlotsPerRow = 4;
 
 // Device-resident join state (one per context, in the "join_meta" region).
 struct JoinMeta {
@@ -494,7 +500,7 @@ int join_plain_impl(bo_ctx* ctx, const bo_join_build_cols& b, const bo_join_prob
   unsigned long long count = 0;
   BO_CUDA(ctx, cudaMemcpyAsync(&count, &ws.meta->count, sizeof(count), cudaMemcpyDeviceToHost, ctx->stream));
   BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  const int32_t cl = std::min(ws.max_log2, std::max(kMinCapLog2, ceil_log2(std::max<uint64_t>(count, 1) * 2)));
+  const int32_t cl = std::min(ws.max_log2, std::max(kMinCapLog2, ceil_log2(std::max<uint64_t>(count, 1) * kPlainSlotsPerRow)));
   void* dout = nullptr;
   if ((rc = region(ctx, "join_out", sizeof(bo_join_result), &dout))) return rc;
   bo_join_result* d = static_cast<bo_join_result*>(dout);
@@ -841,7 +847,7 @@ int bo_join_stream_host(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join
     unsigned long long count = 0;
     BO_CUDA(ctx, cudaMemcpyAsync(&count, &ws.meta->count, sizeof(count), cudaMemcpyDeviceToHost, ctx->stream));
     BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    cl = std::min(ws.max_log2, std::max(kMinCapLog2, ceil_log2(std::max<uint64_t>(count, 1) * 2)));
+    cl = std::min(ws.max_log2, std::max(kMinCapLog2, ceil_log2(std::max<uint64_t>(count, 1) * kPlainSlotsPerRow)));
   }
   if ((rc = stream_compute(ctx, bh, ph, prm, pred_device, cl, ws, in, s, set))) return rc;
   BO_CUDA(ctx, cudaMemcpyAsync(out_host, s.combined, sizeof(bo_join_result), cudaMemcpyDeviceToHost, ctx->stream));

@@ -342,7 +342,7 @@ class JoinSizer:
         return out.as_dict()
 
     # Fan-out of the radix-partitioned join from the predicted qualifying build
-    # rows: one pass while the single-pass table (2.5 slots of 8 bytes per
+    # rows: one pass while the single-pass table (4 slots of 8 bytes per
     # row) fits in half the L2, else partitions of about 4096 keys (half of a
     # partition's 8192-slot shared-memory table).
     PART_KEYS = 4096
@@ -351,7 +351,7 @@ class JoinSizer:
     def fanout(cls, predicted_rows: float, l2_bytes: int = 126 << 20) -> int:
         """log2 of the partition count for a predicted qualifying-row count (0 = single pass)."""
         r = max(0.0, float(predicted_rows))
-        if r * 2.5 * 8 <= l2_bytes / 2:
+        if r * 4 * 8 <= l2_bytes / 2:
             return 0
         return int(min(N.JOIN_MAX_LOG2_PARTITIONS, max(1, math.ceil(math.log2(r / cls.PART_KEYS)))))
 

@@ -612,7 +612,7 @@ typedef struct bo_batch_instance {
   int32_t kind;            /* BO_BATCH_* */
   int32_t tile_rows;       /* largest rows per work item (tiles are smaller for small stages); 0 = default */
   float predicted;         /* join: qualifying build rows; group-by: groups; <= 0 sizes for the upper bound */
-  float presize_factor;    /* slots per predicted row; 0 = 2.5 */
+  float presize_factor;    /* slots per predicted row; 0 = the solo form's (join 4, group-by 2.5) */
   /* scan-agg (wide layout) */
   bo_fact_cols fact;
   int32_t ship_cutoff, n_flag_a, n_flag_b, pad0;
