@@ -453,7 +453,7 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     # ---- the other configurations (rank 0; extra keys of the same line)
     extra = {}
     if rank == 0 and args.sections != "none":
-        wanted = (["scan_agg", "groupby", "join_large", "batch", "serving"] if args.sections == "all"
+        wanted = (["scan_agg", "groupby", "join_large", "batch", "serving", "tpch"] if args.sections == "all"
                   else args.sections.split(","))
         peak_gbs, _ = peaks()
         keep = {}
@@ -470,6 +470,8 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
                     extra[name] = batch_section(eng, stream, K, sizer, keep.get("gb_sizer"))
                 elif name == "serving":
                     extra[name] = serving_section(eng, stream, sizer, keep.get("gb_sizer"))
+                elif name == "tpch":
+                    extra[name] = tpch_section()
             except Exception as e:  # report, never lose the headline line
                 extra[name] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
             if name in extra:
@@ -913,6 +915,87 @@ def serving_section(eng, stream, join_sizer=None, gb_sizer=None, rates=(50, 500,
     return out
 
 
+TPCH_REQUESTS = [  # synthetic parameters; segments SEG_A..SEG_E and comment words of the seeded generator
+    ("1", '1 "90"'), ("3", '3 "SEG_B" "1995-03-17"'), ("6", '6 "1994-02-01" "0.07" "23"'),
+    ("10", '10 "1993-10-01"'), ("13", '13 "pending" "deposits"'), ("18", '18 "250"'),
+]
+
+
+def _driver_times(driver: Path, data: Path, workdir: Path, requests: list[str], unit: str) -> tuple[float, list]:
+    """Run a drop-in driver (load, build, query over stdin) and return its
+    Build ms and each request's execution time in ms."""
+    workdir.mkdir(parents=True, exist_ok=True)
+    env = dict(os.environ, BO_EXEC_US="1")
+    p = subprocess.run([str(driver), str(data) + "/"], input="\n".join(requests) + "\n\n", text=True,
+                       capture_output=True, cwd=workdir, timeout=900, env=env)
+    if p.returncode != 0:
+        raise RuntimeError(f"{driver.name} exited {p.returncode}: {p.stderr[-300:]}")
+    build_ms = float(re.search(r"Build ms: (\d+)", p.stdout).group(1))
+    if unit == "us":
+        t = [int(m) / 1e3 for m in re.findall(r"^\d+ \| Execution us: (\d+)$", p.stderr, re.M)]
+    else:
+        t = [float(m) for m in re.findall(r"^\d+ \| Execution ms: (\d+)$", p.stdout, re.M)]
+    if len(t) != len(requests):
+        raise RuntimeError(f"{driver.name}: {len(t)} timings for {len(requests)} requests")
+    return build_ms, t
+
+
+def tpch_section(reps: int = 10, n_customer: int = 150_000, n_orders: int = 1_500_000) -> dict:
+    """The drop-in end to end: the GPU host library's driver and the reference's
+    own load / build / query (compiled unchanged, single-threaded queries) read
+    the same seeded Parquet files of TPC-H shape (150,000 customers, 1,500,000
+    orders, ~6M lineitems) and answer the same requests, each repeated `reps`
+    times; per query the median execution time of each, and whether the
+    result<idx>.csv files of the first repetition agree (Q3 up to the order of
+    rows tied on revenue and orderdate)."""
+    import csv
+    import shutil
+    import tempfile
+
+    from bespokeolap_artifacts_b200.tpch_data import write_tpch
+
+    gpu = ROOT / "bespokeolap_artifacts_b200" / "host" / "bespoke_tpch_gpu"
+    ref = ROOT / "oracle" / "_ref" / "ref_tpch_driver"
+    if not gpu.exists():
+        raise RuntimeError("GPU drop-in driver not built")
+    tmp = Path(tempfile.mkdtemp(prefix="bo_tpch_"))
+    try:
+        t0 = time.perf_counter()
+        data = write_tpch(tmp / "data", n_customer=n_customer, n_orders=n_orders, seed=11)
+        gen_s = time.perf_counter() - t0
+        reqs = [r for _, r in TPCH_REQUESTS for _ in range(reps)]
+        g_build, g_t = _driver_times(gpu, data, tmp / "gpu", reqs, "us")
+        out = {"data": f"seeded synthetic Parquet: {n_customer} customers, {n_orders} orders, "
+                       f"~{4 * n_orders} lineitems (generated in {gen_s:.0f} s)",
+               "reps": reps, "gpu_build_ms": g_build, "queries": {}}
+        have_ref = ref.exists()
+        if have_ref:
+            r_build, r_t = _driver_times(ref, data, tmp / "ref", reqs, "ms")
+            out["ref_build_ms"] = r_build
+            out["ref_note"] = ("reference query() reports whole milliseconds (truncated), single-threaded; "
+                               f"host {host_cpu()}")
+        for qi, (qid, req) in enumerate(TPCH_REQUESTS):
+            sl = slice(qi * reps, (qi + 1) * reps)
+            q = {"request": req, "gpu_ms": statistics.median(g_t[sl])}
+            if have_ref:
+                q["ref_ms"] = statistics.median(r_t[sl])
+                q["ref_mean_ms"] = sum(r_t[sl]) / reps
+                g_csv, r_csv = tmp / "gpu" / f"result{qi * reps + 1}.csv", tmp / "ref" / f"result{qi * reps + 1}.csv"
+                if qid == "3":
+                    rg, rr = list(csv.reader(open(g_csv))), list(csv.reader(open(r_csv)))
+                    canon = [rr[0]] + sorted(rr[1:], key=lambda x: (-float(x[1]), x[2], int(x[0])))
+                    q["answers_identical"] = rg == canon
+                else:
+                    q["answers_identical"] = g_csv.read_bytes() == r_csv.read_bytes()
+                q["rows"] = sum(1 for _ in open(g_csv)) - 1
+                if q["ref_mean_ms"] > 0:
+                    q["speedup_vs_ref_mean"] = q["ref_mean_ms"] / q["gpu_ms"]
+            out["queries"]["Q" + qid] = q
+        return out
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def cpu_baseline(j) -> dict:
     """The reference's run_q3 (compiled unchanged into oracle/_ref) on the same
     input mapped onto its tables, on one host core (the reference pins queries
@@ -998,7 +1081,7 @@ def main():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--sections", default="all",
                     help="other configurations reported beside the headline: all, none, or a comma list of "
-                         "scan_agg,groupby,batch,serving")
+                         "scan_agg,groupby,join_large,batch,serving,tpch")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))

@@ -814,9 +814,19 @@ void query(Database* db) {
     if (!iss) continue;
     requests.push_back(Request{id, line});
   }
+  // BO_EXEC_US set: each request also reports its time in microseconds on
+  // stderr ("<idx> | Execution us: <us>"); stdout keeps the reference's lines.
+  const bool exec_us = std::getenv("BO_EXEC_US") != nullptr;
   for (size_t idx = 0; idx < requests.size(); ++idx) {
     const auto& r = requests[idx];
     const auto start = std::chrono::steady_clock::now();
+    auto report = [&](std::chrono::steady_clock::time_point end) {
+      std::cout << (idx + 1) << " | Execution ms: "
+                << std::chrono::duration_cast<std::chrono::milliseconds>(end - start).count() << "\n";
+      if (exec_us)
+        std::cerr << (idx + 1) << " | Execution us: "
+                  << std::chrono::duration_cast<std::chrono::microseconds>(end - start).count() << "\n";
+    };
     const std::string file = "result" + std::to_string(idx + 1) + ".csv";
     std::istringstream iss(r.line);
     std::string qid;
@@ -829,49 +839,49 @@ void query(Database* db) {
     if (r.id == "1") {
       const std::string delta = arg("DELTA");
       const auto rows = run_q1(*db, delta);
-      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      const auto end = std::chrono::steady_clock::now();
       write_q1_csv(file, rows);
-      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+      report(end);
     } else if (r.id == "3") {
       const std::string segment = arg("SEGMENT");
       const std::string date = arg("DATE");
       const auto rows = run_q3(*db, segment, date);
-      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      const auto end = std::chrono::steady_clock::now();
       write_q3_csv(*db, file, rows);
-      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+      report(end);
     } else if (r.id == "10") {
       const std::string date = arg("DATE");
       const auto rows = run_q10(*db, date);
-      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      const auto end = std::chrono::steady_clock::now();
       write_q10_csv(file, rows);
-      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+      report(end);
     } else if (r.id == "13") {
       const std::string word1 = arg("WORD1");
       const std::string word2 = arg("WORD2");
       const auto rows = run_q13(*db, word1, word2);
-      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      const auto end = std::chrono::steady_clock::now();
       write_q13_csv(file, rows);
-      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+      report(end);
     } else if (r.id == "18") {
       const std::string quantity = arg("QUANTITY");
       const auto rows = run_q18(*db, quantity);
-      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      const auto end = std::chrono::steady_clock::now();
       write_q18_csv(*db, file, rows);
-      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+      report(end);
     } else if (r.id == "6") {
       const std::string date = arg("DATE");
       const std::string discount = arg("DISCOUNT");
       const std::string quantity = arg("QUANTITY");
       const auto rows = run_q6(*db, date, discount, quantity);
-      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
+      const auto end = std::chrono::steady_clock::now();
       write_q6_csv(file, rows);
-      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+      report(end);
     } else {
       // Not on the GPU path: the reference's stub record.
       std::ofstream out(file);
       out << "query_id,params\n" << escape_csv(r.id) << "," << escape_csv(r.line) << "\n";
-      const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start);
-      std::cout << (idx + 1) << " | Execution ms: " << ms.count() << "\n";
+      const auto end = std::chrono::steady_clock::now();
+      report(end);
     }
   }
 }

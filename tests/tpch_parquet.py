@@ -1,133 +1,2 @@
-"""Seeded TPC-H-shaped Parquet files for the drop-in tests (test data only).
-
-Writes the eight tables the reference's loader reads
-(bespoke_tpch/loader_impl.cpp:12-19) with every column its builder reads, at
-a small scale: customers with five market segments, nations, names,
-addresses, phones and comments (some with quotes and commas), orders with
-dates over 1992..1998, 1..7 lineitems per order sorted by orderkey with
-TPC-H-like quantities, prices, discounts, taxes, flags and ship dates.
-Decimal columns are DOUBLE, or DECIMAL(15,2) with decimal=True.
-
-Key layouts (they select the reference's code paths):
-  order_keys    "sparse": 8 of every 32 keys (the dbgen pattern);
-                "dense": 1..n with key 1 dated first and key n last, so the
-                date-sorted orders start at 1 and end at n while the rows in
-                between are not in key order.
-  customer_keys "dense": 1..n in order; "inner": 1, a shuffle of 2..n-1, n
-                (first and last as dense, the rest not); "sparse": odd keys,
-                shuffled, the last rows repeating earlier keys, and orders
-                that name keys without a customer.
-  shuffle_lineitem  lineitems in random order instead of by orderkey.
-The nation table has keys 0..24 except 7; customers' nationkeys run 0..26.
-"""
-from __future__ import annotations
-
-from pathlib import Path
-
-import numpy as np
-import pyarrow as pa
-import pyarrow.parquet as pq
-
-SEGMENTS = ["SEG_A", "SEG_B", "SEG_C", "SEG_D", "SEG_E"]
-WORDS = ["ironic", "quick", "pending", "bold", 'say "hi"', "a,b", "deposits", "", "x\"y", "final"]
-D1992 = 8035  # 1992-01-01 in days since 1970-01-01
-
-
-def _dec(values: np.ndarray, decimal: bool) -> pa.Array:
-    if not decimal:
-        return pa.array(values, pa.float64())
-    from decimal import Decimal
-
-    return pa.array([Decimal(f"{v:.2f}") for v in values], pa.decimal128(15, 2))
-
-
-def _text(rng, n: int, words: int) -> list[str]:
-    picks = rng.integers(0, len(WORDS), (n, words))
-    return [" ".join(WORDS[i] for i in row) for row in picks]
-
-
-def _ragged_text(rng, n: int, max_words: int) -> list[str]:
-    counts = rng.integers(0, max_words + 1, n)
-    return [" ".join(WORDS[i] for i in rng.integers(0, len(WORDS), c)) for c in counts]
-
-
-def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: int = 0,
-               decimal: bool = False, order_keys: str = "sparse", customer_keys: str = "dense",
-               shuffle_lineitem: bool = False) -> Path:
-    rng = np.random.default_rng(seed)
-    out.mkdir(parents=True, exist_ok=True)
-    if customer_keys == "dense":
-        custkey = np.arange(1, n_customer + 1, dtype=np.int32)
-    elif customer_keys == "inner":
-        custkey = np.concatenate([[1], rng.permutation(np.arange(2, n_customer)), [n_customer]]).astype(np.int32)
-    elif customer_keys == "sparse":
-        custkey = rng.permutation(np.arange(n_customer, dtype=np.int32) * 2 + 1)
-        custkey[-5:] = custkey[:5]  # repeated keys: the last row of each wins
-    else:
-        raise ValueError(customer_keys)
-    seg = rng.integers(0, 5, n_customer)
-    pq.write_table(pa.table({
-        "c_custkey": custkey, "c_name": [f"Customer#{k:09d}" for k in custkey],
-        "c_address": _text(rng, n_customer, 2), "c_nationkey": rng.integers(0, 27, n_customer).astype(np.int32),
-        "c_phone": [f"{10 + a}-{b:03d}-{c:03d}-{d:04d}" for a, b, c, d in
-                    zip(*(rng.integers(0, m, n_customer) for m in (25, 1000, 1000, 10000)))],
-        "c_acctbal": _dec(rng.integers(-99999, 999999, n_customer) / 100.0, decimal),
-        "c_mktsegment": [SEGMENTS[s] for s in seg], "c_comment": _text(rng, n_customer, 3),
-    }), out / "customer.parquet")
-    # dates 1992-01-01 .. 1998-08-02
-    o_date = rng.integers(D1992, D1992 + 2405, n_orders).astype(np.int32)
-    if order_keys == "sparse":  # TPC-H orderkeys: 8 of every 32
-        orderkey = (np.arange(n_orders, dtype=np.int64) // 8 * 32 + np.arange(n_orders) % 8 + 1).astype(np.int32)
-    elif order_keys == "dense":
-        orderkey = np.arange(1, n_orders + 1, dtype=np.int32)
-        o_date[0], o_date[-1] = D1992, D1992 + 2404
-    else:
-        raise ValueError(order_keys)
-    if customer_keys == "sparse":
-        o_cust = rng.choice(np.concatenate([custkey, custkey[:50] - 1]), n_orders).astype(np.int32)
-    else:
-        o_cust = rng.integers(1, n_customer + 1, n_orders).astype(np.int32)
-    pq.write_table(pa.table({
-        "o_orderkey": orderkey, "o_custkey": o_cust, "o_orderstatus": ["O"] * n_orders,
-        "o_totalprice": _dec(rng.integers(100000, 50000000, n_orders) / 100.0, decimal),
-        "o_orderdate": pa.array(o_date, pa.date32()), "o_orderpriority": ["1-URGENT"] * n_orders,
-        "o_clerk": ["Clerk#000000001"] * n_orders, "o_shippriority": np.zeros(n_orders, np.int32),
-        "o_comment": _ragged_text(rng, n_orders, 8),
-    }), out / "orders.parquet")
-    lines = rng.integers(1, 8, n_orders)
-    lk = np.repeat(orderkey, lines)
-    ld = np.repeat(o_date, lines)
-    n = len(lk)
-    qty = rng.integers(1, 51, n)
-    price = qty * rng.integers(90000, 210000, n) / 100.0
-    ship = ld + rng.integers(1, 122, n)
-    rf = np.where(ship <= D1992 + 1267, np.array(["R", "A"])[rng.integers(0, 2, n)], "N")  # before / after 1995-06-17
-    ls = np.where(ship > D1992 + 1267, "O", "F")
-    if shuffle_lineitem:
-        perm = rng.permutation(n)
-        lk, ld, qty, price, ship, rf, ls = (a[perm] for a in (lk, ld, qty, price, ship, rf, ls))
-    pq.write_table(pa.table({
-        "l_orderkey": lk, "l_partkey": rng.integers(1, 200, n).astype(np.int32),
-        "l_suppkey": rng.integers(1, 10, n).astype(np.int32), "l_linenumber": np.ones(n, np.int32),
-        "l_quantity": _dec(qty.astype(np.float64), decimal), "l_extendedprice": _dec(price, decimal),
-        "l_discount": _dec(rng.integers(0, 11, n) / 100.0, decimal), "l_tax": _dec(rng.integers(0, 9, n) / 100.0, decimal),
-        "l_returnflag": rf.tolist(), "l_linestatus": ls.tolist(),
-        "l_shipdate": pa.array(ship.astype(np.int32), pa.date32()),
-        "l_commitdate": pa.array((ld + 30).astype(np.int32), pa.date32()),
-        "l_receiptdate": pa.array((ship + 5).astype(np.int32), pa.date32()),
-        "l_shipinstruct": ["DELIVER IN PERSON"] * n, "l_shipmode": ["TRUCK"] * n, "l_comment": [""] * n,
-    }), out / "lineitem.parquet")
-    one = np.ones(1, np.int32)
-    pq.write_table(pa.table({"p_partkey": one, "p_name": ["p"], "p_mfgr": ["m"], "p_brand": ["b"], "p_type": ["t"],
-                             "p_size": one, "p_container": ["c"], "p_retailprice": _dec(np.ones(1), decimal),
-                             "p_comment": [""]}), out / "part.parquet")
-    pq.write_table(pa.table({"s_suppkey": one, "s_name": ["s"], "s_address": ["a"], "s_nationkey": one * 0,
-                             "s_phone": ["10-0"], "s_acctbal": _dec(np.ones(1), decimal), "s_comment": [""]}),
-                   out / "supplier.parquet")
-    pq.write_table(pa.table({"ps_partkey": one, "ps_suppkey": one, "ps_availqty": one,
-                             "ps_supplycost": _dec(np.ones(1), decimal), "ps_comment": [""]}), out / "partsupp.parquet")
-    nkey = np.array([k for k in range(25) if k != 7], np.int32)
-    pq.write_table(pa.table({"n_nationkey": nkey, "n_name": [f"NATION_{k:02d}" for k in nkey],
-                             "n_regionkey": nkey % 5, "n_comment": [""] * len(nkey)}), out / "nation.parquet")
-    pq.write_table(pa.table({"r_regionkey": one * 0, "r_name": ["REGION0"], "r_comment": [""]}), out / "region.parquet")
-    return out
+"""The drop-in tests' Parquet writer (bespokeolap_artifacts_b200.tpch_data)."""
+from bespokeolap_artifacts_b200.tpch_data import SEGMENTS, WORDS, write_tpch  # noqa: F401
