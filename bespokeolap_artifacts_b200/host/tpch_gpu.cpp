@@ -352,6 +352,22 @@ std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, con
   return {Q6ResultRow{r.revenue_raw}};
 }
 
+namespace {
+// Room for `count` result records of type T in the Database's pinned buffer.
+template <class T>
+T* result_rows(const Database& db, int64_t count) {
+  const size_t bytes = sizeof(T) * static_cast<size_t>(std::max<int64_t>(count, 1));
+  if (bytes > db.result_host_bytes) {
+    if (db.result_host) check(db.ctx, bo_host_free_pinned(db.ctx, db.result_host), "result buffer free");
+    db.result_host = nullptr;
+    db.result_host_bytes = 0;
+    check(db.ctx, bo_host_alloc_pinned(db.ctx, bytes, &db.result_host), "result buffer alloc");
+    db.result_host_bytes = bytes;
+  }
+  return static_cast<T*>(db.result_host);
+}
+}  // namespace
+
 std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, const std::string& date) {
   const int16_t d = date_offset_of(date, db.base_date_days);
   int32_t code = -1;
@@ -376,9 +392,9 @@ std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, 
   t.l_shipdate = col<int16_t>(db.l_shipdate);
   t.l_discounted_price = col<int32_t>(db.l_discounted_price);
   t.n_lineitem = db.n_lineitem;
-  std::vector<bo_tpch_q3_row> out(static_cast<size_t>(std::max<int64_t>(db.n_orders, 1)));
+  bo_tpch_q3_row* out = result_rows<bo_tpch_q3_row>(db, db.n_orders);
   int64_t n = 0;
-  check(db.ctx, bo_tpch_q3(db.ctx, &t, d, code, out.data(), db.n_orders, &n), "q3");
+  check(db.ctx, bo_tpch_q3(db.ctx, &t, d, code, out, db.n_orders, &n), "q3");
   std::vector<Q3ResultRow> rows(static_cast<size_t>(n));
   for (int64_t i = 0; i < n; ++i) {
     rows[i].orderkey = out[i].orderkey;
@@ -417,9 +433,9 @@ std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date) {
   t.n_custkey_map = db.n_custkey_map;
   t.c_nationkey = col<int32_t>(db.c_nationkey);
   t.n_customer = db.n_customer;
-  std::vector<bo_tpch_q10_row> out(static_cast<size_t>(std::max<int64_t>(db.n_custkey_map, 1)));
+  bo_tpch_q10_row* out = result_rows<bo_tpch_q10_row>(db, db.n_custkey_map);
   int64_t n = 0;
-  check(db.ctx, bo_tpch_q10(db.ctx, &t, start, end, rf * ls_count, ls_count, out.data(), db.n_custkey_map, &n),
+  check(db.ctx, bo_tpch_q10(db.ctx, &t, start, end, rf * ls_count, ls_count, out, db.n_custkey_map, &n),
         "q10");
   std::vector<Q10ResultRow> rows(static_cast<size_t>(n));
   for (int64_t i = 0; i < n; ++i) {
@@ -448,11 +464,11 @@ std::vector<Q13ResultRow> run_q13(const Database& db, const std::string& word1, 
   t.n_customer = db.n_customer;
   t.n_count_map = std::max<int64_t>(db.custkey_bound, 1);
   const int64_t cap = db.n_orders + 1;  // distinct order counts
-  std::vector<bo_tpch_q13_row> out(static_cast<size_t>(cap));
+  bo_tpch_q13_row* out = result_rows<bo_tpch_q13_row>(db, cap);
   int64_t n = 0;
   check(db.ctx,
         bo_tpch_q13(db.ctx, &t, word1.data(), static_cast<int64_t>(word1.size()), word2.data(),
-                    static_cast<int64_t>(word2.size()), out.data(), cap, &n),
+                    static_cast<int64_t>(word2.size()), out, cap, &n),
         "q13");
   std::vector<Q13ResultRow> rows(static_cast<size_t>(n));
   for (int64_t i = 0; i < n; ++i) rows[i] = Q13ResultRow{out[i].c_count, out[i].custdist};
@@ -479,9 +495,9 @@ std::vector<Q18ResultRow> run_q18(const Database& db, const std::string& quantit
   t.orderkey_bound = max_key >= 0 ? static_cast<int64_t>(max_key) + 1 : 0;
   t.dense_orderkeys = db.dense_orderkeys ? 1 : 0;
   t.dense_custkeys = db.dense_custkeys ? 1 : 0;
-  std::vector<bo_tpch_q18_row> out(static_cast<size_t>(std::max<int64_t>(db.n_orders, 1)));
+  bo_tpch_q18_row* out = result_rows<bo_tpch_q18_row>(db, db.n_orders);
   int64_t n = 0;
-  check(db.ctx, bo_tpch_q18(db.ctx, &t, threshold, out.data(), db.n_orders, &n), "q18");
+  check(db.ctx, bo_tpch_q18(db.ctx, &t, threshold, out, db.n_orders, &n), "q18");
   std::vector<Q18ResultRow> rows(static_cast<size_t>(n));
   for (int64_t i = 0; i < n; ++i) {
     const auto& g = out[i];
@@ -632,6 +648,7 @@ Database::~Database() {
                           &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
+  if (result_host) bo_host_free_pinned(ctx, result_host);
   bo_destroy(ctx);
 }
 

@@ -96,6 +96,10 @@ struct Database {
   // Result record of the last scan-agg / Q6 query.  Queries on one Database
   // run one at a time (as the reference's single-threaded query()).
   bo_tpch::DeviceColumn scratch;
+  // Pinned host buffer the multi-row queries receive their records in; grown
+  // on demand, never cleared (each call reads only the rows it was given).
+  mutable void* result_host = nullptr;
+  mutable size_t result_host_bytes = 0;
   ~Database();
 };
 
