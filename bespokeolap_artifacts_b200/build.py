@@ -105,7 +105,7 @@ def build_host(force: bool = False) -> Path | None:
     deps = srcs + [HOST / "tpch_gpu.hpp", INCLUDE / "bespoke_gpu.h", LIB_PATH]
     arrow = [f"-L{libdir}", "-l:libarrow.so.2400", "-l:libparquet.so.2400", f"-Wl,-rpath,{libdir}"]
     if force or _stale(HOST_LIB, deps):
-        subprocess.run(["g++", "-std=c++20", "-O2", "-fPIC", "-shared", f"-I{INCLUDE}", f"-I{inc}", *map(str, srcs),
+        subprocess.run(["g++", "-std=c++20", "-O2", "-pthread", "-fPIC", "-shared", f"-I{INCLUDE}", f"-I{inc}", *map(str, srcs),
                         f"-L{PKG}", "-lbespoke_gpu", f"-Wl,-rpath,{PKG}", *arrow, "-o", str(HOST_LIB)], check=True)
     main = HOST / "driver_main.cpp"
     if force or _stale(HOST_DRIVER, [main, HOST_LIB, HOST / "tpch_gpu.hpp"]):

@@ -185,15 +185,17 @@ __device__ __forceinline__ unsigned __int128 block_sum_u128(unsigned __int128 v,
 
 // Last-block epilogue: true in every thread of the block that finished last
 // (all other blocks' global atomics are then visible to it).
-__device__ __forceinline__ bool last_block(uint32_t* done) {
+__device__ __forceinline__ bool last_block(uint32_t* done, uint32_t blocks) {
   __shared__ bool is_last;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) is_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+  if (threadIdx.x == 0) is_last = (atomicAdd(done, 1u) == blocks - 1);
   __syncthreads();
   if (is_last) __threadfence();
   return is_last;
 }
+
+__device__ __forceinline__ bool last_block(uint32_t* done) { return last_block(done, gridDim.x); }
 
 // ------------------------------------------- TMA bulk copies (no multicast) --
 // One-shot global -> shared bulk copy completed on an mbarrier.  Only this

@@ -54,6 +54,11 @@ __global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(const unsigned l
                                                                 uint32_t* __restrict__ done) {
   const int64_t n = sort_n(n_max, n_dev);
   if (n == 0) return;  // nothing to sort: no histogram, no ticket
+  // Blocks past the actual count (the grid covers the upper bound) retire at
+  // once; the last-block ticket counts only the blocks that hold keys.
+  const int64_t blocks_needed = (n + blockDim.x - 1) / blockDim.x;
+  const uint32_t active = blocks_needed < (int64_t)gridDim.x ? (uint32_t)blocks_needed : gridDim.x;
+  if (blockIdx.x >= active) return;
   __shared__ uint32_t h[kMaxPasses][kRadix];
   for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
@@ -65,7 +70,7 @@ __global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(const unsigned l
   __syncthreads();
   for (int i = threadIdx.x; i < n_passes * kRadix; i += blockDim.x)
     if ((&h[0][0])[i]) atomicAdd(&hist[i], (unsigned long long)(&h[0][0])[i]);
-  if (!last_block(done)) return;
+  if (!last_block(done, active)) return;
   __shared__ unsigned long long sc[kRadix];
   for (int p = 0; p < n_passes; ++p) {
     const unsigned long long v = __ldcg(&hist[p * kRadix + threadIdx.x]);
@@ -92,6 +97,9 @@ __global__ void __launch_bounds__(kSortBlock) radix_pass_kernel(
   // order, so no live tile ever looks back at them).
   const int64_t n = sort_n(n_max, n_dev);
   if (n == 0) return;  // nothing to sort: retire before touching the tile counter
+  // Blocks beyond the tiles the actual count needs retire without a ticket
+  // (block 0 always stays, and the staying blocks take every tile in order).
+  if ((int64_t)blockIdx.x * kSortTile >= n) return;
   __shared__ uint32_t warp_cnt[kSortWarps][kRadix];
   __shared__ unsigned long long tile_base[kRadix];
   __shared__ uint32_t tile_s;

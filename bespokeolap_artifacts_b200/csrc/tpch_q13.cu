@@ -24,6 +24,7 @@
 
 #include "common.cuh"
 #include "context.cuh"
+#include "q13_search.cuh"
 
 namespace bo {
 namespace {
@@ -31,6 +32,7 @@ namespace {
 constexpr int kQ13Block = 256;
 constexpr int kQ13Warps = kQ13Block / 32;
 constexpr uint32_t kQ13SliceBytes = 4096;  // per warp: 32 comments of up to 128 bytes on average
+constexpr int kQ13StageBatch = 2;          // 16-byte loads per lane in flight while staging
 constexpr int kQ13SmallBins = 1024;
 
 // First position p >= from with s[p, p + l) == w, else n; an empty word
@@ -74,25 +76,47 @@ __global__ void __launch_bounds__(kQ13Block) q13_orders_kernel(const uint8_t* __
   for (int64_t g = (int64_t)blockIdx.x * kQ13Warps + warp; g * 32 < n; g += warps) {
     const int64_t first = g * 32;
     const int64_t last = min(first + 32, n);
-    const uint32_t b0 = offsets[first], b1 = offsets[last];
+    const int64_t i = first + lane;
+    // Independent loads first: this lane's bounds and custkey, the group's byte range.
+    uint32_t s0 = 0, s1 = 0;
+    int32_t c = 0;
+    if (i < last) {
+      s0 = offsets[i];
+      s1 = offsets[i + 1];
+      c = o_custkey[i];
+    }
+    const uint32_t b0 = __shfl_sync(0xffffffffu, s0, 0);
+    const uint32_t b1 = __shfl_sync(0xffffffffu, s1, (int)(last - first - 1));
     const uint32_t a0 = b0 & ~15u;
     const bool staged = b1 - a0 <= kQ13SliceBytes;
     if (staged) {
-      for (uint32_t off = (uint32_t)lane * 16u; a0 + off < b1; off += 512u) {
-        if (a0 + off + 16u <= total) {
-          *reinterpret_cast<uint4*>(slice + off) = __ldg(reinterpret_cast<const uint4*>(data + a0 + off));
-        } else {
-          for (uint32_t k = 0; a0 + off + k < total; ++k) slice[off + k] = __ldg(data + a0 + off + k);
+      // Up to kQ13StageBatch 16-byte loads per lane in flight, then the stores.
+      for (uint32_t base = (uint32_t)lane * 16u; a0 + base < b1; base += kQ13StageBatch * 512u) {
+        uint4 v[kQ13StageBatch];
+#pragma unroll
+        for (int k = 0; k < kQ13StageBatch; ++k) {
+          const uint32_t off = base + (uint32_t)k * 512u;
+          if (a0 + off < b1 && a0 + off + 16u <= total)
+            v[k] = __ldg(reinterpret_cast<const uint4*>(data + a0 + off));
+        }
+#pragma unroll
+        for (int k = 0; k < kQ13StageBatch; ++k) {
+          const uint32_t off = base + (uint32_t)k * 512u;
+          if (a0 + off < b1) {
+            if (a0 + off + 16u <= total) {
+              *reinterpret_cast<uint4*>(slice + off) = v[k];
+            } else {
+              for (uint32_t j = 0; a0 + off + j < total; ++j) slice[off + j] = __ldg(data + a0 + off + j);
+            }
+          }
         }
       }
     }
     __syncwarp();
-    const int64_t i = first + lane;
     if (i < last) {
-      const uint32_t s0 = offsets[i], s1 = offsets[i + 1];
-      const uint8_t* s = staged ? slice + (s0 - a0) : data + s0;
-      if (!q13_match(s, s1 - s0, w1, l1, w2, l2)) {
-        const int32_t c = o_custkey[i];
+      const bool hit = staged ? q13_match_slice(slice, (int)(s0 - a0), (int)(s1 - s0), w1, (int)l1, w2, (int)l2)
+                              : q13_match(data + s0, s1 - s0, w1, l1, w2, l2);
+      if (!hit) {
         if (c < 0 || (int64_t)c >= n_counts) {
           raise_error(err, kErrValueRange);
         } else {

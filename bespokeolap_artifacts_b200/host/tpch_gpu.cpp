@@ -18,6 +18,7 @@
 #include <numeric>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 #include <unordered_map>
 
 namespace bo_tpch {
@@ -353,6 +354,25 @@ std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, con
 }
 
 namespace {
+// fn(begin, end) over [0, n), split across host threads when n is large: the
+// result rows gather host-resident strings of random customers, a loop bound
+// by memory latency that more threads overlap.
+template <class F>
+void for_row_ranges(int64_t n, const F& fn) {
+  constexpr int64_t kRowsPerThread = 8192;
+  const int64_t hw = std::max<int64_t>(1, static_cast<int64_t>(std::thread::hardware_concurrency()));
+  const int64_t parts = std::min<int64_t>(std::min<int64_t>(hw, 8), (n + kRowsPerThread - 1) / kRowsPerThread);
+  if (parts <= 1) {
+    fn(int64_t{0}, n);
+    return;
+  }
+  const int64_t step = (n + parts - 1) / parts;
+  std::vector<std::thread> pool;
+  for (int64_t p = 1; p < parts; ++p) pool.emplace_back([&fn, p, step, n] { fn(p * step, std::min(n, (p + 1) * step)); });
+  fn(int64_t{0}, std::min(n, step));
+  for (auto& t : pool) t.join();
+}
+
 // Room for `count` result records of type T in the Database's pinned buffer.
 template <class T>
 T* result_rows(const Database& db, int64_t count) {
@@ -438,19 +458,21 @@ std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date) {
   check(db.ctx, bo_tpch_q10(db.ctx, &t, start, end, rf * ls_count, ls_count, out, db.n_custkey_map, &n),
         "q10");
   std::vector<Q10ResultRow> rows(static_cast<size_t>(n));
-  for (int64_t i = 0; i < n; ++i) {
-    const auto& g = out[i];
-    const size_t r = static_cast<size_t>(g.cust_row);
-    auto& row = rows[i];
-    row.custkey = g.custkey;
-    row.name = db.c_name.view(r);
-    row.revenue_raw = g.revenue_raw;
-    row.acctbal_raw = db.c_acctbal[r];
-    row.nation_name = db.nation_name[static_cast<size_t>(g.nationkey)];
-    row.address = db.c_address.view(r);
-    row.phone = db.c_phone.view(r);
-    row.comment = db.c_comment.view(r);
-  }
+  for_row_ranges(n, [&](int64_t lo, int64_t hi) {
+    for (int64_t i = lo; i < hi; ++i) {
+      const auto& g = out[i];
+      const size_t r = static_cast<size_t>(g.cust_row);
+      auto& row = rows[i];
+      row.custkey = g.custkey;
+      row.name = db.c_name.view(r);
+      row.revenue_raw = g.revenue_raw;
+      row.acctbal_raw = db.c_acctbal[r];
+      row.nation_name = db.nation_name[static_cast<size_t>(g.nationkey)];
+      row.address = db.c_address.view(r);
+      row.phone = db.c_phone.view(r);
+      row.comment = db.c_comment.view(r);
+    }
+  });
   return rows;
 }
 
@@ -499,16 +521,18 @@ std::vector<Q18ResultRow> run_q18(const Database& db, const std::string& quantit
   int64_t n = 0;
   check(db.ctx, bo_tpch_q18(db.ctx, &t, threshold, out, db.n_orders, &n), "q18");
   std::vector<Q18ResultRow> rows(static_cast<size_t>(n));
-  for (int64_t i = 0; i < n; ++i) {
-    const auto& g = out[i];
-    auto& row = rows[i];
-    row.c_name = std::string(db.c_name.view(static_cast<size_t>(g.cust_row)));
-    row.c_custkey = g.custkey;
-    row.o_orderkey = g.orderkey;
-    row.o_orderdate_offset = g.orderdate_offset;
-    row.o_totalprice_raw = g.totalprice_raw;
-    row.sum_qty_raw = g.sum_qty_raw;
-  }
+  for_row_ranges(n, [&](int64_t lo, int64_t hi) {
+    for (int64_t i = lo; i < hi; ++i) {
+      const auto& g = out[i];
+      auto& row = rows[i];
+      row.c_name = db.c_name.view(static_cast<size_t>(g.cust_row));
+      row.c_custkey = g.custkey;
+      row.o_orderkey = g.orderkey;
+      row.o_orderdate_offset = g.orderdate_offset;
+      row.o_totalprice_raw = g.totalprice_raw;
+      row.sum_qty_raw = g.sum_qty_raw;
+    }
+  });
   return rows;
 }
 
@@ -619,7 +643,7 @@ void write_q18_csv(const Database& db, const std::string& filename, const std::v
   out.setf(std::ios::fixed);
   out << std::setprecision(2);
   for (const auto& r : rows) {
-    out << escape_csv(r.c_name) << ',' << r.c_custkey << ',' << r.o_orderkey << ','
+    out << escape_csv(std::string(r.c_name)) << ',' << r.c_custkey << ',' << r.o_orderkey << ','
         << format_date(db.base_date_days, r.o_orderdate_offset) << ','
         << static_cast<double>(r.o_totalprice_raw) / kPriceScale << ','
         << static_cast<double>(r.sum_qty_raw) / kPriceScale << "\n";

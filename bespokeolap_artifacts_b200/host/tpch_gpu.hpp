@@ -149,7 +149,7 @@ struct Q10ResultRow {
 };
 
 struct Q18ResultRow {
-  std::string c_name;
+  std::string_view c_name;
   int32_t c_custkey = 0;
   int32_t o_orderkey = 0;
   int16_t o_orderdate_offset = 0;
