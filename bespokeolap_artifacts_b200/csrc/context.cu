@@ -115,6 +115,20 @@ const char* bo_build_info(void) {
   return "bespoke_gpu: sm_100a (B200) build, nvcc " __DATE__;
 }
 
+int bo_device_init(int device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return BO_ERR_UNSUPPORTED;
+  }
+  if (device < 0 || device >= n) return BO_ERR_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess || cudaFree(nullptr) != cudaSuccess) {
+    cudaGetLastError();
+    return BO_ERR_CUDA;
+  }
+  return BO_OK;
+}
+
 int bo_create(bo_ctx** out, int device) {
   if (!out) return BO_ERR_INVALID;
   *out = nullptr;

@@ -7,14 +7,18 @@
 #include <parquet/arrow/reader.h>
 
 #include <algorithm>
+#include <array>
 #include <charconv>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <functional>
+#include <future>
 #include <iomanip>
 #include <iostream>
+#include <mutex>
 #include <numeric>
 #include <sstream>
 #include <stdexcept>
@@ -190,22 +194,36 @@ void for_each_string(const std::shared_ptr<arrow::ChunkedArray>& c, F fn) {
   }
 }
 
-// Dictionary codes in first-appearance order.
+struct ViewHash {
+  using is_transparent = void;
+  size_t operator()(std::string_view v) const { return std::hash<std::string_view>{}(v); }
+};
+
+// Dictionary codes in first-appearance order.  Lookups take the row's view
+// (no per-row string), and a run of equal values reuses the last code.
 std::vector<uint16_t> dictionary_codes(const std::shared_ptr<arrow::ChunkedArray>& c, Dictionary& dict) {
   std::vector<uint16_t> codes;
   codes.reserve(c->length());
-  std::unordered_map<std::string, uint16_t> ids;
+  std::unordered_map<std::string, uint16_t, ViewHash, std::equal_to<>> ids;
+  std::string last;
+  int32_t last_id = -1;
   for_each_string(c, [&](std::string_view sv) {
-    std::string v(sv);
-    auto it = ids.find(v);
-    if (it != ids.end()) {
-      codes.push_back(it->second);
+    if (last_id >= 0 && sv == last) {
+      codes.push_back(static_cast<uint16_t>(last_id));
       return;
     }
-    if (dict.values.size() > 0xffff) throw std::runtime_error("Dictionary column exceeds uint16_t capacity");
-    const uint16_t id = static_cast<uint16_t>(dict.values.size());
-    ids.emplace(v, id);
-    dict.values.push_back(std::move(v));
+    auto it = ids.find(sv);
+    uint16_t id;
+    if (it != ids.end()) {
+      id = it->second;
+    } else {
+      if (dict.values.size() > 0xffff) throw std::runtime_error("Dictionary column exceeds uint16_t capacity");
+      id = static_cast<uint16_t>(dict.values.size());
+      ids.emplace(std::string(sv), id);
+      dict.values.emplace_back(sv);
+    }
+    last.assign(sv);
+    last_id = id;
     codes.push_back(id);
   });
   return codes;
@@ -677,165 +695,299 @@ Database::~Database() {
 }
 
 // ---------------------------------------------------------- entry points --
+namespace {
+int device_from_env() {
+  const char* e = std::getenv("BO_DEVICE");
+  return e ? std::atoi(e) : 0;
+}
+
+// Device start-up begun by load() and awaited by build().
+std::mutex g_device_init_mu;
+std::future<int> g_device_init;
+
+void start_device_init() {
+  std::lock_guard<std::mutex> lock(g_device_init_mu);
+  if (!g_device_init.valid())
+    g_device_init = std::async(std::launch::async, [d = device_from_env()] { return bo_device_init(d); });
+}
+
+void await_device_init() {
+  std::lock_guard<std::mutex> lock(g_device_init_mu);
+  if (g_device_init.valid()) g_device_init.get();  // bo_create reports any failure itself
+}
+}  // namespace
+
 ParquetTables* load(std::string path) {
+  // The CUDA context is created on a background thread while the files are
+  // read (the eight files themselves are read concurrently).
+  start_device_init();
   auto* t = new ParquetTables{};
-  t->customer = read_parquet(path + "customer.parquet");
-  t->lineitem = read_parquet(path + "lineitem.parquet");
-  t->nation = read_parquet(path + "nation.parquet");
-  t->orders = read_parquet(path + "orders.parquet");
-  t->part = read_parquet(path + "part.parquet");
-  t->partsupp = read_parquet(path + "partsupp.parquet");
-  t->region = read_parquet(path + "region.parquet");
-  t->supplier = read_parquet(path + "supplier.parquet");
+  auto read = [&path](const char* name) {
+    return std::async(std::launch::async, [file = path + name] { return read_parquet(file); });
+  };
+  auto customer = read("customer.parquet");
+  auto lineitem = read("lineitem.parquet");
+  auto nation = read("nation.parquet");
+  auto orders = read("orders.parquet");
+  auto part = read("part.parquet");
+  auto partsupp = read("partsupp.parquet");
+  auto region = read("region.parquet");
+  auto supplier = read("supplier.parquet");
+  try {
+    t->customer = customer.get();
+    t->lineitem = lineitem.get();
+    t->nation = nation.get();
+    t->orders = orders.get();
+    t->part = part.get();
+    t->partsupp = partsupp.get();
+    t->region = region.get();
+    t->supplier = supplier.get();
+  } catch (...) {
+    delete t;
+    throw;
+  }
   return t;
 }
 
+namespace {
+
+// Host-side storage-plan columns of one table, derived before the upload.
+struct LineitemHost {
+  std::vector<int32_t> orderkey, price, dprice;
+  std::vector<int16_t> ship, q16;
+  std::vector<uint8_t> code, d8, t8;
+  Dictionary returnflag, linestatus;
+  bool orderkey_sorted = true;
+  int32_t max_orderkey = -1;
+};
+
+struct OrdersHost {
+  std::vector<int32_t> okey, ckey, prio, total, map;
+  std::vector<int16_t> odate;
+  std::vector<uint8_t> comment_bytes;
+  std::vector<uint32_t> comment_offsets;
+};
+
+struct CustomerHost {
+  std::vector<int32_t> ckey, nkey, map, acctbal;
+  std::vector<uint16_t> seg;
+  Dictionary mktsegment;
+  int32_t max_key = 0;
+  StringColumn name, address, phone, comment;
+};
+
+// lineitem: the storage-plan columns of bespoke_tpch/builder_impl.cpp:456-577.
+LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, int32_t base_days) {
+  LineitemHost h;
+  auto price = std::async(std::launch::async, [&] { return scaled_values(column(L, "l_extendedprice"), kPriceScale); });
+  auto discount = std::async(std::launch::async, [&] { return scaled_values(column(L, "l_discount"), kDiscountScale); });
+  auto tax = std::async(std::launch::async, [&] { return scaled_values(column(L, "l_tax"), kDiscountScale); });
+  auto quantity = std::async(std::launch::async, [&] { return scaled_values(column(L, "l_quantity"), kPriceScale); });
+  auto ship = std::async(std::launch::async, [&] { return date_offsets(column(L, "l_shipdate"), base_days); });
+  h.orderkey = int_values(column(L, "l_orderkey"));
+  const auto rf = dictionary_codes(column(L, "l_returnflag"), h.returnflag);
+  const auto ls = dictionary_codes(column(L, "l_linestatus"), h.linestatus);
+  const size_t n = h.orderkey.size();
+  const size_t ls_count = h.linestatus.values.size();
+  if (h.returnflag.values.size() * ls_count > 255)
+    throw std::runtime_error("Lineitem returnflag/linestatus exceeds uint8 capacity");
+  h.price = price.get();
+  const auto disc = discount.get();
+  const auto tx = tax.get();
+  const auto qty = quantity.get();
+  h.ship = ship.get();
+  h.d8.resize(n);
+  h.t8.resize(n);
+  h.code.resize(n);
+  h.q16.resize(n);
+  h.dprice.resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    h.d8[i] = static_cast<uint8_t>(disc[i]);
+    h.t8[i] = static_cast<uint8_t>(tx[i]);
+    h.q16[i] = static_cast<int16_t>(qty[i]);
+    h.dprice[i] = static_cast<int32_t>(static_cast<int64_t>(h.price[i]) * (kDiscountScale - static_cast<int32_t>(h.d8[i])) /
+                                       kDiscountScale);
+    h.code[i] = static_cast<uint8_t>(rf[i] * ls_count + ls[i]);
+  }
+  for (size_t i = 0; i < n; ++i) {  // builder_impl.cpp:569-577
+    if (i > 0 && h.orderkey[i] < h.orderkey[i - 1]) h.orderkey_sorted = false;
+    h.max_orderkey = std::max(h.max_orderkey, h.orderkey[i]);
+  }
+  return h;
+}
+
+// orders, stably sorted by orderdate, the orderkey -> row map and the comments
+// in the same order (bespoke_tpch/builder_impl.cpp:350-371, 580-642).
+OrdersHost derive_orders(const ParquetTables::ArrowTable& O, int32_t base_days) {
+  OrdersHost h;
+  auto comment_f = std::async(std::launch::async, [&] { return string_column(column(O, "o_comment")); });
+  const auto okey = int_values(column(O, "o_orderkey"));
+  const auto ckey = int_values(column(O, "o_custkey"));
+  const auto odate = date_offsets(column(O, "o_orderdate"), base_days);
+  const auto prio = int_values(column(O, "o_shippriority"));
+  const auto total = scaled_values(column(O, "o_totalprice"), kPriceScale);
+  std::vector<uint32_t> order(okey.size());
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return odate[a] < odate[b]; });
+  h.okey = permute(okey, order);
+  h.ckey = permute(ckey, order);
+  h.prio = permute(prio, order);
+  h.odate = permute(odate, order);
+  h.total = permute(total, order);
+  int32_t max_key = -1;
+  for (int32_t k : h.okey) max_key = std::max(max_key, k);
+  h.map.assign(max_key >= 0 ? static_cast<size_t>(max_key) + 1 : 0, -1);
+  for (size_t i = 0; i < h.okey.size(); ++i)
+    if (h.okey[i] >= 0 && static_cast<size_t>(h.okey[i]) < h.map.size()) h.map[static_cast<size_t>(h.okey[i])] = static_cast<int32_t>(i);
+  const StringColumn comment = comment_f.get();
+  h.comment_bytes.reserve(comment.data.size());
+  h.comment_offsets.reserve(order.size() + 1);
+  h.comment_offsets.push_back(0);
+  for (const uint32_t i : order) {
+    const auto v = comment.view(i);
+    h.comment_bytes.insert(h.comment_bytes.end(), v.begin(), v.end());
+    h.comment_offsets.push_back(static_cast<uint32_t>(h.comment_bytes.size()));
+  }
+  return h;
+}
+
+// customer: keys, market-segment codes, nationkeys, the custkey -> row map and
+// the strings of result rows (bespoke_tpch/builder_impl.cpp:670-700).
+CustomerHost derive_customer(const ParquetTables::ArrowTable& C) {
+  CustomerHost h;
+  auto strings = std::async(std::launch::async, [&] {
+    return std::array<StringColumn, 4>{string_column(column(C, "c_name")), string_column(column(C, "c_address")),
+                                       string_column(column(C, "c_phone")), string_column(column(C, "c_comment"))};
+  });
+  h.ckey = int_values(column(C, "c_custkey"));
+  h.seg = dictionary_codes(column(C, "c_mktsegment"), h.mktsegment);
+  h.nkey = int_values(column(C, "c_nationkey"));
+  h.acctbal = scaled_values(column(C, "c_acctbal"), kPriceScale);
+  for (int32_t k : h.ckey) h.max_key = std::max(h.max_key, k);
+  h.map.assign(h.ckey.empty() ? 0 : static_cast<size_t>(h.max_key) + 1, -1);
+  for (size_t i = 0; i < h.ckey.size(); ++i)
+    if (h.ckey[i] >= 0) h.map[static_cast<size_t>(h.ckey[i])] = static_cast<int32_t>(i);
+  auto s = strings.get();
+  h.name = std::move(s[0]);
+  h.address = std::move(s[1]);
+  h.phone = std::move(s[2]);
+  h.comment = std::move(s[3]);
+  return h;
+}
+
+}  // namespace
+
 Database* build(ParquetTables* tables) {
   const auto t0 = std::chrono::steady_clock::now();
+  // BO_BUILD_TRACE set: the phases' end times (ms since build() began) on stderr.
+  const bool trace = std::getenv("BO_BUILD_TRACE") != nullptr;
+  auto phase = [&](const char* name) {
+    if (trace)
+      std::cerr << "build " << name << " ms: "
+                << std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count() /
+                       1000.0
+                << "\n";
+  };
+  const int32_t base_days = static_cast<int32_t>(days_from_civil(1992, 1, 1));
+  // Each table's host derivations on its own thread (as the reference's
+  // builder runs one std::async task per table), overlapped with the
+  // device context's creation.
+  auto lineitem_f = std::async(std::launch::async, [&] { return derive_lineitem(tables->lineitem, base_days); });
+  auto orders_f = std::async(std::launch::async, [&] { return derive_orders(tables->orders, base_days); });
+  auto customer_f = std::async(std::launch::async, [&] { return derive_customer(tables->customer); });
   auto* db = new Database();
-  db->base_date_days = static_cast<int32_t>(days_from_civil(1992, 1, 1));
-  const char* dev_env = std::getenv("BO_DEVICE");
-  const int rc = bo_create(&db->ctx, dev_env ? std::atoi(dev_env) : 0);
+  db->base_date_days = base_days;
+  await_device_init();
+  const int rc = bo_create(&db->ctx, device_from_env());
   if (rc != BO_OK) {
     delete db;
     throw std::runtime_error("bo_create failed (status " + std::to_string(rc) + "): an sm_100 GPU is required");
   }
+  phase("context");
   bo_ctx* ctx = db->ctx;
-  // lineitem: the storage-plan columns of bespoke_tpch/builder_impl.cpp:456-567.
-  {
-    const auto& L = tables->lineitem;
-    const auto orderkey = int_values(column(L, "l_orderkey"));
-    const auto quantity = scaled_values(column(L, "l_quantity"), kPriceScale);
-    const auto price = scaled_values(column(L, "l_extendedprice"), kPriceScale);
-    const auto discount = scaled_values(column(L, "l_discount"), kDiscountScale);
-    const auto tax = scaled_values(column(L, "l_tax"), kDiscountScale);
-    const auto ship = date_offsets(column(L, "l_shipdate"), db->base_date_days);
-    const auto rf = dictionary_codes(column(L, "l_returnflag"), db->returnflag);
-    const auto ls = dictionary_codes(column(L, "l_linestatus"), db->linestatus);
-    const size_t n = orderkey.size();
-    const size_t ls_count = db->linestatus.values.size();
-    if (db->returnflag.values.size() * ls_count > 255)
-      throw std::runtime_error("Lineitem returnflag/linestatus exceeds uint8 capacity");
-    std::vector<uint8_t> d8(n), t8(n), code(n);
-    std::vector<int16_t> q16(n);
-    std::vector<int32_t> dprice(n);
-    for (size_t i = 0; i < n; ++i) {
-      d8[i] = static_cast<uint8_t>(discount[i]);
-      t8[i] = static_cast<uint8_t>(tax[i]);
-      q16[i] = static_cast<int16_t>(quantity[i]);
-      dprice[i] = static_cast<int32_t>(static_cast<int64_t>(price[i]) * (kDiscountScale - static_cast<int32_t>(d8[i])) /
-                                       kDiscountScale);
-      code[i] = static_cast<uint8_t>(rf[i] * ls_count + ls[i]);
+  try {
+    {
+      LineitemHost h = lineitem_f.get();
+      phase("lineitem derived");
+      db->returnflag = std::move(h.returnflag);
+      db->linestatus = std::move(h.linestatus);
+      db->n_lineitem = static_cast<int64_t>(h.orderkey.size());
+      db->lineitem_orderkey_sorted = h.orderkey_sorted;
+      db->max_lineitem_orderkey = h.max_orderkey;
+      db->l_orderkey = upload(ctx, h.orderkey);
+      db->l_shipdate = upload(ctx, h.ship);
+      db->l_returnflag_linestatus = upload(ctx, h.code);
+      db->l_extendedprice = upload(ctx, h.price);
+      db->l_discounted_price = upload(ctx, h.dprice);
+      db->l_discount = upload(ctx, h.d8);
+      db->l_tax = upload(ctx, h.t8);
+      db->l_quantity = upload(ctx, h.q16);
+      phase("lineitem uploaded");
     }
-    db->n_lineitem = static_cast<int64_t>(n);
-    for (size_t i = 0; i < n; ++i) {  // builder_impl.cpp:569-577
-      if (i > 0 && orderkey[i] < orderkey[i - 1]) db->lineitem_orderkey_sorted = false;
-      db->max_lineitem_orderkey = std::max(db->max_lineitem_orderkey, orderkey[i]);
+    {
+      OrdersHost h = orders_f.get();
+      phase("orders derived");
+      db->n_orders = static_cast<int64_t>(h.okey.size());
+      db->n_orderkey_map = static_cast<int64_t>(h.map.size());
+      db->o_orderkey = upload(ctx, h.okey);
+      db->o_custkey = upload(ctx, h.ckey);
+      db->o_orderdate = upload(ctx, h.odate);
+      db->o_shippriority = upload(ctx, h.prio);
+      db->o_totalprice = upload(ctx, h.total);
+      db->orderkey_to_row = upload(ctx, h.map);
+      db->dense_orderkeys = !h.okey.empty() && h.okey.front() == 1 && h.okey.back() == static_cast<int32_t>(h.okey.size());
+      db->o_comment = upload(ctx, h.comment_bytes);
+      db->o_comment_offsets = upload(ctx, h.comment_offsets);
+      // Per-order lineitem ranges (builder_impl.cpp:930-990), built on the device.
+      const size_t bytes = std::max<size_t>(4 * h.okey.size(), 256);
+      check(ctx, bo_device_alloc(ctx, bytes, &db->o_li_begin.ptr), "device alloc");
+      check(ctx, bo_device_alloc(ctx, bytes, &db->o_li_end.ptr), "device alloc");
+      db->o_li_begin.rows = db->o_li_end.rows = db->n_orders;
+      check(ctx,
+            bo_tpch_order_ranges(ctx, col<int32_t>(db->l_orderkey), db->n_lineitem, col<int32_t>(db->orderkey_to_row),
+                                 db->n_orderkey_map, db->n_orders, static_cast<uint32_t*>(db->o_li_begin.ptr),
+                                 static_cast<uint32_t*>(db->o_li_end.ptr)),
+            "order ranges");
+      phase("orders uploaded");
     }
-    db->l_orderkey = upload(ctx, orderkey);
-    db->l_shipdate = upload(ctx, ship);
-    db->l_returnflag_linestatus = upload(ctx, code);
-    db->l_extendedprice = upload(ctx, price);
-    db->l_discounted_price = upload(ctx, dprice);
-    db->l_discount = upload(ctx, d8);
-    db->l_tax = upload(ctx, t8);
-    db->l_quantity = upload(ctx, q16);
-  }
-  // orders, stably sorted by orderdate, and the orderkey -> row map
-  // (bespoke_tpch/builder_impl.cpp:580-642).
-  {
-    const auto& O = tables->orders;
-    const auto okey = int_values(column(O, "o_orderkey"));
-    const auto ckey = int_values(column(O, "o_custkey"));
-    const auto odate = date_offsets(column(O, "o_orderdate"), db->base_date_days);
-    const auto prio = int_values(column(O, "o_shippriority"));
-    const auto total = scaled_values(column(O, "o_totalprice"), kPriceScale);
-    const auto comment = string_column(column(O, "o_comment"));
-    std::vector<uint32_t> order(okey.size());
-    std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return odate[a] < odate[b]; });
-    const auto sk = permute(okey, order), sc = permute(ckey, order), sp = permute(prio, order);
-    const auto sd = permute(odate, order);
-    const auto st = permute(total, order);
-    int32_t max_key = -1;
-    for (int32_t k : sk) max_key = std::max(max_key, k);
-    std::vector<int32_t> map(max_key >= 0 ? static_cast<size_t>(max_key) + 1 : 0, -1);
-    for (size_t i = 0; i < sk.size(); ++i)
-      if (sk[i] >= 0 && static_cast<size_t>(sk[i]) < map.size()) map[static_cast<size_t>(sk[i])] = static_cast<int32_t>(i);
-    db->n_orders = static_cast<int64_t>(sk.size());
-    db->n_orderkey_map = static_cast<int64_t>(map.size());
-    db->o_orderkey = upload(ctx, sk);
-    db->o_custkey = upload(ctx, sc);
-    db->o_orderdate = upload(ctx, sd);
-    db->o_shippriority = upload(ctx, sp);
-    db->o_totalprice = upload(ctx, st);
-    db->orderkey_to_row = upload(ctx, map);
-    db->dense_orderkeys = !sk.empty() && sk.front() == 1 && sk.back() == static_cast<int32_t>(sk.size());
-    {  // comments in the same date order (builder_impl.cpp:350-371, 607)
-      std::vector<uint8_t> bytes;
-      bytes.reserve(comment.data.size());
-      std::vector<uint32_t> offs;
-      offs.reserve(order.size() + 1);
-      offs.push_back(0);
-      for (const uint32_t i : order) {
-        const auto v = comment.view(i);
-        bytes.insert(bytes.end(), v.begin(), v.end());
-        offs.push_back(static_cast<uint32_t>(bytes.size()));
-      }
-      db->o_comment = upload(ctx, bytes);
-      db->o_comment_offsets = upload(ctx, offs);
+    {
+      CustomerHost h = customer_f.get();
+      phase("customer derived");
+      db->n_customer = static_cast<int64_t>(h.ckey.size());
+      db->custkey_bound = h.ckey.empty() ? 0 : h.max_key + 1;
+      db->dense_custkeys = !h.ckey.empty() && h.ckey.front() == 1 && h.ckey.back() == static_cast<int32_t>(h.ckey.size());
+      db->n_custkey_map = static_cast<int64_t>(h.map.size());
+      db->mktsegment = std::move(h.mktsegment);
+      db->c_custkey = upload(ctx, h.ckey);
+      db->c_mktsegment = upload(ctx, h.seg);
+      db->c_nationkey = upload(ctx, h.nkey);
+      db->custkey_to_row = upload(ctx, h.map);
+      db->c_acctbal = std::move(h.acctbal);
+      db->c_name = std::move(h.name);
+      db->c_address = std::move(h.address);
+      db->c_phone = std::move(h.phone);
+      db->c_comment = std::move(h.comment);
+      phase("customer uploaded");
     }
-    // Per-order lineitem ranges (builder_impl.cpp:930-990), built on the device.
-    check(ctx, bo_device_alloc(ctx, std::max<size_t>(4 * sk.size(), 256), &db->o_li_begin.ptr), "device alloc");
-    check(ctx, bo_device_alloc(ctx, std::max<size_t>(4 * sk.size(), 256), &db->o_li_end.ptr), "device alloc");
-    db->o_li_begin.rows = db->o_li_end.rows = db->n_orders;
-    check(ctx,
-          bo_tpch_order_ranges(ctx, col<int32_t>(db->l_orderkey), db->n_lineitem, col<int32_t>(db->orderkey_to_row),
-                               db->n_orderkey_map, db->n_orders, static_cast<uint32_t*>(db->o_li_begin.ptr),
-                               static_cast<uint32_t*>(db->o_li_end.ptr)),
-          "order ranges");
+    // nation names by key (bespoke_tpch/builder_impl.cpp:780-803; query_q10.cpp:497-515)
+    {
+      const auto& N = tables->nation;
+      const auto key = int_values(column(N, "n_nationkey"));
+      const auto name = string_column(column(N, "n_name"));
+      int32_t max_key = 0;
+      for (int32_t k : key) max_key = std::max(max_key, k);
+      db->nation_bound = max_key + 1;
+      db->nation_name.assign(static_cast<size_t>(db->nation_bound), std::string());
+      for (size_t i = 0; i < key.size(); ++i)
+        if (key[i] >= 0) db->nation_name[static_cast<size_t>(key[i])] = std::string(name.view(i));
+    }
+    check(ctx, bo_device_alloc(ctx, sizeof(bo_q1_agg) * BO_Q1_MAX_GROUPS + 256, &db->scratch.ptr), "scratch alloc");
+    check(ctx, bo_synchronize(ctx), "build");
+  } catch (...) {
+    delete db;
+    throw;
   }
-  // customer: keys, market-segment codes, nationkeys, the custkey -> row map
-  // and the strings of result rows (bespoke_tpch/builder_impl.cpp:670-700).
-  {
-    const auto& C = tables->customer;
-    const auto ckey = int_values(column(C, "c_custkey"));
-    const auto seg = dictionary_codes(column(C, "c_mktsegment"), db->mktsegment);
-    const auto nkey = int_values(column(C, "c_nationkey"));
-    int32_t max_key = 0;
-    for (int32_t k : ckey) max_key = std::max(max_key, k);
-    db->n_customer = static_cast<int64_t>(ckey.size());
-    db->custkey_bound = ckey.empty() ? 0 : max_key + 1;
-    db->dense_custkeys =
-        !ckey.empty() && ckey.front() == 1 && ckey.back() == static_cast<int32_t>(ckey.size());
-    std::vector<int32_t> map(ckey.empty() ? 0 : static_cast<size_t>(max_key) + 1, -1);
-    for (size_t i = 0; i < ckey.size(); ++i)
-      if (ckey[i] >= 0) map[static_cast<size_t>(ckey[i])] = static_cast<int32_t>(i);
-    db->n_custkey_map = static_cast<int64_t>(map.size());
-    db->c_custkey = upload(ctx, ckey);
-    db->c_mktsegment = upload(ctx, seg);
-    db->c_nationkey = upload(ctx, nkey);
-    db->custkey_to_row = upload(ctx, map);
-    db->c_acctbal = scaled_values(column(C, "c_acctbal"), kPriceScale);
-    db->c_name = string_column(column(C, "c_name"));
-    db->c_address = string_column(column(C, "c_address"));
-    db->c_phone = string_column(column(C, "c_phone"));
-    db->c_comment = string_column(column(C, "c_comment"));
-  }
-  // nation names by key (bespoke_tpch/builder_impl.cpp:780-803; query_q10.cpp:497-515)
-  {
-    const auto& N = tables->nation;
-    const auto key = int_values(column(N, "n_nationkey"));
-    const auto name = string_column(column(N, "n_name"));
-    int32_t max_key = 0;
-    for (int32_t k : key) max_key = std::max(max_key, k);
-    db->nation_bound = max_key + 1;
-    db->nation_name.assign(static_cast<size_t>(db->nation_bound), std::string());
-    for (size_t i = 0; i < key.size(); ++i)
-      if (key[i] >= 0) db->nation_name[static_cast<size_t>(key[i])] = std::string(name.view(i));
-  }
-  check(ctx, bo_device_alloc(ctx, sizeof(bo_q1_agg) * BO_Q1_MAX_GROUPS + 256, &db->scratch.ptr), "scratch alloc");
-  check(ctx, bo_synchronize(ctx), "build");
+  phase("done");
   const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
   std::cout << "Build ms: " << ms << "\n";
   return db;

@@ -258,6 +258,7 @@ class Sketch(C.Structure):
 _P = C.c_void_p
 _SIGNATURES = {
     "bo_create": (C.c_int, [C.POINTER(_P), C.c_int]),
+    "bo_device_init": (C.c_int, [C.c_int]),
     "bo_destroy": (None, [_P]),
     "bo_last_error": (C.c_char_p, [_P]),
     "bo_set_stream": (C.c_int, [_P, _P]),

@@ -54,6 +54,12 @@ typedef struct bo_i128 {
 /* Replaces the process-level set-up the reference's external driver does
  * before query() (bespoke_tpch/query_impl.cpp:142-143: pin to one core). */
 int bo_create(bo_ctx** out, int device);
+/* Creates the CUDA primary context of `device` -- the cost the first
+ * bo_create on it otherwise pays (driver start-up and context creation, on
+ * the order of a second) -- and nothing else.  Any thread, any number of
+ * times.  No reference counterpart: the drop-in's load() calls it on a
+ * background thread so that this start-up overlaps the Parquet reads. */
+int bo_device_init(int device);
 void bo_destroy(bo_ctx* ctx);
 const char* bo_last_error(const bo_ctx* ctx);
 /* Use an external CUDA stream (cudaStream_t passed as void*); NULL restores the

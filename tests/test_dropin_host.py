@@ -32,4 +32,4 @@ def test_exports_reference_entry_points():
 def test_loader_reads_the_reference_file_names():
     src = (ROOT / "bespokeolap_artifacts_b200" / "host" / "tpch_gpu.cpp").read_text()
     for t in ("customer", "lineitem", "nation", "orders", "part", "partsupp", "region", "supplier"):
-        assert f'path + "{t}.parquet"' in src
+        assert f'"{t}.parquet"' in src
