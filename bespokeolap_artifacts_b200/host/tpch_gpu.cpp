@@ -494,6 +494,56 @@ std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date) {
   return rows;
 }
 
+std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
+                                  const std::string& date) {
+  // query_q12.cpp:171-213: the window [DATE, DATE + 12 months), the two ship
+  // modes' codes (the second only when it names another value) and the codes
+  // of the two high priorities.
+  const int16_t start = date_offset_of(date, db.base_date_days);
+  const int16_t end = date_offset_of(date, db.base_date_days, 12);
+  int32_t code1 = -1, code2 = -1;
+  for (size_t c = 0; c < db.shipmode.values.size(); ++c) {
+    if (db.shipmode.values[c] == shipmode1)
+      code1 = static_cast<int32_t>(c);
+    else if (db.shipmode.values[c] == shipmode2)
+      code2 = static_cast<int32_t>(c);
+  }
+  if (code1 < 0 && code2 < 0) return {};
+  int32_t high1 = -1, high2 = -1;
+  for (size_t c = 0; c < db.orderpriority.values.size(); ++c) {
+    if (db.orderpriority.values[c] == "1-URGENT")
+      high1 = static_cast<int32_t>(c);
+    else if (db.orderpriority.values[c] == "2-HIGH")
+      high2 = static_cast<int32_t>(c);
+  }
+  bo_tpch_q12_tables t{};
+  t.l_shipmode = col<uint16_t>(db.l_shipmode);
+  t.l_commit_receipt = col<uint32_t>(db.l_commit_receipt);
+  t.l_shipdate = col<int16_t>(db.l_shipdate);
+  t.l_orderkey = col<int32_t>(db.l_orderkey);
+  t.l_shard_max_shipdate = db.l_shard_max_shipdate.ptr ? col<int16_t>(db.l_shard_max_shipdate) : nullptr;
+  t.n_lineitem = db.n_lineitem;
+  t.orderkey_to_row = col<int32_t>(db.orderkey_to_row);
+  t.n_orderkey_map = db.n_orderkey_map;
+  t.o_orderpriority = col<uint16_t>(db.o_orderpriority);
+  t.n_orders = db.n_orders;
+  int64_t counts[4] = {0, 0, 0, 0};
+  check(db.ctx, bo_tpch_q12(db.ctx, &t, code1, code2, high1, high2, start, end, counts), "q12");
+  // Groups in code order, empty ones dropped, then by shipmode (:321-352).
+  std::vector<Q12ResultRow> rows;
+  for (size_t c = 0; c < db.shipmode.values.size(); ++c) {
+    const int32_t code = static_cast<int32_t>(c);
+    if (code != code1 && code != code2) continue;
+    const int64_t high = code == code1 ? counts[0] : counts[2];
+    const int64_t low = code == code1 ? counts[1] : counts[3];
+    if (high == 0 && low == 0) continue;
+    rows.push_back(Q12ResultRow{db.shipmode.values[c], high, low});
+  }
+  std::sort(rows.begin(), rows.end(),
+            [](const Q12ResultRow& a, const Q12ResultRow& b) { return a.shipmode < b.shipmode; });
+  return rows;
+}
+
 std::vector<Q13ResultRow> run_q13(const Database& db, const std::string& word1, const std::string& word2) {
   bo_tpch_q13_tables t{};
   t.o_comment = col<uint8_t>(db.o_comment);
@@ -649,6 +699,12 @@ void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>&
   out.write(buf.data(), static_cast<std::streamsize>(buf.size()));
 }
 
+void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q12.cpp:362-368
+  out << "l_shipmode,high_line_count,low_line_count\n";
+  for (const auto& r : rows) out << escape_csv(r.shipmode) << ',' << r.high_line_count << ',' << r.low_line_count << "\n";
+}
+
 void write_q13_csv(const std::string& filename, const std::vector<Q13ResultRow>& rows) {
   std::ofstream out(filename);
   out << "c_count,custdist\n";
@@ -686,8 +742,8 @@ Database::~Database() {
   DeviceColumn* cols[] = {&l_orderkey, &l_shipdate, &l_returnflag_linestatus, &l_extendedprice, &l_discounted_price,
                           &l_discount, &l_tax, &l_quantity, &o_orderkey, &o_custkey, &o_orderdate,
                           &o_shippriority, &o_totalprice, &orderkey_to_row, &o_li_begin, &o_li_end,
-                          &o_comment, &o_comment_offsets,
-                          &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
+                          &o_comment, &o_comment_offsets, &o_orderpriority, &l_shipmode, &l_commit_receipt,
+                          &l_shard_max_shipdate, &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
   if (result_host) bo_host_free_pinned(ctx, result_host);
@@ -754,15 +810,19 @@ namespace {
 // Host-side storage-plan columns of one table, derived before the upload.
 struct LineitemHost {
   std::vector<int32_t> orderkey, price, dprice;
-  std::vector<int16_t> ship, q16;
+  std::vector<int16_t> ship, q16, shard_max_ship;
   std::vector<uint8_t> code, d8, t8;
-  Dictionary returnflag, linestatus;
+  std::vector<uint16_t> shipmode;
+  std::vector<uint32_t> commit_receipt;
+  Dictionary returnflag, linestatus, shipmode_dict;
   bool orderkey_sorted = true;
   int32_t max_orderkey = -1;
 };
 
 struct OrdersHost {
   std::vector<int32_t> okey, ckey, prio, total, map;
+  std::vector<uint16_t> priority;
+  Dictionary priority_dict;
   std::vector<int16_t> odate;
   std::vector<uint8_t> comment_bytes;
   std::vector<uint32_t> comment_offsets;
@@ -777,8 +837,65 @@ struct CustomerHost {
 };
 
 // lineitem: the storage-plan columns of bespoke_tpch/builder_impl.cpp:456-577.
-LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, int32_t base_days) {
+// Latest shipdate of each lineitem's builder shard (bespoke_tpch/builder_impl.cpp:838-911):
+// shards group lineitems by (ship year-month, discount, quantity / 100,
+// supplier nation), the nation through supplier's nationkey_by_suppkey
+// (:719-742).  Keys and buckets are formed by the builder's own expressions.
+std::vector<int16_t> shard_max_shipdates(const LineitemHost& h, const ParquetTables::ArrowTable& L,
+                                         const ParquetTables::ArrowTable& S, int32_t base_days) {
+  const auto suppkey = int_values(column(L, "l_suppkey"));
+  const auto s_key = int_values(column(S, "s_suppkey"));
+  const auto s_nation = int_values(column(S, "s_nationkey"));
+  int32_t max_suppkey = -1;
+  for (int32_t k : s_key) max_suppkey = std::max(max_suppkey, k);
+  std::vector<int16_t> nation_by_key(max_suppkey >= 0 ? static_cast<size_t>(max_suppkey) + 1 : 0, int16_t(-1));
+  for (size_t i = 0; i < s_key.size(); ++i)
+    if (s_key[i] >= 0 && static_cast<size_t>(s_key[i]) < nation_by_key.size())
+      nation_by_key[static_cast<size_t>(s_key[i])] = static_cast<int16_t>(s_nation[i]);
+  const size_t n = h.ship.size();
+  std::vector<int64_t> keys(n);
+  std::unordered_map<int64_t, int16_t> shard_max;
+  for (size_t i = 0; i < n; ++i) {
+    int y = 0;
+    unsigned m = 0, d = 0;
+    civil_from_days(base_days + h.ship[i], y, m, d);
+    int16_t supp_nation = -1;
+    if (suppkey[i] >= 0 && static_cast<size_t>(suppkey[i]) < nation_by_key.size())
+      supp_nation = nation_by_key[static_cast<size_t>(suppkey[i])];
+    const int32_t discount_bucket = static_cast<int32_t>(h.d8[i]);
+    const int32_t quantity_bucket = static_cast<int32_t>(h.q16[i]) / 100;
+    const int32_t month_index = y * 12 + (static_cast<int32_t>(m) - 1);
+    const uint8_t supp_bucket = static_cast<uint8_t>(supp_nation >= 0 ? supp_nation : 255);
+    keys[i] = (static_cast<int64_t>(month_index) << 24) | (static_cast<int64_t>(discount_bucket) << 16) |
+              (static_cast<int64_t>(quantity_bucket) << 8) | static_cast<int64_t>(supp_bucket);
+    auto it = shard_max.find(keys[i]);
+    if (it == shard_max.end())
+      shard_max.emplace(keys[i], h.ship[i]);
+    else
+      it->second = std::max(it->second, h.ship[i]);
+  }
+  std::vector<int16_t> out(n);
+  for (size_t i = 0; i < n; ++i) out[i] = shard_max.find(keys[i])->second;
+  return out;
+}
+
+LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, const ParquetTables::ArrowTable& S,
+                             int32_t base_days) {
   LineitemHost h;
+  auto commit_receipt = std::async(std::launch::async, [&] {
+    const auto commit = date_offsets(column(L, "l_commitdate"), base_days);
+    const auto receipt = date_offsets(column(L, "l_receiptdate"), base_days);
+    std::vector<uint32_t> packed(commit.size());  // builder_impl.cpp:534-544
+    for (size_t i = 0; i < commit.size(); ++i)
+      packed[i] = (static_cast<uint32_t>(static_cast<uint16_t>(receipt[i])) << 16) |
+                  static_cast<uint32_t>(static_cast<uint16_t>(commit[i]));
+    return packed;
+  });
+  auto shipmode = std::async(std::launch::async, [&] {
+    Dictionary dict;
+    auto codes = dictionary_codes(column(L, "l_shipmode"), dict);
+    return std::make_pair(std::move(codes), std::move(dict));
+  });
   auto price = std::async(std::launch::async, [&] { return scaled_values(column(L, "l_extendedprice"), kPriceScale); });
   auto discount = std::async(std::launch::async, [&] { return scaled_values(column(L, "l_discount"), kDiscountScale); });
   auto tax = std::async(std::launch::async, [&] { return scaled_values(column(L, "l_tax"), kDiscountScale); });
@@ -813,6 +930,16 @@ LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, int32_t base_da
     if (i > 0 && h.orderkey[i] < h.orderkey[i - 1]) h.orderkey_sorted = false;
     h.max_orderkey = std::max(h.max_orderkey, h.orderkey[i]);
   }
+  h.commit_receipt = commit_receipt.get();
+  auto sm = shipmode.get();
+  h.shipmode = std::move(sm.first);
+  h.shipmode_dict = std::move(sm.second);
+  // Q12's shard pruning can only drop a lineitem received more than 30 days
+  // after shipping; without one the per-shard maxima are not needed.
+  bool late = false;
+  for (size_t i = 0; i < n && !late; ++i)
+    late = static_cast<int32_t>(static_cast<int16_t>(h.commit_receipt[i] >> 16)) - static_cast<int32_t>(h.ship[i]) > 30;
+  if (late) h.shard_max_ship = shard_max_shipdates(h, L, S, base_days);
   return h;
 }
 
@@ -826,6 +953,7 @@ OrdersHost derive_orders(const ParquetTables::ArrowTable& O, int32_t base_days) 
   const auto odate = date_offsets(column(O, "o_orderdate"), base_days);
   const auto prio = int_values(column(O, "o_shippriority"));
   const auto total = scaled_values(column(O, "o_totalprice"), kPriceScale);
+  const auto priority = dictionary_codes(column(O, "o_orderpriority"), h.priority_dict);
   std::vector<uint32_t> order(okey.size());
   std::iota(order.begin(), order.end(), 0u);
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return odate[a] < odate[b]; });
@@ -834,6 +962,7 @@ OrdersHost derive_orders(const ParquetTables::ArrowTable& O, int32_t base_days) 
   h.prio = permute(prio, order);
   h.odate = permute(odate, order);
   h.total = permute(total, order);
+  h.priority = permute(priority, order);
   int32_t max_key = -1;
   for (int32_t k : h.okey) max_key = std::max(max_key, k);
   h.map.assign(max_key >= 0 ? static_cast<size_t>(max_key) + 1 : 0, -1);
@@ -892,7 +1021,7 @@ Database* build(ParquetTables* tables) {
   // Each table's host derivations on its own thread (as the reference's
   // builder runs one std::async task per table), overlapped with the
   // device context's creation.
-  auto lineitem_f = std::async(std::launch::async, [&] { return derive_lineitem(tables->lineitem, base_days); });
+  auto lineitem_f = std::async(std::launch::async, [&] { return derive_lineitem(tables->lineitem, tables->supplier, base_days); });
   auto orders_f = std::async(std::launch::async, [&] { return derive_orders(tables->orders, base_days); });
   auto customer_f = std::async(std::launch::async, [&] { return derive_customer(tables->customer); });
   auto* db = new Database();
@@ -922,6 +1051,10 @@ Database* build(ParquetTables* tables) {
       db->l_discount = upload(ctx, h.d8);
       db->l_tax = upload(ctx, h.t8);
       db->l_quantity = upload(ctx, h.q16);
+      db->shipmode = std::move(h.shipmode_dict);
+      db->l_shipmode = upload(ctx, h.shipmode);
+      db->l_commit_receipt = upload(ctx, h.commit_receipt);
+      if (!h.shard_max_ship.empty()) db->l_shard_max_shipdate = upload(ctx, h.shard_max_ship);
       phase("lineitem uploaded");
     }
     {
@@ -934,6 +1067,8 @@ Database* build(ParquetTables* tables) {
       db->o_orderdate = upload(ctx, h.odate);
       db->o_shippriority = upload(ctx, h.prio);
       db->o_totalprice = upload(ctx, h.total);
+      db->orderpriority = std::move(h.priority_dict);
+      db->o_orderpriority = upload(ctx, h.priority);
       db->orderkey_to_row = upload(ctx, h.map);
       db->dense_orderkeys = !h.okey.empty() && h.okey.front() == 1 && h.okey.back() == static_cast<int32_t>(h.okey.size());
       db->o_comment = upload(ctx, h.comment_bytes);
@@ -1047,6 +1182,14 @@ void query(Database* db) {
       const auto rows = run_q10(*db, date);
       const auto end = std::chrono::steady_clock::now();
       write_q10_csv(file, rows);
+      report(end);
+    } else if (r.id == "12") {
+      const std::string mode1 = arg("SHIPMODE1");
+      const std::string mode2 = arg("SHIPMODE2");
+      const std::string date = arg("DATE");
+      const auto rows = run_q12(*db, mode1, mode2, date);
+      const auto end = std::chrono::steady_clock::now();
+      write_q12_csv(file, rows);
       report(end);
     } else if (r.id == "13") {
       const std::string word1 = arg("WORD1");

@@ -71,14 +71,18 @@ struct Database {
   // lineitem (row order of the input)
   int64_t n_lineitem = 0;
   bo_tpch::DeviceColumn l_orderkey, l_shipdate, l_returnflag_linestatus, l_extendedprice, l_discounted_price,
-      l_discount, l_tax, l_quantity;
-  bo_tpch::Dictionary returnflag, linestatus;
+      l_discount, l_tax, l_quantity, l_shipmode, l_commit_receipt;
+  // Latest shipdate of each lineitem's builder shard; only built when some
+  // lineitem is received more than 30 days after shipping (Q12's shard pruning).
+  bo_tpch::DeviceColumn l_shard_max_shipdate;
+  bo_tpch::Dictionary returnflag, linestatus, shipmode;
   bool lineitem_orderkey_sorted = true;
   int32_t max_lineitem_orderkey = -1;
   // orders, sorted by orderdate (stable); each row's lineitem range
   int64_t n_orders = 0;
   bo_tpch::DeviceColumn o_orderkey, o_custkey, o_orderdate, o_shippriority, o_totalprice, orderkey_to_row,
-      o_li_begin, o_li_end, o_comment, o_comment_offsets;
+      o_li_begin, o_li_end, o_comment, o_comment_offsets, o_orderpriority;
+  bo_tpch::Dictionary orderpriority;
   int64_t n_orderkey_map = 0;
   bool dense_orderkeys = false;  // first orderkey 1, last n_orders (date order)
   // customer; custkey_to_row keeps the last row of each custkey >= 0
@@ -132,6 +136,12 @@ struct Q6ResultRow {
   int64_t revenue_raw = 0;
 };
 
+struct Q12ResultRow {
+  std::string shipmode;
+  int64_t high_line_count = 0;
+  int64_t low_line_count = 0;
+};
+
 struct Q13ResultRow {
   int64_t c_count = 0;
   int64_t custdist = 0;
@@ -170,6 +180,8 @@ std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, 
 std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, const std::string& discount,
                                 const std::string& quantity);
 std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date);
+std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
+                                  const std::string& date);
 std::vector<Q13ResultRow> run_q13(const Database& db, const std::string& word1, const std::string& word2);
 std::vector<Q18ResultRow> run_q18(const Database& db, const std::string& quantity);
 
@@ -177,6 +189,7 @@ void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& r
 void write_q3_csv(const Database& db, const std::string& filename, const std::vector<Q3ResultRow>& rows);
 void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& rows);
 void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows);
+void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);
 void write_q13_csv(const std::string& filename, const std::vector<Q13ResultRow>& rows);
 void write_q18_csv(const Database& db, const std::string& filename, const std::vector<Q18ResultRow>& rows);
 

@@ -215,6 +215,15 @@ class TpchQ18Row(C.Structure):
                 ("pad0", C.c_int16), ("pad1", C.c_int32)]
 
 
+class TpchQ12Tables(C.Structure):
+    """``bo_tpch_q12_tables``: lineitem ship modes, packed commit / receipt dates, shipdates, orderkeys,
+    optional shard maxima; orders map and priorities."""
+    _fields_ = [("l_shipmode", C.c_void_p), ("l_commit_receipt", C.c_void_p), ("l_shipdate", C.c_void_p),
+                ("l_orderkey", C.c_void_p), ("l_shard_max_shipdate", C.c_void_p), ("n_lineitem", C.c_int64),
+                ("orderkey_to_row", C.c_void_p), ("n_orderkey_map", C.c_int64), ("o_orderpriority", C.c_void_p),
+                ("n_orders", C.c_int64)]
+
+
 class TpchQ13Tables(C.Structure):
     """``bo_tpch_q13_tables``: order comments (bytes + offsets), custkeys, customer keys."""
     _fields_ = [("o_comment", C.c_void_p), ("o_comment_offsets", C.c_void_p), ("o_custkey", C.c_void_p),
@@ -319,6 +328,8 @@ _SIGNATURES = {
     "bo_tpch_order_ranges": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, C.c_int64, _P, _P]),
     "bo_tpch_q10": (C.c_int, [_P, C.POINTER(TpchQ10Tables), C.c_int16, C.c_int16, C.c_int32, C.c_int32,
                               C.POINTER(TpchQ10Row), C.c_int64, C.POINTER(C.c_int64)]),
+    "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,
+                              C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q13": (C.c_int, [_P, C.POINTER(TpchQ13Tables), C.c_char_p, C.c_int64, C.c_char_p, C.c_int64,
                               C.POINTER(TpchQ13Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q18": (C.c_int, [_P, C.POINTER(TpchQ18Tables), C.c_int32, C.POINTER(TpchQ18Row), C.c_int64,

@@ -19,6 +19,13 @@ Key layouts (they select the reference's code paths):
                 shuffled, the last rows repeating earlier keys, and orders
                 that name keys without a customer.
   shuffle_lineitem  lineitems in random order instead of by orderkey.
+  late_receipts     receipt dates up to 60 days after shipping (TPC-H's are
+                    at most 30), which the reference's Q12 shard pruning
+                    notices.
+Ship modes MODE_A..MODE_G; order priorities 1-URGENT and 2-HIGH (the two the
+reference's Q12 counts as high) and three others.  Commit dates 30..90 days
+after the order, receipts 1..30 days after shipping.  These columns come from
+a second seeded stream, so the other columns do not depend on them.
 The nation table has keys 0..24 except 7; customers' nationkeys run 0..26.
 """
 from __future__ import annotations
@@ -31,6 +38,8 @@ import pyarrow.parquet as pq
 
 SEGMENTS = ["SEG_A", "SEG_B", "SEG_C", "SEG_D", "SEG_E"]
 WORDS = ["ironic", "quick", "pending", "bold", 'say "hi"', "a,b", "deposits", "", "x\"y", "final"]
+SHIPMODES = ["MODE_A", "MODE_B", "MODE_C", "MODE_D", "MODE_E", "MODE_F", "MODE_G"]
+PRIORITIES = ["1-URGENT", "2-HIGH", "3-PRIO_C", "4-PRIO_D", "5-PRIO_E"]
 D1992 = 8035  # 1992-01-01 in days since 1970-01-01
 
 
@@ -54,8 +63,9 @@ def _ragged_text(rng, n: int, max_words: int) -> list[str]:
 
 def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: int = 0,
                decimal: bool = False, order_keys: str = "sparse", customer_keys: str = "dense",
-               shuffle_lineitem: bool = False) -> Path:
+               shuffle_lineitem: bool = False, late_receipts: bool = False) -> Path:
     rng = np.random.default_rng(seed)
+    rng2 = np.random.default_rng([seed, 12])
     out.mkdir(parents=True, exist_ok=True)
     if customer_keys == "dense":
         custkey = np.arange(1, n_customer + 1, dtype=np.int32)
@@ -91,7 +101,8 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
     pq.write_table(pa.table({
         "o_orderkey": orderkey, "o_custkey": o_cust, "o_orderstatus": ["O"] * n_orders,
         "o_totalprice": _dec(rng.integers(100000, 50000000, n_orders) / 100.0, decimal),
-        "o_orderdate": pa.array(o_date, pa.date32()), "o_orderpriority": ["1-URGENT"] * n_orders,
+        "o_orderdate": pa.array(o_date, pa.date32()),
+        "o_orderpriority": [PRIORITIES[i] for i in rng2.integers(0, len(PRIORITIES), n_orders)],
         "o_clerk": ["Clerk#000000001"] * n_orders, "o_shippriority": np.zeros(n_orders, np.int32),
         "o_comment": _ragged_text(rng, n_orders, 8),
     }), out / "orders.parquet")
@@ -104,9 +115,13 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
     ship = ld + rng.integers(1, 122, n)
     rf = np.where(ship <= D1992 + 1267, np.array(["R", "A"])[rng.integers(0, 2, n)], "N")  # before / after 1995-06-17
     ls = np.where(ship > D1992 + 1267, "O", "F")
+    commit = ld + rng2.integers(30, 91, n)
+    receipt = ship + rng2.integers(1, 61 if late_receipts else 31, n)
+    mode = rng2.integers(0, len(SHIPMODES), n)
     if shuffle_lineitem:
         perm = rng.permutation(n)
-        lk, ld, qty, price, ship, rf, ls = (a[perm] for a in (lk, ld, qty, price, ship, rf, ls))
+        lk, ld, qty, price, ship, rf, ls, commit, receipt, mode = (
+            a[perm] for a in (lk, ld, qty, price, ship, rf, ls, commit, receipt, mode))
     pq.write_table(pa.table({
         "l_orderkey": lk, "l_partkey": rng.integers(1, 200, n).astype(np.int32),
         "l_suppkey": rng.integers(1, 10, n).astype(np.int32), "l_linenumber": np.ones(n, np.int32),
@@ -114,9 +129,10 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
         "l_discount": _dec(rng.integers(0, 11, n) / 100.0, decimal), "l_tax": _dec(rng.integers(0, 9, n) / 100.0, decimal),
         "l_returnflag": rf.tolist(), "l_linestatus": ls.tolist(),
         "l_shipdate": pa.array(ship.astype(np.int32), pa.date32()),
-        "l_commitdate": pa.array((ld + 30).astype(np.int32), pa.date32()),
-        "l_receiptdate": pa.array((ship + 5).astype(np.int32), pa.date32()),
-        "l_shipinstruct": ["DELIVER IN PERSON"] * n, "l_shipmode": ["TRUCK"] * n, "l_comment": [""] * n,
+        "l_commitdate": pa.array(commit.astype(np.int32), pa.date32()),
+        "l_receiptdate": pa.array(receipt.astype(np.int32), pa.date32()),
+        "l_shipinstruct": ["DELIVER IN PERSON"] * n, "l_shipmode": [SHIPMODES[i] for i in mode],
+        "l_comment": [""] * n,
     }), out / "lineitem.parquet")
     one = np.ones(1, np.int32)
     pq.write_table(pa.table({"p_partkey": one, "p_name": ["p"], "p_mfgr": ["m"], "p_brand": ["b"], "p_type": ["t"],

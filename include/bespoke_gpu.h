@@ -600,6 +600,35 @@ typedef struct bo_tpch_q13_row {      /* Q13ResultRow (bespoke_tpch/query_q13.hp
 int bo_tpch_q13(bo_ctx* ctx, const bo_tpch_q13_tables* tables, const char* word1, int64_t len1, const char* word2,
                 int64_t len2, bo_tpch_q13_row* out_host, int64_t max_rows, int64_t* n_rows);
 
+/* TPC-H Q12 over the storage-plan layout: run_q12 of
+ * bespoke_tpch/query_q12.cpp:162-360.  Lineitems whose shipmode code is
+ * mode_code1 or mode_code2 (-1: none), with shipdate < commitdate <
+ * receiptdate and receiptdate in [start_offset, end_offset), joined to their
+ * order through orderkey_to_row and counted by shipmode as high (order
+ * priority code high_code1 or high_code2) or low.  l_shard_max_shipdate, when
+ * given, is the latest shipdate of each lineitem's builder shard
+ * (builder_impl.cpp:855-911); a lineitem whose shard ends more than 30 days
+ * before start_offset is skipped, as the reference's sharded scan skips the
+ * whole shard (:265-270).  NULL when no lineitem is received more than 30
+ * days after shipping, where that pruning removes nothing.
+ * counts_out[0..1] = high / low of mode_code1, [2..3] of mode_code2. */
+typedef struct bo_tpch_q12_tables {
+  const uint16_t* l_shipmode;          /* dictionary codes */
+  const uint32_t* l_commit_receipt;    /* (uint16)receipt << 16 | (uint16)commit, int16 day offsets */
+  const int16_t* l_shipdate;
+  const int32_t* l_orderkey;
+  const int16_t* l_shard_max_shipdate; /* optional (NULL) */
+  int64_t n_lineitem;
+  const int32_t* orderkey_to_row;
+  int64_t n_orderkey_map;
+  const uint16_t* o_orderpriority;     /* dictionary codes, orders row order */
+  int64_t n_orders;
+} bo_tpch_q12_tables;
+
+int bo_tpch_q12(bo_ctx* ctx, const bo_tpch_q12_tables* tables, int32_t mode_code1, int32_t mode_code2,
+                int32_t high_code1, int32_t high_code2, int16_t start_offset, int16_t end_offset,
+                int64_t counts_out[4]);
+
 /* ================================================================= BATCH ==
  * Many pipelines of uneven sizes in ONE persistent kernel fed by a device work
  * queue of (instance, stage, tile) items, captured in a CUDA graph.  Stages of

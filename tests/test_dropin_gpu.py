@@ -2,12 +2,13 @@
 query (bespokeolap_artifacts_b200/host) and the reference's own load / build /
 query (compiled unchanged into oracle/_ref/ref_tpch_driver) read the same
 Parquet files and the same stdin requests; their result<idx>.csv files must
-agree: Q1, Q6, Q10, Q13 and Q18 byte for byte, Q3 row for row (the reference's
+agree: Q1, Q6, Q10, Q12, Q13 and Q18 byte for byte, Q3 row for row (the reference's
 std::sort leaves rows equal in revenue and orderdate in unspecified order;
 the GPU emits them in orderkey order).  The key layouts select each of the
 reference's paths: dense and sparse orderkeys (Q18's two scans), dense,
 partly shuffled and sparse custkeys (its customer lookups), lineitems sorted
-by orderkey or not (Q10's two range loops)."""
+by orderkey or not (Q10's two range loops), receipts within 30 days of
+shipping or later (Q12's shard pruning drops some of the later ones)."""
 import csv
 import re
 import subprocess
@@ -29,17 +30,19 @@ REQUESTS = [
     '6 "1994-02-01" "0.07" "23"', '6 "1996-02-29" "0.05" "25"', '6 "1992-01-01" "0.10" "50"',
     '10 "1993-10-01"', '10 "1995-01-31"', '10 "1992-11-30"', '10 "1998-07-01"', '10 "1999-01-01"',
     '18 "250"', '18 "150.5"', '18 "0"', '18 "-1"', '18 "400"', '18 "<<NULL>>"',
+    '12 "MODE_A" "MODE_C" "1994-01-01"', '12 "MODE_B" "MODE_B" "1995-06-30"', '12 "NOSUCH" "MODE_D" "1993-03-01"',
+    '12 "X" "Y" "1994-01-01"', '12 "MODE_G" "MODE_E" "1998-12-01"', '12 "MODE_F" "MODE_A" "1992-02-29"',
     '13 "pending" "deposits"', '13 "quick" "quick"', '13 "" ""', '13 "bold" ""', '13 "" "final"',
     '13 "x\\"y" "a,b"', '13 "ironic quick pending bold deposits final final" "x"', '13 "zzz" "ironic"',
 ]
 
-LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem)
-    (4, False, "sparse", "dense", False),
-    (3, True, "sparse", "dense", False),
-    (5, False, "dense", "inner", False),
-    (6, False, "dense", "sparse", False),
-    (7, False, "sparse", "sparse", True),
-    (8, False, "dense", "dense", True),
+LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem, late_receipts)
+    (4, False, "sparse", "dense", False, False),
+    (3, True, "sparse", "dense", False, False),
+    (5, False, "dense", "inner", False, True),
+    (6, False, "dense", "sparse", False, False),
+    (7, False, "sparse", "sparse", True, True),
+    (8, False, "dense", "dense", True, False),
 ]
 
 
@@ -60,9 +63,9 @@ def q3_rows(path: Path):
 def test_dropin_matches_reference_driver(tmp_path, layout):
     if not REF_DRIVER.exists() or not GPU_DRIVER.exists():
         pytest.skip("drivers not built")
-    seed, decimal, order_keys, customer_keys, shuffle = layout
+    seed, decimal, order_keys, customer_keys, shuffle, late = layout
     data = write_tpch(tmp_path / "data", seed=seed, decimal=decimal, order_keys=order_keys,
-                      customer_keys=customer_keys, shuffle_lineitem=shuffle)
+                      customer_keys=customer_keys, shuffle_lineitem=shuffle, late_receipts=late)
     out_gpu = run(GPU_DRIVER, data, tmp_path / "gpu", REQUESTS)
     out_ref = run(REF_DRIVER, data, tmp_path / "ref", REQUESTS)
     for out in (out_gpu, out_ref):
