@@ -494,6 +494,33 @@ std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date) {
   return rows;
 }
 
+std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date) {
+  // query_q4.cpp:179-181: the window [DATE, DATE + 3 months).
+  const int16_t start = date_offset_of(date, db.base_date_days);
+  const int16_t end = date_offset_of(date, db.base_date_days, 3);
+  bo_tpch_q4_tables t{};
+  t.o_orderkey = col<int32_t>(db.o_orderkey);
+  t.o_orderdate = col<int16_t>(db.o_orderdate);
+  t.o_orderpriority = col<uint16_t>(db.o_orderpriority);
+  t.o_li_begin = col<uint32_t>(db.o_li_begin);
+  t.o_li_end = col<uint32_t>(db.o_li_end);
+  t.n_orders = db.n_orders;
+  t.l_orderkey = col<int32_t>(db.l_orderkey);
+  t.l_commit_receipt = col<uint32_t>(db.l_commit_receipt);
+  t.n_lineitem = db.n_lineitem;
+  t.lineitem_orderkey_sorted = db.lineitem_orderkey_sorted ? 1 : 0;
+  t.n_priorities = static_cast<int32_t>(db.orderpriority.values.size());
+  std::vector<int64_t> counts(db.orderpriority.values.size(), 0);
+  check(db.ctx, bo_tpch_q4(db.ctx, &t, start, end, counts.data()), "q4");
+  // Non-empty priorities in code order, then by name (:321-346).
+  std::vector<Q4ResultRow> rows;
+  for (size_t c = 0; c < counts.size(); ++c)
+    if (counts[c] != 0) rows.push_back(Q4ResultRow{db.orderpriority.values[c], counts[c]});
+  std::sort(rows.begin(), rows.end(),
+            [](const Q4ResultRow& a, const Q4ResultRow& b) { return a.orderpriority < b.orderpriority; });
+  return rows;
+}
+
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
                                   const std::string& date) {
   // query_q12.cpp:171-213: the window [DATE, DATE + 12 months), the two ship
@@ -697,6 +724,12 @@ void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>&
     }
   }
   out.write(buf.data(), static_cast<std::streamsize>(buf.size()));
+}
+
+void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q4.cpp:357-362
+  out << "o_orderpriority,order_count\n";
+  for (const auto& r : rows) out << escape_csv(r.orderpriority) << ',' << r.order_count << "\n";
 }
 
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows) {
@@ -1182,6 +1215,12 @@ void query(Database* db) {
       const auto rows = run_q10(*db, date);
       const auto end = std::chrono::steady_clock::now();
       write_q10_csv(file, rows);
+      report(end);
+    } else if (r.id == "4") {
+      const std::string date = arg("DATE");
+      const auto rows = run_q4(*db, date);
+      const auto end = std::chrono::steady_clock::now();
+      write_q4_csv(file, rows);
       report(end);
     } else if (r.id == "12") {
       const std::string mode1 = arg("SHIPMODE1");

@@ -136,6 +136,11 @@ struct Q6ResultRow {
   int64_t revenue_raw = 0;
 };
 
+struct Q4ResultRow {
+  std::string orderpriority;
+  int64_t order_count = 0;
+};
+
 struct Q12ResultRow {
   std::string shipmode;
   int64_t high_line_count = 0;
@@ -180,6 +185,7 @@ std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, 
 std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, const std::string& discount,
                                 const std::string& quantity);
 std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date);
+std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date);
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
                                   const std::string& date);
 std::vector<Q13ResultRow> run_q13(const Database& db, const std::string& word1, const std::string& word2);
@@ -189,6 +195,7 @@ void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& r
 void write_q3_csv(const Database& db, const std::string& filename, const std::vector<Q3ResultRow>& rows);
 void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& rows);
 void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows);
+void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& rows);
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);
 void write_q13_csv(const std::string& filename, const std::vector<Q13ResultRow>& rows);
 void write_q18_csv(const Database& db, const std::string& filename, const std::vector<Q18ResultRow>& rows);

@@ -215,6 +215,15 @@ class TpchQ18Row(C.Structure):
                 ("pad0", C.c_int16), ("pad1", C.c_int32)]
 
 
+class TpchQ4Tables(C.Structure):
+    """``bo_tpch_q4_tables``: date-sorted orders (keys, dates, priorities, lineitem ranges), lineitem keys and
+    packed commit / receipt dates."""
+    _fields_ = [("o_orderkey", C.c_void_p), ("o_orderdate", C.c_void_p), ("o_orderpriority", C.c_void_p),
+                ("o_li_begin", C.c_void_p), ("o_li_end", C.c_void_p), ("n_orders", C.c_int64),
+                ("l_orderkey", C.c_void_p), ("l_commit_receipt", C.c_void_p), ("n_lineitem", C.c_int64),
+                ("lineitem_orderkey_sorted", C.c_int32), ("n_priorities", C.c_int32)]
+
+
 class TpchQ12Tables(C.Structure):
     """``bo_tpch_q12_tables``: lineitem ship modes, packed commit / receipt dates, shipdates, orderkeys,
     optional shard maxima; orders map and priorities."""
@@ -328,6 +337,7 @@ _SIGNATURES = {
     "bo_tpch_order_ranges": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, C.c_int64, _P, _P]),
     "bo_tpch_q10": (C.c_int, [_P, C.POINTER(TpchQ10Tables), C.c_int16, C.c_int16, C.c_int32, C.c_int32,
                               C.POINTER(TpchQ10Row), C.c_int64, C.POINTER(C.c_int64)]),
+    "bo_tpch_q4": (C.c_int, [_P, C.POINTER(TpchQ4Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,
                               C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q13": (C.c_int, [_P, C.POINTER(TpchQ13Tables), C.c_char_p, C.c_int64, C.c_char_p, C.c_int64,

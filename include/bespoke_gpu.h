@@ -600,6 +600,31 @@ typedef struct bo_tpch_q13_row {      /* Q13ResultRow (bespoke_tpch/query_q13.hp
 int bo_tpch_q13(bo_ctx* ctx, const bo_tpch_q13_tables* tables, const char* word1, int64_t len1, const char* word2,
                 int64_t len2, bo_tpch_q13_row* out_host, int64_t max_rows, int64_t* n_rows);
 
+/* TPC-H Q4 over the storage-plan layout: run_q4 of
+ * bespoke_tpch/query_q4.cpp:172-355.  Orders dated in [start_offset,
+ * end_offset) (the date-sorted rows the reference finds by lower_bound,
+ * :190-197) with at least one lineitem in their range whose commit date is
+ * before its receipt date, compared as unsigned 16-bit offsets (q4_is_late,
+ * :71-73), counted by order-priority code.  With lineitems not sorted by
+ * orderkey only the range's lineitems of the order's own key count (:259-311).
+ * counts_out holds n_priorities counts. */
+typedef struct bo_tpch_q4_tables {
+  const int32_t* o_orderkey;
+  const int16_t* o_orderdate;          /* sorted ascending */
+  const uint16_t* o_orderpriority;     /* dictionary codes < n_priorities */
+  const uint32_t* o_li_begin;          /* per-order lineitem range; end 0 = none */
+  const uint32_t* o_li_end;
+  int64_t n_orders;
+  const int32_t* l_orderkey;
+  const uint32_t* l_commit_receipt;    /* (uint16)receipt << 16 | (uint16)commit */
+  int64_t n_lineitem;
+  int32_t lineitem_orderkey_sorted;
+  int32_t n_priorities;
+} bo_tpch_q4_tables;
+
+int bo_tpch_q4(bo_ctx* ctx, const bo_tpch_q4_tables* tables, int16_t start_offset, int16_t end_offset,
+               int64_t* counts_out);
+
 /* TPC-H Q12 over the storage-plan layout: run_q12 of
  * bespoke_tpch/query_q12.cpp:162-360.  Lineitems whose shipmode code is
  * mode_code1 or mode_code2 (-1: none), with shipdate < commitdate <
