@@ -521,6 +521,25 @@ std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date) {
   return rows;
 }
 
+std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date) {
+  // query_q14.cpp:189-200: the month [DATE, DATE + 1 month); no part keys: one zero row.
+  const int16_t start = date_offset_of(date, db.base_date_days);
+  const int16_t end = date_offset_of(date, db.base_date_days, 1);
+  if (db.max_partkey < 0) return {Q14ResultRow{}};
+  bo_tpch_q14_tables t{};
+  t.l_shipdate = col<int16_t>(db.l_shipdate);
+  t.l_partkey = col<int32_t>(db.l_partkey);
+  t.l_discounted_price = col<int32_t>(db.l_discounted_price);
+  t.n_lineitem = db.n_lineitem;
+  t.p_promo_by_key = col<int8_t>(db.p_promo_by_key);
+  t.n_promo_map = db.n_promo_map;
+  int64_t sums[2] = {0, 0};
+  check(db.ctx, bo_tpch_q14(db.ctx, &t, start, end, sums), "q14");
+  Q14ResultRow row;  // :347-355
+  if (sums[1] > 0) row.promo_revenue = 100.0 * static_cast<double>(sums[0]) / static_cast<double>(sums[1]);
+  return {row};
+}
+
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
                                   const std::string& date) {
   // query_q12.cpp:171-213: the window [DATE, DATE + 12 months), the two ship
@@ -732,6 +751,14 @@ void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& r
   for (const auto& r : rows) out << escape_csv(r.orderpriority) << ',' << r.order_count << "\n";
 }
 
+void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q14.cpp:367-374
+  out << "promo_revenue\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows) out << r.promo_revenue << "\n";
+}
+
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows) {
   std::ofstream out(filename);  // query_q12.cpp:362-368
   out << "l_shipmode,high_line_count,low_line_count\n";
@@ -776,7 +803,7 @@ Database::~Database() {
                           &l_discount, &l_tax, &l_quantity, &o_orderkey, &o_custkey, &o_orderdate,
                           &o_shippriority, &o_totalprice, &orderkey_to_row, &o_li_begin, &o_li_end,
                           &o_comment, &o_comment_offsets, &o_orderpriority, &l_shipmode, &l_commit_receipt,
-                          &l_shard_max_shipdate, &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
+                          &l_shard_max_shipdate, &l_partkey, &p_promo_by_key, &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
   if (result_host) bo_host_free_pinned(ctx, result_host);
@@ -842,7 +869,7 @@ namespace {
 
 // Host-side storage-plan columns of one table, derived before the upload.
 struct LineitemHost {
-  std::vector<int32_t> orderkey, price, dprice;
+  std::vector<int32_t> orderkey, price, dprice, partkey;
   std::vector<int16_t> ship, q16, shard_max_ship;
   std::vector<uint8_t> code, d8, t8;
   std::vector<uint16_t> shipmode;
@@ -963,6 +990,7 @@ LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, const ParquetTa
     if (i > 0 && h.orderkey[i] < h.orderkey[i - 1]) h.orderkey_sorted = false;
     h.max_orderkey = std::max(h.max_orderkey, h.orderkey[i]);
   }
+  h.partkey = int_values(column(L, "l_partkey"));
   h.commit_receipt = commit_receipt.get();
   auto sm = shipmode.get();
   h.shipmode = std::move(sm.first);
@@ -1037,6 +1065,31 @@ CustomerHost derive_customer(const ParquetTables::ArrowTable& C) {
   return h;
 }
 
+// Q14's partkey -> promo flag table (bespoke_tpch/query_q14.cpp:193-223):
+// types starting with "PROMO" by dictionary code, then each part row's key
+// (non-negative keys; a later row with the same key wins).
+struct PartHost {
+  std::vector<int8_t> promo_by_key;
+  int32_t max_key = -1;
+};
+
+PartHost derive_part(const ParquetTables::ArrowTable& P) {
+  PartHost h;
+  const auto key = int_values(column(P, "p_partkey"));
+  Dictionary types;
+  const auto type = dictionary_codes(column(P, "p_type"), types);
+  if (key.empty()) return h;
+  h.max_key = *std::max_element(key.begin(), key.end());
+  if (h.max_key < 0) return h;
+  std::vector<int8_t> promo_type(types.values.size(), 0);
+  for (size_t c = 0; c < types.values.size(); ++c)
+    promo_type[c] = types.values[c].size() >= 5 && types.values[c].compare(0, 5, "PROMO") == 0 ? 1 : 0;
+  h.promo_by_key.assign(static_cast<size_t>(h.max_key) + 1, int8_t(-1));
+  for (size_t i = 0; i < key.size(); ++i)
+    if (key[i] >= 0) h.promo_by_key[static_cast<size_t>(key[i])] = promo_type[type[i]];
+  return h;
+}
+
 }  // namespace
 
 Database* build(ParquetTables* tables) {
@@ -1057,6 +1110,7 @@ Database* build(ParquetTables* tables) {
   auto lineitem_f = std::async(std::launch::async, [&] { return derive_lineitem(tables->lineitem, tables->supplier, base_days); });
   auto orders_f = std::async(std::launch::async, [&] { return derive_orders(tables->orders, base_days); });
   auto customer_f = std::async(std::launch::async, [&] { return derive_customer(tables->customer); });
+  auto part_f = std::async(std::launch::async, [&] { return derive_part(tables->part); });
   auto* db = new Database();
   db->base_date_days = base_days;
   await_device_init();
@@ -1088,6 +1142,7 @@ Database* build(ParquetTables* tables) {
       db->l_shipmode = upload(ctx, h.shipmode);
       db->l_commit_receipt = upload(ctx, h.commit_receipt);
       if (!h.shard_max_ship.empty()) db->l_shard_max_shipdate = upload(ctx, h.shard_max_ship);
+      db->l_partkey = upload(ctx, h.partkey);
       phase("lineitem uploaded");
     }
     {
@@ -1136,6 +1191,12 @@ Database* build(ParquetTables* tables) {
       db->c_phone = std::move(h.phone);
       db->c_comment = std::move(h.comment);
       phase("customer uploaded");
+    }
+    {
+      PartHost h = part_f.get();
+      db->max_partkey = h.max_key;
+      db->n_promo_map = static_cast<int64_t>(h.promo_by_key.size());
+      db->p_promo_by_key = upload(ctx, h.promo_by_key);
     }
     // nation names by key (bespoke_tpch/builder_impl.cpp:780-803; query_q10.cpp:497-515)
     {
@@ -1221,6 +1282,12 @@ void query(Database* db) {
       const auto rows = run_q4(*db, date);
       const auto end = std::chrono::steady_clock::now();
       write_q4_csv(file, rows);
+      report(end);
+    } else if (r.id == "14") {
+      const std::string date = arg("DATE");
+      const auto rows = run_q14(*db, date);
+      const auto end = std::chrono::steady_clock::now();
+      write_q14_csv(file, rows);
       report(end);
     } else if (r.id == "12") {
       const std::string mode1 = arg("SHIPMODE1");

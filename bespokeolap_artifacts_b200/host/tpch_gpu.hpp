@@ -71,7 +71,7 @@ struct Database {
   // lineitem (row order of the input)
   int64_t n_lineitem = 0;
   bo_tpch::DeviceColumn l_orderkey, l_shipdate, l_returnflag_linestatus, l_extendedprice, l_discounted_price,
-      l_discount, l_tax, l_quantity, l_shipmode, l_commit_receipt;
+      l_discount, l_tax, l_quantity, l_shipmode, l_commit_receipt, l_partkey;
   // Latest shipdate of each lineitem's builder shard; only built when some
   // lineitem is received more than 30 days after shipping (Q12's shard pruning).
   bo_tpch::DeviceColumn l_shard_max_shipdate;
@@ -94,6 +94,11 @@ struct Database {
   bo_tpch::Dictionary mktsegment;
   std::vector<int32_t> c_acctbal;
   bo_tpch::StringColumn c_name, c_address, c_phone, c_comment;
+  // part: per partkey 1 (PROMO type), 0 (other type), -1 (no part row); the
+  // largest partkey (-1 without parts)
+  bo_tpch::DeviceColumn p_promo_by_key;
+  int64_t n_promo_map = 0;
+  int32_t max_partkey = -1;
   // nation names by nationkey in [0, nation_bound) (last row of each key)
   int32_t nation_bound = 1;
   std::vector<std::string> nation_name;
@@ -141,6 +146,10 @@ struct Q4ResultRow {
   int64_t order_count = 0;
 };
 
+struct Q14ResultRow {
+  double promo_revenue = 0.0;
+};
+
 struct Q12ResultRow {
   std::string shipmode;
   int64_t high_line_count = 0;
@@ -186,6 +195,7 @@ std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, con
                                 const std::string& quantity);
 std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date);
 std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date);
+std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date);
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
                                   const std::string& date);
 std::vector<Q13ResultRow> run_q13(const Database& db, const std::string& word1, const std::string& word2);
@@ -196,6 +206,7 @@ void write_q3_csv(const Database& db, const std::string& filename, const std::ve
 void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& rows);
 void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows);
 void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& rows);
+void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows);
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);
 void write_q13_csv(const std::string& filename, const std::vector<Q13ResultRow>& rows);
 void write_q18_csv(const Database& db, const std::string& filename, const std::vector<Q18ResultRow>& rows);

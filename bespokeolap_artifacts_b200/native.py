@@ -224,6 +224,12 @@ class TpchQ4Tables(C.Structure):
                 ("lineitem_orderkey_sorted", C.c_int32), ("n_priorities", C.c_int32)]
 
 
+class TpchQ14Tables(C.Structure):
+    """``bo_tpch_q14_tables``: lineitem shipdates, partkeys, discounted prices; the part promo flag per key."""
+    _fields_ = [("l_shipdate", C.c_void_p), ("l_partkey", C.c_void_p), ("l_discounted_price", C.c_void_p),
+                ("n_lineitem", C.c_int64), ("p_promo_by_key", C.c_void_p), ("n_promo_map", C.c_int64)]
+
+
 class TpchQ12Tables(C.Structure):
     """``bo_tpch_q12_tables``: lineitem ship modes, packed commit / receipt dates, shipdates, orderkeys,
     optional shard maxima; orders map and priorities."""
@@ -338,6 +344,7 @@ _SIGNATURES = {
     "bo_tpch_q10": (C.c_int, [_P, C.POINTER(TpchQ10Tables), C.c_int16, C.c_int16, C.c_int32, C.c_int32,
                               C.POINTER(TpchQ10Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q4": (C.c_int, [_P, C.POINTER(TpchQ4Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
+    "bo_tpch_q14": (C.c_int, [_P, C.POINTER(TpchQ14Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,
                               C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q13": (C.c_int, [_P, C.POINTER(TpchQ13Tables), C.c_char_p, C.c_int64, C.c_char_p, C.c_int64,

@@ -23,7 +23,8 @@ Key layouts (they select the reference's code paths):
                     at most 30), which the reference's Q12 shard pruning
                     notices.
 Ship modes MODE_A..MODE_G; order priorities 1-URGENT and 2-HIGH (the two the
-reference's Q12 counts as high) and three others.  Commit dates 30..90 days
+reference's Q12 counts as high) and three others; part types with and
+without the PROMO prefix Q14 looks for.  Commit dates 30..90 days
 after the order, receipts 1..30 days after shipping.  These columns come from
 a second seeded stream, so the other columns do not depend on them.
 The nation table has keys 0..24 except 7; customers' nationkeys run 0..26.
@@ -40,6 +41,7 @@ SEGMENTS = ["SEG_A", "SEG_B", "SEG_C", "SEG_D", "SEG_E"]
 WORDS = ["ironic", "quick", "pending", "bold", 'say "hi"', "a,b", "deposits", "", "x\"y", "final"]
 SHIPMODES = ["MODE_A", "MODE_B", "MODE_C", "MODE_D", "MODE_E", "MODE_F", "MODE_G"]
 PRIORITIES = ["1-URGENT", "2-HIGH", "3-PRIO_C", "4-PRIO_D", "5-PRIO_E"]
+PART_TYPES = ["PROMO_A", "PROMO_B", "STD_A", "STD_B", "ECO_A", "PROMOTION", "PROM", "LARGE_PROMO"]
 D1992 = 8035  # 1992-01-01 in days since 1970-01-01
 
 
@@ -135,9 +137,18 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
         "l_comment": [""] * n,
     }), out / "lineitem.parquet")
     one = np.ones(1, np.int32)
-    pq.write_table(pa.table({"p_partkey": one, "p_name": ["p"], "p_mfgr": ["m"], "p_brand": ["b"], "p_type": ["t"],
-                             "p_size": one, "p_container": ["c"], "p_retailprice": _dec(np.ones(1), decimal),
-                             "p_comment": [""]}), out / "part.parquet")
+    # parts 1..150 (lineitems name 1..199, so some have no part) and a last row
+    # repeating key 3 with another type (the later row wins)
+    rng3 = np.random.default_rng([seed, 14])
+    pkey = np.concatenate([np.arange(1, 151), [3]]).astype(np.int32)
+    n_part = len(pkey)
+    ptype = [PART_TYPES[i] for i in rng3.integers(0, len(PART_TYPES), n_part)]
+    ptype[-1] = "STD_A" if ptype[2].startswith("PROMO") else "PROMO_B"
+    pq.write_table(pa.table({"p_partkey": pkey, "p_name": [f"part {k}" for k in pkey], "p_mfgr": ["m"] * n_part,
+                             "p_brand": ["b"] * n_part, "p_type": ptype,
+                             "p_size": rng3.integers(1, 51, n_part).astype(np.int32), "p_container": ["c"] * n_part,
+                             "p_retailprice": _dec(np.ones(n_part), decimal), "p_comment": [""] * n_part}),
+                   out / "part.parquet")
     pq.write_table(pa.table({"s_suppkey": one, "s_name": ["s"], "s_address": ["a"], "s_nationkey": one * 0,
                              "s_phone": ["10-0"], "s_acctbal": _dec(np.ones(1), decimal), "s_comment": [""]}),
                    out / "supplier.parquet")

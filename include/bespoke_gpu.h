@@ -625,6 +625,26 @@ typedef struct bo_tpch_q4_tables {
 int bo_tpch_q4(bo_ctx* ctx, const bo_tpch_q4_tables* tables, int16_t start_offset, int16_t end_offset,
                int64_t* counts_out);
 
+/* TPC-H Q14 over the storage-plan layout: run_q14 of
+ * bespoke_tpch/query_q14.cpp:176-352.  Lineitems shipped in [start_offset,
+ * end_offset) whose partkey has a part row: sums_out[1] = the sum of their
+ * discounted prices, sums_out[0] = the same over parts whose type starts
+ * with PROMO (int64, as the reference's promo_sum / total_sum).
+ * p_promo_by_key[k] = 1 (promo type), 0 (other type) or -1 (no part row
+ * with key k), the reference's partkey_promo (:193-223), built once by the
+ * drop-in's build(). */
+typedef struct bo_tpch_q14_tables {
+  const int16_t* l_shipdate;           /* 16-byte aligned */
+  const int32_t* l_partkey;
+  const int32_t* l_discounted_price;
+  int64_t n_lineitem;
+  const int8_t* p_promo_by_key;
+  int64_t n_promo_map;                 /* max partkey + 1 */
+} bo_tpch_q14_tables;
+
+int bo_tpch_q14(bo_ctx* ctx, const bo_tpch_q14_tables* tables, int16_t start_offset, int16_t end_offset,
+                int64_t sums_out[2]);
+
 /* TPC-H Q12 over the storage-plan layout: run_q12 of
  * bespoke_tpch/query_q12.cpp:162-360.  Lineitems whose shipmode code is
  * mode_code1 or mode_code2 (-1: none), with shipdate < commitdate <

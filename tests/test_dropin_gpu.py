@@ -2,7 +2,7 @@
 query (bespokeolap_artifacts_b200/host) and the reference's own load / build /
 query (compiled unchanged into oracle/_ref/ref_tpch_driver) read the same
 Parquet files and the same stdin requests; their result<idx>.csv files must
-agree: Q1, Q4, Q6, Q10, Q12, Q13 and Q18 byte for byte, Q3 row for row (the reference's
+agree: Q1, Q4, Q6, Q10, Q12, Q13, Q14 and Q18 byte for byte, Q3 row for row (the reference's
 std::sort leaves rows equal in revenue and orderdate in unspecified order;
 the GPU emits them in orderkey order).  The key layouts select each of the
 reference's paths: dense and sparse orderkeys (Q18's two scans), dense,
@@ -31,6 +31,7 @@ REQUESTS = [
     '10 "1993-10-01"', '10 "1995-01-31"', '10 "1992-11-30"', '10 "1998-07-01"', '10 "1999-01-01"',
     '18 "250"', '18 "150.5"', '18 "0"', '18 "-1"', '18 "400"', '18 "<<NULL>>"',
     '4 "1993-07-01"', '4 "1995-11-30"', '4 "1999-01-01"', '4 "1992-01-01"',
+    '14 "1995-09-01"', '14 "1993-01-31"', '14 "2000-01-01"',
     '12 "MODE_A" "MODE_C" "1994-01-01"', '12 "MODE_B" "MODE_B" "1995-06-30"', '12 "NOSUCH" "MODE_D" "1993-03-01"',
     '12 "X" "Y" "1994-01-01"', '12 "MODE_G" "MODE_E" "1998-12-01"', '12 "MODE_F" "MODE_A" "1992-02-29"',
     '13 "pending" "deposits"', '13 "quick" "quick"', '13 "" ""', '13 "bold" ""', '13 "" "final"',
