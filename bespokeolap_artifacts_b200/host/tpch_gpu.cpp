@@ -521,6 +521,43 @@ std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date) {
   return rows;
 }
 
+std::vector<Q5ResultRow> run_q5(const Database& db, const std::string& region, const std::string& date) {
+  // query_q5.cpp:204-240: the region's key, the window [DATE, DATE + 1 year),
+  // the nations of the region by key (any nation row of the key in it).
+  const auto it = db.region_key_by_name.find(region);
+  if (it == db.region_key_by_name.end()) return {};
+  const int32_t region_key = it->second;
+  const int16_t start = date_offset_of(date, db.base_date_days);
+  const int16_t end = date_offset_of(date, db.base_date_days, 12);
+  const int32_t n_nations = db.nation_bound;
+  std::vector<uint8_t> in_region(static_cast<size_t>(n_nations), 0);
+  for (size_t i = 0; i < db.nation_key.size(); ++i)
+    if (db.nation_key[i] >= 0 && db.nation_regionkey[i] == region_key) in_region[static_cast<size_t>(db.nation_key[i])] = 1;
+  bo_tpch_q5_tables t{};
+  t.o_orderkey = col<int32_t>(db.o_orderkey);
+  t.o_orderdate = col<int16_t>(db.o_orderdate);
+  t.o_cust_nation = col<int16_t>(db.o_cust_nation);
+  t.o_li_begin = col<uint32_t>(db.o_li_begin);
+  t.o_li_end = col<uint32_t>(db.o_li_end);
+  t.n_orders = db.n_orders;
+  t.l_orderkey = col<int32_t>(db.l_orderkey);
+  t.l_supp_nation = col<int16_t>(db.l_supp_nation);
+  t.l_discounted_price = col<int32_t>(db.l_discounted_price);
+  t.n_lineitem = db.n_lineitem;
+  t.lineitem_orderkey_sorted = db.lineitem_orderkey_sorted ? 1 : 0;
+  t.n_nations = n_nations;
+  std::vector<int64_t> revenue(static_cast<size_t>(n_nations), 0);
+  check(db.ctx, bo_tpch_q5(db.ctx, &t, in_region.data(), start, end, revenue.data()), "q5");
+  // Region nations with non-zero revenue, by revenue desc then name (:497-548).
+  std::vector<Q5ResultRow> rows;
+  for (size_t n = 0; n < revenue.size(); ++n)
+    if (in_region[n] && revenue[n] != 0) rows.push_back(Q5ResultRow{db.nation_name[n], revenue[n]});
+  std::sort(rows.begin(), rows.end(), [](const Q5ResultRow& a, const Q5ResultRow& b) {
+    return a.revenue_raw != b.revenue_raw ? a.revenue_raw > b.revenue_raw : a.n_name < b.n_name;
+  });
+  return rows;
+}
+
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date) {
   // query_q14.cpp:189-200: the month [DATE, DATE + 1 month); no part keys: one zero row.
   const int16_t start = date_offset_of(date, db.base_date_days);
@@ -751,6 +788,15 @@ void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& r
   for (const auto& r : rows) out << escape_csv(r.orderpriority) << ',' << r.order_count << "\n";
 }
 
+void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q5.cpp:560-569
+  out << "n_name,revenue\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows)
+    out << escape_csv(r.n_name) << ',' << static_cast<double>(r.revenue_raw) / static_cast<double>(kPriceScale) << "\n";
+}
+
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows) {
   std::ofstream out(filename);  // query_q14.cpp:367-374
   out << "promo_revenue\n";
@@ -803,7 +849,8 @@ Database::~Database() {
                           &l_discount, &l_tax, &l_quantity, &o_orderkey, &o_custkey, &o_orderdate,
                           &o_shippriority, &o_totalprice, &orderkey_to_row, &o_li_begin, &o_li_end,
                           &o_comment, &o_comment_offsets, &o_orderpriority, &l_shipmode, &l_commit_receipt,
-                          &l_shard_max_shipdate, &l_partkey, &p_promo_by_key, &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
+                          &l_shard_max_shipdate, &l_partkey, &p_promo_by_key, &l_supp_nation, &o_cust_nation,
+                          &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
   if (result_host) bo_host_free_pinned(ctx, result_host);
@@ -870,7 +917,7 @@ namespace {
 // Host-side storage-plan columns of one table, derived before the upload.
 struct LineitemHost {
   std::vector<int32_t> orderkey, price, dprice, partkey;
-  std::vector<int16_t> ship, q16, shard_max_ship;
+  std::vector<int16_t> ship, q16, shard_max_ship, supp_nation;
   std::vector<uint8_t> code, d8, t8;
   std::vector<uint16_t> shipmode;
   std::vector<uint32_t> commit_receipt;
@@ -897,12 +944,10 @@ struct CustomerHost {
 };
 
 // lineitem: the storage-plan columns of bespoke_tpch/builder_impl.cpp:456-577.
-// Latest shipdate of each lineitem's builder shard (bespoke_tpch/builder_impl.cpp:838-911):
-// shards group lineitems by (ship year-month, discount, quantity / 100,
-// supplier nation), the nation through supplier's nationkey_by_suppkey
-// (:719-742).  Keys and buckets are formed by the builder's own expressions.
-std::vector<int16_t> shard_max_shipdates(const LineitemHost& h, const ParquetTables::ArrowTable& L,
-                                         const ParquetTables::ArrowTable& S, int32_t base_days) {
+// Each lineitem's supplier nation (bespoke_tpch/builder_impl.cpp:838-853):
+// supplier's nationkey_by_suppkey (:719-742, last row of a key wins), -1 for
+// suppkeys without a supplier.
+std::vector<int16_t> supplier_nations(const ParquetTables::ArrowTable& L, const ParquetTables::ArrowTable& S) {
   const auto suppkey = int_values(column(L, "l_suppkey"));
   const auto s_key = int_values(column(S, "s_suppkey"));
   const auto s_nation = int_values(column(S, "s_nationkey"));
@@ -912,6 +957,17 @@ std::vector<int16_t> shard_max_shipdates(const LineitemHost& h, const ParquetTab
   for (size_t i = 0; i < s_key.size(); ++i)
     if (s_key[i] >= 0 && static_cast<size_t>(s_key[i]) < nation_by_key.size())
       nation_by_key[static_cast<size_t>(s_key[i])] = static_cast<int16_t>(s_nation[i]);
+  std::vector<int16_t> out(suppkey.size(), int16_t(-1));
+  for (size_t i = 0; i < suppkey.size(); ++i)
+    if (suppkey[i] >= 0 && static_cast<size_t>(suppkey[i]) < nation_by_key.size())
+      out[i] = nation_by_key[static_cast<size_t>(suppkey[i])];
+  return out;
+}
+
+// Latest shipdate of each lineitem's builder shard (bespoke_tpch/builder_impl.cpp:855-911):
+// shards group lineitems by (ship year-month, discount, quantity / 100,
+// supplier nation).  Keys and buckets are formed by the builder's own expressions.
+std::vector<int16_t> shard_max_shipdates(const LineitemHost& h, int32_t base_days) {
   const size_t n = h.ship.size();
   std::vector<int64_t> keys(n);
   std::unordered_map<int64_t, int16_t> shard_max;
@@ -919,9 +975,7 @@ std::vector<int16_t> shard_max_shipdates(const LineitemHost& h, const ParquetTab
     int y = 0;
     unsigned m = 0, d = 0;
     civil_from_days(base_days + h.ship[i], y, m, d);
-    int16_t supp_nation = -1;
-    if (suppkey[i] >= 0 && static_cast<size_t>(suppkey[i]) < nation_by_key.size())
-      supp_nation = nation_by_key[static_cast<size_t>(suppkey[i])];
+    const int16_t supp_nation = h.supp_nation[i];
     const int32_t discount_bucket = static_cast<int32_t>(h.d8[i]);
     const int32_t quantity_bucket = static_cast<int32_t>(h.q16[i]) / 100;
     const int32_t month_index = y * 12 + (static_cast<int32_t>(m) - 1);
@@ -951,6 +1005,7 @@ LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, const ParquetTa
                   static_cast<uint32_t>(static_cast<uint16_t>(commit[i]));
     return packed;
   });
+  auto supp_nation = std::async(std::launch::async, [&] { return supplier_nations(L, S); });
   auto shipmode = std::async(std::launch::async, [&] {
     Dictionary dict;
     auto codes = dictionary_codes(column(L, "l_shipmode"), dict);
@@ -991,6 +1046,7 @@ LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, const ParquetTa
     h.max_orderkey = std::max(h.max_orderkey, h.orderkey[i]);
   }
   h.partkey = int_values(column(L, "l_partkey"));
+  h.supp_nation = supp_nation.get();
   h.commit_receipt = commit_receipt.get();
   auto sm = shipmode.get();
   h.shipmode = std::move(sm.first);
@@ -1000,7 +1056,7 @@ LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, const ParquetTa
   bool late = false;
   for (size_t i = 0; i < n && !late; ++i)
     late = static_cast<int32_t>(static_cast<int16_t>(h.commit_receipt[i] >> 16)) - static_cast<int32_t>(h.ship[i]) > 30;
-  if (late) h.shard_max_ship = shard_max_shipdates(h, L, S, base_days);
+  if (late) h.shard_max_ship = shard_max_shipdates(h, base_days);
   return h;
 }
 
@@ -1143,8 +1199,10 @@ Database* build(ParquetTables* tables) {
       db->l_commit_receipt = upload(ctx, h.commit_receipt);
       if (!h.shard_max_ship.empty()) db->l_shard_max_shipdate = upload(ctx, h.shard_max_ship);
       db->l_partkey = upload(ctx, h.partkey);
+      db->l_supp_nation = upload(ctx, h.supp_nation);
       phase("lineitem uploaded");
     }
+    std::vector<int32_t> order_custkeys;  // date-sorted orders' custkeys, for orders.cust_nationkey
     {
       OrdersHost h = orders_f.get();
       phase("orders derived");
@@ -1166,6 +1224,7 @@ Database* build(ParquetTables* tables) {
       check(ctx, bo_device_alloc(ctx, bytes, &db->o_li_begin.ptr), "device alloc");
       check(ctx, bo_device_alloc(ctx, bytes, &db->o_li_end.ptr), "device alloc");
       db->o_li_begin.rows = db->o_li_end.rows = db->n_orders;
+      order_custkeys = std::move(h.ckey);
       check(ctx,
             bo_tpch_order_ranges(ctx, col<int32_t>(db->l_orderkey), db->n_lineitem, col<int32_t>(db->orderkey_to_row),
                                  db->n_orderkey_map, db->n_orders, static_cast<uint32_t*>(db->o_li_begin.ptr),
@@ -1185,6 +1244,18 @@ Database* build(ParquetTables* tables) {
       db->c_mktsegment = upload(ctx, h.seg);
       db->c_nationkey = upload(ctx, h.nkey);
       db->custkey_to_row = upload(ctx, h.map);
+      // Each order's customer nation (builder_impl.cpp:672-690, 913-928): the
+      // nationkey (as int16) of the last customer row of its custkey, -1 without one.
+      std::vector<int16_t> nation_by_custkey(h.ckey.empty() || h.max_key < 0 ? 0 : static_cast<size_t>(h.max_key) + 1,
+                                             int16_t(-1));
+      for (size_t i = 0; i < h.ckey.size(); ++i)
+        if (h.ckey[i] >= 0 && static_cast<size_t>(h.ckey[i]) < nation_by_custkey.size())
+          nation_by_custkey[static_cast<size_t>(h.ckey[i])] = static_cast<int16_t>(h.nkey[i]);
+      std::vector<int16_t> cust_nation(order_custkeys.size(), int16_t(-1));
+      for (size_t i = 0; i < order_custkeys.size(); ++i)
+        if (order_custkeys[i] >= 0 && static_cast<size_t>(order_custkeys[i]) < nation_by_custkey.size())
+          cust_nation[i] = nation_by_custkey[static_cast<size_t>(order_custkeys[i])];
+      db->o_cust_nation = upload(ctx, cust_nation);
       db->c_acctbal = std::move(h.acctbal);
       db->c_name = std::move(h.name);
       db->c_address = std::move(h.address);
@@ -1209,6 +1280,14 @@ Database* build(ParquetTables* tables) {
       db->nation_name.assign(static_cast<size_t>(db->nation_bound), std::string());
       for (size_t i = 0; i < key.size(); ++i)
         if (key[i] >= 0) db->nation_name[static_cast<size_t>(key[i])] = std::string(name.view(i));
+      db->nation_key = key;
+      db->nation_regionkey = int_values(column(N, "n_regionkey"));
+    }
+    {  // region name -> key, the first row of a name (builder_impl.cpp:805-826)
+      const auto& R = tables->region;
+      const auto key = int_values(column(R, "r_regionkey"));
+      const auto name = string_column(column(R, "r_name"));
+      for (size_t i = 0; i < key.size(); ++i) db->region_key_by_name.emplace(std::string(name.view(i)), key[i]);
     }
     check(ctx, bo_device_alloc(ctx, sizeof(bo_q1_agg) * BO_Q1_MAX_GROUPS + 256, &db->scratch.ptr), "scratch alloc");
     check(ctx, bo_synchronize(ctx), "build");
@@ -1282,6 +1361,13 @@ void query(Database* db) {
       const auto rows = run_q4(*db, date);
       const auto end = std::chrono::steady_clock::now();
       write_q4_csv(file, rows);
+      report(end);
+    } else if (r.id == "5") {
+      const std::string region = arg("REGION");
+      const std::string date = arg("DATE");
+      const auto rows = run_q5(*db, region, date);
+      const auto end = std::chrono::steady_clock::now();
+      write_q5_csv(file, rows);
       report(end);
     } else if (r.id == "14") {
       const std::string date = arg("DATE");

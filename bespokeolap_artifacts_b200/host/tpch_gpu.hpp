@@ -21,6 +21,7 @@
 #include <cstdint>
 #include <memory>
 #include <string>
+#include <unordered_map>
 #include <string_view>
 #include <vector>
 
@@ -71,7 +72,7 @@ struct Database {
   // lineitem (row order of the input)
   int64_t n_lineitem = 0;
   bo_tpch::DeviceColumn l_orderkey, l_shipdate, l_returnflag_linestatus, l_extendedprice, l_discounted_price,
-      l_discount, l_tax, l_quantity, l_shipmode, l_commit_receipt, l_partkey;
+      l_discount, l_tax, l_quantity, l_shipmode, l_commit_receipt, l_partkey, l_supp_nation;
   // Latest shipdate of each lineitem's builder shard; only built when some
   // lineitem is received more than 30 days after shipping (Q12's shard pruning).
   bo_tpch::DeviceColumn l_shard_max_shipdate;
@@ -81,7 +82,7 @@ struct Database {
   // orders, sorted by orderdate (stable); each row's lineitem range
   int64_t n_orders = 0;
   bo_tpch::DeviceColumn o_orderkey, o_custkey, o_orderdate, o_shippriority, o_totalprice, orderkey_to_row,
-      o_li_begin, o_li_end, o_comment, o_comment_offsets, o_orderpriority;
+      o_li_begin, o_li_end, o_comment, o_comment_offsets, o_orderpriority, o_cust_nation;
   bo_tpch::Dictionary orderpriority;
   int64_t n_orderkey_map = 0;
   bool dense_orderkeys = false;  // first orderkey 1, last n_orders (date order)
@@ -102,6 +103,9 @@ struct Database {
   // nation names by nationkey in [0, nation_bound) (last row of each key)
   int32_t nation_bound = 1;
   std::vector<std::string> nation_name;
+  // nation rows' keys and region keys; region name -> key (first row of a name)
+  std::vector<int32_t> nation_key, nation_regionkey;
+  std::unordered_map<std::string, int32_t> region_key_by_name;
   // Result record of the last scan-agg / Q6 query.  Queries on one Database
   // run one at a time (as the reference's single-threaded query()).
   bo_tpch::DeviceColumn scratch;
@@ -144,6 +148,11 @@ struct Q6ResultRow {
 struct Q4ResultRow {
   std::string orderpriority;
   int64_t order_count = 0;
+};
+
+struct Q5ResultRow {
+  std::string n_name;
+  int64_t revenue_raw = 0;
 };
 
 struct Q14ResultRow {
@@ -195,6 +204,7 @@ std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, con
                                 const std::string& quantity);
 std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date);
 std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date);
+std::vector<Q5ResultRow> run_q5(const Database& db, const std::string& region, const std::string& date);
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date);
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
                                   const std::string& date);
@@ -206,6 +216,7 @@ void write_q3_csv(const Database& db, const std::string& filename, const std::ve
 void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& rows);
 void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows);
 void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& rows);
+void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& rows);
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows);
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);
 void write_q13_csv(const std::string& filename, const std::vector<Q13ResultRow>& rows);

@@ -224,6 +224,15 @@ class TpchQ4Tables(C.Structure):
                 ("lineitem_orderkey_sorted", C.c_int32), ("n_priorities", C.c_int32)]
 
 
+class TpchQ5Tables(C.Structure):
+    """``bo_tpch_q5_tables``: date-sorted orders (keys, dates, customer nations, lineitem ranges), lineitem keys,
+    supplier nations and discounted prices."""
+    _fields_ = [("o_orderkey", C.c_void_p), ("o_orderdate", C.c_void_p), ("o_cust_nation", C.c_void_p),
+                ("o_li_begin", C.c_void_p), ("o_li_end", C.c_void_p), ("n_orders", C.c_int64),
+                ("l_orderkey", C.c_void_p), ("l_supp_nation", C.c_void_p), ("l_discounted_price", C.c_void_p),
+                ("n_lineitem", C.c_int64), ("lineitem_orderkey_sorted", C.c_int32), ("n_nations", C.c_int32)]
+
+
 class TpchQ14Tables(C.Structure):
     """``bo_tpch_q14_tables``: lineitem shipdates, partkeys, discounted prices; the part promo flag per key."""
     _fields_ = [("l_shipdate", C.c_void_p), ("l_partkey", C.c_void_p), ("l_discounted_price", C.c_void_p),
@@ -344,6 +353,7 @@ _SIGNATURES = {
     "bo_tpch_q10": (C.c_int, [_P, C.POINTER(TpchQ10Tables), C.c_int16, C.c_int16, C.c_int32, C.c_int32,
                               C.POINTER(TpchQ10Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q4": (C.c_int, [_P, C.POINTER(TpchQ4Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
+    "bo_tpch_q5": (C.c_int, [_P, C.POINTER(TpchQ5Tables), C.c_char_p, C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q14": (C.c_int, [_P, C.POINTER(TpchQ14Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,
                               C.c_int16, C.POINTER(C.c_int64)]),

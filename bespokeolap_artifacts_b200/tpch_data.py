@@ -22,6 +22,14 @@ Key layouts (they select the reference's code paths):
   late_receipts     receipt dates up to 60 days after shipping (TPC-H's are
                     at most 30), which the reference's Q12 shard pruning
                     notices.
+  customer_nations  "wide": nationkeys 0..26, some without a nation row (Q10
+                    drops those customers); "known": 0..24, inside the nation
+                    table's key range (the reference's Q5 indexes its
+                    per-nation arrays by the customer's nationkey unchecked).
+  n_supplier        suppliers 1..n with nations 0..24 (default: one
+                    supplier, key 1, nation 0).
+Regions REGION0..REGION4 (keys 0..4; nations' regionkey = nationkey % 5) and
+a later row repeating REGION1 with key 9.
 Ship modes MODE_A..MODE_G; order priorities 1-URGENT and 2-HIGH (the two the
 reference's Q12 counts as high) and three others; part types with and
 without the PROMO prefix Q14 looks for.  Commit dates 30..90 days
@@ -53,6 +61,16 @@ def _dec(values: np.ndarray, decimal: bool) -> pa.Array:
     return pa.array([Decimal(f"{v:.2f}") for v in values], pa.decimal128(15, 2))
 
 
+def _nations(keys: np.ndarray, mode: str) -> np.ndarray:
+    """Customer nationkeys: "wide" 0..26 (25 and 26 have no nation row), or
+    "known" within the nation table's key range 0..24."""
+    if mode == "wide":
+        return keys.astype(np.int32)
+    if mode == "known":
+        return (keys % 25).astype(np.int32)
+    raise ValueError(mode)
+
+
 def _text(rng, n: int, words: int) -> list[str]:
     picks = rng.integers(0, len(WORDS), (n, words))
     return [" ".join(WORDS[i] for i in row) for row in picks]
@@ -65,7 +83,8 @@ def _ragged_text(rng, n: int, max_words: int) -> list[str]:
 
 def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: int = 0,
                decimal: bool = False, order_keys: str = "sparse", customer_keys: str = "dense",
-               shuffle_lineitem: bool = False, late_receipts: bool = False) -> Path:
+               shuffle_lineitem: bool = False, late_receipts: bool = False, customer_nations: str = "wide",
+               n_supplier: int = 1) -> Path:
     rng = np.random.default_rng(seed)
     rng2 = np.random.default_rng([seed, 12])
     out.mkdir(parents=True, exist_ok=True)
@@ -81,7 +100,7 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
     seg = rng.integers(0, 5, n_customer)
     pq.write_table(pa.table({
         "c_custkey": custkey, "c_name": [f"Customer#{k:09d}" for k in custkey],
-        "c_address": _text(rng, n_customer, 2), "c_nationkey": rng.integers(0, 27, n_customer).astype(np.int32),
+        "c_address": _text(rng, n_customer, 2), "c_nationkey": _nations(rng.integers(0, 27, n_customer), customer_nations),
         "c_phone": [f"{10 + a}-{b:03d}-{c:03d}-{d:04d}" for a, b, c, d in
                     zip(*(rng.integers(0, m, n_customer) for m in (25, 1000, 1000, 10000)))],
         "c_acctbal": _dec(rng.integers(-99999, 999999, n_customer) / 100.0, decimal),
@@ -149,13 +168,22 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
                              "p_size": rng3.integers(1, 51, n_part).astype(np.int32), "p_container": ["c"] * n_part,
                              "p_retailprice": _dec(np.ones(n_part), decimal), "p_comment": [""] * n_part}),
                    out / "part.parquet")
-    pq.write_table(pa.table({"s_suppkey": one, "s_name": ["s"], "s_address": ["a"], "s_nationkey": one * 0,
-                             "s_phone": ["10-0"], "s_acctbal": _dec(np.ones(1), decimal), "s_comment": [""]}),
+    if n_supplier <= 1:
+        skey, snation = one, one * 0
+    else:
+        skey = np.arange(1, n_supplier + 1, dtype=np.int32)
+        snation = np.random.default_rng([seed, 5]).integers(0, 25, n_supplier).astype(np.int32)
+    ns = len(skey)
+    pq.write_table(pa.table({"s_suppkey": skey, "s_name": ["s"] * ns, "s_address": ["a"] * ns, "s_nationkey": snation,
+                             "s_phone": ["10-0"] * ns, "s_acctbal": _dec(np.ones(ns), decimal), "s_comment": [""] * ns}),
                    out / "supplier.parquet")
     pq.write_table(pa.table({"ps_partkey": one, "ps_suppkey": one, "ps_availqty": one,
                              "ps_supplycost": _dec(np.ones(1), decimal), "ps_comment": [""]}), out / "partsupp.parquet")
     nkey = np.array([k for k in range(25) if k != 7], np.int32)
     pq.write_table(pa.table({"n_nationkey": nkey, "n_name": [f"NATION_{k:02d}" for k in nkey],
                              "n_regionkey": nkey % 5, "n_comment": [""] * len(nkey)}), out / "nation.parquet")
-    pq.write_table(pa.table({"r_regionkey": one * 0, "r_name": ["REGION0"], "r_comment": [""]}), out / "region.parquet")
+    # five regions and a later row repeating a name (the first row of a name wins)
+    pq.write_table(pa.table({"r_regionkey": np.array([0, 1, 2, 3, 4, 9], np.int32),
+                             "r_name": [f"REGION{k}" for k in range(5)] + ["REGION1"], "r_comment": [""] * 6}),
+                   out / "region.parquet")
     return out

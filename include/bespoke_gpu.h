@@ -600,6 +600,33 @@ typedef struct bo_tpch_q13_row {      /* Q13ResultRow (bespoke_tpch/query_q13.hp
 int bo_tpch_q13(bo_ctx* ctx, const bo_tpch_q13_tables* tables, const char* word1, int64_t len1, const char* word2,
                 int64_t len2, bo_tpch_q13_row* out_host, int64_t max_rows, int64_t* n_rows);
 
+/* TPC-H Q5 over the storage-plan layout: run_q5 of
+ * bespoke_tpch/query_q5.cpp:197-540.  Orders dated in [start_offset,
+ * end_offset) whose customer's nation (o_cust_nation, the builder's
+ * orders.cust_nationkey, builder_impl.cpp:913-928) is in the region
+ * (nation_in_region_host[nation] != 0, n_nations entries), summing the
+ * discounted price of the lineitems in their range whose supplier's nation
+ * (l_supp_nation, builder_impl.cpp:838-853) is that same nation; with
+ * lineitems not sorted by orderkey only the range's lineitems of the order's
+ * own key count.  revenue_out holds n_nations int64 sums. */
+typedef struct bo_tpch_q5_tables {
+  const int32_t* o_orderkey;
+  const int16_t* o_orderdate;          /* sorted ascending */
+  const int16_t* o_cust_nation;        /* -1: no customer row */
+  const uint32_t* o_li_begin;
+  const uint32_t* o_li_end;
+  int64_t n_orders;
+  const int32_t* l_orderkey;
+  const int16_t* l_supp_nation;        /* -1: no supplier row */
+  const int32_t* l_discounted_price;
+  int64_t n_lineitem;
+  int32_t lineitem_orderkey_sorted;
+  int32_t n_nations;                   /* max nationkey + 1 */
+} bo_tpch_q5_tables;
+
+int bo_tpch_q5(bo_ctx* ctx, const bo_tpch_q5_tables* tables, const uint8_t* nation_in_region_host,
+               int16_t start_offset, int16_t end_offset, int64_t* revenue_out);
+
 /* TPC-H Q4 over the storage-plan layout: run_q4 of
  * bespoke_tpch/query_q4.cpp:172-355.  Orders dated in [start_offset,
  * end_offset) (the date-sorted rows the reference finds by lower_bound,

@@ -87,6 +87,38 @@ def test_dropin_matches_reference_driver(tmp_path, layout):
             assert g.read_bytes() == r.read_bytes(), req
 
 
+Q5_REQUESTS = ['5 "REGION0" "1994-01-01"', '5 "REGION1" "1995-02-28"', '5 "REGION4" "1996-02-29"',
+               '5 "NOSUCH" "1994-01-01"', '5 "REGION3" "1999-01-01"', '5 "REGION2" "1992-01-01"']
+
+Q5_LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem): known nations, 25 suppliers
+    (11, False, "sparse", "dense", False),
+    (12, True, "dense", "sparse", True),
+]
+
+
+@pytest.mark.parametrize("layout", Q5_LAYOUTS, ids=lambda l: "-".join(map(str, l)))
+def test_dropin_q5_matches_reference_driver(tmp_path, layout):
+    """Q5 (with every other request) on data whose customer nationkeys lie in
+    the nation table's key range: the reference's run_q5 indexes its
+    per-nation arrays by them unchecked (query_q5.cpp:337-338, 423-424)."""
+    if not REF_DRIVER.exists() or not GPU_DRIVER.exists():
+        pytest.skip("drivers not built")
+    seed, decimal, order_keys, customer_keys, shuffle = layout
+    data = write_tpch(tmp_path / "data", seed=seed, decimal=decimal, order_keys=order_keys,
+                      customer_keys=customer_keys, shuffle_lineitem=shuffle, customer_nations="known", n_supplier=25)
+    requests = Q5_REQUESTS + REQUESTS
+    run(GPU_DRIVER, data, tmp_path / "gpu", requests)
+    run(REF_DRIVER, data, tmp_path / "ref", requests)
+    for i, req in enumerate(requests, start=1):
+        g, r = tmp_path / "gpu" / f"result{i}.csv", tmp_path / "ref" / f"result{i}.csv"
+        if req.startswith("3 "):
+            hg, rows_g = q3_rows(g)
+            hr, rows_r = q3_rows(r)
+            assert hg == hr and rows_g == sorted(rows_r, key=lambda x: (-float(x[1]), x[2], x[0])), req
+        else:
+            assert g.read_bytes() == r.read_bytes(), req
+
+
 def test_dropin_stub_for_queries_off_the_gpu_path(tmp_path):
     if not GPU_DRIVER.exists():
         pytest.skip("driver not built")
