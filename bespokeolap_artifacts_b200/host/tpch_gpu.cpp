@@ -558,6 +558,32 @@ std::vector<Q5ResultRow> run_q5(const Database& db, const std::string& region, c
   return rows;
 }
 
+std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container) {
+  // query_q17.cpp:125-155: NULL arguments, no parts, or an unknown brand or
+  // container give a zero row.
+  if (brand == "<<NULL>>" || container == "<<NULL>>" || db.max_partkey < 0) return {Q17ResultRow{}};
+  auto code_of = [](const Dictionary& d, const std::string& v) {
+    for (size_t c = 0; c < d.values.size(); ++c)
+      if (d.values[c] == v) return static_cast<int32_t>(c);
+    return int32_t(-1);
+  };
+  const int32_t b = code_of(db.brand, brand), c = code_of(db.container, container);
+  if (b < 0 || c < 0) return {Q17ResultRow{}};
+  bo_tpch_q17_tables t{};
+  t.l_partkey = col<int32_t>(db.l_partkey);
+  t.l_quantity = col<int16_t>(db.l_quantity);
+  t.l_extendedprice = col<int32_t>(db.l_extendedprice);
+  t.n_lineitem = db.n_lineitem;
+  t.p_partkey = col<int32_t>(db.p_partkey);
+  t.p_brand = col<uint16_t>(db.p_brand);
+  t.p_container = col<uint16_t>(db.p_container);
+  t.n_part = db.n_part;
+  t.max_partkey = db.max_partkey;
+  int64_t sum = 0;
+  check(db.ctx, bo_tpch_q17(db.ctx, &t, b, c, &sum), "q17");
+  return {Q17ResultRow{sum}};
+}
+
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date) {
   // query_q14.cpp:189-200: the month [DATE, DATE + 1 month); no part keys: one zero row.
   const int16_t start = date_offset_of(date, db.base_date_days);
@@ -797,6 +823,15 @@ void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& r
     out << escape_csv(r.n_name) << ',' << static_cast<double>(r.revenue_raw) / static_cast<double>(kPriceScale) << "\n";
 }
 
+void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q17.cpp:311-321
+  out << "avg_yearly\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows)
+    out << static_cast<double>(r.sum_extendedprice_raw) / (7.0 * static_cast<double>(kPriceScale)) << "\n";
+}
+
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows) {
   std::ofstream out(filename);  // query_q14.cpp:367-374
   out << "promo_revenue\n";
@@ -850,6 +885,7 @@ Database::~Database() {
                           &o_shippriority, &o_totalprice, &orderkey_to_row, &o_li_begin, &o_li_end,
                           &o_comment, &o_comment_offsets, &o_orderpriority, &l_shipmode, &l_commit_receipt,
                           &l_shard_max_shipdate, &l_partkey, &p_promo_by_key, &l_supp_nation, &o_cust_nation,
+                          &p_partkey, &p_brand, &p_container,
                           &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
@@ -1127,11 +1163,17 @@ CustomerHost derive_customer(const ParquetTables::ArrowTable& C) {
 struct PartHost {
   std::vector<int8_t> promo_by_key;
   int32_t max_key = -1;
+  std::vector<int32_t> key;
+  std::vector<uint16_t> brand, container;
+  Dictionary brand_dict, container_dict;
 };
 
 PartHost derive_part(const ParquetTables::ArrowTable& P) {
   PartHost h;
-  const auto key = int_values(column(P, "p_partkey"));
+  h.key = int_values(column(P, "p_partkey"));
+  const auto& key = h.key;
+  h.brand = dictionary_codes(column(P, "p_brand"), h.brand_dict);
+  h.container = dictionary_codes(column(P, "p_container"), h.container_dict);
   Dictionary types;
   const auto type = dictionary_codes(column(P, "p_type"), types);
   if (key.empty()) return h;
@@ -1268,6 +1310,12 @@ Database* build(ParquetTables* tables) {
       db->max_partkey = h.max_key;
       db->n_promo_map = static_cast<int64_t>(h.promo_by_key.size());
       db->p_promo_by_key = upload(ctx, h.promo_by_key);
+      db->n_part = static_cast<int64_t>(h.key.size());
+      db->p_partkey = upload(ctx, h.key);
+      db->p_brand = upload(ctx, h.brand);
+      db->p_container = upload(ctx, h.container);
+      db->brand = std::move(h.brand_dict);
+      db->container = std::move(h.container_dict);
     }
     // nation names by key (bespoke_tpch/builder_impl.cpp:780-803; query_q10.cpp:497-515)
     {
@@ -1368,6 +1416,13 @@ void query(Database* db) {
       const auto rows = run_q5(*db, region, date);
       const auto end = std::chrono::steady_clock::now();
       write_q5_csv(file, rows);
+      report(end);
+    } else if (r.id == "17") {
+      const std::string brand = arg("BRAND");
+      const std::string container = arg("CONTAINER");
+      const auto rows = run_q17(*db, brand, container);
+      const auto end = std::chrono::steady_clock::now();
+      write_q17_csv(file, rows);
       report(end);
     } else if (r.id == "14") {
       const std::string date = arg("DATE");

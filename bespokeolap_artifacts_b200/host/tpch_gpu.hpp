@@ -100,6 +100,10 @@ struct Database {
   bo_tpch::DeviceColumn p_promo_by_key;
   int64_t n_promo_map = 0;
   int32_t max_partkey = -1;
+  // part rows: keys, brand and container codes (Q17)
+  bo_tpch::DeviceColumn p_partkey, p_brand, p_container;
+  int64_t n_part = 0;
+  bo_tpch::Dictionary brand, container;
   // nation names by nationkey in [0, nation_bound) (last row of each key)
   int32_t nation_bound = 1;
   std::vector<std::string> nation_name;
@@ -155,6 +159,10 @@ struct Q5ResultRow {
   int64_t revenue_raw = 0;
 };
 
+struct Q17ResultRow {
+  int64_t sum_extendedprice_raw = 0;
+};
+
 struct Q14ResultRow {
   double promo_revenue = 0.0;
 };
@@ -205,6 +213,7 @@ std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, con
 std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date);
 std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date);
 std::vector<Q5ResultRow> run_q5(const Database& db, const std::string& region, const std::string& date);
+std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container);
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date);
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
                                   const std::string& date);
@@ -217,6 +226,7 @@ void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& r
 void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows);
 void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& rows);
 void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& rows);
+void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows);
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows);
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);
 void write_q13_csv(const std::string& filename, const std::vector<Q13ResultRow>& rows);

@@ -233,6 +233,14 @@ class TpchQ5Tables(C.Structure):
                 ("n_lineitem", C.c_int64), ("lineitem_orderkey_sorted", C.c_int32), ("n_nations", C.c_int32)]
 
 
+class TpchQ17Tables(C.Structure):
+    """``bo_tpch_q17_tables``: lineitem partkeys, quantities, extended prices; part keys, brand and container
+    codes; the largest part key."""
+    _fields_ = [("l_partkey", C.c_void_p), ("l_quantity", C.c_void_p), ("l_extendedprice", C.c_void_p),
+                ("n_lineitem", C.c_int64), ("p_partkey", C.c_void_p), ("p_brand", C.c_void_p),
+                ("p_container", C.c_void_p), ("n_part", C.c_int64), ("max_partkey", C.c_int32), ("pad", C.c_int32)]
+
+
 class TpchQ14Tables(C.Structure):
     """``bo_tpch_q14_tables``: lineitem shipdates, partkeys, discounted prices; the part promo flag per key."""
     _fields_ = [("l_shipdate", C.c_void_p), ("l_partkey", C.c_void_p), ("l_discounted_price", C.c_void_p),
@@ -354,6 +362,7 @@ _SIGNATURES = {
                               C.POINTER(TpchQ10Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q4": (C.c_int, [_P, C.POINTER(TpchQ4Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q5": (C.c_int, [_P, C.POINTER(TpchQ5Tables), C.c_char_p, C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
+    "bo_tpch_q17": (C.c_int, [_P, C.POINTER(TpchQ17Tables), C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
     "bo_tpch_q14": (C.c_int, [_P, C.POINTER(TpchQ14Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,
                               C.c_int16, C.POINTER(C.c_int64)]),

@@ -28,6 +28,10 @@ Key layouts (they select the reference's code paths):
                     per-nation arrays by the customer's nationkey unchecked).
   n_supplier        suppliers 1..n with nations 0..24 (default: one
                     supplier, key 1, nation 0).
+  n_part            parts 1..n (default 150; lineitems name parts 1..199).
+                    The reference's Q17 reads its part bitmap at each
+                    lineitem's partkey unchecked (query_q17.cpp:205-259), so
+                    its parity data covers every lineitem partkey.
 Regions REGION0..REGION4 (keys 0..4; nations' regionkey = nationkey % 5) and
 a later row repeating REGION1 with key 9.
 Ship modes MODE_A..MODE_G; order priorities 1-URGENT and 2-HIGH (the two the
@@ -50,6 +54,8 @@ WORDS = ["ironic", "quick", "pending", "bold", 'say "hi"', "a,b", "deposits", ""
 SHIPMODES = ["MODE_A", "MODE_B", "MODE_C", "MODE_D", "MODE_E", "MODE_F", "MODE_G"]
 PRIORITIES = ["1-URGENT", "2-HIGH", "3-PRIO_C", "4-PRIO_D", "5-PRIO_E"]
 PART_TYPES = ["PROMO_A", "PROMO_B", "STD_A", "STD_B", "ECO_A", "PROMOTION", "PROM", "LARGE_PROMO"]
+BRANDS = ["BRAND_A", "BRAND_B", "BRAND_C", "BRAND_D", "BRAND_E"]
+CONTAINERS = ["CONT_A", "CONT_B", "CONT_C", "CONT_D"]
 D1992 = 8035  # 1992-01-01 in days since 1970-01-01
 
 
@@ -84,7 +90,7 @@ def _ragged_text(rng, n: int, max_words: int) -> list[str]:
 def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: int = 0,
                decimal: bool = False, order_keys: str = "sparse", customer_keys: str = "dense",
                shuffle_lineitem: bool = False, late_receipts: bool = False, customer_nations: str = "wide",
-               n_supplier: int = 1) -> Path:
+               n_supplier: int = 1, n_part: int = 150) -> Path:
     rng = np.random.default_rng(seed)
     rng2 = np.random.default_rng([seed, 12])
     out.mkdir(parents=True, exist_ok=True)
@@ -156,17 +162,19 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
         "l_comment": [""] * n,
     }), out / "lineitem.parquet")
     one = np.ones(1, np.int32)
-    # parts 1..150 (lineitems name 1..199, so some have no part) and a last row
-    # repeating key 3 with another type (the later row wins)
+    # parts 1..n_part (lineitems name 1..199, so by default some have no part)
+    # and a last row repeating key 3 with another type (the later row wins)
     rng3 = np.random.default_rng([seed, 14])
-    pkey = np.concatenate([np.arange(1, 151), [3]]).astype(np.int32)
-    n_part = len(pkey)
-    ptype = [PART_TYPES[i] for i in rng3.integers(0, len(PART_TYPES), n_part)]
+    pkey = np.concatenate([np.arange(1, n_part + 1), [3]]).astype(np.int32)
+    rows_p = len(pkey)
+    ptype = [PART_TYPES[i] for i in rng3.integers(0, len(PART_TYPES), rows_p)]
     ptype[-1] = "STD_A" if ptype[2].startswith("PROMO") else "PROMO_B"
-    pq.write_table(pa.table({"p_partkey": pkey, "p_name": [f"part {k}" for k in pkey], "p_mfgr": ["m"] * n_part,
-                             "p_brand": ["b"] * n_part, "p_type": ptype,
-                             "p_size": rng3.integers(1, 51, n_part).astype(np.int32), "p_container": ["c"] * n_part,
-                             "p_retailprice": _dec(np.ones(n_part), decimal), "p_comment": [""] * n_part}),
+    psize = rng3.integers(1, 51, rows_p).astype(np.int32)
+    pbrand = [BRANDS[i] for i in rng3.integers(0, len(BRANDS), rows_p)]
+    pcont = [CONTAINERS[i] for i in rng3.integers(0, len(CONTAINERS), rows_p)]
+    pq.write_table(pa.table({"p_partkey": pkey, "p_name": [f"part {k}" for k in pkey], "p_mfgr": ["m"] * rows_p,
+                             "p_brand": pbrand, "p_type": ptype, "p_size": psize, "p_container": pcont,
+                             "p_retailprice": _dec(np.ones(rows_p), decimal), "p_comment": [""] * rows_p}),
                    out / "part.parquet")
     if n_supplier <= 1:
         skey, snation = one, one * 0

@@ -672,6 +672,29 @@ typedef struct bo_tpch_q14_tables {
 int bo_tpch_q14(bo_ctx* ctx, const bo_tpch_q14_tables* tables, int16_t start_offset, int16_t end_offset,
                 int64_t sums_out[2]);
 
+/* TPC-H Q17 over the storage-plan layout: run_q17 of
+ * bespoke_tpch/query_q17.cpp:119-311.  Parts with keys in [0, max_partkey]
+ * of the given brand and container codes; the lineitems of those parts,
+ * their quantity sum and count per part; *sum_out = the sum of the
+ * extended prices of those lineitems with 5 * quantity * count < sum (the
+ * reference's integer form of quantity < 0.2 * avg).  Lineitem partkeys are
+ * read as unsigned and beyond max_partkey match no part. */
+typedef struct bo_tpch_q17_tables {
+  const int32_t* l_partkey;            /* 32-byte aligned */
+  const int16_t* l_quantity;
+  const int32_t* l_extendedprice;
+  int64_t n_lineitem;
+  const int32_t* p_partkey;
+  const uint16_t* p_brand;             /* dictionary codes */
+  const uint16_t* p_container;
+  int64_t n_part;
+  int32_t max_partkey;                 /* largest part key; < 0: none */
+  int32_t pad;
+} bo_tpch_q17_tables;
+
+int bo_tpch_q17(bo_ctx* ctx, const bo_tpch_q17_tables* tables, int32_t brand_code, int32_t container_code,
+                int64_t* sum_out);
+
 /* TPC-H Q12 over the storage-plan layout: run_q12 of
  * bespoke_tpch/query_q12.cpp:162-360.  Lineitems whose shipmode code is
  * mode_code1 or mode_code2 (-1: none), with shipdate < commitdate <
