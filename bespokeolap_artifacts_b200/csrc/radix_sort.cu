@@ -100,6 +100,24 @@ __global__ void __launch_bounds__(kSortBlock) radix_pass_kernel(
   // Blocks beyond the tiles the actual count needs retire without a ticket
   // (block 0 always stays, and the staying blocks take every tile in order).
   if ((int64_t)blockIdx.x * kSortTile >= n) return;
+  // A pass over a digit that every key shares (one non-empty bin) is the
+  // identity permutation: the tiles are copied in place of ranking and
+  // look-back.  Result sets of a few thousand keys sorted by 64-bit keys
+  // have several such passes (complemented or narrow fields).
+  {
+    const unsigned long long lo = digit_base[threadIdx.x];
+    const unsigned long long hi = threadIdx.x + 1 < kRadix ? digit_base[threadIdx.x + 1] : (unsigned long long)n;
+    if (__syncthreads_count(hi > lo) == 1) {
+      for (int64_t t = blockIdx.x; t * kSortTile < n; t += gridDim.x) {
+        const int64_t end = min((t + 1) * (int64_t)kSortTile, n);
+        for (int64_t i = t * kSortTile + threadIdx.x; i < end; i += kSortBlock) {
+          kout[i] = kin[i];
+          vout[i] = vin[i];
+        }
+      }
+      return;
+    }
+  }
   __shared__ uint32_t warp_cnt[kSortWarps][kRadix];
   __shared__ unsigned long long tile_base[kRadix];
   __shared__ uint32_t tile_s;
