@@ -1,2 +1,3 @@
 """The drop-in tests' Parquet writer (bespokeolap_artifacts_b200.tpch_data)."""
-from bespokeolap_artifacts_b200.tpch_data import PART_TYPES, PRIORITIES, SEGMENTS, SHIPMODES, WORDS, write_tpch  # noqa: F401
+from bespokeolap_artifacts_b200.tpch_data import (  # noqa: F401
+    BRANDS, CONTAINERS, PART_TYPES, PRIORITIES, SEGMENTS, SHIPMODES, WORDS, write_tpch)
