@@ -558,6 +558,79 @@ std::vector<Q5ResultRow> run_q5(const Database& db, const std::string& region, c
   return rows;
 }
 
+std::vector<Q7ResultRow> run_q7(const Database& db, const std::string& nation1, const std::string& nation2) {
+  // query_q7.cpp:141-199: both names' keys (the first nation row of a name),
+  // the window 1995-01-01 .. 1996-12-31, supplier tags by supplier row.
+  auto key_of = [&](const std::string& name, int32_t& key) {
+    for (size_t i = 0; i < db.nation_row_name.size(); ++i)
+      if (db.nation_row_name[i] == name) {
+        key = db.nation_key[i];
+        return true;
+      }
+    return false;
+  };
+  int32_t n1 = 0, n2 = 0;
+  if (!key_of(nation1, n1) || !key_of(nation2, n2)) return {};
+  const bool same = n1 == n2;
+  const int16_t start = date_offset_of("1995-01-01", db.base_date_days);
+  const int16_t last = date_offset_of("1996-12-31", db.base_date_days);
+  const int16_t year2 = date_offset_of("1996-01-01", db.base_date_days);
+  int32_t max_suppkey = -1;
+  for (int32_t k : db.s_suppkey) max_suppkey = std::max(max_suppkey, k);
+  std::vector<int8_t> tag(max_suppkey >= 0 ? static_cast<size_t>(max_suppkey) + 1 : 0, int8_t(-1));
+  for (size_t i = 0; i < db.s_suppkey.size(); ++i) {
+    const int32_t k = db.s_suppkey[i];
+    if (k < 0) continue;
+    if (db.s_nationkey[i] == n1)
+      tag[static_cast<size_t>(k)] = 0;
+    else if (!same && db.s_nationkey[i] == n2)
+      tag[static_cast<size_t>(k)] = 1;
+  }
+  bo_tpch_q7_tables t{};
+  t.l_shipdate = col<int16_t>(db.l_shipdate);
+  t.l_suppkey = col<int32_t>(db.l_suppkey);
+  t.l_orderkey = col<int32_t>(db.l_orderkey);
+  t.l_discounted_price = col<int32_t>(db.l_discounted_price);
+  t.n_lineitem = db.n_lineitem;
+  t.orderkey_to_row = col<int32_t>(db.orderkey_to_row);
+  t.n_orderkey_map = db.n_orderkey_map;
+  t.o_cust_nation = col<int16_t>(db.o_cust_nation);
+  t.n_orders = db.n_orders;
+  int64_t revenue[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  check(db.ctx,
+        bo_tpch_q7(db.ctx, &t, tag.data(), static_cast<int64_t>(tag.size()), n1, n2, start, last, year2, revenue),
+        "q7");
+  // Rows per (supplier nation, customer nation, year) with a non-zero sum,
+  // named by the first nation row of each key (:372-412).
+  auto name_of = [&](int32_t key, const std::string** out) {
+    for (size_t i = 0; i < db.nation_key.size(); ++i)
+      if (db.nation_key[i] == key) {
+        *out = &db.nation_row_name[i];
+        return true;
+      }
+    return false;
+  };
+  const int32_t nations[2] = {n1, n2};
+  const int count = same ? 1 : 2;
+  std::vector<Q7ResultRow> rows;
+  for (int s = 0; s < count; ++s)
+    for (int c = 0; c < count; ++c) {
+      if (same ? (s != 0 || c != 0) : s == c) continue;
+      const std::string *sn = nullptr, *cn = nullptr;
+      if (!name_of(nations[s], &sn) || !name_of(nations[c], &cn)) continue;
+      for (int y = 0; y < 2; ++y) {
+        const int64_t v = revenue[s * 4 + c * 2 + y];
+        if (v != 0) rows.push_back(Q7ResultRow{*sn, *cn, y == 0 ? 1995 : 1996, v});
+      }
+    }
+  std::sort(rows.begin(), rows.end(), [](const Q7ResultRow& a, const Q7ResultRow& b) {
+    if (a.supp_nation != b.supp_nation) return a.supp_nation < b.supp_nation;
+    if (a.cust_nation != b.cust_nation) return a.cust_nation < b.cust_nation;
+    return a.l_year < b.l_year;
+  });
+  return rows;
+}
+
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container) {
   // query_q17.cpp:125-155: NULL arguments, no parts, or an unknown brand or
   // container give a zero row.
@@ -823,6 +896,16 @@ void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& r
     out << escape_csv(r.n_name) << ',' << static_cast<double>(r.revenue_raw) / static_cast<double>(kPriceScale) << "\n";
 }
 
+void write_q7_csv(const std::string& filename, const std::vector<Q7ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q7.cpp:425-435
+  out << "supp_nation,cust_nation,l_year,revenue\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows)
+    out << escape_csv(r.supp_nation) << ',' << escape_csv(r.cust_nation) << ',' << r.l_year << ','
+        << static_cast<double>(r.revenue_raw) / kPriceScale << "\n";
+}
+
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows) {
   std::ofstream out(filename);  // query_q17.cpp:311-321
   out << "avg_yearly\n";
@@ -885,7 +968,7 @@ Database::~Database() {
                           &o_shippriority, &o_totalprice, &orderkey_to_row, &o_li_begin, &o_li_end,
                           &o_comment, &o_comment_offsets, &o_orderpriority, &l_shipmode, &l_commit_receipt,
                           &l_shard_max_shipdate, &l_partkey, &p_promo_by_key, &l_supp_nation, &o_cust_nation,
-                          &p_partkey, &p_brand, &p_container,
+                          &p_partkey, &p_brand, &p_container, &l_suppkey,
                           &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
@@ -952,7 +1035,7 @@ namespace {
 
 // Host-side storage-plan columns of one table, derived before the upload.
 struct LineitemHost {
-  std::vector<int32_t> orderkey, price, dprice, partkey;
+  std::vector<int32_t> orderkey, price, dprice, partkey, suppkey;
   std::vector<int16_t> ship, q16, shard_max_ship, supp_nation;
   std::vector<uint8_t> code, d8, t8;
   std::vector<uint16_t> shipmode;
@@ -1082,6 +1165,7 @@ LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, const ParquetTa
     h.max_orderkey = std::max(h.max_orderkey, h.orderkey[i]);
   }
   h.partkey = int_values(column(L, "l_partkey"));
+  h.suppkey = int_values(column(L, "l_suppkey"));
   h.supp_nation = supp_nation.get();
   h.commit_receipt = commit_receipt.get();
   auto sm = shipmode.get();
@@ -1242,6 +1326,7 @@ Database* build(ParquetTables* tables) {
       if (!h.shard_max_ship.empty()) db->l_shard_max_shipdate = upload(ctx, h.shard_max_ship);
       db->l_partkey = upload(ctx, h.partkey);
       db->l_supp_nation = upload(ctx, h.supp_nation);
+      db->l_suppkey = upload(ctx, h.suppkey);
       phase("lineitem uploaded");
     }
     std::vector<int32_t> order_custkeys;  // date-sorted orders' custkeys, for orders.cust_nationkey
@@ -1330,6 +1415,12 @@ Database* build(ParquetTables* tables) {
         if (key[i] >= 0) db->nation_name[static_cast<size_t>(key[i])] = std::string(name.view(i));
       db->nation_key = key;
       db->nation_regionkey = int_values(column(N, "n_regionkey"));
+      for (size_t i = 0; i < key.size(); ++i) db->nation_row_name.emplace_back(name.view(i));
+    }
+    {
+      const auto& S = tables->supplier;
+      db->s_suppkey = int_values(column(S, "s_suppkey"));
+      db->s_nationkey = int_values(column(S, "s_nationkey"));
     }
     {  // region name -> key, the first row of a name (builder_impl.cpp:805-826)
       const auto& R = tables->region;
@@ -1416,6 +1507,13 @@ void query(Database* db) {
       const auto rows = run_q5(*db, region, date);
       const auto end = std::chrono::steady_clock::now();
       write_q5_csv(file, rows);
+      report(end);
+    } else if (r.id == "7") {
+      const std::string nation1 = arg("NATION1");
+      const std::string nation2 = arg("NATION2");
+      const auto rows = run_q7(*db, nation1, nation2);
+      const auto end = std::chrono::steady_clock::now();
+      write_q7_csv(file, rows);
       report(end);
     } else if (r.id == "17") {
       const std::string brand = arg("BRAND");

@@ -72,7 +72,7 @@ struct Database {
   // lineitem (row order of the input)
   int64_t n_lineitem = 0;
   bo_tpch::DeviceColumn l_orderkey, l_shipdate, l_returnflag_linestatus, l_extendedprice, l_discounted_price,
-      l_discount, l_tax, l_quantity, l_shipmode, l_commit_receipt, l_partkey, l_supp_nation;
+      l_discount, l_tax, l_quantity, l_shipmode, l_commit_receipt, l_partkey, l_supp_nation, l_suppkey;
   // Latest shipdate of each lineitem's builder shard; only built when some
   // lineitem is received more than 30 days after shipping (Q12's shard pruning).
   bo_tpch::DeviceColumn l_shard_max_shipdate;
@@ -107,8 +107,11 @@ struct Database {
   // nation names by nationkey in [0, nation_bound) (last row of each key)
   int32_t nation_bound = 1;
   std::vector<std::string> nation_name;
-  // nation rows' keys and region keys; region name -> key (first row of a name)
+  // nation rows' keys, region keys and names; region name -> key (first row of a name)
   std::vector<int32_t> nation_key, nation_regionkey;
+  std::vector<std::string> nation_row_name;
+  // supplier rows' keys and nationkeys (Q7's supplier tags)
+  std::vector<int32_t> s_suppkey, s_nationkey;
   std::unordered_map<std::string, int32_t> region_key_by_name;
   // Result record of the last scan-agg / Q6 query.  Queries on one Database
   // run one at a time (as the reference's single-threaded query()).
@@ -156,6 +159,13 @@ struct Q4ResultRow {
 
 struct Q5ResultRow {
   std::string n_name;
+  int64_t revenue_raw = 0;
+};
+
+struct Q7ResultRow {
+  std::string supp_nation;
+  std::string cust_nation;
+  int32_t l_year = 0;
   int64_t revenue_raw = 0;
 };
 
@@ -213,6 +223,7 @@ std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, con
 std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date);
 std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date);
 std::vector<Q5ResultRow> run_q5(const Database& db, const std::string& region, const std::string& date);
+std::vector<Q7ResultRow> run_q7(const Database& db, const std::string& nation1, const std::string& nation2);
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container);
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date);
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
@@ -226,6 +237,7 @@ void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& r
 void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows);
 void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& rows);
 void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& rows);
+void write_q7_csv(const std::string& filename, const std::vector<Q7ResultRow>& rows);
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows);
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows);
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);

@@ -233,6 +233,14 @@ class TpchQ5Tables(C.Structure):
                 ("n_lineitem", C.c_int64), ("lineitem_orderkey_sorted", C.c_int32), ("n_nations", C.c_int32)]
 
 
+class TpchQ7Tables(C.Structure):
+    """``bo_tpch_q7_tables``: lineitem shipdates, suppkeys, orderkeys, discounted prices; the orderkey map and
+    orders' customer nations."""
+    _fields_ = [("l_shipdate", C.c_void_p), ("l_suppkey", C.c_void_p), ("l_orderkey", C.c_void_p),
+                ("l_discounted_price", C.c_void_p), ("n_lineitem", C.c_int64), ("orderkey_to_row", C.c_void_p),
+                ("n_orderkey_map", C.c_int64), ("o_cust_nation", C.c_void_p), ("n_orders", C.c_int64)]
+
+
 class TpchQ17Tables(C.Structure):
     """``bo_tpch_q17_tables``: lineitem partkeys, quantities, extended prices; part keys, brand and container
     codes; the largest part key."""
@@ -362,6 +370,8 @@ _SIGNATURES = {
                               C.POINTER(TpchQ10Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q4": (C.c_int, [_P, C.POINTER(TpchQ4Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q5": (C.c_int, [_P, C.POINTER(TpchQ5Tables), C.c_char_p, C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
+    "bo_tpch_q7": (C.c_int, [_P, C.POINTER(TpchQ7Tables), C.c_char_p, C.c_int64, C.c_int32, C.c_int32, C.c_int16,
+                             C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q17": (C.c_int, [_P, C.POINTER(TpchQ17Tables), C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
     "bo_tpch_q14": (C.c_int, [_P, C.POINTER(TpchQ14Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,

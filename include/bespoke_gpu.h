@@ -672,6 +672,31 @@ typedef struct bo_tpch_q14_tables {
 int bo_tpch_q14(bo_ctx* ctx, const bo_tpch_q14_tables* tables, int16_t start_offset, int16_t end_offset,
                 int64_t sums_out[2]);
 
+/* TPC-H Q7 over the storage-plan layout: run_q7 of
+ * bespoke_tpch/query_q7.cpp:140-435.  Lineitems shipped in [ship_start,
+ * ship_last] (both ends included) whose supplier is tagged (supp_tag_host:
+ * per suppkey 0 = the first nation, 1 = the second, -1 = neither, the
+ * reference's supp_tag :170-181) and whose order's customer nation
+ * (o_cust_nation) is nation1 (0) or, when the nations differ, nation2 (1);
+ * pairs of the same nation count only when nation1 == nation2.  The
+ * discounted price is summed into revenue_out[supp * 4 + cust * 2 + year],
+ * year 1 from year2_start on.  Suppkeys outside the tag table are untagged. */
+typedef struct bo_tpch_q7_tables {
+  const int16_t* l_shipdate;           /* 16-byte aligned */
+  const int32_t* l_suppkey;
+  const int32_t* l_orderkey;
+  const int32_t* l_discounted_price;
+  int64_t n_lineitem;
+  const int32_t* orderkey_to_row;
+  int64_t n_orderkey_map;
+  const int16_t* o_cust_nation;
+  int64_t n_orders;
+} bo_tpch_q7_tables;
+
+int bo_tpch_q7(bo_ctx* ctx, const bo_tpch_q7_tables* tables, const int8_t* supp_tag_host, int64_t n_supp_tag,
+               int32_t nation1, int32_t nation2, int16_t ship_start, int16_t ship_last, int16_t year2_start,
+               int64_t revenue_out[8]);
+
 /* TPC-H Q17 over the storage-plan layout: run_q17 of
  * bespoke_tpch/query_q17.cpp:119-311.  Parts with keys in [0, max_partkey]
  * of the given brand and container codes; the lineitems of those parts,

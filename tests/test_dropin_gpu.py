@@ -89,6 +89,8 @@ def test_dropin_matches_reference_driver(tmp_path, layout):
 
 Q5_REQUESTS = ['5 "REGION0" "1994-01-01"', '5 "REGION1" "1995-02-28"', '5 "REGION4" "1996-02-29"',
                '5 "NOSUCH" "1994-01-01"', '5 "REGION3" "1999-01-01"', '5 "REGION2" "1992-01-01"',
+               '7 "NATION_01" "NATION_10"', '7 "NATION_03" "NATION_03"', '7 "NATION_07" "NATION_02"',
+               '7 "NATION_24" "NATION_00"', '7 "NATION_10" "NATION_01"',
                '17 "BRAND_B" "CONT_C"', '17 "BRAND_E" "CONT_A"', '17 "NOSUCH" "CONT_A"', '17 "<<NULL>>" "CONT_A"',
                '17 "BRAND_A" "<<NULL>>"']
 
@@ -100,11 +102,13 @@ Q5_LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem): 
 
 @pytest.mark.parametrize("layout", Q5_LAYOUTS, ids=lambda l: "-".join(map(str, l)))
 def test_dropin_q5_matches_reference_driver(tmp_path, layout):
-    """Q5 and Q17 (with every other request) on data whose customer
-    nationkeys lie in the nation table's key range and whose parts cover every
-    lineitem partkey: the reference's run_q5 indexes its per-nation arrays by
-    customer nations unchecked (query_q5.cpp:337-338, 423-424), run_q17 its
-    part bitmap by lineitem partkeys (query_q17.cpp:205-259)."""
+    """Q5, Q7 and Q17 (with every other request) on data whose customer
+    nationkeys lie in the nation table's key range, whose suppliers cover every
+    lineitem suppkey and whose parts cover every lineitem partkey: the
+    reference's run_q5 indexes its per-nation arrays by customer nations
+    unchecked (query_q5.cpp:337-338, 423-424), run_q7 its supplier tags by
+    lineitem suppkeys (query_q7.cpp:275, 322), run_q17 its part bitmap
+    by lineitem partkeys (query_q17.cpp:205-259)."""
     if not REF_DRIVER.exists() or not GPU_DRIVER.exists():
         pytest.skip("drivers not built")
     seed, decimal, order_keys, customer_keys, shuffle = layout
