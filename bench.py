@@ -918,6 +918,7 @@ def serving_section(eng, stream, join_sizer=None, gb_sizer=None, rates=(50, 500,
 TPCH_REQUESTS = [  # synthetic parameters: segments, ship modes and comment words of the seeded generator
     ("1", '1 "90"'), ("3", '3 "SEG_B" "1995-03-17"'), ("4", '4 "1993-07-01"'), ("5", '5 "REGION0" "1994-01-01"'),
     ("6", '6 "1994-02-01" "0.07" "23"'), ("7", '7 "NATION_01" "NATION_10"'),
+    ("8", '8 "NATION_10" "REGION0" "STD_B"'),
     ("10", '10 "1993-10-01"'), ("12", '12 "MODE_A" "MODE_C" "1994-01-01"'), ("13", '13 "pending" "deposits"'),
     ("14", '14 "1995-09-01"'), ("17", '17 "BRAND_B" "CONT_C"'), ("18", '18 "250"'),
 ]

@@ -631,6 +631,72 @@ std::vector<Q7ResultRow> run_q7(const Database& db, const std::string& nation1, 
   return rows;
 }
 
+std::vector<Q8ResultRow> run_q8(const Database& db, const std::string& nation, const std::string& region,
+                                const std::string& type) {
+  // query_q8.cpp:123-198: the region's and the nation's keys (first row of a
+  // name), the window 1995-01-01 .. 1996-12-31, the region's nations, the
+  // target nation's suppliers, the type's code.
+  const auto rit = db.region_key_by_name.find(region);
+  if (rit == db.region_key_by_name.end()) return {};
+  int32_t target = 0;
+  bool found = false;
+  for (size_t i = 0; i < db.nation_row_name.size() && !found; ++i)
+    if (db.nation_row_name[i] == nation) {
+      target = db.nation_key[i];
+      found = true;
+    }
+  if (!found) return {};
+  const int16_t start = date_offset_of("1995-01-01", db.base_date_days);
+  const int16_t last = date_offset_of("1996-12-31", db.base_date_days);
+  const int16_t year2 = date_offset_of("1996-01-01", db.base_date_days);
+  std::vector<uint8_t> in_region(static_cast<size_t>(db.nation_bound), 0);
+  for (size_t i = 0; i < db.nation_key.size(); ++i)
+    if (db.nation_key[i] >= 0 && db.nation_key[i] < db.nation_bound && db.nation_regionkey[i] == rit->second)
+      in_region[static_cast<size_t>(db.nation_key[i])] = 1;
+  int32_t max_suppkey = -1;
+  for (int32_t k : db.s_suppkey) max_suppkey = std::max(max_suppkey, k);
+  std::vector<uint8_t> supp(max_suppkey >= 0 ? static_cast<size_t>(max_suppkey) + 1 : 0, 0);
+  for (size_t i = 0; i < db.s_suppkey.size(); ++i)
+    if (db.s_suppkey[i] >= 0 && db.s_nationkey[i] == target) supp[static_cast<size_t>(db.s_suppkey[i])] = 1;
+  int32_t type_code = -1;
+  for (size_t c = 0; c < db.part_type.values.size(); ++c)
+    if (db.part_type.values[c] == type) {
+      type_code = static_cast<int32_t>(c);
+      break;
+    }
+  bo_tpch_q8_tables t{};
+  t.l_partkey = col<int32_t>(db.l_partkey);
+  t.l_suppkey = col<int32_t>(db.l_suppkey);
+  t.l_orderkey = col<int32_t>(db.l_orderkey);
+  t.l_extendedprice = col<int32_t>(db.l_extendedprice);
+  t.l_discount = col<uint8_t>(db.l_discount);
+  t.n_lineitem = db.n_lineitem;
+  t.orderkey_to_row = col<int32_t>(db.orderkey_to_row);
+  t.n_orderkey_map = db.n_orderkey_map;
+  t.o_custkey = col<int32_t>(db.o_custkey);
+  t.o_orderdate = col<int16_t>(db.o_orderdate);
+  t.n_orders = db.n_orders;
+  t.c_custkey = col<int32_t>(db.c_custkey);
+  t.c_nationkey = col<int32_t>(db.c_nationkey);
+  t.n_customer = db.n_customer;
+  t.max_custkey = db.custkey_bound - 1;
+  t.max_partkey = db.max_partkey;
+  t.p_partkey = col<int32_t>(db.p_partkey);
+  t.p_type = col<uint16_t>(db.p_type);
+  t.n_part = db.n_part;
+  int64_t sums[4] = {0, 0, 0, 0};
+  check(db.ctx,
+        bo_tpch_q8(db.ctx, &t, in_region.data(), static_cast<int32_t>(in_region.size()), supp.data(),
+                   static_cast<int64_t>(supp.size()), type_code, start, last, year2, sums),
+        "q8");
+  // One row per year with a non-zero total, share = nation / total (:364-378).
+  std::vector<Q8ResultRow> rows;
+  for (int y = 0; y < 2; ++y)
+    if (sums[2 + y] != 0)
+      rows.push_back(Q8ResultRow{1995 + y, static_cast<double>(sums[y]) / static_cast<double>(sums[2 + y])});
+  return rows;
+}
+
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container) {
   // query_q17.cpp:125-155: NULL arguments, no parts, or an unknown brand or
   // container give a zero row.
@@ -906,6 +972,14 @@ void write_q7_csv(const std::string& filename, const std::vector<Q7ResultRow>& r
         << static_cast<double>(r.revenue_raw) / kPriceScale << "\n";
 }
 
+void write_q8_csv(const std::string& filename, const std::vector<Q8ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q8.cpp:382-389
+  out << "o_year,mkt_share\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows) out << r.o_year << "," << r.mkt_share << "\n";
+}
+
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows) {
   std::ofstream out(filename);  // query_q17.cpp:311-321
   out << "avg_yearly\n";
@@ -968,7 +1042,7 @@ Database::~Database() {
                           &o_shippriority, &o_totalprice, &orderkey_to_row, &o_li_begin, &o_li_end,
                           &o_comment, &o_comment_offsets, &o_orderpriority, &l_shipmode, &l_commit_receipt,
                           &l_shard_max_shipdate, &l_partkey, &p_promo_by_key, &l_supp_nation, &o_cust_nation,
-                          &p_partkey, &p_brand, &p_container, &l_suppkey,
+                          &p_partkey, &p_brand, &p_container, &l_suppkey, &p_type,
                           &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
@@ -1248,8 +1322,8 @@ struct PartHost {
   std::vector<int8_t> promo_by_key;
   int32_t max_key = -1;
   std::vector<int32_t> key;
-  std::vector<uint16_t> brand, container;
-  Dictionary brand_dict, container_dict;
+  std::vector<uint16_t> brand, container, type;
+  Dictionary brand_dict, container_dict, type_dict;
 };
 
 PartHost derive_part(const ParquetTables::ArrowTable& P) {
@@ -1258,8 +1332,9 @@ PartHost derive_part(const ParquetTables::ArrowTable& P) {
   const auto& key = h.key;
   h.brand = dictionary_codes(column(P, "p_brand"), h.brand_dict);
   h.container = dictionary_codes(column(P, "p_container"), h.container_dict);
-  Dictionary types;
-  const auto type = dictionary_codes(column(P, "p_type"), types);
+  h.type = dictionary_codes(column(P, "p_type"), h.type_dict);
+  const auto& type = h.type;
+  const Dictionary& types = h.type_dict;
   if (key.empty()) return h;
   h.max_key = *std::max_element(key.begin(), key.end());
   if (h.max_key < 0) return h;
@@ -1401,6 +1476,8 @@ Database* build(ParquetTables* tables) {
       db->p_container = upload(ctx, h.container);
       db->brand = std::move(h.brand_dict);
       db->container = std::move(h.container_dict);
+      db->p_type = upload(ctx, h.type);
+      db->part_type = std::move(h.type_dict);
     }
     // nation names by key (bespoke_tpch/builder_impl.cpp:780-803; query_q10.cpp:497-515)
     {
@@ -1514,6 +1591,14 @@ void query(Database* db) {
       const auto rows = run_q7(*db, nation1, nation2);
       const auto end = std::chrono::steady_clock::now();
       write_q7_csv(file, rows);
+      report(end);
+    } else if (r.id == "8") {
+      const std::string nation = arg("NATION");
+      const std::string region = arg("REGION");
+      const std::string type = arg("TYPE");
+      const auto rows = run_q8(*db, nation, region, type);
+      const auto end = std::chrono::steady_clock::now();
+      write_q8_csv(file, rows);
       report(end);
     } else if (r.id == "17") {
       const std::string brand = arg("BRAND");

@@ -101,9 +101,9 @@ struct Database {
   int64_t n_promo_map = 0;
   int32_t max_partkey = -1;
   // part rows: keys, brand and container codes (Q17)
-  bo_tpch::DeviceColumn p_partkey, p_brand, p_container;
+  bo_tpch::DeviceColumn p_partkey, p_brand, p_container, p_type;
   int64_t n_part = 0;
-  bo_tpch::Dictionary brand, container;
+  bo_tpch::Dictionary brand, container, part_type;
   // nation names by nationkey in [0, nation_bound) (last row of each key)
   int32_t nation_bound = 1;
   std::vector<std::string> nation_name;
@@ -169,6 +169,11 @@ struct Q7ResultRow {
   int64_t revenue_raw = 0;
 };
 
+struct Q8ResultRow {
+  int32_t o_year = 0;
+  double mkt_share = 0.0;
+};
+
 struct Q17ResultRow {
   int64_t sum_extendedprice_raw = 0;
 };
@@ -224,6 +229,8 @@ std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date);
 std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date);
 std::vector<Q5ResultRow> run_q5(const Database& db, const std::string& region, const std::string& date);
 std::vector<Q7ResultRow> run_q7(const Database& db, const std::string& nation1, const std::string& nation2);
+std::vector<Q8ResultRow> run_q8(const Database& db, const std::string& nation, const std::string& region,
+                                const std::string& type);
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container);
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date);
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
@@ -238,6 +245,7 @@ void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>&
 void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& rows);
 void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& rows);
 void write_q7_csv(const std::string& filename, const std::vector<Q7ResultRow>& rows);
+void write_q8_csv(const std::string& filename, const std::vector<Q8ResultRow>& rows);
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows);
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows);
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);

@@ -241,6 +241,17 @@ class TpchQ7Tables(C.Structure):
                 ("n_orderkey_map", C.c_int64), ("o_cust_nation", C.c_void_p), ("n_orders", C.c_int64)]
 
 
+class TpchQ8Tables(C.Structure):
+    """``bo_tpch_q8_tables``: lineitem part/supp/order keys, prices, discounts; the orderkey map, orders'
+    custkeys and dates; customer keys and nations; part keys and type codes."""
+    _fields_ = [("l_partkey", C.c_void_p), ("l_suppkey", C.c_void_p), ("l_orderkey", C.c_void_p),
+                ("l_extendedprice", C.c_void_p), ("l_discount", C.c_void_p), ("n_lineitem", C.c_int64),
+                ("orderkey_to_row", C.c_void_p), ("n_orderkey_map", C.c_int64), ("o_custkey", C.c_void_p),
+                ("o_orderdate", C.c_void_p), ("n_orders", C.c_int64), ("c_custkey", C.c_void_p),
+                ("c_nationkey", C.c_void_p), ("n_customer", C.c_int64), ("max_custkey", C.c_int32),
+                ("max_partkey", C.c_int32), ("p_partkey", C.c_void_p), ("p_type", C.c_void_p), ("n_part", C.c_int64)]
+
+
 class TpchQ17Tables(C.Structure):
     """``bo_tpch_q17_tables``: lineitem partkeys, quantities, extended prices; part keys, brand and container
     codes; the largest part key."""
@@ -372,6 +383,8 @@ _SIGNATURES = {
     "bo_tpch_q5": (C.c_int, [_P, C.POINTER(TpchQ5Tables), C.c_char_p, C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q7": (C.c_int, [_P, C.POINTER(TpchQ7Tables), C.c_char_p, C.c_int64, C.c_int32, C.c_int32, C.c_int16,
                              C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
+    "bo_tpch_q8": (C.c_int, [_P, C.POINTER(TpchQ8Tables), C.c_char_p, C.c_int32, C.c_char_p, C.c_int64, C.c_int32,
+                             C.c_int16, C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q17": (C.c_int, [_P, C.POINTER(TpchQ17Tables), C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
     "bo_tpch_q14": (C.c_int, [_P, C.POINTER(TpchQ14Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,

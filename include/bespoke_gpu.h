@@ -697,6 +697,42 @@ int bo_tpch_q7(bo_ctx* ctx, const bo_tpch_q7_tables* tables, const int8_t* supp_
                int32_t nation1, int32_t nation2, int16_t ship_start, int16_t ship_last, int16_t year2_start,
                int64_t revenue_out[8]);
 
+/* TPC-H Q8 over the storage-plan layout: run_q8 of
+ * bespoke_tpch/query_q8.cpp:122-380.  Lineitems of parts of the given type
+ * code whose order (through orderkey_to_row) is dated in [date_start,
+ * date_last] and placed by a customer of a nation in the region
+ * (nation_in_region_host, n_nations bytes; a custkey qualifies when any of
+ * its customer rows does, :160-167): the volume extendedprice *
+ * (100 - discount) summed per order year (index 1 from year2_start on) into
+ * sums_out[2 + year], and into sums_out[year] when the lineitem's supplier
+ * is of the target nation (supp_target_host, per suppkey, :169-176).
+ * Keys outside a table match nothing. */
+typedef struct bo_tpch_q8_tables {
+  const int32_t* l_partkey;            /* 32-byte aligned */
+  const int32_t* l_suppkey;
+  const int32_t* l_orderkey;
+  const int32_t* l_extendedprice;
+  const uint8_t* l_discount;
+  int64_t n_lineitem;
+  const int32_t* orderkey_to_row;
+  int64_t n_orderkey_map;
+  const int32_t* o_custkey;
+  const int16_t* o_orderdate;
+  int64_t n_orders;
+  const int32_t* c_custkey;
+  const int32_t* c_nationkey;
+  int64_t n_customer;
+  int32_t max_custkey;                 /* < 0: no customers */
+  int32_t max_partkey;                 /* < 0: no parts */
+  const int32_t* p_partkey;
+  const uint16_t* p_type;              /* dictionary codes */
+  int64_t n_part;
+} bo_tpch_q8_tables;
+
+int bo_tpch_q8(bo_ctx* ctx, const bo_tpch_q8_tables* tables, const uint8_t* nation_in_region_host, int32_t n_nations,
+               const uint8_t* supp_target_host, int64_t n_supp, int32_t type_code, int16_t date_start,
+               int16_t date_last, int16_t year2_start, int64_t sums_out[4]);
+
 /* TPC-H Q17 over the storage-plan layout: run_q17 of
  * bespoke_tpch/query_q17.cpp:119-311.  Parts with keys in [0, max_partkey]
  * of the given brand and container codes; the lineitems of those parts,

@@ -91,6 +91,8 @@ Q5_REQUESTS = ['5 "REGION0" "1994-01-01"', '5 "REGION1" "1995-02-28"', '5 "REGIO
                '5 "NOSUCH" "1994-01-01"', '5 "REGION3" "1999-01-01"', '5 "REGION2" "1992-01-01"',
                '7 "NATION_01" "NATION_10"', '7 "NATION_03" "NATION_03"', '7 "NATION_07" "NATION_02"',
                '7 "NATION_24" "NATION_00"', '7 "NATION_10" "NATION_01"',
+               '8 "NATION_03" "REGION3" "PROMO_A"', '8 "NATION_10" "REGION0" "STD_B"', '8 "NOSUCH" "REGION0" "STD_B"',
+               '8 "NATION_01" "NOSUCH" "STD_B"', '8 "NATION_02" "REGION2" "NOSUCH"', '8 "NATION_05" "REGION1" "PROM"',
                '17 "BRAND_B" "CONT_C"', '17 "BRAND_E" "CONT_A"', '17 "NOSUCH" "CONT_A"', '17 "<<NULL>>" "CONT_A"',
                '17 "BRAND_A" "<<NULL>>"']
 
@@ -102,7 +104,7 @@ Q5_LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem): 
 
 @pytest.mark.parametrize("layout", Q5_LAYOUTS, ids=lambda l: "-".join(map(str, l)))
 def test_dropin_q5_matches_reference_driver(tmp_path, layout):
-    """Q5, Q7 and Q17 (with every other request) on data whose customer
+    """Q5, Q7, Q8 and Q17 (with every other request) on data whose customer
     nationkeys lie in the nation table's key range, whose suppliers cover every
     lineitem suppkey and whose parts cover every lineitem partkey: the
     reference's run_q5 indexes its per-nation arrays by customer nations
