@@ -921,6 +921,7 @@ TPCH_REQUESTS = [  # synthetic parameters: segments, ship modes and comment word
     ("8", '8 "NATION_10" "REGION0" "STD_B"'),
     ("10", '10 "1993-10-01"'), ("12", '12 "MODE_A" "MODE_C" "1994-01-01"'), ("13", '13 "pending" "deposits"'),
     ("14", '14 "1995-09-01"'), ("17", '17 "BRAND_B" "CONT_C"'), ("18", '18 "250"'),
+    ("22", '22 "13" "31" "23" "29" "30" "18" "17"'),
 ]
 
 
@@ -965,7 +966,7 @@ def tpch_section(reps: int = 10, n_customer: int = 150_000, n_orders: int = 1_50
     try:
         t0 = time.perf_counter()
         data = write_tpch(tmp / "data", n_customer=n_customer, n_orders=n_orders, seed=11, customer_nations="known",
-                          n_supplier=25, n_part=199)
+                          n_supplier=25, n_part=199, orderless_customers=True)
         gen_s = time.perf_counter() - t0
         reqs = [r for _, r in TPCH_REQUESTS for _ in range(reps)]
         g_build, g_t = _driver_times(gpu, data, tmp / "gpu", reqs, "us")

@@ -697,6 +697,56 @@ std::vector<Q8ResultRow> run_q8(const Database& db, const std::string& nation, c
   return rows;
 }
 
+std::vector<Q22ResultRow> run_q22(const Database& db, const std::vector<std::string>& codes) {
+  // query_q22.cpp:24-60 (add_code): NULL and one-character codes are
+  // skipped; a code whose first two characters are digits is that numeric
+  // prefix, any other its first two characters; repeats are dropped.
+  uint8_t numeric[100] = {};
+  std::vector<int32_t> numeric_codes;
+  std::vector<std::string> extra;
+  std::vector<uint16_t> extra_pairs;
+  for (const auto& v : codes) {
+    if (v == "<<NULL>>" || v.size() < 2) continue;
+    if (v[0] >= '0' && v[0] <= '9' && v[1] >= '0' && v[1] <= '9') {
+      const int32_t code = (v[0] - '0') * 10 + (v[1] - '0');
+      if (!numeric[code]) {
+        numeric[code] = 1;
+        numeric_codes.push_back(code);
+      }
+      continue;
+    }
+    const uint16_t packed = static_cast<uint16_t>((static_cast<uint8_t>(v[0]) << 8) | static_cast<uint8_t>(v[1]));
+    if (std::find(extra_pairs.begin(), extra_pairs.end(), packed) != extra_pairs.end()) continue;
+    extra.push_back(v.substr(0, 2));
+    extra_pairs.push_back(packed);
+  }
+  if (numeric_codes.empty() && extra.empty()) return {};
+  bo_tpch_q22_tables t{};
+  t.c_custkey = col<int32_t>(db.c_custkey);
+  t.c_acctbal = col<int32_t>(db.c_acctbal_device);
+  t.c_phone_prefix = col<uint8_t>(db.c_phone_prefix);
+  t.c_phone_pair = col<uint32_t>(db.c_phone_pair);
+  t.n_customer = db.n_customer;
+  t.o_has_order = col<uint32_t>(db.o_has_order);
+  t.n_order_custkeys = db.n_order_custkeys;
+  int64_t counts[107] = {}, sums[107] = {};
+  check(db.ctx,
+        bo_tpch_q22(db.ctx, &t, numeric, extra_pairs.data(), static_cast<int32_t>(extra_pairs.size()), counts, sums),
+        "q22");
+  // Numeric classes in request order, then the extra prefixes; non-empty
+  // ones, by country code (:490-530).
+  std::vector<Q22ResultRow> rows;
+  for (const int32_t c : numeric_codes)
+    if (counts[c] != 0)
+      rows.push_back(Q22ResultRow{std::string{static_cast<char>('0' + c / 10), static_cast<char>('0' + c % 10)},
+                                  counts[c], sums[c]});
+  for (size_t i = 0; i < extra.size(); ++i)
+    if (counts[100 + i] != 0) rows.push_back(Q22ResultRow{extra[i], counts[100 + i], sums[100 + i]});
+  std::sort(rows.begin(), rows.end(),
+            [](const Q22ResultRow& a, const Q22ResultRow& b) { return a.cntrycode < b.cntrycode; });
+  return rows;
+}
+
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container) {
   // query_q17.cpp:125-155: NULL arguments, no parts, or an unknown brand or
   // container give a zero row.
@@ -980,6 +1030,16 @@ void write_q8_csv(const std::string& filename, const std::vector<Q8ResultRow>& r
   for (const auto& r : rows) out << r.o_year << "," << r.mkt_share << "\n";
 }
 
+void write_q22_csv(const std::string& filename, const std::vector<Q22ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q22.cpp:544-554
+  out << "cntrycode,numcust,totacctbal\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows)
+    out << escape_csv(r.cntrycode) << ',' << r.numcust << ',' << static_cast<double>(r.totacctbal_raw) / kPriceScale
+        << "\n";
+}
+
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows) {
   std::ofstream out(filename);  // query_q17.cpp:311-321
   out << "avg_yearly\n";
@@ -1042,7 +1102,8 @@ Database::~Database() {
                           &o_shippriority, &o_totalprice, &orderkey_to_row, &o_li_begin, &o_li_end,
                           &o_comment, &o_comment_offsets, &o_orderpriority, &l_shipmode, &l_commit_receipt,
                           &l_shard_max_shipdate, &l_partkey, &p_promo_by_key, &l_supp_nation, &o_cust_nation,
-                          &p_partkey, &p_brand, &p_container, &l_suppkey, &p_type,
+                          &p_partkey, &p_brand, &p_container, &l_suppkey, &p_type, &c_acctbal_device,
+                          &c_phone_prefix, &c_phone_pair, &o_has_order,
                           &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
@@ -1458,6 +1519,28 @@ Database* build(ParquetTables* tables) {
         if (order_custkeys[i] >= 0 && static_cast<size_t>(order_custkeys[i]) < nation_by_custkey.size())
           cust_nation[i] = nation_by_custkey[static_cast<size_t>(order_custkeys[i])];
       db->o_cust_nation = upload(ctx, cust_nation);
+      // Q22's per-custkey order bits (the builder's orders-by-customer
+      // offsets, builder_impl.cpp:625-660: custkeys 0 .. largest order custkey).
+      int32_t max_order_custkey = -1;
+      for (int32_t k : order_custkeys) max_order_custkey = std::max(max_order_custkey, k);
+      db->n_order_custkeys = max_order_custkey >= 0 ? static_cast<int64_t>(max_order_custkey) + 1 : 0;
+      std::vector<uint32_t> has_order(static_cast<size_t>((db->n_order_custkeys + 31) / 32), 0u);
+      for (int32_t k : order_custkeys)
+        if (k >= 0) has_order[static_cast<size_t>(k) >> 5] |= 1u << (k & 31);
+      db->o_has_order = upload(ctx, has_order);
+      // Phone classes (builder_impl.cpp:152-178; query_q22.cpp:120-140).
+      std::vector<uint8_t> prefix(h.ckey.size(), uint8_t(255));
+      std::vector<uint32_t> pair(h.ckey.size(), 0u);
+      for (size_t i = 0; i < h.ckey.size() && i + 1 < h.phone.offsets.size(); ++i) {
+        const auto v = h.phone.view(i);
+        if (v.size() < 2) continue;
+        const char c0 = v[0], c1 = v[1];
+        if (c0 >= '0' && c0 <= '9' && c1 >= '0' && c1 <= '9') prefix[i] = static_cast<uint8_t>((c0 - '0') * 10 + (c1 - '0'));
+        pair[i] = 0x10000u | (static_cast<uint32_t>(static_cast<uint8_t>(c0)) << 8) | static_cast<uint8_t>(c1);
+      }
+      db->c_phone_prefix = upload(ctx, prefix);
+      db->c_phone_pair = upload(ctx, pair);
+      db->c_acctbal_device = upload(ctx, h.acctbal);
       db->c_acctbal = std::move(h.acctbal);
       db->c_name = std::move(h.name);
       db->c_address = std::move(h.address);
@@ -1599,6 +1682,13 @@ void query(Database* db) {
       const auto rows = run_q8(*db, nation, region, type);
       const auto end = std::chrono::steady_clock::now();
       write_q8_csv(file, rows);
+      report(end);
+    } else if (r.id == "22") {
+      std::vector<std::string> codes;
+      for (const char* name : {"I1", "I2", "I3", "I4", "I5", "I6", "I7"}) codes.push_back(arg(name));
+      const auto rows = run_q22(*db, codes);
+      const auto end = std::chrono::steady_clock::now();
+      write_q22_csv(file, rows);
       report(end);
     } else if (r.id == "17") {
       const std::string brand = arg("BRAND");

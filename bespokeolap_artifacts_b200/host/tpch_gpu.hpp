@@ -94,6 +94,11 @@ struct Database {
   int64_t n_custkey_map = 0;
   bo_tpch::Dictionary mktsegment;
   std::vector<int32_t> c_acctbal;
+  // Q22: balances on the device, phone classes (numeric two-digit prefix or
+  // 255; 0x10000 | first two bytes for phones of two bytes or more), and a
+  // bit per custkey that has an order (custkeys 0 .. largest order custkey)
+  bo_tpch::DeviceColumn c_acctbal_device, c_phone_prefix, c_phone_pair, o_has_order;
+  int64_t n_order_custkeys = 0;
   bo_tpch::StringColumn c_name, c_address, c_phone, c_comment;
   // part: per partkey 1 (PROMO type), 0 (other type), -1 (no part row); the
   // largest partkey (-1 without parts)
@@ -174,6 +179,12 @@ struct Q8ResultRow {
   double mkt_share = 0.0;
 };
 
+struct Q22ResultRow {
+  std::string cntrycode;
+  int64_t numcust = 0;
+  int64_t totacctbal_raw = 0;
+};
+
 struct Q17ResultRow {
   int64_t sum_extendedprice_raw = 0;
 };
@@ -231,6 +242,7 @@ std::vector<Q5ResultRow> run_q5(const Database& db, const std::string& region, c
 std::vector<Q7ResultRow> run_q7(const Database& db, const std::string& nation1, const std::string& nation2);
 std::vector<Q8ResultRow> run_q8(const Database& db, const std::string& nation, const std::string& region,
                                 const std::string& type);
+std::vector<Q22ResultRow> run_q22(const Database& db, const std::vector<std::string>& codes);
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container);
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date);
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
@@ -246,6 +258,7 @@ void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& r
 void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& rows);
 void write_q7_csv(const std::string& filename, const std::vector<Q7ResultRow>& rows);
 void write_q8_csv(const std::string& filename, const std::vector<Q8ResultRow>& rows);
+void write_q22_csv(const std::string& filename, const std::vector<Q22ResultRow>& rows);
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows);
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows);
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);

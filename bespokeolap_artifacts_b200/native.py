@@ -252,6 +252,13 @@ class TpchQ8Tables(C.Structure):
                 ("max_partkey", C.c_int32), ("p_partkey", C.c_void_p), ("p_type", C.c_void_p), ("n_part", C.c_int64)]
 
 
+class TpchQ22Tables(C.Structure):
+    """``bo_tpch_q22_tables``: customer keys, balances, phone classes; the per-custkey order bits."""
+    _fields_ = [("c_custkey", C.c_void_p), ("c_acctbal", C.c_void_p), ("c_phone_prefix", C.c_void_p),
+                ("c_phone_pair", C.c_void_p), ("n_customer", C.c_int64), ("o_has_order", C.c_void_p),
+                ("n_order_custkeys", C.c_int64)]
+
+
 class TpchQ17Tables(C.Structure):
     """``bo_tpch_q17_tables``: lineitem partkeys, quantities, extended prices; part keys, brand and container
     codes; the largest part key."""
@@ -385,6 +392,8 @@ _SIGNATURES = {
                              C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q8": (C.c_int, [_P, C.POINTER(TpchQ8Tables), C.c_char_p, C.c_int32, C.c_char_p, C.c_int64, C.c_int32,
                              C.c_int16, C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
+    "bo_tpch_q22": (C.c_int, [_P, C.POINTER(TpchQ22Tables), C.c_char_p, C.c_void_p, C.c_int32,
+                              C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "bo_tpch_q17": (C.c_int, [_P, C.POINTER(TpchQ17Tables), C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
     "bo_tpch_q14": (C.c_int, [_P, C.POINTER(TpchQ14Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,

@@ -28,6 +28,10 @@ Key layouts (they select the reference's code paths):
                     per-nation arrays by the customer's nationkey unchecked).
   n_supplier        suppliers 1..n with nations 0..24 (default: one
                     supplier, key 1, nation 0).
+  orderless_customers  custkeys divisible by 3 (but the largest order
+                    custkey) place no order (Q22 counts customers without
+                    orders); order custkeys keep the customers' key range,
+                    which the reference's Q13 and Q22 index unchecked.
   n_part            parts 1..n (default 150; lineitems name parts 1..199).
                     The reference's Q17 reads its part bitmap at each
                     lineitem's partkey unchecked (query_q17.cpp:205-259), so
@@ -90,7 +94,7 @@ def _ragged_text(rng, n: int, max_words: int) -> list[str]:
 def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: int = 0,
                decimal: bool = False, order_keys: str = "sparse", customer_keys: str = "dense",
                shuffle_lineitem: bool = False, late_receipts: bool = False, customer_nations: str = "wide",
-               n_supplier: int = 1, n_part: int = 150) -> Path:
+               n_supplier: int = 1, n_part: int = 150, orderless_customers: bool = False) -> Path:
     rng = np.random.default_rng(seed)
     rng2 = np.random.default_rng([seed, 12])
     out.mkdir(parents=True, exist_ok=True)
@@ -125,6 +129,11 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
         o_cust = rng.choice(np.concatenate([custkey, custkey[:50] - 1]), n_orders).astype(np.int32)
     else:
         o_cust = rng.integers(1, n_customer + 1, n_orders).astype(np.int32)
+    if orderless_customers:
+        # custkeys divisible by 3 (but the largest) place no order: their orders
+        # go to the key below, so order custkeys keep the customers' key range
+        top = o_cust.max()
+        o_cust = np.where((o_cust % 3 == 0) & (o_cust != top), o_cust - 1, o_cust).astype(np.int32)
     pq.write_table(pa.table({
         "o_orderkey": orderkey, "o_custkey": o_cust, "o_orderstatus": ["O"] * n_orders,
         "o_totalprice": _dec(rng.integers(100000, 50000000, n_orders) / 100.0, decimal),

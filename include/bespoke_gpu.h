@@ -733,6 +733,31 @@ int bo_tpch_q8(bo_ctx* ctx, const bo_tpch_q8_tables* tables, const uint8_t* nati
                const uint8_t* supp_target_host, int64_t n_supp, int32_t type_code, int16_t date_start,
                int16_t date_last, int16_t year2_start, int64_t sums_out[4]);
 
+/* TPC-H Q22 over the storage-plan layout: run_q22 of
+ * bespoke_tpch/query_q22.cpp:272-540.  A customer's phone class is its
+ * numeric two-digit prefix (c_phone_prefix, 0..99; 255 otherwise) or, when
+ * that is 255, one of the n_extra non-numeric two-character prefixes
+ * (extra_pairs: (c0 << 8) | c1; c_phone_pair = 0x10000 | (c0 << 8) | c1 for
+ * phones of two characters or more, else 0).  Over the customers of an
+ * allowed class with a positive balance, avg = sum / count (int64); then the
+ * customers of an allowed class with a balance above avg whose custkey has
+ * no order (o_has_order bit clear; custkeys beyond n_order_custkeys count as
+ * without orders) are counted per class: counts_out / sums_out[code] for
+ * numeric classes 0..99, [100 + i] for extra prefix i (n_extra <= 7). */
+typedef struct bo_tpch_q22_tables {
+  const int32_t* c_custkey;
+  const int32_t* c_acctbal;            /* x100 */
+  const uint8_t* c_phone_prefix;
+  const uint32_t* c_phone_pair;
+  int64_t n_customer;
+  const uint32_t* o_has_order;         /* bit per custkey */
+  int64_t n_order_custkeys;
+} bo_tpch_q22_tables;
+
+#define BO_Q22_MAX_EXTRA 7
+int bo_tpch_q22(bo_ctx* ctx, const bo_tpch_q22_tables* tables, const uint8_t numeric_allowed[100],
+                const uint16_t* extra_pairs, int32_t n_extra, int64_t counts_out[107], int64_t sums_out[107]);
+
 /* TPC-H Q17 over the storage-plan layout: run_q17 of
  * bespoke_tpch/query_q17.cpp:119-311.  Parts with keys in [0, max_partkey]
  * of the given brand and container codes; the lineitems of those parts,

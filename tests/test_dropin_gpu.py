@@ -93,6 +93,9 @@ Q5_REQUESTS = ['5 "REGION0" "1994-01-01"', '5 "REGION1" "1995-02-28"', '5 "REGIO
                '7 "NATION_24" "NATION_00"', '7 "NATION_10" "NATION_01"',
                '8 "NATION_03" "REGION3" "PROMO_A"', '8 "NATION_10" "REGION0" "STD_B"', '8 "NOSUCH" "REGION0" "STD_B"',
                '8 "NATION_01" "NOSUCH" "STD_B"', '8 "NATION_02" "REGION2" "NOSUCH"', '8 "NATION_05" "REGION1" "PROM"',
+               '22 "13" "31" "23" "29" "30" "18" "17"', '22 "10" "10" "11" "<<NULL>>" "X" "AB" "34"',
+               '22 "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>"',
+               '22 "99" "98" "97" "96" "95" "94" "93"',
                '17 "BRAND_B" "CONT_C"', '17 "BRAND_E" "CONT_A"', '17 "NOSUCH" "CONT_A"', '17 "<<NULL>>" "CONT_A"',
                '17 "BRAND_A" "<<NULL>>"']
 
@@ -104,7 +107,7 @@ Q5_LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem): 
 
 @pytest.mark.parametrize("layout", Q5_LAYOUTS, ids=lambda l: "-".join(map(str, l)))
 def test_dropin_q5_matches_reference_driver(tmp_path, layout):
-    """Q5, Q7, Q8 and Q17 (with every other request) on data whose customer
+    """Q5, Q7, Q8, Q17 and Q22 (with every other request) on data whose customer
     nationkeys lie in the nation table's key range, whose suppliers cover every
     lineitem suppkey and whose parts cover every lineitem partkey: the
     reference's run_q5 indexes its per-nation arrays by customer nations
@@ -116,8 +119,14 @@ def test_dropin_q5_matches_reference_driver(tmp_path, layout):
     seed, decimal, order_keys, customer_keys, shuffle = layout
     data = write_tpch(tmp_path / "data", seed=seed, decimal=decimal, order_keys=order_keys,
                       customer_keys=customer_keys, shuffle_lineitem=shuffle, customer_nations="known", n_supplier=25,
-                      n_part=199)
+                      n_part=199, orderless_customers=True)
     requests = Q5_REQUESTS + REQUESTS
+    # Q22 reads the builder's orders-by-customer offsets at every customer's
+    # key (query_q22.cpp:358, 468) and Q13 its counts at every order's
+    # custkey (query_q13.cpp:218), both unchecked: the two key ranges match.
+    import pyarrow.parquet as pq
+    assert (pq.read_table(data / "customer.parquet")["c_custkey"].to_numpy().max()
+            == pq.read_table(data / "orders.parquet")["o_custkey"].to_numpy().max())
     run(GPU_DRIVER, data, tmp_path / "gpu", requests)
     run(REF_DRIVER, data, tmp_path / "ref", requests)
     for i, req in enumerate(requests, start=1):
