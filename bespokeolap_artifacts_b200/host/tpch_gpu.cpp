@@ -747,6 +747,43 @@ std::vector<Q22ResultRow> run_q22(const Database& db, const std::vector<std::str
   return rows;
 }
 
+std::vector<Q15ResultRow> run_q15(const Database& db, const std::string& date) {
+  // query_q15.cpp:223-244: the quarter [DATE, DATE + 3 months), totals per
+  // suppkey up to the largest supplier key.
+  const int16_t start = date_offset_of(date, db.base_date_days);
+  const int16_t end = date_offset_of(date, db.base_date_days, 3);
+  int32_t max_suppkey = -1;
+  for (int32_t k : db.s_suppkey) max_suppkey = std::max(max_suppkey, k);
+  const int64_t n_supp = std::max<int64_t>(static_cast<int64_t>(max_suppkey) + 1, 1);
+  bo_tpch_q15_tables t{};
+  t.l_shipdate = col<int16_t>(db.l_shipdate);
+  t.l_suppkey = col<int32_t>(db.l_suppkey);
+  t.l_discounted_price = col<int32_t>(db.l_discounted_price);
+  t.n_lineitem = db.n_lineitem;
+  std::vector<int64_t> revenue(static_cast<size_t>(n_supp), 0);
+  int64_t shipped = 0;
+  check(db.ctx, bo_tpch_q15(db.ctx, &t, n_supp, start, end, revenue.data(), &shipped), "q15");
+  // :454-530: nothing shipped, or no positive total: no rows; else the
+  // suppliers (last row of a key) whose total is the largest, by suppkey.
+  if (shipped == 0) return {};
+  int64_t max_revenue = 0;
+  for (int64_t v : revenue)
+    if (v > 0) max_revenue = std::max(max_revenue, v);
+  if (max_revenue == 0) return {};
+  std::vector<int32_t> row_of(revenue.size(), -1);
+  for (size_t i = 0; i < db.s_suppkey.size(); ++i)
+    if (db.s_suppkey[i] >= 0 && static_cast<size_t>(db.s_suppkey[i]) < row_of.size())
+      row_of[static_cast<size_t>(db.s_suppkey[i])] = static_cast<int32_t>(i);
+  std::vector<Q15ResultRow> rows;
+  for (size_t k = 0; k < revenue.size(); ++k) {
+    if (revenue[k] != max_revenue || row_of[k] < 0) continue;
+    const size_t r = static_cast<size_t>(row_of[k]);
+    rows.push_back(Q15ResultRow{static_cast<int32_t>(k), db.s_name.view(r), db.s_address.view(r), db.s_phone.view(r),
+                                revenue[k]});
+  }
+  return rows;
+}
+
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container) {
   // query_q17.cpp:125-155: NULL arguments, no parts, or an unknown brand or
   // container give a zero row.
@@ -1038,6 +1075,17 @@ void write_q22_csv(const std::string& filename, const std::vector<Q22ResultRow>&
   for (const auto& r : rows)
     out << escape_csv(r.cntrycode) << ',' << r.numcust << ',' << static_cast<double>(r.totacctbal_raw) / kPriceScale
         << "\n";
+}
+
+void write_q15_csv(const std::string& filename, const std::vector<Q15ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q15.cpp:536-548
+  out << "s_suppkey,s_name,s_address,s_phone,total_revenue\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows)
+    out << r.s_suppkey << ',' << escape_csv(std::string(r.s_name)) << ',' << escape_csv(std::string(r.s_address))
+        << ',' << escape_csv(std::string(r.s_phone)) << ','
+        << static_cast<double>(r.total_revenue_raw) / kPriceScale << "\n";
 }
 
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows) {
@@ -1581,6 +1629,9 @@ Database* build(ParquetTables* tables) {
       const auto& S = tables->supplier;
       db->s_suppkey = int_values(column(S, "s_suppkey"));
       db->s_nationkey = int_values(column(S, "s_nationkey"));
+      db->s_name = string_column(column(S, "s_name"));
+      db->s_address = string_column(column(S, "s_address"));
+      db->s_phone = string_column(column(S, "s_phone"));
     }
     {  // region name -> key, the first row of a name (builder_impl.cpp:805-826)
       const auto& R = tables->region;
@@ -1689,6 +1740,13 @@ void query(Database* db) {
       const auto rows = run_q22(*db, codes);
       const auto end = std::chrono::steady_clock::now();
       write_q22_csv(file, rows);
+      report(end);
+    } else if (r.id == "15") {
+      const std::string date = arg("DATE");
+      arg("STREAM_ID");  // parsed as the reference does; not used by the query
+      const auto rows = run_q15(*db, date);
+      const auto end = std::chrono::steady_clock::now();
+      write_q15_csv(file, rows);
       report(end);
     } else if (r.id == "17") {
       const std::string brand = arg("BRAND");

@@ -115,8 +115,9 @@ struct Database {
   // nation rows' keys, region keys and names; region name -> key (first row of a name)
   std::vector<int32_t> nation_key, nation_regionkey;
   std::vector<std::string> nation_row_name;
-  // supplier rows' keys and nationkeys (Q7's supplier tags)
+  // supplier rows' keys and nationkeys (Q7's supplier tags), strings (Q15)
   std::vector<int32_t> s_suppkey, s_nationkey;
+  bo_tpch::StringColumn s_name, s_address, s_phone;
   std::unordered_map<std::string, int32_t> region_key_by_name;
   // Result record of the last scan-agg / Q6 query.  Queries on one Database
   // run one at a time (as the reference's single-threaded query()).
@@ -185,6 +186,12 @@ struct Q22ResultRow {
   int64_t totacctbal_raw = 0;
 };
 
+struct Q15ResultRow {
+  int32_t s_suppkey = 0;
+  std::string_view s_name, s_address, s_phone;
+  int64_t total_revenue_raw = 0;
+};
+
 struct Q17ResultRow {
   int64_t sum_extendedprice_raw = 0;
 };
@@ -243,6 +250,7 @@ std::vector<Q7ResultRow> run_q7(const Database& db, const std::string& nation1, 
 std::vector<Q8ResultRow> run_q8(const Database& db, const std::string& nation, const std::string& region,
                                 const std::string& type);
 std::vector<Q22ResultRow> run_q22(const Database& db, const std::vector<std::string>& codes);
+std::vector<Q15ResultRow> run_q15(const Database& db, const std::string& date);
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container);
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date);
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
@@ -259,6 +267,7 @@ void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& r
 void write_q7_csv(const std::string& filename, const std::vector<Q7ResultRow>& rows);
 void write_q8_csv(const std::string& filename, const std::vector<Q8ResultRow>& rows);
 void write_q22_csv(const std::string& filename, const std::vector<Q22ResultRow>& rows);
+void write_q15_csv(const std::string& filename, const std::vector<Q15ResultRow>& rows);
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows);
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows);
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);

@@ -259,6 +259,12 @@ class TpchQ22Tables(C.Structure):
                 ("n_order_custkeys", C.c_int64)]
 
 
+class TpchQ15Tables(C.Structure):
+    """``bo_tpch_q15_tables``: lineitem shipdates, suppkeys, discounted prices."""
+    _fields_ = [("l_shipdate", C.c_void_p), ("l_suppkey", C.c_void_p), ("l_discounted_price", C.c_void_p),
+                ("n_lineitem", C.c_int64)]
+
+
 class TpchQ17Tables(C.Structure):
     """``bo_tpch_q17_tables``: lineitem partkeys, quantities, extended prices; part keys, brand and container
     codes; the largest part key."""
@@ -394,6 +400,8 @@ _SIGNATURES = {
                              C.c_int16, C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q22": (C.c_int, [_P, C.POINTER(TpchQ22Tables), C.c_char_p, C.c_void_p, C.c_int32,
                               C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "bo_tpch_q15": (C.c_int, [_P, C.POINTER(TpchQ15Tables), C.c_int64, C.c_int16, C.c_int16, C.POINTER(C.c_int64),
+                              C.POINTER(C.c_int64)]),
     "bo_tpch_q17": (C.c_int, [_P, C.POINTER(TpchQ17Tables), C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
     "bo_tpch_q14": (C.c_int, [_P, C.POINTER(TpchQ14Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,

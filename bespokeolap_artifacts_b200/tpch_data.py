@@ -191,8 +191,10 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
         skey = np.arange(1, n_supplier + 1, dtype=np.int32)
         snation = np.random.default_rng([seed, 5]).integers(0, 25, n_supplier).astype(np.int32)
     ns = len(skey)
-    pq.write_table(pa.table({"s_suppkey": skey, "s_name": ["s"] * ns, "s_address": ["a"] * ns, "s_nationkey": snation,
-                             "s_phone": ["10-0"] * ns, "s_acctbal": _dec(np.ones(ns), decimal), "s_comment": [""] * ns}),
+    pq.write_table(pa.table({"s_suppkey": skey, "s_name": [f"Supplier#{k:09d}" for k in skey],
+                             "s_address": [f"addr {k}, \"{k % 7}\"" for k in skey], "s_nationkey": snation,
+                             "s_phone": [f"{10 + k % 25}-{k:03d}-000-0000" for k in skey],
+                             "s_acctbal": _dec(np.ones(ns), decimal), "s_comment": [""] * ns}),
                    out / "supplier.parquet")
     pq.write_table(pa.table({"ps_partkey": one, "ps_suppkey": one, "ps_availqty": one,
                              "ps_supplycost": _dec(np.ones(1), decimal), "ps_comment": [""]}), out / "partsupp.parquet")

@@ -758,6 +758,22 @@ typedef struct bo_tpch_q22_tables {
 int bo_tpch_q22(bo_ctx* ctx, const bo_tpch_q22_tables* tables, const uint8_t numeric_allowed[100],
                 const uint16_t* extra_pairs, int32_t n_extra, int64_t counts_out[107], int64_t sums_out[107]);
 
+/* TPC-H Q15 over the storage-plan layout: run_q15 of
+ * bespoke_tpch/query_q15.cpp:215-534.  The discounted prices of lineitems
+ * shipped in [start_offset, end_offset), summed per suppkey into
+ * revenue_out[0 .. n_supp) (suppkeys outside it are not summed);
+ * *shipped_out = the number of lineitems in the window (the reference
+ * returns no rows when it is 0, :454-456). */
+typedef struct bo_tpch_q15_tables {
+  const int16_t* l_shipdate;           /* 16-byte aligned */
+  const int32_t* l_suppkey;
+  const int32_t* l_discounted_price;
+  int64_t n_lineitem;
+} bo_tpch_q15_tables;
+
+int bo_tpch_q15(bo_ctx* ctx, const bo_tpch_q15_tables* tables, int64_t n_supp, int16_t start_offset,
+                int16_t end_offset, int64_t* revenue_out, int64_t* shipped_out);
+
 /* TPC-H Q17 over the storage-plan layout: run_q17 of
  * bespoke_tpch/query_q17.cpp:119-311.  Parts with keys in [0, max_partkey]
  * of the given brand and container codes; the lineitems of those parts,

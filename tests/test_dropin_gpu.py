@@ -96,6 +96,7 @@ Q5_REQUESTS = ['5 "REGION0" "1994-01-01"', '5 "REGION1" "1995-02-28"', '5 "REGIO
                '22 "13" "31" "23" "29" "30" "18" "17"', '22 "10" "10" "11" "<<NULL>>" "X" "AB" "34"',
                '22 "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>"',
                '22 "99" "98" "97" "96" "95" "94" "93"',
+               '15 "1996-01-01" "1"', '15 "1995-11-30" "0"', '15 "1999-01-01" "2"', '15 "1993-05-17" "3"',
                '17 "BRAND_B" "CONT_C"', '17 "BRAND_E" "CONT_A"', '17 "NOSUCH" "CONT_A"', '17 "<<NULL>>" "CONT_A"',
                '17 "BRAND_A" "<<NULL>>"']
 
@@ -107,7 +108,7 @@ Q5_LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem): 
 
 @pytest.mark.parametrize("layout", Q5_LAYOUTS, ids=lambda l: "-".join(map(str, l)))
 def test_dropin_q5_matches_reference_driver(tmp_path, layout):
-    """Q5, Q7, Q8, Q17 and Q22 (with every other request) on data whose customer
+    """Q5, Q7, Q8, Q15, Q17 and Q22 (with every other request) on data whose customer
     nationkeys lie in the nation table's key range, whose suppliers cover every
     lineitem suppkey and whose parts cover every lineitem partkey: the
     reference's run_q5 indexes its per-nation arrays by customer nations

@@ -1,4 +1,4 @@
-"""Python restatements of Q4, Q5, Q7, Q8, Q12, Q14, Q17 and Q22 (the
+"""Python restatements of Q4, Q5, Q7, Q8, Q12, Q14, Q15, Q17 and Q22 (the
 semantics the GPU tests restate), pinned against the reference itself: its own load / build / query (compiled
 unchanged into oracle/_ref/ref_tpch_driver) answers the same requests on the
 same seeded Parquet files, on the CPU.  Q12 runs on data with receipts up to
@@ -288,6 +288,28 @@ def q22(t, codes):
     return [[p, str(n), f"{s / 100:.2f}"] for p, (n, s) in sorted(out.items())]
 
 
+def q15(t, date):
+    L, S = t["lineitem"], t["supplier"]
+    start, end = offset(date), offset(date, 3)
+    ship = days(L["l_shipdate"])
+    win = (ship >= start) & (ship < end)
+    if not win.any():
+        return []
+    rev = {}
+    for sk, v in zip(L["l_suppkey"].to_numpy()[win].tolist(), dprices(L)[win].tolist()):
+        rev[sk] = rev.get(sk, 0) + v
+    top = max([v for v in rev.values() if v > 0], default=0)
+    if top == 0:
+        return []
+    srow = last_wins(S["s_suppkey"].to_pylist(),
+                     zip(S["s_name"].to_pylist(), S["s_address"].to_pylist(), S["s_phone"].to_pylist()))
+    # the reference's CSV fields: quoted, inner quotes as \" (parsed here as the reference's file is)
+    esc = lambda x: '"' + x.replace('"', '\\"') + '"'  # noqa: E731
+    lines = [",".join([str(k), *map(esc, srow[k]), f"{v / 100:.2f}"])
+             for k, v in sorted(rev.items()) if v == top and k in srow]
+    return list(csv.reader(lines))
+
+
 def test_q5_q7_q8_q17_q22_restatements_match_the_reference(known, tmp_path):
     data, t = known
     cases = [
@@ -300,6 +322,8 @@ def test_q5_q7_q8_q17_q22_restatements_match_the_reference(known, tmp_path):
         ('7 "NATION_01" "NATION_10"', lambda: q7(t, "NATION_01", "NATION_10")),
         ('7 "NATION_06" "NATION_06"', lambda: q7(t, "NATION_06", "NATION_06")),
         ('8 "NATION_10" "REGION0" "STD_B"', lambda: q8(t, "NATION_10", "REGION0", "STD_B")),
+        ('15 "1996-01-01" "1"', lambda: q15(t, "1996-01-01")),
+        ('15 "1995-11-30" "0"', lambda: q15(t, "1995-11-30")),
         ('17 "BRAND_B" "CONT_C"', lambda: q17(t, "BRAND_B", "CONT_C")),
         ('22 "13" "31" "23" "29" "30" "18" "17"', lambda: q22(t, ["13", "31", "23", "29", "30", "18", "17"])),
     ]
@@ -307,6 +331,6 @@ def test_q5_q7_q8_q17_q22_restatements_match_the_reference(known, tmp_path):
     for (req, want), g in zip(cases, got):
         assert g[1:] == want(), req
     # every query family has a non-empty, non-zero answer among the cases
-    for q in ("5 ", "7 ", "8 ", "17 ", "22 "):
+    for q in ("5 ", "7 ", "8 ", "15 ", "17 ", "22 "):
         assert any(len(g) > 1 and any(x != "0.00" for row in g[1:] for x in (row[1:] if len(row) > 1 else row))
                    for (req, _), g in zip(cases, got) if req.startswith(q)), q
