@@ -919,7 +919,7 @@ TPCH_REQUESTS = [  # synthetic parameters: segments, ship modes and comment word
     ("1", '1 "90"'), ("3", '3 "SEG_B" "1995-03-17"'), ("4", '4 "1993-07-01"'), ("5", '5 "REGION0" "1994-01-01"'),
     ("6", '6 "1994-02-01" "0.07" "23"'), ("7", '7 "NATION_01" "NATION_10"'),
     ("8", '8 "NATION_10" "REGION0" "STD_B"'),
-    ("10", '10 "1993-10-01"'), ("12", '12 "MODE_A" "MODE_C" "1994-01-01"'), ("13", '13 "pending" "deposits"'),
+    ("10", '10 "1993-10-01"'), ("11", '11 "NATION_04" "0.0001"'), ("12", '12 "MODE_A" "MODE_C" "1994-01-01"'), ("13", '13 "pending" "deposits"'),
     ("14", '14 "1995-09-01"'), ("15", '15 "1996-01-01" "1"'), ("17", '17 "BRAND_B" "CONT_C"'), ("18", '18 "250"'),
     ("22", '22 "13" "31" "23" "29" "30" "18" "17"'),
 ]

@@ -747,6 +747,49 @@ std::vector<Q22ResultRow> run_q22(const Database& db, const std::vector<std::str
   return rows;
 }
 
+std::vector<Q11ResultRow> run_q11(const Database& db, const std::string& nation, const std::string& fraction) {
+  // query_q11.cpp:112-143: the nation's key (first nation row of the name),
+  // FRACTION as a double, the nation's suppliers by key.
+  int32_t key = 0;
+  bool found = false;
+  for (size_t i = 0; i < db.nation_row_name.size() && !found; ++i)
+    if (db.nation_row_name[i] == nation) {
+      key = db.nation_key[i];
+      found = true;
+    }
+  if (!found) return {};
+  const double frac = std::stod(fraction);
+  int32_t max_suppkey = -1;
+  for (int32_t k : db.s_suppkey) max_suppkey = std::max(max_suppkey, k);
+  std::vector<uint8_t> in_nation(max_suppkey >= 0 ? static_cast<size_t>(max_suppkey) + 1 : 0, 0);
+  for (size_t i = 0; i < db.s_suppkey.size(); ++i)
+    if (db.s_nationkey[i] == key && db.s_suppkey[i] >= 0) in_nation[static_cast<size_t>(db.s_suppkey[i])] = 1;
+  if (db.n_partsupp == 0) return {};
+  bo_tpch_q11_tables t{};
+  t.ps_partkey = col<int32_t>(db.ps_partkey);
+  t.ps_suppkey = col<int32_t>(db.ps_suppkey);
+  t.ps_value = col<int32_t>(db.ps_value);
+  t.n_partsupp = db.n_partsupp;
+  t.min_partkey = db.ps_min_partkey;
+  t.max_partkey = db.ps_max_partkey;
+  const int64_t range = static_cast<int64_t>(db.ps_max_partkey) - db.ps_min_partkey + 1;
+  std::vector<int64_t> sums(static_cast<size_t>(range), 0);
+  int64_t total = 0;
+  check(db.ctx,
+        bo_tpch_q11(db.ctx, &t, in_nation.data(), static_cast<int64_t>(in_nation.size()), sums.data(), &total),
+        "q11");
+  // :180-215: non-zero part sums above total * FRACTION, by value desc then partkey.
+  const double threshold = static_cast<double>(total) * frac;
+  std::vector<Q11ResultRow> rows;
+  for (int64_t i = 0; i < range; ++i)
+    if (sums[static_cast<size_t>(i)] != 0 && static_cast<double>(sums[static_cast<size_t>(i)]) > threshold)
+      rows.push_back(Q11ResultRow{static_cast<int32_t>(db.ps_min_partkey + i), sums[static_cast<size_t>(i)]});
+  std::sort(rows.begin(), rows.end(), [](const Q11ResultRow& a, const Q11ResultRow& b) {
+    return a.value_raw != b.value_raw ? a.value_raw > b.value_raw : a.ps_partkey < b.ps_partkey;
+  });
+  return rows;
+}
+
 std::vector<Q15ResultRow> run_q15(const Database& db, const std::string& date) {
   // query_q15.cpp:223-244: the quarter [DATE, DATE + 3 months), totals per
   // suppkey up to the largest supplier key.
@@ -1077,6 +1120,14 @@ void write_q22_csv(const std::string& filename, const std::vector<Q22ResultRow>&
         << "\n";
 }
 
+void write_q11_csv(const std::string& filename, const std::vector<Q11ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q11.cpp:226-234
+  out << "ps_partkey,value\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows) out << r.ps_partkey << ',' << static_cast<double>(r.value_raw) / kPriceScale << "\n";
+}
+
 void write_q15_csv(const std::string& filename, const std::vector<Q15ResultRow>& rows) {
   std::ofstream out(filename);  // query_q15.cpp:536-548
   out << "s_suppkey,s_name,s_address,s_phone,total_revenue\n";
@@ -1151,7 +1202,7 @@ Database::~Database() {
                           &o_comment, &o_comment_offsets, &o_orderpriority, &l_shipmode, &l_commit_receipt,
                           &l_shard_max_shipdate, &l_partkey, &p_promo_by_key, &l_supp_nation, &o_cust_nation,
                           &p_partkey, &p_brand, &p_container, &l_suppkey, &p_type, &c_acctbal_device,
-                          &c_phone_prefix, &c_phone_pair, &o_has_order,
+                          &c_phone_prefix, &c_phone_pair, &o_has_order, &ps_partkey, &ps_suppkey, &ps_value,
                           &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
@@ -1625,6 +1676,30 @@ Database* build(ParquetTables* tables) {
       db->nation_regionkey = int_values(column(N, "n_regionkey"));
       for (size_t i = 0; i < key.size(); ++i) db->nation_row_name.emplace_back(name.view(i));
     }
+    {  // partsupp (bespoke_tpch/builder_impl.cpp:751-777): value = supplycost * availqty, rows by partkey
+      const auto& PS = tables->partsupp;
+      const auto pk = int_values(column(PS, "ps_partkey"));
+      const auto sk = int_values(column(PS, "ps_suppkey"));
+      const auto qty = int_values(column(PS, "ps_availqty"));
+      const auto cost = scaled_values(column(PS, "ps_supplycost"), kPriceScale);
+      std::vector<uint32_t> order(pk.size());
+      std::iota(order.begin(), order.end(), 0u);
+      std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return pk[a] < pk[b]; });
+      std::vector<int32_t> spk(pk.size()), ssk(pk.size()), val(pk.size());
+      for (size_t i = 0; i < order.size(); ++i) {
+        spk[i] = pk[order[i]];
+        ssk[i] = sk[order[i]];
+        val[i] = static_cast<int32_t>(static_cast<int64_t>(cost[order[i]]) * qty[order[i]]);
+      }
+      db->n_partsupp = static_cast<int64_t>(pk.size());
+      if (!spk.empty()) {
+        db->ps_min_partkey = spk.front();
+        db->ps_max_partkey = spk.back();
+      }
+      db->ps_partkey = upload(ctx, spk);
+      db->ps_suppkey = upload(ctx, ssk);
+      db->ps_value = upload(ctx, val);
+    }
     {
       const auto& S = tables->supplier;
       db->s_suppkey = int_values(column(S, "s_suppkey"));
@@ -1740,6 +1815,13 @@ void query(Database* db) {
       const auto rows = run_q22(*db, codes);
       const auto end = std::chrono::steady_clock::now();
       write_q22_csv(file, rows);
+      report(end);
+    } else if (r.id == "11") {
+      const std::string nation = arg("NATION");
+      const std::string fraction = arg("FRACTION");
+      const auto rows = run_q11(*db, nation, fraction);
+      const auto end = std::chrono::steady_clock::now();
+      write_q11_csv(file, rows);
       report(end);
     } else if (r.id == "15") {
       const std::string date = arg("DATE");

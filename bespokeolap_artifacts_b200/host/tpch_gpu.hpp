@@ -115,6 +115,10 @@ struct Database {
   // nation rows' keys, region keys and names; region name -> key (first row of a name)
   std::vector<int32_t> nation_key, nation_regionkey;
   std::vector<std::string> nation_row_name;
+  // partsupp sorted by partkey (stable), value = supplycost * availqty (x100)
+  bo_tpch::DeviceColumn ps_partkey, ps_suppkey, ps_value;
+  int64_t n_partsupp = 0;
+  int32_t ps_min_partkey = 0, ps_max_partkey = -1;
   // supplier rows' keys and nationkeys (Q7's supplier tags), strings (Q15)
   std::vector<int32_t> s_suppkey, s_nationkey;
   bo_tpch::StringColumn s_name, s_address, s_phone;
@@ -186,6 +190,11 @@ struct Q22ResultRow {
   int64_t totacctbal_raw = 0;
 };
 
+struct Q11ResultRow {
+  int32_t ps_partkey = 0;
+  int64_t value_raw = 0;
+};
+
 struct Q15ResultRow {
   int32_t s_suppkey = 0;
   std::string_view s_name, s_address, s_phone;
@@ -250,6 +259,7 @@ std::vector<Q7ResultRow> run_q7(const Database& db, const std::string& nation1, 
 std::vector<Q8ResultRow> run_q8(const Database& db, const std::string& nation, const std::string& region,
                                 const std::string& type);
 std::vector<Q22ResultRow> run_q22(const Database& db, const std::vector<std::string>& codes);
+std::vector<Q11ResultRow> run_q11(const Database& db, const std::string& nation, const std::string& fraction);
 std::vector<Q15ResultRow> run_q15(const Database& db, const std::string& date);
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container);
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date);
@@ -267,6 +277,7 @@ void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& r
 void write_q7_csv(const std::string& filename, const std::vector<Q7ResultRow>& rows);
 void write_q8_csv(const std::string& filename, const std::vector<Q8ResultRow>& rows);
 void write_q22_csv(const std::string& filename, const std::vector<Q22ResultRow>& rows);
+void write_q11_csv(const std::string& filename, const std::vector<Q11ResultRow>& rows);
 void write_q15_csv(const std::string& filename, const std::vector<Q15ResultRow>& rows);
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows);
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows);

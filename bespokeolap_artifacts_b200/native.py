@@ -259,6 +259,12 @@ class TpchQ22Tables(C.Structure):
                 ("n_order_custkeys", C.c_int64)]
 
 
+class TpchQ11Tables(C.Structure):
+    """``bo_tpch_q11_tables``: partsupp rows by partkey (partkeys, suppkeys, values) and the partkey range."""
+    _fields_ = [("ps_partkey", C.c_void_p), ("ps_suppkey", C.c_void_p), ("ps_value", C.c_void_p),
+                ("n_partsupp", C.c_int64), ("min_partkey", C.c_int32), ("max_partkey", C.c_int32)]
+
+
 class TpchQ15Tables(C.Structure):
     """``bo_tpch_q15_tables``: lineitem shipdates, suppkeys, discounted prices."""
     _fields_ = [("l_shipdate", C.c_void_p), ("l_suppkey", C.c_void_p), ("l_discounted_price", C.c_void_p),
@@ -400,6 +406,8 @@ _SIGNATURES = {
                              C.c_int16, C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q22": (C.c_int, [_P, C.POINTER(TpchQ22Tables), C.c_char_p, C.c_void_p, C.c_int32,
                               C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "bo_tpch_q11": (C.c_int, [_P, C.POINTER(TpchQ11Tables), C.c_char_p, C.c_int64, C.POINTER(C.c_int64),
+                              C.POINTER(C.c_int64)]),
     "bo_tpch_q15": (C.c_int, [_P, C.POINTER(TpchQ15Tables), C.c_int64, C.c_int16, C.c_int16, C.POINTER(C.c_int64),
                               C.POINTER(C.c_int64)]),
     "bo_tpch_q17": (C.c_int, [_P, C.POINTER(TpchQ17Tables), C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),

@@ -196,8 +196,16 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
                              "s_phone": [f"{10 + k % 25}-{k:03d}-000-0000" for k in skey],
                              "s_acctbal": _dec(np.ones(ns), decimal), "s_comment": [""] * ns}),
                    out / "supplier.parquet")
-    pq.write_table(pa.table({"ps_partkey": one, "ps_suppkey": one, "ps_availqty": one,
-                             "ps_supplycost": _dec(np.ones(1), decimal), "ps_comment": [""]}), out / "partsupp.parquet")
+    # four suppliers per part (key 1..n_part), rows in random order
+    rng4 = np.random.default_rng([seed, 11])
+    ps_part = np.repeat(np.arange(1, n_part + 1), 4)
+    ps_supp = ((ps_part - 1 + np.tile(np.arange(4), n_part) * (ns // 4 + 1)) % ns + 1)
+    perm = rng4.permutation(len(ps_part))
+    n_ps = len(ps_part)
+    pq.write_table(pa.table({"ps_partkey": ps_part[perm].astype(np.int32), "ps_suppkey": skey[ps_supp[perm] - 1],
+                             "ps_availqty": rng4.integers(1, 10_000, n_ps).astype(np.int32),
+                             "ps_supplycost": _dec(rng4.integers(100, 100_001, n_ps) / 100.0, decimal),
+                             "ps_comment": [""] * n_ps}), out / "partsupp.parquet")
     nkey = np.array([k for k in range(25) if k != 7], np.int32)
     pq.write_table(pa.table({"n_nationkey": nkey, "n_name": [f"NATION_{k:02d}" for k in nkey],
                              "n_regionkey": nkey % 5, "n_comment": [""] * len(nkey)}), out / "nation.parquet")

@@ -758,6 +758,25 @@ typedef struct bo_tpch_q22_tables {
 int bo_tpch_q22(bo_ctx* ctx, const bo_tpch_q22_tables* tables, const uint8_t numeric_allowed[100],
                 const uint16_t* extra_pairs, int32_t n_extra, int64_t counts_out[107], int64_t sums_out[107]);
 
+/* TPC-H Q11 over the storage-plan layout: run_q11 of
+ * bespoke_tpch/query_q11.cpp:109-224.  Over the partsupp rows whose
+ * supplier is in the nation (supp_in_nation_host, per suppkey, n_supp
+ * bytes; suppkeys outside it are not), the value supplycost * availqty
+ * (x100, the builder's supplycost_availqty) summed into
+ * sums_out[partkey - min_partkey] (max_partkey - min_partkey + 1 entries)
+ * and into *total_out.  Every partsupp partkey lies in [min, max]. */
+typedef struct bo_tpch_q11_tables {
+  const int32_t* ps_partkey;
+  const int32_t* ps_suppkey;
+  const int32_t* ps_value;
+  int64_t n_partsupp;
+  int32_t min_partkey;
+  int32_t max_partkey;
+} bo_tpch_q11_tables;
+
+int bo_tpch_q11(bo_ctx* ctx, const bo_tpch_q11_tables* tables, const uint8_t* supp_in_nation_host, int64_t n_supp,
+                int64_t* sums_out, int64_t* total_out);
+
 /* TPC-H Q15 over the storage-plan layout: run_q15 of
  * bespoke_tpch/query_q15.cpp:215-534.  The discounted prices of lineitems
  * shipped in [start_offset, end_offset), summed per suppkey into

@@ -2,7 +2,7 @@
 query (bespokeolap_artifacts_b200/host) and the reference's own load / build /
 query (compiled unchanged into oracle/_ref/ref_tpch_driver) read the same
 Parquet files and the same stdin requests; their result<idx>.csv files must
-agree: Q1, Q4, Q6, Q10, Q12, Q13, Q14 and Q18 byte for byte, Q3 row for row (the reference's
+agree: Q1, Q4, Q6, Q10, Q11, Q12, Q13, Q14 and Q18 byte for byte, Q3 row for row (the reference's
 std::sort leaves rows equal in revenue and orderdate in unspecified order;
 the GPU emits them in orderkey order).  The key layouts select each of the
 reference's paths: dense and sparse orderkeys (Q18's two scans), dense,
@@ -34,6 +34,7 @@ REQUESTS = [
     '14 "1995-09-01"', '14 "1993-01-31"', '14 "2000-01-01"',
     '12 "MODE_A" "MODE_C" "1994-01-01"', '12 "MODE_B" "MODE_B" "1995-06-30"', '12 "NOSUCH" "MODE_D" "1993-03-01"',
     '12 "X" "Y" "1994-01-01"', '12 "MODE_G" "MODE_E" "1998-12-01"', '12 "MODE_F" "MODE_A" "1992-02-29"',
+    '11 "NATION_00" "0.001"', '11 "NATION_00" "0"', '11 "NATION_05" "0.5"',
     '13 "pending" "deposits"', '13 "quick" "quick"', '13 "" ""', '13 "bold" ""', '13 "" "final"',
     '13 "x\\"y" "a,b"', '13 "ironic quick pending bold deposits final final" "x"', '13 "zzz" "ironic"',
 ]
@@ -96,6 +97,8 @@ Q5_REQUESTS = ['5 "REGION0" "1994-01-01"', '5 "REGION1" "1995-02-28"', '5 "REGIO
                '22 "13" "31" "23" "29" "30" "18" "17"', '22 "10" "10" "11" "<<NULL>>" "X" "AB" "34"',
                '22 "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>"',
                '22 "99" "98" "97" "96" "95" "94" "93"',
+               '11 "NATION_04" "0.0001"', '11 "NATION_19" "0.01"', '11 "NOSUCH" "0.1"', '11 "NATION_02" "0"',
+               '11 "NATION_04" "-1"',
                '15 "1996-01-01" "1"', '15 "1995-11-30" "0"', '15 "1999-01-01" "2"', '15 "1993-05-17" "3"',
                '17 "BRAND_B" "CONT_C"', '17 "BRAND_E" "CONT_A"', '17 "NOSUCH" "CONT_A"', '17 "<<NULL>>" "CONT_A"',
                '17 "BRAND_A" "<<NULL>>"']
@@ -108,7 +111,7 @@ Q5_LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem): 
 
 @pytest.mark.parametrize("layout", Q5_LAYOUTS, ids=lambda l: "-".join(map(str, l)))
 def test_dropin_q5_matches_reference_driver(tmp_path, layout):
-    """Q5, Q7, Q8, Q15, Q17 and Q22 (with every other request) on data whose customer
+    """Q5, Q7, Q8, Q11, Q15, Q17 and Q22 (with every other request) on data whose customer
     nationkeys lie in the nation table's key range, whose suppliers cover every
     lineitem suppkey and whose parts cover every lineitem partkey: the
     reference's run_q5 indexes its per-nation arrays by customer nations

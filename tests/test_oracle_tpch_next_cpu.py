@@ -1,4 +1,4 @@
-"""Python restatements of Q4, Q5, Q7, Q8, Q12, Q14, Q15, Q17 and Q22 (the
+"""Python restatements of Q4, Q5, Q7, Q8, Q11, Q12, Q14, Q15, Q17 and Q22 (the
 semantics the GPU tests restate), pinned against the reference itself: its own load / build / query (compiled
 unchanged into oracle/_ref/ref_tpch_driver) answers the same requests on the
 same seeded Parquet files, on the CPU.  Q12 runs on data with receipts up to
@@ -141,7 +141,7 @@ def known(tmp_path_factory):
     d = write_tpch(tmp_path_factory.mktemp("tpch_known") / "d", n_customer=3000, n_orders=40000, seed=10,
                    customer_nations="known", n_supplier=25, n_part=199, orderless_customers=True)
     t = {n: pq.read_table(d / f"{n}.parquet")
-         for n in ("lineitem", "orders", "part", "supplier", "customer", "nation", "region")}
+         for n in ("lineitem", "orders", "part", "supplier", "customer", "nation", "region", "partsupp")}
     return d, t
 
 
@@ -288,6 +288,24 @@ def q22(t, codes):
     return [[p, str(n), f"{s / 100:.2f}"] for p, (n, s) in sorted(out.items())]
 
 
+def q11(t, nation, fraction):
+    N, S = t["nation"], t["supplier"]
+    PS = t["partsupp"]
+    key = first_wins(N["n_name"].to_pylist(), N["n_nationkey"].to_pylist()).get(nation)
+    if key is None:
+        return []
+    supp = {k for k, n in zip(S["s_suppkey"].to_pylist(), S["s_nationkey"].to_pylist()) if n == key}
+    value = scaled(PS["ps_supplycost"]) * PS["ps_availqty"].to_numpy().astype(np.int64)
+    sums, total = {}, 0
+    for pk, sk, v in zip(PS["ps_partkey"].to_pylist(), PS["ps_suppkey"].to_pylist(), value.tolist()):
+        if sk in supp:
+            sums[pk] = sums.get(pk, 0) + v
+            total += v
+    thr = total * float(fraction)
+    rows = sorted(((k, v) for k, v in sums.items() if v != 0 and v > thr), key=lambda x: (-x[1], x[0]))
+    return [[str(k), f"{v / 100:.2f}"] for k, v in rows]
+
+
 def q15(t, date):
     L, S = t["lineitem"], t["supplier"]
     start, end = offset(date), offset(date, 3)
@@ -322,6 +340,8 @@ def test_q5_q7_q8_q17_q22_restatements_match_the_reference(known, tmp_path):
         ('7 "NATION_01" "NATION_10"', lambda: q7(t, "NATION_01", "NATION_10")),
         ('7 "NATION_06" "NATION_06"', lambda: q7(t, "NATION_06", "NATION_06")),
         ('8 "NATION_10" "REGION0" "STD_B"', lambda: q8(t, "NATION_10", "REGION0", "STD_B")),
+        ('11 "NATION_04" "0.0001"', lambda: q11(t, "NATION_04", "0.0001")),
+        ('11 "NATION_19" "-1"', lambda: q11(t, "NATION_19", "-1")),
         ('15 "1996-01-01" "1"', lambda: q15(t, "1996-01-01")),
         ('15 "1995-11-30" "0"', lambda: q15(t, "1995-11-30")),
         ('17 "BRAND_B" "CONT_C"', lambda: q17(t, "BRAND_B", "CONT_C")),
@@ -331,6 +351,6 @@ def test_q5_q7_q8_q17_q22_restatements_match_the_reference(known, tmp_path):
     for (req, want), g in zip(cases, got):
         assert g[1:] == want(), req
     # every query family has a non-empty, non-zero answer among the cases
-    for q in ("5 ", "7 ", "8 ", "15 ", "17 ", "22 "):
+    for q in ("5 ", "7 ", "8 ", "11 ", "15 ", "17 ", "22 "):
         assert any(len(g) > 1 and any(x != "0.00" for row in g[1:] for x in (row[1:] if len(row) > 1 else row))
                    for (req, _), g in zip(cases, got) if req.startswith(q)), q
