@@ -65,3 +65,23 @@ def test_null_context_is_rejected():
     assert lib.bo_synchronize(None) == -1
     assert lib.bo_q1_fact_device(None, None, 0, 3, 2, None) == -1
     assert lib.bo_last_error(None) == b"null context"
+
+
+def declared_arities():
+    out = {}
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b(bo_\w+)\s*\(([^;{]*?)\)\s*;", text, flags=re.M | re.S):
+            params = m.group(2).strip()
+            out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_python_binding_arities_match_the_header():
+    from bespokeolap_artifacts_b200 import native
+
+    arity = declared_arities()
+    assert len(arity) >= 60
+    wrong = {name: (n, len(native._SIGNATURES[name][1])) for name, n in arity.items()
+             if name in native._SIGNATURES and len(native._SIGNATURES[name][1]) != n}
+    assert not wrong, wrong
