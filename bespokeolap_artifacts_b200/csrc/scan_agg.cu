@@ -355,7 +355,9 @@ int launch_q1_lineitem(bo_ctx* ctx, const bo_lineitem_cols& c, int32_t cutoff, u
 int check_fact(bo_ctx* ctx, const bo_fact_cols* c, int32_t nfa, int32_t nfb) {
   if (!c) return set_error(ctx, BO_ERR_INVALID, "q1: null column set");
   if (c->n_rows < 0) return set_error(ctx, BO_ERR_INVALID, "q1: negative row count");
-  if (nfa < 1 || nfb < 1 || nfa * nfb > BO_Q1_MAX_GROUPS)
+  // Each factor is bounded before the product is formed, so the product
+  // cannot overflow int32 (a wrapped product would pass the group bound).
+  if (nfa < 1 || nfb < 1 || nfa > BO_Q1_MAX_GROUPS || nfb > BO_Q1_MAX_GROUPS || nfa * nfb > BO_Q1_MAX_GROUPS)
     return set_error(ctx, BO_ERR_INVALID, "q1: group domain %d x %d exceeds %d groups", nfa, nfb,
                      BO_Q1_MAX_GROUPS);
   if (c->n_rows > 0) {
@@ -633,7 +635,9 @@ extern "C" int bo_q1_fact_device_noalloc(const bo_fact_cols* cols, int32_t ship_
                                          int32_t n_flag_b, bo_q1_agg* out_device, uint32_t* status_device,
                                          void* cuda_stream) {
   if (!cols || !out_device || cols->n_rows < 0) return BO_ERR_INVALID;
-  if (n_flag_a < 1 || n_flag_b < 1 || n_flag_a * n_flag_b > BO_Q1_MAX_GROUPS) return BO_ERR_INVALID;
+  if (n_flag_a < 1 || n_flag_b < 1 || n_flag_a > BO_Q1_MAX_GROUPS || n_flag_b > BO_Q1_MAX_GROUPS ||
+      n_flag_a * n_flag_b > BO_Q1_MAX_GROUPS)
+    return BO_ERR_INVALID;
   if (cols->n_rows > 0) {
     const void* ptrs[] = {cols->ship_date, cols->quantity, cols->ext_price, cols->discount,
                           cols->tax,       cols->flag_a,   cols->flag_b};

@@ -157,6 +157,10 @@ int bo_q1_fact_host(bo_ctx* ctx, const bo_fact_cols* host_cols, int32_t ship_cut
  * (cudaStream_t as void*, NULL = legacy default stream), the device columns,
  * out_device (n_flag_a*n_flag_b records) and an optional status_device word
  * that the kernel ORs device-side error bits into (the caller zeroes it).
+ * With status_device NULL, device-side errors (a value outside its range, a
+ * group code outside the domain, a 128-bit total that does not narrow) go
+ * unreported: the call still returns BO_OK and the totals may be partial, so
+ * pass a status word unless the inputs are known to be valid.
  * The kernel's scratch -- 128-bit per-group totals and a ticket counter --
  * is a fixed file-scope device array of (2*8*BO_Q1_MAX_GROUPS + 32) 64-bit
  * words (1,280 bytes) that every GPU loading this library holds until exit;
@@ -164,7 +168,10 @@ int bo_q1_fact_host(bo_ctx* ctx, const bo_fact_cols* host_cols, int32_t ship_cut
  * Each call clears that array on its stream first; calls that overlap on the
  * GPU share it and race, so the caller must serialise them.  The first call
  * on a device resolves the array's device address and sets a kernel
- * attribute: make it before any stream capture.  Returns BO_OK, BO_ERR_INVALID
+ * attribute: make it before any stream capture.  That address is kept per
+ * device number for the life of the process, so do not call this entry point
+ * again on a device after cudaDeviceReset there (the reset unloads the module
+ * and the kept address would be stale).  Returns BO_OK, BO_ERR_INVALID
  * or BO_ERR_CUDA (no message: there is no context). */
 int bo_q1_fact_device_noalloc(const bo_fact_cols* cols, int32_t ship_cutoff, int32_t n_flag_a,
                               int32_t n_flag_b, bo_q1_agg* out_device, uint32_t* status_device,

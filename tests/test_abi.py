@@ -85,3 +85,17 @@ def test_python_binding_arities_match_the_header():
     wrong = {name: (n, len(native._SIGNATURES[name][1])) for name, n in arity.items()
              if name in native._SIGNATURES and len(native._SIGNATURES[name][1]) != n}
     assert not wrong, wrong
+
+
+def test_no_alloc_rejects_group_factors_whose_product_wraps():
+    """65536 x 65536 wraps to 0 in 32-bit arithmetic; the entry point bounds
+    each factor first, so the call is rejected before any CUDA call (no GPU
+    needed)."""
+    import ctypes as C
+
+    from bespokeolap_artifacts_b200 import native
+
+    lib = native.lib()
+    cols = native.FactCols(*([None] * 7), 16)
+    for nfa, nfb in ((65536, 65536), (1 << 16, 1 << 15), (9, 1), (1, 9), (-1, 4)):
+        assert lib.bo_q1_fact_device_noalloc(C.byref(cols), 0, nfa, nfb, C.c_void_p(16), None, None) == -1
