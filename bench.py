@@ -579,9 +579,45 @@ def scan_agg_section(eng, stream, peak: float) -> dict:
         res[f"rows_{n}"] = {"us_per_launch": us, "rows_per_s": n / (us * 1e-6), "achieved_gbs": gbs,
                             "frac_of_measured_hbm": gbs / peak, "kernel": "q1_fact_kernel",
                             "algorithmic_bytes_per_launch": n * 38}
+        if n == 6_000_000:
+            try:
+                res["cpu_baseline"] = scan_agg_cpu_baseline(eng, cols[0], n, out)
+            except Exception as e:  # a prebuilt checker file; report, never fail the section
+                res["cpu_baseline"] = {"value": None, "error": f"{type(e).__name__}: {str(e)[:200]}"}
         del insts, cols
     torch.cuda.empty_cache()
     return res
+
+
+def scan_agg_cpu_baseline(eng, cols, n: int, out) -> dict:
+    """The reference's run_q1 (compiled unchanged into oracle/_ref) on one host
+    core over the same 6M rows mapped onto lineitem (DELTA 90 is the scan
+    config's cutoff); its group counts are checked against the GPU's."""
+    from bespokeolap_artifacts_b200 import datagen as dg
+    from bespokeolap_artifacts_b200 import native as N
+    from oracle import oracle as O
+
+    host = [c.cpu().numpy() for c in cols]
+    t = dg.FactTable(*host)
+    db = O.RefDatabase(dg.fact_as_lineitem(t))
+    try:
+        ref, _ = db.q1(90)
+        ts = []
+        t_end = time.perf_counter() + 10.0
+        while time.perf_counter() < t_end and len(ts) < 20:
+            ts.append(db.q1(90)[1])
+    finally:
+        db.close()
+    eng.q1_fact_device(cols, n, dg.Q1_CUTOFF, 3, 2, out)
+    eng.synchronize()
+    aggs = (N.Q1Agg * 6).from_buffer_copy(out.cpu().numpy().tobytes()[:6 * C.sizeof(N.Q1Agg)])
+    gpu_counts = sorted(a.count for a in aggs if a.count)
+    med = statistics.median(ts)
+    return {"value": n / (med * 1e-3), "unit": "rows/s", "cores": 1, "kind": "reference", "ms_per_query": med,
+            "gbs_over_38_b_per_row": n * 38 / (med * 1e-3) / 1e9,
+            "group_counts_equal_gpu": sorted(r["count_order"] for r in ref) == gpu_counts,
+            "sample": f"run_q1 (DELTA 90) on the 6,000,000 rows mapped to lineitem, {len(ts)} runs (median), "
+                      f"host {host_cpu()}"}
 
 
 def groupby_section(eng, stream, n_queries: int = 10, keep: dict | None = None) -> dict:
@@ -707,7 +743,12 @@ def groupby_section(eng, stream, n_queries: int = 10, keep: dict | None = None) 
             "answers_identical": bool(same_hc)},
     }
     del hc
+    try:
+        cpu = groupby_cpu_baseline(c, queries, exact)
+    except Exception as e:  # a prebuilt checker file; report, never fail the section
+        cpu = {"value": None, "error": f"{type(e).__name__}: {str(e)[:200]}"}
     return {
+        "cpu_baseline": cpu,
         "workload": "A 2,500,000 ids; B 36,000,000 (a_id Zipf 1.1, c_id Zipf 0.9); C 4,000,000 (category 0..112, "
                     "year 1900..2020); category in a seeded 8-value set, year in [1990, 2010]; group by a_id, "
                     "count + min(year), order by count desc, a_id asc, limit 10",
@@ -724,6 +765,37 @@ def groupby_section(eng, stream, n_queries: int = 10, keep: dict | None = None) 
                 f"{setup_s:.1f} s outside the timing",
         "partitioned": partition_out,
     }
+
+
+def groupby_cpu_baseline(cols: dict, queries: list, exact: list) -> dict:
+    """The CPU restatement of the group-by (oracle/bo_oracle.c: dense C mask,
+    dense per-id counts and min year, stable ordering, top 10; the reference's
+    dense-mask / dense-count pattern) on one host core over the same tables and
+    queries; its answers are checked against the GPU's."""
+    from bespokeolap_artifacts_b200 import datagen as dg
+    from oracle import oracle as O
+
+    host = {k: cols[k].cpu().numpy() for k in ("a_ids", "b_a", "b_c", "c_cat", "c_year")}
+    host["c_cat"] = host["c_cat"].view(np.uint16)  # stored as int16 on the device: same bits
+    ts, same = [], True
+    t_end = time.perf_counter() + 20.0
+    i = 0
+    while i < 3 or (time.perf_counter() < t_end and i < 9):
+        g = dg.GroupByInput(host["a_ids"], host["b_a"], host["b_c"], host["c_cat"], host["c_year"],
+                            np.asarray(queries[i % 3], np.uint16), 1990, 2010, 10)
+        t0 = time.perf_counter()
+        o = O.groupby_topk(g)
+        ts.append((time.perf_counter() - t0) * 1e3)
+        e = exact[i % 3]
+        same &= (o["n_groups"], o["joined_rows"], o["keys"], o["counts"], o["min_years"]) == (
+            e["n_groups"], e["joined_rows"], e["keys"], e["counts"], e["min_years"])
+        i += 1
+    med = statistics.median(ts)
+    rows = sum(len(v) for v in host.values()) - len(host["b_c"]) - len(host["c_year"])
+    return {"value": rows / (med * 1e-3), "unit": "rows/s", "cores": 1, "kind": "port", "ms_per_query": med,
+            "gbs_over_322_mb": 322_000_000 / (med * 1e-3) / 1e9, "answers_equal_gpu": bool(same),
+            "sample": f"{len(ts)} queries (3 category sets rotated) over the full A 2.5M / B 36M / C 4M tables, "
+                      f"median, host {host_cpu()}"}
 
 
 def join_large_section(eng, sizer, headline_feats) -> dict:

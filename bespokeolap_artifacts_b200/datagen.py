@@ -263,3 +263,47 @@ def join_as_q3_tables(j: JoinInput) -> tuple[dict, dict]:
         n_customer=j.n_build, c_custkey=j.b_key, c_mktsegment=j.b_seg,
     )
     return tables, dict(segment=j.seg_eq, date=date_string(j.date_lt))
+
+
+def groupby_joined_a_ids(g: GroupByInput) -> np.ndarray:
+    """a_id of every B row that survives the three-way join: its c_id names a
+    row of C whose category is in the set and whose year is in range, and its
+    a_id is an id of A.  Plain numpy; the group-by's input rows."""
+    n_c = len(g.c_cat)
+    cmask = np.isin(g.c_cat, np.asarray(g.cat_set, dtype=np.uint16)) & (g.c_year >= g.year_lo) & (
+        g.c_year <= g.year_hi)
+    cid = g.b_c.astype(np.int64)
+    inside = (cid >= 0) & (cid < n_c)
+    keep = inside.copy()
+    keep[inside] = cmask[cid[inside]]
+    a = g.b_a[keep]
+    return a[np.isin(a, g.a_ids)]
+
+
+def groupby_as_q18_tables(g: GroupByInput) -> dict:
+    """Maps the group-by's count onto run_q18's dense path
+    (bespoke_tpch/query_q18.cpp:205-262): one order per id 1..max(A) (dense
+    orderkeys, one customer), one lineitem of quantity 1.00 per joined B row
+    with l_orderkey = its a_id.  run_q18's sum_qty[orderkey] is then 100 x the
+    group's count, and QUANTITY "0" returns every group."""
+    a = groupby_joined_a_ids(g)
+    n_orders = int(max(int(g.a_ids.max()) if len(g.a_ids) else 1, 1))
+    n = len(a)
+    return dict(
+        n_lineitem=n,
+        l_orderkey=np.ascontiguousarray(a, dtype=np.int32),
+        l_shipdate=np.full(n, DATE_LO, np.int32),
+        l_quantity=np.ones(n, np.float64),
+        n_orders=n_orders, o_orderkey=np.arange(1, n_orders + 1, dtype=np.int32),
+        o_custkey=np.ones(n_orders, np.int32), o_orderdate=np.full(n_orders, DATE_LO, np.int32),
+        n_customer=1, c_custkey=np.ones(1, np.int32), c_mktsegment=np.zeros(1, np.uint8),
+    )
+
+
+def groupby_with_bad_ids(g: GroupByInput) -> GroupByInput:
+    """The group-by input with ids no table holds: negative c_ids and c_ids
+    past C (rows that join nothing) and a_ids that are not ids of A."""
+    g.b_c[::97] = -3
+    g.b_c[1::89] = len(g.c_cat) + 5
+    g.b_a[2::83] = 10 ** 8
+    return g

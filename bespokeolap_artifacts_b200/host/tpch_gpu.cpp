@@ -827,6 +827,136 @@ std::vector<Q15ResultRow> run_q15(const Database& db, const std::string& date) {
   return rows;
 }
 
+std::vector<Q9ResultRow> run_q9(const Database& db, const std::string& color) {
+  // query_q9.cpp:188-226: the years of the orders' date span (no orders: no rows).
+  if (db.n_orders == 0 || db.o_max_date < db.o_min_date) return {};
+  const int32_t n_dates = static_cast<int32_t>(db.o_max_date) - db.o_min_date + 1;
+  std::vector<int16_t> year_by_date(static_cast<size_t>(n_dates));
+  for (int32_t i = 0; i < n_dates; ++i) {
+    int y = 0;
+    unsigned m = 0, d = 0;
+    civil_from_days(static_cast<int64_t>(db.base_date_days) + db.o_min_date + i, y, m, d);
+    year_by_date[static_cast<size_t>(i)] = static_cast<int16_t>(y);
+  }
+  const int32_t first_year = year_by_date.front(), last_year = year_by_date.back();
+  const int32_t year_span = last_year - first_year + 1;
+  check(db.ctx,
+        bo_tpch_order_years(db.ctx, col<int32_t>(db.orderkey_to_row), db.n_orderkey_map, col<int16_t>(db.o_orderdate),
+                            db.n_orders, db.o_min_date, year_by_date.data(), n_dates, first_year,
+                            static_cast<uint8_t*>(db.o_year_by_key.ptr)),
+        "q9 order years");
+  // Groups (supplier nation, year) over nationkeys 0 .. the largest nation
+  // row key (query_q9.cpp:153-163, 310-312).
+  int32_t max_nationkey = 0;
+  for (int32_t k : db.nation_key) max_nationkey = std::max(max_nationkey, k);
+  std::vector<std::string> name_of(static_cast<size_t>(max_nationkey) + 1);
+  for (size_t i = 0; i < db.nation_key.size(); ++i)
+    if (db.nation_key[i] >= 0) name_of[static_cast<size_t>(db.nation_key[i])] = db.nation_row_name[i];
+  const int32_t nation_bound = max_nationkey + 1;
+  std::vector<int64_t> totals(static_cast<size_t>(nation_bound) * year_span);
+  std::vector<uint8_t> used(totals.size());
+  bo_tpch_q9_tables t{};
+  t.l_partkey = col<int32_t>(db.l_partkey);
+  t.l_suppkey = col<int32_t>(db.l_suppkey);
+  t.l_orderkey = col<int32_t>(db.l_orderkey);
+  t.l_quantity = col<int16_t>(db.l_quantity);
+  t.l_discounted_price = col<int32_t>(db.l_discounted_price);
+  t.l_supp_nation = col<int16_t>(db.l_supp_nation);
+  t.n_lineitem = db.n_lineitem;
+  t.p_name = col<char>(db.p_name);
+  t.p_name_offsets = col<uint32_t>(db.p_name_offsets);
+  t.p_partkey = col<int32_t>(db.p_partkey);
+  t.n_part = db.n_part;
+  t.ps_suppkey = col<int32_t>(db.ps_suppkey);
+  t.ps_supplycost = col<int32_t>(db.ps_supplycost);
+  t.ps_part_begin = col<int32_t>(db.ps_part_begin);
+  t.n_part_keys = db.n_ps_part_keys;
+  t.slots_per_part = db.ps_slots_per_part;
+  t.o_year_by_key = static_cast<const uint8_t*>(db.o_year_by_key.ptr);
+  t.n_orderkeys = db.n_orderkey_map;
+  check(db.ctx,
+        bo_tpch_q9(db.ctx, &t, color.data(), static_cast<int32_t>(color.size()), nation_bound, year_span,
+                   totals.data(), used.data()),
+        "q9");
+  std::vector<Q9ResultRow> rows;
+  for (int32_t n = 0; n < nation_bound; ++n) {
+    if (name_of[static_cast<size_t>(n)].empty()) continue;
+    for (int32_t y = 0; y < year_span; ++y) {
+      const size_t g = static_cast<size_t>(n) * year_span + y;
+      if (!used[g]) continue;
+      rows.push_back(Q9ResultRow{name_of[static_cast<size_t>(n)], first_year + y, totals[g]});
+    }
+  }
+  // ORDER BY nation, o_year DESC (query_q9.cpp:440-446)
+  std::sort(rows.begin(), rows.end(), [](const Q9ResultRow& a, const Q9ResultRow& b) {
+    if (a.nation != b.nation) return a.nation < b.nation;
+    return a.o_year > b.o_year;
+  });
+  return rows;
+}
+
+std::vector<Q19ResultRow> run_q19(const Database& db, const std::string quantity[3], const std::string brand[3]) {
+  // query_q19.cpp:133-157: every group off, or no partkey at all: one zero row.
+  bool enabled[3], any = false;
+  for (int g = 0; g < 3; ++g) any |= enabled[g] = quantity[g] != "<<NULL>>" && brand[g] != "<<NULL>>";
+  const int32_t max_key = std::max(db.max_partkey, db.max_lineitem_partkey);
+  if (!any || max_key < 0) return {Q19ResultRow{}};
+  auto trim = [](std::string_view v) {
+    while (!v.empty() && v.back() == ' ') v.remove_suffix(1);
+    return v;
+  };
+  // Ship-mode codes: the last dictionary entry that trims to each mode; the
+  // instruction code: the first that trims to it (query_q19.cpp:160-179).
+  int32_t mode1 = -1, mode2 = -1, instruct = -1;
+  for (size_t c = 0; c < db.shipmode.values.size(); ++c) {
+    const auto v = trim(db.shipmode.values[c]);
+    if (v == "AIR") mode1 = static_cast<int32_t>(c);
+    else if (v == "AIR REG") mode2 = static_cast<int32_t>(c);
+  }
+  for (size_t c = 0; c < db.shipinstruct.values.size() && instruct < 0; ++c)
+    if (trim(db.shipinstruct.values[c]) == "DELIVER IN PERSON") instruct = static_cast<int32_t>(c);
+  int32_t brand_code[3], qty_low[3];
+  const int32_t size_high[3] = {5, 10, 15};  // query_q19.cpp:221-240
+  for (int g = 0; g < 3; ++g) {
+    brand_code[g] = -1;
+    qty_low[g] = 0;
+    if (!enabled[g]) continue;
+    qty_low[g] = static_cast<int32_t>(std::llround(std::stod(quantity[g]) * kPriceScale));
+    for (size_t c = 0; c < db.brand.values.size(); ++c)
+      if (db.brand.values[c] == brand[g]) brand_code[g] = static_cast<int32_t>(c);
+  }
+  // The three container lists (query_q19.cpp:203-208), as group bits per code.
+  static const char* const kLists[3][4] = {{"SM CASE", "SM BOX", "SM PACK", "SM PKG"},
+                                           {"MED BAG", "MED BOX", "MED PKG", "MED PACK"},
+                                           {"LG CASE", "LG BOX", "LG PACK", "LG PKG"}};
+  std::vector<uint8_t> groups(db.container.values.size(), 0);
+  for (size_t c = 0; c < groups.size(); ++c)
+    for (int g = 0; g < 3; ++g)
+      for (const char* v : kLists[g])
+        if (db.container.values[c] == v) groups[c] |= static_cast<uint8_t>(1u << g);
+  bo_tpch_q19_tables t{};
+  t.l_shipmode = col<uint16_t>(db.l_shipmode);
+  t.l_shipinstruct = col<uint16_t>(db.l_shipinstruct);
+  t.l_partkey = col<int32_t>(db.l_partkey);
+  t.l_quantity = col<int16_t>(db.l_quantity);
+  t.l_extendedprice = col<int32_t>(db.l_extendedprice);
+  t.l_discount = col<uint8_t>(db.l_discount);
+  t.n_lineitem = db.n_lineitem;
+  t.p_row_by_key = col<int32_t>(db.p_row_by_key);
+  t.n_part_keys = db.p_row_by_key.rows;
+  t.p_brand = col<uint16_t>(db.p_brand);
+  t.p_container = col<uint16_t>(db.p_container);
+  t.p_size = col<int32_t>(db.p_size);
+  t.n_part = db.n_part;
+  t.n_mask = static_cast<int64_t>(max_key) + 1;
+  int64_t revenue = 0;
+  check(db.ctx,
+        bo_tpch_q19(db.ctx, &t, brand_code, groups.data(), static_cast<int32_t>(groups.size()), size_high, qty_low,
+                    mode1, mode2, instruct, &revenue),
+        "q19");
+  return {Q19ResultRow{revenue}};
+}
+
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container) {
   // query_q17.cpp:125-155: NULL arguments, no parts, or an unknown brand or
   // container give a zero row.
@@ -1102,6 +1232,23 @@ void write_q7_csv(const std::string& filename, const std::vector<Q7ResultRow>& r
         << static_cast<double>(r.revenue_raw) / kPriceScale << "\n";
 }
 
+void write_q9_csv(const std::string& filename, const std::vector<Q9ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q9.cpp:449-460
+  out << "nation,o_year,sum_profit\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows)
+    out << escape_csv(r.nation) << ',' << r.o_year << ',' << static_cast<double>(r.sum_profit_raw) / kPriceScale << "\n";
+}
+
+void write_q19_csv(const std::string& filename, const std::vector<Q19ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q19.cpp:340-351
+  out << "revenue\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows) out << static_cast<double>(r.revenue_raw) / (kPriceScale * kDiscountScale) << "\n";
+}
+
 void write_q8_csv(const std::string& filename, const std::vector<Q8ResultRow>& rows) {
   std::ofstream out(filename);  // query_q8.cpp:382-389
   out << "o_year,mkt_share\n";
@@ -1203,7 +1350,9 @@ Database::~Database() {
                           &l_shard_max_shipdate, &l_partkey, &p_promo_by_key, &l_supp_nation, &o_cust_nation,
                           &p_partkey, &p_brand, &p_container, &l_suppkey, &p_type, &c_acctbal_device,
                           &c_phone_prefix, &c_phone_pair, &o_has_order, &ps_partkey, &ps_suppkey, &ps_value,
-                          &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch};
+                          &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch, &p_name,
+                          &p_name_offsets, &ps_supplycost, &ps_part_begin, &o_year_by_key, &l_shipinstruct,
+                          &p_size, &p_row_by_key};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
   if (result_host) bo_host_free_pinned(ctx, result_host);
@@ -1272,9 +1421,10 @@ struct LineitemHost {
   std::vector<int32_t> orderkey, price, dprice, partkey, suppkey;
   std::vector<int16_t> ship, q16, shard_max_ship, supp_nation;
   std::vector<uint8_t> code, d8, t8;
-  std::vector<uint16_t> shipmode;
+  std::vector<uint16_t> shipmode, shipinstruct;
   std::vector<uint32_t> commit_receipt;
-  Dictionary returnflag, linestatus, shipmode_dict;
+  Dictionary returnflag, linestatus, shipmode_dict, shipinstruct_dict;
+  int32_t max_partkey = -1;
   bool orderkey_sorted = true;
   int32_t max_orderkey = -1;
 };
@@ -1364,6 +1514,11 @@ LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, const ParquetTa
     auto codes = dictionary_codes(column(L, "l_shipmode"), dict);
     return std::make_pair(std::move(codes), std::move(dict));
   });
+  auto shipinstruct = std::async(std::launch::async, [&] {
+    Dictionary dict;
+    auto codes = dictionary_codes(column(L, "l_shipinstruct"), dict);
+    return std::make_pair(std::move(codes), std::move(dict));
+  });
   auto price = std::async(std::launch::async, [&] { return scaled_values(column(L, "l_extendedprice"), kPriceScale); });
   auto discount = std::async(std::launch::async, [&] { return scaled_values(column(L, "l_discount"), kDiscountScale); });
   auto tax = std::async(std::launch::async, [&] { return scaled_values(column(L, "l_tax"), kDiscountScale); });
@@ -1405,6 +1560,10 @@ LineitemHost derive_lineitem(const ParquetTables::ArrowTable& L, const ParquetTa
   auto sm = shipmode.get();
   h.shipmode = std::move(sm.first);
   h.shipmode_dict = std::move(sm.second);
+  auto si = shipinstruct.get();
+  h.shipinstruct = std::move(si.first);
+  h.shipinstruct_dict = std::move(si.second);
+  for (int32_t k : h.partkey) h.max_partkey = std::max(h.max_partkey, k);
   // Q12's shard pruning can only drop a lineitem received more than 30 days
   // after shipping; without one the per-shard maxima are not needed.
   bool late = false;
@@ -1481,7 +1640,8 @@ CustomerHost derive_customer(const ParquetTables::ArrowTable& C) {
 struct PartHost {
   std::vector<int8_t> promo_by_key;
   int32_t max_key = -1;
-  std::vector<int32_t> key;
+  std::vector<int32_t> key, size, row_by_key;
+  StringColumn name;
   std::vector<uint16_t> brand, container, type;
   Dictionary brand_dict, container_dict, type_dict;
 };
@@ -1489,6 +1649,8 @@ struct PartHost {
 PartHost derive_part(const ParquetTables::ArrowTable& P) {
   PartHost h;
   h.key = int_values(column(P, "p_partkey"));
+  h.name = string_column(column(P, "p_name"));
+  h.size = int_values(column(P, "p_size"));
   const auto& key = h.key;
   h.brand = dictionary_codes(column(P, "p_brand"), h.brand_dict);
   h.container = dictionary_codes(column(P, "p_container"), h.container_dict);
@@ -1504,6 +1666,9 @@ PartHost derive_part(const ParquetTables::ArrowTable& P) {
   h.promo_by_key.assign(static_cast<size_t>(h.max_key) + 1, int8_t(-1));
   for (size_t i = 0; i < key.size(); ++i)
     if (key[i] >= 0) h.promo_by_key[static_cast<size_t>(key[i])] = promo_type[type[i]];
+  h.row_by_key.assign(static_cast<size_t>(h.max_key) + 1, -1);  // the last row of a key (query_q19.cpp:242)
+  for (size_t i = 0; i < key.size(); ++i)
+    if (key[i] >= 0) h.row_by_key[static_cast<size_t>(key[i])] = static_cast<int32_t>(i);
   return h;
 }
 
@@ -1562,6 +1727,9 @@ Database* build(ParquetTables* tables) {
       db->l_partkey = upload(ctx, h.partkey);
       db->l_supp_nation = upload(ctx, h.supp_nation);
       db->l_suppkey = upload(ctx, h.suppkey);
+      db->shipinstruct = std::move(h.shipinstruct_dict);
+      db->l_shipinstruct = upload(ctx, h.shipinstruct);
+      db->max_lineitem_partkey = h.max_partkey;
       phase("lineitem uploaded");
     }
     std::vector<int32_t> order_custkeys;  // date-sorted orders' custkeys, for orders.cust_nationkey
@@ -1570,6 +1738,12 @@ Database* build(ParquetTables* tables) {
       phase("orders derived");
       db->n_orders = static_cast<int64_t>(h.okey.size());
       db->n_orderkey_map = static_cast<int64_t>(h.map.size());
+      if (!h.odate.empty()) {  // date-sorted: the first and last rows
+        db->o_min_date = h.odate.front();
+        db->o_max_date = h.odate.back();
+      }
+      check(ctx, bo_device_alloc(ctx, std::max<size_t>(h.map.size(), 256), &db->o_year_by_key.ptr), "device alloc");
+      db->o_year_by_key.rows = db->n_orderkey_map;
       db->o_orderkey = upload(ctx, h.okey);
       db->o_custkey = upload(ctx, h.ckey);
       db->o_orderdate = upload(ctx, h.odate);
@@ -1660,6 +1834,10 @@ Database* build(ParquetTables* tables) {
       db->container = std::move(h.container_dict);
       db->p_type = upload(ctx, h.type);
       db->part_type = std::move(h.type_dict);
+      db->p_name = upload(ctx, std::vector<char>(h.name.data.begin(), h.name.data.end()));
+      db->p_name_offsets = upload(ctx, h.name.offsets);
+      db->p_size = upload(ctx, h.size);
+      db->p_row_by_key = upload(ctx, h.row_by_key);
     }
     // nation names by key (bespoke_tpch/builder_impl.cpp:780-803; query_q10.cpp:497-515)
     {
@@ -1685,12 +1863,35 @@ Database* build(ParquetTables* tables) {
       std::vector<uint32_t> order(pk.size());
       std::iota(order.begin(), order.end(), 0u);
       std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return pk[a] < pk[b]; });
-      std::vector<int32_t> spk(pk.size()), ssk(pk.size()), val(pk.size());
+      std::vector<int32_t> spk(pk.size()), ssk(pk.size()), val(pk.size()), scost(pk.size());
       for (size_t i = 0; i < order.size(); ++i) {
         spk[i] = pk[order[i]];
         ssk[i] = sk[order[i]];
+        scost[i] = cost[order[i]];
         val[i] = static_cast<int32_t>(static_cast<int64_t>(cost[order[i]]) * qty[order[i]]);
       }
+      // Q9's part slots (query_q9.cpp:140-186): keys 0 .. the largest part or
+      // partsupp key (0 without keys), each key's rows in this order.
+      int32_t max_part_key = 0;
+      for (int32_t k : spk) max_part_key = std::max(max_part_key, k);
+      if (db->max_partkey > max_part_key) max_part_key = db->max_partkey;
+      std::vector<int32_t> begin(static_cast<size_t>(max_part_key) + 2, 0);
+      int32_t slots = 0;
+      {
+        size_t r = 0;
+        while (r < spk.size() && spk[r] < 0) ++r;  // negative keys have no slot
+        for (int64_t k = 0; k <= max_part_key; ++k) {
+          begin[static_cast<size_t>(k)] = static_cast<int32_t>(r);
+          const size_t r0 = r;
+          while (r < spk.size() && spk[r] == k) ++r;
+          slots = std::max(slots, static_cast<int32_t>(r - r0));
+        }
+        begin[static_cast<size_t>(max_part_key) + 1] = static_cast<int32_t>(r);
+      }
+      db->n_ps_part_keys = static_cast<int64_t>(max_part_key) + 1;
+      db->ps_slots_per_part = std::max(slots, 1);
+      db->ps_supplycost = upload(ctx, scost);
+      db->ps_part_begin = upload(ctx, begin);
       db->n_partsupp = static_cast<int64_t>(pk.size());
       if (!spk.empty()) {
         db->ps_min_partkey = spk.front();
@@ -1829,6 +2030,20 @@ void query(Database* db) {
       const auto rows = run_q15(*db, date);
       const auto end = std::chrono::steady_clock::now();
       write_q15_csv(file, rows);
+      report(end);
+    } else if (r.id == "9") {
+      const std::string color = arg("COLOR");
+      const auto rows = run_q9(*db, color);
+      const auto end = std::chrono::steady_clock::now();
+      write_q9_csv(file, rows);
+      report(end);
+    } else if (r.id == "19") {
+      std::string quantity[3], brand[3];
+      for (int g = 0; g < 3; ++g) quantity[g] = arg(("QUANTITY" + std::to_string(g + 1)).c_str());
+      for (int g = 0; g < 3; ++g) brand[g] = arg(("BRAND" + std::to_string(g + 1)).c_str());
+      const auto rows = run_q19(*db, quantity, brand);
+      const auto end = std::chrono::steady_clock::now();
+      write_q19_csv(file, rows);
       report(end);
     } else if (r.id == "17") {
       const std::string brand = arg("BRAND");

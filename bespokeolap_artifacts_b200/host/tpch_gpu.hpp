@@ -76,7 +76,9 @@ struct Database {
   // Latest shipdate of each lineitem's builder shard; only built when some
   // lineitem is received more than 30 days after shipping (Q12's shard pruning).
   bo_tpch::DeviceColumn l_shard_max_shipdate;
-  bo_tpch::Dictionary returnflag, linestatus, shipmode;
+  bo_tpch::Dictionary returnflag, linestatus, shipmode, shipinstruct;
+  bo_tpch::DeviceColumn l_shipinstruct;  // dictionary codes (Q19)
+  int32_t max_lineitem_partkey = -1;
   bool lineitem_orderkey_sorted = true;
   int32_t max_lineitem_orderkey = -1;
   // orders, sorted by orderdate (stable); each row's lineitem range
@@ -105,8 +107,11 @@ struct Database {
   bo_tpch::DeviceColumn p_promo_by_key;
   int64_t n_promo_map = 0;
   int32_t max_partkey = -1;
-  // part rows: keys, brand and container codes (Q17)
-  bo_tpch::DeviceColumn p_partkey, p_brand, p_container, p_type;
+  // part rows: keys, brand and container codes (Q17); names as bytes with
+  // n_part + 1 offsets (Q9's color search on the device)
+  bo_tpch::DeviceColumn p_partkey, p_brand, p_container, p_type, p_name, p_name_offsets;
+  // part sizes and the last part row of each key 0 .. max_partkey, -1 = none (Q19)
+  bo_tpch::DeviceColumn p_size, p_row_by_key;
   int64_t n_part = 0;
   bo_tpch::Dictionary brand, container, part_type;
   // nation names by nationkey in [0, nation_bound) (last row of each key)
@@ -118,6 +123,17 @@ struct Database {
   // partsupp sorted by partkey (stable), value = supplycost * availqty (x100)
   bo_tpch::DeviceColumn ps_partkey, ps_suppkey, ps_value;
   int64_t n_partsupp = 0;
+  // Q9: supplycost (x100) in the same order; each partkey's rows
+  // [ps_part_begin[k], ps_part_begin[k + 1]) for k in [0, n_ps_part_keys)
+  // (the largest part / partsupp key + 1, query_q9.cpp:140-141) and the
+  // largest row count of a key (the reference's slots per part)
+  bo_tpch::DeviceColumn ps_supplycost, ps_part_begin;
+  int64_t n_ps_part_keys = 0;
+  int32_t ps_slots_per_part = 1;
+  // orders' first and last date offsets; Q9's per-orderkey year table
+  // (filled per query, n_orderkey_map entries)
+  int16_t o_min_date = 0, o_max_date = -1;
+  bo_tpch::DeviceColumn o_year_by_key;
   int32_t ps_min_partkey = 0, ps_max_partkey = -1;
   // supplier rows' keys and nationkeys (Q7's supplier tags), strings (Q15)
   std::vector<int32_t> s_suppkey, s_nationkey;
@@ -188,6 +204,16 @@ struct Q22ResultRow {
   std::string cntrycode;
   int64_t numcust = 0;
   int64_t totacctbal_raw = 0;
+};
+
+struct Q9ResultRow {
+  std::string nation;
+  int32_t o_year = 0;
+  int64_t sum_profit_raw = 0;
+};
+
+struct Q19ResultRow {
+  int64_t revenue_raw = 0;
 };
 
 struct Q11ResultRow {
@@ -261,6 +287,8 @@ std::vector<Q8ResultRow> run_q8(const Database& db, const std::string& nation, c
 std::vector<Q22ResultRow> run_q22(const Database& db, const std::vector<std::string>& codes);
 std::vector<Q11ResultRow> run_q11(const Database& db, const std::string& nation, const std::string& fraction);
 std::vector<Q15ResultRow> run_q15(const Database& db, const std::string& date);
+std::vector<Q9ResultRow> run_q9(const Database& db, const std::string& color);
+std::vector<Q19ResultRow> run_q19(const Database& db, const std::string quantity[3], const std::string brand[3]);
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container);
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date);
 std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmode1, const std::string& shipmode2,
@@ -279,6 +307,8 @@ void write_q8_csv(const std::string& filename, const std::vector<Q8ResultRow>& r
 void write_q22_csv(const std::string& filename, const std::vector<Q22ResultRow>& rows);
 void write_q11_csv(const std::string& filename, const std::vector<Q11ResultRow>& rows);
 void write_q15_csv(const std::string& filename, const std::vector<Q15ResultRow>& rows);
+void write_q9_csv(const std::string& filename, const std::vector<Q9ResultRow>& rows);
+void write_q19_csv(const std::string& filename, const std::vector<Q19ResultRow>& rows);
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows);
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows);
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);

@@ -279,6 +279,29 @@ class TpchQ17Tables(C.Structure):
                 ("p_container", C.c_void_p), ("n_part", C.c_int64), ("max_partkey", C.c_int32), ("pad", C.c_int32)]
 
 
+class TpchQ9Tables(C.Structure):
+    """``bo_tpch_q9_tables``: lineitem partkeys, suppkeys, orderkeys, quantities, discounted prices and
+    supplier nations; part names (bytes + offsets) and keys; partsupp suppkeys and supply costs sorted by
+    partkey with per-key row offsets; the per-orderkey year table."""
+    _fields_ = [("l_partkey", C.c_void_p), ("l_suppkey", C.c_void_p), ("l_orderkey", C.c_void_p),
+                ("l_quantity", C.c_void_p), ("l_discounted_price", C.c_void_p), ("l_supp_nation", C.c_void_p),
+                ("n_lineitem", C.c_int64), ("p_name", C.c_void_p), ("p_name_offsets", C.c_void_p),
+                ("p_partkey", C.c_void_p), ("n_part", C.c_int64), ("ps_suppkey", C.c_void_p),
+                ("ps_supplycost", C.c_void_p), ("ps_part_begin", C.c_void_p), ("n_part_keys", C.c_int64),
+                ("slots_per_part", C.c_int32), ("pad", C.c_int32), ("o_year_by_key", C.c_void_p),
+                ("n_orderkeys", C.c_int64)]
+
+
+class TpchQ19Tables(C.Structure):
+    """``bo_tpch_q19_tables``: lineitem ship-mode and ship-instruct codes, partkeys, quantities, prices and
+    discounts; the last part row per key, part brand / container codes and sizes; the mask's key count."""
+    _fields_ = [("l_shipmode", C.c_void_p), ("l_shipinstruct", C.c_void_p), ("l_partkey", C.c_void_p),
+                ("l_quantity", C.c_void_p), ("l_extendedprice", C.c_void_p), ("l_discount", C.c_void_p),
+                ("n_lineitem", C.c_int64), ("p_row_by_key", C.c_void_p), ("n_part_keys", C.c_int64),
+                ("p_brand", C.c_void_p), ("p_container", C.c_void_p), ("p_size", C.c_void_p), ("n_part", C.c_int64),
+                ("n_mask", C.c_int64)]
+
+
 class TpchQ14Tables(C.Structure):
     """``bo_tpch_q14_tables``: lineitem shipdates, partkeys, discounted prices; the part promo flag per key."""
     _fields_ = [("l_shipdate", C.c_void_p), ("l_partkey", C.c_void_p), ("l_discounted_price", C.c_void_p),
@@ -411,6 +434,11 @@ _SIGNATURES = {
     "bo_tpch_q15": (C.c_int, [_P, C.POINTER(TpchQ15Tables), C.c_int64, C.c_int16, C.c_int16, C.POINTER(C.c_int64),
                               C.POINTER(C.c_int64)]),
     "bo_tpch_q17": (C.c_int, [_P, C.POINTER(TpchQ17Tables), C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
+    "bo_tpch_q19": (C.c_int, [_P, C.POINTER(TpchQ19Tables), C.POINTER(C.c_int32), _P, C.c_int32,
+                              C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.c_int32,
+                              C.POINTER(C.c_int64)]),
+    "bo_tpch_q9": (C.c_int, [_P, C.POINTER(TpchQ9Tables), C.c_char_p, C.c_int32, C.c_int32, C.c_int32, _P, _P]),
+    "bo_tpch_order_years": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, C.c_int16, _P, C.c_int32, C.c_int32, _P]),
     "bo_tpch_q14": (C.c_int, [_P, C.POINTER(TpchQ14Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,
                               C.c_int16, C.POINTER(C.c_int64)]),

@@ -38,7 +38,9 @@ Key layouts (they select the reference's code paths):
                     its parity data covers every lineitem partkey.
 Regions REGION0..REGION4 (keys 0..4; nations' regionkey = nationkey % 5) and
 a later row repeating REGION1 with key 9.
-Ship modes MODE_A..MODE_G; order priorities 1-URGENT and 2-HIGH (the two the
+Part names are three words of COLORS.  Ship modes MODE_A..MODE_G, AIR and AIR REG, ship
+instructions from SHIPINSTRUCTS (one with trailing spaces), containers CONT_A..CONT_D and
+Q19's twelve (a stream of their own for the instructions); order priorities 1-URGENT and 2-HIGH (the two the
 reference's Q12 counts as high) and three others; part types with and
 without the PROMO prefix Q14 looks for.  Commit dates 30..90 days
 after the order, receipts 1..30 days after shipping.  These columns come from
@@ -55,11 +57,19 @@ import pyarrow.parquet as pq
 
 SEGMENTS = ["SEG_A", "SEG_B", "SEG_C", "SEG_D", "SEG_E"]
 WORDS = ["ironic", "quick", "pending", "bold", 'say "hi"', "a,b", "deposits", "", "x\"y", "final"]
-SHIPMODES = ["MODE_A", "MODE_B", "MODE_C", "MODE_D", "MODE_E", "MODE_F", "MODE_G"]
+# the two ship modes, the ship instruction and the container lists run_q19
+# compares against (bespoke_tpch/query_q19.cpp:160-179, 203-208), among others
+SHIPMODES = ["MODE_A", "MODE_B", "MODE_C", "MODE_D", "MODE_E", "MODE_F", "MODE_G", "AIR", "AIR REG"]
+SHIPINSTRUCTS = ["DELIVER IN PERSON", "LEAVE AT DOOR", "HOLD AT DEPOT", "DELIVER IN PERSON  "]
+Q19_CONTAINERS = ["SM CASE", "SM BOX", "SM PACK", "SM PKG", "MED BAG", "MED BOX", "MED PKG", "MED PACK",
+                  "LG CASE", "LG BOX", "LG PACK", "LG PKG"]
 PRIORITIES = ["1-URGENT", "2-HIGH", "3-PRIO_C", "4-PRIO_D", "5-PRIO_E"]
 PART_TYPES = ["PROMO_A", "PROMO_B", "STD_A", "STD_B", "ECO_A", "PROMOTION", "PROM", "LARGE_PROMO"]
 BRANDS = ["BRAND_A", "BRAND_B", "BRAND_C", "BRAND_D", "BRAND_E"]
-CONTAINERS = ["CONT_A", "CONT_B", "CONT_C", "CONT_D"]
+# part-name words (Q9 looks for a substring of the name)
+COLORS = ["amber", "azure", "cobalt", "coral", "crimson", "ivory", "jade", "khaki", "lilac", "maroon", "ochre",
+          "olive", "pearl", "plum", "rust", "sage", "sand", "slate", "teal", "umber"]
+CONTAINERS = ["CONT_A", "CONT_B", "CONT_C", "CONT_D"] + Q19_CONTAINERS
 D1992 = 8035  # 1992-01-01 in days since 1970-01-01
 
 
@@ -167,7 +177,8 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
         "l_shipdate": pa.array(ship.astype(np.int32), pa.date32()),
         "l_commitdate": pa.array(commit.astype(np.int32), pa.date32()),
         "l_receiptdate": pa.array(receipt.astype(np.int32), pa.date32()),
-        "l_shipinstruct": ["DELIVER IN PERSON"] * n, "l_shipmode": [SHIPMODES[i] for i in mode],
+        "l_shipinstruct": [SHIPINSTRUCTS[i] for i in np.random.default_rng([seed, 16]).integers(0, 4, n)],
+        "l_shipmode": [SHIPMODES[i] for i in mode],
         "l_comment": [""] * n,
     }), out / "lineitem.parquet")
     one = np.ones(1, np.int32)
@@ -181,7 +192,11 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
     psize = rng3.integers(1, 51, rows_p).astype(np.int32)
     pbrand = [BRANDS[i] for i in rng3.integers(0, len(BRANDS), rows_p)]
     pcont = [CONTAINERS[i] for i in rng3.integers(0, len(CONTAINERS), rows_p)]
-    pq.write_table(pa.table({"p_partkey": pkey, "p_name": [f"part {k}" for k in pkey], "p_mfgr": ["m"] * rows_p,
+    # names of three words from COLORS (a stream of their own, so the other
+    # part columns do not depend on them)
+    rng5 = np.random.default_rng([seed, 15])
+    pname = [" ".join(COLORS[i] for i in row) for row in rng5.integers(0, len(COLORS), (rows_p, 3))]
+    pq.write_table(pa.table({"p_partkey": pkey, "p_name": pname, "p_mfgr": ["m"] * rows_p,
                              "p_brand": pbrand, "p_type": ptype, "p_size": psize, "p_container": pcont,
                              "p_retailprice": _dec(np.ones(rows_p), decimal), "p_comment": [""] * rows_p}),
                    out / "part.parquet")

@@ -823,6 +823,92 @@ typedef struct bo_tpch_q17_tables {
 int bo_tpch_q17(bo_ctx* ctx, const bo_tpch_q17_tables* tables, int32_t brand_code, int32_t container_code,
                 int64_t* sum_out);
 
+/* TPC-H Q9 over the storage-plan layout: run_q9 of
+ * bespoke_tpch/query_q9.cpp:130-447.  Parts whose name contains `color`
+ * (byte substring, :147-150; an empty color matches every name) with keys in
+ * [0, n_part_keys); their lineitems whose (partkey, suppkey) has a partsupp
+ * row -- the first of the partkey's rows in partsupp order with that
+ * suppkey (:160-186 and the slot scans of :262-300) -- add
+ * discounted_price - supplycost * quantity / 100 (int64, truncated) to
+ * totals_out[supp_nation * year_span + year], year = o_year_by_key[orderkey]
+ * (the order's year minus the first order year; 255 = no order), and set
+ * used_out at the same index (:313-318).  partsupp is sorted by partkey
+ * (stable, as the builder sorts it); ps_part_begin[k] .. ps_part_begin[k+1]
+ * are partkey k's rows (n_part_keys + 1 offsets).  slots_per_part is the
+ * largest row count of a partkey: when it is 4 the reference tests all four
+ * slots of every part, and the empty ones carry suppkey -1 and cost 0
+ * (:262-291), which this entry point reproduces.  Lineitems with a negative
+ * supplier nation, a nation at or beyond nation_bound, an orderkey outside
+ * o_year_by_key or a year offset at or beyond year_span, or a partkey outside
+ * [0, n_part_keys) add nothing (the reference reads out of bounds there). */
+typedef struct bo_tpch_q9_tables {
+  const int32_t* l_partkey;            /* 32-byte aligned */
+  const int32_t* l_suppkey;
+  const int32_t* l_orderkey;
+  const int16_t* l_quantity;           /* x100 */
+  const int32_t* l_discounted_price;   /* x100 */
+  const int16_t* l_supp_nation;
+  int64_t n_lineitem;
+  const char* p_name;                  /* part names, concatenated */
+  const uint32_t* p_name_offsets;      /* n_part + 1 */
+  const int32_t* p_partkey;
+  int64_t n_part;
+  const int32_t* ps_suppkey;           /* partsupp sorted by partkey */
+  const int32_t* ps_supplycost;        /* x100 */
+  const int32_t* ps_part_begin;        /* n_part_keys + 1 */
+  int64_t n_part_keys;                 /* largest part / partsupp key + 1 */
+  int32_t slots_per_part;
+  int32_t pad;
+  const uint8_t* o_year_by_key;
+  int64_t n_orderkeys;
+} bo_tpch_q9_tables;
+
+int bo_tpch_q9(bo_ctx* ctx, const bo_tpch_q9_tables* tables, const char* color, int32_t color_len,
+               int32_t nation_bound, int32_t year_span, int64_t* totals_out, uint8_t* used_out);
+
+/* The order-year table run_q9 derives (bespoke_tpch/query_q9.cpp:188-226):
+ * out_device[k] = year(orderdate of row orderkey_to_row[k]) - first_year
+ * (the map keeps the last date-sorted row of each orderkey, as run_q9's loop
+ * over the rows does), 255 where the map holds no row; n_keys entries.
+ * year_by_date_host holds the year of each date offset in
+ * [min_orderdate, min_orderdate + n_dates). */
+int bo_tpch_order_years(bo_ctx* ctx, const int32_t* orderkey_to_row, int64_t n_keys, const int16_t* o_orderdate,
+                        int64_t n_orders, int16_t min_orderdate, const int16_t* year_by_date_host, int32_t n_dates,
+                        int32_t first_year, uint8_t* out_device);
+
+/* TPC-H Q19 over the storage-plan layout: run_q19 of
+ * bespoke_tpch/query_q19.cpp:130-338.  A partkey k in [0, n_mask) belongs to
+ * group g (bit g of its mask, g = 0, 1, 2) when the last part row of k
+ * (p_row_by_key[k]; -1 = no part row, mask 0) has brand_code[g] (-1: group
+ * off or brand unknown), a container whose code has bit g set in
+ * container_groups_host[code] (n_containers bytes) and a size in
+ * [1, size_high[g]].  Lineitems with shipmode code mode1 or mode2 (-1:
+ * none), shipinstruct code instruct_code, a partkey in [0, n_mask) whose
+ * mask is non-zero and a quantity (x100) in [qty_low[g], qty_low[g] + 1000]
+ * for a group of the mask add extendedprice * (100 - discount) to
+ * *revenue_out (x1e4).  Partkeys outside [0, n_mask) add nothing (the
+ * reference reads out of bounds there). */
+typedef struct bo_tpch_q19_tables {
+  const uint16_t* l_shipmode;          /* dictionary codes, 16-byte aligned */
+  const uint16_t* l_shipinstruct;      /* dictionary codes, 16-byte aligned */
+  const int32_t* l_partkey;
+  const int16_t* l_quantity;           /* x100 */
+  const int32_t* l_extendedprice;      /* x100 */
+  const uint8_t* l_discount;           /* x100 */
+  int64_t n_lineitem;
+  const int32_t* p_row_by_key;         /* last part row of each key, -1 = none */
+  int64_t n_part_keys;                 /* entries of p_row_by_key */
+  const uint16_t* p_brand;             /* dictionary codes per part row */
+  const uint16_t* p_container;
+  const int32_t* p_size;
+  int64_t n_part;
+  int64_t n_mask;                      /* largest part / lineitem partkey + 1 */
+} bo_tpch_q19_tables;
+
+int bo_tpch_q19(bo_ctx* ctx, const bo_tpch_q19_tables* tables, const int32_t brand_code[3],
+                const uint8_t* container_groups_host, int32_t n_containers, const int32_t size_high[3],
+                const int32_t qty_low[3], int32_t mode1, int32_t mode2, int32_t instruct_code, int64_t* revenue_out);
+
 /* TPC-H Q12 over the storage-plan layout: run_q12 of
  * bespoke_tpch/query_q12.cpp:162-360.  Lineitems whose shipmode code is
  * mode_code1 or mode_code2 (-1: none), with shipdate < commitdate <

@@ -193,6 +193,8 @@ def ref_lib(trace: bool = False) -> C.CDLL:
         l.ref_q3.restype = C.c_int64
         l.ref_q3.argtypes = [_P, C.c_int32, C.c_char_p, C.POINTER(C.c_int64), _P, _P, C.c_int64,
                              C.POINTER(C.c_double)]
+        l.ref_q18.restype = C.c_int64
+        l.ref_q18.argtypes = [_P, C.c_char_p, _P, _P, C.c_int64, C.POINTER(C.c_double)]
         l.ref_q6.argtypes = [_P, C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
         l.ref_parallel.restype = C.c_double
         l.ref_parallel.argtypes = [C.POINTER(_P), C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_char_p,
@@ -287,6 +289,16 @@ class RefDatabase:
             self.lib.ref_trace_end(buf, 1 << 16)
             out["trace"] = parse_trace(buf.value.decode())
         return out
+
+    def q18(self, quantity: str, max_rows: int) -> tuple[np.ndarray, np.ndarray, float]:
+        """run_q18's result rows in its own order: (orderkeys, sum_qty_raw, ms)."""
+        ok = np.zeros(max(max_rows, 1), np.int32)
+        sq = np.zeros(max(max_rows, 1), np.int64)
+        ms = C.c_double()
+        n = self.lib.ref_q18(self.handle, quantity.encode(), ok.ctypes.data, sq.ctypes.data, max_rows, C.byref(ms))
+        if n > max_rows:
+            raise RuntimeError(f"run_q18 returned {n} rows, more than the {max_rows} asked for")
+        return ok[:n], sq[:n], ms.value
 
     def q6(self, date: str, discount: str, quantity: str) -> tuple[int, float]:
         r = C.c_int64()

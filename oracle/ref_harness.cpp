@@ -306,6 +306,23 @@ int ref_q6(void* db, const char* date, const char* discount, const char* quantit
   return (int)out.size();
 }
 
+// run_q18 (bespoke_tpch/query_q18.cpp:183) with QUANTITY = quantity (decimal
+// text).  Returns the number of result rows and writes, in the reference's
+// output order, each row's orderkey and sum_qty_raw (x100) up to max_rows.
+int64_t ref_q18(void* db, const char* quantity, int32_t* orderkeys, int64_t* sum_qty, int64_t max_rows,
+                double* elapsed_ms) {
+  Q18Args args;
+  args.QUANTITY = quantity;
+  const auto t0 = std::chrono::steady_clock::now();
+  auto out = run_q18(*static_cast<Database*>(db), args);
+  if (elapsed_ms) *elapsed_ms = ms_since(t0);
+  for (size_t i = 0; i < out.size() && (int64_t)i < max_rows; ++i) {
+    if (orderkeys) orderkeys[i] = out[i].o_orderkey;
+    if (sum_qty) sum_qty[i] = out[i].sum_qty_raw;
+  }
+  return (int64_t)out.size();
+}
+
 // Runs run_q1 (which != 3) or run_q3 on n_db independent databases, one host
 // thread each, and returns the wall time of the slowest: the reference path
 // spread over row shards (its sums are decomposable).

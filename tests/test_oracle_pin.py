@@ -159,3 +159,32 @@ def test_join_oracle_matches_live_reference_q3():
     o = O.join_agg(j)
     assert r["revenue_sum"] == o["sum_trunc"]
     assert r["trace"]["q3_lineitem_scan_rows_emitted"] == o["match_count"]
+
+
+GB_CASES = json.loads((GOLDEN / "groupby_q18_reference.json").read_text())
+
+
+def groupby_golden_input(case):
+    """Regenerates a group-by fixture's input (tests/golden/make_golden_groupby.py)
+    and checks it against the fixture's SHA-256."""
+    import sys
+
+    if str(GOLDEN) not in sys.path:
+        sys.path.insert(0, str(GOLDEN))
+    import make_golden_groupby as MG
+
+    g = MG.make_case(case["n_a"], case["n_b"], case["n_c"], case["seed"], case["variant"])
+    assert MG.input_sha(g) == case["input_sha256"], "the seeded generator changed: regenerate the fixtures"
+    return g
+
+
+@pytest.mark.parametrize("case", GB_CASES, ids=lambda c: f"b{c['n_b']}-seed{c['seed']}-{c['variant']}")
+def test_groupby_oracle_matches_reference_q18_golden(case):
+    """Counts, group count, joined rows and (count desc, a_id asc) order of the
+    C restatement equal run_q18's dense aggregation of the same joined rows."""
+    g = groupby_golden_input(case)
+    r = O.groupby_topk(g, k=len(case["keys"]) or 1)
+    assert r["n_groups"] == case["n_groups"]
+    assert r["joined_rows"] == case["joined_rows"]
+    assert r["keys"] == case["keys"]
+    assert r["counts"] == case["counts"]

@@ -1,4 +1,4 @@
-"""Python restatements of Q4, Q5, Q7, Q8, Q11, Q12, Q14, Q15, Q17 and Q22 (the
+"""Python restatements of Q4, Q5, Q7, Q8, Q9, Q11, Q12, Q14, Q15, Q17, Q19 and Q22 (the
 semantics the GPU tests restate), pinned against the reference itself: its own load / build / query (compiled
 unchanged into oracle/_ref/ref_tpch_driver) answers the same requests on the
 same seeded Parquet files, on the CPU.  Q12 runs on data with receipts up to
@@ -328,7 +328,80 @@ def q15(t, date):
     return list(csv.reader(lines))
 
 
-def test_q5_q7_q8_q17_q22_restatements_match_the_reference(known, tmp_path):
+def q9(t, color):
+    """run_q9 (bespoke_tpch/query_q9.cpp:130-447) restated: parts whose name
+    contains the color, the first partsupp row (sorted by partkey, stable) of
+    each (partkey, suppkey), the supplier nation and order year per lineitem,
+    profit = discounted price - supplycost * quantity / 100 per (nation,
+    year), ordered by nation name, year descending."""
+    P, PS, L, O, S, N = (t[k] for k in ("part", "partsupp", "lineitem", "orders", "supplier", "nation"))
+    ok_parts = {k for k, nm in zip(P["p_partkey"].to_pylist(), P["p_name"].to_pylist()) if color in nm}
+    ps_pk = PS["ps_partkey"].to_numpy()
+    order = np.argsort(ps_pk, kind="stable")
+    cost = {}
+    for pk, sk, c in zip(ps_pk[order].tolist(), PS["ps_suppkey"].to_numpy()[order].tolist(),
+                         scaled(PS["ps_supplycost"])[order].tolist()):
+        cost.setdefault((pk, sk), c)
+    nation_of_supp = last_wins(S["s_suppkey"].to_pylist(), S["s_nationkey"].to_pylist())
+    years = (np.datetime64("1992-01-01") + days(O["o_orderdate"]).astype("timedelta64[D]")).astype("datetime64[Y]")
+    year_of_order = dict(zip(O["o_orderkey"].to_pylist(), (years.astype(np.int64) + 1970).tolist()))
+    name = last_wins(N["n_nationkey"].to_pylist(), N["n_name"].to_pylist())
+    qty, dp = scaled(L["l_quantity"]), dprices(L)
+    sums = {}
+    for pk, sk, ok, q, v in zip(L["l_partkey"].to_pylist(), L["l_suppkey"].to_pylist(), L["l_orderkey"].to_pylist(),
+                                qty.tolist(), dp.tolist()):
+        if pk not in ok_parts or (pk, sk) not in cost:
+            continue
+        nat = nation_of_supp.get(sk, -1)
+        if nat < 0 or nat not in name:
+            continue
+        g = (name[nat], year_of_order[ok])
+        sums[g] = sums.get(g, 0) + v - cost[(pk, sk)] * q // 100
+    return [[n, str(y), f"{v / 100:.2f}"] for (n, y), v in sorted(sums.items(), key=lambda x: (x[0][0], -x[0][1]))]
+
+
+Q19_LISTS = ({"SM CASE", "SM BOX", "SM PACK", "SM PKG"}, {"MED BAG", "MED BOX", "MED PKG", "MED PACK"},
+             {"LG CASE", "LG BOX", "LG PACK", "LG PKG"})
+
+
+def q19(t, quantity, brand):
+    """run_q19 (bespoke_tpch/query_q19.cpp:130-338) restated: a mask per
+    partkey from its last part row (brand, container list, size 1..5 / 10 /
+    15 per group), lineitems of ship mode AIR or AIR REG and instruction
+    DELIVER IN PERSON (right-trimmed) whose quantity lies in [q, q + 10] for a
+    group of the mask; revenue = sum price * (100 - discount).  Of the
+    instruction's spellings only the first to appear counts (:170-179)."""
+    P, L = t["part"], t["lineitem"]
+    on = [q != "<<NULL>>" and b != "<<NULL>>" for q, b in zip(quantity, brand)]
+    if not any(on):
+        return [["0.00"]]
+    mask = {}
+    for k, b, c, sz in zip(P["p_partkey"].to_pylist(), P["p_brand"].to_pylist(), P["p_container"].to_pylist(),
+                           P["p_size"].to_pylist()):
+        m = 0
+        for g, hi in enumerate((5, 10, 15)):
+            if on[g] and b == brand[g] and c in Q19_LISTS[g] and 1 <= sz <= hi:
+                m |= 1 << g
+        mask[k] = m
+    lo = [round(float(q) * 100) if on[g] else 0 for g, q in enumerate(quantity)]
+    mode = [m.rstrip(" ") for m in L["l_shipmode"].to_pylist()]
+    # one instruction code: the first value (in order of appearance) that
+    # trims to the instruction; rows of other spellings do not count
+    raw = L["l_shipinstruct"].to_pylist()
+    want = next((v for v in dict.fromkeys(raw) if v.rstrip(" ") == "DELIVER IN PERSON"), None)
+    instr = ["DELIVER IN PERSON" if v == want else "" for v in raw]
+    qty, price, disc = scaled(L["l_quantity"]), scaled(L["l_extendedprice"]), scaled(L["l_discount"])
+    total = 0
+    for i, pk in enumerate(L["l_partkey"].to_pylist()):
+        m = mask.get(pk, 0)
+        if not m or mode[i] not in ("AIR", "AIR REG") or instr[i] != "DELIVER IN PERSON":
+            continue
+        if any((m >> g) & 1 and lo[g] <= qty[i] <= lo[g] + 1000 for g in range(3)):
+            total += int(price[i]) * (100 - int(disc[i]))
+    return [[f"{total / 10000:.2f}"]]
+
+
+def test_q5_q7_q8_q9_q17_q19_q22_restatements_match_the_reference(known, tmp_path):
     data, t = known
     cases = [
         ('5 "REGION0" "1994-01-01"', lambda: q5(t, "REGION0", "1994-01-01")),
@@ -345,12 +418,21 @@ def test_q5_q7_q8_q17_q22_restatements_match_the_reference(known, tmp_path):
         ('15 "1996-01-01" "1"', lambda: q15(t, "1996-01-01")),
         ('15 "1995-11-30" "0"', lambda: q15(t, "1995-11-30")),
         ('17 "BRAND_B" "CONT_C"', lambda: q17(t, "BRAND_B", "CONT_C")),
+        ('19 "1" "10" "20" "BRAND_A" "BRAND_B" "BRAND_C"',
+         lambda: q19(t, ["1", "10", "20"], ["BRAND_A", "BRAND_B", "BRAND_C"])),
+        ('19 "5" "<<NULL>>" "30" "BRAND_D" "BRAND_D" "BRAND_D"',
+         lambda: q19(t, ["5", "<<NULL>>", "30"], ["BRAND_D", "BRAND_D", "BRAND_D"])),
+        ('19 "2.5" "2.5" "2.5" "BRAND_E" "BRAND_E" "BRAND_E"',
+         lambda: q19(t, ["2.5", "2.5", "2.5"], ["BRAND_E", "BRAND_E", "BRAND_E"])),
+        ('9 "co"', lambda: q9(t, "co")),
+        ('9 "slate"', lambda: q9(t, "slate")),
+        ('9 "e p"', lambda: q9(t, "e p")),
         ('22 "13" "31" "23" "29" "30" "18" "17"', lambda: q22(t, ["13", "31", "23", "29", "30", "18", "17"])),
     ]
     got = reference(data, tmp_path / "ref", [r for r, _ in cases])
     for (req, want), g in zip(cases, got):
         assert g[1:] == want(), req
     # every query family has a non-empty, non-zero answer among the cases
-    for q in ("5 ", "7 ", "8 ", "11 ", "15 ", "17 ", "22 "):
+    for q in ("5 ", "7 ", "8 ", "9 ", "11 ", "15 ", "17 ", "19 ", "22 "):
         assert any(len(g) > 1 and any(x != "0.00" for row in g[1:] for x in (row[1:] if len(row) > 1 else row))
                    for (req, _), g in zip(cases, got) if req.startswith(q)), q
