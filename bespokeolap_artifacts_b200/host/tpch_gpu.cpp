@@ -957,6 +957,60 @@ std::vector<Q19ResultRow> run_q19(const Database& db, const std::string quantity
   return {Q19ResultRow{revenue}};
 }
 
+std::vector<Q21ResultRow> run_q21(const Database& db, const std::string& nation) {
+  // query_q21.cpp:148-190: a known nation (the first row of a name), an "F"
+  // status code and a supplier key >= 0, else no rows.
+  if (nation == "<<NULL>>") return {};
+  int32_t target_nation = 0;
+  bool found = false;
+  for (size_t i = 0; i < db.nation_row_name.size() && !found; ++i)
+    if (db.nation_row_name[i] == nation) {
+      target_nation = db.nation_key[i];
+      found = true;
+    }
+  if (!found) return {};
+  int32_t final_code = -1;
+  for (size_t c = 0; c < db.orderstatus.values.size() && final_code < 0; ++c)
+    if (db.orderstatus.values[c] == "F") final_code = static_cast<int32_t>(c);
+  if (final_code < 0) return {};
+  int32_t max_suppkey = -1;
+  for (int32_t k : db.s_suppkey) max_suppkey = std::max(max_suppkey, k);
+  if (max_suppkey < 0) return {};
+  // suppkey -> last supplier row; a target when any of its rows is of the nation
+  std::vector<int32_t> row_of(static_cast<size_t>(max_suppkey) + 1, -1);
+  std::vector<uint8_t> target(row_of.size(), 0);
+  for (size_t r = 0; r < db.s_suppkey.size(); ++r) {
+    const int32_t k = db.s_suppkey[r];
+    if (k < 0) continue;
+    row_of[static_cast<size_t>(k)] = static_cast<int32_t>(r);
+    if (db.s_nationkey[r] == target_nation) target[static_cast<size_t>(k)] = 1;
+  }
+  bo_tpch_q21_tables t{};
+  t.l_orderkey = col<int32_t>(db.l_orderkey);
+  t.l_suppkey = col<int32_t>(db.l_suppkey);
+  t.l_commit_receipt = col<uint32_t>(db.l_commit_receipt);
+  t.n_lineitem = db.n_lineitem;
+  t.o_orderkey = col<int32_t>(db.o_orderkey);
+  t.o_orderstatus = col<uint16_t>(db.o_orderstatus);
+  t.o_li_begin = col<uint32_t>(db.o_li_begin);
+  t.o_li_end = col<uint32_t>(db.o_li_end);
+  t.n_orders = db.n_orders;
+  t.lineitem_orderkey_sorted = db.lineitem_orderkey_sorted ? 1 : 0;
+  std::vector<int64_t> waits(row_of.size());
+  check(db.ctx, bo_tpch_q21(db.ctx, &t, final_code, target.data(), max_suppkey, waits.data()), "q21");
+  std::vector<Q21ResultRow> rows;
+  for (size_t k = 0; k < waits.size(); ++k) {
+    if (waits[k] == 0 || row_of[k] < 0) continue;
+    rows.push_back(Q21ResultRow{db.s_name.view(static_cast<size_t>(row_of[k])), waits[k]});
+  }
+  // ORDER BY numwait DESC, s_name (query_q21.cpp:374-385)
+  std::sort(rows.begin(), rows.end(), [](const Q21ResultRow& a, const Q21ResultRow& b) {
+    if (a.numwait != b.numwait) return a.numwait > b.numwait;
+    return a.s_name < b.s_name;
+  });
+  return rows;
+}
+
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container) {
   // query_q17.cpp:125-155: NULL arguments, no parts, or an unknown brand or
   // container give a zero row.
@@ -1249,6 +1303,12 @@ void write_q19_csv(const std::string& filename, const std::vector<Q19ResultRow>&
   for (const auto& r : rows) out << static_cast<double>(r.revenue_raw) / (kPriceScale * kDiscountScale) << "\n";
 }
 
+void write_q21_csv(const std::string& filename, const std::vector<Q21ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q21.cpp:394-400
+  out << "s_name,numwait\n";
+  for (const auto& r : rows) out << escape_csv(std::string(r.s_name)) << ',' << r.numwait << "\n";
+}
+
 void write_q8_csv(const std::string& filename, const std::vector<Q8ResultRow>& rows) {
   std::ofstream out(filename);  // query_q8.cpp:382-389
   out << "o_year,mkt_share\n";
@@ -1352,7 +1412,7 @@ Database::~Database() {
                           &c_phone_prefix, &c_phone_pair, &o_has_order, &ps_partkey, &ps_suppkey, &ps_value,
                           &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch, &p_name,
                           &p_name_offsets, &ps_supplycost, &ps_part_begin, &o_year_by_key, &l_shipinstruct,
-                          &p_size, &p_row_by_key};
+                          &p_size, &p_row_by_key, &o_orderstatus};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
   if (result_host) bo_host_free_pinned(ctx, result_host);
@@ -1431,8 +1491,8 @@ struct LineitemHost {
 
 struct OrdersHost {
   std::vector<int32_t> okey, ckey, prio, total, map;
-  std::vector<uint16_t> priority;
-  Dictionary priority_dict;
+  std::vector<uint16_t> priority, status;
+  Dictionary priority_dict, status_dict;
   std::vector<int16_t> odate;
   std::vector<uint8_t> comment_bytes;
   std::vector<uint32_t> comment_offsets;
@@ -1584,6 +1644,7 @@ OrdersHost derive_orders(const ParquetTables::ArrowTable& O, int32_t base_days) 
   const auto prio = int_values(column(O, "o_shippriority"));
   const auto total = scaled_values(column(O, "o_totalprice"), kPriceScale);
   const auto priority = dictionary_codes(column(O, "o_orderpriority"), h.priority_dict);
+  const auto status = dictionary_codes(column(O, "o_orderstatus"), h.status_dict);
   std::vector<uint32_t> order(okey.size());
   std::iota(order.begin(), order.end(), 0u);
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return odate[a] < odate[b]; });
@@ -1593,6 +1654,7 @@ OrdersHost derive_orders(const ParquetTables::ArrowTable& O, int32_t base_days) 
   h.odate = permute(odate, order);
   h.total = permute(total, order);
   h.priority = permute(priority, order);
+  h.status = permute(status, order);
   int32_t max_key = -1;
   for (int32_t k : h.okey) max_key = std::max(max_key, k);
   h.map.assign(max_key >= 0 ? static_cast<size_t>(max_key) + 1 : 0, -1);
@@ -1751,6 +1813,8 @@ Database* build(ParquetTables* tables) {
       db->o_totalprice = upload(ctx, h.total);
       db->orderpriority = std::move(h.priority_dict);
       db->o_orderpriority = upload(ctx, h.priority);
+      db->orderstatus = std::move(h.status_dict);
+      db->o_orderstatus = upload(ctx, h.status);
       db->orderkey_to_row = upload(ctx, h.map);
       db->dense_orderkeys = !h.okey.empty() && h.okey.front() == 1 && h.okey.back() == static_cast<int32_t>(h.okey.size());
       db->o_comment = upload(ctx, h.comment_bytes);
@@ -2036,6 +2100,12 @@ void query(Database* db) {
       const auto rows = run_q9(*db, color);
       const auto end = std::chrono::steady_clock::now();
       write_q9_csv(file, rows);
+      report(end);
+    } else if (r.id == "21") {
+      const std::string nation = arg("NATION");
+      const auto rows = run_q21(*db, nation);
+      const auto end = std::chrono::steady_clock::now();
+      write_q21_csv(file, rows);
       report(end);
     } else if (r.id == "19") {
       std::string quantity[3], brand[3];

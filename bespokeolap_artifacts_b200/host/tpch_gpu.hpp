@@ -85,7 +85,8 @@ struct Database {
   int64_t n_orders = 0;
   bo_tpch::DeviceColumn o_orderkey, o_custkey, o_orderdate, o_shippriority, o_totalprice, orderkey_to_row,
       o_li_begin, o_li_end, o_comment, o_comment_offsets, o_orderpriority, o_cust_nation;
-  bo_tpch::Dictionary orderpriority;
+  bo_tpch::Dictionary orderpriority, orderstatus;
+  bo_tpch::DeviceColumn o_orderstatus;  // dictionary codes (Q21)
   int64_t n_orderkey_map = 0;
   bool dense_orderkeys = false;  // first orderkey 1, last n_orders (date order)
   // customer; custkey_to_row keeps the last row of each custkey >= 0
@@ -216,6 +217,11 @@ struct Q19ResultRow {
   int64_t revenue_raw = 0;
 };
 
+struct Q21ResultRow {
+  std::string_view s_name;
+  int64_t numwait = 0;
+};
+
 struct Q11ResultRow {
   int32_t ps_partkey = 0;
   int64_t value_raw = 0;
@@ -288,6 +294,7 @@ std::vector<Q22ResultRow> run_q22(const Database& db, const std::vector<std::str
 std::vector<Q11ResultRow> run_q11(const Database& db, const std::string& nation, const std::string& fraction);
 std::vector<Q15ResultRow> run_q15(const Database& db, const std::string& date);
 std::vector<Q9ResultRow> run_q9(const Database& db, const std::string& color);
+std::vector<Q21ResultRow> run_q21(const Database& db, const std::string& nation);
 std::vector<Q19ResultRow> run_q19(const Database& db, const std::string quantity[3], const std::string brand[3]);
 std::vector<Q17ResultRow> run_q17(const Database& db, const std::string& brand, const std::string& container);
 std::vector<Q14ResultRow> run_q14(const Database& db, const std::string& date);
@@ -308,6 +315,7 @@ void write_q22_csv(const std::string& filename, const std::vector<Q22ResultRow>&
 void write_q11_csv(const std::string& filename, const std::vector<Q11ResultRow>& rows);
 void write_q15_csv(const std::string& filename, const std::vector<Q15ResultRow>& rows);
 void write_q9_csv(const std::string& filename, const std::vector<Q9ResultRow>& rows);
+void write_q21_csv(const std::string& filename, const std::vector<Q21ResultRow>& rows);
 void write_q19_csv(const std::string& filename, const std::vector<Q19ResultRow>& rows);
 void write_q17_csv(const std::string& filename, const std::vector<Q17ResultRow>& rows);
 void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>& rows);

@@ -302,6 +302,41 @@ class TpchQ19Tables(C.Structure):
                 ("n_mask", C.c_int64)]
 
 
+class TpchQ21Tables(C.Structure):
+    """``bo_tpch_q21_tables``: lineitem orderkeys, suppkeys, packed commit / receipt dates; date-sorted orders'
+    keys, status codes and lineitem ranges; whether lineitems are sorted by orderkey."""
+    _fields_ = [("l_orderkey", C.c_void_p), ("l_suppkey", C.c_void_p), ("l_commit_receipt", C.c_void_p),
+                ("n_lineitem", C.c_int64), ("o_orderkey", C.c_void_p), ("o_orderstatus", C.c_void_p),
+                ("o_li_begin", C.c_void_p), ("o_li_end", C.c_void_p), ("n_orders", C.c_int64),
+                ("lineitem_orderkey_sorted", C.c_int32), ("pad", C.c_int32)]
+
+
+class CebCol(C.Structure):
+    """``bo_ceb_col``: int32 values (string columns: dictionary codes) and an optional null byte per row."""
+    _fields_ = [("values", C.c_void_p), ("is_null", C.c_void_p)]
+
+
+class CebQ1aTables(C.Structure):
+    """``bo_ceb_q1a_tables``: the columns CEB query 1a reads, in the reference's column layout."""
+    _fields_ = [("t_id", CebCol), ("t_kind_id", CebCol), ("t_year", CebCol), ("n_title", C.c_int64),
+                ("max_title_id", C.c_int32), ("pad0", C.c_int32),
+                ("mi_movie_id", CebCol), ("mi_info_type_id", CebCol), ("mi_info", CebCol), ("n_movie_info", C.c_int64),
+                ("ci_movie_id", CebCol), ("ci_person_id", CebCol), ("ci_role_id", CebCol), ("n_cast_info", C.c_int64),
+                ("kt_id", CebCol), ("kt_kind", CebCol), ("n_kind_type", C.c_int64),
+                ("rt_id", CebCol), ("rt_role", CebCol), ("n_role_type", C.c_int64),
+                ("nm_id", CebCol), ("nm_gender", CebCol), ("n_name", C.c_int64)]
+
+
+class CebQ1aParams(C.Structure):
+    """``bo_ceb_q1a_params``: years, the info-type filter and the per-code byte arrays (host memory)."""
+    _fields_ = [("year1", C.c_int32), ("year2", C.c_int32), ("info_type_filter", C.c_void_p),
+                ("info_type_size", C.c_int32), ("n_info_codes", C.c_int32), ("info_match", C.c_void_p),
+                ("kind_allowed", C.c_void_p), ("role_allowed", C.c_void_p), ("gender_allowed", C.c_void_p),
+                ("n_kind_codes", C.c_int32), ("n_role_codes", C.c_int32), ("n_gender_codes", C.c_int32),
+                ("kind_mask_size", C.c_int32), ("role_mask_size", C.c_int32), ("person_mask_size", C.c_int32),
+                ("pad", C.c_int32)]
+
+
 class TpchQ14Tables(C.Structure):
     """``bo_tpch_q14_tables``: lineitem shipdates, partkeys, discounted prices; the part promo flag per key."""
     _fields_ = [("l_shipdate", C.c_void_p), ("l_partkey", C.c_void_p), ("l_discounted_price", C.c_void_p),
@@ -437,6 +472,11 @@ _SIGNATURES = {
     "bo_tpch_q19": (C.c_int, [_P, C.POINTER(TpchQ19Tables), C.POINTER(C.c_int32), _P, C.c_int32,
                               C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.c_int32,
                               C.POINTER(C.c_int64)]),
+    "bo_tpch_q21": (C.c_int, [_P, C.POINTER(TpchQ21Tables), C.c_int32, _P, C.c_int32, _P]),
+    "bo_ceb_sort_rows": (C.c_int, [_P, _P, _P, C.c_int64, _P]),
+    "bo_ceb_gather_i32": (C.c_int, [_P, _P, _P, C.c_int64, _P]),
+    "bo_ceb_gather_u8": (C.c_int, [_P, _P, _P, C.c_int64, _P]),
+    "bo_ceb_q1a": (C.c_int, [_P, C.POINTER(CebQ1aTables), C.POINTER(CebQ1aParams), C.POINTER(C.c_int64)]),
     "bo_tpch_q9": (C.c_int, [_P, C.POINTER(TpchQ9Tables), C.c_char_p, C.c_int32, C.c_int32, C.c_int32, _P, _P]),
     "bo_tpch_order_years": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int64, C.c_int16, _P, C.c_int32, C.c_int32, _P]),
     "bo_tpch_q14": (C.c_int, [_P, C.POINTER(TpchQ14Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),

@@ -39,7 +39,7 @@ Key layouts (they select the reference's code paths):
 Regions REGION0..REGION4 (keys 0..4; nations' regionkey = nationkey % 5) and
 a later row repeating REGION1 with key 9.
 Part names are three words of COLORS.  Ship modes MODE_A..MODE_G, AIR and AIR REG, ship
-instructions from SHIPINSTRUCTS (one with trailing spaces), containers CONT_A..CONT_D and
+instructions from SHIPINSTRUCTS (one with trailing spaces), order statuses O, F and P, containers CONT_A..CONT_D and
 Q19's twelve (a stream of their own for the instructions); order priorities 1-URGENT and 2-HIGH (the two the
 reference's Q12 counts as high) and three others; part types with and
 without the PROMO prefix Q14 looks for.  Commit dates 30..90 days
@@ -60,6 +60,7 @@ WORDS = ["ironic", "quick", "pending", "bold", 'say "hi"', "a,b", "deposits", ""
 # the two ship modes, the ship instruction and the container lists run_q19
 # compares against (bespoke_tpch/query_q19.cpp:160-179, 203-208), among others
 SHIPMODES = ["MODE_A", "MODE_B", "MODE_C", "MODE_D", "MODE_E", "MODE_F", "MODE_G", "AIR", "AIR REG"]
+STATUSES = ["O", "F", "P"]  # run_q21 walks the orders of status "F" (query_q21.cpp:166-178)
 SHIPINSTRUCTS = ["DELIVER IN PERSON", "LEAVE AT DOOR", "HOLD AT DEPOT", "DELIVER IN PERSON  "]
 Q19_CONTAINERS = ["SM CASE", "SM BOX", "SM PACK", "SM PKG", "MED BAG", "MED BOX", "MED PKG", "MED PACK",
                   "LG CASE", "LG BOX", "LG PACK", "LG PKG"]
@@ -145,7 +146,8 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
         top = o_cust.max()
         o_cust = np.where((o_cust % 3 == 0) & (o_cust != top), o_cust - 1, o_cust).astype(np.int32)
     pq.write_table(pa.table({
-        "o_orderkey": orderkey, "o_custkey": o_cust, "o_orderstatus": ["O"] * n_orders,
+        "o_orderkey": orderkey, "o_custkey": o_cust,
+        "o_orderstatus": [STATUSES[i] for i in np.random.default_rng([seed, 17]).integers(0, 3, n_orders)],
         "o_totalprice": _dec(rng.integers(100000, 50000000, n_orders) / 100.0, decimal),
         "o_orderdate": pa.array(o_date, pa.date32()),
         "o_orderpriority": [PRIORITIES[i] for i in rng2.integers(0, len(PRIORITIES), n_orders)],

@@ -909,6 +909,105 @@ int bo_tpch_q19(bo_ctx* ctx, const bo_tpch_q19_tables* tables, const int32_t bra
                 const uint8_t* container_groups_host, int32_t n_containers, const int32_t size_high[3],
                 const int32_t qty_low[3], int32_t mode1, int32_t mode2, int32_t instruct_code, int64_t* revenue_out);
 
+/* TPC-H Q21 over the storage-plan layout: run_q21 of
+ * bespoke_tpch/query_q21.cpp:145-392.  For every (date-sorted) order whose
+ * orderstatus code is final_code and whose lineitem range holds more than one
+ * row: its lineitems (in the unsorted layout only those with the order's key)
+ * with a suppkey in [0, max_suppkey] are walked; the order counts when they
+ * name more than one supplier and every late one (receipt > commit, both as
+ * unsigned 16-bit offsets) has the same supplier, and that supplier is a
+ * target (target_host, max_suppkey + 1 bytes): its wait count (waits_out,
+ * max_suppkey + 1 entries) grows by the order's late lineitems.  The walk
+ * stops at a second late supplier (:257-266). */
+typedef struct bo_tpch_q21_tables {
+  const int32_t* l_orderkey;
+  const int32_t* l_suppkey;
+  const uint32_t* l_commit_receipt;    /* receipt << 16 | commit */
+  int64_t n_lineitem;
+  const int32_t* o_orderkey;
+  const uint16_t* o_orderstatus;       /* dictionary codes */
+  const uint32_t* o_li_begin;
+  const uint32_t* o_li_end;
+  int64_t n_orders;
+  int32_t lineitem_orderkey_sorted;
+  int32_t pad;
+} bo_tpch_q21_tables;
+
+int bo_tpch_q21(bo_ctx* ctx, const bo_tpch_q21_tables* tables, int32_t final_code, const uint8_t* target_host,
+                int32_t max_suppkey, int64_t* waits_out);
+
+/* ==================================================================== CEB ==
+ * The reference's CEB engine keeps every column as values plus a null byte
+ * per row (ColumnData, bespoke_ceb/builder_impl.hpp:97-111): int32 values
+ * (0 where null) and, for strings, ids into a string pool.  The GPU form is
+ * the same layout per column: int32 values (string columns: codes of the
+ * column's dictionary) and an optional is_null byte array (NULL: the column
+ * has no nulls). */
+typedef struct bo_ceb_col {
+  const int32_t* values;
+  const uint8_t* is_null;
+} bo_ceb_col;
+
+/* CEB query 1a: run_q1a of bespoke_ceb/query_q1a.cpp:155-655.  Titles of an
+ * allowed kind with year2 <= production_year <= year1; per title movie the
+ * movie_info rows of an info type in ID1 with an info value in INFO1
+ * (count1), likewise ID2 / INFO2 (count2); the cast_info rows of the movies
+ * with both counts, an allowed role and an allowed person (cast count);
+ * *count_out = sum over the qualifying title rows of cast * count1 * count2.
+ * Rows with a null in a column the reference tests are skipped as it skips
+ * them.  Kind / role / person masks come from the dimension rows whose
+ * dictionary code is allowed (kind_allowed etc., one byte per code) and whose
+ * id lies in [0, *_mask_size); the info-type filter holds one byte per
+ * info-type id in [0, info_type_size) (bit 0: ID1, bit 1: ID2) and the info
+ * match one byte per movie_info.info code (bit 0: INFO1, bit 1: INFO2).
+ * Movie ids beyond the largest qualifying title id are dropped, as the
+ * reference drops them; max_title_id bounds every title id. */
+typedef struct bo_ceb_q1a_tables {
+  bo_ceb_col t_id, t_kind_id, t_year;
+  int64_t n_title;
+  int32_t max_title_id;                /* largest title id (< 0: none) */
+  int32_t pad0;
+  bo_ceb_col mi_movie_id, mi_info_type_id, mi_info;
+  int64_t n_movie_info;
+  bo_ceb_col ci_movie_id, ci_person_id, ci_role_id;
+  int64_t n_cast_info;
+  bo_ceb_col kt_id, kt_kind;
+  int64_t n_kind_type;
+  bo_ceb_col rt_id, rt_role;
+  int64_t n_role_type;
+  bo_ceb_col nm_id, nm_gender;
+  int64_t n_name;
+} bo_ceb_q1a_tables;
+
+typedef struct bo_ceb_q1a_params {
+  int32_t year1, year2;
+  const uint8_t* info_type_filter;     /* host */
+  int32_t info_type_size;
+  int32_t n_info_codes;
+  const uint8_t* info_match;           /* host */
+  const uint8_t* kind_allowed;         /* host, per kind code */
+  const uint8_t* role_allowed;         /* host, per role code */
+  const uint8_t* gender_allowed;       /* host, per gender code */
+  int32_t n_kind_codes, n_role_codes, n_gender_codes;
+  int32_t kind_mask_size, role_mask_size, person_mask_size;
+  int32_t pad;
+} bo_ceb_q1a_params;
+
+int bo_ceb_q1a(bo_ctx* ctx, const bo_ceb_q1a_tables* tables, const bo_ceb_q1a_params* params, int64_t* count_out);
+
+/* The CEB builder's fact-table order (bespoke_ceb/builder_impl.cpp:255-360,
+ * 432-452): rows sorted by a primary int32 column and, optionally, a
+ * secondary one (movie_info by (movie_id, info_type_id), cast_info by
+ * (movie_id, role_id), movie_companies by movie_id, ...), comparing the
+ * stored values (0 where null).  perm_device (n entries) receives the source
+ * row of every output row; ties keep their input order (the reference's
+ * std::sort leaves their order unspecified).  bo_ceb_gather_i32 / _u8 then
+ * reorder a column: dst[i] = src[perm[i]]. */
+int bo_ceb_sort_rows(bo_ctx* ctx, const int32_t* primary, const int32_t* secondary, int64_t n,
+                     uint32_t* perm_device);
+int bo_ceb_gather_i32(bo_ctx* ctx, const int32_t* src, const uint32_t* perm, int64_t n, int32_t* dst);
+int bo_ceb_gather_u8(bo_ctx* ctx, const uint8_t* src, const uint32_t* perm, int64_t n, uint8_t* dst);
+
 /* TPC-H Q12 over the storage-plan layout: run_q12 of
  * bespoke_tpch/query_q12.cpp:162-360.  Lineitems whose shipmode code is
  * mode_code1 or mode_code2 (-1: none), with shipdate < commitdate <

@@ -8,6 +8,9 @@
   pyarrow.  Built only where the reference sources are present (the development
   container); the outputs are plain files that travel with the repository
   snapshot, so machines without the sources use the prebuilt copies.
+* ``oracle/_ref/ref_tpch_driver`` and ``ref_ceb_driver``: the reference's own
+  load / build / query of its TPC-H and CEB engines behind a stand-in driver
+  main (``ref_driver_main.cpp``).
 
 Usage: ``python oracle/build_oracle.py [--force]``.  The reference tree is
 read from ``$BO_REFERENCE_DIR`` (default ``/root/reference``).
@@ -76,6 +79,19 @@ def build_reference(force: bool = False) -> list[Path]:
             "g++", "-std=c++20", "-O2", f"-I{tpch}", f"-I{HERE / 'ref_stubs'}", f"-I{inc}", *map(str, dsrcs),
             f"-L{libdir}", "-l:libarrow.so.2400", "-l:libparquet.so.2400", f"-Wl,-rpath,{libdir}", "-lpthread",
             "-o", str(drv)]))
+    # The reference's CEB engine (its generic column builder and the IMDB
+    # queries) behind the same stand-in driver main.
+    ceb = REF_DIR / "bespoke_ceb"
+    if (ceb / "query_impl.cpp").exists():
+        cdrv = OUT_REF / "ref_ceb_driver"
+        outs.append(cdrv)
+        csrcs = [HERE / "ref_driver_main.cpp", ceb / "query_impl.cpp", ceb / "builder_impl.cpp", ceb / "loader_impl.cpp"]
+        cdeps = csrcs + list(ceb.glob("*.hpp")) + list(ceb.glob("query_q*.cpp")) + list((HERE / "ref_stubs").glob("*.hpp"))
+        if force or _stale(cdrv, cdeps):
+            jobs.append(subprocess.Popen([
+                "g++", "-std=c++20", "-O2", f"-I{ceb}", f"-I{HERE / 'ref_stubs'}", f"-I{inc}", *map(str, csrcs),
+                f"-L{libdir}", "-l:libarrow.so.2400", "-l:libparquet.so.2400", f"-Wl,-rpath,{libdir}", "-lpthread",
+                "-o", str(cdrv)]))
     for j in jobs:
         if j.wait() != 0:
             raise RuntimeError("building the reference harness failed")

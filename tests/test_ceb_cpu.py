@@ -1,0 +1,62 @@
+"""CEB query 1a: the plain-Python restatement (tests/ceb_restate.py) against
+the reference itself -- its CEB load / build / query compiled unchanged into
+oracle/_ref/ref_ceb_driver -- on seeded IMDB-shaped Parquet files
+(bespokeolap_artifacts_b200.ceb_data), with and without nulls.  CPU only."""
+import csv
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from bespokeolap_artifacts_b200.ceb_data import write_ceb
+from ceb_restate import q1a
+
+ROOT = Path(__file__).resolve().parent.parent
+REF_CEB = ROOT / "oracle" / "_ref" / "ref_ceb_driver"
+
+# (ID1, ID2, INFO1, INFO2, KIND, ROLE, GENDER, YEAR1, YEAR2)
+Q1A_CASES = [
+    (["1", "2", "3", "5"], ["7", "8", "9"], ["V000", "V001", "V005"], ["V002", "V003"],
+     ["KIND_A", "KIND_B", "KIND_C"], ["ROLE_A", "ROLE_B", "ROLE_D"], ["GENDER_F", "GENDER_M"], "2015", "1950"),
+    (["1"], ["2"], ["V000"], ["V000"], ["KIND_A"], ["ROLE_A"], ["GENDER_F"], "2020", "1880"),
+    (["1", "1"], ["1"], ["V000", "V001"], ["V001", "V000"], ["KIND_A", "KIND_G"], ["ROLE_L"], ["GENDER_M"],
+     "1990", "1990"),
+    (["114", "116", "NULL", "2x"], ["2", "-1"], ["V000", "NOSUCH"], ["V004", "<<NULL>>"], ["KIND_D", "NOSUCH"],
+     ["ROLE_C", "ROLE_E"], ["GENDER_F"], "2020", "1880"),
+    (["3"], ["4"], ["V010"], ["V011"], ["NOSUCH"], ["ROLE_A"], ["GENDER_F"], "2020", "1880"),
+    (["1", "2"], ["3", "4"], ["V000", "V001"], ["V002", "V003"], ["KIND_A", "KIND_B"], ["ROLE_A"], ["GENDER_M"],
+     "1900", "2000"),
+]
+
+
+def lit(vals):
+    return "(" + ", ".join("'" + v.replace("'", "''") + "'" for v in vals) + ")"
+
+
+def request(case) -> str:
+    id1, id2, i1, i2, k, r, g, y1, y2 = case
+    return f'1a {lit(id1)} {lit(id2)} {lit(i1)} {lit(i2)} {lit(k)} {lit(r)} {lit(g)} "{y1}" "{y2}"'
+
+
+def reference(data: Path, workdir: Path, requests: list[str]) -> list[list[list[str]]]:
+    workdir.mkdir(parents=True, exist_ok=True)
+    p = subprocess.run([str(REF_CEB), str(data) + "/"], input="\n".join(requests) + "\n\n", text=True,
+                       capture_output=True, cwd=workdir, timeout=300)
+    assert p.returncode == 0, p.stderr
+    return [list(csv.reader(open(workdir / f"result{i + 1}.csv"))) for i in range(len(requests))]
+
+
+@pytest.mark.parametrize("nulls,seed", [(False, 1), (True, 2)])
+def test_q1a_restatement_matches_reference(tmp_path, nulls, seed):
+    if not REF_CEB.exists():
+        pytest.skip("reference CEB driver not built")
+    data = write_ceb(tmp_path / "d", n_title=4000, n_name=8000, n_cast=40_000, n_movie_info=30_000, seed=seed,
+                     nulls=nulls)
+    got = reference(data, tmp_path / "ref", [request(c) for c in Q1A_CASES])
+    nonzero = 0
+    for case, g in zip(Q1A_CASES, got):
+        assert g[0] == ["count_star()"]
+        want = q1a(data, *case)
+        assert int(g[1][0]) == want, case
+        nonzero += want > 0
+    assert nonzero >= 3

@@ -1,0 +1,71 @@
+"""CEB query 1a on the GPU (bo_ceb_q1a through the C ABI) against the
+reference's own CEB engine (compiled unchanged into
+oracle/_ref/ref_ceb_driver) on the same seeded IMDB-shaped Parquet files,
+with and without nulls, and at a larger size against the restatement: the
+counts must be equal."""
+from pathlib import Path
+
+import pytest
+
+from bespokeolap_artifacts_b200 import ceb
+from bespokeolap_artifacts_b200.ceb_data import write_ceb
+from ceb_restate import q1a as q1a_restated
+from test_ceb_cpu import Q1A_CASES, REF_CEB, reference, request
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("nulls,seed", [(False, 1), (True, 2), (True, 3)])
+def test_q1a_gpu_matches_reference(engine, torch_cuda, tmp_path, nulls, seed):
+    if not REF_CEB.exists():
+        pytest.skip("reference CEB driver not built")
+    data = write_ceb(tmp_path / "d", n_title=4000, n_name=8000, n_cast=40_000, n_movie_info=30_000, seed=seed,
+                     nulls=nulls)
+    tables = ceb.load_tables(data)
+    got = reference(data, tmp_path / "ref", [request(c) for c in Q1A_CASES])
+    for case, g in zip(Q1A_CASES, got):
+        assert ceb.q1a(engine, tables, *case) == int(g[1][0]), case
+
+
+def test_q1a_gpu_larger_tables(engine, torch_cuda, tmp_path):
+    data = write_ceb(tmp_path / "d", n_title=200_000, n_name=400_000, n_cast=3_000_000, n_movie_info=1_500_000,
+                     seed=5, nulls=True)
+    tables = ceb.load_tables(data)
+    for case in Q1A_CASES[:3]:
+        assert ceb.q1a(engine, tables, *case) == q1a_restated(data, *case), case
+
+
+def test_q1a_gpu_empty_title(engine, torch_cuda, tmp_path):
+    data = write_ceb(tmp_path / "d", n_title=100, n_name=100, n_cast=1000, n_movie_info=1000, seed=6)
+    tables = ceb.load_tables(data)
+    case = list(Q1A_CASES[0])
+    case[7], case[8] = "1000", "3000"  # no production year in range: no title row qualifies
+    assert ceb.q1a(engine, tables, *case) == 0
+
+
+def test_builder_order_on_gpu(engine, torch_cuda, tmp_path):
+    """cast_info by (movie_id, role_id) and movie_info by (movie_id,
+    info_type_id), as the reference builder orders them: the device columns
+    come out in numpy's stable lexicographic order of the stored values (0
+    where null), every column moved with its row, and q1a's count is
+    unchanged."""
+    import numpy as np
+    import pyarrow.parquet as pq
+
+    data = write_ceb(tmp_path / "d", n_title=3000, n_name=6000, n_cast=500_000, n_movie_info=200_000, seed=7,
+                     nulls=True)
+    tables = ceb.load_tables(data)
+    before = ceb.q1a(engine, tables, *Q1A_CASES[0])
+    ceb.builder_order(engine, tables)
+    for table, (p, s) in (("cast_info", ("movie_id", "role_id")), ("movie_info", ("movie_id", "info_type_id"))):
+        raw = pq.read_table(data / f"{table}.parquet")
+        cols = {c: np.nan_to_num(raw[c].to_numpy(zero_copy_only=False)).astype(np.int64) for c in raw.column_names
+                if c in tables.tables[table]}
+        order = np.lexsort((cols[s], cols[p]))  # stable: ties keep the input order
+        for c in cols:
+            dev = tables.col(table, c).values.cpu().numpy()
+            if tables.col(table, c).dictionary is None:
+                assert np.array_equal(dev, cols[c][order]), (table, c)
+        nl = tables.col(table, "movie_id").is_null
+        assert nl is None or not nl.any().item()
+    assert ceb.q1a(engine, tables, *Q1A_CASES[0]) == before

@@ -40,6 +40,7 @@ REQUESTS = [
     '19 "1" "10" "20" "BRAND_A" "BRAND_B" "BRAND_C"', '19 "5" "<<NULL>>" "30" "BRAND_D" "BRAND_D" "BRAND_D"',
     '19 "2.5" "2.5" "2.5" "BRAND_E" "BRAND_E" "BRAND_E"', '19 "<<NULL>>" "1" "1" "BRAND_A" "<<NULL>>" "<<NULL>>"',
     '19 "1" "1" "1" "NOSUCH" "BRAND_A" "BRAND_A"', '19 "45" "40" "45" "BRAND_B" "BRAND_C" "BRAND_B"',
+    '21 "NATION_00"', '21 "NATION_04"', '21 "NOSUCH"', '21 "<<NULL>>"',
 ]
 
 LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem, late_receipts)
@@ -105,7 +106,8 @@ Q5_REQUESTS = ['5 "REGION0" "1994-01-01"', '5 "REGION1" "1995-02-28"', '5 "REGIO
                '15 "1996-01-01" "1"', '15 "1995-11-30" "0"', '15 "1999-01-01" "2"', '15 "1993-05-17" "3"',
                '17 "BRAND_B" "CONT_C"', '17 "BRAND_E" "CONT_A"', '17 "NOSUCH" "CONT_A"', '17 "<<NULL>>" "CONT_A"',
                '17 "BRAND_A" "<<NULL>>"',
-               '9 "co"', '9 "slate"', '9 "e p"', '9 ""', '9 "nosuchcolor"', '9 "umber umber"']
+               '9 "co"', '9 "slate"', '9 "e p"', '9 ""', '9 "nosuchcolor"', '9 "umber umber"',
+               '21 "NATION_04"', '21 "NATION_10"', '21 "NATION_19"', '21 "NATION_07"']
 
 Q5_LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem): known nations, 25 suppliers
     (11, False, "sparse", "dense", False),
@@ -115,7 +117,7 @@ Q5_LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem): 
 
 @pytest.mark.parametrize("layout", Q5_LAYOUTS, ids=lambda l: "-".join(map(str, l)))
 def test_dropin_q5_matches_reference_driver(tmp_path, layout):
-    """Q5, Q7, Q8, Q9, Q11, Q15, Q17 and Q22 (with every other request) on data whose customer
+    """Q5, Q7, Q8, Q9, Q11, Q15, Q17, Q21 and Q22 (with every other request) on data whose customer
     nationkeys lie in the nation table's key range, whose suppliers cover every
     lineitem suppkey and whose parts cover every lineitem partkey: the
     reference's run_q5 indexes its per-nation arrays by customer nations

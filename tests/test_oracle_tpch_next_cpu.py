@@ -1,4 +1,4 @@
-"""Python restatements of Q4, Q5, Q7, Q8, Q9, Q11, Q12, Q14, Q15, Q17, Q19 and Q22 (the
+"""Python restatements of Q4, Q5, Q7, Q8, Q9, Q11, Q12, Q14, Q15, Q17, Q19, Q21 and Q22 (the
 semantics the GPU tests restate), pinned against the reference itself: its own load / build / query (compiled
 unchanged into oracle/_ref/ref_tpch_driver) answers the same requests on the
 same seeded Parquet files, on the CPU.  Q12 runs on data with receipts up to
@@ -401,7 +401,43 @@ def q19(t, quantity, brand):
     return [[f"{total / 10000:.2f}"]]
 
 
-def test_q5_q7_q8_q9_q17_q19_q22_restatements_match_the_reference(known, tmp_path):
+def q21(t, nation):
+    """run_q21 (bespoke_tpch/query_q21.cpp:145-392) restated: orders of status
+    F with at least two lineitems whose valid suppkeys name at least two
+    suppliers and whose late lineitems (receipt > commit) all have one
+    supplier of the nation: that supplier waits once per late lineitem;
+    ordered by count desc, name."""
+    N, S, O, L = t["nation"], t["supplier"], t["orders"], t["lineitem"]
+    key = first_wins(N["n_name"].to_pylist(), N["n_nationkey"].to_pylist()).get(nation)
+    if key is None or "F" not in O["o_orderstatus"].to_pylist():
+        return []
+    sk_all = S["s_suppkey"].to_pylist()
+    max_sk = max(sk_all) if sk_all else -1
+    target = {k for k, n in zip(sk_all, S["s_nationkey"].to_pylist()) if n == key}
+    name = last_wins(sk_all, S["s_name"].to_pylist())
+    final = {k for k, st in zip(O["o_orderkey"].to_pylist(), O["o_orderstatus"].to_pylist()) if st == "F"}
+    rows = {}
+    late = days(L["l_receiptdate"]) > days(L["l_commitdate"])
+    for ok, sk, lt in zip(L["l_orderkey"].to_pylist(), L["l_suppkey"].to_pylist(), late.tolist()):
+        if ok in final:
+            rows.setdefault(ok, []).append((sk, lt))
+    waits = {}
+    for ok, lines in rows.items():
+        if len(lines) <= 1:
+            continue
+        valid = [(sk, lt) for sk, lt in lines if 0 <= sk <= max_sk]
+        late_s = {sk for sk, lt in valid if lt}
+        if len({sk for sk, _ in valid}) < 2 or len(late_s) != 1:
+            continue
+        s_ = next(iter(late_s))
+        if s_ in target:
+            waits[s_] = waits.get(s_, 0) + sum(1 for sk, lt in valid if lt)
+    esc = lambda x: '"' + x.replace('"', '\\"') + '"'  # noqa: E731
+    out = sorted(((name[k], v) for k, v in waits.items() if k in name), key=lambda x: (-x[1], x[0]))
+    return list(csv.reader([f"{esc(n)},{v}" for n, v in out]))
+
+
+def test_q5_q7_q8_q9_q17_q19_q21_q22_restatements_match_the_reference(known, tmp_path):
     data, t = known
     cases = [
         ('5 "REGION0" "1994-01-01"', lambda: q5(t, "REGION0", "1994-01-01")),
@@ -424,6 +460,9 @@ def test_q5_q7_q8_q9_q17_q19_q22_restatements_match_the_reference(known, tmp_pat
          lambda: q19(t, ["5", "<<NULL>>", "30"], ["BRAND_D", "BRAND_D", "BRAND_D"])),
         ('19 "2.5" "2.5" "2.5" "BRAND_E" "BRAND_E" "BRAND_E"',
          lambda: q19(t, ["2.5", "2.5", "2.5"], ["BRAND_E", "BRAND_E", "BRAND_E"])),
+        ('21 "NATION_04"', lambda: q21(t, "NATION_04")),
+        ('21 "NATION_10"', lambda: q21(t, "NATION_10")),
+        ('21 "NATION_19"', lambda: q21(t, "NATION_19")),
         ('9 "co"', lambda: q9(t, "co")),
         ('9 "slate"', lambda: q9(t, "slate")),
         ('9 "e p"', lambda: q9(t, "e p")),
@@ -433,6 +472,6 @@ def test_q5_q7_q8_q9_q17_q19_q22_restatements_match_the_reference(known, tmp_pat
     for (req, want), g in zip(cases, got):
         assert g[1:] == want(), req
     # every query family has a non-empty, non-zero answer among the cases
-    for q in ("5 ", "7 ", "8 ", "9 ", "11 ", "15 ", "17 ", "19 ", "22 "):
+    for q in ("5 ", "7 ", "8 ", "9 ", "11 ", "15 ", "17 ", "19 ", "21 ", "22 "):
         assert any(len(g) > 1 and any(x != "0.00" for row in g[1:] for x in (row[1:] if len(row) > 1 else row))
                    for (req, _), g in zip(cases, got) if req.startswith(q)), q
