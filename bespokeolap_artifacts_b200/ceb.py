@@ -41,6 +41,8 @@ class Column:
     dictionary: list | None = None   # string columns: code -> value
     max_value: int = -1         # largest non-null value (int columns), -1 without one
     rows: int = 0
+    dict_bytes: object = None   # string columns: the dictionary's bytes and
+    dict_offsets: object = None  # n + 1 uint32 offsets, on the device
 
     def c(self) -> N.CebCol:
         return N.CebCol(N.ptr(self.values), N.ptr(self.is_null) if self.is_null is not None else None)
@@ -53,6 +55,7 @@ class Column:
 @dataclass
 class CebTables:
     tables: dict = field(default_factory=dict)   # table -> {"rows": n, column -> Column}
+    pool: set = field(default_factory=set)       # every string of the database (the reference's pool)
 
     def col(self, table: str, name: str) -> Column:
         return self.tables[table][name]
@@ -77,17 +80,23 @@ def _column(arr, torch) -> Column:
         values = np.asarray(idx, dtype=np.int32)
         dictionary = enc.dictionary.to_pylist()
         mx = -1
+        raw = [v.encode() for v in dictionary]
+        offs = np.zeros(len(raw) + 1, np.uint32)
+        offs[1:] = np.cumsum([len(b) for b in raw], dtype=np.int64).astype(np.uint32) if raw else []
+        blob = np.frombuffer(b"".join(raw) or b"\0", dtype=np.uint8)
+        dict_dev = (torch.from_numpy(blob.copy()).cuda(), torch.from_numpy(offs.view(np.int32).copy()).cuda())
     else:
         v = arr.to_numpy(zero_copy_only=False)
         if v.dtype.kind == "f":
             v = np.where(np.isnan(v), 0, v)
         values = np.asarray(v, dtype=np.int64).astype(np.int32)
         dictionary = None
+        dict_dev = (None, None)
         valid = values[null == 0] if null is not None else values
         mx = int(valid.max()) if len(valid) else -1
     dev = torch.from_numpy(np.ascontiguousarray(values)).cuda()
     ndev = torch.from_numpy(null).cuda() if null is not None else None
-    return Column(dev, ndev, dictionary, mx, n)
+    return Column(dev, ndev, dictionary, mx, n, dict_dev[0], dict_dev[1])
 
 
 Q1A_COLUMNS = {
@@ -101,12 +110,38 @@ Q1A_COLUMNS = {
 }
 
 
+Q10A_COLUMNS = {
+    "title": ("id", "kind_id", "production_year"),
+    "movie_info": ("movie_id", "info_type_id", "info"),
+    "cast_info": ("movie_id", "person_id", "role_id"),
+    "kind_type": ("id", "kind"),
+    "role_type": ("id", "role"),
+    "name": ("id", "name"),
+    "info_type": ("id",),
+}
+
+
+def string_pool(path: Path) -> set:
+    """Every string value of every table (the reference interns all of them
+    into one pool, bespoke_ceb/builder_impl.cpp:408-422)."""
+    import pyarrow as pa
+    import pyarrow.parquet as pq
+
+    pool = set()
+    for f in sorted(Path(path).glob("*.parquet")):
+        t = pq.read_table(f)
+        for c in t.column_names:
+            if pa.types.is_string(t[c].type) or pa.types.is_large_string(t[c].type):
+                pool.update(v for v in t[c].unique().to_pylist() if v is not None)
+    return pool
+
+
 def load_tables(path: Path, columns: dict = Q1A_COLUMNS) -> CebTables:
     """Reads the named columns of the CEB Parquet files onto the device."""
     import pyarrow.parquet as pq
     import torch
 
-    out = CebTables()
+    out = CebTables(pool=string_pool(path))
     for table, cols in columns.items():
         t = pq.read_table(Path(path) / f"{table}.parquet", columns=list(cols))
         d = {"rows": t.num_rows}
@@ -228,3 +263,131 @@ def builder_order(engine, t: CebTables) -> None:
     for table, (p, s) in BUILDER_ORDER.items():
         if table in t.tables and p in t.tables[table] and (s is None or s in t.tables[table]):
             sort_table(engine, t, table, p, s)
+
+
+# ------------------------------------------------------------------ 10a ----
+def string_filter(pool: set, values) -> set:
+    """build_string_filter_for_column (bespoke_ceb/query_q10a.cpp:248-282):
+    IN-list values were split at commas by the request parser, so runs of
+    consecutive values are re-joined with ", " or "," and the longest run
+    that names a string of the database is taken."""
+    out, i = set(), 0
+    while i < len(values):
+        if values[i] in NULL_WORDS:
+            i += 1
+            continue
+        sp = nsp = values[i]
+        found, found_idx = None, i
+        for j in range(i, len(values)):
+            if j != i:
+                if values[j] in NULL_WORDS:
+                    break
+                sp += ", " + values[j]
+                nsp += "," + values[j]
+            if sp in pool:
+                found, found_idx = sp, j
+            if nsp in pool:
+                found, found_idx = nsp, j
+        if found is not None:
+            out.add(found)
+            i = found_idx + 1
+        else:
+            i += 1
+    return out
+
+
+def ascii_lower(s: str) -> str:
+    return "".join(chr(ord(c) + 32) if "A" <= c <= "Z" else c for c in s)
+
+
+def ilike_pattern(raw: str) -> tuple[int, str]:
+    """build_ilike_pattern (bespoke_ceb/query_q10a.cpp:172-214): the pattern
+    kind (0 all, 1 exact, 2 prefix, 3 suffix, 4 contains, 5 general) and its
+    lower-cased token or pattern."""
+    p = raw[1:-1] if len(raw) >= 2 and raw[0] == "'" and raw[-1] == "'" else raw
+    p = ascii_lower(p)
+    if p == "%":
+        return 0, ""
+    if "_" not in p:
+        first = p.find("%")
+        if first < 0:
+            return 1, p
+        last = p.rfind("%")
+        if first == 0 and last == len(p) - 1 and p.find("%", 1) == last:
+            return 4, p[1:-1] if len(p) > 2 else ""
+        if first == 0 and p.find("%", 1) < 0:
+            return 3, p[1:]
+        if last == len(p) - 1 and p.find("%") == last:
+            return 2, p[:-1]
+    return 5, p
+
+
+def q10a(engine, t: CebTables, ids, infos, name, kinds, roles, max_rows: int = 1 << 16) -> list:
+    """CEB query 10a (run_q10a, bespoke_ceb/query_q10a.cpp:334-1130) on the
+    GPU: rows (name, info, has_year, min_year, max_year), in no particular
+    order (the reference's are in its aggregation order)."""
+    type_ids = {i for i in (stoi(v) for v in ids if v not in NULL_WORDS) if i is not None}
+    if not type_ids:
+        return []
+    kf, rf, inf = string_filter(t.pool, kinds), string_filter(t.pool, roles), string_filter(t.pool, infos)
+    if not kf or not rf or not inf:
+        return []
+    size_it = t.rows("info_type") + 1
+    tmask = np.zeros(size_it, np.uint8)
+    for i in type_ids:
+        if 0 <= i < size_it:
+            tmask[i] = 1
+    if not tmask.any():
+        return []
+    info = t.col("movie_info", "info")
+    dense_vals = sorted(inf)
+    dense_of = {v: k for k, v in enumerate(dense_vals)}
+    info_dense = np.full(max(len(info.dictionary or []), 1), -1, np.int32)
+    for c, v in enumerate(info.dictionary or []):
+        if v in dense_of:
+            info_dense[c] = dense_of[v]
+    ka = _code_bytes(t.col("kind_type", "kind"), kf)
+    ra = _code_bytes(t.col("role_type", "role"), rf)
+    ptype, pat = ilike_pattern(name)
+    pat_b = pat.encode()
+    pat_buf = np.frombuffer(pat_b or b"\0", np.uint8).copy()
+    nm = t.col("name", "name")
+    tab = N.CebQ10aTables()
+    tab.t_id, tab.t_kind_id, tab.t_year = (t.col("title", c).c() for c in ("id", "kind_id", "production_year"))
+    tab.n_title = t.rows("title")
+    tab.mi_movie_id, tab.mi_info_type_id, tab.mi_info = (t.col("movie_info", c).c()
+                                                         for c in ("movie_id", "info_type_id", "info"))
+    tab.n_movie_info = t.rows("movie_info")
+    tab.ci_movie_id, tab.ci_person_id, tab.ci_role_id = (t.col("cast_info", c).c()
+                                                         for c in ("movie_id", "person_id", "role_id"))
+    tab.n_cast_info = t.rows("cast_info")
+    tab.kt_id, tab.kt_kind = t.col("kind_type", "id").c(), t.col("kind_type", "kind").c()
+    tab.n_kind_type = t.rows("kind_type")
+    tab.rt_id, tab.rt_role = t.col("role_type", "id").c(), t.col("role_type", "role").c()
+    tab.n_role_type = t.rows("role_type")
+    tab.nm_id, tab.nm_name = t.col("name", "id").c(), nm.c()
+    tab.n_name = t.rows("name")
+    tab.name_dict, tab.name_dict_offsets = N.ptr(nm.dict_bytes), N.ptr(nm.dict_offsets)
+    tab.n_name_codes = len(nm.dictionary or [])
+    p = N.CebQ10aParams()
+    p.info_type_mask, p.info_type_size = tmask.ctypes.data, size_it
+    p.info_dense, p.n_info_codes, p.n_info_dense = info_dense.ctypes.data, len(info.dictionary or []), len(dense_vals)
+    p.kind_allowed, p.n_kind_codes = ka.ctypes.data, len(t.col("kind_type", "kind").dictionary or [])
+    p.role_allowed, p.n_role_codes = ra.ctypes.data, len(t.col("role_type", "role").dictionary or [])
+    p.pattern_type, p.pattern, p.pattern_len = ptype, pat_buf.ctypes.data, len(pat_b)
+    while True:
+        rows = (N.CebQ10aRow * max(max_rows, 1))()
+        n, dense = C.c_int64(), C.c_int32()
+        rc = N.lib().bo_ceb_q10a(engine.ctx.handle, C.byref(tab), C.byref(p), rows, max_rows, C.byref(n),
+                                 C.byref(dense))
+        if rc == N.BO_ERR_OVERFLOW and n.value > max_rows:
+            max_rows = int(n.value)  # more groups than rows offered: run again with room for all
+            continue
+        engine.ctx.check(rc, "bo_ceb_q10a")
+        break
+    out = []
+    for r in rows[:n.value]:
+        out.append((nm.dictionary[r.name_code], dense_vals[r.info_dense], bool(r.has_year),
+                    r.min_year if r.has_year else None, r.max_year if r.has_year else None))
+    q10a.last_dense = bool(dense.value)
+    return out

@@ -10,7 +10,7 @@ vocabularies, names and titles are numbered strings.
 
   title       id (1..n_title, shuffled), kind_id (1..7), production_year
               (1880..2020), title; with nulls=True some kind_ids and years
-              are null and a few ids repeat.
+              are null and a few ids repeat (in rows of equal kind and year).
   kind_type   id 1..7, kind KIND_A..KIND_G.
   role_type   id 1..12, role ROLE_A..ROLE_L.
   info_type   id 1..n_info_type (113), info INFO_TYPE_<id>.
@@ -20,8 +20,8 @@ vocabularies, names and titles are numbered strings.
   cast_info   movie_id (bounded Zipf), person_id (bounded Zipf over the
               name ids), role_id (1..12); with nulls=True some null
               person_ids / role_ids.
-  name        id 1..n_name (shuffled), name NAME_<id>, gender GENDER_M /
-              GENDER_F / null.
+  name        id 1..n_name (shuffled), name NAME_<id> (some in mixed case,
+              some shared by two persons), gender GENDER_M / GENDER_F / null.
 """
 from __future__ import annotations
 
@@ -50,6 +50,14 @@ def _int(values: np.ndarray, null: np.ndarray | None = None) -> pa.Array:
     return pa.array(values.astype(np.int32), pa.int32(), mask=null)
 
 
+def person_name(k: int) -> str:
+    """NAME_<k>, every 7th in mixed case (Name_<k>), every 11th the name of
+    person k // 11 (persons sharing a name)."""
+    if k % 11 == 0:
+        k //= 11
+    return f"Name_{k:07d}" if k % 7 == 0 else f"NAME_{k:07d}"
+
+
 def info_value(i: int) -> str:
     return f"V{i:03d}"
 
@@ -67,7 +75,11 @@ def write_ceb(out: Path, n_title: int = 20_000, n_name: int = 50_000, n_cast: in
     if nulls:
         kind_null = rng.random(n_title) < 0.03
         year_null = rng.random(n_title) < 0.05
-        tid[-3:] = tid[:3]  # repeated ids: the last row of an id wins where the pipelines keep one
+        # repeated ids, rows equal in kind and year (which of two rows of an id
+        # the reference's unstable id sort puts last is unspecified)
+        tid[-3:] = tid[:3]
+        kind[-3:], year[-3:] = kind[:3], year[:3]
+        kind_null[-3:], year_null[-3:] = kind_null[:3], year_null[:3]
     pq.write_table(pa.table({"id": _int(tid), "kind_id": _int(kind, kind_null),
                              "production_year": _int(year, year_null),
                              "title": [f"TITLE_{k}" for k in tid]}), out / "title.parquet")
@@ -80,7 +92,7 @@ def write_ceb(out: Path, n_title: int = 20_000, n_name: int = 50_000, n_cast: in
     nid = rng.permutation(np.arange(1, n_name + 1)).astype(np.int32)
     g = rng.integers(0, 3, n_name)
     gender = pa.array([GENDERS[x] if x < 2 else None for x in g], pa.string())
-    pq.write_table(pa.table({"id": _int(nid), "name": [f"NAME_{k:07d}" for k in nid], "gender": gender}),
+    pq.write_table(pa.table({"id": _int(nid), "name": [person_name(k) for k in nid], "gender": gender}),
                    out / "name.parquet")
     # movie_info: movie ids Zipf over titles (a few beyond the largest id)
     mi_movie = _zipf(rng, n_movie_info, n_title, 0.6) + 1

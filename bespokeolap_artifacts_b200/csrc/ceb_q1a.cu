@@ -19,46 +19,17 @@
 //   ceb_sum_kernel        the factorised sum over the title list.
 #include <algorithm>
 
-#include "common.cuh"
+#include "ceb.cuh"
 #include "context.cuh"
 
 namespace bo {
 namespace {
-
-constexpr int kCebBlock = 256;
-
-__device__ __forceinline__ bool ceb_null(const bo_ceb_col& c, int64_t r) { return c.is_null && c.is_null[r]; }
 
 struct CebMeta {
   unsigned int n_list;
   int max_movie;
   unsigned long long total;
 };
-
-__global__ void __launch_bounds__(kCebBlock) ceb_dim_mask_kernel(bo_ceb_col id, bo_ceb_col code, int64_t n,
-                                                                 const uint8_t* __restrict__ allowed, int32_t n_codes,
-                                                                 int32_t mask_size, uint8_t* __restrict__ mask) {
-  const int64_t stride = (int64_t)gridDim.x * kCebBlock;
-  for (int64_t r = (int64_t)blockIdx.x * kCebBlock + threadIdx.x; r < n; r += stride) {
-    if (ceb_null(id, r) || ceb_null(code, r)) continue;  // query_q1a.cpp:104-106
-    const int32_t i = id.values[r], c = code.values[r];
-    if (i < 0 || i >= mask_size || c < 0 || c >= n_codes || !allowed[c]) continue;
-    mask[i] = 1;
-  }
-}
-
-// Appends v to list[] with one reservation per warp (the lanes whose `take` holds).
-__device__ __forceinline__ void warp_append(bool take, int32_t v, int32_t* __restrict__ list,
-                                            unsigned int* __restrict__ count) {
-  const unsigned int mask = __ballot_sync(0xffffffffu, take);
-  if (!mask) return;
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(mask) - 1;
-  unsigned int base = 0;
-  if (lane == leader) base = atomicAdd(count, (unsigned int)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (take) list[base + __popc(mask & ((1u << lane) - 1u))] = v;
-}
 
 __global__ void __launch_bounds__(kCebBlock) ceb_title_kernel(bo_ceb_q1a_tables t, int32_t year1, int32_t year2,
                                                               const uint8_t* __restrict__ kind_mask,
@@ -76,7 +47,7 @@ __global__ void __launch_bounds__(kCebBlock) ceb_title_kernel(bo_ceb_q1a_tables 
       const int32_t year = t.t_year.values[r], kind = t.t_kind_id.values[r];
       take = movie >= 0 && year <= year1 && year >= year2 && kind >= 0 && kind < kind_mask_size && kind_mask[kind];
     }
-    warp_append(take, movie, list, &meta->n_list);
+    warp_append<int32_t>(take, movie, list, &meta->n_list);
     if (take) best = max(best, movie);
   }
   for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
@@ -275,7 +246,7 @@ extern "C" int bo_ceb_q1a(bo_ctx* ctx, const bo_ceb_q1a_tables* t, const bo_ceb_
   for (const auto& d : dims) {
     if (d.n == 0 || d.size == 0) continue;
     ceb_dim_mask_kernel<<<ceb_grid(ctx, kd, d.n), kCebBlock, 0, ctx->stream>>>(d.id, d.code, d.n, d.allowed,
-                                                                             d.n_codes, d.size, d.mask);
+                                                                             d.n_codes, d.size, d.mask, nullptr);
     if ((rc = after_launch(ctx, "ceb_dim_mask_kernel"))) return rc;
   }
   const void* kt = reinterpret_cast<const void*>(&ceb_title_kernel);

@@ -14,6 +14,7 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "libbespoke_gpu.so"
 
 BO_OK = 0
+BO_ERR_OVERFLOW = -3
 STATUS_NAMES = {
     0: "BO_OK",
     -1: "BO_ERR_INVALID",
@@ -337,6 +338,31 @@ class CebQ1aParams(C.Structure):
                 ("pad", C.c_int32)]
 
 
+class CebQ10aTables(C.Structure):
+    """``bo_ceb_q10a_tables``: the columns CEB query 10a reads and the name dictionary on the device."""
+    _fields_ = [("t_id", CebCol), ("t_kind_id", CebCol), ("t_year", CebCol), ("n_title", C.c_int64),
+                ("mi_movie_id", CebCol), ("mi_info_type_id", CebCol), ("mi_info", CebCol), ("n_movie_info", C.c_int64),
+                ("ci_movie_id", CebCol), ("ci_person_id", CebCol), ("ci_role_id", CebCol), ("n_cast_info", C.c_int64),
+                ("kt_id", CebCol), ("kt_kind", CebCol), ("n_kind_type", C.c_int64),
+                ("rt_id", CebCol), ("rt_role", CebCol), ("n_role_type", C.c_int64),
+                ("nm_id", CebCol), ("nm_name", CebCol), ("n_name", C.c_int64),
+                ("name_dict", C.c_void_p), ("name_dict_offsets", C.c_void_p), ("n_name_codes", C.c_int64)]
+
+
+class CebQ10aParams(C.Structure):
+    """``bo_ceb_q10a_params``: the info-type mask, dense info indices per code, kind / role codes and the
+    ILIKE pattern (host memory)."""
+    _fields_ = [("info_type_mask", C.c_void_p), ("info_type_size", C.c_int32), ("n_info_codes", C.c_int32),
+                ("info_dense", C.c_void_p), ("n_info_dense", C.c_int32), ("n_kind_codes", C.c_int32),
+                ("kind_allowed", C.c_void_p), ("role_allowed", C.c_void_p), ("n_role_codes", C.c_int32),
+                ("pattern_type", C.c_int32), ("pattern", C.c_void_p), ("pattern_len", C.c_int32), ("pad", C.c_int32)]
+
+
+class CebQ10aRow(C.Structure):
+    _fields_ = [("name_code", C.c_int32), ("info_dense", C.c_int32), ("has_year", C.c_int32),
+                ("min_year", C.c_int32), ("max_year", C.c_int32)]
+
+
 class TpchQ14Tables(C.Structure):
     """``bo_tpch_q14_tables``: lineitem shipdates, partkeys, discounted prices; the part promo flag per key."""
     _fields_ = [("l_shipdate", C.c_void_p), ("l_partkey", C.c_void_p), ("l_discounted_price", C.c_void_p),
@@ -473,6 +499,8 @@ _SIGNATURES = {
                               C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.c_int32,
                               C.POINTER(C.c_int64)]),
     "bo_tpch_q21": (C.c_int, [_P, C.POINTER(TpchQ21Tables), C.c_int32, _P, C.c_int32, _P]),
+    "bo_ceb_q10a": (C.c_int, [_P, C.POINTER(CebQ10aTables), C.POINTER(CebQ10aParams), _P, C.c_int64,
+                              C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "bo_ceb_sort_rows": (C.c_int, [_P, _P, _P, C.c_int64, _P]),
     "bo_ceb_gather_i32": (C.c_int, [_P, _P, _P, C.c_int64, _P]),
     "bo_ceb_gather_u8": (C.c_int, [_P, _P, _P, C.c_int64, _P]),

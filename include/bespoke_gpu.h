@@ -995,6 +995,69 @@ typedef struct bo_ceb_q1a_params {
 
 int bo_ceb_q1a(bo_ctx* ctx, const bo_ceb_q1a_tables* tables, const bo_ceb_q1a_params* params, int64_t* count_out);
 
+/* CEB query 10a: run_q10a of bespoke_ceb/query_q10a.cpp:334-1130 -- per
+ * (person name, movie info value) the MIN and MAX production year over the
+ * joined rows: titles of an allowed kind (ids in [0, n_title + 1); the last
+ * row of an id gives its year, or no year when null); their movie_info rows
+ * with an info type allowed by info_type_mask (one byte per id in
+ * [0, info_type_size)) and an info code with a dense index in info_dense
+ * (-1: not in the IN list); their cast_info rows of an allowed role with a
+ * person id in [0, n_name + 1); the persons whose name (a code of the name
+ * dictionary, name_dict bytes with n_name_codes + 1 offsets on the device)
+ * matches the ILIKE pattern (pattern_type: 0 all, 1 exact, 2 prefix,
+ * 3 suffix, 4 contains, 5 general with '%' / '_'; the token or pattern
+ * lower-cased, host memory).  Groups are aggregated in a dense name-code x
+ * info matrix when it has at most BO_CEB_AGG_MAX_SLOTS slots, else in a hash
+ * table (the reference's switch, :843-856).  Rows (any order, as the
+ * reference's) go to rows_out (host, max_rows); *n_rows_out receives the
+ * group count; BO_ERR_OVERFLOW when it exceeds max_rows (nothing written).
+ * *dense_out (optional) tells which aggregation ran (1 = matrix). */
+#define BO_CEB_AGG_MAX_SLOTS 5000000
+typedef struct bo_ceb_q10a_tables {
+  bo_ceb_col t_id, t_kind_id, t_year;
+  int64_t n_title;
+  bo_ceb_col mi_movie_id, mi_info_type_id, mi_info;
+  int64_t n_movie_info;
+  bo_ceb_col ci_movie_id, ci_person_id, ci_role_id;
+  int64_t n_cast_info;
+  bo_ceb_col kt_id, kt_kind;
+  int64_t n_kind_type;
+  bo_ceb_col rt_id, rt_role;
+  int64_t n_role_type;
+  bo_ceb_col nm_id, nm_name;
+  int64_t n_name;
+  const char* name_dict;               /* device */
+  const uint32_t* name_dict_offsets;   /* device, n_name_codes + 1 */
+  int64_t n_name_codes;
+} bo_ceb_q10a_tables;
+
+typedef struct bo_ceb_q10a_params {
+  const uint8_t* info_type_mask;       /* host */
+  int32_t info_type_size;
+  int32_t n_info_codes;
+  const int32_t* info_dense;           /* host, per movie_info.info code */
+  int32_t n_info_dense;
+  int32_t n_kind_codes;
+  const uint8_t* kind_allowed;         /* host, per kind code */
+  const uint8_t* role_allowed;         /* host, per role code */
+  int32_t n_role_codes;
+  int32_t pattern_type;
+  const char* pattern;                 /* host */
+  int32_t pattern_len;
+  int32_t pad;
+} bo_ceb_q10a_params;
+
+typedef struct bo_ceb_q10a_row {
+  int32_t name_code;
+  int32_t info_dense;
+  int32_t has_year;
+  int32_t min_year;
+  int32_t max_year;
+} bo_ceb_q10a_row;
+
+int bo_ceb_q10a(bo_ctx* ctx, const bo_ceb_q10a_tables* tables, const bo_ceb_q10a_params* params,
+                bo_ceb_q10a_row* rows_out, int64_t max_rows, int64_t* n_rows_out, int32_t* dense_out);
+
 /* The CEB builder's fact-table order (bespoke_ceb/builder_impl.cpp:255-360,
  * 432-452): rows sorted by a primary int32 column and, optionally, a
  * secondary one (movie_info by (movie_id, info_type_id), cast_info by

@@ -4,6 +4,7 @@ the reference's id masks, null skips, dense per-movie counts and the
 factorised sum over the qualifying title rows."""
 from __future__ import annotations
 
+import re
 from pathlib import Path
 
 import pyarrow.parquet as pq
@@ -56,3 +57,76 @@ def q1a(path, id1, id2, info1, info2, kind, role, gender, year1, year2) -> int:
             continue
         cast[m] = cast.get(m, 0) + 1
     return sum(cast.get(m, 0) * c1.get(m, 0) * c2.get(m, 0) for m in movies)
+
+
+def q10a(path, ids, infos, name, kinds, roles, pool) -> list:
+    """run_q10a (bespoke_ceb/query_q10a.cpp:334-1130) restated: rows
+    (name, info, min year, max year) -- years None without one -- sorted."""
+    from bespokeolap_artifacts_b200.ceb import ascii_lower, ilike_pattern, string_filter
+
+    type_ids = {i for i in (stoi(v) for v in ids if v not in NULL_WORDS) if i is not None}
+    kf, rf, inf = string_filter(pool, kinds), string_filter(pool, roles), string_filter(pool, infos)
+    if not type_ids or not kf or not rf or not inf:
+        return []
+    (it_ids,), n_it = _cols(path, "info_type", ("id",))
+    tmask = {i for i in type_ids if 0 <= i < n_it + 1}
+    (kid, kk), n_k = _cols(path, "kind_type", ("id", "kind"))
+    kinds_ok = {i for i, v in zip(kid, kk) if i is not None and v is not None and 0 <= i < n_k + 1 and v in kf}
+    (rid, rr), n_r = _cols(path, "role_type", ("id", "role"))
+    roles_ok = {i for i, v in zip(rid, rr) if i is not None and v is not None and 0 <= i < n_r + 1 and v in rf}
+    if not tmask or not kinds_ok or not roles_ok:
+        return []
+    (tid, tkind, tyear), n_t = _cols(path, "title", ("id", "kind_id", "production_year"))
+    present, year = set(), {}
+    for i, k, y in zip(tid, tkind, tyear):
+        if i is None or k is None or k not in kinds_ok or not 0 <= i < n_t + 1:
+            continue
+        present.add(i)
+        year[i] = y
+    (mm, mt, mi), _ = _cols(path, "movie_info", ("movie_id", "info_type_id", "info"))
+    infos_of = {}
+    for m, ty, v in zip(mm, mt, mi):
+        if ty is None or v is None or ty not in tmask or v not in inf or m is None or m not in present:
+            continue
+        infos_of.setdefault(m, []).append(v)
+    (nid, nname), n_n = _cols(path, "name", ("id", "name"))
+    (cm, cp, cr), _ = _cols(path, "cast_info", ("movie_id", "person_id", "role_id"))
+    pairs = [(m, p) for m, p, r in zip(cm, cp, cr)
+             if m is not None and p is not None and r is not None and m in infos_of and r in roles_ok
+             and 0 <= p < n_n + 1]
+    cand = {p for _, p in pairs}
+    ptype, pat = ilike_pattern(name)
+
+    def like(s: str) -> bool:
+        s = ascii_lower(s)
+        if ptype == 0:
+            return True
+        if ptype == 1:
+            return s == pat
+        if ptype == 2:
+            return s.startswith(pat)
+        if ptype == 3:
+            return s.endswith(pat)
+        if ptype == 4:
+            return pat in s
+        return re.fullmatch("".join(".*" if c == "%" else "." if c == "_" else re.escape(c) for c in pat), s,
+                            re.S) is not None
+
+    pname = {}
+    for i, nm in zip(nid, nname):
+        if i is None or nm is None or i not in cand or not like(nm):
+            continue
+        pname[i] = nm
+    agg = {}
+    for m, p in pairs:
+        if p not in pname:
+            continue
+        y = year.get(m)
+        for v in infos_of[m]:
+            key = (pname[p], v)
+            lo, hi = agg.get(key, (None, None))
+            if y is not None:
+                lo = y if lo is None else min(lo, y)
+                hi = y if hi is None else max(hi, y)
+            agg[key] = (lo, hi)
+    return sorted((n, v, lo, hi) for (n, v), (lo, hi) in agg.items())

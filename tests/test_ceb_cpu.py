@@ -60,3 +60,47 @@ def test_q1a_restatement_matches_reference(tmp_path, nulls, seed):
         assert int(g[1][0]) == want, case
         nonzero += want > 0
     assert nonzero >= 3
+
+
+# (ID, INFO, NAME, KIND, ROLE)
+Q10A_CASES = [
+    (["1", "2", "3", "5"], ["V000", "V001", "V005"], "%00%", ["KIND_A", "KIND_B", "KIND_C"], ["ROLE_A", "ROLE_B"]),
+    (["1"], ["V000", "V002"], "name_000%", ["KIND_A", "KIND_D"], ["ROLE_A", "ROLE_C", "ROLE_D"]),
+    (["2", "3"], ["V001"], "%7", ["KIND_B"], ["ROLE_B"]),
+    (["1", "4"], ["V000", "V003"], "%", ["KIND_A"], ["ROLE_A"]),
+    (["1", "2"], ["V000"], "n_me_0_0%1", ["KIND_A", "KIND_B"], ["ROLE_A", "ROLE_E"]),
+    (["1"], ["V000"], "'NAME_0000014'", ["KIND_A", "KIND_B", "KIND_C"], ["ROLE_A", "ROLE_B", "ROLE_C"]),
+    (["x"], ["V000"], "%", ["KIND_A"], ["ROLE_A"]),
+    (["1"], ["NOSUCH"], "%", ["KIND_A"], ["ROLE_A"]),
+]
+
+
+def request10a(case) -> str:
+    ids, infos, name, kinds, roles = case
+    return f'10a {lit(ids)} {lit(infos)} "{name}" {lit(kinds)} {lit(roles)}'
+
+
+def q10a_csv_rows(g):
+    """The reference's 10a CSV rows as (name, info, min, max), sorted (its
+    row order is its aggregation order)."""
+    return sorted((r[0], r[1], int(r[2]) if r[2] else None, int(r[3]) if r[3] else None) for r in g[1:])
+
+
+@pytest.mark.parametrize("nulls,seed", [(False, 1), (True, 2)])
+def test_q10a_restatement_matches_reference(tmp_path, nulls, seed):
+    if not REF_CEB.exists():
+        pytest.skip("reference CEB driver not built")
+    from bespokeolap_artifacts_b200.ceb import string_pool
+    from ceb_restate import q10a
+
+    data = write_ceb(tmp_path / "d", n_title=4000, n_name=8000, n_cast=40_000, n_movie_info=30_000, seed=seed,
+                     nulls=nulls)
+    pool = string_pool(data)
+    got = reference(data, tmp_path / "ref", [request10a(c) for c in Q10A_CASES])
+    nonempty = 0
+    for case, g in zip(Q10A_CASES, got):
+        assert g[0] == ["name", "info", "min(t.production_year)", "max(t.production_year)"]
+        want = q10a(data, *case, pool)
+        assert q10a_csv_rows(g) == want, case
+        nonempty += len(want) > 0
+    assert nonempty >= 4

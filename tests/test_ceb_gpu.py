@@ -69,3 +69,43 @@ def test_builder_order_on_gpu(engine, torch_cuda, tmp_path):
         nl = tables.col(table, "movie_id").is_null
         assert nl is None or not nl.any().item()
     assert ceb.q1a(engine, tables, *Q1A_CASES[0]) == before
+
+
+def gpu_q10a_rows(engine, tables, case):
+    rows = ceb.q10a(engine, tables, *case)
+    return sorted((n, v, lo, hi) for n, v, _, lo, hi in rows)
+
+
+@pytest.mark.parametrize("nulls,seed", [(False, 1), (True, 2)])
+def test_q10a_gpu_matches_reference(engine, torch_cuda, tmp_path, nulls, seed):
+    """CEB query 10a: the GPU's (name, info, min, max) rows equal the
+    reference engine's as sets (the reference emits them in its aggregation
+    order); the dense-matrix aggregation runs here."""
+    if not REF_CEB.exists():
+        pytest.skip("reference CEB driver not built")
+    from test_ceb_cpu import Q10A_CASES, q10a_csv_rows, request10a
+
+    data = write_ceb(tmp_path / "d", n_title=4000, n_name=8000, n_cast=40_000, n_movie_info=30_000, seed=seed,
+                     nulls=nulls)
+    tables = ceb.load_tables(data, ceb.Q10A_COLUMNS)
+    got = reference(data, tmp_path / "ref", [request10a(c) for c in Q10A_CASES])
+    for case, g in zip(Q10A_CASES, got):
+        assert gpu_q10a_rows(engine, tables, case) == q10a_csv_rows(g), case
+
+
+def test_q10a_gpu_hash_aggregation(engine, torch_cuda, tmp_path):
+    """More name strings x info values than the dense matrix holds: the hash
+    aggregation runs and agrees with the restatement."""
+    from bespokeolap_artifacts_b200.ceb import string_pool
+    from ceb_restate import q10a as q10a_restated
+
+    data = write_ceb(tmp_path / "d", n_title=100_000, n_name=700_000, n_cast=2_000_000, n_movie_info=600_000,
+                     seed=8, nulls=True)
+    tables = ceb.load_tables(data, ceb.Q10A_COLUMNS)
+    pool = string_pool(data)
+    infos = [f"V{i:03d}" for i in range(10)]
+    case = (["1", "2", "3", "4", "5"], infos, "%1%", ["KIND_A", "KIND_B", "KIND_C"], ["ROLE_A", "ROLE_B", "ROLE_C"])
+    got = gpu_q10a_rows(engine, tables, case)
+    assert not ceb.q10a.last_dense
+    assert got == q10a_restated(data, *case, pool)
+    assert len(got) > 1000
