@@ -43,6 +43,11 @@ class Column:
     rows: int = 0
     dict_bytes: object = None   # string columns: the dictionary's bytes and
     dict_offsets: object = None  # n + 1 uint32 offsets, on the device
+    dict_rank: object = None    # string columns: each code's position in string order (device)
+
+    def dict_c(self) -> N.CebDict:
+        return N.CebDict(N.ptr(self.dict_bytes), N.ptr(self.dict_offsets), N.ptr(self.dict_rank),
+                         len(self.dictionary or []))
 
     def c(self) -> N.CebCol:
         return N.CebCol(N.ptr(self.values), N.ptr(self.is_null) if self.is_null is not None else None)
@@ -84,19 +89,23 @@ def _column(arr, torch) -> Column:
         offs = np.zeros(len(raw) + 1, np.uint32)
         offs[1:] = np.cumsum([len(b) for b in raw], dtype=np.int64).astype(np.uint32) if raw else []
         blob = np.frombuffer(b"".join(raw) or b"\0", dtype=np.uint8)
-        dict_dev = (torch.from_numpy(blob.copy()).cuda(), torch.from_numpy(offs.view(np.int32).copy()).cuda())
+        rank = np.empty(max(len(dictionary), 1), np.int32)
+        rank[np.array(sorted(range(len(dictionary)), key=lambda i: raw[i]), dtype=np.int64)] = np.arange(
+            len(dictionary), dtype=np.int32)
+        dict_dev = (torch.from_numpy(blob.copy()).cuda(), torch.from_numpy(offs.view(np.int32).copy()).cuda(),
+                    torch.from_numpy(rank).cuda())
     else:
         v = arr.to_numpy(zero_copy_only=False)
         if v.dtype.kind == "f":
             v = np.where(np.isnan(v), 0, v)
         values = np.asarray(v, dtype=np.int64).astype(np.int32)
         dictionary = None
-        dict_dev = (None, None)
+        dict_dev = (None, None, None)
         valid = values[null == 0] if null is not None else values
         mx = int(valid.max()) if len(valid) else -1
     dev = torch.from_numpy(np.ascontiguousarray(values)).cuda()
     ndev = torch.from_numpy(null).cuda() if null is not None else None
-    return Column(dev, ndev, dictionary, mx, n, dict_dev[0], dict_dev[1])
+    return Column(dev, ndev, dictionary, mx, n, *dict_dev)
 
 
 Q1A_COLUMNS = {
@@ -118,6 +127,18 @@ Q10A_COLUMNS = {
     "role_type": ("id", "role"),
     "name": ("id", "name"),
     "info_type": ("id",),
+}
+
+
+Q3B_COLUMNS = {
+    "kind_type": ("id", "kind"),
+    "role_type": ("id", "role"),
+    "company_name": ("id", "name"),
+    "movie_companies": ("movie_id", "company_id", "company_type_id"),
+    "movie_keyword": ("movie_id", "keyword_id"),
+    "title": ("id", "title", "kind_id"),
+    "cast_info": ("movie_id", "person_id", "role_id"),
+    "name": ("id", "name", "name_pcode_nf"),
 }
 
 
@@ -391,3 +412,57 @@ def q10a(engine, t: CebTables, ids, infos, name, kinds, roles, max_rows: int = 1
                     r.min_year if r.has_year else None, r.max_year if r.has_year else None))
     q10a.last_dense = bool(dense.value)
     return out
+
+
+# ------------------------------------------------------------------- 3b ----
+def q3b(engine, t: CebTables, title: str, pcode: str, company: str, kinds, roles, max_rows: int = 1 << 16) -> list:
+    """CEB query 3b (run_q3b, bespoke_ceb/query_q3b.cpp:728-1420) on the GPU:
+    rows (title, name, company, count) in the reference's order (count desc,
+    then the three strings)."""
+    kt, rt = t.col("kind_type", "kind"), t.col("role_type", "role")
+    # the IN lists against the column's own strings (query_q3b.cpp:208-254)
+    kf = string_filter(set(kt.dictionary or []), kinds)
+    rf = string_filter(set(rt.dictionary or []), roles)
+    ka, ra = _code_bytes(kt, kf), _code_bytes(rt, rf)
+    pats = [ilike_pattern(x) for x in (title, pcode, company)]
+    bufs = [np.frombuffer(pt.encode() or b"\0", np.uint8).copy() for _, pt in pats]
+    tab = N.CebQ3bTables()
+    tab.kt_id, tab.kt_kind, tab.n_kind_type = t.col("kind_type", "id").c(), kt.c(), t.rows("kind_type")
+    tab.rt_id, tab.rt_role, tab.n_role_type = t.col("role_type", "id").c(), rt.c(), t.rows("role_type")
+    cn = t.col("company_name", "name")
+    tab.cn_id, tab.cn_name, tab.n_company_name = t.col("company_name", "id").c(), cn.c(), t.rows("company_name")
+    tab.mc_movie_id, tab.mc_company_id, tab.mc_company_type_id = (
+        t.col("movie_companies", c).c() for c in ("movie_id", "company_id", "company_type_id"))
+    tab.n_movie_companies = t.rows("movie_companies")
+    tab.mk_movie_id, tab.mk_keyword_id = (t.col("movie_keyword", c).c() for c in ("movie_id", "keyword_id"))
+    tab.n_movie_keyword = t.rows("movie_keyword")
+    tt = t.col("title", "title")
+    tab.t_id, tab.t_title, tab.t_kind_id = t.col("title", "id").c(), tt.c(), t.col("title", "kind_id").c()
+    tab.n_title = t.rows("title")
+    tab.ci_movie_id, tab.ci_person_id, tab.ci_role_id = (t.col("cast_info", c).c()
+                                                         for c in ("movie_id", "person_id", "role_id"))
+    tab.n_cast_info = t.rows("cast_info")
+    nm, pc = t.col("name", "name"), t.col("name", "name_pcode_nf")
+    tab.nm_id, tab.nm_name, tab.nm_pcode, tab.n_name = t.col("name", "id").c(), nm.c(), pc.c(), t.rows("name")
+    tab.title_dict, tab.name_dict, tab.company_dict, tab.pcode_dict = tt.dict_c(), nm.dict_c(), cn.dict_c(), pc.dict_c()
+    tab.movie_bound = max(t.col("movie_companies", "movie_id").max_value, -1) + 1
+    tab.person_bound = max(t.col("cast_info", "person_id").max_value, -1) + 1
+    p = N.CebQ3bParams()
+    p.kind_allowed, p.role_allowed = ka.ctypes.data, ra.ctypes.data
+    p.n_kind_codes, p.n_role_codes = len(kt.dictionary or []), len(rt.dictionary or [])
+    p.kind_mask_size, p.role_mask_size = _mask_size(t, "kind_type"), _mask_size(t, "role_type")
+    p.company_map_size = _mask_size(t, "company_name")
+    (p.title_type, _), (p.pcode_type, _), (p.company_type, _) = pats
+    p.title_pat, p.pcode_pat, p.company_pat = (b.ctypes.data for b in bufs)
+    p.title_len, p.pcode_len, p.company_len = (len(pt.encode()) for _, pt in pats)
+    while True:
+        rows = (N.CebQ3bRow * max(max_rows, 1))()
+        n = C.c_int64()
+        rc = N.lib().bo_ceb_q3b(engine.ctx.handle, C.byref(tab), C.byref(p), rows, max_rows, C.byref(n))
+        if rc == N.BO_ERR_OVERFLOW and n.value > max_rows:
+            max_rows = int(n.value)  # more groups than rows offered: run again with room for all
+            continue
+        engine.ctx.check(rc, "bo_ceb_q3b")
+        break
+    return [(tt.dictionary[r.title_code], nm.dictionary[r.name_code], cn.dictionary[r.company_code], int(r.count))
+            for r in rows[:n.value]]

@@ -21,7 +21,14 @@ vocabularies, names and titles are numbered strings.
               name ids), role_id (1..12); with nulls=True some null
               person_ids / role_ids.
   name        id 1..n_name (shuffled), name NAME_<id> (some in mixed case,
-              some shared by two persons), gender GENDER_M / GENDER_F / null.
+              some shared by two persons), gender GENDER_M / GENDER_F / null,
+              name_pcode_nf (letter + 3 digits; some null with nulls=True).
+  company_name id 1..n_company (shuffled), name COMP_<id> (some in mixed
+              case, some shared); company_type id 1..4, kind CT_A..CT_D.
+  movie_companies movie_id (bounded Zipf), company_id (bounded Zipf),
+              company_type_id (1..4; some null with nulls=True).
+  keyword     id 1..n_keyword, keyword KW_<id>; movie_keyword movie_id
+              (bounded Zipf), keyword_id (some null with nulls=True).
 """
 from __future__ import annotations
 
@@ -34,9 +41,9 @@ import pyarrow.parquet as pq
 KINDS = [f"KIND_{c}" for c in "ABCDEFG"]
 ROLES = [f"ROLE_{c}" for c in "ABCDEFGHIJKL"]
 GENDERS = ["GENDER_M", "GENDER_F"]
-OTHER_TABLES = ["aka_name", "aka_title", "char_name", "comp_cast_type", "company_name", "company_type",
-                "complete_cast", "keyword", "link_type", "movie_companies", "movie_info_idx", "movie_keyword",
-                "movie_link", "person_info"]
+COMPANY_TYPES = ["CT_A", "CT_B", "CT_C", "CT_D"]
+OTHER_TABLES = ["aka_name", "aka_title", "char_name", "comp_cast_type", "complete_cast", "link_type",
+                "movie_info_idx", "movie_link", "person_info"]
 
 
 def _zipf(rng, n: int, n_ranks: int, s: float) -> np.ndarray:
@@ -62,9 +69,22 @@ def info_value(i: int) -> str:
     return f"V{i:03d}"
 
 
+def name_pcode(k: int) -> str:
+    """A short synthetic phonetic-style code per person: letter + 3 digits."""
+    return f"{chr(65 + k % 26)}{(k * 7) % 1000:03d}"
+
+
+def company(k: int) -> str:
+    """COMP_<k>, every 5th in mixed case, every 13th sharing the name of k // 13."""
+    if k % 13 == 0:
+        k //= 13
+    return f"Comp_{k:06d}" if k % 5 == 0 else f"COMP_{k:06d}"
+
+
 def write_ceb(out: Path, n_title: int = 20_000, n_name: int = 50_000, n_cast: int = 300_000,
               n_movie_info: int = 200_000, n_info_type: int = 113, n_info_values: int = 60, seed: int = 0,
-              nulls: bool = False) -> Path:
+              nulls: bool = False, n_company: int = 2000, n_movie_companies: int = 60_000, n_keyword: int = 3000,
+              n_movie_keyword: int = 80_000) -> Path:
     rng = np.random.default_rng(seed)
     out.mkdir(parents=True, exist_ok=True)
     # title
@@ -92,7 +112,9 @@ def write_ceb(out: Path, n_title: int = 20_000, n_name: int = 50_000, n_cast: in
     nid = rng.permutation(np.arange(1, n_name + 1)).astype(np.int32)
     g = rng.integers(0, 3, n_name)
     gender = pa.array([GENDERS[x] if x < 2 else None for x in g], pa.string())
-    pq.write_table(pa.table({"id": _int(nid), "name": [person_name(k) for k in nid], "gender": gender}),
+    pcode_null = rng.random(n_name) < 0.02 if nulls else None
+    pq.write_table(pa.table({"id": _int(nid), "name": [person_name(k) for k in nid], "gender": gender,
+                             "name_pcode_nf": pa.array([name_pcode(k) for k in nid], pa.string(), mask=pcode_null)}),
                    out / "name.parquet")
     # movie_info: movie ids Zipf over titles (a few beyond the largest id)
     mi_movie = _zipf(rng, n_movie_info, n_title, 0.6) + 1
@@ -114,6 +136,26 @@ def write_ceb(out: Path, n_title: int = 20_000, n_name: int = 50_000, n_cast: in
         r_null = rng.random(n_cast) < 0.01
     pq.write_table(pa.table({"movie_id": _int(ci_movie), "person_id": _int(ci_person, p_null),
                              "role_id": _int(ci_role, r_null)}), out / "cast_info.parquet")
+    # companies, movie_companies, keywords, movie_keyword (a stream of their
+    # own, so the tables above do not depend on these sizes)
+    rng2 = np.random.default_rng([seed, 3])
+    cid = rng2.permutation(np.arange(1, n_company + 1)).astype(np.int32)
+    pq.write_table(pa.table({"id": _int(cid), "name": [company(k) for k in cid]}), out / "company_name.parquet")
+    pq.write_table(pa.table({"id": _int(np.arange(1, len(COMPANY_TYPES) + 1)), "kind": COMPANY_TYPES}),
+                   out / "company_type.parquet")
+    mc_movie = _zipf(rng2, n_movie_companies, n_title, 0.5) + 1
+    mc_comp = _zipf(rng2, n_movie_companies, n_company, 0.8) + 1
+    mc_type = rng2.integers(1, len(COMPANY_TYPES) + 1, n_movie_companies)
+    mc_null = rng2.random(n_movie_companies) < 0.01 if nulls else None
+    pq.write_table(pa.table({"movie_id": _int(mc_movie), "company_id": _int(mc_comp),
+                             "company_type_id": _int(mc_type, mc_null)}), out / "movie_companies.parquet")
+    pq.write_table(pa.table({"id": _int(np.arange(1, n_keyword + 1)),
+                             "keyword": [f"KW_{k:05d}" for k in range(1, n_keyword + 1)]}), out / "keyword.parquet")
+    mk_movie = _zipf(rng2, n_movie_keyword, n_title, 0.5) + 1
+    mk_kw = rng2.integers(1, n_keyword + 1, n_movie_keyword)
+    mk_null = rng2.random(n_movie_keyword) < 0.01 if nulls else None
+    pq.write_table(pa.table({"movie_id": _int(mk_movie), "keyword_id": _int(mk_kw, mk_null)}),
+                   out / "movie_keyword.parquet")
     for t in OTHER_TABLES:
         pq.write_table(pa.table({"id": _int(np.arange(1, 4))}), out / f"{t}.parquet")
     return out

@@ -13,18 +13,23 @@ __device__ __forceinline__ bool ceb_null(const bo_ceb_col& c, int64_t r) { retur
 
 // Appends v to list[] with one reservation per warp (the lanes whose `take`
 // holds).  Every lane of the warp must call it.
-template <class T>
-__device__ __forceinline__ void warp_append(bool take, const T& v, T* __restrict__ list,
-                                            unsigned int* __restrict__ count) {
+template <class T, class Count = unsigned int>
+__device__ __forceinline__ void warp_append(bool take, const T& v, T* __restrict__ list, Count* __restrict__ count) {
   const unsigned int mask = __ballot_sync(0xffffffffu, take);
   if (!mask) return;
   const int lane = threadIdx.x & 31;
   const int leader = __ffs(mask) - 1;
-  unsigned int base = 0;
-  if (lane == leader) base = atomicAdd(count, (unsigned int)__popc(mask));
+  Count base = 0;
+  if (lane == leader) base = atomicAdd(count, (Count)__popc(mask));
   base = __shfl_sync(0xffffffffu, base, leader);
   if (take) list[base + __popc(mask & ((1u << lane) - 1u))] = v;
 }
+
+// match[c] = whether dictionary string c matches the ILIKE pattern (one
+// thread per distinct string).
+__global__ void ceb_like_dict_kernel(const char* __restrict__ bytes, const uint32_t* __restrict__ off, int64_t n,
+                                     int32_t type, const char* __restrict__ pat, int32_t len,
+                                     uint8_t* __restrict__ match);
 
 // mask[id] = 1 for the dimension rows with a non-null id in [0, mask_size)
 // and a non-null string whose code is allowed (the reference's
@@ -34,6 +39,11 @@ __global__ void __launch_bounds__(kCebBlock) ceb_dim_mask_kernel(bo_ceb_col id, 
                                                                  const uint8_t* __restrict__ allowed, int32_t n_codes,
                                                                  int32_t mask_size, uint8_t* __restrict__ mask,
                                                                  unsigned int* __restrict__ any);
+
+// Exclusive scan of n uint32 counts into out[0..n] (out[n] = the total), on
+// the context's stream: per-tile sums, their scan in one block, then each
+// tile's scan plus its base.
+int ceb_exclusive_scan(bo_ctx* ctx, const unsigned int* in, int64_t n, unsigned int* out);
 
 // ILIKE on lower-cased text, the reference's LikePattern kinds
 // (bespoke_ceb/query_q10a.cpp:73-246): the text is lower-cased byte by byte

@@ -10,7 +10,7 @@
 //   ceb_dim_mask_kernel        kind and role id masks;
 //   q10a_title_kernel          present / has-year / year per title id;
 //   q10a_info_kernel<false>    per-title counts of passing movie_info rows,
-//   ceb scan                   their offsets (exclusive scan, three launches),
+//   ceb_exclusive_scan         their offsets (exclusive scan, three launches),
 //   q10a_info_kernel<true>     the rows' dense info indices scattered per title;
 //   q10a_cast_kernel           (title, person) pairs of the allowed roles and
 //                              the candidate persons (warp-aggregated appends);
@@ -31,8 +31,6 @@ namespace bo {
 namespace {
 
 constexpr unsigned long long kEmptyKey = ~0ull;
-constexpr int kScanItems = 4;                        // per thread
-constexpr int kScanTile = kCebBlock * kScanItems;    // per block
 
 struct Q10aMeta {
   unsigned int any_kind, any_role, n_pairs, n_rows;
@@ -85,84 +83,6 @@ __global__ void __launch_bounds__(kCebBlock) q10a_info_kernel(bo_ceb_q10a_tables
     else
       atomicAdd(count + m, 1u);
   }
-}
-
-// Exclusive scan of n counts: per-tile sums, a scan of the tile sums in one
-// block, then each tile's scan plus its base.
-__global__ void __launch_bounds__(kCebBlock) ceb_tile_sum_kernel(const unsigned int* __restrict__ in, int64_t n,
-                                                                 unsigned int* __restrict__ tile_sum) {
-  const int64_t base = (int64_t)blockIdx.x * kScanTile;
-  unsigned int s = 0;
-  for (int i = threadIdx.x; i < kScanTile; i += kCebBlock)
-    if (base + i < n) s += in[base + i];
-  s = warp_sum_u32(s);
-  __shared__ unsigned int part[kCebBlock / 32];
-  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned int t = 0;
-    for (int w = 0; w < kCebBlock / 32; ++w) t += part[w];
-    tile_sum[blockIdx.x] = t;
-  }
-}
-
-// Block-wide exclusive scan of one value per thread; returns the block total.
-__device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int v, unsigned int* total) {
-  __shared__ unsigned int warp_tot[kCebBlock / 32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  unsigned int x = v;
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) warp_tot[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    unsigned int s = lane < kCebBlock / 32 ? warp_tot[lane] : 0u;
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned int y = __shfl_up_sync(0xffffffffu, s, o);
-      if (lane >= o) s += y;
-    }
-    if (lane < kCebBlock / 32) warp_tot[lane] = s;  // inclusive
-  }
-  __syncthreads();
-  const unsigned int before = (w ? warp_tot[w - 1] : 0u) + x - v;
-  *total = warp_tot[kCebBlock / 32 - 1];
-  __syncthreads();
-  return before;
-}
-
-__global__ void __launch_bounds__(kCebBlock) ceb_scan_tile_sums_kernel(unsigned int* __restrict__ tile_sum,
-                                                                       int64_t n_tiles) {
-  unsigned int carry = 0;
-  for (int64_t b = 0; b < n_tiles; b += kCebBlock) {
-    const int64_t i = b + threadIdx.x;
-    const unsigned int v = i < n_tiles ? tile_sum[i] : 0u;
-    unsigned int tot = 0;
-    const unsigned int ex = block_exclusive_scan(v, &tot);
-    if (i < n_tiles) tile_sum[i] = carry + ex;
-    carry += tot;
-  }
-}
-
-__global__ void __launch_bounds__(kCebBlock) ceb_scan_tiles_kernel(const unsigned int* __restrict__ in, int64_t n,
-                                                                   const unsigned int* __restrict__ tile_base,
-                                                                   unsigned int* __restrict__ out) {
-  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
-  unsigned int v[kScanItems], s = 0;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    v[k] = base + k < n ? in[base + k] : 0u;
-    s += v[k];
-  }
-  unsigned int tot = 0;
-  unsigned int run = tile_base[blockIdx.x] + block_exclusive_scan(s, &tot);
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    if (base + k < n) out[base + k] = run;
-    run += v[k];
-  }
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == kCebBlock - 1) out[n] = run;  // the total at out[n]
 }
 
 __global__ void __launch_bounds__(kCebBlock) q10a_cast_kernel(bo_ceb_q10a_tables t, const uint8_t* __restrict__ role,
@@ -367,7 +287,6 @@ extern "C" int bo_ceb_q10a(bo_ctx* ctx, const bo_ceb_q10a_tables* t, const bo_ce
     return BO_OK;  // nothing can join: no rows (query_q10a.cpp:338-520 return early)
   const int64_t title_bound = t->n_title + 1, person_bound = t->n_name + 1;
   const int32_t kind_size = (int32_t)(t->n_kind_type + 1), role_size = (int32_t)(t->n_role_type + 1);
-  const int64_t n_tiles = (title_bound + kScanTile - 1) / kScanTile;
   // Workspace (everything before `zero_end` starts at zero).
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -383,7 +302,6 @@ extern "C" int bo_ceb_q10a(bo_ctx* ctx, const bo_ceb_q10a_tables* t, const bo_ce
   const size_t zero_end = off;
   const size_t o_year = take(4 * (size_t)title_bound);
   const size_t o_offset = take(4 * ((size_t)title_bound + 1));
-  const size_t o_tiles = take(4 * (size_t)n_tiles);
   const size_t o_values = take(4 * (size_t)t->n_movie_info);
   const size_t o_pairs = take(sizeof(int2) * (size_t)t->n_cast_info);
   const size_t o_pname = take(4 * (size_t)person_bound);
@@ -405,7 +323,6 @@ extern "C" int bo_ceb_q10a(bo_ctx* ctx, const bo_ceb_q10a_tables* t, const bo_ce
   auto* cand = reinterpret_cast<uint8_t*>(ws + o_cand);
   auto* year = reinterpret_cast<int32_t*>(ws + o_year);
   auto* offset = reinterpret_cast<unsigned int*>(ws + o_offset);
-  auto* tiles = reinterpret_cast<unsigned int*>(ws + o_tiles);
   auto* values = reinterpret_cast<int32_t*>(ws + o_values);
   auto* pairs = reinterpret_cast<int2*>(ws + o_pairs);
   auto* pname = reinterpret_cast<int32_t*>(ws + o_pname);
@@ -447,12 +364,7 @@ extern "C" int bo_ceb_q10a(bo_ctx* ctx, const bo_ceb_q10a_tables* t, const bo_ce
   q10a_info_kernel<false><<<gi, kCebBlock, 0, ctx->stream>>>(*t, tmask, p->info_type_size, dense, p->n_info_codes,
                                                              present, title_bound, count, nullptr, nullptr, nullptr);
   if ((rc = after_launch(ctx, "q10a_info_kernel"))) return rc;
-  ceb_tile_sum_kernel<<<(int)n_tiles, kCebBlock, 0, ctx->stream>>>(count, title_bound, tiles);
-  if ((rc = after_launch(ctx, "ceb_tile_sum_kernel"))) return rc;
-  ceb_scan_tile_sums_kernel<<<1, kCebBlock, 0, ctx->stream>>>(tiles, n_tiles);
-  if ((rc = after_launch(ctx, "ceb_scan_tile_sums_kernel"))) return rc;
-  ceb_scan_tiles_kernel<<<(int)n_tiles, kCebBlock, 0, ctx->stream>>>(count, title_bound, tiles, offset);
-  if ((rc = after_launch(ctx, "ceb_scan_tiles_kernel"))) return rc;
+  if ((rc = ceb_exclusive_scan(ctx, count, title_bound, offset))) return rc;
   q10a_info_kernel<true><<<gi, kCebBlock, 0, ctx->stream>>>(*t, tmask, p->info_type_size, dense, p->n_info_codes,
                                                             present, title_bound, nullptr, offset, cursor, values);
   if ((rc = after_launch(ctx, "q10a_info_kernel"))) return rc;

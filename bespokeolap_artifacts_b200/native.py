@@ -338,6 +338,41 @@ class CebQ1aParams(C.Structure):
                 ("pad", C.c_int32)]
 
 
+class CebDict(C.Structure):
+    """``bo_ceb_dict``: a string dictionary on the device (bytes, n + 1 offsets, each code's string rank)."""
+    _fields_ = [("bytes", C.c_void_p), ("offsets", C.c_void_p), ("rank", C.c_void_p), ("n", C.c_int64)]
+
+
+class CebQ3bTables(C.Structure):
+    """``bo_ceb_q3b_tables``: the columns CEB query 3b reads, its string dictionaries and id bounds."""
+    _fields_ = [("kt_id", CebCol), ("kt_kind", CebCol), ("n_kind_type", C.c_int64),
+                ("rt_id", CebCol), ("rt_role", CebCol), ("n_role_type", C.c_int64),
+                ("cn_id", CebCol), ("cn_name", CebCol), ("n_company_name", C.c_int64),
+                ("mc_movie_id", CebCol), ("mc_company_id", CebCol), ("mc_company_type_id", CebCol),
+                ("n_movie_companies", C.c_int64),
+                ("mk_movie_id", CebCol), ("mk_keyword_id", CebCol), ("n_movie_keyword", C.c_int64),
+                ("t_id", CebCol), ("t_title", CebCol), ("t_kind_id", CebCol), ("n_title", C.c_int64),
+                ("ci_movie_id", CebCol), ("ci_person_id", CebCol), ("ci_role_id", CebCol), ("n_cast_info", C.c_int64),
+                ("nm_id", CebCol), ("nm_name", CebCol), ("nm_pcode", CebCol), ("n_name", C.c_int64),
+                ("title_dict", CebDict), ("name_dict", CebDict), ("company_dict", CebDict), ("pcode_dict", CebDict),
+                ("movie_bound", C.c_int32), ("person_bound", C.c_int32)]
+
+
+class CebQ3bParams(C.Structure):
+    """``bo_ceb_q3b_params``: kind / role codes, id mask sizes and the three ILIKE patterns (host memory)."""
+    _fields_ = [("kind_allowed", C.c_void_p), ("role_allowed", C.c_void_p), ("n_kind_codes", C.c_int32),
+                ("n_role_codes", C.c_int32), ("kind_mask_size", C.c_int32), ("role_mask_size", C.c_int32),
+                ("company_map_size", C.c_int32), ("title_type", C.c_int32), ("pcode_type", C.c_int32),
+                ("company_type", C.c_int32), ("title_pat", C.c_void_p), ("pcode_pat", C.c_void_p),
+                ("company_pat", C.c_void_p), ("title_len", C.c_int32), ("pcode_len", C.c_int32),
+                ("company_len", C.c_int32), ("pad", C.c_int32)]
+
+
+class CebQ3bRow(C.Structure):
+    _fields_ = [("title_code", C.c_int32), ("name_code", C.c_int32), ("company_code", C.c_int32),
+                ("pad", C.c_int32), ("count", C.c_int64)]
+
+
 class CebQ10aTables(C.Structure):
     """``bo_ceb_q10a_tables``: the columns CEB query 10a reads and the name dictionary on the device."""
     _fields_ = [("t_id", CebCol), ("t_kind_id", CebCol), ("t_year", CebCol), ("n_title", C.c_int64),
@@ -499,6 +534,8 @@ _SIGNATURES = {
                               C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.c_int32,
                               C.POINTER(C.c_int64)]),
     "bo_tpch_q21": (C.c_int, [_P, C.POINTER(TpchQ21Tables), C.c_int32, _P, C.c_int32, _P]),
+    "bo_ceb_q3b": (C.c_int, [_P, C.POINTER(CebQ3bTables), C.POINTER(CebQ3bParams), _P, C.c_int64,
+                             C.POINTER(C.c_int64)]),
     "bo_ceb_q10a": (C.c_int, [_P, C.POINTER(CebQ10aTables), C.POINTER(CebQ10aParams), _P, C.c_int64,
                               C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "bo_ceb_sort_rows": (C.c_int, [_P, _P, _P, C.c_int64, _P]),

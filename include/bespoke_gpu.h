@@ -1058,6 +1058,72 @@ typedef struct bo_ceb_q10a_row {
 int bo_ceb_q10a(bo_ctx* ctx, const bo_ceb_q10a_tables* tables, const bo_ceb_q10a_params* params,
                 bo_ceb_q10a_row* rows_out, int64_t max_rows, int64_t* n_rows_out, int32_t* dense_out);
 
+/* CEB query 3b: run_q3b of bespoke_ceb/query_q3b.cpp:728-1420 -- COUNT(*)
+ * per (title, person name, company name) over movies with companies whose
+ * name matches `company` (ILIKE), keywords, a title of an allowed kind that
+ * matches `title`, and cast rows of an allowed role whose person's
+ * name_pcode_nf matches `pcode`; the count of a movie's (person, company)
+ * is keywords x cast rows x company rows (the reference's nested
+ * per-movie maps, :1330-1360), summed per group and ordered by count desc,
+ * then the title, name and company strings (:1369-1385; str_rank arrays give
+ * each dictionary code its string order).  Movie ids are bounded by
+ * movie_bound (the largest movie_companies movie id + 1), person ids by
+ * person_bound.  Dictionary codes are packed into one 64-bit group key, so
+ * the three dictionaries' code widths must add up to 64 bits at most
+ * (BO_ERR_UNSUPPORTED otherwise).  Rows go to rows_out (host) in the
+ * reference's order; BO_ERR_OVERFLOW with *n_rows_out set when there are
+ * more than max_rows. */
+typedef struct bo_ceb_dict {
+  const char* bytes;                   /* device */
+  const uint32_t* offsets;             /* device, n + 1 */
+  const int32_t* rank;                 /* device: order of each code's string */
+  int64_t n;
+} bo_ceb_dict;
+
+typedef struct bo_ceb_q3b_tables {
+  bo_ceb_col kt_id, kt_kind;
+  int64_t n_kind_type;
+  bo_ceb_col rt_id, rt_role;
+  int64_t n_role_type;
+  bo_ceb_col cn_id, cn_name;
+  int64_t n_company_name;
+  bo_ceb_col mc_movie_id, mc_company_id, mc_company_type_id;
+  int64_t n_movie_companies;
+  bo_ceb_col mk_movie_id, mk_keyword_id;
+  int64_t n_movie_keyword;
+  bo_ceb_col t_id, t_title, t_kind_id;
+  int64_t n_title;
+  bo_ceb_col ci_movie_id, ci_person_id, ci_role_id;
+  int64_t n_cast_info;
+  bo_ceb_col nm_id, nm_name, nm_pcode;
+  int64_t n_name;
+  bo_ceb_dict title_dict, name_dict, company_dict, pcode_dict;
+  int32_t movie_bound, person_bound;
+} bo_ceb_q3b_tables;
+
+typedef struct bo_ceb_q3b_params {
+  const uint8_t* kind_allowed;         /* host, per kind code */
+  const uint8_t* role_allowed;         /* host, per role code */
+  int32_t n_kind_codes, n_role_codes;
+  int32_t kind_mask_size, role_mask_size, company_map_size;
+  int32_t title_type, pcode_type, company_type;  /* ILIKE kinds as for 10a */
+  const char* title_pat;               /* host, lower-cased */
+  const char* pcode_pat;
+  const char* company_pat;
+  int32_t title_len, pcode_len, company_len, pad;
+} bo_ceb_q3b_params;
+
+typedef struct bo_ceb_q3b_row {
+  int32_t title_code;
+  int32_t name_code;
+  int32_t company_code;
+  int32_t pad;
+  int64_t count;
+} bo_ceb_q3b_row;
+
+int bo_ceb_q3b(bo_ctx* ctx, const bo_ceb_q3b_tables* tables, const bo_ceb_q3b_params* params,
+               bo_ceb_q3b_row* rows_out, int64_t max_rows, int64_t* n_rows_out);
+
 /* The CEB builder's fact-table order (bespoke_ceb/builder_impl.cpp:255-360,
  * 432-452): rows sorted by a primary int32 column and, optionally, a
  * secondary one (movie_info by (movie_id, info_type_id), cast_info by

@@ -130,3 +130,93 @@ def q10a(path, ids, infos, name, kinds, roles, pool) -> list:
                 hi = y if hi is None else max(hi, y)
             agg[key] = (lo, hi)
     return sorted((n, v, lo, hi) for (n, v), (lo, hi) in agg.items())
+
+
+def _like(ptype: int, pat: str, s: str) -> bool:
+    from bespokeolap_artifacts_b200.ceb import ascii_lower
+
+    s = ascii_lower(s)
+    if ptype == 0:
+        return True
+    if ptype == 1:
+        return s == pat
+    if ptype == 2:
+        return s.startswith(pat)
+    if ptype == 3:
+        return s.endswith(pat)
+    if ptype == 4:
+        return pat in s
+    return re.fullmatch("".join(".*" if c == "%" else "." if c == "_" else re.escape(c) for c in pat), s,
+                        re.S) is not None
+
+
+def q3b(path, title, pcode, company, kinds, roles) -> list:
+    """run_q3b (bespoke_ceb/query_q3b.cpp:728-1420) restated: per movie the
+    movie_companies counts of companies whose name matches, the
+    movie_keyword count, the title (allowed kind, matching title), the
+    cast_info counts of persons of an allowed role whose pcode matches;
+    count = keywords x cast x companies per (title, name, company), ordered
+    by count desc, title, name, company."""
+    from bespokeolap_artifacts_b200.ceb import ilike_pattern, string_filter
+
+    tp, pp, cp = ilike_pattern(title), ilike_pattern(pcode), ilike_pattern(company)
+    (kid, kk), n_k = _cols(path, "kind_type", ("id", "kind"))
+    kf = string_filter({v for v in kk if v is not None}, kinds)
+    kinds_ok = {i for i, v in zip(kid, kk) if i is not None and v is not None and i >= 0 and v in kf}
+    (rid, rr), n_r = _cols(path, "role_type", ("id", "role"))
+    rf = string_filter({v for v in rr if v is not None}, roles)
+    roles_ok = {i for i, v in zip(rid, rr) if i is not None and v is not None and i >= 0 and v in rf}
+    if not kinds_ok or not roles_ok:
+        return []
+    (cid, cname), _ = _cols(path, "company_name", ("id", "name"))
+    comp = {}
+    for i, nm in zip(cid, cname):
+        if i is not None and nm is not None and i >= 0 and _like(*cp, nm):
+            comp[i] = nm
+    if not comp:
+        return []
+    (mm, mc, mt), _ = _cols(path, "movie_companies", ("movie_id", "company_id", "company_type_id"))
+    mc_by = {}
+    for m, c, ty in zip(mm, mc, mt):
+        if m is None or c is None or ty is None or c not in comp:
+            continue
+        d = mc_by.setdefault(m, {})
+        d[c] = d.get(c, 0) + 1
+    (km, kw), _ = _cols(path, "movie_keyword", ("movie_id", "keyword_id"))
+    mk = {}
+    for m, k in zip(km, kw):
+        if m is None or k is None or m not in mc_by:
+            continue
+        mk[m] = mk.get(m, 0) + 1
+    cand = {m for m in mc_by if mk.get(m)}
+    (tid, ttitle, tkind), _ = _cols(path, "title", ("id", "title", "kind_id"))
+    titles = {}
+    for i, tt, k in zip(tid, ttitle, tkind):
+        if i is None or i not in cand or i in titles or tt is None or k is None or k not in kinds_ok:
+            continue
+        if _like(*tp, tt):
+            titles[i] = tt
+    (cm, cpers, crole), _ = _cols(path, "cast_info", ("movie_id", "person_id", "role_id"))
+    ci_by = {}
+    for m, p, r in zip(cm, cpers, crole):
+        if m is None or p is None or r is None or m not in titles or r not in roles_ok:
+            continue
+        d = ci_by.setdefault(m, {})
+        d[p] = d.get(p, 0) + 1
+    persons = {p for d in ci_by.values() for p in d if p >= 0}
+    (nid, nname, npc), _ = _cols(path, "name", ("id", "name", "name_pcode_nf"))
+    pname = {}
+    for i, nm, pc in zip(nid, nname, npc):
+        if i is None or i not in persons or i in pname or nm is None or pc is None:
+            continue
+        if _like(*pp, pc):
+            pname[i] = nm
+    out = {}
+    for m, d in ci_by.items():
+        for p, ci in d.items():
+            if p not in pname:
+                continue
+            for c, n in mc_by[m].items():
+                key = (titles[m], pname[p], comp[c])
+                out[key] = out.get(key, 0) + mk[m] * ci * n
+    return sorted(((t, n, c, v) for (t, n, c), v in out.items()), key=lambda r: (-r[3], r[0], r[1], r[2]))

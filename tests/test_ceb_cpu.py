@@ -104,3 +104,40 @@ def test_q10a_restatement_matches_reference(tmp_path, nulls, seed):
         assert q10a_csv_rows(g) == want, case
         nonempty += len(want) > 0
     assert nonempty >= 4
+
+
+# (TITLE, NAME_PCODE_NF, NAME, KIND, ROLE)
+Q3B_CASES = [
+    ("%1%", "a%", "%00%", ["KIND_A", "KIND_B", "KIND_C"], ["ROLE_A", "ROLE_B", "ROLE_C"]),
+    ("title_1%", "%", "comp_%", ["KIND_A"], ["ROLE_A", "ROLE_D"]),
+    ("%", "_1%", "%5", ["KIND_B", "KIND_C", "KIND_D"], ["ROLE_B"]),
+    ("%2", "b%", "comp_0000%", ["KIND_A", "KIND_B"], ["ROLE_A", "ROLE_B", "ROLE_C", "ROLE_D"]),
+    ("%", "%", "nosuch%", ["KIND_A"], ["ROLE_A"]),
+]
+
+
+def request3b(case) -> str:
+    title, pcode, company, kinds, roles = case
+    return f'3b "{title}" "{pcode}" "{company}" {lit(kinds)} {lit(roles)}'
+
+
+def q3b_csv_rows(g):
+    return [(r[0], r[1], r[2], int(r[3])) for r in g[1:]]
+
+
+@pytest.mark.parametrize("nulls,seed", [(False, 1), (True, 2)])
+def test_q3b_restatement_matches_reference(tmp_path, nulls, seed):
+    if not REF_CEB.exists():
+        pytest.skip("reference CEB driver not built")
+    from ceb_restate import q3b
+
+    data = write_ceb(tmp_path / "d", n_title=4000, n_name=8000, n_cast=40_000, n_movie_info=30_000, seed=seed,
+                     nulls=nulls, n_company=500, n_movie_companies=12_000, n_keyword=800, n_movie_keyword=15_000)
+    got = reference(data, tmp_path / "ref", [request3b(c) for c in Q3B_CASES])
+    nonempty = 0
+    for case, g in zip(Q3B_CASES, got):
+        assert g[0] == ["title", "name", "name_1", "count_star()"]
+        want = q3b(data, *case)
+        assert q3b_csv_rows(g) == want, case
+        nonempty += len(want) > 0
+    assert nonempty >= 3

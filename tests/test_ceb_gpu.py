@@ -109,3 +109,33 @@ def test_q10a_gpu_hash_aggregation(engine, torch_cuda, tmp_path):
     assert not ceb.q10a.last_dense
     assert got == q10a_restated(data, *case, pool)
     assert len(got) > 1000
+
+
+@pytest.mark.parametrize("nulls,seed", [(False, 1), (True, 2)])
+def test_q3b_gpu_matches_reference(engine, torch_cuda, tmp_path, nulls, seed):
+    """CEB query 3b: the GPU's rows equal the reference engine's, in its
+    order (count desc, then title, name, company)."""
+    if not REF_CEB.exists():
+        pytest.skip("reference CEB driver not built")
+    from test_ceb_cpu import Q3B_CASES, q3b_csv_rows, request3b
+
+    data = write_ceb(tmp_path / "d", n_title=4000, n_name=8000, n_cast=40_000, n_movie_info=30_000, seed=seed,
+                     nulls=nulls, n_company=500, n_movie_companies=12_000, n_keyword=800, n_movie_keyword=15_000)
+    tables = ceb.load_tables(data, ceb.Q3B_COLUMNS)
+    ceb.builder_order(engine, tables)
+    got = reference(data, tmp_path / "ref", [request3b(c) for c in Q3B_CASES])
+    for case, g in zip(Q3B_CASES, got):
+        assert ceb.q3b(engine, tables, *case) == q3b_csv_rows(g), case
+
+
+def test_q3b_gpu_larger_tables(engine, torch_cuda, tmp_path):
+    from ceb_restate import q3b as q3b_restated
+
+    data = write_ceb(tmp_path / "d", n_title=100_000, n_name=200_000, n_cast=1_500_000, n_movie_info=1000, seed=9,
+                     nulls=True, n_company=20_000, n_movie_companies=400_000, n_keyword=5000,
+                     n_movie_keyword=500_000)
+    tables = ceb.load_tables(data, ceb.Q3B_COLUMNS)
+    case = ("%1%", "a%", "%00%", ["KIND_A", "KIND_B", "KIND_C"], ["ROLE_A", "ROLE_B", "ROLE_C"])
+    got = ceb.q3b(engine, tables, *case)
+    assert got == q3b_restated(data, *case)
+    assert len(got) > 100
