@@ -178,10 +178,14 @@ class Slot:
     gb_pred_h: object = None            # their predicted group counts (pinned host, device)
     gb_pred_d: object = None
     event: object = None                # recorded after the slot's last launch
+    q1_out: object = None               # device groups of a lone scan-agg request
+    pred_h: object = None               # pinned / device prediction of a lone join request
+    pred_d: object = None
     reqs: list = field(default_factory=list)
     joins: list = field(default_factory=list)
     gbs: list = field(default_factory=list)
     others: list = field(default_factory=list)
+    lone: object = None                 # a request run alone through its standalone kernels
     busy: bool = False
 
 
@@ -195,7 +199,9 @@ class BatchedServer:
     prediction, A's id mask built once at load; an overflowed table is rerun
     exactly), and the scan-agg requests run as instances of the slot's
     persistent batch kernel -- all on the slot's stream, one event at the
-    end.  With shared=False every request is a batch instance."""
+    end.  A request that finds an idle slot with nothing else waiting runs
+    alone through its standalone kernel (scan-agg) or the presized join.
+    With shared=False every request is a batch instance."""
 
     def __init__(self, tables: ServingTables, n_slots: int = 2, max_batch: int = 16,
                  pool_bytes: int = 2 << 30, max_items: int = 65536, workers_per_sm: int = 1,
@@ -219,6 +225,9 @@ class BatchedServer:
             slot.gb_out = torch.zeros(max_batch * C.sizeof(N.GbResult), dtype=torch.uint8, device="cuda")
             slot.gb_pred_h = torch.zeros(max_batch, dtype=torch.float32).pin_memory()
             slot.gb_pred_d = torch.zeros(max_batch, dtype=torch.float32, device="cuda")
+            slot.q1_out = torch.zeros(N.Q1_MAX_GROUPS * C.sizeof(N.Q1Agg), dtype=torch.uint8, device="cuda")
+            slot.pred_h = torch.zeros(1, dtype=torch.float32).pin_memory()
+            slot.pred_d = torch.zeros(1, dtype=torch.float32, device="cuda")
             self.slots.append(slot)
         self.launches = 0
 
@@ -235,11 +244,43 @@ class BatchedServer:
             return tb, 0  # its own pipeline: HBM footprint from the prediction, no batch work items
         return tb, items
 
+    def _launch_lone(self, s: Slot, r: Request) -> None:
+        """A request that finds an idle slot and no other request waiting runs
+        alone through its standalone kernels (the scan-agg kernel, the
+        presized join), not through the batch machinery: at low load nothing
+        is there to share, and the batch kernel's re-plan would only add to
+        its latency."""
+        import torch
+
+        s.lone = r
+        if r.kind == N.BATCH_SCAN_AGG:
+            f, p = self.tables.fact, r.params
+            cols = [f[k] for k in ("ship_date", "quantity", "ext_price", "discount", "tax", "flag_a", "flag_b")]
+            s.engine.q1_fact_device(cols, int(f["ship_date"].numel()), p["cutoff"], p["n_flag_a"], p["n_flag_b"],
+                                    s.q1_out)
+        else:
+            j = self.tables.join
+            s.pred_h[0] = float(r.predicted) if r.predicted > 0 else float(j["b_key"].numel())
+            with torch.cuda.stream(s.stream):
+                s.pred_d.copy_(s.pred_h, non_blocking=True)
+            s.engine.join_presized_device((j["b_key"], j["b_date"], j["b_seg"]), (j["p_fk"], j["p_price"], j["p_disc"]),
+                                          int(j["b_key"].numel()), int(j["p_fk"].numel()), r.params["date_lt"],
+                                          r.params["seg_eq"], s.pred_d, s.join_out)
+
     def _launch(self, s: Slot, reqs: list) -> None:
         """Enqueues one slot's requests on its stream: the shared joins, then
         the batch kernel over the rest; an event marks the end."""
         import torch
 
+        s.lone = None
+        if self.shared and len(reqs) == 1 and reqs[0].kind in (N.BATCH_SCAN_AGG, N.BATCH_JOIN):
+            s.joins, s.gbs, s.others = [], [], []
+            self._launch_lone(s, reqs[0])
+            s.event = torch.cuda.Event()
+            s.event.record(s.stream)
+            s.reqs, s.busy = reqs, True
+            self.launches += 1
+            return
         s.joins = [r for r in reqs if self.shared and r.kind == N.BATCH_JOIN]
         s.gbs = [r for r in reqs if self.shared and r.kind == N.BATCH_GROUPBY]
         s.others = [r for r in reqs if not (self.shared and r.kind in (N.BATCH_JOIN, N.BATCH_GROUPBY))]
@@ -271,6 +312,22 @@ class BatchedServer:
     def _results(self, s: Slot) -> None:
         """Fills the results of a finished slot's requests (an overflowed
         instance or a shared join over repeated keys is rerun exactly)."""
+        if s.lone is not None:
+            r = s.lone
+            s.engine.ctx.call("bo_check_errors")
+            if r.kind == N.BATCH_SCAN_AGG:
+                ng = r.params["n_flag_a"] * r.params["n_flag_b"]
+                host = s.q1_out[: ng * C.sizeof(N.Q1Agg)].cpu().numpy().tobytes()
+                aggs = (N.Q1Agg * ng).from_buffer_copy(host)
+                r.result = {"kind": "scan_agg", "groups": [aggs[g].as_dict() for g in range(ng)], "reruns": 0}
+            else:
+                d = N.JoinResult.from_buffer_copy(s.join_out[: C.sizeof(N.JoinResult)].cpu().numpy().tobytes()).as_dict()
+                if d["overflowed"]:  # predicted too few qualifying rows: the exact form
+                    d = B.solo_result(s.engine, instance_of(self.tables, r))
+                    d["reruns"] = 1
+                d["kind"] = "join"
+                r.result = d
+            return
         if s.others:
             for r, x in zip(s.others, s.batch.results()):
                 r.result = x
