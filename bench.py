@@ -453,7 +453,7 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     # ---- the other configurations (rank 0; extra keys of the same line)
     extra = {}
     if rank == 0 and args.sections != "none":
-        wanted = (["scan_agg", "groupby", "join_large", "batch", "serving", "tpch"] if args.sections == "all"
+        wanted = (["scan_agg", "groupby", "join_large", "batch", "serving", "tpch", "ceb"] if args.sections == "all"
                   else args.sections.split(","))
         peak_gbs, _ = peaks()
         keep = {}
@@ -472,6 +472,8 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
                     extra[name] = serving_section(eng, stream, sizer, keep.get("gb_sizer"))
                 elif name == "tpch":
                     extra[name] = tpch_section()
+                elif name == "ceb":
+                    extra[name] = ceb_section(eng)
             except Exception as e:  # report, never lose the headline line
                 extra[name] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
             if name in extra:
@@ -993,7 +995,8 @@ TPCH_REQUESTS = [  # synthetic parameters: segments, ship modes and comment word
     ("8", '8 "NATION_10" "REGION0" "STD_B"'),
     ("10", '10 "1993-10-01"'), ("11", '11 "NATION_04" "0.0001"'), ("12", '12 "MODE_A" "MODE_C" "1994-01-01"'), ("13", '13 "pending" "deposits"'),
     ("14", '14 "1995-09-01"'), ("15", '15 "1996-01-01" "1"'), ("17", '17 "BRAND_B" "CONT_C"'), ("18", '18 "250"'),
-    ("22", '22 "13" "31" "23" "29" "30" "18" "17"'),
+    ("22", '22 "13" "31" "23" "29" "30" "18" "17"'), ("9", '9 "co"'),
+    ("19", '19 "1" "10" "20" "BRAND_A" "BRAND_B" "BRAND_C"'), ("21", '21 "NATION_04"'),
 ]
 
 
@@ -1068,6 +1071,104 @@ def tpch_section(reps: int = 10, n_customer: int = 150_000, n_orders: int = 1_50
                 if q["ref_mean_ms"] > 0:
                     q["speedup_vs_ref_mean"] = q["ref_mean_ms"] / q["gpu_ms"]
             out["queries"]["Q" + qid] = q
+        return out
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+CEB_REQUESTS = [  # synthetic parameters over the seeded IMDB-shaped vocabularies
+    ("1a", (["1", "2", "3", "5"], ["7", "8", "9"], ["V000", "V001", "V005"], ["V002", "V003"],
+            ["KIND_A", "KIND_B", "KIND_C"], ["ROLE_A", "ROLE_B", "ROLE_D"], ["GENDER_F", "GENDER_M"], "2015", "1950")),
+    ("10a", (["1", "2", "3", "5"], ["V000", "V001", "V005"], "%00%", ["KIND_A", "KIND_B", "KIND_C"],
+             ["ROLE_A", "ROLE_B"])),
+    ("3b", ("%1%", "a%", "%00%", ["KIND_A", "KIND_B", "KIND_C"], ["ROLE_A", "ROLE_B", "ROLE_C"])),
+]
+
+
+def _ceb_lit(vals):
+    return "(" + ", ".join("'" + v.replace("'", "''") + "'" for v in vals) + ")"
+
+
+def _ceb_request(qid: str, a) -> str:
+    L = _ceb_lit
+    if qid == "1a":
+        return f'1a {L(a[0])} {L(a[1])} {L(a[2])} {L(a[3])} {L(a[4])} {L(a[5])} {L(a[6])} "{a[7]}" "{a[8]}"'
+    if qid == "10a":
+        return f'10a {L(a[0])} {L(a[1])} "{a[2]}" {L(a[3])} {L(a[4])}'
+    return f'3b "{a[0]}" "{a[1]}" "{a[2]}" {L(a[3])} {L(a[4])}'
+
+
+def ceb_section(eng, reps: int = 5) -> dict:
+    """CEB queries 1a, 10a and 3b: the GPU pipelines over device columns in
+    the reference's layout (builder's order applied on the device) against
+    the reference's own CEB engine (compiled unchanged, its query() pinned to
+    one core) on the same seeded IMDB-shaped Parquet files; per query the
+    median time of each and whether the answers agree (1a: the count; 10a:
+    the rows as a set -- the reference emits them in its aggregation order;
+    3b: the rows in order).  GPU times are wall times of the C-ABI call with
+    the result rows copied to the host as codes (no Python strings)."""
+    import csv
+    import shutil
+    import tempfile
+
+    from bespokeolap_artifacts_b200 import ceb
+    from bespokeolap_artifacts_b200.ceb_data import write_ceb
+
+    sizes = dict(n_title=1_000_000, n_name=1_500_000, n_cast=20_000_000, n_movie_info=8_000_000,
+                 n_company=100_000, n_movie_companies=2_000_000, n_keyword=50_000, n_movie_keyword=4_000_000)
+    tmp = Path(tempfile.mkdtemp(prefix="bo_ceb_"))
+    try:
+        t0 = time.perf_counter()
+        data = write_ceb(tmp / "d", seed=21, nulls=True, **sizes)
+        gen_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        cols = {}
+        for cs in (ceb.Q1A_COLUMNS, ceb.Q10A_COLUMNS, ceb.Q3B_COLUMNS):
+            for tname, cn in cs.items():
+                cols[tname] = tuple(dict.fromkeys(cols.get(tname, ()) + cn))
+        tables = ceb.load_tables(data, cols)
+        ceb.builder_order(eng, tables)
+        load_s = time.perf_counter() - t0
+        out = {"data": f"seeded synthetic IMDB-shaped Parquet: {sizes} (generated in {gen_s:.0f} s, loaded and "
+                       f"ordered on the device in {load_s:.1f} s)", "reps": reps, "queries": {}}
+        gpu_rows = {}
+        for qid, a in CEB_REQUESTS:
+            fn = {"1a": ceb.q1a, "10a": ceb.q10a, "3b": ceb.q3b}[qid]
+            gpu_rows[qid] = fn(eng, tables, *a)
+            kw = {} if qid == "1a" else {"raw": True}
+            ts = []
+            for _ in range(reps):
+                eng.synchronize()
+                t1 = time.perf_counter()
+                fn(eng, tables, *a, **kw)
+                ts.append((time.perf_counter() - t1) * 1e3)
+            out["queries"][qid] = {"gpu_ms": statistics.median(ts)}
+        ref = ROOT / "oracle" / "_ref" / "ref_ceb_driver"
+        if ref.exists():
+            reqs = [_ceb_request(q, a) for q, a in CEB_REQUESTS for _ in range(reps)]
+            wd = tmp / "ref"
+            wd.mkdir()
+            p = subprocess.run([str(ref), str(data) + "/"], input="\n".join(reqs) + "\n\n", text=True,
+                               capture_output=True, cwd=wd, timeout=900)
+            times = [float(m.group(1)) for m in re.finditer(r"\| Execution ms: (\d+)", p.stdout)]
+            for qi, (qid, _) in enumerate(CEB_REQUESTS):
+                q = out["queries"][qid]
+                q["ref_ms"] = statistics.median(times[qi * reps:(qi + 1) * reps]) if len(times) == len(reqs) else None
+                rows = list(csv.reader(open(wd / f"result{qi * reps + 1}.csv")))
+                g = gpu_rows[qid]
+                if qid == "1a":
+                    q["answers_identical"] = int(rows[1][0]) == g
+                elif qid == "10a":
+                    want = sorted((r[0], r[1], int(r[2]) if r[2] else None, int(r[3]) if r[3] else None)
+                                  for r in rows[1:])
+                    q["answers_identical"] = sorted((n, v, lo, hi) for n, v, _, lo, hi in g) == want
+                    q["rows"] = len(want)
+                else:
+                    q["answers_identical"] = [(r[0], r[1], r[2], int(r[3])) for r in rows[1:]] == g
+                    q["rows"] = len(g)
+                if q["ref_ms"]:
+                    q["speedup_vs_ref"] = q["ref_ms"] / q["gpu_ms"]
+            out["ref_note"] = f"reference query() reports whole milliseconds, single-threaded; host {host_cpu()}"
         return out
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
@@ -1158,7 +1259,7 @@ def main():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--sections", default="all",
                     help="other configurations reported beside the headline: all, none, or a comma list of "
-                         "scan_agg,groupby,join_large,batch,serving,tpch")
+                         "scan_agg,groupby,join_large,batch,serving,tpch,ceb")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))

@@ -343,10 +343,12 @@ def ilike_pattern(raw: str) -> tuple[int, str]:
     return 5, p
 
 
-def q10a(engine, t: CebTables, ids, infos, name, kinds, roles, max_rows: int = 1 << 16) -> list:
+def q10a(engine, t: CebTables, ids, infos, name, kinds, roles, max_rows: int = 1 << 16, raw: bool = False):
     """CEB query 10a (run_q10a, bespoke_ceb/query_q10a.cpp:334-1130) on the
     GPU: rows (name, info, has_year, min_year, max_year), in no particular
-    order (the reference's are in its aggregation order)."""
+    order (the reference's are in its aggregation order).  raw=True returns
+    the row count instead (the rows stay as codes: no strings are built)."""
+    max_rows = max(max_rows, getattr(q10a, "room", 0))
     type_ids = {i for i in (stoi(v) for v in ids if v not in NULL_WORDS) if i is not None}
     if not type_ids:
         return []
@@ -406,6 +408,9 @@ def q10a(engine, t: CebTables, ids, infos, name, kinds, roles, max_rows: int = 1
             continue
         engine.ctx.check(rc, "bo_ceb_q10a")
         break
+    q10a.room = max_rows
+    if raw:
+        return int(n.value)
     out = []
     for r in rows[:n.value]:
         out.append((nm.dictionary[r.name_code], dense_vals[r.info_dense], bool(r.has_year),
@@ -415,10 +420,12 @@ def q10a(engine, t: CebTables, ids, infos, name, kinds, roles, max_rows: int = 1
 
 
 # ------------------------------------------------------------------- 3b ----
-def q3b(engine, t: CebTables, title: str, pcode: str, company: str, kinds, roles, max_rows: int = 1 << 16) -> list:
+def q3b(engine, t: CebTables, title: str, pcode: str, company: str, kinds, roles, max_rows: int = 1 << 16,
+        raw: bool = False):
     """CEB query 3b (run_q3b, bespoke_ceb/query_q3b.cpp:728-1420) on the GPU:
     rows (title, name, company, count) in the reference's order (count desc,
-    then the three strings)."""
+    then the three strings).  raw=True returns the row count instead."""
+    max_rows = max(max_rows, getattr(q3b, "room", 0))
     kt, rt = t.col("kind_type", "kind"), t.col("role_type", "role")
     # the IN lists against the column's own strings (query_q3b.cpp:208-254)
     kf = string_filter(set(kt.dictionary or []), kinds)
@@ -464,5 +471,8 @@ def q3b(engine, t: CebTables, title: str, pcode: str, company: str, kinds, roles
             continue
         engine.ctx.check(rc, "bo_ceb_q3b")
         break
+    q3b.room = max_rows
+    if raw:
+        return int(n.value)
     return [(tt.dictionary[r.title_code], nm.dictionary[r.name_code], cn.dictionary[r.company_code], int(r.count))
             for r in rows[:n.value]]
