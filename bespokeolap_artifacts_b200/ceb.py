@@ -14,7 +14,7 @@ from __future__ import annotations
 
 import ctypes as C
 import re
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 from pathlib import Path
 
 import numpy as np
@@ -275,7 +275,7 @@ def sort_table(engine, t: CebTables, table: str, primary: str, secondary: str | 
             nl = torch.empty_like(col.is_null)
             engine.ctx.call("bo_ceb_gather_u8", C.c_void_p(col.is_null.data_ptr()), C.c_void_p(perm.data_ptr()), n,
                             C.c_void_p(nl.data_ptr()))
-        d[name] = Column(v, nl, col.dictionary, col.max_value, col.rows)
+        d[name] = replace(col, values=v, is_null=nl)  # the device dictionary stays with the codes
     engine.synchronize()
 
 

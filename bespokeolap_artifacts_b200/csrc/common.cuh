@@ -29,6 +29,15 @@ enum : uint32_t {
   kErrSumOverflow = 1u << 5,    // a 128-bit total does not fit the 64-bit result field
 };
 
+// ------------------------------------------- programmatic dependent launch --
+// A kernel launched with the programmatic-serialization attribute may start
+// while the kernel before it on the stream still runs.  pdl_wait() blocks
+// until that kernel has completed and its writes are visible (a no-op for a
+// kernel launched the ordinary way); pdl_launch_dependents() lets the next
+// such kernel be scheduled once every block of this one has issued it.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 // ---------------------------------------------------------------- loads ----
 // Streaming 128-bit loads: read-only, not allocated in L1 (each byte of a fact
 // column is touched exactly once per scan).

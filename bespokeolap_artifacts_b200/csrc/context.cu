@@ -28,6 +28,7 @@ int region(bo_ctx* ctx, const char* name, size_t bytes, void** out) {
   auto& r = ctx->regions[name];
   if (r.bytes < bytes) {
     if (r.ptr) {
+      drain_host_work(ctx);  // queued host work may still enqueue kernels that read the region
       cudaStreamSynchronize(ctx->stream);
       cudaFree(r.ptr);
       r.ptr = nullptr;
@@ -66,6 +67,7 @@ int after_launch(bo_ctx* ctx, const char* what) {
 }
 
 int consume_device_errors(bo_ctx* ctx, uint32_t* bits_out) {
+  if (int rc = drain_host_work(ctx)) return rc;
   BO_CUDA(ctx, cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                ctx->stream));
   BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -149,6 +151,8 @@ int bo_create(bo_ctx** out, int device) {
   if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&ctx->d_err, sizeof(uint32_t)) != cudaSuccess ||
       cudaHostAlloc(&ctx->h_err, sizeof(uint32_t), cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_word), sizeof(unsigned long long), cudaHostAllocDefault) !=
+          cudaSuccess ||
       cudaMemset(ctx->d_err, 0, sizeof(uint32_t)) != cudaSuccess) {
     bo_destroy(ctx);
     return BO_ERR_CUDA;
@@ -161,11 +165,13 @@ int bo_create(bo_ctx** out, int device) {
 void bo_destroy(bo_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  bo::destroy_host_work(ctx);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& kv : ctx->regions)
     if (kv.second.ptr) cudaFree(kv.second.ptr);
   if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->h_err) cudaFreeHost(ctx->h_err);
+  if (ctx->h_word) cudaFreeHost(ctx->h_word);
   if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   if (ctx->copy_stream) {
     cudaStreamSynchronize(ctx->copy_stream);
@@ -191,6 +197,7 @@ void* bo_get_stream(const bo_ctx* ctx) { return ctx ? static_cast<void*>(ctx->st
 
 int bo_synchronize(bo_ctx* ctx) {
   BO_CHECK_CTX(ctx);
+  if (int rc = bo::drain_host_work(ctx)) return rc;
   BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return BO_OK;
 }

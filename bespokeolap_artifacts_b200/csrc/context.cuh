@@ -12,6 +12,10 @@
 
 #include "bespoke_gpu.h"
 
+namespace bo {
+struct GatherState;  // host threads and buffers of the streamed join's host-gather form (csrc/join.cu)
+}
+
 struct bo_ctx {
   int device = 0;
   int num_sms = 0;
@@ -26,6 +30,7 @@ struct bo_ctx {
   // grown on demand; kernels that accumulate into them leave them zeroed.
   uint32_t* d_err = nullptr;
   uint32_t* h_err = nullptr;  // pinned mirror for the single end-of-call read
+  unsigned long long* h_word = nullptr;  // pinned word for a device count read back mid-call
   struct Region {
     void* ptr = nullptr;
     size_t bytes = 0;
@@ -39,6 +44,10 @@ struct bo_ctx {
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> events;
   int stream_set = 0;  // buffer set of the streamed join's next query
+  // Host threads that gather the payload of matching probe rows in the
+  // streamed join (-1: chosen from the machine; 0: payload read in place).
+  int gather_threads = -1;
+  bo::GatherState* gather = nullptr;
 };
 
 namespace bo {
@@ -62,6 +71,12 @@ int cuda_fail(bo_ctx* ctx, cudaError_t e, const char* what);
 int region(bo_ctx* ctx, const char* name, size_t bytes, void** out);
 // Pinned host staging buffer of at least `bytes`.
 int host_stage(bo_ctx* ctx, size_t bytes, void** out);
+// Waits for the work the context's host threads have queued (the streamed
+// join's gathers) and for the device work they enqueued; reports their first
+// failure.  Must not be called from those threads.
+int drain_host_work(bo_ctx* ctx);
+// Stops the context's host threads (after draining) and frees their buffers.
+void destroy_host_work(bo_ctx* ctx);
 // Records one kernel launch and checks the launch status.
 int after_launch(bo_ctx* ctx, const char* what);
 // Reads and clears the device error word (call only after a stream sync).
@@ -80,12 +95,19 @@ T* carve(char*& p, size_t count) {
 }
 
 // Stable LSD radix sort of (key, value) pairs by bits [begin_bit, end_bit)
-// (csrc/radix_sort.cu); n_dev, if given, is the actual count (<= n) on the device.
+// (csrc/radix_sort.cu); n_dev, if given, is the actual count (<= n) on the
+// device.  Without n_dev, up to 65536 pairs are sorted by one thread-block
+// cluster in distributed shared memory (one launch).
 int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsigned long long* tmp_keys,
                      uint32_t* tmp_vals, int64_t n, int begin_bit, int end_bit, const unsigned long long* n_dev);
 
-// The k smallest keys (ascending) of (keys, vals) into the front of
-// (cand_keys, cand_vals): radix select + small sort (csrc/radix_sort.cu).
+// Copies the device count *n_dev (clamped to n_max) to the host; synchronises
+// the stream.  Lets a caller sort an exact number of pairs.
+int read_device_count(bo_ctx* ctx, const unsigned long long* n_dev, int64_t n_max, int64_t* n);
+
+// The k smallest of unique keys (ascending, k <= 64) of (keys, vals) into the
+// front of (cand_keys, cand_vals): one cooperative radix-select launch
+// (csrc/radix_sort.cu); tmp_keys / tmp_vals are not used.
 // lo_bits / hi_max_dev (optional): keys are (hi << lo_bits) | lo with all hi
 // equal above the highest bit of *hi_max_dev; the select digit sits there.
 int radix_topk_pairs(bo_ctx* ctx, const unsigned long long* keys, const uint32_t* vals, int64_t n_max,

@@ -22,10 +22,14 @@
 //                                  writes the result.
 // Build-side keys are read densely with the filter columns (one streaming pass).
 #include <algorithm>
+#include <string>
+#include <thread>
+#include <utility>
 
 #include "common.cuh"
 #include "rows.cuh"
 #include "context.cuh"
+#include "host_threads.cuh"
 #include "mlp.cuh"
 
 namespace bo {
@@ -101,6 +105,7 @@ __device__ __forceinline__ int32_t presize_log2(const float* pred, int32_t host_
 
 __global__ void join_init_kernel(unsigned long long* slots, uint32_t* bloom, JoinMeta* meta, const float* pred,
                                  int32_t host_log2, int32_t max_log2) {
+  pdl_launch_dependents();  // the build kernel may be scheduled now (it waits before touching the table)
   const int32_t cl = presize_log2(pred, host_log2, max_log2);
   const uint64_t cap = 1ull << cl;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -132,6 +137,7 @@ __global__ void __launch_bounds__(kPredThreads) join_learned_init_kernel(const f
                                                                          JoinMeta* meta, int32_t max_log2,
                                                                          float* pred_out) {
   __shared__ float y[kMaxO];
+  pdl_launch_dependents();  // the build kernel may be scheduled now (it waits before touching the table)
   mlp_predict_block(params, xv, F, O, y);
   const float c = expm1f(y[0]);
   const float pred = c > 0.0f ? c : 0.0f;
@@ -169,10 +175,12 @@ constexpr int kBuildRowsPerThread = 16;
 __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_cols b, int32_t date_lt, uint32_t seg,
                                                                  unsigned long long* slots, uint32_t* bloom,
                                                                  JoinMeta* meta, uint64_t probe_limit) {
-  // Read-only for this kernel (written by the init kernel): the L1-cached path
-  // avoids every warp hitting the same L2 sector.
-  const int32_t cl = __ldg(&meta->cap_log2);
-  const uint64_t mask = (1ull << cl) - 1;
+  // Launched right behind the init kernel (programmatic dependent launch):
+  // each thread loads and filters its first rows, then waits for the init
+  // kernel to finish before it reads the table's size or touches the table.
+  pdl_launch_dependents();
+  bool waited = false;
+  uint64_t mask = 0;
   uint32_t qual = 0, newkeys = 0;
   bool full = false;
   __shared__ uint32_t build_q[kBuildBlock / 32][32 * kBuildRowsPerThread];
@@ -213,6 +221,13 @@ __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_c
         }
       }
     }
+    if (!waited) {
+      pdl_wait();
+      waited = true;
+      // Read-only for this kernel (written by the init kernel): the L1-cached
+      // path avoids every warp hitting the same L2 sector.
+      mask = (1ull << __ldg(&meta->cap_log2)) - 1;
+    }
     qual += __popc(q);
     // Compact the qualifying keys of the whole warp into its queue so the CAS
     // insertions spread over all 32 lanes.
@@ -226,6 +241,7 @@ __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_c
     for (uint32_t i = lane; i < total; i += 32) join_insert(slots, bloom, mask, (int32_t)bq[i], newkeys, full, probe_limit);
     __syncwarp();
   }
+  if (!waited) pdl_wait();  // threads without rows: before the counters below
   // Block-level totals, then one atomic per counter per block.
   __shared__ uint32_t part[3][kBuildBlock / 32];
   const uint32_t wq = warp_sum_u32(qual), wn = warp_sum_u32(newkeys);
@@ -271,16 +287,87 @@ constexpr int kRowsPerWarpStep = 32 * kRowsPerLane;
 constexpr int kQueue = 32 * kRowsPerLane;
 constexpr int kJoinResolveR = 2;  // candidates per lane per resolve round
 
+// Match list of the host-gather form: instead of reading price / discount
+// over PCIe, the probe appends each matching row (relative to the launch's
+// first row) to pinned host memory and its build-side multiplicity to device
+// memory; the host gathers the payload of exactly those rows.
+struct EmitOut {
+  uint32_t* rows = nullptr;        // device view of mapped host memory
+  uint32_t* mult = nullptr;        // device memory, same index as rows
+  uint32_t* counter = nullptr;     // device: entries appended (zeroed again by the last block)
+  uint32_t* count_host = nullptr;  // device view of mapped host memory: the launch's entry count
+  uint32_t capacity = 0;
+};
+
+// probe_resolve's lookups, then warp-aggregated appends of the matches (one
+// atomic per warp and round) in place of the payload loads.
+template <int R>
+__device__ __forceinline__ void probe_emit(const int32_t* qf, const uint16_t* qo, uint32_t total, int64_t base,
+                                           const unsigned long long* slots, uint64_t mask, uint64_t limit,
+                                           const EmitOut& eo, ProbeAcc& acc) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (uint32_t i0 = 0; i0 < total; i0 += 32 * R) {
+    int32_t key[R];
+    int64_t row[R];
+    uint64_t idx[R];
+    unsigned long long v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const uint32_t i = i0 + r * 32 + lane;
+      const bool ok = i < total;
+      key[r] = ok ? qf[i] : 0;
+      row[r] = ok ? base + qo[i] : 0;
+      idx[r] = hash32((uint32_t)key[r]) & mask;
+      v[r] = ok ? __ldg(slots + idx[r]) : kEmptySlot;
+    }
+    unsigned long long mult[R];
+    uint32_t bal[R], n = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      mult[r] = 0;
+      if (v[r] != kEmptySlot) {
+        if ((uint32_t)(v[r] >> 32) == (uint32_t)key[r])
+          mult[r] = v[r] & 0xffffffffull;
+        else
+          mult[r] = probe_slow<false>(slots, mask, idx[r], (uint32_t)key[r], limit);
+      }
+      bal[r] = __ballot_sync(0xffffffffu, mult[r] != 0);
+      n += __popc(bal[r]);
+    }
+    if (n == 0) continue;  // warp-uniform
+    uint32_t pos = 0;
+    if (lane == 0) pos = atomicAdd(eo.counter, n);
+    pos = __shfl_sync(0xffffffffu, pos, 0);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (mult[r]) {
+        const uint32_t at = pos + __popc(bal[r] & lt);
+        if (at < eo.capacity) {
+          eo.rows[at] = (uint32_t)row[r];
+          eo.mult[at] = (uint32_t)mult[r];
+          acc.cnt += mult[r];
+        } else {
+          acc.bad |= kErrOutputOverflow;
+        }
+      }
+      pos += __popc(bal[r]);
+    }
+  }
+}
+
+template <bool kEmit>
 __global__ void __launch_bounds__(kJoinBlock, 2) join_probe_kernel(bo_join_probe_cols p,
                                                                 const unsigned long long* slots,
                                                                 const uint32_t* bloom_g, JoinMeta* meta,
                                                                 bo_join_result* out, int32_t mode, uint64_t probe_limit,
-                                                                uint32_t* err) {
+                                                                uint32_t* err, EmitOut eo) {
   extern __shared__ __align__(128) uint32_t bloom_s[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ unsigned __int128 red[kJoinBlock + 32];
   __shared__ int32_t q_fk[kProbeWarps][kQueue];
   __shared__ uint16_t q_off[kProbeWarps][kQueue];
+  pdl_wait();  // launched behind the build kernel: its table and Bloom filter must be complete
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     mbar_arrive_expect_tx(&bar, kBloomBytes);
@@ -342,7 +429,10 @@ __global__ void __launch_bounds__(kJoinBlock, 2) join_probe_kernel(bo_join_probe
       }
     }
     __syncwarp();
-    probe_resolve<kJoinResolveR, false>(qf, qo, total, base, slots, mask, probe_limit, p.price, p.discount, acc);
+    if constexpr (kEmit)
+      probe_emit<kJoinResolveR>(qf, qo, total, base, slots, mask, probe_limit, eo, acc);
+    else
+      probe_resolve<kJoinResolveR, false>(qf, qo, total, base, slots, mask, probe_limit, p.price, p.discount, acc);
     __syncwarp();
   }
   if (!use_bloom) {
@@ -379,8 +469,52 @@ __global__ void __launch_bounds__(kJoinBlock, 2) join_probe_kernel(bo_join_probe
 #pragma unroll
       for (int i = 0; i < 6; ++i) meta->acc[i] = 0;
       meta->done = 0;
+      if constexpr (kEmit) {
+        const uint32_t entries = atomicExch(eo.counter, 0u);
+        *reinterpret_cast<volatile uint32_t*>(eo.count_host) = entries < eo.capacity ? entries : eo.capacity;
+      }
       if (fbad) raise_error(err, fbad);
     }
+  }
+}
+
+// Host-gather form, second half: the payload of a probe launch's matches,
+// gathered on the host into (price, discount) records and copied in, summed
+// with the multiplicities the probe kept; the last block adds the totals to
+// that launch's partial result (whose match count the probe wrote).
+struct GatherAcc {
+  unsigned long long acc[4];  // 128-bit totals: sum T, sum rr
+  uint32_t done;
+  uint32_t pad;
+};
+
+constexpr int kGatherBlock = 256;
+
+__global__ void __launch_bounds__(kGatherBlock) join_gather_sum_kernel(const longlong2* __restrict__ rec,
+                                                                       const uint32_t* __restrict__ mult, int64_t n,
+                                                                       GatherAcc* ga, bo_join_result* part,
+                                                                       uint32_t* err) {
+  __shared__ unsigned __int128 red[kGatherBlock + 32];
+  ProbeAcc a;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const longlong2 r = __ldcs(rec + i);
+    accumulate_match((uint64_t)r.x, (uint64_t)r.y, __ldcs(mult + i), a);
+  }
+  if (a.bad) raise_error(err, a.bad);
+  const unsigned __int128 bt = block_sum_u128(a.tsum, red);
+  const unsigned __int128 br = block_sum_u128(a.rsum, red);
+  if (threadIdx.x == 0) {
+    if (bt) atomic_add_i128(&ga->acc[0], (__int128)bt);
+    if (br) atomic_add_i128(&ga->acc[2], (__int128)br);
+  }
+  if (last_block(&ga->done) && threadIdx.x == 0) {
+    const __int128 t = load_i128(&ga->acc[0]), rr = load_i128(&ga->acc[2]);
+    part->sum_trunc = to_bo_i128(t);
+    part->sum_exact = to_bo_i128(t * 100 + rr);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) ga->acc[i] = 0;
+    ga->done = 0;
   }
 }
 
@@ -444,19 +578,46 @@ int grid_for(bo_ctx* ctx, const void* k, int block, size_t smem, int64_t work_it
   return (int)std::max<int64_t>(g, 1);
 }
 
+// Launches a kernel that may start while the previous kernel on the stream
+// still runs (programmatic dependent launch); the kernel itself waits
+// (pdl_wait) before it reads that kernel's output.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dependent(void (*k)(KArgs...), int grid, int block, size_t smem, cudaStream_t st,
+                             Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
+
+// Probe launch; a match list (eo.rows set) selects the host-gather form.
 int launch_probe(bo_ctx* ctx, const bo_join_probe_cols& p, const JoinWs& ws, bo_join_result* out, int32_t mode,
-                 uint64_t probe_limit) {
-  const void* k = reinterpret_cast<const void*>(&join_probe_kernel);
-  static bool ready = false;
-  if (!ready) {
+                 uint64_t probe_limit, bool dependent = false, const EmitOut& eo = EmitOut()) {
+  const bool emit = eo.rows != nullptr;
+  auto* kfn = emit ? &join_probe_kernel<true> : &join_probe_kernel<false>;
+  const void* k = reinterpret_cast<const void*>(kfn);
+  static bool ready[2] = {false, false};
+  if (!ready[emit]) {
     BO_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBloomBytes));
-    ready = true;
+    ready[emit] = true;
   }
   // Enough blocks to fill the GPU, but each thread should see a few 8-row
   // chunks so the per-block Bloom-filter copy is amortised.
   const int grid = grid_for(ctx, k, kJoinBlock, kBloomBytes, (p.n_rows + kRowsPerLane - 1) / kRowsPerLane);
-  join_probe_kernel<<<grid, kJoinBlock, kBloomBytes, ctx->stream>>>(p, ws.slots, ws.bloom, ws.meta, out, mode,
-                                                                     probe_limit, ctx->d_err);
+  if (dependent)
+    BO_CUDA(ctx, launch_dependent(kfn, grid, kJoinBlock, kBloomBytes, ctx->stream, p,
+                                  (const unsigned long long*)ws.slots, (const uint32_t*)ws.bloom, ws.meta, out, mode,
+                                  probe_limit, ctx->d_err, eo));
+  else
+    kfn<<<grid, kJoinBlock, kBloomBytes, ctx->stream>>>(p, ws.slots, ws.bloom, ws.meta, out, mode, probe_limit,
+                                                        ctx->d_err, eo);
   return after_launch(ctx, "join_probe_kernel");
 }
 
@@ -472,10 +633,10 @@ int join_run(bo_ctx* ctx, const bo_join_build_cols& b, const bo_join_probe_cols&
   const int gb = grid_for(ctx, kb, kBuildBlock, 0, (b.n_rows + kBuildRowsPerThread - 1) / kBuildRowsPerThread);
   // Exact-size tables (mode 0) probe without a bound; presized ones fail fast.
   const uint64_t limit = mode == 0 ? ~0ull : kPresizedProbeLimit;
-  join_build_kernel<<<gb, kBuildBlock, 0, ctx->stream>>>(b, prm.date_lt, (uint32_t)prm.segment_eq, ws.slots,
-                                                          ws.bloom, ws.meta, limit);
+  BO_CUDA(ctx, launch_dependent(&join_build_kernel, gb, kBuildBlock, 0, ctx->stream, b, prm.date_lt,
+                                (uint32_t)prm.segment_eq, ws.slots, ws.bloom, ws.meta, limit));
   if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
-  return launch_probe(ctx, p, ws, out, mode, limit);
+  return launch_probe(ctx, p, ws, out, mode, limit, true);
 }
 
 int finish_join(bo_ctx* ctx, bo_join_result* host, const bo_join_result* dev) {
@@ -671,7 +832,281 @@ int stream_compute(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join_prob
   return BO_OK;
 }
 
+// ---------------------------------------- streamed join, host gather ---
+// Of a probe row's 16 payload bytes (price, discount) only the matching rows'
+// are needed, a few percent.  Read in place over PCIe each match costs two
+// small read requests, and the link serves those about one round trip at a
+// time (0.6 ms for 240K matches on B200 behind PCIe 5).  In this form the
+// probe lists the matching rows in pinned host memory instead; host threads
+// gather those rows' payload into contiguous (price, discount) records while
+// later chunks are still being copied and probed, and one bulk copy per chunk
+// brings the records to a summing kernel.  The gather's device work runs on
+// its own stream, enqueued by the context's HostQueue thread, so the caller
+// never waits for it; bo_synchronize (or any synchronous call) drains it.
+constexpr int kGatherRing = 4;  // staging buffers of gathered records in flight
+
 }  // namespace
+
+struct GatherSet {
+  uint32_t* rows_h = nullptr;       // pinned, mapped: chunk c's match rows from c * kStreamChunkRows
+  uint32_t* rows_d = nullptr;       // device view of rows_h
+  uint32_t* count_h = nullptr;      // pinned, mapped: entries per chunk
+  uint32_t* count_d = nullptr;      // device view of count_h
+  uint32_t* mult = nullptr;         // device: multiplicities, laid out as rows_h
+  uint32_t* counter = nullptr;      // device: per-chunk append counters
+  bo_join_result* res_h = nullptr;  // pinned result slot of the synchronous form
+  std::vector<cudaEvent_t> probed;  // chunk c's probe has finished
+  uint64_t ticket = 0;              // queue task of the set's latest query
+};
+
+struct GatherState {
+  GatherState(int device, int threads) : pool(threads), queue([device] { cudaSetDevice(device); }) {}
+  HostPool pool;    // declared before the queue: the queue's tasks use it
+  HostQueue queue;
+  cudaStream_t stream = nullptr;
+  GatherSet set[2];
+  int64_t rows_cap = 0, chunk_cap = 0;  // per set
+  longlong2* rec_h[kGatherRing] = {};   // pinned staging, kStreamChunkRows records each
+  cudaEvent_t rec_ev[kGatherRing] = {};  // the copy out of rec_h[i] has finished
+  bool rec_busy[kGatherRing] = {};
+  int next_rec = 0;
+  longlong2* rec_d = nullptr;  // kGatherRing x kStreamChunkRows records
+  GatherAcc* acc = nullptr;
+};
+
+namespace {
+
+int auto_gather_threads() {
+  const unsigned hc = std::thread::hardware_concurrency();
+  return (int)std::min(8u, std::max(1u, hc / 2));
+}
+
+void free_gather_sets(GatherState* g) {
+  for (GatherSet& st : g->set) {
+    if (st.rows_h) cudaFreeHost(st.rows_h);
+    if (st.count_h) cudaFreeHost(st.count_h);
+    if (st.res_h) cudaFreeHost(st.res_h);
+    if (st.mult) cudaFree(st.mult);
+    if (st.counter) cudaFree(st.counter);
+    for (cudaEvent_t e : st.probed) cudaEventDestroy(e);
+    st = GatherSet();
+  }
+  g->rows_cap = g->chunk_cap = 0;
+}
+
+void free_gather(GatherState* g) {
+  free_gather_sets(g);
+  for (int i = 0; i < kGatherRing; ++i) {
+    if (g->rec_h[i]) cudaFreeHost(g->rec_h[i]);
+    if (g->rec_ev[i]) cudaEventDestroy(g->rec_ev[i]);
+  }
+  if (g->rec_d) cudaFree(g->rec_d);
+  if (g->acc) cudaFree(g->acc);
+  if (g->stream) cudaStreamDestroy(g->stream);
+}
+
+// The context's gather state (created on first use), or null in *out when the
+// context reads the payload in place (no gather threads).
+int gather_state(bo_ctx* ctx, GatherState** out) {
+  *out = nullptr;
+  const int threads = ctx->gather_threads < 0 ? auto_gather_threads() : ctx->gather_threads;
+  if (threads == 0) return BO_OK;
+  if (!ctx->gather) {
+    auto* g = new GatherState(ctx->device, threads);
+    auto init = [&]() -> int {
+      BO_CUDA(ctx, cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+      for (int i = 0; i < kGatherRing; ++i) {
+        BO_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&g->rec_h[i]), sizeof(longlong2) * kStreamChunkRows,
+                                   cudaHostAllocDefault));
+        BO_CUDA(ctx, cudaEventCreateWithFlags(&g->rec_ev[i], cudaEventDisableTiming));
+      }
+      BO_CUDA(ctx, cudaMalloc(&g->rec_d, sizeof(longlong2) * kStreamChunkRows * kGatherRing));
+      BO_CUDA(ctx, cudaMalloc(&g->acc, sizeof(GatherAcc)));
+      BO_CUDA(ctx, cudaMemset(g->acc, 0, sizeof(GatherAcc)));
+      return BO_OK;
+    };
+    if (int rc = init()) {
+      free_gather(g);
+      delete g;
+      return rc;
+    }
+    ctx->gather = g;
+  }
+  *out = ctx->gather;
+  return BO_OK;
+}
+
+// Per-set buffers for `np` probe rows in `chunks` chunks; growing them first
+// drains every queued gather (their tasks hold the old buffers).
+int gather_reserve(bo_ctx* ctx, GatherState* g, int64_t np, int64_t chunks) {
+  const int64_t rows = std::max<int64_t>(np, 1);
+  if (rows <= g->rows_cap && chunks <= g->chunk_cap) return BO_OK;
+  if (int rc = drain_host_work(ctx)) return rc;
+  free_gather_sets(g);
+  for (GatherSet& st : g->set) {
+    BO_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&st.rows_h), sizeof(uint32_t) * rows, cudaHostAllocMapped));
+    BO_CUDA(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&st.rows_d), st.rows_h, 0));
+    BO_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&st.count_h), sizeof(uint32_t) * chunks, cudaHostAllocMapped));
+    BO_CUDA(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&st.count_d), st.count_h, 0));
+    BO_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&st.res_h), sizeof(bo_join_result), cudaHostAllocDefault));
+    BO_CUDA(ctx, cudaMalloc(&st.mult, sizeof(uint32_t) * rows));
+    BO_CUDA(ctx, cudaMalloc(&st.counter, sizeof(uint32_t) * chunks));
+    BO_CUDA(ctx, cudaMemset(st.counter, 0, sizeof(uint32_t) * chunks));
+    st.probed.resize(chunks);
+    for (cudaEvent_t& e : st.probed) BO_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  g->rows_cap = rows;
+  g->chunk_cap = chunks;
+  return BO_OK;
+}
+
+// (price, discount) of the listed rows [b, e) into records; the rows of one
+// warp's appends are close together, so prefetching a few entries ahead keeps
+// several cache misses in flight per thread.
+void gather_rows(const uint32_t* rows, const int64_t* price, const int64_t* disc, longlong2* out, int64_t b,
+                 int64_t e) {
+  constexpr int64_t kAhead = 16;
+  for (int64_t i = b; i < e; ++i) {
+    if (i + kAhead < e) {
+      const uint32_t ra = rows[i + kAhead];
+      __builtin_prefetch(price + ra);
+      __builtin_prefetch(disc + ra);
+    }
+    const uint32_t r = rows[i];
+    out[i].x = price[r];
+    out[i].y = disc[r];
+  }
+}
+
+// init + build + chunked listing probe on the compute stream, then the
+// gather task: per chunk, wait for its probe, gather, copy the records in and
+// sum them on the gather stream; combine, and copy the result to `dst`
+// (pinned host memory).
+int stream_compute_gather(bo_ctx* ctx, GatherState* g, const bo_join_build_cols* bh, const bo_join_probe_cols* ph,
+                          const bo_join_params* prm, const float* pred, int32_t host_log2, const JoinWs& ws,
+                          const StreamIn& in, const StreamSet& s, int set, bo_join_result* dst) {
+  cudaEvent_t* ev = ctx->events.data();
+  GatherSet& gs = g->set[set];
+  BO_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ev[2], 0));
+  const int64_t nb = bh->n_rows, np = ph->n_rows;
+  const int32_t mode = pred ? 1 : 0;
+  const uint64_t limit = mode == 0 ? ~0ull : kPresizedProbeLimit;
+  const bo_join_build_cols b = {in.key, s.date, s.seg, nb};
+  const void* ki = reinterpret_cast<const void*>(&join_init_kernel);
+  join_init_kernel<<<grid_for(ctx, ki, 256, 0, (int64_t)1 << std::min(ws.max_log2, 24)), 256, 0, ctx->stream>>>(
+      ws.slots, ws.bloom, ws.meta, pred, host_log2, ws.max_log2);
+  int rc = after_launch(ctx, "join_init_kernel");
+  if (rc) return rc;
+  const void* kb = reinterpret_cast<const void*>(&join_build_kernel);
+  join_build_kernel<<<grid_for(ctx, kb, kBuildBlock, 0, (nb + kBuildRowsPerThread - 1) / kBuildRowsPerThread),
+                      kBuildBlock, 0, ctx->stream>>>(b, prm->date_lt, (uint32_t)prm->segment_eq, ws.slots, ws.bloom,
+                                                     ws.meta, limit);
+  if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
+  for (int64_t c = 0; c < in.chunks; ++c) {
+    const int64_t lo = c * kStreamChunkRows, n = std::max<int64_t>(0, std::min(np - lo, kStreamChunkRows));
+    BO_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ev[3 + c], 0));
+    const bo_join_probe_cols pc = {s.fk + lo, nullptr, nullptr, n};
+    EmitOut eo;
+    eo.rows = gs.rows_d + lo;
+    eo.mult = gs.mult + lo;
+    eo.counter = gs.counter + c;
+    eo.count_host = gs.count_d + c;
+    eo.capacity = (uint32_t)std::max<int64_t>(n, 0);
+    if ((rc = launch_probe(ctx, pc, ws, s.part + c, mode, limit, false, eo))) return rc;
+    BO_CUDA(ctx, cudaEventRecord(gs.probed[c], ctx->stream));
+  }
+  // Everything the task needs, by value: the set's buffers stay untouched
+  // until the task has recorded the set's "done" event (the next query on the
+  // set waits for the task's ticket first).
+  const int64_t chunks = in.chunks;
+  const std::vector<cudaEvent_t> probed(gs.probed.begin(), gs.probed.begin() + chunks);
+  const uint32_t* rows_h = gs.rows_h;
+  const volatile uint32_t* count_h = gs.count_h;
+  const uint32_t* mult = gs.mult;
+  const int64_t* price_h = ph->price;
+  const int64_t* disc_h = ph->discount;
+  bo_join_result* part = s.part;
+  bo_join_result* combined = s.combined;
+  const cudaEvent_t done_ev = ev[set];
+  uint32_t* d_err = ctx->d_err;
+  std::atomic<int64_t>* launches = &ctx->launches;
+  const int max_grid = 2 * std::max(ctx->num_sms, 1);
+  gs.ticket = g->queue.post([=](std::string& msg) -> int {
+    GatherState& G = *g;
+    auto fail = [&](cudaError_t e, const char* what) {
+      msg = std::string(what) + ": " + cudaGetErrorString(e);
+      return e == cudaErrorMemoryAllocation ? BO_ERR_OOM : BO_ERR_CUDA;
+    };
+    auto body = [&]() -> int {
+      cudaError_t e;
+      for (int64_t c = 0; c < chunks; ++c) {
+        if ((e = cudaEventSynchronize(probed[c])) != cudaSuccess) return fail(e, "waiting for a probe chunk");
+        const uint32_t n = count_h[c];
+        if (n == 0) continue;
+        if (n > (uint32_t)kStreamChunkRows) {
+          msg = "match list longer than its chunk";
+          return BO_ERR_DATA;
+        }
+        const int slot = G.next_rec;
+        G.next_rec = (slot + 1) % kGatherRing;
+        if (G.rec_busy[slot] && (e = cudaEventSynchronize(G.rec_ev[slot])) != cudaSuccess)
+          return fail(e, "waiting for a staging buffer");
+        const int64_t lo = c * kStreamChunkRows;
+        const uint32_t* rows = rows_h + lo;
+        const int64_t* pr = price_h + lo;
+        const int64_t* dc = disc_h + lo;
+        longlong2* out = G.rec_h[slot];
+        G.pool.parallel_for((int64_t)n, [&](int64_t b0, int64_t e0) { gather_rows(rows, pr, dc, out, b0, e0); });
+        longlong2* rec = G.rec_d + (size_t)slot * kStreamChunkRows;
+        if ((e = cudaMemcpyAsync(rec, out, sizeof(longlong2) * n, cudaMemcpyHostToDevice, G.stream)) != cudaSuccess)
+          return fail(e, "copying gathered records");
+        if ((e = cudaEventRecord(G.rec_ev[slot], G.stream)) != cudaSuccess) return fail(e, "recording a copy");
+        G.rec_busy[slot] = true;
+        const int grid = (int)std::min<int64_t>(max_grid, ((int64_t)n + 4 * kGatherBlock - 1) / (4 * kGatherBlock));
+        join_gather_sum_kernel<<<grid, kGatherBlock, 0, G.stream>>>(rec, mult + lo, (int64_t)n, G.acc, part + c,
+                                                                     d_err);
+        if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "join_gather_sum_kernel");
+        launches->fetch_add(1, std::memory_order_relaxed);
+      }
+      join_combine_kernel<<<1, 32, 0, G.stream>>>(part, chunks, combined);
+      if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "join_combine_kernel");
+      launches->fetch_add(1, std::memory_order_relaxed);
+      if ((e = cudaMemcpyAsync(dst, combined, sizeof(bo_join_result), cudaMemcpyDeviceToHost, G.stream)) !=
+          cudaSuccess)
+        return fail(e, "copying the result");
+      return 0;
+    };
+    const int rc2 = body();
+    // The set's buffers are free once the gather stream gets here, also after a failure.
+    const cudaError_t e = cudaEventRecord(done_ev, G.stream);
+    if (!rc2 && e != cudaSuccess) return fail(e, "recording the set's done event");
+    return rc2;
+  });
+  return BO_OK;
+}
+
+}  // namespace
+
+int drain_host_work(bo_ctx* ctx) {
+  GatherState* g = ctx ? ctx->gather : nullptr;
+  if (!g) return BO_OK;
+  std::string msg;
+  const int rc = g->queue.drain(&msg);
+  const cudaError_t e = g->stream ? cudaStreamSynchronize(g->stream) : cudaSuccess;
+  if (rc) return set_error(ctx, rc, "join_stream gather: %s", msg.c_str());
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "gather stream");
+  return BO_OK;
+}
+
+void destroy_host_work(bo_ctx* ctx) {
+  GatherState* g = ctx ? ctx->gather : nullptr;
+  if (!g) return;
+  drain_host_work(ctx);
+  free_gather(g);
+  delete g;  // joins the queue's thread, then the pool's
+  ctx->gather = nullptr;
+}
+
 }  // namespace bo
 
 using namespace bo;
@@ -732,10 +1167,10 @@ int bo_join_learned_device(bo_ctx* ctx, const bo_mlp* m, const float* features_h
   if ((rc = after_launch(ctx, "join_learned_init_kernel"))) return rc;
   const void* kb = reinterpret_cast<const void*>(&join_build_kernel);
   const int gb = grid_for(ctx, kb, kBuildBlock, 0, (b->n_rows + kBuildRowsPerThread - 1) / kBuildRowsPerThread);
-  join_build_kernel<<<gb, kBuildBlock, 0, ctx->stream>>>(*b, prm->date_lt, (uint32_t)prm->segment_eq, ws.slots,
-                                                          ws.bloom, ws.meta, kPresizedProbeLimit);
+  BO_CUDA(ctx, launch_dependent(&join_build_kernel, gb, kBuildBlock, 0, ctx->stream, *b, prm->date_lt,
+                                (uint32_t)prm->segment_eq, ws.slots, ws.bloom, ws.meta, (uint64_t)kPresizedProbeLimit));
   if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
-  return launch_probe(ctx, *p, ws, out_device, 1, kPresizedProbeLimit);
+  return launch_probe(ctx, *p, ws, out_device, 1, kPresizedProbeLimit, true);
 }
 
 int bo_join_learned(bo_ctx* ctx, const bo_mlp* m, const float* features_host, const bo_join_build_cols* b,
@@ -829,9 +1264,15 @@ int bo_join_stream_host(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join
   StreamIn in;
   int rc = stream_check(ctx, bh, ph, prm, &in);
   if (rc) return rc;
+  GatherState* g = nullptr;
+  if ((rc = gather_state(ctx, &g))) return rc;
   JoinWs ws;
   StreamSet s;
   const int set = ctx->stream_set ^= 1;
+  if (g) {  // the set's previous query must have handed its buffers back first
+    g->queue.wait_for(g->set[set].ticket);
+    if ((rc = gather_reserve(ctx, g, ph->n_rows, in.chunks))) return rc;
+  }
   if ((rc = join_workspace(ctx, bh->n_rows, &ws)) || (rc = stream_set(ctx, bh->n_rows, ph->n_rows, in.chunks, set, &s)) ||
       (rc = stream_events(ctx, in.chunks)) || (rc = stream_copies(ctx, bh, ph, in, s, set)))
     return rc;
@@ -849,11 +1290,17 @@ int bo_join_stream_host(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join
     BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     cl = std::min(ws.max_log2, std::max(kMinCapLog2, ceil_log2(std::max<uint64_t>(count, 1) * kPlainSlotsPerRow)));
   }
-  if ((rc = stream_compute(ctx, bh, ph, prm, pred_device, cl, ws, in, s, set))) return rc;
-  BO_CUDA(ctx, cudaMemcpyAsync(out_host, s.combined, sizeof(bo_join_result), cudaMemcpyDeviceToHost, ctx->stream));
+  if (g) {
+    if ((rc = stream_compute_gather(ctx, g, bh, ph, prm, pred_device, cl, ws, in, s, set, g->set[set].res_h)))
+      return rc;
+  } else {
+    if ((rc = stream_compute(ctx, bh, ph, prm, pred_device, cl, ws, in, s, set))) return rc;
+    BO_CUDA(ctx, cudaMemcpyAsync(out_host, s.combined, sizeof(bo_join_result), cudaMemcpyDeviceToHost, ctx->stream));
+  }
   uint32_t bits = 0;
-  if ((rc = consume_device_errors(ctx, &bits))) return rc;  // synchronises the stream
+  if ((rc = consume_device_errors(ctx, &bits))) return rc;  // drains the gather, synchronises the stream
   if ((rc = device_error_status(ctx, bits, "join_stream"))) return rc;
+  if (g) *out_host = *g->set[set].res_h;
   out_host->mode = pred_device ? 1 : 0;
   if (out_host->overflowed && pred_device) {  // the prediction was too low: rerun with the exact count
     if ((rc = bo_join_stream_host(ctx, bh, ph, prm, nullptr, out_host))) return rc;
@@ -874,15 +1321,38 @@ int bo_join_stream_host_async(bo_ctx* ctx, const bo_join_build_cols* bh, const b
   StreamIn in;
   int rc = stream_check(ctx, bh, ph, prm, &in);
   if (rc) return rc;
+  GatherState* g = nullptr;
+  if ((rc = gather_state(ctx, &g))) return rc;
   JoinWs ws;
   StreamSet s;
   const int set = ctx->stream_set ^= 1;
+  if (g) {  // the set's previous query must have handed its buffers back first
+    g->queue.wait_for(g->set[set].ticket);
+    if ((rc = gather_reserve(ctx, g, ph->n_rows, in.chunks))) return rc;
+  }
   if ((rc = join_workspace(ctx, bh->n_rows, &ws)) || (rc = stream_set(ctx, bh->n_rows, ph->n_rows, in.chunks, set, &s)) ||
-      (rc = stream_events(ctx, in.chunks)) || (rc = stream_copies(ctx, bh, ph, in, s, set)) ||
-      (rc = stream_compute(ctx, bh, ph, prm, pred_device, 0, ws, in, s, set)))
+      (rc = stream_events(ctx, in.chunks)) || (rc = stream_copies(ctx, bh, ph, in, s, set)))
     return rc;
+  if (g) return stream_compute_gather(ctx, g, bh, ph, prm, pred_device, 0, ws, in, s, set, out_pinned);
+  if ((rc = stream_compute(ctx, bh, ph, prm, pred_device, 0, ws, in, s, set))) return rc;
   BO_CUDA(ctx, cudaMemcpyAsync(out_pinned, s.combined, sizeof(bo_join_result), cudaMemcpyDeviceToHost, ctx->stream));
   return BO_OK;
+}
+
+int bo_set_host_threads(bo_ctx* ctx, int32_t threads) {
+  BO_CHECK_CTX(ctx);
+  if (threads > 256) return set_error(ctx, BO_ERR_INVALID, "set_host_threads: %d threads", threads);
+  const int t = threads < 0 ? -1 : threads;
+  if (t == ctx->gather_threads) return BO_OK;
+  if (int rc = drain_host_work(ctx)) return rc;
+  destroy_host_work(ctx);  // recreated with the new count by the next streamed join
+  ctx->gather_threads = t;
+  return BO_OK;
+}
+
+int bo_host_threads(const bo_ctx* ctx) {
+  if (!ctx) return 0;
+  return ctx->gather_threads < 0 ? auto_gather_threads() : ctx->gather_threads;
 }
 
 }  // extern "C"

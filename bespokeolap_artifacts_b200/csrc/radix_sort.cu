@@ -1,5 +1,6 @@
 // LSD onesweep radix sort of (uint64 key, uint32 value) pairs with decoupled
-// look-back (K5), and top-k as sort + truncate (K6).
+// look-back (K5), a one-launch cluster sort for up to 64K pairs, and top-k by
+// radix select (K6).
 //
 // Reference counterpart: the stable LSD counting sorts with 16-bit digits of
 // bespoke_tpch/query_q10.cpp:134-168, 285-316, 318-372 (descending order via
@@ -22,11 +23,15 @@
 //    stale words from earlier passes read as "not ready", so status arrays are
 //    never cleared.  Every spin is bounded by the global timer; a timeout sets
 //    an error bit instead of hanging.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <atomic>
 
 #include "common.cuh"
 #include "context.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace bo {
 
@@ -228,24 +233,26 @@ __global__ void __launch_bounds__(kSortBlock) radix_pass_kernel(
 }
 
 // ------------------------------------------------------------ top-k (K6) --
-// Radix select: the k smallest keys all have a top digit <= d*, the smallest
-// digit whose cumulative count reaches k.  One histogram pass over the top
-// digit (its last block finds d* and the threshold), one filter pass that
-// compacts the candidates (keys below the threshold), then the candidates --
-// usually a few hundred -- are sorted: inside one CTA when they fit in a tile
-// (a stable 8-bit LSD counting sort in shared memory), otherwise by the
-// onesweep passes.  Keys are unique (packed count and id), so the first k of
-// the sorted candidates are exactly the first k of the full order.
-constexpr int kTopkBlock = 256;
+// The k smallest of n unique keys (packed count and id) in one cooperative
+// launch: an exact radix select, 8 bits per round from the key's highest
+// varying digit down.  Each round every block histograms the digit of the keys
+// that still match the selected prefix (shared-memory counters, one global
+// atomic per bin per block), a grid barrier, and every block finds the same
+// digit where the cumulative count reaches the number of keys still needed.
+// When that digit's bin holds exactly the keys still needed, or after the last
+// digit, the selected keys are those at or below the prefix: they are
+// compacted (at most k <= 64), and block 0 orders them by rank.  The grid
+// barriers spin on a generation word bounded by the global timer (a timeout
+// sets an error bit); cooperative launch keeps every block resident.
+constexpr int kSelBlock = 256;
+constexpr int kSelMaxK = 64;
+constexpr int kSelMaxRounds = 8;
 
-struct TopkState {
-  unsigned long long threshold;  // candidates: select digit <= threshold
-  unsigned long long shift;      // bit position of the select digit
-  unsigned long long n_cand;     // compacted candidates
-  unsigned long long small;      // 1 when the candidates fit one CTA tile
-  uint32_t done;                 // ticket for the histogram's last block
-  uint32_t pad;
-  unsigned long long hist[kRadix];
+struct SelectState {
+  unsigned long long hist[kSelMaxRounds][kRadix];
+  unsigned long long n_sel;
+  uint32_t bar_count;
+  uint32_t bar_gen;
 };
 
 // The select digit: by default the top digit of the key; with (lo_bits,
@@ -260,122 +267,190 @@ __device__ __forceinline__ int topk_shift(int top_shift, int lo_bits, const unsi
   return s < top_shift ? s : top_shift;
 }
 
-__global__ void __launch_bounds__(kTopkBlock) topk_hist_kernel(const unsigned long long* __restrict__ keys,
-                                                              int64_t n_max, const unsigned long long* __restrict__ n_dev,
-                                                              int top_shift_default, int lo_bits,
-                                                              const unsigned long long* __restrict__ hi_max_dev, int k,
-                                                              TopkState* st) {
-  const int64_t n = sort_n(n_max, n_dev);
-  const int top_shift = topk_shift(top_shift_default, lo_bits, hi_max_dev);
-  __shared__ uint32_t h[kRadix];
-  h[threadIdx.x] = 0;
-  __syncthreads();
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int lane = threadIdx.x & 31;
-  const int64_t n_w = (n + 31) & ~int64_t(31);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_w; i += stride) {
-    // Warp-aggregated increments: most keys share a few top digits.
-    const uint32_t d = i < n ? (uint32_t)((keys[i] >> top_shift) & 0xffu) : 0x100u;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    if (d < 0x100u && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
-  }
-  __syncthreads();
-  if (h[threadIdx.x]) atomicAdd(&st->hist[threadIdx.x], (unsigned long long)h[threadIdx.x]);
-  if (!last_block(&st->done)) return;
-  // Inclusive scan of the 256 bins (one per thread), then the first digit
-  // whose cumulative count reaches k.
-  __shared__ unsigned long long cum[kRadix];
-  __shared__ int first;
-  unsigned long long x = __ldcg(&st->hist[threadIdx.x]);
-  cum[threadIdx.x] = x;
-  if (threadIdx.x == 0) first = kRadix;
-  __syncthreads();
-  for (int o = 1; o < kRadix; o <<= 1) {
-    const unsigned long long y = threadIdx.x >= o ? cum[threadIdx.x - o] : 0ull;
-    __syncthreads();
-    x += y;
-    cum[threadIdx.x] = x;
-    __syncthreads();
-  }
-  if (x >= (unsigned long long)k) atomicMin(&first, (int)threadIdx.x);
+
+__device__ __forceinline__ void grid_barrier(SelectState* st, uint32_t& bad) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    // keys whose select digit is <= first (all keys when the count never reaches k)
-    st->threshold = (unsigned long long)(first >= kRadix ? kRadix - 1 : first);
-    st->shift = (unsigned long long)top_shift;
-    st->n_cand = 0;
+    const uint32_t g = ld_acquire_u32(&st->bar_gen);
+    __threadfence();
+    if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+      st->bar_count = 0;
+      __threadfence();
+      atomicAdd(&st->bar_gen, 1u);
+    } else {
+      const uint64_t t0 = global_ns();
+      while (ld_acquire_u32(&st->bar_gen) == g) {
+        if (global_ns() - t0 > kWaitLimitNs) {
+          bad |= kErrSpinTimeout;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
   }
+  __syncthreads();
 }
 
-__global__ void __launch_bounds__(kTopkBlock) topk_filter_kernel(const unsigned long long* __restrict__ keys,
-                                                                const uint32_t* __restrict__ vals, int64_t n_max,
-                                                                const unsigned long long* __restrict__ n_dev,
-                                                                TopkState* st, unsigned long long* __restrict__ ck,
-                                                                uint32_t* __restrict__ cv) {
+__global__ void __launch_bounds__(kSelBlock) topk_select_kernel(const unsigned long long* __restrict__ keys,
+                                                               const uint32_t* __restrict__ vals, int64_t n_max,
+                                                               const unsigned long long* __restrict__ n_dev,
+                                                               int top_shift_default, int lo_bits,
+                                                               const unsigned long long* __restrict__ hi_max_dev,
+                                                               int k, SelectState* st, unsigned long long* __restrict__ ck,
+                                                               uint32_t* __restrict__ cv, uint32_t* err) {
   const int64_t n = sort_n(n_max, n_dev);
-  const unsigned long long thr = __ldcg(&st->threshold);
-  const int shift = (int)__ldcg(&st->shift);
+  const int64_t kk = k < kSelMaxK ? (int64_t)k : (int64_t)kSelMaxK;
+  const unsigned long long want = (unsigned long long)(n < kk ? n : kk);
+  if (want == 0) return;  // the same in every block
+  // Keys lie below 2^(s0 + 8): every bit above the first digit is zero.
+  const int s0 = topk_shift(top_shift_default, lo_bits, hi_max_dev);
+  __shared__ uint32_t h[kRadix];
+  __shared__ unsigned long long cum[kRadix];
+  __shared__ int first;
+  const int t = threadIdx.x, lane = t & 31;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int lane = threadIdx.x & 31;
   const int64_t n_w = (n + 31) & ~int64_t(31);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_w; i += stride) {
+  uint32_t bad = 0;
+  unsigned long long prefix = 0, pmask = 0, need = want;
+  int round = 0;
+  for (int sh = s0; sh > -8 && round < kSelMaxRounds; sh -= 8, ++round) {
+    const int shift = sh < 0 ? 0 : sh;
+    const unsigned long long dmask = (1ull << (sh < 0 ? sh + 8 : 8)) - 1ull;
+    h[t] = 0;
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + t; i < n_w; i += stride) {
+      const unsigned long long key = i < n ? keys[i] : 0ull;
+      const uint32_t d = (i < n && (key & pmask) == prefix) ? (uint32_t)((key >> shift) & dmask) : 0x100u;
+      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      if (d < 0x100u && lane == __ffs(peers) - 1) atomicAdd(&h[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    if (h[t]) atomicAdd(&st->hist[round][t], (unsigned long long)h[t]);
+    grid_barrier(st, bad);
+    // Inclusive scan of the round's bins (one per thread); the first digit
+    // whose cumulative count reaches `need`.
+    const unsigned long long own = __ldcg(&st->hist[round][t]);
+    unsigned long long x = own;
+    cum[t] = x;
+    if (t == 0) first = kRadix;
+    __syncthreads();
+    for (int o = 1; o < kRadix; o <<= 1) {
+      const unsigned long long y = t >= o ? cum[t - o] : 0ull;
+      __syncthreads();
+      x += y;
+      cum[t] = x;
+      __syncthreads();
+    }
+    if (x >= need) atomicMin(&first, t);
+    __syncthreads();
+    const int dg = first < kRadix ? first : kRadix - 1;  // (always found: the matching keys number >= need)
+    const unsigned long long below = dg > 0 ? cum[dg - 1] : 0ull;
+    const unsigned long long at = cum[dg] - below;
+    __syncthreads();
+    need -= below;
+    prefix |= (unsigned long long)dg << shift;
+    pmask |= dmask << shift;
+    if (at == need) break;  // every key of this digit is taken: the prefix decides
+  }
+  // Selected: the keys whose bits under pmask are at or below the prefix.
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + t; i < n_w; i += stride) {
     const unsigned long long key = i < n ? keys[i] : ~0ull;
-    const bool take = i < n && ((key >> shift) & 0xffull) <= thr;
+    const bool take = i < n && (key & pmask) <= prefix;
     const uint32_t ballot = __ballot_sync(0xffffffffu, take);
     if (!ballot) continue;
     unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(&st->n_cand, (unsigned long long)__popc(ballot));
+    if (lane == 0) base = atomicAdd(&st->n_sel, (unsigned long long)__popc(ballot));
     base = __shfl_sync(0xffffffffu, base, 0);
     if (take) {
       const unsigned long long pos = base + __popc(ballot & ((1u << lane) - 1u));
-      if (pos < (unsigned long long)n_max) {
+      if (pos < (unsigned long long)kSelMaxK) {
         ck[pos] = key;
         cv[pos] = vals[i];
+      } else {
+        bad |= kErrOutputOverflow;
       }
     }
   }
+  grid_barrier(st, bad);
+  if (blockIdx.x == 0) {
+    __shared__ unsigned long long sk[kSelMaxK];
+    __shared__ uint32_t sv[kSelMaxK];
+    const unsigned long long ns = __ldcg(&st->n_sel);
+    const int m = (int)(ns < (unsigned long long)kSelMaxK ? ns : (unsigned long long)kSelMaxK);
+    if (ns != want) bad |= kErrOutputOverflow;
+    if (t < m) {
+      sk[t] = ck[t];
+      sv[t] = cv[t];
+    }
+    __syncthreads();
+    if (t < m) {  // unique keys: the rank is the count of smaller keys
+      int r = 0;
+      for (int j = 0; j < m; ++j) r += sk[j] < sk[t];
+      ck[r] = sk[t];
+      cv[r] = sv[t];
+    }
+  }
+  if (bad) raise_error(err, bad);
 }
 
-// Stable LSD radix sort of <= kBlockSortMax pairs inside one CTA (8-bit digits
-// over [begin_bit, end_bit)), with the same warp ranking as the onesweep pass
-// (each warp owns a contiguous segment, rounds and lanes in input order).
-// Sets st->small = 0 and leaves the data alone if there are more candidates
-// (the onesweep passes then sort them).
-constexpr int kBlockSortMax = 2048;
-constexpr int kBlockSortRounds = kBlockSortMax / kSortBlock;  // keys per lane
+// Stable LSD radix sort of up to kClusterSortMax pairs by one thread-block
+// cluster, the pairs held in the CTAs' shared memory for the whole sort: CTA
+// r holds global positions [r*S, r*S + S).  Per 8-bit digit every warp ranks
+// its contiguous 512-pair segment (rounds and lanes in input order, as the
+// onesweep pass), each CTA publishes its 256 digit totals, every CTA reads the
+// cluster's totals through distributed shared memory to place its digits, and
+// each pair is stored straight into the shared memory of the CTA that owns
+// its destination (st.shared::cluster); one cluster barrier per digit.  A
+// digit that every key shares is skipped.  No global memory between the load
+// and the final store, one launch for the whole sort.
+constexpr int kCsBlock = 512;
+constexpr int kCsWarps = kCsBlock / 32;
+constexpr int kCsCap = 8192;                    // pairs per CTA
+constexpr int kCsRounds = kCsCap / kCsBlock;    // rounds of 32 per warp
+constexpr int kCsMaxCluster = 8;                // portable cluster size
+constexpr int64_t kClusterSortMax = (int64_t)kCsCap * kCsMaxCluster;
+constexpr size_t kCsDynSmem = (size_t)2 * kCsCap * (sizeof(unsigned long long) + sizeof(uint32_t));
 
-__global__ void __launch_bounds__(kSortBlock) block_sort_kernel(unsigned long long* __restrict__ ck,
-                                                                uint32_t* __restrict__ cv, TopkState* st,
-                                                                int begin_bit, int end_bit) {
-  extern __shared__ __align__(16) unsigned char bs_smem[];
-  unsigned long long* sk = reinterpret_cast<unsigned long long*>(bs_smem);       // [2][kBlockSortMax]
-  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + 2 * kBlockSortMax);           // [2][kBlockSortMax]
-  __shared__ uint32_t warp_cnt[kSortWarps][kRadix];
-  __shared__ uint32_t dig_base[kRadix];
-  const unsigned long long n = __ldcg(&st->n_cand);
-  if (n > (unsigned long long)kBlockSortMax) {
-    if (threadIdx.x == 0) st->small = 0;
-    return;
+__global__ void __launch_bounds__(kCsBlock, 1) cluster_sort_kernel(unsigned long long* __restrict__ keys,
+                                                                  uint32_t* __restrict__ vals, int64_t n,
+                                                                  int begin_bit, int end_bit) {
+  cg::cluster_group cl = cg::this_cluster();
+  const uint32_t cs = cl.num_blocks();
+  const uint32_t me = cl.block_rank();
+  extern __shared__ __align__(16) unsigned char cs_smem[];
+  unsigned long long* sk = reinterpret_cast<unsigned long long*>(cs_smem);  // [2][kCsCap]
+  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + 2 * kCsCap);              // [2][kCsCap]
+  __shared__ uint32_t warp_cnt[kCsWarps][kRadix];
+  __shared__ uint32_t tot[kRadix];   // this CTA's digit totals, read by the whole cluster
+  __shared__ uint32_t base[kRadix];  // where this CTA's pairs of each digit start
+  __shared__ uint32_t wsum[kRadix / 32];
+  __shared__ int skip;
+  const uint32_t S = (uint32_t)((n + cs - 1) / cs);  // <= kCsCap (checked by the host)
+  const int64_t lo = (int64_t)me * S;
+  const int64_t left = n - lo;
+  const uint32_t m = left <= 0 ? 0u : (left < (int64_t)S ? (uint32_t)left : S);
+  for (uint32_t i = threadIdx.x; i < m; i += kCsBlock) {
+    sk[i] = keys[lo + i];
+    sv[i] = vals[lo + i];
   }
-  if (threadIdx.x == 0) st->small = 1;
-  for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) {
-    sk[i] = ck[i];
-    sv[i] = cv[i];
-  }
+  cl.sync();  // every CTA runs (and has loaded) before any pair moves between them
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt_mask = (1u << lane) - 1u;
   int src = 0;
   for (int shift = begin_bit; shift < end_bit; shift += 8) {
-    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += blockDim.x) (&warp_cnt[0][0])[i] = 0;
+    const uint32_t dmask = (1u << min(8, end_bit - shift)) - 1u;
+    for (int i = threadIdx.x; i < kCsWarps * kRadix; i += kCsBlock) (&warp_cnt[0][0])[i] = 0;
+    if (threadIdx.x == 0) skip = 0;
     __syncthreads();
-    const unsigned long long* ks = sk + src * kBlockSortMax;
-    const uint32_t* vs = sv + src * kBlockSortMax;
-    uint32_t rank[kBlockSortRounds], dig[kBlockSortRounds];
+    const unsigned long long* ks = sk + src * kCsCap;
+    const uint32_t* vs = sv + src * kCsCap;
+    uint32_t rank[kCsRounds], dig[kCsRounds];
 #pragma unroll
-    for (int r = 0; r < kBlockSortRounds; ++r) {
-      const unsigned long long idx = (unsigned long long)warp * (32 * kBlockSortRounds) + r * 32 + lane;
-      const bool valid = idx < n;
-      const uint32_t d = valid ? (uint32_t)((ks[idx] >> shift) & 0xffu) : 0x100u;
+    for (int r = 0; r < kCsRounds; ++r) {
+      const uint32_t idx = (uint32_t)warp * (32 * kCsRounds) + r * 32 + lane;
+      const bool valid = idx < m;
+      const uint32_t d = valid ? (uint32_t)((ks[idx] >> shift) & dmask) : 0x100u;
       dig[r] = d;
       const uint32_t peers = __match_any_sync(0xffffffffu, d);
       const uint32_t before = valid ? warp_cnt[warp][d] : 0u;
@@ -385,52 +460,63 @@ __global__ void __launch_bounds__(kSortBlock) block_sort_kernel(unsigned long lo
       rank[r] = before + __popc(peers & lt_mask);
     }
     __syncthreads();
-    {
-      const int d = threadIdx.x;  // one digit per thread
-      uint32_t tot = 0;
-      for (int w = 0; w < kSortWarps; ++w) {
+    if (threadIdx.x < kRadix) {  // one digit per thread: warps' exclusive prefix, CTA total
+      const int d = threadIdx.x;
+      uint32_t t = 0;
+      for (int w = 0; w < kCsWarps; ++w) {
         const uint32_t c = warp_cnt[w][d];
-        warp_cnt[w][d] = tot;
-        tot += c;
+        warp_cnt[w][d] = t;
+        t += c;
       }
-      // exclusive scan of the digit totals across the 256 threads
-      dig_base[d] = tot;
-      __syncthreads();
-      uint32_t x = tot;
-      for (int o = 1; o < kRadix; o <<= 1) {
-        const uint32_t y = d >= o ? dig_base[d - o] : 0u;
-        __syncthreads();
-        x += y;
-        dig_base[d] = x;
-        __syncthreads();
-      }
-      dig_base[d] = x - tot;
+      tot[d] = t;
     }
-    __syncthreads();
-    unsigned long long* kd = sk + (src ^ 1) * kBlockSortMax;
-    uint32_t* vd = sv + (src ^ 1) * kBlockSortMax;
+    cl.sync();  // every CTA's totals are published
+    uint32_t all = 0, below = 0, incl = 0;
+    if (threadIdx.x < kRadix) {
+      const int d = threadIdx.x;
+      for (uint32_t q = 0; q < cs; ++q) {
+        const uint32_t v = cl.map_shared_rank(tot, q)[d];
+        all += v;
+        if (q < me) below += v;
+      }
+      incl = all;  // inclusive scan over the digits: within the warp, then across the 8 warps
 #pragma unroll
-    for (int r = 0; r < kBlockSortRounds; ++r) {
-      const uint32_t d = dig[r];
-      if (d < 0x100u) {
-        const unsigned long long idx = (unsigned long long)warp * (32 * kBlockSortRounds) + r * 32 + lane;
-        const uint32_t pos = dig_base[d] + warp_cnt[warp][d] + rank[r];
-        kd[pos] = ks[idx];
-        vd[pos] = vs[idx];
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
       }
+      if (lane == 31) wsum[warp] = incl;
+      if (all == (uint32_t)n) skip = 1;  // every key has this digit: the pass would not move anything
     }
     __syncthreads();
-    src ^= 1;
+    if (threadIdx.x < kRadix) {
+      uint32_t pre = 0;
+      for (int w = 0; w < warp; ++w) pre += wsum[w];
+      base[threadIdx.x] = pre + incl - all + below;
+    }
+    __syncthreads();
+    if (!skip) {
+      unsigned long long* kd = sk + (src ^ 1) * kCsCap;
+      uint32_t* vd = sv + (src ^ 1) * kCsCap;
+#pragma unroll
+      for (int r = 0; r < kCsRounds; ++r) {
+        const uint32_t d = dig[r];
+        if (d < 0x100u) {
+          const uint32_t idx = (uint32_t)warp * (32 * kCsRounds) + r * 32 + lane;
+          const uint32_t pos = base[d] + warp_cnt[warp][d] + rank[r];
+          const uint32_t q = pos / S, slot = pos - q * S;
+          cl.map_shared_rank(kd, q)[slot] = ks[idx];
+          cl.map_shared_rank(vd, q)[slot] = vs[idx];
+        }
+      }
+    }
+    cl.sync();  // all pairs placed and all totals read before the next digit
+    if (!skip) src ^= 1;
   }
-  for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) {
-    ck[i] = sk[src * kBlockSortMax + i];
-    cv[i] = sv[src * kBlockSortMax + i];
+  for (uint32_t i = threadIdx.x; i < m; i += kCsBlock) {
+    keys[lo + i] = sk[src * kCsCap + i];
+    vals[lo + i] = sv[src * kCsCap + i];
   }
-}
-
-// Key count for the onesweep fallback: 0 when the CTA sort already handled it.
-__global__ void topk_big_count_kernel(const TopkState* st, unsigned long long* big) {
-  if (threadIdx.x == 0) *big = __ldcg(&st->small) ? 0ull : __ldcg(&st->n_cand);
 }
 
 }  // namespace bo
@@ -444,9 +530,47 @@ std::atomic<uint32_t> g_sort_epoch{1};
 namespace bo {
 // Sorts (keys, vals) ascending by bits [begin_bit, end_bit) of the key, stably.
 // tmp_keys / tmp_vals must hold n entries.  The sorted data ends in keys/vals.
+// One cluster of the smallest power-of-two size whose shared memory holds the
+// pairs (n <= kClusterSortMax).
+int cluster_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, int64_t n, int begin_bit,
+                       int end_bit) {
+  if (n <= 1 || end_bit <= begin_bit) return BO_OK;
+  if (n > kClusterSortMax) return set_error(ctx, BO_ERR_INVALID, "cluster_sort: %lld pairs", (long long)n);
+  unsigned cs = 1;
+  while ((int64_t)cs * kCsCap < n) cs <<= 1;
+  static bool ready = false;
+  if (!ready) {
+    BO_CUDA(ctx, cudaFuncSetAttribute(cluster_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kCsDynSmem));
+    ready = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cs);
+  cfg.blockDim = dim3(kCsBlock);
+  cfg.dynamicSmemBytes = kCsDynSmem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BO_CUDA(ctx, cudaLaunchKernelEx(&cfg, cluster_sort_kernel, keys, vals, n, begin_bit, end_bit));
+  return after_launch(ctx, "cluster_sort_kernel");
+}
+
+int read_device_count(bo_ctx* ctx, const unsigned long long* n_dev, int64_t n_max, int64_t* n) {
+  BO_CUDA(ctx, cudaMemcpyAsync(ctx->h_word, n_dev, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+  BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *n = (int64_t)std::min<unsigned long long>(*ctx->h_word, (unsigned long long)std::max<int64_t>(n_max, 0));
+  return BO_OK;
+}
+
 int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsigned long long* tmp_keys,
                      uint32_t* tmp_vals, int64_t n, int begin_bit, int end_bit, const unsigned long long* n_dev) {
   if (end_bit <= begin_bit || (n <= 1 && !n_dev)) return BO_OK;
+  if (!n_dev && n <= kClusterSortMax) return cluster_sort_pairs(ctx, keys, vals, n, begin_bit, end_bit);
   // An even number of passes leaves the result in keys/vals; pad with a pass
   // over zero bits (a stable copy of the actual keys) rather than copying the
   // whole upper-bound buffer back.
@@ -491,43 +615,31 @@ int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsi
 }  // namespace bo
 
 namespace bo {
-// The k smallest keys in ascending order, written to the front of
-// (cand_keys, cand_vals) (capacity n_max each); the count of keys comes from
-// n_dev.  Asynchronous; no host round trip.
+// The k smallest keys (k <= 64; the keys must be unique) in ascending order,
+// written to the front of (cand_keys, cand_vals); the count of keys comes
+// from n_dev.  One memset and one cooperative launch; no host round trip.
 int radix_topk_pairs(bo_ctx* ctx, const unsigned long long* keys, const uint32_t* vals, int64_t n_max,
                      const unsigned long long* n_dev, int key_bits, int k, unsigned long long* cand_keys,
                      uint32_t* cand_vals, unsigned long long* tmp_keys, uint32_t* tmp_vals, int lo_bits,
                      const unsigned long long* hi_max_dev) {
+  (void)tmp_keys;
+  (void)tmp_vals;
+  if (k < 0 || k > kSelMaxK) return set_error(ctx, BO_ERR_INVALID, "top-k: k = %d outside [0, %d]", k, kSelMaxK);
   void* p = nullptr;
-  int rc = region(ctx, "topk_state", sizeof(TopkState), &p);
+  int rc = region(ctx, "topk_select", sizeof(SelectState), &p);
   if (rc) return rc;
-  TopkState* st = static_cast<TopkState*>(p);
-  BO_CUDA(ctx, cudaMemsetAsync(st, 0, sizeof(TopkState), ctx->stream));
+  SelectState* st = static_cast<SelectState*>(p);
+  BO_CUDA(ctx, cudaMemsetAsync(st, 0, sizeof(SelectState), ctx->stream));
   const int bits = std::max(8, ((key_bits + 7) / 8) * 8);
-  const int top_shift = bits - 8;
-  const int g = (int)std::max<int64_t>(1, std::min<int64_t>((n_max + kTopkBlock - 1) / kTopkBlock, ctx->num_sms));
-  topk_hist_kernel<<<g, kTopkBlock, 0, ctx->stream>>>(keys, n_max, n_dev, top_shift, lo_bits, hi_max_dev,
-                                                       std::max(k, 1), st);
-  if ((rc = after_launch(ctx, "topk_hist_kernel"))) return rc;
-  topk_filter_kernel<<<g, kTopkBlock, 0, ctx->stream>>>(keys, vals, n_max, n_dev, st, cand_keys, cand_vals);
-  if ((rc = after_launch(ctx, "topk_filter_kernel"))) return rc;
-  const size_t bs_smem = (sizeof(unsigned long long) + sizeof(uint32_t)) * 2 * kBlockSortMax;
-  static bool bs_ready = false;
-  if (!bs_ready) {
-    BO_CUDA(ctx, cudaFuncSetAttribute(reinterpret_cast<const void*>(&block_sort_kernel),
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bs_smem));
-    bs_ready = true;
-  }
-  block_sort_kernel<<<1, kSortBlock, bs_smem, ctx->stream>>>(cand_keys, cand_vals, st, 0, bits);
-  if ((rc = after_launch(ctx, "block_sort_kernel"))) return rc;
-  // Large candidate sets (heavy ties in the top digit): the onesweep passes.
-  // With a small set they see a zero count and retire immediately.
-  void* q = nullptr;
-  if ((rc = region(ctx, "topk_bigcount", 64, &q))) return rc;
-  unsigned long long* big = static_cast<unsigned long long*>(q);
-  topk_big_count_kernel<<<1, 32, 0, ctx->stream>>>(st, big);
-  if ((rc = after_launch(ctx, "topk_big_count_kernel"))) return rc;
-  return radix_sort_pairs(ctx, cand_keys, cand_vals, tmp_keys, tmp_vals, n_max, 0, bits, big);
+  const int top_shift = std::min(bits, 64) - 8;
+  const void* kf = reinterpret_cast<const void*>(&topk_select_kernel);
+  const int64_t resident = (int64_t)ctx->num_sms * occupancy_blocks(kf, kSelBlock, 0);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(resident, (n_max + 4 * kSelBlock - 1) / (4 * kSelBlock)));
+  uint32_t* err = ctx->d_err;
+  void* args[] = {(void*)&keys, (void*)&vals, (void*)&n_max, (void*)&n_dev, (void*)&top_shift, (void*)&lo_bits,
+                  (void*)&hi_max_dev, (void*)&k, (void*)&st, (void*)&cand_keys, (void*)&cand_vals, (void*)&err};
+  BO_CUDA(ctx, cudaLaunchCooperativeKernel(kf, dim3((unsigned)grid), dim3(kSelBlock), args, 0, ctx->stream));
+  return after_launch(ctx, "topk_select_kernel");
 }
 }  // namespace bo
 

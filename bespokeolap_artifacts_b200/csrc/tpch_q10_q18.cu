@@ -426,10 +426,14 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
                                                                     t->n_customer, t->nation_bound, keys, vals,
                                                                     n_out);
   if ((rc = after_launch(ctx, "q10_emit_kernel"))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, nm, 0, 32, n_out))) return rc;
+  // The result's size, read back once: up to 64K rows sort in one cluster
+  // launch per key instead of a pass sequence sized for every customer.
+  int64_t ns = 0;
+  if ((rc = read_device_count(ctx, n_out, nm, &ns))) return rc;
+  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 32, nullptr))) return rc;
   q10_key2_kernel<<<grid_for(ctx, nm), kTpBlock, 0, ctx->stream>>>(vals, rev, n_out, keys);
   if ((rc = after_launch(ctx, "q10_key2_kernel"))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, nm, 0, 64, n_out))) return rc;
+  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
   q10_gather_kernel<<<grid_for(ctx, nm), kTpBlock, 0, ctx->stream>>>(vals, rev, t->custkey_to_row, t->c_nationkey,
                                                                       n_out, rows);
   if ((rc = after_launch(ctx, "q10_gather_kernel"))) return rc;
@@ -499,11 +503,13 @@ extern "C" int bo_tpch_q18(bo_ctx* ctx, const bo_tpch_q18_tables* t, int32_t qua
       t->o_orderkey, t->o_custkey, no, dense ? 1 : 0, bound, sum, use_mark ? mark : nullptr, quantity_threshold,
       cust, keys, vals, n_out, ctx->d_err);
   if ((rc = after_launch(ctx, "q18_qualify_kernel"))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, cap, 0, 32, n_out))) return rc;
+  int64_t ns = 0;  // the result's size, read back once (see bo_tpch_q10)
+  if ((rc = read_device_count(ctx, n_out, cap, &ns))) return rc;
+  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 32, nullptr))) return rc;
   q18_key2_kernel<<<grid_for(ctx, no), kTpBlock, 0, ctx->stream>>>(vals, t->o_totalprice, t->o_orderdate, n_out,
                                                                      keys);
   if ((rc = after_launch(ctx, "q18_key2_kernel"))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, cap, 0, 48, n_out))) return rc;
+  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 48, nullptr))) return rc;
   q18_gather_kernel<<<grid_for(ctx, no), kTpBlock, 0, ctx->stream>>>(vals, t->o_orderkey, t->o_custkey,
                                                                        t->o_orderdate, t->o_totalprice,
                                                                        dense ? 1 : 0, sum, cust, n_out, rows);

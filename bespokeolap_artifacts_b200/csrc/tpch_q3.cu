@@ -216,11 +216,15 @@ extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_
   }
   q3_compact_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(cnt, t->o_orderkey, no, keys, vals, n_out);
   if ((rc = after_launch(ctx, "q3_compact_kernel"))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, no, 0, 32, n_out))) return rc;
+  // The result's size, read back once: up to 64K rows sort in one cluster
+  // launch per key instead of a pass sequence sized for every order.
+  int64_t ns = 0;
+  if ((rc = read_device_count(ctx, n_out, no, &ns))) return rc;
+  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 32, nullptr))) return rc;
   q3_key2_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(vals, rev, t->o_orderdate, n_out, keys,
                                                                    ctx->d_err);
   if ((rc = after_launch(ctx, "q3_key2_kernel"))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, no, 0, 64, n_out))) return rc;
+  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
   q3_gather_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(vals, rev, t->o_orderkey, t->o_orderdate,
                                                                      t->o_shippriority, n_out, rows);
   if ((rc = after_launch(ctx, "q3_gather_kernel"))) return rc;

@@ -105,6 +105,15 @@ class Engine:
     def synchronize(self):
         self.ctx.synchronize()
 
+    @property
+    def host_threads(self) -> int:
+        """Host threads of the streamed join's payload gather (0: read in place)."""
+        return int(N.lib().bo_host_threads(self.ctx.handle))
+
+    @host_threads.setter
+    def host_threads(self, threads: int) -> None:
+        self.ctx.call("bo_set_host_threads", int(threads))
+
     # ------------------------------------------------------------ Q1 -------
     @staticmethod
     def fact_cols(cols, n_rows: int) -> N.FactCols:

@@ -15,6 +15,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libbespoke_gpu.so"
 
 BO_OK = 0
 BO_ERR_OVERFLOW = -3
+BO_ERR_DATA = -6
 STATUS_NAMES = {
     0: "BO_OK",
     -1: "BO_ERR_INVALID",
@@ -566,6 +567,8 @@ _SIGNATURES = {
                                       _P, C.POINTER(JoinResult)]),
     "bo_join_stream_host_async": (C.c_int, [_P, C.POINTER(JoinBuildCols), C.POINTER(JoinProbeCols),
                                             C.POINTER(JoinParams), _P, _P]),
+    "bo_set_host_threads": (C.c_int, [_P, C.c_int32]),
+    "bo_host_threads": (C.c_int, [_P]),
     "bo_groupby_topk_partitioned_device": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),
                                                      C.POINTER(GbParams), C.c_int32, C.c_float, _P]),
     "bo_groupby_topk_partitioned": (C.c_int, [_P, C.POINTER(GbACols), C.POINTER(GbBCols), C.POINTER(GbCCols),

@@ -310,9 +310,16 @@ int bo_join_multi_host(bo_ctx* ctx, const bo_join_build_cols* build, const bo_jo
  * cudaHostRegister'd): only the columns every row needs cross PCIe as copies
  * (build date and segment, probe fk, the latter in 1M-row chunks overlapped
  * with the probe of the previous chunks); the build keys of qualifying rows
- * and the price / discount of matching rows are read in place by the kernels
- * (zero-copy).  pred_device = NULL runs the exact-count form; otherwise the
- * table is presized from the device prediction and rerun exactly on overflow. */
+ * are read in place by the build kernel (zero-copy).  The price / discount of
+ * matching probe rows are, by default, gathered by host threads: the probe
+ * lists the matching rows of each chunk in pinned host memory, the context's
+ * threads copy those rows' price and discount into contiguous records while
+ * later chunks are copied and probed, and one bulk copy per chunk feeds a
+ * summing kernel (bo_set_host_threads).  With 0 host threads the probe reads
+ * them in place instead.  pred_device = NULL runs the exact-count form;
+ * otherwise the table is presized from the device prediction and rerun
+ * exactly on overflow.  Inputs must stay valid until the call (or, for the
+ * _async form, bo_synchronize) returns. */
 int bo_join_stream_host(bo_ctx* ctx, const bo_join_build_cols* build_host, const bo_join_probe_cols* probe_host,
                         const bo_join_params* prm, const float* pred_device, bo_join_result* out_host);
 /* The presized streamed form without waiting: the result lands in out_pinned
@@ -322,6 +329,13 @@ int bo_join_stream_host(bo_ctx* ctx, const bo_join_build_cols* build_host, const
  * is invalid: rerun that query with bo_join_stream_host. */
 int bo_join_stream_host_async(bo_ctx* ctx, const bo_join_build_cols* build_host, const bo_join_probe_cols* probe_host,
                               const bo_join_params* prm, const float* pred_device, bo_join_result* out_pinned);
+/* Host threads the streamed join uses to gather the payload of matching probe
+ * rows: threads < 0 chooses from the machine (half its hardware threads, at
+ * most 8; the default), 0 reads the payload in place over PCIe instead, at
+ * most 256.  Waits for queued streamed joins before it takes effect.
+ * bo_host_threads returns the count in effect. */
+int bo_set_host_threads(bo_ctx* ctx, int32_t threads);
+int bo_host_threads(const bo_ctx* ctx);
 
 /* =============================================================== GROUP-BY ==
  * Skewed three-way join + high-cardinality group-by + ordered top-k.  Restates

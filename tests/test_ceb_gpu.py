@@ -59,13 +59,20 @@ def test_builder_order_on_gpu(engine, torch_cuda, tmp_path):
     ceb.builder_order(engine, tables)
     for table, (p, s) in (("cast_info", ("movie_id", "role_id")), ("movie_info", ("movie_id", "info_type_id"))):
         raw = pq.read_table(data / f"{table}.parquet")
-        cols = {c: np.nan_to_num(raw[c].to_numpy(zero_copy_only=False)).astype(np.int64) for c in raw.column_names
-                if c in tables.tables[table]}
-        order = np.lexsort((cols[s], cols[p]))  # stable: ties keep the input order
-        for c in cols:
-            dev = tables.col(table, c).values.cpu().numpy()
-            if tables.col(table, c).dictionary is None:
-                assert np.array_equal(dev, cols[c][order]), (table, c)
+        loaded = [c for c in raw.column_names if c in tables.tables[table]]
+        ints = {c: np.nan_to_num(raw[c].to_numpy(zero_copy_only=False)).astype(np.int64) for c in loaded
+                if tables.col(table, c).dictionary is None}
+        order = np.lexsort((ints[s], ints[p]))  # stable: ties keep the input order
+        for c in loaded:
+            col = tables.col(table, c)
+            dev = col.values.cpu().numpy()
+            if col.dictionary is None:
+                assert np.array_equal(dev, ints[c][order]), (table, c)
+            else:  # string column: the codes decode to the input strings in the new order
+                want = raw[c].to_pylist()
+                nl = col.is_null.cpu().numpy() if col.is_null is not None else np.zeros(len(dev), np.uint8)
+                got = [None if nl[i] else col.dictionary[dev[i]] for i in range(len(dev))]
+                assert got == [want[i] for i in order], (table, c)
         nl = tables.col(table, "movie_id").is_null
         assert nl is None or not nl.any().item()
     assert ceb.q1a(engine, tables, *Q1A_CASES[0]) == before
