@@ -576,6 +576,105 @@ def _median_wall_ms(fn, n: int) -> float:
     return statistics.median(ts)
 
 
+def groupby_graph_forms(eng, stream, sizer, feats, args, exact, n: int) -> dict:
+    """The learned and the plain group-by, each query's device work captured
+    once as a CUDA graph and replayed (the same treatment the join's forms get):
+    learned = MLP prediction + the presized pipeline in one graph; plain = the
+    exact distinct pre-pass graph, one host round trip for its count, then the
+    presized pipeline graph sized from that count (2 slots per group, as the
+    plain form sizes its table).  Per-query latency with the result on the host."""
+    import torch
+
+    from bespokeolap_artifacts_b200 import batching as B
+    from bespokeolap_artifacts_b200 import native as N
+
+    res_sz = C.sizeof(N.GbResult)
+    pin = C.c_void_p()
+    eng.ctx.call("bo_host_alloc_pinned", C.c_size_t(res_sz + 64), C.byref(pin))
+    g_learned, g_sized, g_distinct, preds, outs, cnts = [], [], [], [], [], []
+    for i in range(3):
+        a, b, cc, prm, _ = args[i]
+        pl = torch.zeros(2, dtype=torch.float32, device="cuda")
+        ob = torch.zeros(res_sz, dtype=torch.uint8, device="cuda")
+        cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+
+        def lseq(a=a, b=b, cc=cc, prm=prm, pl=pl, ob=ob, i=i):
+            sizer.predict_device(feats[i], pl[0:1])
+            eng.ctx.call("bo_groupby_topk_presized_device", C.byref(a), C.byref(b), C.byref(cc), C.byref(prm),
+                         C.c_void_p(pl.data_ptr()), C.c_void_p(ob.data_ptr()))
+
+        def sseq(a=a, b=b, cc=cc, prm=prm, pl=pl, ob=ob):
+            eng.ctx.call("bo_groupby_topk_presized_device", C.byref(a), C.byref(b), C.byref(cc), C.byref(prm),
+                         C.c_void_p(pl.data_ptr() + 4), C.c_void_p(ob.data_ptr()))
+
+        def dseq(a=a, b=b, cc=cc, prm=prm, cnt=cnt):
+            eng.ctx.call("bo_groupby_distinct_device", C.byref(a), C.byref(b), C.byref(cc), C.byref(prm),
+                         C.c_void_p(cnt.data_ptr()))
+
+        pl[1] = float(exact[i]["n_groups"]) * 0.8
+        for fn in (lseq, sseq, dseq):
+            fn()
+            torch.cuda.synchronize()
+        gl, gs, gd = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gl, stream=stream):
+            lseq()
+        with torch.cuda.graph(gs, stream=stream):
+            sseq()
+        with torch.cuda.graph(gd, stream=stream):
+            dseq()
+        g_learned.append(gl)
+        g_sized.append(gs)
+        g_distinct.append(gd)
+        preds.append(pl)
+        outs.append(ob)
+        cnts.append(cnt)
+    cnt_host = (C.c_int64 * 2)()
+    pred_pin = C.c_void_p()
+    eng.ctx.call("bo_host_alloc_pinned", C.c_size_t(64), C.byref(pred_pin))
+
+    def read_result(k):
+        eng.ctx.call("bo_copy_d2h", pin, C.c_void_p(outs[k].data_ptr()), C.c_size_t(res_sz))
+        eng.ctx.call("bo_check_errors")
+        return N.GbResult.from_address(pin.value).as_dict()
+
+    def learned_graph(i):
+        k = i % 3
+        g_learned[k].replay()
+        r = read_result(k)
+        if r["overflowed"]:  # predicted too few groups: the exact form
+            a, b, cc, prm, _ = args[k]
+            out = N.GbResult()
+            eng.ctx.call("bo_groupby_topk_plain", C.byref(a), C.byref(b), C.byref(cc), C.byref(prm), C.byref(out))
+            return out.as_dict()
+        return r
+
+    def plain_graph(i):
+        k = i % 3
+        g_distinct[k].replay()
+        eng.ctx.call("bo_copy_d2h", cnt_host, C.c_void_p(cnts[k].data_ptr()), C.c_size_t(16))
+        # 2 slots per group (the plain form's exact sizing; the presize factor is 2.5)
+        C.c_float.from_address(pred_pin.value).value = float(cnt_host[0]) * 0.8
+        eng.ctx.call("bo_copy_h2d", C.c_void_p(preds[k].data_ptr() + 4), pred_pin, C.c_size_t(4))
+        g_sized[k].replay()
+        return read_result(k)
+
+    same = True
+    for i in range(3):
+        for fn in (learned_graph, plain_graph):
+            r = fn(i)
+            same &= all(r[f] == exact[i][f] for f in B.ANSWER_FIELDS["groupby"])
+    ms_l = _median_wall_ms(learned_graph, max(n, 10))
+    ms_p = _median_wall_ms(plain_graph, max(n, 10))
+    del g_learned, g_sized, g_distinct
+    eng.ctx.call("bo_host_free_pinned", pin)
+    eng.ctx.call("bo_host_free_pinned", pred_pin)
+    return {"learned_ms_per_query": ms_l, "plain_ms_per_query": ms_p, "speedup": ms_p / ms_l,
+            "answers_identical": bool(same),
+            "form": "CUDA graphs: learned = MLP prediction + presized pipeline in one graph per query; plain = "
+                    "exact distinct pre-pass graph + host round trip for its count + the presized pipeline "
+                    "graph sized from it; result copied to pinned host memory each query"}
+
+
 def scan_agg_section(eng, stream, peak: float) -> dict:
     """Scan-filter-group-aggregate (wide fact layout, 38 B/row): 6M rows (two
     copies alternated, 2 x 228 MB > L2) and a 60M-row table; device time per
@@ -679,8 +778,14 @@ def groupby_section(eng, stream, n_queries: int = 10, keep: dict | None = None) 
         insts.append(q)
     feats = [L.groupby_features(st, q.params["cat_set"], 1990, 2010) for q in insts]
     pred = torch.zeros(2, dtype=torch.float32, device="cuda")
+    # A's id bitmap depends on table A alone: built once at load (an index over
+    # A, like the sketches), and every form below reads it.
+    a_id_max = int(insts[0].params["a_id_max"])
+    amask = torch.zeros((a_id_max + 32) // 32, dtype=torch.int32, device="cuda")
+    eng.ctx.call("bo_groupby_a_mask_device", C.byref(N.GbACols(N.ptr(c["a_ids"]), n_a)), a_id_max,
+                 C.c_void_p(amask.data_ptr()))
     args = [eng.gb_args(c["a_ids"], c["b_a"], c["b_c"], c["c_cat"], c["c_year"], n_a, n_b, n_c,
-                        q.params["cat_set"], 1990, 2010, 10, q.params["a_id_max"]) for q in insts]
+                        q.params["cat_set"], 1990, 2010, 10, q.params["a_id_max"], amask) for q in insts]
 
     def plain(i):
         a, b, cc, prm, _ = args[i % 3]
@@ -720,6 +825,7 @@ def groupby_section(eng, stream, n_queries: int = 10, keep: dict | None = None) 
     torch.cuda.nvtx.range_push("groupby_learned")  # the range an ncu launch list of this form filters on
     ms_kern = _median_wall_ms(learned_kernels, n)
     torch.cuda.nvtx.range_pop()
+    graphs = groupby_graph_forms(eng, stream, sizer, feats, args, exact, n)
     ms_graph = _median_wall_ms(learned_graph, n)
     pg = [float(sizer.predict_host(f[None, :])[0, 0]) for f in feats]
     batch.close()
@@ -787,6 +893,8 @@ def groupby_section(eng, stream, n_queries: int = 10, keep: dict | None = None) 
         "plain_ms_per_query": ms_plain,
         "learned_multikernel_ms_per_query": ms_kern,
         "learned_persistent_ms_per_query": ms_graph,
+        "graph_forms": graphs,
+        "a_mask": "A's id bitmap built once at load (bo_groupby_a_mask_device), read by every form",
         "speedup_learned_persistent_vs_plain": ms_plain / ms_graph,
         "speedup_learned_multikernel_vs_plain": ms_plain / ms_kern,
         "q_error_groups": [float(L.q_error([p], [e["n_groups"]])[0]) for p, e in zip(pg, exact)],

@@ -102,10 +102,11 @@ def build_host(force: bool = False) -> Path | None:
         return None
     inc, libdir = pa.get_include(), pa.get_library_dirs()[0]
     srcs = [HOST / "tpch_gpu.cpp"]
-    deps = srcs + [HOST / "tpch_gpu.hpp", INCLUDE / "bespoke_gpu.h", LIB_PATH]
+    deps = srcs + [HOST / "tpch_gpu.hpp", INCLUDE / "bespoke_gpu.h", CSRC / "host_threads.cuh", LIB_PATH]
     arrow = [f"-L{libdir}", "-l:libarrow.so.2400", "-l:libparquet.so.2400", f"-Wl,-rpath,{libdir}"]
     if force or _stale(HOST_LIB, deps):
-        subprocess.run(["g++", "-std=c++20", "-O2", "-pthread", "-fPIC", "-shared", f"-I{INCLUDE}", f"-I{inc}", *map(str, srcs),
+        subprocess.run(["g++", "-std=c++20", "-O2", "-pthread", "-fPIC", "-shared", f"-I{INCLUDE}", f"-I{CSRC}", f"-I{inc}",
+                        *map(str, srcs),
                         f"-L{PKG}", "-lbespoke_gpu", f"-Wl,-rpath,{PKG}", *arrow, "-o", str(HOST_LIB)], check=True)
     main = HOST / "driver_main.cpp"
     if force or _stale(HOST_DRIVER, [main, HOST_LIB, HOST / "tpch_gpu.hpp"]):
@@ -134,5 +135,6 @@ if __name__ == "__main__":
     info = "--ptxas" in sys.argv
     build_gpu_lib(force=force or info, verbose="-v" in sys.argv, ptxas_info=info)
     if "--gpu-only" not in sys.argv:
+        build_host(force=force)
         build_oracle(force=force)
     print(f"built {LIB_PATH}")

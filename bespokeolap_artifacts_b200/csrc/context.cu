@@ -148,7 +148,10 @@ int bo_create(bo_ctx** out, int device) {
   ctx->device = device;
   ctx->num_sms = prop.multiProcessorCount;
   ctx->l2_bytes = prop.l2CacheSize;
-  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+  // A blocking stream: it is ordered with the legacy default stream, so data a
+  // caller wrote there (PyTorch's default stream, a cudaMemcpy) is complete
+  // before the context's kernels read it, without an explicit synchronise.
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamDefault) != cudaSuccess ||
       cudaMalloc(&ctx->d_err, sizeof(uint32_t)) != cudaSuccess ||
       cudaHostAlloc(&ctx->h_err, sizeof(uint32_t), cudaHostAllocDefault) != cudaSuccess ||
       cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_word), sizeof(unsigned long long), cudaHostAllocDefault) !=

@@ -169,9 +169,12 @@ __global__ void __launch_bounds__(kPredThreads) join_learned_init_kernel(const f
 // dependent DRAM round trip on every warp's path, 2 us per 1.5M-row build on
 // B200); the qualifying keys of the whole warp are then compacted into a
 // shared-memory queue and inserted by all lanes together.
+// kSparseKeys (the streamed forms, whose keys stay in pinned host memory):
+// only the qualifying rows' keys are loaded, one 4-byte read over PCIe each,
+// instead of the whole key column.
 constexpr int kBuildRowsPerThread = 16;
 
-
+template <bool kSparseKeys>
 __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_cols b, int32_t date_lt, uint32_t seg,
                                                                  unsigned long long* slots, uint32_t* bloom,
                                                                  JoinMeta* meta, uint64_t probe_limit) {
@@ -204,12 +207,22 @@ __global__ void __launch_bounds__(kBuildBlock) join_build_kernel(bo_join_build_c
       const int4 sg = ld_stream_v4(b.segment + r0);
       const uint32_t sw[4] = {(uint32_t)sg.x, (uint32_t)sg.y, (uint32_t)sg.z, (uint32_t)sg.w};
       const int8v d0 = ld_stream_v8(b.date + r0), d1 = ld_stream_v8(b.date + r0 + 8);
-      const int8v k0 = ld_stream_v8(b.key + r0), k1 = ld_stream_v8(b.key + r0 + 8);
+      if constexpr (kSparseKeys) {
 #pragma unroll
-      for (int k = 0; k < kBuildRowsPerThread; ++k) {
-        const int32_t dk = k < 8 ? d0.v[k] : d1.v[k - 8];
-        q |= (uint32_t)build_qual(dk, (sw[k >> 2] >> (8 * (k & 3))) & 0xffu, date_lt, seg) << k;
-        keys[k] = k < 8 ? k0.v[k] : k1.v[k - 8];
+        for (int k = 0; k < kBuildRowsPerThread; ++k) {
+          const int32_t dk = k < 8 ? d0.v[k] : d1.v[k - 8];
+          q |= (uint32_t)build_qual(dk, (sw[k >> 2] >> (8 * (k & 3))) & 0xffu, date_lt, seg) << k;
+        }
+#pragma unroll
+        for (int k = 0; k < kBuildRowsPerThread; ++k) keys[k] = ((q >> k) & 1u) ? b.key[r0 + k] : 0;
+      } else {
+        const int8v k0 = ld_stream_v8(b.key + r0), k1 = ld_stream_v8(b.key + r0 + 8);
+#pragma unroll
+        for (int k = 0; k < kBuildRowsPerThread; ++k) {
+          const int32_t dk = k < 8 ? d0.v[k] : d1.v[k - 8];
+          q |= (uint32_t)build_qual(dk, (sw[k >> 2] >> (8 * (k & 3))) & 0xffu, date_lt, seg) << k;
+          keys[k] = k < 8 ? k0.v[k] : k1.v[k - 8];
+        }
       }
     } else {
 #pragma unroll
@@ -629,11 +642,11 @@ int join_run(bo_ctx* ctx, const bo_join_build_cols& b, const bo_join_probe_cols&
   join_init_kernel<<<gi, 256, 0, ctx->stream>>>(ws.slots, ws.bloom, ws.meta, pred, host_log2, ws.max_log2);
   int rc = after_launch(ctx, "join_init_kernel");
   if (rc) return rc;
-  const void* kb = reinterpret_cast<const void*>(&join_build_kernel);
+  const void* kb = reinterpret_cast<const void*>(&join_build_kernel<false>);
   const int gb = grid_for(ctx, kb, kBuildBlock, 0, (b.n_rows + kBuildRowsPerThread - 1) / kBuildRowsPerThread);
   // Exact-size tables (mode 0) probe without a bound; presized ones fail fast.
   const uint64_t limit = mode == 0 ? ~0ull : kPresizedProbeLimit;
-  BO_CUDA(ctx, launch_dependent(&join_build_kernel, gb, kBuildBlock, 0, ctx->stream, b, prm.date_lt,
+  BO_CUDA(ctx, launch_dependent(&join_build_kernel<false>, gb, kBuildBlock, 0, ctx->stream, b, prm.date_lt,
                                 (uint32_t)prm.segment_eq, ws.slots, ws.bloom, ws.meta, limit));
   if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
   return launch_probe(ctx, p, ws, out, mode, limit, true);
@@ -815,8 +828,8 @@ int stream_compute(bo_ctx* ctx, const bo_join_build_cols* bh, const bo_join_prob
       ws.slots, ws.bloom, ws.meta, pred, host_log2, ws.max_log2);
   int rc = after_launch(ctx, "join_init_kernel");
   if (rc) return rc;
-  const void* kb = reinterpret_cast<const void*>(&join_build_kernel);
-  join_build_kernel<<<grid_for(ctx, kb, kBuildBlock, 0, (nb + kBuildRowsPerThread - 1) / kBuildRowsPerThread),
+  const void* kb = reinterpret_cast<const void*>(&join_build_kernel<true>);
+  join_build_kernel<true><<<grid_for(ctx, kb, kBuildBlock, 0, (nb + kBuildRowsPerThread - 1) / kBuildRowsPerThread),
                       kBuildBlock, 0, ctx->stream>>>(b, prm->date_lt, (uint32_t)prm->segment_eq, ws.slots, ws.bloom,
                                                      ws.meta, limit);
   if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
@@ -997,8 +1010,8 @@ int stream_compute_gather(bo_ctx* ctx, GatherState* g, const bo_join_build_cols*
       ws.slots, ws.bloom, ws.meta, pred, host_log2, ws.max_log2);
   int rc = after_launch(ctx, "join_init_kernel");
   if (rc) return rc;
-  const void* kb = reinterpret_cast<const void*>(&join_build_kernel);
-  join_build_kernel<<<grid_for(ctx, kb, kBuildBlock, 0, (nb + kBuildRowsPerThread - 1) / kBuildRowsPerThread),
+  const void* kb = reinterpret_cast<const void*>(&join_build_kernel<true>);
+  join_build_kernel<true><<<grid_for(ctx, kb, kBuildBlock, 0, (nb + kBuildRowsPerThread - 1) / kBuildRowsPerThread),
                       kBuildBlock, 0, ctx->stream>>>(b, prm->date_lt, (uint32_t)prm->segment_eq, ws.slots, ws.bloom,
                                                      ws.meta, limit);
   if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
@@ -1165,9 +1178,9 @@ int bo_join_learned_device(bo_ctx* ctx, const bo_mlp* m, const float* features_h
   join_learned_init_kernel<<<ctx->num_sms * 2, kPredThreads, 0, ctx->stream>>>(params, fv, F, O, ws.slots, ws.bloom,
                                                                              ws.meta, ws.max_log2, pred_device);
   if ((rc = after_launch(ctx, "join_learned_init_kernel"))) return rc;
-  const void* kb = reinterpret_cast<const void*>(&join_build_kernel);
+  const void* kb = reinterpret_cast<const void*>(&join_build_kernel<false>);
   const int gb = grid_for(ctx, kb, kBuildBlock, 0, (b->n_rows + kBuildRowsPerThread - 1) / kBuildRowsPerThread);
-  BO_CUDA(ctx, launch_dependent(&join_build_kernel, gb, kBuildBlock, 0, ctx->stream, *b, prm->date_lt,
+  BO_CUDA(ctx, launch_dependent(&join_build_kernel<false>, gb, kBuildBlock, 0, ctx->stream, *b, prm->date_lt,
                                 (uint32_t)prm->segment_eq, ws.slots, ws.bloom, ws.meta, (uint64_t)kPresizedProbeLimit));
   if ((rc = after_launch(ctx, "join_build_kernel"))) return rc;
   return launch_probe(ctx, *p, ws, out_device, 1, kPresizedProbeLimit, true);

@@ -635,10 +635,19 @@ int radix_topk_pairs(bo_ctx* ctx, const unsigned long long* keys, const uint32_t
   const void* kf = reinterpret_cast<const void*>(&topk_select_kernel);
   const int64_t resident = (int64_t)ctx->num_sms * occupancy_blocks(kf, kSelBlock, 0);
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(resident, (n_max + 4 * kSelBlock - 1) / (4 * kSelBlock)));
-  uint32_t* err = ctx->d_err;
-  void* args[] = {(void*)&keys, (void*)&vals, (void*)&n_max, (void*)&n_dev, (void*)&top_shift, (void*)&lo_bits,
-                  (void*)&hi_max_dev, (void*)&k, (void*)&st, (void*)&cand_keys, (void*)&cand_vals, (void*)&err};
-  BO_CUDA(ctx, cudaLaunchCooperativeKernel(kf, dim3((unsigned)grid), dim3(kSelBlock), args, 0, ctx->stream));
+  // A cooperative launch (every block resident: the grid barriers rely on it),
+  // through cudaLaunchKernelEx so that stream capture records it as a graph node.
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kSelBlock);
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BO_CUDA(ctx, cudaLaunchKernelEx(&cfg, topk_select_kernel, keys, vals, n_max, n_dev, top_shift, lo_bits, hi_max_dev, k,
+                                  st, cand_keys, cand_vals, ctx->d_err));
   return after_launch(ctx, "topk_select_kernel");
 }
 }  // namespace bo

@@ -2,6 +2,8 @@
 // See tpch_gpu.hpp for the contract.
 #include "tpch_gpu.hpp"
 
+#include "host_threads.cuh"  // the engine's host thread pool (plain C++)
+
 #include <arrow/api.h>
 #include <arrow/io/file.h>
 #include <parquet/arrow/reader.h>
@@ -374,22 +376,39 @@ std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, con
 namespace {
 // fn(begin, end) over [0, n), split across host threads when n is large: the
 // result rows gather host-resident strings of random customers, a loop bound
-// by memory latency that more threads overlap.
+// by memory latency that more threads overlap.  The threads are created once
+// per process (a pool that spins briefly between loops, then sleeps).
 template <class F>
 void for_row_ranges(int64_t n, const F& fn) {
   constexpr int64_t kRowsPerThread = 8192;
-  const int64_t hw = std::max<int64_t>(1, static_cast<int64_t>(std::thread::hardware_concurrency()));
-  const int64_t parts = std::min<int64_t>(std::min<int64_t>(hw, 8), (n + kRowsPerThread - 1) / kRowsPerThread);
+  static bo::HostPool pool(static_cast<int>(
+      std::min<int64_t>(8, std::max<int64_t>(1, static_cast<int64_t>(std::thread::hardware_concurrency())))));
+  const int64_t parts = std::min<int64_t>(pool.threads(), (n + kRowsPerThread - 1) / kRowsPerThread);
   if (parts <= 1) {
     fn(int64_t{0}, n);
     return;
   }
-  const int64_t step = (n + parts - 1) / parts;
-  std::vector<std::thread> pool;
-  for (int64_t p = 1; p < parts; ++p) pool.emplace_back([&fn, p, step, n] { fn(p * step, std::min(n, (p + 1) * step)); });
-  fn(int64_t{0}, std::min(n, step));
-  for (auto& t : pool) t.join();
+  pool.parallel_for(n, [&fn](int64_t lo, int64_t hi) { fn(lo, hi); }, 2 * kRowsPerThread);
 }
+
+// BO_QUERY_TRACE set: a query's phases (the GPU call with its result copy,
+// the host-side row materialisation) on stderr, in microseconds.
+class QueryTrace {
+ public:
+  explicit QueryTrace(const char* query) : query_(query), on_(std::getenv("BO_QUERY_TRACE") != nullptr) {}
+  void mark(const char* phase) {
+    if (!on_) return;
+    const auto now = std::chrono::steady_clock::now();
+    std::cerr << query_ << " " << phase << " us: "
+              << std::chrono::duration_cast<std::chrono::microseconds>(now - last_).count() << "\n";
+    last_ = now;
+  }
+
+ private:
+  const char* query_;
+  bool on_;
+  std::chrono::steady_clock::time_point last_ = std::chrono::steady_clock::now();
+};
 
 // Room for `count` result records of type T in the Database's pinned buffer.
 template <class T>
@@ -430,9 +449,11 @@ std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, 
   t.l_shipdate = col<int16_t>(db.l_shipdate);
   t.l_discounted_price = col<int32_t>(db.l_discounted_price);
   t.n_lineitem = db.n_lineitem;
+  QueryTrace trace("q3");
   bo_tpch_q3_row* out = result_rows<bo_tpch_q3_row>(db, db.n_orders);
   int64_t n = 0;
   check(db.ctx, bo_tpch_q3(db.ctx, &t, d, code, out, db.n_orders, &n), "q3");
+  trace.mark("gpu");
   std::vector<Q3ResultRow> rows(static_cast<size_t>(n));
   for (int64_t i = 0; i < n; ++i) {
     rows[i].orderkey = out[i].orderkey;
@@ -440,6 +461,7 @@ std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, 
     rows[i].orderdate_offset = out[i].orderdate_offset;
     rows[i].shippriority = out[i].shippriority;
   }
+  trace.mark("rows");
   return rows;
 }
 
@@ -471,10 +493,12 @@ std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date) {
   t.n_custkey_map = db.n_custkey_map;
   t.c_nationkey = col<int32_t>(db.c_nationkey);
   t.n_customer = db.n_customer;
+  QueryTrace trace("q10");
   bo_tpch_q10_row* out = result_rows<bo_tpch_q10_row>(db, db.n_custkey_map);
   int64_t n = 0;
   check(db.ctx, bo_tpch_q10(db.ctx, &t, start, end, rf * ls_count, ls_count, out, db.n_custkey_map, &n),
         "q10");
+  trace.mark("gpu");
   std::vector<Q10ResultRow> rows(static_cast<size_t>(n));
   for_row_ranges(n, [&](int64_t lo, int64_t hi) {
     for (int64_t i = lo; i < hi; ++i) {
@@ -491,6 +515,7 @@ std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date) {
       row.comment = db.c_comment.view(r);
     }
   });
+  trace.mark("rows");
   return rows;
 }
 

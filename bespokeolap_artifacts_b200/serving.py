@@ -149,22 +149,59 @@ def predict_requests(tables: ServingTables, reqs: list[Request], join_sizer=None
             r.predicted = float(p)
 
 
-def admit(pending: deque, footprints: dict, max_batch: int, pool_bytes: int, max_items: int) -> list:
+def admit(pending: deque, footprints: dict, max_batch: int, pool_bytes: int, max_items: int,
+          kind: int | None = None) -> list:
     """Takes requests from the head of `pending` (arrival order) while the
     batch stays within max_batch requests, pool_bytes of tables and max_items
     work items.  footprints[rid] = (table bytes, items).  A request whose
     footprint alone exceeds the slot is admitted alone (its tables are then
-    sized for the upper bound by the caller) so nothing starves."""
+    sized for the upper bound by the caller) so nothing starves.  With `kind`
+    set, only requests of that kind are taken (in arrival order); the others
+    keep their places."""
     out, tb, it = [], 0, 0
-    while pending and len(out) < max_batch:
-        r = pending[0]
+    if kind is None:
+        while pending and len(out) < max_batch:
+            r = pending[0]
+            b, i = footprints[r.rid]
+            if out and (tb + b > pool_bytes or it + i > max_items):
+                break
+            out.append(pending.popleft())
+            tb += b
+            it += i
+        return out
+    keep = deque()
+    while pending:
+        r = pending.popleft()
         b, i = footprints[r.rid]
-        if out and (tb + b > pool_bytes or it + i > max_items):
-            break
-        out.append(pending.popleft())
+        if r.kind != kind or len(out) >= max_batch or (out and (tb + b > pool_bytes or it + i > max_items)):
+            keep.append(r)
+            continue
+        out.append(r)
         tb += b
         it += i
+    pending.extend(keep)
     return out
+
+
+# Service order of the kinds under the short-first policy: scan-agg (a single
+# streaming pass, ~0.4 ms on the serving tables) before the join and the
+# group-by (~1 ms each).
+SHORT_FIRST = (N.BATCH_SCAN_AGG, N.BATCH_JOIN, N.BATCH_GROUPBY)
+
+
+def next_kind(pending: deque, policy: str, waited_ms: float, max_wait_ms: float) -> int | None:
+    """The kind a free slot takes next: None (arrival order, mixed kinds) for
+    "fifo"; for "short_first" the shortest kind waiting, unless the oldest
+    request has waited longer than max_wait_ms (then its kind: no starvation)."""
+    if policy != "short_first" or not pending:
+        return None
+    if waited_ms > max_wait_ms:
+        return pending[0].kind
+    present = {r.kind for r in pending}
+    for k in SHORT_FIRST:
+        if k in present:
+            return k
+    return pending[0].kind
 
 
 # ----------------------------------------------------------------- server ---
@@ -201,11 +238,18 @@ class BatchedServer:
     persistent batch kernel -- all on the slot's stream, one event at the
     end.  A request that finds an idle slot with nothing else waiting runs
     alone through its standalone kernel (scan-agg) or the presized join.
-    With shared=False every request is a batch instance."""
+    With shared=False every request is a batch instance.
+
+    Admission policy: "fifo" takes waiting requests in arrival order, kinds
+    mixed; "short_first" fills a free slot with requests of one kind only,
+    the shortest kind waiting first (scan-agg, join, group-by), unless the
+    oldest request has waited max_wait_ms, so that a short request neither
+    waits behind nor completes with a long one in the same slot."""
 
     def __init__(self, tables: ServingTables, n_slots: int = 2, max_batch: int = 16,
                  pool_bytes: int = 2 << 30, max_items: int = 65536, workers_per_sm: int = 1,
-                 join_sizer=None, gb_sizer=None, tile_table: B.TileTable | None = None, shared: bool = True):
+                 join_sizer=None, gb_sizer=None, tile_table: B.TileTable | None = None, shared: bool = True,
+                 policy: str = "fifo", max_wait_ms: float = 4.0):
         import torch
 
         from .engine import Engine
@@ -215,6 +259,9 @@ class BatchedServer:
         self.join_sizer, self.gb_sizer = join_sizer, gb_sizer
         self.tile_table = tile_table
         self.shared = shared
+        if policy not in ("fifo", "short_first"):
+            raise ValueError(f"unknown admission policy {policy!r}")
+        self.policy, self.max_wait_ms = policy, max_wait_ms
         self.slots = []
         for _ in range(n_slots):
             e = Engine(0)
@@ -380,7 +427,9 @@ class BatchedServer:
                     s.reqs, s.busy = [], False
             for s in self.slots:
                 if not s.busy and pending:
-                    reqs = admit(pending, foot, self.max_batch, self.pool_bytes, self.max_items)
+                    waited = (time.perf_counter() - t0 - pending[0].arrival) * 1e3
+                    kind = next_kind(pending, self.policy, waited, self.max_wait_ms)
+                    reqs = admit(pending, foot, self.max_batch, self.pool_bytes, self.max_items, kind)
                     tb = sum(foot[r.rid][0] for r in reqs)
                     if tb > self.pool_bytes:  # a single request above the pool: upper-bound tables do not fit
                         raise RuntimeError(f"request {reqs[0].rid} needs {tb} bytes of tables, slot holds "

@@ -63,7 +63,10 @@ int bo_device_init(int device);
 void bo_destroy(bo_ctx* ctx);
 const char* bo_last_error(const bo_ctx* ctx);
 /* Use an external CUDA stream (cudaStream_t passed as void*); NULL restores the
- * context's own stream. */
+ * context's own stream.  The own stream is a blocking stream: it is ordered
+ * with the legacy default stream (work a caller issued there, e.g. a PyTorch
+ * tensor written on its default stream, completes before the context reads
+ * it).  With an external stream the caller orders its inputs itself. */
 int bo_set_stream(bo_ctx* ctx, void* cuda_stream);
 void* bo_get_stream(const bo_ctx* ctx);
 int bo_synchronize(bo_ctx* ctx);

@@ -41,3 +41,25 @@ def test_latency_stats():
         r.done = r.arrival + 0.002
     st = S.latency_stats(reqs)
     assert abs(st["p50_ms"] - 2.0) < 1e-9 and abs(st["p99_ms"] - 2.0) < 1e-9 and st["requests"] == 100
+
+
+def test_admission_of_one_kind_keeps_the_others_in_order():
+    kinds = [N.BATCH_GROUPBY, N.BATCH_SCAN_AGG, N.BATCH_JOIN, N.BATCH_SCAN_AGG, N.BATCH_GROUPBY]
+    q = deque(S.Request(i, k, {}, float(i)) for i, k in enumerate(kinds))
+    foot = {i: (10, 10) for i in range(5)}
+    got = S.admit(q, foot, max_batch=8, pool_bytes=400, max_items=1000, kind=N.BATCH_SCAN_AGG)
+    assert [r.rid for r in got] == [1, 3]
+    assert [r.rid for r in q] == [0, 2, 4]          # the rest keep arrival order
+    got = S.admit(q, foot, max_batch=1, pool_bytes=400, max_items=1000, kind=N.BATCH_GROUPBY)
+    assert [r.rid for r in got] == [0] and [r.rid for r in q] == [2, 4]
+
+
+def test_short_first_picks_the_shortest_kind_unless_the_oldest_waited_too_long():
+    q = deque([S.Request(0, N.BATCH_GROUPBY, {}, 0.0), S.Request(1, N.BATCH_JOIN, {}, 0.1),
+               S.Request(2, N.BATCH_SCAN_AGG, {}, 0.2)])
+    assert S.next_kind(q, "fifo", 0.0, 4.0) is None
+    assert S.next_kind(q, "short_first", 1.0, 4.0) == N.BATCH_SCAN_AGG
+    assert S.next_kind(q, "short_first", 5.0, 4.0) == N.BATCH_GROUPBY   # no starvation
+    q.pop()
+    assert S.next_kind(q, "short_first", 1.0, 4.0) == N.BATCH_JOIN
+    assert S.next_kind(deque(), "short_first", 1.0, 4.0) is None
