@@ -457,10 +457,10 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     for r in (r_in_place, r_gather):
         assert r["match_count"] == rs[0]["match_count"] and r["sum_exact"] == rs[0]["sum_exact"]
     # Gather form: the build keys of qualifying rows are still read in place;
-    # the matching rows' (price, discount) records are copied in (16 B each),
+    # the matching rows' (price, discount) records are copied in (8 B each),
     # and the probe writes each match's row index (4 B) to pinned host memory.
     zero_copy = 4 * e2e_res["build_rows"]
-    h2d_gather = h2d + 16 * e2e_res["match_count"]
+    h2d_gather = h2d + 8 * e2e_res["match_count"]
     d2h_gather = 4 * e2e_res["match_count"]
     pc.close()
 
@@ -526,7 +526,7 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
                             "bo_join_stream_host_async (build date/segment and probe fk copied, fk in 1M-row chunks "
                             "overlapped with the probe; keys of qualifying build rows read in place over PCIe, "
                             "counted in zero_copy_read_bytes_per_step; the probe lists each chunk's matching rows "
-                            "in pinned host memory, host_threads threads gather their price/discount into 16-byte "
+                            "in pinned host memory, host_threads threads gather their price/discount into 8-byte "
                             "records, one copy per chunk feeds a summing kernel -- list and records counted in "
                             "d2h/h2d_bytes_per_step; result copied to pinned host memory); queries pipelined, one "
                             "synchronise per run",

@@ -74,6 +74,17 @@ __device__ __forceinline__ int8v ld_stream_v8(const void* p) {
                : "l"(p));
   return r;
 }
+// The same 256-bit streaming load, marked evict-first in L2: for a column
+// scanned once alongside lookups into structures that should stay in L2 (hash
+// tables, bitmaps, filters), so the stream does not push them out.
+__device__ __forceinline__ int8v ld_first_v8(const void* p) {
+  int8v r;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::evict_first.v8.s32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]),
+                 "=r"(r.v[6]), "=r"(r.v[7])
+               : "l"(p));
+  return r;
+}
 struct long4v {
   long long v[4];
 };

@@ -15,8 +15,8 @@
 //   cfilter  C rows -> exact pass bitmap (one 32-row word per thread, no
 //            atomics) and the passing ids into a 64 KB blocked Bloom filter;
 //   amask    A ids -> bitmap over [0, a_id_max];
-//   scan     B streamed 16 rows per lane (256-bit c_id loads); the Bloom filter
-//            (TMA-staged into shared memory) rejects ~97% of rows without
+//   scan     B streamed 16 rows per lane (256-bit c_id loads, L2 evict-first);
+//            the Bloom filter (read through L1) rejects ~97% of rows without
 //            leaving the SM; hits are compacted per warp, checked against the
 //            exact bitmap and the A mask, and only survivors load their a_id
 //            and the C year (late materialisation).  Survivors aggregate first
@@ -235,34 +235,24 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
                                                            unsigned long long* slots, int32_t* mins, uint32_t* dbits,
                                                            GbMeta* meta, uint64_t probe_limit, GbParts parts,
                                                            uint32_t* err) {
-  extern __shared__ __align__(128) uint32_t bloom_s[];
-  __shared__ __align__(8) uint64_t bar;
   __shared__ int32_t q_c[kGbWarps][kGbQueue];
   __shared__ uint32_t q_row[kGbWarps][kGbQueue];
   __shared__ uint32_t l_key[kGbLocalSlots];
   __shared__ uint32_t l_cnt[kGbLocalSlots];
   __shared__ int32_t l_min[kGbLocalSlots];
   __shared__ uint32_t red[3][kGbWarps];
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    mbar_arrive_expect_tx(&bar, kGbBloomBytes);
-    bulk_copy_g2s(bloom_s, bloom_g, kGbBloomBytes, &bar);
-  }
   for (int i = threadIdx.x; i < kGbLocalSlots; i += blockDim.x) {
     l_key[i] = 0xffffffffu;
     l_cnt[i] = 0;
     l_min[i] = 0x7fffffff;
   }
   __syncthreads();
-  // On a (never expected) timeout the filter is not used; the exact bitmap
-  // check below still decides, so the answer is unchanged.
-  const bool use_bloom = mbar_wait_bounded(&bar, 0, kWaitLimitNs);
-  uint32_t bad = use_bloom ? 0u : kErrSpinTimeout;
-  __shared__ uint32_t all_ones;
-  if (threadIdx.x == 0) all_ones = 0xffffffffu;
-  __syncthreads();
-  const uint32_t* bl = use_bloom ? bloom_s : &all_ones;
-  const uint32_t wmask = use_bloom ? (kGbBloomWords - 1u) : 0u;
+  uint32_t bad = 0;
+  // The Bloom filter is read through L1 (64 KB, shared by the SM's CTAs) rather
+  // than copied into every CTA's shared memory: registers then allow 3 CTAs
+  // per SM instead of 2 (measured ~8% faster per query than the staged copy).
+  const uint32_t* bl = bloom_g;
+  const uint32_t wmask = kGbBloomWords - 1u;
   const int32_t cl = kMode ? __ldg(&meta->cap_log2) : 0;
   const uint64_t mask = (1ull << cl) - 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -280,7 +270,7 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
     vmask = 0;
     if (st >= steps) return;
     if (r0 + kGbRowsPerLane <= n) {
-      const int8v c0 = ld_stream_v8(b.c_id + r0), c1 = ld_stream_v8(b.c_id + r0 + 8);
+      const int8v c0 = ld_first_v8(b.c_id + r0), c1 = ld_first_v8(b.c_id + r0 + 8);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         out[k] = c0.v[k];
@@ -409,7 +399,7 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
 #pragma unroll
     for (int k = kGbRowsPerLane - 1; k >= 0; --k) {
       const uint32_t h = (uint32_t)cid[k] * 0x9E3779B1u;
-      const uint32_t x = bl[(h >> (32 - kGbBloomLog2Words)) & wmask];
+      const uint32_t x = __ldg(bl + ((h >> (32 - kGbBloomLog2Words)) & wmask));
       hit = (hit << 1) | (__funnelshift_r(x, x, h) & __funnelshift_r(x, x, h >> 5) & 1u);
     }
     hit &= valid;
@@ -456,7 +446,6 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
         if (!parts.put(atomicAdd(parts.cursor, 1u), l_key[i], l_cnt[i], l_min[i])) full = 1;
     }
   }
-  if (!use_bloom) mbar_wait_bounded(&bar, 0, kWaitLimitNs);
   if (bad) raise_error(err, bad);
   const uint32_t wj = warp_sum_u32(joined), wn = warp_sum_u32(newkeys);
   const unsigned wf = __any_sync(0xffffffffu, full != 0);
@@ -871,13 +860,8 @@ template <int kMode>
 int gb_launch_scan(bo_ctx* ctx, const bo_gb_b_cols& b, const bo_gb_c_cols& c, const bo_gb_params& prm,
                    const GbWs& ws, uint64_t probe_limit = ~0ull, GbParts parts = GbParts{}) {
   const void* k = reinterpret_cast<const void*>(&gb_scan_kernel<kMode>);
-  static bool ready = false;
-  if (!ready) {
-    BO_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGbBloomBytes));
-    ready = true;
-  }
-  const int grid = grid_res(ctx, k, kGbBlock, kGbBloomBytes, (b.n_rows + kGbRowsPerLane - 1) / kGbRowsPerLane);
-  gb_scan_kernel<kMode><<<grid, kGbBlock, kGbBloomBytes, ctx->stream>>>(
+  const int grid = grid_res(ctx, k, kGbBlock, 0, (b.n_rows + kGbRowsPerLane - 1) / kGbRowsPerLane);
+  gb_scan_kernel<kMode><<<grid, kGbBlock, 0, ctx->stream>>>(
       b, c.n_rows, prm.a_id_max, ws.bloom, ws.cbits, c.year, prm.a_mask ? prm.a_mask : ws.amask, ws.slots, ws.mins,
       ws.dbits, ws.meta, probe_limit, parts, ctx->d_err);
   return after_launch(ctx, "gb_scan_kernel");

@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(kJoinBlock, 2) join_probe_kernel(bo_join_probe
     int32_t fk[kRowsPerLane];
     uint32_t valid = 0xffu;
     if (r0 + kRowsPerLane <= n) {
-      const int8v f0 = ld_stream_v8(p.fk + r0);
+      const int8v f0 = ld_first_v8(p.fk + r0);  // the table and payload lookups keep L2
 #pragma unroll
       for (int k = 0; k < kRowsPerLane; ++k) fk[k] = f0.v[k];
     } else {
@@ -503,7 +503,7 @@ struct GatherAcc {
 
 constexpr int kGatherBlock = 256;
 
-__global__ void __launch_bounds__(kGatherBlock) join_gather_sum_kernel(const longlong2* __restrict__ rec,
+__global__ void __launch_bounds__(kGatherBlock) join_gather_sum_kernel(const uint2* __restrict__ rec,
                                                                        const uint32_t* __restrict__ mult, int64_t n,
                                                                        GatherAcc* ga, bo_join_result* part,
                                                                        uint32_t* err) {
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(kGatherBlock) join_gather_sum_kernel(const lon
   ProbeAcc a;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const longlong2 r = __ldcs(rec + i);
+    const uint2 r = __ldcs(rec + i);
     accumulate_match((uint64_t)r.x, (uint64_t)r.y, __ldcs(mult + i), a);
   }
   if (a.bad) raise_error(err, a.bad);
@@ -879,11 +879,11 @@ struct GatherState {
   cudaStream_t stream = nullptr;
   GatherSet set[2];
   int64_t rows_cap = 0, chunk_cap = 0;  // per set
-  longlong2* rec_h[kGatherRing] = {};   // pinned staging, kStreamChunkRows records each
+  uint2* rec_h[kGatherRing] = {};       // pinned staging, kStreamChunkRows records each
   cudaEvent_t rec_ev[kGatherRing] = {};  // the copy out of rec_h[i] has finished
   bool rec_busy[kGatherRing] = {};
   int next_rec = 0;
-  longlong2* rec_d = nullptr;  // kGatherRing x kStreamChunkRows records
+  uint2* rec_d = nullptr;  // kGatherRing x kStreamChunkRows records
   GatherAcc* acc = nullptr;
 };
 
@@ -929,11 +929,11 @@ int gather_state(bo_ctx* ctx, GatherState** out) {
     auto init = [&]() -> int {
       BO_CUDA(ctx, cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
       for (int i = 0; i < kGatherRing; ++i) {
-        BO_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&g->rec_h[i]), sizeof(longlong2) * kStreamChunkRows,
+        BO_CUDA(ctx, cudaHostAlloc(reinterpret_cast<void**>(&g->rec_h[i]), sizeof(uint2) * kStreamChunkRows,
                                    cudaHostAllocDefault));
         BO_CUDA(ctx, cudaEventCreateWithFlags(&g->rec_ev[i], cudaEventDisableTiming));
       }
-      BO_CUDA(ctx, cudaMalloc(&g->rec_d, sizeof(longlong2) * kStreamChunkRows * kGatherRing));
+      BO_CUDA(ctx, cudaMalloc(&g->rec_d, sizeof(uint2) * kStreamChunkRows * kGatherRing));
       BO_CUDA(ctx, cudaMalloc(&g->acc, sizeof(GatherAcc)));
       BO_CUDA(ctx, cudaMemset(g->acc, 0, sizeof(GatherAcc)));
       return BO_OK;
@@ -976,7 +976,7 @@ int gather_reserve(bo_ctx* ctx, GatherState* g, int64_t np, int64_t chunks) {
 // (price, discount) of the listed rows [b, e) into records; the rows of one
 // warp's appends are close together, so prefetching a few entries ahead keeps
 // several cache misses in flight per thread.
-void gather_rows(const uint32_t* rows, const int64_t* price, const int64_t* disc, longlong2* out, int64_t b,
+void gather_rows(const uint32_t* rows, const int64_t* price, const int64_t* disc, uint2* out, int64_t b,
                  int64_t e) {
   constexpr int64_t kAhead = 16;
   for (int64_t i = b; i < e; ++i) {
@@ -986,8 +986,12 @@ void gather_rows(const uint32_t* rows, const int64_t* price, const int64_t* disc
       __builtin_prefetch(disc + ra);
     }
     const uint32_t r = rows[i];
-    out[i].x = price[r];
-    out[i].y = disc[r];
+    const int64_t pv = price[r], dv = disc[r];
+    // 4 + 4 bytes: the exact-arithmetic contract (0 <= price < 2^31, 0 <=
+    // discount <= 100) fits; a value outside it becomes a price the summing
+    // kernel rejects (a data error, as in the in-place form).
+    const bool ok = pv >= 0 && pv < 0x80000000ll && dv >= 0 && dv <= 100;
+    out[i] = make_uint2(ok ? (uint32_t)pv : 0xffffffffu, ok ? (uint32_t)dv : 0u);
   }
 }
 
@@ -1068,10 +1072,10 @@ int stream_compute_gather(bo_ctx* ctx, GatherState* g, const bo_join_build_cols*
         const uint32_t* rows = rows_h + lo;
         const int64_t* pr = price_h + lo;
         const int64_t* dc = disc_h + lo;
-        longlong2* out = G.rec_h[slot];
+        uint2* out = G.rec_h[slot];
         G.pool.parallel_for((int64_t)n, [&](int64_t b0, int64_t e0) { gather_rows(rows, pr, dc, out, b0, e0); });
-        longlong2* rec = G.rec_d + (size_t)slot * kStreamChunkRows;
-        if ((e = cudaMemcpyAsync(rec, out, sizeof(longlong2) * n, cudaMemcpyHostToDevice, G.stream)) != cudaSuccess)
+        uint2* rec = G.rec_d + (size_t)slot * kStreamChunkRows;
+        if ((e = cudaMemcpyAsync(rec, out, sizeof(uint2) * n, cudaMemcpyHostToDevice, G.stream)) != cudaSuccess)
           return fail(e, "copying gathered records");
         if ((e = cudaEventRecord(G.rec_ev[slot], G.stream)) != cudaSuccess) return fail(e, "recording a copy");
         G.rec_busy[slot] = true;

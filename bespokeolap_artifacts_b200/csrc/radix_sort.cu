@@ -437,6 +437,10 @@ __global__ void __launch_bounds__(kCsBlock, 1) cluster_sort_kernel(unsigned long
   cl.sync();  // every CTA runs (and has loaded) before any pair moves between them
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt_mask = (1u << lane) - 1u;
+  // Warp segments of `seg` pairs (a multiple of 32, the same in every CTA):
+  // only as many rounds as the CTA's pairs need.
+  const uint32_t seg = ((S + kCsWarps * 32 - 1) / (kCsWarps * 32)) * 32;
+  const int rounds = (int)(seg / 32);
   int src = 0;
   for (int shift = begin_bit; shift < end_bit; shift += 8) {
     const uint32_t dmask = (1u << min(8, end_bit - shift)) - 1u;
@@ -448,7 +452,10 @@ __global__ void __launch_bounds__(kCsBlock, 1) cluster_sort_kernel(unsigned long
     uint32_t rank[kCsRounds], dig[kCsRounds];
 #pragma unroll
     for (int r = 0; r < kCsRounds; ++r) {
-      const uint32_t idx = (uint32_t)warp * (32 * kCsRounds) + r * 32 + lane;
+      dig[r] = 0x100u;
+      rank[r] = 0;
+      if (r >= rounds) continue;  // the same for every lane of the warp
+      const uint32_t idx = (uint32_t)warp * seg + r * 32 + lane;
       const bool valid = idx < m;
       const uint32_t d = valid ? (uint32_t)((ks[idx] >> shift) & dmask) : 0x100u;
       dig[r] = d;
@@ -502,7 +509,7 @@ __global__ void __launch_bounds__(kCsBlock, 1) cluster_sort_kernel(unsigned long
       for (int r = 0; r < kCsRounds; ++r) {
         const uint32_t d = dig[r];
         if (d < 0x100u) {
-          const uint32_t idx = (uint32_t)warp * (32 * kCsRounds) + r * 32 + lane;
+          const uint32_t idx = (uint32_t)warp * seg + r * 32 + lane;
           const uint32_t pos = base[d] + warp_cnt[warp][d] + rank[r];
           const uint32_t q = pos / S, slot = pos - q * S;
           cl.map_shared_rank(kd, q)[slot] = ks[idx];

@@ -11,10 +11,11 @@
 //            a bit in a customer bitmap (the order's "non-zero" test is kept
 //            per order, as in the reference, so totals that cancel to zero
 //            still make a group);
-//   emit     customers with their bit set, a row and a nation (block-level
-//            reservations);
-//   sort     the onesweep radix sort twice, stable: by custkey, then by the
-//            complemented revenue (64 bits) -- the reference's own key order.
+//   emit     customers with their bit set, a row and a nation, in ascending
+//            custkey order (order-preserving compaction, compact.cuh) -- the
+//            order the reference's first sort, by custkey, produces;
+//   sort     one stable radix sort by the complemented revenue (64 bits), the
+//            reference's own key order (one cluster launch up to 64K rows).
 //
 // Q18 (run_q18, bespoke_tpch/query_q18.cpp:183-455).
 //   sum      sum_qty[orderkey] += l_quantity: each thread takes eight
@@ -30,6 +31,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "compact.cuh"
 #include "context.cuh"
 
 namespace bo {
@@ -124,33 +126,24 @@ __global__ void q10_orders_kernel(const int32_t* __restrict__ o_orderkey, const 
   }
 }
 
-// Customers with a non-zero order, a row and a nation -> (custkey, custkey).
-__global__ void __launch_bounds__(kTpBlock) q10_emit_kernel(const uint32_t* __restrict__ cust_hit, int64_t n_map,
-                                                            const int32_t* __restrict__ key_to_row,
-                                                            const int32_t* __restrict__ c_nationkey,
-                                                            int64_t n_customer, int32_t nation_bound,
-                                                            unsigned long long* __restrict__ keys,
-                                                            uint32_t* __restrict__ vals,
-                                                            unsigned long long* n_out) {
-  __shared__ uint32_t warp_off[kTpBlock / 32];
-  __shared__ unsigned long long base;
-  for (int64_t b0 = (int64_t)blockIdx.x * kTpBlock; b0 < n_map; b0 += (int64_t)gridDim.x * kTpBlock) {
-    const int64_t c = b0 + threadIdx.x;
-    bool keep = false;
-    if (c < n_map && ((cust_hit[c >> 5] >> (c & 31)) & 1u)) {
-      const int32_t row = key_to_row[c];
-      if (row >= 0 && (int64_t)row < n_customer) {
-        const int32_t nk = c_nationkey[row];
-        keep = nk >= 0 && nk < nation_bound;
-      }
-    }
-    const unsigned long long pos = block_reserve(keep, n_out, warp_off, &base);
-    if (keep) {
-      keys[pos] = (unsigned long long)c;
-      vals[pos] = (uint32_t)c;
-    }
+// Customers with revenue in the window, in ascending custkey order (the value
+// is the custkey): the order the reference's first LSD sort by custkey gives
+// (query_q10.cpp:318-345), so only the revenue sort remains.
+struct Q10Kept {
+  const uint32_t* hit;
+  const int32_t* key_to_row;
+  const int32_t* c_nationkey;
+  int64_t n_customer;
+  int32_t nation_bound;
+  __device__ __forceinline__ bool operator()(int64_t c, uint32_t& v) const {
+    if (!((__ldg(hit + (c >> 5)) >> (c & 31)) & 1u)) return false;
+    const int32_t row = __ldg(key_to_row + c);
+    if (row < 0 || (int64_t)row >= n_customer) return false;
+    const int32_t nk = __ldg(c_nationkey + row);
+    v = (uint32_t)c;
+    return nk >= 0 && nk < nation_bound;
   }
-}
+};
 
 // Revenue descending as an unsigned 64-bit value: the reference's ~revenue key.
 __global__ void q10_key2_kernel(const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ cust_rev,
@@ -161,9 +154,17 @@ __global__ void q10_key2_kernel(const uint32_t* __restrict__ vals, const unsigne
     keys[i] = ~cust_rev[vals[i]];
 }
 
+// Per customer row, the host's string offsets and balance (all null: not
+// gathered).
+struct Q10CustStrings {
+  const uint32_t* off[4];  // name, address, phone, comment
+  const int32_t* acctbal;
+};
+
 __global__ void q10_gather_kernel(const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ cust_rev,
                                   const int32_t* __restrict__ key_to_row, const int32_t* __restrict__ c_nationkey,
-                                  const unsigned long long* n_out, bo_tpch_q10_row* __restrict__ out) {
+                                  Q10CustStrings cs, const unsigned long long* n_out,
+                                  bo_tpch_q10_row* __restrict__ out) {
   const unsigned long long n = *n_out;
   for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (unsigned long long)gridDim.x * blockDim.x) {
@@ -174,7 +175,23 @@ __global__ void q10_gather_kernel(const uint32_t* __restrict__ vals, const unsig
     r.custkey = (int32_t)c;
     r.cust_row = row;
     r.nationkey = c_nationkey[row];
-    r.pad0 = 0;
+    r.acctbal_raw = cs.acctbal ? __ldg(cs.acctbal + row) : 0;
+    uint32_t b[4] = {0, 0, 0, 0}, l[4] = {0, 0, 0, 0};
+    if (cs.off[0]) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        b[k] = __ldg(cs.off[k] + row);
+        l[k] = __ldg(cs.off[k] + row + 1) - b[k];
+      }
+    }
+    r.name_begin = b[0];
+    r.name_len = l[0];
+    r.address_begin = b[1];
+    r.address_len = l[1];
+    r.phone_begin = b[2];
+    r.phone_len = l[2];
+    r.comment_begin = b[3];
+    r.comment_len = l[3];
     out[i] = r;
   }
 }
@@ -381,6 +398,11 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
       (t->n_lineitem > 0 && (!t->l_orderkey || !t->l_returnflag_linestatus || !t->l_discounted_price)) ||
       (t->n_custkey_map > 0 && !t->custkey_to_row) || (t->n_customer > 0 && !t->c_nationkey))
     return set_error(ctx, BO_ERR_INVALID, "q10: null column");
+  {
+    const bool any = t->c_name_offsets || t->c_address_offsets || t->c_phone_offsets || t->c_comment_offsets;
+    const bool all = t->c_name_offsets && t->c_address_offsets && t->c_phone_offsets && t->c_comment_offsets;
+    if (any && !all) return set_error(ctx, BO_ERR_INVALID, "q10: give all four string offset columns or none");
+  }
   *n_rows = 0;
   const int64_t nm = t->n_custkey_map;
   if (group_lo < 0 || t->n_orders == 0 || nm == 0 || t->n_lineitem == 0) return BO_OK;
@@ -394,6 +416,8 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
   add(8 * (size_t)nm);  // tmp keys
   add(4 * (size_t)nm);  // tmp vals
   add(sizeof(bo_tpch_q10_row) * (size_t)nm);
+  const int64_t tiles = (nm + kCompactTile - 1) / kCompactTile;
+  add(4 * (size_t)std::max<int64_t>(tiles, 1));  // ordered compaction's tile counts
   add(64);
   void* basep = nullptr;
   int rc = region(ctx, "q10_ws", total, &basep);
@@ -406,6 +430,7 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
   auto* tkeys = carve<unsigned long long>(p, (size_t)nm);
   auto* tvals = carve<uint32_t>(p, (size_t)nm);
   auto* rows = carve<bo_tpch_q10_row>(p, (size_t)nm);
+  auto* tile_counts = carve<uint32_t>(p, (size_t)std::max<int64_t>(tiles, 1));
   auto* n_out = carve<unsigned long long>(p, 8);
   BO_CUDA(ctx, cudaMemsetAsync(rev, 0, 8 * (size_t)nm, ctx->stream));
   BO_CUDA(ctx, cudaMemsetAsync(hit, 0, 4 * (size_t)hit_words, ctx->stream));
@@ -422,20 +447,21 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
         t->l_returnflag_linestatus, t->l_discounted_price, t->n_lineitem, start_offset, end_offset,
         (uint32_t)group_lo, (uint32_t)group_count, nm, rev, hit, ctx->d_err);
   if ((rc = after_launch(ctx, "q10_orders_kernel"))) return rc;
-  q10_emit_kernel<<<grid_for(ctx, nm), kTpBlock, 0, ctx->stream>>>(hit, nm, t->custkey_to_row, t->c_nationkey,
-                                                                    t->n_customer, t->nation_bound, keys, vals,
-                                                                    n_out);
-  if ((rc = after_launch(ctx, "q10_emit_kernel"))) return rc;
+  // Customers with revenue, in ascending custkey order (no sort by custkey needed).
+  if ((rc = ordered_compact(ctx, Q10Kept{hit, t->custkey_to_row, t->c_nationkey, t->n_customer, t->nation_bound}, nm,
+                            tile_counts, vals, n_out)))
+    return rc;
   // The result's size, read back once: up to 64K rows sort in one cluster
-  // launch per key instead of a pass sequence sized for every customer.
+  // launch instead of a pass sequence sized for every customer.
   int64_t ns = 0;
   if ((rc = read_device_count(ctx, n_out, nm, &ns))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 32, nullptr))) return rc;
   q10_key2_kernel<<<grid_for(ctx, nm), kTpBlock, 0, ctx->stream>>>(vals, rev, n_out, keys);
   if ((rc = after_launch(ctx, "q10_key2_kernel"))) return rc;
   if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
-  q10_gather_kernel<<<grid_for(ctx, nm), kTpBlock, 0, ctx->stream>>>(vals, rev, t->custkey_to_row, t->c_nationkey,
-                                                                      n_out, rows);
+  const Q10CustStrings cs{{t->c_name_offsets, t->c_address_offsets, t->c_phone_offsets, t->c_comment_offsets},
+                          t->c_acctbal};
+  q10_gather_kernel<<<grid_for(ctx, std::max<int64_t>(ns, 1)), kTpBlock, 0, ctx->stream>>>(
+      vals, rev, t->custkey_to_row, t->c_nationkey, cs, n_out, rows);
   if ((rc = after_launch(ctx, "q10_gather_kernel"))) return rc;
   return finish_rows(ctx, "q10", n_out, rows, out_host, max_rows, n_rows);
 }

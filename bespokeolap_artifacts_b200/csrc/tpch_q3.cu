@@ -13,14 +13,17 @@
 //          bespoke_tpch/builder_impl.cpp:930-990) and, if that order
 //          qualifies, adds its discounted price and a count with 64-bit
 //          atomics (only the ~2% of lineitems that pass both filters do);
-//   compact orders with at least one such lineitem (`has_lineitem`, :248);
-//   sort   the onesweep radix sort twice, stable: by orderkey, then by
-//          (revenue desc, orderdate asc).  The reference's std::sort leaves
-//          rows equal in both keys in unspecified order; here they come out in
+//   compact orders with at least one such lineitem (`has_lineitem`, :248),
+//          visited through the orderkey map so they come out in ascending
+//          orderkey order (order-preserving compaction, compact.cuh);
+//   sort   one stable radix sort by (revenue desc, orderdate asc) -- one
+//          cluster launch up to 64K result rows.  The reference's std::sort
+//          leaves rows equal in both keys in unspecified order; here they keep
 //          orderkey order, a canonical form of the same result.
 #include <algorithm>
 
 #include "common.cuh"
+#include "compact.cuh"
 #include "context.cuh"
 
 namespace bo {
@@ -74,40 +77,6 @@ __global__ void q3_lineitem_kernel(const int32_t* __restrict__ l_orderkey, const
 }
 
 // Orders with a counted lineitem -> (orderkey, row) pairs; one reservation per block.
-__global__ void __launch_bounds__(kQ3Block) q3_compact_kernel(const uint32_t* __restrict__ cnt,
-                                                              const int32_t* __restrict__ o_orderkey, int64_t n,
-                                                              unsigned long long* __restrict__ keys,
-                                                              uint32_t* __restrict__ vals,
-                                                              unsigned long long* n_out) {
-  __shared__ uint32_t warp_off[kQ3Block / 32];
-  __shared__ unsigned long long base;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t b0 = (int64_t)blockIdx.x * kQ3Block; b0 < n; b0 += (int64_t)gridDim.x * kQ3Block) {
-    const int64_t i = b0 + threadIdx.x;
-    const bool keep = i < n && cnt[i] > 0u;
-    const uint32_t m = __ballot_sync(0xffffffffu, keep);
-    if (lane == 0) warp_off[warp] = __popc(m);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t t = 0;
-      for (int w = 0; w < kQ3Block / 32; ++w) {
-        const uint32_t c = warp_off[w];
-        warp_off[w] = t;
-        t += c;
-      }
-      base = t ? atomicAdd(n_out, (unsigned long long)t) : 0ull;
-    }
-    __syncthreads();
-    if (keep) {
-      const unsigned long long pos = base + warp_off[warp] + __popc(m & ((1u << lane) - 1u));
-      keys[pos] = (unsigned long long)(uint32_t)o_orderkey[i];  // orderkey >= 0: it indexed the map
-      vals[pos] = (uint32_t)i;
-    }
-    __syncthreads();
-  }
-}
-
-// Second sort key in orderkey order: (2^47 - 1 - revenue) << 16 | (orderdate + 32768).
 __global__ void q3_key2_kernel(const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ rev,
                                const int16_t* __restrict__ o_orderdate, const unsigned long long* n_out,
                                unsigned long long* __restrict__ keys, uint32_t* err) {
@@ -140,6 +109,81 @@ __global__ void q3_gather_kernel(const uint32_t* __restrict__ vals, const unsign
     out[i] = r;
   }
 }
+
+// The lineitem pass, 8 rows per thread per step: one 16-byte load of 8
+// shipdates, and for a step with any row past the date one 32-byte pair of
+// orderkey loads; the map lookups of the passing rows are all issued before
+// any is used (independent loads in flight), then the qualification bits,
+// then the atomics.  Columns 16-byte aligned (checked by the caller); the
+// last n % 8 rows go through the scalar loop.
+__global__ void __launch_bounds__(kQ3Block) q3_lineitem_v8_kernel(
+    const int32_t* __restrict__ l_orderkey, const int16_t* __restrict__ l_shipdate,
+    const int32_t* __restrict__ l_dprice, int64_t n, int16_t date_offset, const int32_t* __restrict__ key_to_row,
+    int64_t n_map, int64_t n_orders, const uint32_t* __restrict__ qual, unsigned long long* __restrict__ rev,
+    uint32_t* __restrict__ cnt) {
+  const int64_t chunks = n >> 3;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t c = tid; c < chunks; c += stride) {
+    const int64_t r0 = c << 3;
+    const int4 sd = ld_stream_v4(l_shipdate + r0);
+    const uint32_t sw[4] = {(uint32_t)sd.x, (uint32_t)sd.y, (uint32_t)sd.z, (uint32_t)sd.w};
+    uint32_t pass = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int16_t d = (int16_t)((sw[k >> 1] >> (16 * (k & 1))) & 0xffffu);
+      pass |= (uint32_t)(d > date_offset) << k;
+    }
+    if (!pass) continue;
+    const int4 k0 = ld_stream_v4(l_orderkey + r0), k1 = ld_stream_v4(l_orderkey + r0 + 4);
+    const int32_t key[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+    int32_t row[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      row[k] = -1;
+      if (((pass >> k) & 1u) && key[k] >= 0 && (int64_t)key[k] < n_map) row[k] = __ldg(key_to_row + key[k]);
+    }
+    uint32_t word[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const bool in = row[k] >= 0 && (int64_t)row[k] < n_orders;
+      word[k] = in ? __ldg(qual + (row[k] >> 5)) : 0u;
+      if (!in) row[k] = -1;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (row[k] < 0 || !((word[k] >> (row[k] & 31)) & 1u)) continue;
+      atomicAdd(rev + row[k], (unsigned long long)(int64_t)__ldg(l_dprice + r0 + k));
+      atomicAdd(cnt + row[k], 1u);
+    }
+  }
+  for (int64_t i = (chunks << 3) + tid; i < n; i += stride) {
+    if (l_shipdate[i] <= date_offset) continue;
+    const int32_t key = l_orderkey[i];
+    if (key < 0 || (int64_t)key >= n_map) continue;
+    const int32_t row = key_to_row[key];
+    if (row < 0 || (int64_t)row >= n_orders) continue;
+    if (!((qual[row >> 5] >> (row & 31)) & 1u)) continue;
+    atomicAdd(rev + row, (unsigned long long)(int64_t)l_dprice[i]);
+    atomicAdd(cnt + row, 1u);
+  }
+}
+
+// Orders that got revenue, visited in ascending orderkey order through the
+// orderkey -> row map (the value is the order's row): the result rows then
+// need one sort only, whose ties keep this order (query_q3.cpp:348-355 breaks
+// them by orderkey).
+struct Q3Kept {
+  const int32_t* map;
+  int64_t n_orders;
+  const uint32_t* cnt;
+  __device__ __forceinline__ bool operator()(int64_t key, uint32_t& row) const {
+    const int32_t r = __ldg(map + key);
+    if (r < 0 || (int64_t)r >= n_orders) return false;
+    row = (uint32_t)r;
+    return __ldg(cnt + r) > 0u;
+  }
+};
 
 int grid_of(bo_ctx* ctx, int64_t items) {
   const int64_t need = (items + kQ3Block - 1) / kQ3Block;
@@ -180,6 +224,8 @@ extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_
   add(8 * (size_t)no);  // tmp keys
   add(4 * (size_t)no);  // tmp vals
   add(sizeof(bo_tpch_q3_row) * (size_t)no);
+  const int64_t tiles = (t->n_orderkey_map + kCompactTile - 1) / kCompactTile;
+  add(4 * (size_t)std::max<int64_t>(tiles, 1));  // ordered compaction's tile counts
   add(64);
   void* base = nullptr;
   int rc = region(ctx, "q3_ws", total, &base);
@@ -194,6 +240,7 @@ extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_
   unsigned long long* tkeys = carve<unsigned long long>(p, (size_t)no);
   uint32_t* tvals = carve<uint32_t>(p, (size_t)no);
   bo_tpch_q3_row* rows = carve<bo_tpch_q3_row>(p, (size_t)no);
+  uint32_t* tile_counts = carve<uint32_t>(p, (size_t)std::max<int64_t>(tiles, 1));
   unsigned long long* n_out = carve<unsigned long long>(p, 8);
   // Scratch that accumulates starts at zero (the bitmaps are written whole or by atomicOr).
   BO_CUDA(ctx, cudaMemsetAsync(mask, 0, 4 * (size_t)mask_words, ctx->stream));
@@ -209,18 +256,25 @@ extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_
                                                                      t->custkey_bound, mask, qual);
   if ((rc = after_launch(ctx, "q3_orders_kernel"))) return rc;
   if (t->n_lineitem > 0 && t->n_orderkey_map > 0) {
-    q3_lineitem_kernel<<<grid_of(ctx, t->n_lineitem), kQ3Block, 0, ctx->stream>>>(
-        t->l_orderkey, t->l_shipdate, t->l_discounted_price, t->n_lineitem, date_offset, t->orderkey_to_row,
-        t->n_orderkey_map, no, qual, rev, cnt);
-    if ((rc = after_launch(ctx, "q3_lineitem_kernel"))) return rc;
+    if (aligned16(t->l_orderkey) && aligned16(t->l_shipdate)) {
+      q3_lineitem_v8_kernel<<<grid_of(ctx, (t->n_lineitem + 7) / 8), kQ3Block, 0, ctx->stream>>>(
+          t->l_orderkey, t->l_shipdate, t->l_discounted_price, t->n_lineitem, date_offset, t->orderkey_to_row,
+          t->n_orderkey_map, no, qual, rev, cnt);
+      if ((rc = after_launch(ctx, "q3_lineitem_v8_kernel"))) return rc;
+    } else {
+      q3_lineitem_kernel<<<grid_of(ctx, t->n_lineitem), kQ3Block, 0, ctx->stream>>>(
+          t->l_orderkey, t->l_shipdate, t->l_discounted_price, t->n_lineitem, date_offset, t->orderkey_to_row,
+          t->n_orderkey_map, no, qual, rev, cnt);
+      if ((rc = after_launch(ctx, "q3_lineitem_kernel"))) return rc;
+    }
   }
-  q3_compact_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(cnt, t->o_orderkey, no, keys, vals, n_out);
-  if ((rc = after_launch(ctx, "q3_compact_kernel"))) return rc;
+  // Qualifying orders in ascending orderkey order (no sort by orderkey needed).
+  if ((rc = ordered_compact(ctx, Q3Kept{t->orderkey_to_row, no, cnt}, t->n_orderkey_map, tile_counts, vals, n_out)))
+    return rc;
   // The result's size, read back once: up to 64K rows sort in one cluster
-  // launch per key instead of a pass sequence sized for every order.
+  // launch instead of a pass sequence sized for every order.
   int64_t ns = 0;
   if ((rc = read_device_count(ctx, n_out, no, &ns))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 32, nullptr))) return rc;
   q3_key2_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(vals, rev, t->o_orderdate, n_out, keys,
                                                                    ctx->d_err);
   if ((rc = after_launch(ctx, "q3_key2_kernel"))) return rc;

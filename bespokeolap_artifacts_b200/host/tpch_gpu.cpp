@@ -8,6 +8,8 @@
 #include <arrow/io/file.h>
 #include <parquet/arrow/reader.h>
 
+#include <malloc.h>
+
 #include <algorithm>
 #include <array>
 #include <charconv>
@@ -465,7 +467,7 @@ std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, 
   return rows;
 }
 
-std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date) {
+Q10Rows run_q10(const Database& db, const std::string& date) {
   const int16_t start = date_offset_of(date, db.base_date_days);
   const int16_t end = date_offset_of(date, db.base_date_days, 3);
   int32_t rf = -1;
@@ -493,26 +495,37 @@ std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date) {
   t.n_custkey_map = db.n_custkey_map;
   t.c_nationkey = col<int32_t>(db.c_nationkey);
   t.n_customer = db.n_customer;
+  t.c_name_offsets = col<uint32_t>(db.c_name_offsets);
+  t.c_address_offsets = col<uint32_t>(db.c_address_offsets);
+  t.c_phone_offsets = col<uint32_t>(db.c_phone_offsets);
+  t.c_comment_offsets = col<uint32_t>(db.c_comment_offsets);
+  t.c_acctbal = col<int32_t>(db.c_acctbal_device);
   QueryTrace trace("q10");
   bo_tpch_q10_row* out = result_rows<bo_tpch_q10_row>(db, db.n_custkey_map);
   int64_t n = 0;
   check(db.ctx, bo_tpch_q10(db.ctx, &t, start, end, rf * ls_count, ls_count, out, db.n_custkey_map, &n),
         "q10");
   trace.mark("gpu");
-  std::vector<Q10ResultRow> rows(static_cast<size_t>(n));
+  // Every field of every row is written below (RowAlloc leaves them unset);
+  // the GPU gathered each customer's string ranges and balance, so this loop
+  // reads the records in order and touches no customer data of its own.
+  Q10Rows rows(static_cast<size_t>(n));
+  const char* name = db.c_name.data.data();
+  const char* address = db.c_address.data.data();
+  const char* phone = db.c_phone.data.data();
+  const char* comment = db.c_comment.data.data();
   for_row_ranges(n, [&](int64_t lo, int64_t hi) {
     for (int64_t i = lo; i < hi; ++i) {
       const auto& g = out[i];
-      const size_t r = static_cast<size_t>(g.cust_row);
       auto& row = rows[i];
       row.custkey = g.custkey;
-      row.name = db.c_name.view(r);
+      row.name = std::string_view(name + g.name_begin, g.name_len);
       row.revenue_raw = g.revenue_raw;
-      row.acctbal_raw = db.c_acctbal[r];
+      row.acctbal_raw = g.acctbal_raw;
       row.nation_name = db.nation_name[static_cast<size_t>(g.nationkey)];
-      row.address = db.c_address.view(r);
-      row.phone = db.c_phone.view(r);
-      row.comment = db.c_comment.view(r);
+      row.address = std::string_view(address + g.address_begin, g.address_len);
+      row.phone = std::string_view(phone + g.phone_begin, g.phone_len);
+      row.comment = std::string_view(comment + g.comment_begin, g.comment_len);
     }
   });
   trace.mark("rows");
@@ -1254,7 +1267,7 @@ void write_q3_csv(const Database& db, const std::string& filename, const std::ve
 }
 
 
-void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows) {
+void write_q10_csv(const std::string& filename, const Q10Rows& rows) {
   std::ofstream out(filename, std::ios::binary);
   std::string buf;
   buf.reserve(1 << 20);
@@ -1437,7 +1450,8 @@ Database::~Database() {
                           &c_phone_prefix, &c_phone_pair, &o_has_order, &ps_partkey, &ps_suppkey, &ps_value,
                           &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch, &p_name,
                           &p_name_offsets, &ps_supplycost, &ps_part_begin, &o_year_by_key, &l_shipinstruct,
-                          &p_size, &p_row_by_key, &o_orderstatus};
+                          &p_size, &p_row_by_key, &o_orderstatus, &c_name_offsets, &c_address_offsets,
+                          &c_phone_offsets, &c_comment_offsets};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
   if (result_host) bo_host_free_pinned(ctx, result_host);
@@ -1763,6 +1777,13 @@ PartHost derive_part(const ParquetTables::ArrowTable& P) {
 
 Database* build(ParquetTables* tables) {
   const auto t0 = std::chrono::steady_clock::now();
+  // A query's result rows are one std::vector of a few MB (Q10: ~100 bytes per
+  // customer of the result).  Above glibc's default mmap threshold each such
+  // vector is a fresh mapping, so every query would pay a page fault per 4 KB
+  // of rows (0.8 ms of Q10's 1.1 ms at 38k rows); kept on the heap below 256 MB
+  // and not trimmed, they reuse pages already faulted in by earlier queries.
+  mallopt(M_MMAP_THRESHOLD, 256 << 20);
+  mallopt(M_TRIM_THRESHOLD, 1 << 30);
   // BO_BUILD_TRACE set: the phases' end times (ms since build() began) on stderr.
   const bool trace = std::getenv("BO_BUILD_TRACE") != nullptr;
   auto phase = [&](const char* name) {
@@ -1903,6 +1924,10 @@ Database* build(ParquetTables* tables) {
       db->c_phone_prefix = upload(ctx, prefix);
       db->c_phone_pair = upload(ctx, pair);
       db->c_acctbal_device = upload(ctx, h.acctbal);
+      db->c_name_offsets = upload(ctx, h.name.offsets);
+      db->c_address_offsets = upload(ctx, h.address.offsets);
+      db->c_phone_offsets = upload(ctx, h.phone.offsets);
+      db->c_comment_offsets = upload(ctx, h.comment.offsets);
       db->c_acctbal = std::move(h.acctbal);
       db->c_name = std::move(h.name);
       db->c_address = std::move(h.address);

@@ -22,6 +22,7 @@
 #include <memory>
 #include <string>
 #include <unordered_map>
+#include <utility>
 #include <string_view>
 #include <vector>
 
@@ -103,6 +104,8 @@ struct Database {
   bo_tpch::DeviceColumn c_acctbal_device, c_phone_prefix, c_phone_pair, o_has_order;
   int64_t n_order_custkeys = 0;
   bo_tpch::StringColumn c_name, c_address, c_phone, c_comment;
+  // their offsets on the device (Q10 result rows carry each customer's ranges)
+  bo_tpch::DeviceColumn c_name_offsets, c_address_offsets, c_phone_offsets, c_comment_offsets;
   // part: per partkey 1 (PROMO type), 0 (other type), -1 (no part row); the
   // largest partkey (-1 without parts)
   bo_tpch::DeviceColumn p_promo_by_key;
@@ -252,6 +255,27 @@ struct Q13ResultRow {
   int64_t custdist = 0;
 };
 
+// Allocator that leaves elements default-constructed as nothing: for result
+// rows every field of which the query writes in parallel right after the
+// allocation (a value-initialising std::vector would first write the whole
+// buffer on one thread).  For implicit-lifetime row types only.
+template <class T>
+struct RowAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = RowAlloc<U>;
+  };
+  RowAlloc() = default;
+  template <class U>
+  RowAlloc(const RowAlloc<U>&) noexcept {}
+  template <class U>
+  void construct(U*) noexcept {}
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+
 struct Q10ResultRow {
   int32_t custkey = 0;
   std::string_view name;
@@ -284,7 +308,8 @@ std::vector<Q1ResultRow> run_q1(const Database& db, const std::string& delta);
 std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, const std::string& date);
 std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, const std::string& discount,
                                 const std::string& quantity);
-std::vector<Q10ResultRow> run_q10(const Database& db, const std::string& date);
+using Q10Rows = std::vector<Q10ResultRow, RowAlloc<Q10ResultRow>>;
+Q10Rows run_q10(const Database& db, const std::string& date);
 std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date);
 std::vector<Q5ResultRow> run_q5(const Database& db, const std::string& region, const std::string& date);
 std::vector<Q7ResultRow> run_q7(const Database& db, const std::string& nation1, const std::string& nation2);
@@ -306,7 +331,7 @@ std::vector<Q18ResultRow> run_q18(const Database& db, const std::string& quantit
 void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& rows);
 void write_q3_csv(const Database& db, const std::string& filename, const std::vector<Q3ResultRow>& rows);
 void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& rows);
-void write_q10_csv(const std::string& filename, const std::vector<Q10ResultRow>& rows);
+void write_q10_csv(const std::string& filename, const Q10Rows& rows);
 void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& rows);
 void write_q5_csv(const std::string& filename, const std::vector<Q5ResultRow>& rows);
 void write_q7_csv(const std::string& filename, const std::vector<Q7ResultRow>& rows);

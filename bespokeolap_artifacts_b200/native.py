@@ -194,12 +194,16 @@ class TpchQ10Tables(C.Structure):
                 ("l_discounted_price", C.c_void_p), ("n_lineitem", C.c_int64),
                 ("lineitem_orderkey_sorted", C.c_int32), ("nation_bound", C.c_int32),
                 ("custkey_to_row", C.c_void_p), ("n_custkey_map", C.c_int64), ("c_nationkey", C.c_void_p),
-                ("n_customer", C.c_int64)]
+                ("n_customer", C.c_int64), ("c_name_offsets", C.c_void_p), ("c_address_offsets", C.c_void_p),
+                ("c_phone_offsets", C.c_void_p), ("c_comment_offsets", C.c_void_p), ("c_acctbal", C.c_void_p)]
 
 
 class TpchQ10Row(C.Structure):
     _fields_ = [("revenue_raw", C.c_int64), ("custkey", C.c_int32), ("cust_row", C.c_int32),
-                ("nationkey", C.c_int32), ("pad0", C.c_int32)]
+                ("nationkey", C.c_int32), ("acctbal_raw", C.c_int32),
+                ("name_begin", C.c_uint32), ("name_len", C.c_uint32), ("address_begin", C.c_uint32),
+                ("address_len", C.c_uint32), ("phone_begin", C.c_uint32), ("phone_len", C.c_uint32),
+                ("comment_begin", C.c_uint32), ("comment_len", C.c_uint32)]
 
 
 class TpchQ18Tables(C.Structure):

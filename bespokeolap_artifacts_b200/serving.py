@@ -216,8 +216,11 @@ class Slot:
     gb_pred_d: object = None
     event: object = None                # recorded after the slot's last launch
     q1_out: object = None               # device groups of a lone scan-agg request
-    pred_h: object = None               # pinned / device prediction of a lone join request
+    pred_h: object = None               # pinned / device table size of a lone join request
     pred_d: object = None
+    cnt_d: object = None                # a lone join's exact qualifying-row count (device, pinned host)
+    cnt_h: object = None
+    phase: str = "run"                  # "count": a lone join's count is in flight, its join not yet launched
     reqs: list = field(default_factory=list)
     joins: list = field(default_factory=list)
     gbs: list = field(default_factory=list)
@@ -237,19 +240,23 @@ class BatchedServer:
     exactly), and the scan-agg requests run as instances of the slot's
     persistent batch kernel -- all on the slot's stream, one event at the
     end.  A request that finds an idle slot with nothing else waiting runs
-    alone through its standalone kernel (scan-agg) or the presized join.
+    alone through its standalone kernel (scan-agg) or the join sized from an
+    exact count (count kernel, then the presized pipeline, no host wait).
     With shared=False every request is a batch instance.
 
     Admission policy: "fifo" takes waiting requests in arrival order, kinds
     mixed; "short_first" fills a free slot with requests of one kind only,
     the shortest kind waiting first (scan-agg, join, group-by), unless the
     oldest request has waited max_wait_ms, so that a short request neither
-    waits behind nor completes with a long one in the same slot."""
+    waits behind nor completes with a long one in the same slot.  Spill: with
+    a slot running, an idle one starts only once spill_queue requests wait or
+    the oldest has waited spill_wait_ms."""
 
     def __init__(self, tables: ServingTables, n_slots: int = 2, max_batch: int = 16,
                  pool_bytes: int = 2 << 30, max_items: int = 65536, workers_per_sm: int = 1,
                  join_sizer=None, gb_sizer=None, tile_table: B.TileTable | None = None, shared: bool = True,
-                 policy: str = "fifo", max_wait_ms: float = 4.0):
+                 policy: str = "fifo", max_wait_ms: float = 4.0, spill_queue: int = 1,
+                 spill_wait_ms: float = 1.0):
         import torch
 
         from .engine import Engine
@@ -262,6 +269,12 @@ class BatchedServer:
         if policy not in ("fifo", "short_first"):
             raise ValueError(f"unknown admission policy {policy!r}")
         self.policy, self.max_wait_ms = policy, max_wait_ms
+        # While a slot is running, another one starts only once spill_queue
+        # requests wait or the oldest has waited spill_wait_ms: at low load a
+        # request then waits a little for the running one instead of sharing
+        # the GPU with it (two pipelines that each stream 1-2 GB slow each
+        # other down by more than the wait).  spill_queue=1: start at once.
+        self.spill_queue, self.spill_wait_ms = max(1, int(spill_queue)), spill_wait_ms
         self.slots = []
         for _ in range(n_slots):
             e = Engine(0)
@@ -275,6 +288,8 @@ class BatchedServer:
             slot.q1_out = torch.zeros(N.Q1_MAX_GROUPS * C.sizeof(N.Q1Agg), dtype=torch.uint8, device="cuda")
             slot.pred_h = torch.zeros(1, dtype=torch.float32).pin_memory()
             slot.pred_d = torch.zeros(1, dtype=torch.float32, device="cuda")
+            slot.cnt_d = torch.zeros(1, dtype=torch.int64, device="cuda")
+            slot.cnt_h = torch.zeros(1, dtype=torch.int64).pin_memory()
             self.slots.append(slot)
         self.launches = 0
 
@@ -293,8 +308,8 @@ class BatchedServer:
 
     def _launch_lone(self, s: Slot, r: Request) -> None:
         """A request that finds an idle slot and no other request waiting runs
-        alone through its standalone kernels (the scan-agg kernel, the
-        presized join), not through the batch machinery: at low load nothing
+        alone through its standalone kernels (the scan-agg kernel; the count
+        kernel, then the join sized from it), not through the batch machinery: at low load nothing
         is there to share, and the batch kernel's re-plan would only add to
         its latency."""
         import torch
@@ -306,13 +321,33 @@ class BatchedServer:
             s.engine.q1_fact_device(cols, int(f["ship_date"].numel()), p["cutoff"], p["n_flag_a"], p["n_flag_b"],
                                     s.q1_out)
         else:
+            # First phase of a lone join: the exact qualifying-row count (a 5-byte-per-row pass), copied
+            # to the host without a wait; _join_phase2 launches the join sized from it.
             j = self.tables.join
-            s.pred_h[0] = float(r.predicted) if r.predicted > 0 else float(j["b_key"].numel())
+            s.engine.join_count_device((j["b_key"], j["b_date"], j["b_seg"]), int(j["b_key"].numel()),
+                                       r.params["date_lt"], r.params["seg_eq"], s.cnt_d)
             with torch.cuda.stream(s.stream):
-                s.pred_d.copy_(s.pred_h, non_blocking=True)
-            s.engine.join_presized_device((j["b_key"], j["b_date"], j["b_seg"]), (j["p_fk"], j["p_price"], j["p_disc"]),
-                                          int(j["b_key"].numel()), int(j["p_fk"].numel()), r.params["date_lt"],
-                                          r.params["seg_eq"], s.pred_d, s.join_out)
+                s.cnt_h.copy_(s.cnt_d, non_blocking=True)
+            s.phase = "count"
+
+    def _join_phase2(self, s: Slot) -> None:
+        """Second phase of a lone join: the presized pipeline with its table
+        sized from the exact count (4 slots per qualifying row, the plain
+        form's table) -- at low load an MLP-presized table (prediction times
+        the calibrated margin) is larger than needed and misses L2 on a
+        60M-row probe, while the count costs one pass over the build side."""
+        import torch
+
+        j, r = self.tables.join, s.lone
+        s.pred_h[0] = float(max(int(s.cnt_h[0]), 1))
+        with torch.cuda.stream(s.stream):
+            s.pred_d.copy_(s.pred_h, non_blocking=True)
+        s.engine.join_presized_device((j["b_key"], j["b_date"], j["b_seg"]), (j["p_fk"], j["p_price"], j["p_disc"]),
+                                      int(j["b_key"].numel()), int(j["p_fk"].numel()), r.params["date_lt"],
+                                      r.params["seg_eq"], s.pred_d, s.join_out)
+        s.event = torch.cuda.Event()
+        s.event.record(s.stream)
+        s.phase = "run"
 
     def _launch(self, s: Slot, reqs: list) -> None:
         """Enqueues one slot's requests on its stream: the shared joins, then
@@ -320,6 +355,7 @@ class BatchedServer:
         import torch
 
         s.lone = None
+        s.phase = "run"
         if self.shared and len(reqs) == 1 and reqs[0].kind in (N.BATCH_SCAN_AGG, N.BATCH_JOIN):
             s.joins, s.gbs, s.others = [], [], []
             self._launch_lone(s, reqs[0])
@@ -419,15 +455,22 @@ class BatchedServer:
                     pending.append(r)
             for s in self.slots:
                 if s.busy and s.event.query():
+                    if s.phase == "count":  # a lone join's count has arrived: launch the join itself
+                        self._join_phase2(s)
+                        continue
                     self._results(s)
                     t_done = time.perf_counter() - t0
                     for r in s.reqs:
                         r.done = t_done
                     finished += len(s.reqs)
                     s.reqs, s.busy = [], False
+            running = sum(1 for s in self.slots if s.busy)
             for s in self.slots:
                 if not s.busy and pending:
                     waited = (time.perf_counter() - t0 - pending[0].arrival) * 1e3
+                    if running and len(pending) < self.spill_queue and waited < self.spill_wait_ms:
+                        break  # the running slot keeps the GPU a little longer
+                    running += 1
                     kind = next_kind(pending, self.policy, waited, self.max_wait_ms)
                     reqs = admit(pending, foot, self.max_batch, self.pool_bytes, self.max_items, kind)
                     tb = sum(foot[r.rid][0] for r in reqs)

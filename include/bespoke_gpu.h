@@ -529,6 +529,16 @@ typedef struct bo_tpch_q10_tables {
   int64_t n_custkey_map;              /* max custkey + 1 (0 if no customer) */
   const int32_t* c_nationkey;         /* per customer row */
   int64_t n_customer;
+  /* Optional (all NULL: not gathered): per customer row the string offsets of
+   * the host's name / address / phone / comment columns (n_customer + 1
+   * each: row i's bytes are [off[i], off[i + 1])) and acctbal (x100).  Given,
+   * each result row carries its customer's ranges and balance, so the host
+   * materialises Q10ResultRow without random reads of its own. */
+  const uint32_t* c_name_offsets;
+  const uint32_t* c_address_offsets;
+  const uint32_t* c_phone_offsets;
+  const uint32_t* c_comment_offsets;
+  const int32_t* c_acctbal;
 } bo_tpch_q10_tables;
 
 typedef struct bo_tpch_q10_row {      /* Q10ResultRow keys (bespoke_tpch/query_q10.hpp:10-19) */
@@ -536,7 +546,11 @@ typedef struct bo_tpch_q10_row {      /* Q10ResultRow keys (bespoke_tpch/query_q
   int32_t custkey;
   int32_t cust_row;                   /* customer row: name, acctbal, address, phone, comment */
   int32_t nationkey;
-  int32_t pad0;
+  int32_t acctbal_raw;                /* x100; 0 unless the tables carry c_acctbal */
+  /* [begin, begin + len) of the customer's strings in the host columns
+   * (0, 0 unless the tables carry the offsets) */
+  uint32_t name_begin, name_len, address_begin, address_len;
+  uint32_t phone_begin, phone_len, comment_begin, comment_len;
 } bo_tpch_q10_row;
 
 /* Device columns in, rows on the host (first min(n, max_rows); *n_rows = n).

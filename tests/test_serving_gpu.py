@@ -73,3 +73,31 @@ def test_served_without_sharing(engine, tables):
     srv.serve(reqs)
     check(engine, tables, reqs)
     srv.close()
+
+
+@pytest.mark.parametrize("policy,slots,spill", [("short_first", 2, 1), ("short_first", 3, 1), ("short_first", 2, 3),
+                                                ("fifo", 2, 2)])
+def test_served_short_first_equals_solo(engine, tables, policy, slots, spill):
+    """Short-first admission (one kind per launch, shortest kind first, no
+    starvation) and the spill rule (a second slot starts only once requests
+    queue): answers unchanged, every request served."""
+    reqs = S.poisson_requests(20000.0, 60, seed=12)
+    srv = S.BatchedServer(tables, n_slots=slots, max_batch=8, pool_bytes=512 << 20, max_items=32768,
+                          policy=policy, max_wait_ms=1.0, spill_queue=spill)
+    srv.serve(reqs)
+    assert all(r.result is not None and r.done >= r.arrival for r in reqs)
+    check(engine, tables, reqs)
+    srv.close()
+
+
+def test_served_lone_requests_at_low_rate(engine, tables):
+    """At a low arrival rate every request finds an idle slot: scan-agg runs
+    alone through its kernel and each join in two phases (exact count, then
+    the join sized from it, the serve loop never waiting on the device)."""
+    reqs = S.poisson_requests(300.0, 18, seed=13, mix=(1, 2, 0))
+    srv = S.BatchedServer(tables, n_slots=2, max_batch=8, pool_bytes=512 << 20, max_items=32768)
+    srv.serve(reqs)
+    assert srv.launches == len(reqs)
+    assert all(r.result.get("reruns", 0) == 0 for r in reqs)
+    check(engine, tables, reqs)
+    srv.close()
