@@ -1084,12 +1084,15 @@ def serving_section(eng, stream, join_sizer=None, gb_sizer=None, rates=(50, 500,
     load_s = time.perf_counter() - t_load
     tile = B.load_tile_table()
     srv = S.BatchedServer(tables, n_slots=2, max_batch=16, pool_bytes=2 << 30, max_items=65536, workers_per_sm=1,
-                          join_sizer=join_sizer, gb_sizer=gb_sizer, tile_table=tile)
+                          join_sizer=join_sizer, gb_sizer=gb_sizer, tile_table=tile, policy="short_first")
     # warm-up of both servers: every pipeline shape, plans, graphs, workspaces
     srv.serve(S.poisson_requests(1000.0, 48, seed=1))
     S.serve_one_per_launch(eng, tables, S.poisson_requests(1000.0, 30, seed=2))
     out = {"tables": "fact 60M rows; join build 15M x probe 60M; group-by A 25M, B 60M, C 40M (device-resident)",
            "load_s": round(load_s, 2), "slots": 2, "max_batch": 16, "pool_bytes_per_slot": 2 << 30,
+           "admission": "short_first (one kind per launch, shortest kind waiting first, oldest after 4 ms); a "
+                        "request that finds an idle slot and nothing else waiting runs alone (scan-agg kernel, "
+                        "join sized from its exact count on the device)",
            "shared": "the joins a slot admits run as one bo_join_multi_device pass, each group-by as the "
                      "presized multi-kernel pipeline (MLP-sized table, A id mask built at load), scan-agg "
                      "requests as instances of the slot's persistent batch kernel; one stream per slot",

@@ -218,9 +218,7 @@ class Slot:
     q1_out: object = None               # device groups of a lone scan-agg request
     pred_h: object = None               # pinned / device table size of a lone join request
     pred_d: object = None
-    cnt_d: object = None                # a lone join's exact qualifying-row count (device, pinned host)
-    cnt_h: object = None
-    phase: str = "run"                  # "count": a lone join's count is in flight, its join not yet launched
+    cnt_d: object = None                # a lone join's exact qualifying-row count (device)
     reqs: list = field(default_factory=list)
     joins: list = field(default_factory=list)
     gbs: list = field(default_factory=list)
@@ -240,8 +238,8 @@ class BatchedServer:
     exactly), and the scan-agg requests run as instances of the slot's
     persistent batch kernel -- all on the slot's stream, one event at the
     end.  A request that finds an idle slot with nothing else waiting runs
-    alone through its standalone kernel (scan-agg) or the join sized from an
-    exact count (count kernel, then the presized pipeline, no host wait).
+    alone through its standalone kernel (scan-agg) or the join sized from its
+    exact count on the device (count kernel, then the presized pipeline).
     With shared=False every request is a batch instance.
 
     Admission policy: "fifo" takes waiting requests in arrival order, kinds
@@ -289,7 +287,6 @@ class BatchedServer:
             slot.pred_h = torch.zeros(1, dtype=torch.float32).pin_memory()
             slot.pred_d = torch.zeros(1, dtype=torch.float32, device="cuda")
             slot.cnt_d = torch.zeros(1, dtype=torch.int64, device="cuda")
-            slot.cnt_h = torch.zeros(1, dtype=torch.int64).pin_memory()
             self.slots.append(slot)
         self.launches = 0
 
@@ -309,7 +306,7 @@ class BatchedServer:
     def _launch_lone(self, s: Slot, r: Request) -> None:
         """A request that finds an idle slot and no other request waiting runs
         alone through its standalone kernels (the scan-agg kernel; the count
-        kernel, then the join sized from it), not through the batch machinery: at low load nothing
+        kernel, then the join sized from it on the device), not through the batch machinery: at low load nothing
         is there to share, and the batch kernel's re-plan would only add to
         its latency."""
         import torch
@@ -321,33 +318,19 @@ class BatchedServer:
             s.engine.q1_fact_device(cols, int(f["ship_date"].numel()), p["cutoff"], p["n_flag_a"], p["n_flag_b"],
                                     s.q1_out)
         else:
-            # First phase of a lone join: the exact qualifying-row count (a 5-byte-per-row pass), copied
-            # to the host without a wait; _join_phase2 launches the join sized from it.
+            # A lone join sized from its exact count without a host round trip:
+            # the count kernel, the count turned into the presized path's size
+            # input on the device, then the presized pipeline (4 slots per
+            # qualifying row: the plain form's table), all enqueued at once.
             j = self.tables.join
             s.engine.join_count_device((j["b_key"], j["b_date"], j["b_seg"]), int(j["b_key"].numel()),
                                        r.params["date_lt"], r.params["seg_eq"], s.cnt_d)
             with torch.cuda.stream(s.stream):
-                s.cnt_h.copy_(s.cnt_d, non_blocking=True)
-            s.phase = "count"
-
-    def _join_phase2(self, s: Slot) -> None:
-        """Second phase of a lone join: the presized pipeline with its table
-        sized from the exact count (4 slots per qualifying row, the plain
-        form's table) -- at low load an MLP-presized table (prediction times
-        the calibrated margin) is larger than needed and misses L2 on a
-        60M-row probe, while the count costs one pass over the build side."""
-        import torch
-
-        j, r = self.tables.join, s.lone
-        s.pred_h[0] = float(max(int(s.cnt_h[0]), 1))
-        with torch.cuda.stream(s.stream):
-            s.pred_d.copy_(s.pred_h, non_blocking=True)
-        s.engine.join_presized_device((j["b_key"], j["b_date"], j["b_seg"]), (j["p_fk"], j["p_price"], j["p_disc"]),
-                                      int(j["b_key"].numel()), int(j["p_fk"].numel()), r.params["date_lt"],
-                                      r.params["seg_eq"], s.pred_d, s.join_out)
-        s.event = torch.cuda.Event()
-        s.event.record(s.stream)
-        s.phase = "run"
+                s.pred_d.copy_(s.cnt_d.to(torch.float32).clamp_(min=1.0))
+            s.engine.join_presized_device((j["b_key"], j["b_date"], j["b_seg"]),
+                                          (j["p_fk"], j["p_price"], j["p_disc"]), int(j["b_key"].numel()),
+                                          int(j["p_fk"].numel()), r.params["date_lt"], r.params["seg_eq"], s.pred_d,
+                                          s.join_out)
 
     def _launch(self, s: Slot, reqs: list) -> None:
         """Enqueues one slot's requests on its stream: the shared joins, then
@@ -355,7 +338,6 @@ class BatchedServer:
         import torch
 
         s.lone = None
-        s.phase = "run"
         if self.shared and len(reqs) == 1 and reqs[0].kind in (N.BATCH_SCAN_AGG, N.BATCH_JOIN):
             s.joins, s.gbs, s.others = [], [], []
             self._launch_lone(s, reqs[0])
@@ -449,15 +431,14 @@ class BatchedServer:
                 arrived.append(requests[i])
                 i += 1
             if arrived:
-                predict_requests(self.tables, arrived, self.join_sizer, self.gb_sizer)
+                # Shared joins size their tables from exact counts (the lone one's and the
+                # shared pass's count kernel): only batch-instance joins use a prediction.
+                predict_requests(self.tables, arrived, None if self.shared else self.join_sizer, self.gb_sizer)
                 for r in arrived:
                     foot[r.rid] = self._footprint(r)
                     pending.append(r)
             for s in self.slots:
                 if s.busy and s.event.query():
-                    if s.phase == "count":  # a lone join's count has arrived: launch the join itself
-                        self._join_phase2(s)
-                        continue
                     self._results(s)
                     t_done = time.perf_counter() - t0
                     for r in s.reqs:

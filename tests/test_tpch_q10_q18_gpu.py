@@ -149,16 +149,37 @@ def test_q10_matches_numpy(engine, torch_cuda, shuffle):
     tb.nation_bound = 25
     tb.custkey_to_row, tb.n_custkey_map = g["cmap"].data_ptr(), len(t["cmap"])
     tb.c_nationkey, tb.n_customer = g["cnation"].data_ptr(), len(t["cnation"])
-    for start, end_ in [(640, 730), (0, 2405), (100, 100)]:
+    # Every other pass also gathers the customers' string ranges and balances
+    # (random offsets per column, as the host's string columns store them).
+    nc = len(t["cnation"])
+    rng = np.random.default_rng(5)
+    offs = [np.concatenate([[0], np.cumsum(rng.integers(0, 90, size=nc))]).astype(np.uint32) for _ in range(4)]
+    acct = rng.integers(-99_999, 999_999, size=nc).astype(np.int32)
+    offs_d = [torch.from_numpy(o).cuda() for o in offs]
+    acct_d = torch.from_numpy(acct).cuda()
+    row_t = np.dtype([("rev", "<i8"), ("cust", "<i4"), ("crow", "<i4"), ("nk", "<i4"), ("acct", "<i4"),
+                      ("b0", "<u4"), ("l0", "<u4"), ("b1", "<u4"), ("l1", "<u4"), ("b2", "<u4"), ("l2", "<u4"),
+                      ("b3", "<u4"), ("l3", "<u4")])
+    assert row_t.itemsize == C.sizeof(N.TpchQ10Row)
+    for pass_no, (start, end_) in enumerate([(640, 730), (0, 2405), (100, 100), (0, 2405)]):
+        strings = pass_no % 2 == 1
+        tb.c_name_offsets, tb.c_address_offsets, tb.c_phone_offsets, tb.c_comment_offsets = (
+            [o.data_ptr() for o in offs_d] if strings else [None] * 4)
+        tb.c_acctbal = acct_d.data_ptr() if strings else None
         out = (N.TpchQ10Row * len(t["cmap"]))()
         n = C.c_int64()
         engine.ctx.call("bo_tpch_q10", C.byref(tb), start, end_, 2, 2, out, len(t["cmap"]), C.byref(n))
         want = q10_oracle(t, start, end_, 2, 2, 25)
         assert n.value == len(want[0])
-        got = np.frombuffer(out, dtype=np.dtype([("rev", "<i8"), ("cust", "<i4"), ("crow", "<i4"), ("nk", "<i4"),
-                                                ("p0", "<i4")]))[: n.value]
+        got = np.frombuffer(out, dtype=row_t)[: n.value]
         for name, w in zip(("rev", "cust", "crow", "nk"), want):
             assert np.array_equal(got[name], w), (name, start, end_)
+        crow = want[2]
+        assert np.array_equal(got["acct"], acct[crow] if strings else np.zeros_like(crow))
+        for k in range(4):
+            b = offs[k][crow] if strings else np.zeros_like(crow)
+            ln = offs[k][crow + 1] - offs[k][crow] if strings else np.zeros_like(crow)
+            assert np.array_equal(got[f"b{k}"], b) and np.array_equal(got[f"l{k}"], ln), k
     out = (N.TpchQ10Row * 1)()
     n = C.c_int64(-1)
     engine.ctx.call("bo_tpch_q10", C.byref(tb), 0, 2405, -1, 2, out, 1, C.byref(n))  # no 'R' in the dictionary
