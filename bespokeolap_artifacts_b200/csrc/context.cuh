@@ -96,8 +96,9 @@ T* carve(char*& p, size_t count) {
 
 // Stable LSD radix sort of (key, value) pairs by bits [begin_bit, end_bit)
 // (csrc/radix_sort.cu); n_dev, if given, is the actual count (<= n) on the
-// device.  Without n_dev, up to 65536 pairs are sorted by one thread-block
-// cluster in distributed shared memory (one launch).
+// device.  Without n_dev, up to 131,072 pairs (65,536 where the device
+// schedules no 16-CTA cluster) are sorted by one thread-block cluster in
+// distributed shared memory (one launch).
 int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsigned long long* tmp_keys,
                      uint32_t* tmp_vals, int64_t n, int begin_bit, int end_bit, const unsigned long long* n_dev);
 

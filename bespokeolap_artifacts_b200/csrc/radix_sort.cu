@@ -1,5 +1,5 @@
 // LSD onesweep radix sort of (uint64 key, uint32 value) pairs with decoupled
-// look-back (K5), a one-launch cluster sort for up to 64K pairs, and top-k by
+// look-back (K5), a one-launch cluster sort for up to 128K pairs, and top-k by
 // radix select (K6).
 //
 // Reference counterpart: the stable LSD counting sorts with 16-bit digits of
@@ -394,6 +394,19 @@ __global__ void __launch_bounds__(kSelBlock) topk_select_kernel(const unsigned l
   if (bad) raise_error(err, bad);
 }
 
+// Lanes of the warp holding the same digit (0..0x100, 0x100 = no row), from
+// 9 ballots (measured faster than __match_any_sync in the sort below).
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d) {
+  uint32_t m = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < 9; ++b) {
+    const uint32_t bit = (d >> b) & 1u;
+    const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+    m &= bit ? bal : ~bal;
+  }
+  return m;
+}
+
 // Stable LSD radix sort of up to kClusterSortMax pairs by one thread-block
 // cluster, the pairs held in the CTAs' shared memory for the whole sort: CTA
 // r holds global positions [r*S, r*S + S).  Per 8-bit digit every warp ranks
@@ -408,7 +421,9 @@ constexpr int kCsBlock = 512;
 constexpr int kCsWarps = kCsBlock / 32;
 constexpr int kCsCap = 8192;                    // pairs per CTA
 constexpr int kCsRounds = kCsCap / kCsBlock;    // rounds of 32 per warp
-constexpr int kCsMaxCluster = 8;                // portable cluster size
+constexpr int kCsPortable = 8;                  // portable cluster size
+constexpr int kCsMaxCluster = 16;               // non-portable, where the device schedules it
+constexpr int64_t kCsTargetPerCta = 1024;       // spread: about this many pairs per CTA
 constexpr int64_t kClusterSortMax = (int64_t)kCsCap * kCsMaxCluster;
 constexpr size_t kCsDynSmem = (size_t)2 * kCsCap * (sizeof(unsigned long long) + sizeof(uint32_t));
 
@@ -419,14 +434,16 @@ __global__ void __launch_bounds__(kCsBlock, 1) cluster_sort_kernel(unsigned long
   const uint32_t cs = cl.num_blocks();
   const uint32_t me = cl.block_rank();
   extern __shared__ __align__(16) unsigned char cs_smem[];
-  unsigned long long* sk = reinterpret_cast<unsigned long long*>(cs_smem);  // [2][kCsCap]
-  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + 2 * kCsCap);              // [2][kCsCap]
+  // [2][S] keys then [2][S] values: the launch sizes the dynamic shared
+  // memory to the pairs per CTA (S <= kCsCap), not to the capacity.
+  unsigned long long* sk = reinterpret_cast<unsigned long long*>(cs_smem);
   __shared__ uint32_t warp_cnt[kCsWarps][kRadix];
   __shared__ uint32_t tot[kRadix];   // this CTA's digit totals, read by the whole cluster
   __shared__ uint32_t base[kRadix];  // where this CTA's pairs of each digit start
   __shared__ uint32_t wsum[kRadix / 32];
   __shared__ int skip;
   const uint32_t S = (uint32_t)((n + cs - 1) / cs);  // <= kCsCap (checked by the host)
+  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + 2 * S);
   const int64_t lo = (int64_t)me * S;
   const int64_t left = n - lo;
   const uint32_t m = left <= 0 ? 0u : (left < (int64_t)S ? (uint32_t)left : S);
@@ -447,8 +464,8 @@ __global__ void __launch_bounds__(kCsBlock, 1) cluster_sort_kernel(unsigned long
     for (int i = threadIdx.x; i < kCsWarps * kRadix; i += kCsBlock) (&warp_cnt[0][0])[i] = 0;
     if (threadIdx.x == 0) skip = 0;
     __syncthreads();
-    const unsigned long long* ks = sk + src * kCsCap;
-    const uint32_t* vs = sv + src * kCsCap;
+    const unsigned long long* ks = sk + src * S;
+    const uint32_t* vs = sv + src * S;
     uint32_t rank[kCsRounds], dig[kCsRounds];
 #pragma unroll
     for (int r = 0; r < kCsRounds; ++r) {
@@ -459,7 +476,7 @@ __global__ void __launch_bounds__(kCsBlock, 1) cluster_sort_kernel(unsigned long
       const bool valid = idx < m;
       const uint32_t d = valid ? (uint32_t)((ks[idx] >> shift) & dmask) : 0x100u;
       dig[r] = d;
-      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      const uint32_t peers = digit_peers(d);
       const uint32_t before = valid ? warp_cnt[warp][d] : 0u;
       __syncwarp();
       if (valid && lane == __ffs(peers) - 1) warp_cnt[warp][d] = before + __popc(peers);
@@ -503,8 +520,8 @@ __global__ void __launch_bounds__(kCsBlock, 1) cluster_sort_kernel(unsigned long
     }
     __syncthreads();
     if (!skip) {
-      unsigned long long* kd = sk + (src ^ 1) * kCsCap;
-      uint32_t* vd = sv + (src ^ 1) * kCsCap;
+      unsigned long long* kd = sk + (src ^ 1) * S;
+      uint32_t* vd = sv + (src ^ 1) * S;
 #pragma unroll
       for (int r = 0; r < kCsRounds; ++r) {
         const uint32_t d = dig[r];
@@ -521,8 +538,8 @@ __global__ void __launch_bounds__(kCsBlock, 1) cluster_sort_kernel(unsigned long
     if (!skip) src ^= 1;
   }
   for (uint32_t i = threadIdx.x; i < m; i += kCsBlock) {
-    keys[lo + i] = sk[src * kCsCap + i];
-    vals[lo + i] = sv[src * kCsCap + i];
+    keys[lo + i] = sk[src * S + i];
+    vals[lo + i] = sv[src * S + i];
   }
 }
 
@@ -539,22 +556,63 @@ namespace bo {
 // tmp_keys / tmp_vals must hold n entries.  The sorted data ends in keys/vals.
 // One cluster of the smallest power-of-two size whose shared memory holds the
 // pairs (n <= kClusterSortMax).
+// The largest cluster the device schedules for the sort: 16 CTAs where a
+// non-portable cluster of that size fits (B200), else 8.  Checked once.
+int cluster_sort_max(bo_ctx* ctx) {
+  static int cached = 0;
+  if (cached) return cached;
+  if (cudaFuncSetAttribute(cluster_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCsDynSmem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return kCsPortable;
+  }
+  int best = kCsPortable;
+  if (cudaFuncSetAttribute(cluster_sort_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kCsMaxCluster);
+    cfg.blockDim = dim3(kCsBlock);
+    cfg.dynamicSmemBytes = kCsDynSmem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kCsMaxCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, reinterpret_cast<const void*>(&cluster_sort_kernel), &cfg) ==
+            cudaSuccess &&
+        clusters >= 1)
+      best = kCsMaxCluster;
+  }
+  cudaGetLastError();
+  (void)ctx;
+  cached = best;
+  return cached;
+}
+
 int cluster_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, int64_t n, int begin_bit,
                        int end_bit) {
   if (n <= 1 || end_bit <= begin_bit) return BO_OK;
-  if (n > kClusterSortMax) return set_error(ctx, BO_ERR_INVALID, "cluster_sort: %lld pairs", (long long)n);
+  const int max_cs = cluster_sort_max(ctx);
+  if (n > (int64_t)kCsCap * max_cs) return set_error(ctx, BO_ERR_INVALID, "cluster_sort: %lld pairs", (long long)n);
+  // Enough CTAs to hold the pairs, and more (up to the largest cluster) so
+  // that each CTA ranks about kCsTargetPerCta of them: one CTA's passes are
+  // instruction-bound, so the sort takes time in proportion to its share.
   unsigned cs = 1;
   while ((int64_t)cs * kCsCap < n) cs <<= 1;
+  while ((int)cs < max_cs && (int64_t)cs * kCsTargetPerCta < n) cs <<= 1;
   static bool ready = false;
   if (!ready) {
     BO_CUDA(ctx, cudaFuncSetAttribute(cluster_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kCsDynSmem));
     ready = true;
   }
+  const int64_t per_cta = (n + cs - 1) / cs;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs);
   cfg.blockDim = dim3(kCsBlock);
-  cfg.dynamicSmemBytes = kCsDynSmem;
+  cfg.dynamicSmemBytes = (size_t)2 * per_cta * (sizeof(unsigned long long) + sizeof(uint32_t));
   cfg.stream = ctx->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -577,7 +635,8 @@ int read_device_count(bo_ctx* ctx, const unsigned long long* n_dev, int64_t n_ma
 int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsigned long long* tmp_keys,
                      uint32_t* tmp_vals, int64_t n, int begin_bit, int end_bit, const unsigned long long* n_dev) {
   if (end_bit <= begin_bit || (n <= 1 && !n_dev)) return BO_OK;
-  if (!n_dev && n <= kClusterSortMax) return cluster_sort_pairs(ctx, keys, vals, n, begin_bit, end_bit);
+  if (!n_dev && n <= (int64_t)kCsCap * cluster_sort_max(ctx))
+    return cluster_sort_pairs(ctx, keys, vals, n, begin_bit, end_bit);
   // An even number of passes leaves the result in keys/vals; pad with a pass
   // over zero bits (a stable copy of the actual keys) rather than copying the
   // whole upper-bound buffer back.

@@ -15,7 +15,7 @@
 //            custkey order (order-preserving compaction, compact.cuh) -- the
 //            order the reference's first sort, by custkey, produces;
 //   sort     one stable radix sort by the complemented revenue (64 bits), the
-//            reference's own key order (one cluster launch up to 64K rows).
+//            reference's own key order (one cluster launch up to 128K rows).
 //
 // Q18 (run_q18, bespoke_tpch/query_q18.cpp:183-455).
 //   sum      sum_qty[orderkey] += l_quantity: each thread takes eight
@@ -451,7 +451,7 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
   if ((rc = ordered_compact(ctx, Q10Kept{hit, t->custkey_to_row, t->c_nationkey, t->n_customer, t->nation_bound}, nm,
                             tile_counts, vals, n_out)))
     return rc;
-  // The result's size, read back once: up to 64K rows sort in one cluster
+  // The result's size, read back once: up to 128K rows sort in one cluster
   // launch instead of a pass sequence sized for every customer.
   int64_t ns = 0;
   if ((rc = read_device_count(ctx, n_out, nm, &ns))) return rc;

@@ -17,7 +17,7 @@
 //          visited through the orderkey map so they come out in ascending
 //          orderkey order (order-preserving compaction, compact.cuh);
 //   sort   one stable radix sort by (revenue desc, orderdate asc) -- one
-//          cluster launch up to 64K result rows.  The reference's std::sort
+//          cluster launch up to 128K result rows.  The reference's std::sort
 //          leaves rows equal in both keys in unspecified order; here they keep
 //          orderkey order, a canonical form of the same result.
 #include <algorithm>
@@ -271,7 +271,7 @@ extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_
   // Qualifying orders in ascending orderkey order (no sort by orderkey needed).
   if ((rc = ordered_compact(ctx, Q3Kept{t->orderkey_to_row, no, cnt}, t->n_orderkey_map, tile_counts, vals, n_out)))
     return rc;
-  // The result's size, read back once: up to 64K rows sort in one cluster
+  // The result's size, read back once: up to 128K rows sort in one cluster
   // launch instead of a pass sequence sized for every order.
   int64_t ns = 0;
   if ((rc = read_device_count(ctx, n_out, no, &ns))) return rc;

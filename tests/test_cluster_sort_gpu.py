@@ -1,8 +1,9 @@
-"""The one-launch cluster sort (up to 65,536 pairs held in the distributed
-shared memory of 1, 2, 4 or 8 CTAs) against the oracle's stable LSD sort and
-numpy's stable argsort: sizes at every cluster-size boundary, ties (stability
-across CTAs), bit ranges, and digits that every key shares (skipped passes).
-65,537 pairs take the onesweep passes again."""
+"""The one-launch cluster sort (pairs held in the distributed shared memory of
+1 to 16 CTAs, about 1K pairs per CTA; up to 131,072 pairs where the device
+schedules a 16-CTA cluster, else 65,536) against the oracle's stable LSD sort
+and numpy's stable argsort: sizes at every cluster-size boundary, ties
+(stability across CTAs), bit ranges, and digits that every key shares
+(skipped passes).  Above the limit the onesweep passes sort again."""
 import numpy as np
 import pytest
 
@@ -11,7 +12,8 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n", [2, 3, 511, 8191, 8192, 8193, 16384, 16385, 32768, 32769, 65535, 65536, 65537])
+@pytest.mark.parametrize("n", [2, 3, 511, 1024, 1025, 2049, 4097, 8191, 8192, 8193, 16384, 16385, 32768, 32769,
+                               65535, 65536, 65537, 131072, 131073])
 def test_cluster_sort_sizes_match_oracle(engine, n):
     rng = np.random.default_rng(n)
     k = rng.integers(0, 2**64, size=n, dtype=np.uint64)
