@@ -785,6 +785,187 @@ std::vector<Q22ResultRow> run_q22(const Database& db, const std::vector<std::str
   return rows;
 }
 
+std::vector<Q16ResultRow> run_q16(const Database& db, const std::string& brand, const std::string& type,
+                                  const std::string sizes[8]) {
+  // query_q16.cpp:185-221: sizes that are all digits ("" is 0, "<<NULL>>"
+  // and other text are skipped); none: no rows.  Sizes above 50 set no bit.
+  uint64_t size_mask = 0;
+  bool any = false;
+  for (int i = 0; i < 8; ++i) {
+    const std::string& v = sizes[i];
+    if (v == "<<NULL>>") continue;
+    uint32_t parsed = 0;
+    bool digits = true;
+    for (char ch : v) {
+      if (ch < '0' || ch > '9') {
+        digits = false;
+        break;
+      }
+      parsed = parsed * 10u + static_cast<uint32_t>(ch - '0');
+    }
+    if (!digits) continue;
+    any = true;
+    if (static_cast<int32_t>(parsed) >= 0 && parsed <= 50) size_mask |= 1ull << parsed;
+  }
+  // :223-231, :346-355: no part rows or no supplier rows, no rows.
+  if (!any || db.n_part == 0 || db.s_suppkey.empty()) return {};
+  if (db.brand_rank.size() != db.brand.values.size() || db.type_rank.size() != db.part_type.values.size())
+    throw std::runtime_error("Q16: dictionaries too large for ranks");
+  // :233-270: types starting with TYPE are banned; the brand equal to BRAND.
+  std::vector<uint8_t> type_banned(db.part_type.values.size(), 0);
+  for (size_t i = 0; i < type_banned.size(); ++i)
+    type_banned[i] = db.part_type.values[i].compare(0, type.size(), type) == 0 && db.part_type.values[i].size() >= type.size();
+  int32_t banned_brand = -1;
+  for (size_t i = 0; i < db.brand.values.size(); ++i)
+    if (db.brand.values[i] == brand) {
+      banned_brand = static_cast<int32_t>(i);
+      break;
+    }
+  bo_tpch_q16_tables t{};
+  t.p_partkey = col<int32_t>(db.p_partkey);
+  t.p_brand = col<uint16_t>(db.p_brand);
+  t.p_type = col<uint16_t>(db.p_type);
+  t.p_size = col<int32_t>(db.p_size);
+  t.n_part = db.n_part;
+  t.ps_partkey = col<int32_t>(db.ps_partkey);
+  t.ps_suppkey = col<int32_t>(db.ps_suppkey);
+  t.n_partsupp = db.n_partsupp;
+  t.s_banned = col<uint8_t>(db.s_banned);
+  t.n_banned = db.n_s_banned;
+  bo_tpch_q16_params prm{};
+  prm.size_mask = size_mask;
+  prm.banned_brand = banned_brand;
+  // :383-388: a partsupp row count that is a multiple of the part rows is walked by position.
+  prm.rows_per_part = db.n_partsupp % db.n_part == 0 ? static_cast<int32_t>(db.n_partsupp / db.n_part) : 0;
+  prm.n_brand = static_cast<int32_t>(db.brand.values.size());
+  prm.n_type = static_cast<int32_t>(db.part_type.values.size());
+  prm.brand_rank = db.brand_rank.data();
+  prm.type_rank = db.type_rank.data();
+  prm.type_banned = type_banned.data();
+  std::vector<bo_tpch_q16_row> out(static_cast<size_t>(db.n_part));
+  int64_t n = 0;
+  check(db.ctx, bo_tpch_q16(db.ctx, &t, &prm, out.data(), static_cast<int64_t>(out.size()), &n), "q16");
+  std::vector<Q16ResultRow> rows(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    const auto& r = out[static_cast<size_t>(i)];
+    rows[static_cast<size_t>(i)] = Q16ResultRow{db.brand.values[static_cast<size_t>(r.brand_code)],
+                                                db.part_type.values[static_cast<size_t>(r.type_code)], r.size,
+                                                r.supplier_cnt};
+  }
+  return rows;
+}
+
+std::vector<Q20ResultRow> run_q20(const Database& db, const std::string& color, const std::string& date,
+                                  const std::string& nation) {
+  // query_q20.cpp:344-361: a NULL parameter or an unknown nation, no rows
+  // (the nation's first row by name).
+  if (color == "<<NULL>>" || date == "<<NULL>>" || nation == "<<NULL>>") return {};
+  int32_t key = 0;
+  bool found = false;
+  for (size_t i = 0; i < db.nation_row_name.size() && !found; ++i)
+    if (db.nation_row_name[i] == nation) {
+      key = db.nation_key[i];
+      found = true;
+    }
+  if (!found) return {};
+  const int16_t start = date_offset_of(date, db.base_date_days);
+  const int16_t end = date_offset_of(date, db.base_date_days, 12);
+  bo_tpch_q20_tables t{};
+  t.p_partkey = col<int32_t>(db.p_partkey);
+  t.p_name = col<char>(db.p_name);
+  t.p_name_offsets = col<uint32_t>(db.p_name_offsets);
+  t.n_part = db.n_part;
+  t.max_partkey = db.max_partkey;
+  t.max_suppkey = db.s_max_suppkey;
+  t.l_shipdate = col<int16_t>(db.l_shipdate);
+  t.l_partkey = col<int32_t>(db.l_partkey);
+  t.l_suppkey = col<int32_t>(db.l_suppkey);
+  t.l_supp_nation = col<int16_t>(db.l_supp_nation);
+  t.l_quantity = col<int16_t>(db.l_quantity);
+  t.n_lineitem = db.n_lineitem;
+  t.ps_partkey = col<int32_t>(db.ps_partkey);
+  t.ps_suppkey = col<int32_t>(db.ps_suppkey);
+  t.ps_availqty = col<int32_t>(db.ps_availqty);
+  t.n_partsupp = db.n_partsupp;
+  t.ps_part_begin = col<int32_t>(db.ps_part_begin);
+  t.n_ps_part_keys = db.n_ps_part_keys;
+  t.s_nation_by_key = col<int16_t>(db.s_nation_by_key);
+  t.s_suppkey = col<int32_t>(db.s_suppkey_device);
+  t.s_nationkey = col<int32_t>(db.s_nationkey_device);
+  t.s_row_by_name = col<int32_t>(db.s_row_by_name);
+  t.n_supplier = static_cast<int64_t>(db.s_suppkey.size());
+  std::vector<int32_t> out(db.s_suppkey.size());
+  int64_t n = 0;
+  check(db.ctx,
+        bo_tpch_q20(db.ctx, &t, color.data(), static_cast<int32_t>(color.size()), key, start, end, out.data(),
+                    static_cast<int64_t>(out.size()), &n),
+        "q20");
+  std::vector<Q20ResultRow> rows(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    const size_t r = static_cast<size_t>(out[static_cast<size_t>(i)]);
+    rows[static_cast<size_t>(i)] = Q20ResultRow{db.s_name.view(r), db.s_address.view(r)};
+  }
+  return rows;
+}
+
+std::vector<Q2ResultRow> run_q2(const Database& db, const std::string& size, const std::string& type,
+                                const std::string& region) {
+  // query_q2.cpp:149-157: SIZE as std::stoi reads it; an unknown region, no rows.
+  const int32_t target_size = std::stoi(size);
+  const auto it = db.region_key_by_name.find(region);
+  if (it == db.region_key_by_name.end()) return {};
+  const int32_t region_key = it->second;
+  // :166-183: nations by key below the row count; in the region when any row
+  // of the key is.
+  const size_t n_nation = db.nation_key.size();
+  std::vector<uint8_t> nation_ok(n_nation, 0);
+  for (size_t i = 0; i < n_nation; ++i)
+    if (db.nation_key[i] >= 0 && static_cast<size_t>(db.nation_key[i]) < n_nation &&
+        db.nation_regionkey[i] == region_key)
+      nation_ok[static_cast<size_t>(db.nation_key[i])] = 1;
+  // :214-230: types ending in TYPE.
+  std::vector<uint8_t> type_ok(db.part_type.values.size(), 0);
+  for (size_t i = 0; i < type_ok.size(); ++i) {
+    const std::string& v = db.part_type.values[i];
+    type_ok[i] = v.size() >= type.size() && v.compare(v.size() - type.size(), type.size(), type) == 0;
+  }
+  bo_tpch_q2_tables t{};
+  t.p_size = col<int32_t>(db.p_size);
+  t.p_type = col<uint16_t>(db.p_type);
+  t.p_mfgr = col<uint16_t>(db.p_mfgr);
+  t.n_part = db.n_part;
+  t.ps_suppkey = col<int32_t>(db.ps_suppkey);
+  t.ps_supplycost = col<int32_t>(db.ps_supplycost);
+  t.n_partsupp = db.n_partsupp;
+  t.ps_part_begin = col<int32_t>(db.ps_part_begin);
+  t.n_ps_part_keys = db.n_ps_part_keys;
+  t.s_nation_idx = col<int32_t>(db.s_nation_idx_device);
+  t.s_rank = col<uint32_t>(db.s_rank);
+  t.n_supplier = static_cast<int64_t>(db.s_suppkey.size());
+  std::vector<bo_tpch_q2_row> out(static_cast<size_t>(std::max<int64_t>(db.n_partsupp, 0)));
+  int64_t n = 0;
+  check(db.ctx,
+        bo_tpch_q2(db.ctx, &t, target_size, type_ok.data(), static_cast<int32_t>(type_ok.size()), nation_ok.data(),
+                   static_cast<int32_t>(n_nation), out.data(), static_cast<int64_t>(out.size()), &n),
+        "q2");
+  std::vector<Q2ResultRow> rows(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    const auto& o = out[static_cast<size_t>(i)];
+    const size_t srow = static_cast<size_t>(o.supplier_row);
+    const int32_t idx = db.s_nation_idx[srow];
+    rows[static_cast<size_t>(i)] =
+        Q2ResultRow{db.s_acctbal[srow],
+                    db.s_name.view(srow),
+                    idx >= 0 ? std::string_view(db.nation_name_by_idx[static_cast<size_t>(idx)]) : std::string_view(),
+                    o.partkey,
+                    db.mfgr.values[static_cast<size_t>(o.mfgr_code)],
+                    db.s_address.view(srow),
+                    db.s_phone.view(srow),
+                    db.s_comment.view(srow)};
+  }
+  return rows;
+}
+
 std::vector<Q11ResultRow> run_q11(const Database& db, const std::string& nation, const std::string& fraction) {
   // query_q11.cpp:112-143: the nation's key (first nation row of the name),
   // FRACTION as a double, the nation's suppliers by key.
@@ -1365,6 +1546,33 @@ void write_q22_csv(const std::string& filename, const std::vector<Q22ResultRow>&
         << "\n";
 }
 
+void write_q16_csv(const std::string& filename, const std::vector<Q16ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q16.cpp:543-556
+  out << "p_brand,p_type,p_size,supplier_cnt\n";
+  for (const auto& r : rows)
+    out << escape_csv(std::string(r.p_brand)) << ',' << escape_csv(std::string(r.p_type)) << ',' << r.p_size << ','
+        << r.supplier_cnt << "\n";
+}
+
+void write_q20_csv(const std::string& filename, const std::vector<Q20ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q20.cpp:678-686
+  out << "s_name,s_address\n";
+  for (const auto& r : rows)
+    out << escape_csv(std::string(r.s_name)) << ',' << escape_csv(std::string(r.s_address)) << "\n";
+}
+
+void write_q2_csv(const std::string& filename, const std::vector<Q2ResultRow>& rows) {
+  std::ofstream out(filename);  // query_q2.cpp:432-454
+  out << "s_acctbal,s_name,n_name,p_partkey,p_mfgr,s_address,s_phone,s_comment\n";
+  out.setf(std::ios::fixed);
+  out << std::setprecision(2);
+  for (const auto& r : rows)
+    out << static_cast<double>(r.s_acctbal_raw) / kPriceScale << ',' << escape_csv(std::string(r.s_name)) << ','
+        << escape_csv(std::string(r.n_name)) << ',' << r.p_partkey << ',' << escape_csv(std::string(r.p_mfgr)) << ','
+        << escape_csv(std::string(r.s_address)) << ',' << escape_csv(std::string(r.s_phone)) << ','
+        << escape_csv(std::string(r.s_comment)) << "\n";
+}
+
 void write_q11_csv(const std::string& filename, const std::vector<Q11ResultRow>& rows) {
   std::ofstream out(filename);  // query_q11.cpp:226-234
   out << "ps_partkey,value\n";
@@ -1451,7 +1659,9 @@ Database::~Database() {
                           &c_custkey, &c_mktsegment, &c_nationkey, &custkey_to_row, &scratch, &p_name,
                           &p_name_offsets, &ps_supplycost, &ps_part_begin, &o_year_by_key, &l_shipinstruct,
                           &p_size, &p_row_by_key, &o_orderstatus, &c_name_offsets, &c_address_offsets,
-                          &c_phone_offsets, &c_comment_offsets};
+                          &c_phone_offsets, &c_comment_offsets, &s_comment_chars, &s_comment_offsets,
+                          &s_suppkey_device, &s_banned, &s_nation_by_key, &s_nationkey_device,
+                          &s_row_by_name, &ps_availqty, &s_nation_idx_device, &s_rank, &p_mfgr};
   for (auto* c : cols)
     if (c->ptr) bo_device_free(ctx, c->ptr);
   if (result_host) bo_host_free_pinned(ctx, result_host);
@@ -1743,8 +1953,8 @@ struct PartHost {
   int32_t max_key = -1;
   std::vector<int32_t> key, size, row_by_key;
   StringColumn name;
-  std::vector<uint16_t> brand, container, type;
-  Dictionary brand_dict, container_dict, type_dict;
+  std::vector<uint16_t> brand, container, type, mfgr;
+  Dictionary brand_dict, container_dict, type_dict, mfgr_dict;
 };
 
 PartHost derive_part(const ParquetTables::ArrowTable& P) {
@@ -1754,6 +1964,7 @@ PartHost derive_part(const ParquetTables::ArrowTable& P) {
   h.size = int_values(column(P, "p_size"));
   const auto& key = h.key;
   h.brand = dictionary_codes(column(P, "p_brand"), h.brand_dict);
+  h.mfgr = dictionary_codes(column(P, "p_mfgr"), h.mfgr_dict);
   h.container = dictionary_codes(column(P, "p_container"), h.container_dict);
   h.type = dictionary_codes(column(P, "p_type"), h.type_dict);
   const auto& type = h.type;
@@ -1947,6 +2158,8 @@ Database* build(ParquetTables* tables) {
       db->brand = std::move(h.brand_dict);
       db->container = std::move(h.container_dict);
       db->p_type = upload(ctx, h.type);
+      db->p_mfgr = upload(ctx, h.mfgr);
+      db->mfgr = std::move(h.mfgr_dict);
       db->part_type = std::move(h.type_dict);
       db->p_name = upload(ctx, std::vector<char>(h.name.data.begin(), h.name.data.end()));
       db->p_name_offsets = upload(ctx, h.name.offsets);
@@ -1977,11 +2190,12 @@ Database* build(ParquetTables* tables) {
       std::vector<uint32_t> order(pk.size());
       std::iota(order.begin(), order.end(), 0u);
       std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return pk[a] < pk[b]; });
-      std::vector<int32_t> spk(pk.size()), ssk(pk.size()), val(pk.size()), scost(pk.size());
+      std::vector<int32_t> spk(pk.size()), ssk(pk.size()), val(pk.size()), scost(pk.size()), sqty(pk.size());
       for (size_t i = 0; i < order.size(); ++i) {
         spk[i] = pk[order[i]];
         ssk[i] = sk[order[i]];
         scost[i] = cost[order[i]];
+        sqty[i] = qty[order[i]];
         val[i] = static_cast<int32_t>(static_cast<int64_t>(cost[order[i]]) * qty[order[i]]);
       }
       // Q9's part slots (query_q9.cpp:140-186): keys 0 .. the largest part or
@@ -2014,6 +2228,7 @@ Database* build(ParquetTables* tables) {
       db->ps_partkey = upload(ctx, spk);
       db->ps_suppkey = upload(ctx, ssk);
       db->ps_value = upload(ctx, val);
+      db->ps_availqty = upload(ctx, sqty);
     }
     {
       const auto& S = tables->supplier;
@@ -2022,6 +2237,86 @@ Database* build(ParquetTables* tables) {
       db->s_name = string_column(column(S, "s_name"));
       db->s_address = string_column(column(S, "s_address"));
       db->s_phone = string_column(column(S, "s_phone"));
+      db->s_comment = string_column(column(S, "s_comment"));
+      // run_q16's supplier scan (query_q16.cpp:348-368): flags by suppkey over
+      // keys 0 .. max(row count, largest key).
+      int64_t bound = static_cast<int64_t>(db->s_suppkey.size());
+      for (int32_t k : db->s_suppkey) bound = std::max<int64_t>(bound, k);
+      db->n_s_banned = db->s_suppkey.empty() ? 0 : bound + 1;
+      if (db->n_s_banned > 0) {
+        db->s_comment_chars =
+            upload(ctx, std::vector<char>(db->s_comment.data.begin(), db->s_comment.data.end()));
+        db->s_comment_offsets = upload(ctx, db->s_comment.offsets);
+        db->s_suppkey_device = upload(ctx, db->s_suppkey);
+        check(ctx, bo_device_alloc(ctx, static_cast<size_t>(db->n_s_banned), &db->s_banned.ptr), "supplier flags");
+        db->s_banned.rows = db->n_s_banned;
+        check(ctx,
+              bo_tpch_supplier_complaints(ctx, static_cast<const char*>(db->s_comment_chars.ptr),
+                                          static_cast<const uint32_t*>(db->s_comment_offsets.ptr),
+                                          static_cast<const int32_t*>(db->s_suppkey_device.ptr),
+                                          static_cast<int64_t>(db->s_suppkey.size()),
+                                          static_cast<uint8_t*>(db->s_banned.ptr), db->n_s_banned),
+              "supplier flags");
+      }
+    }
+    {  // Q20 and Q2 supplier derivations (query_q20.cpp:566-644, query_q2.cpp:167-212, 386-401)
+      const auto& S = tables->supplier;
+      const size_t ns = db->s_suppkey.size();
+      db->s_acctbal = scaled_values(column(S, "s_acctbal"), kPriceScale);
+      for (int32_t k : db->s_suppkey) db->s_max_suppkey = std::max(db->s_max_suppkey, k);
+      // nationkey by suppkey, the last row of a key winning (builder_impl.cpp:725-742)
+      std::vector<int16_t> by_key(db->s_max_suppkey >= 0 ? static_cast<size_t>(db->s_max_suppkey) + 1 : 0, int16_t(-1));
+      for (size_t i = 0; i < ns; ++i)
+        if (db->s_suppkey[i] >= 0) by_key[static_cast<size_t>(db->s_suppkey[i])] = static_cast<int16_t>(db->s_nationkey[i]);
+      if (!by_key.empty()) db->s_nation_by_key = upload(ctx, by_key);
+      // rows in s_name order
+      std::vector<int32_t> by_name(ns);
+      std::iota(by_name.begin(), by_name.end(), 0);
+      std::stable_sort(by_name.begin(), by_name.end(),
+                       [&](int32_t a, int32_t b) { return db->s_name.view(a) < db->s_name.view(b); });
+      // run_q2's nation names by key, for keys below the nation row count (last row wins)
+      const size_t n_nation = db->nation_key.size();
+      db->nation_name_by_idx.assign(n_nation, std::string());
+      for (size_t i = 0; i < n_nation; ++i)
+        if (db->nation_key[i] >= 0 && static_cast<size_t>(db->nation_key[i]) < n_nation)
+          db->nation_name_by_idx[static_cast<size_t>(db->nation_key[i])] = db->nation_row_name[i];
+      db->s_nation_idx.assign(ns, -1);
+      for (size_t i = 0; i < ns; ++i)
+        if (static_cast<uint32_t>(db->s_nationkey[i]) < n_nation) db->s_nation_idx[i] = db->s_nationkey[i];
+      auto nation_of = [&](size_t row) -> std::string_view {
+        const int32_t idx = db->s_nation_idx[row];
+        return idx >= 0 ? std::string_view(db->nation_name_by_idx[static_cast<size_t>(idx)]) : std::string_view();
+      };
+      std::vector<int32_t> order(ns);
+      std::iota(order.begin(), order.end(), 0);
+      std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        if (db->s_acctbal[a] != db->s_acctbal[b]) return db->s_acctbal[a] > db->s_acctbal[b];
+        const auto na = nation_of(a), nb = nation_of(b);
+        if (na != nb) return na < nb;
+        const auto sa = db->s_name.view(a), sb = db->s_name.view(b);
+        if (sa != sb) return sa < sb;
+        return a < b;
+      });
+      std::vector<uint32_t> rank(ns);
+      for (size_t i = 0; i < ns; ++i) rank[static_cast<size_t>(order[i])] = static_cast<uint32_t>(i);
+      if (ns > 0) {
+        db->s_nationkey_device = upload(ctx, db->s_nationkey);
+        db->s_row_by_name = upload(ctx, by_name);
+        db->s_nation_idx_device = upload(ctx, db->s_nation_idx);
+        db->s_rank = upload(ctx, rank);
+      }
+    }
+    {  // brand and type ranks in string order (query_q16.cpp:491-512)
+      auto ranks = [](const std::vector<std::string>& dict) {
+        std::vector<uint32_t> idx(dict.size());
+        std::iota(idx.begin(), idx.end(), 0u);
+        std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return dict[a] < dict[b]; });
+        std::vector<uint16_t> rank(dict.size());
+        for (size_t i = 0; i < idx.size(); ++i) rank[idx[i]] = static_cast<uint16_t>(i);
+        return rank;
+      };
+      if (db->brand.values.size() <= 65536) db->brand_rank = ranks(db->brand.values);
+      if (db->part_type.values.size() <= 65536) db->type_rank = ranks(db->part_type.values);
     }
     {  // region name -> key, the first row of a name (builder_impl.cpp:805-826)
       const auto& R = tables->region;
@@ -2198,6 +2493,33 @@ void query(Database* db) {
       const auto rows = run_q18(*db, quantity);
       const auto end = std::chrono::steady_clock::now();
       write_q18_csv(*db, file, rows);
+      report(end);
+    } else if (r.id == "20") {
+      const std::string color = arg("COLOR");
+      const std::string date = arg("DATE");
+      const std::string nation = arg("NATION");
+      const auto rows = run_q20(*db, color, date, nation);
+      const auto end = std::chrono::steady_clock::now();
+      write_q20_csv(file, rows);
+      report(end);
+    } else if (r.id == "2") {
+      const std::string size = arg("SIZE");
+      const std::string type = arg("TYPE");
+      const std::string region = arg("REGION");
+      const auto rows = run_q2(*db, size, type, region);
+      const auto end = std::chrono::steady_clock::now();
+      write_q2_csv(file, rows);
+      report(end);
+    } else if (r.id == "16") {
+      const std::string brand = arg("BRAND");
+      const std::string type = arg("TYPE");
+      std::string sizes[8];
+      static const char* const kSizeNames[8] = {"SIZE1", "SIZE2", "SIZE3", "SIZE4",
+                                                "SIZE5", "SIZE6", "SIZE7", "SIZE8"};
+      for (int i = 0; i < 8; ++i) sizes[i] = arg(kSizeNames[i]);
+      const auto rows = run_q16(*db, brand, type, sizes);
+      const auto end = std::chrono::steady_clock::now();
+      write_q16_csv(file, rows);
       report(end);
     } else if (r.id == "6") {
       const std::string date = arg("DATE");

@@ -142,6 +142,23 @@ struct Database {
   // supplier rows' keys and nationkeys (Q7's supplier tags), strings (Q15)
   std::vector<int32_t> s_suppkey, s_nationkey;
   bo_tpch::StringColumn s_name, s_address, s_phone;
+  // Supplier comments and, by suppkey, run_q16's complaint flags (computed on
+  // the device at build: they do not depend on a query's parameters).
+  bo_tpch::StringColumn s_comment;
+  bo_tpch::DeviceColumn s_comment_chars, s_comment_offsets, s_suppkey_device, s_banned;
+  int64_t n_s_banned = 0;
+  // Ranks of the brand and type dictionary entries in string order (Q16's tie order).
+  std::vector<uint16_t> brand_rank, type_rank;
+  // Q20: supplier nations by suppkey (-1: none), nations and rows in s_name order.
+  bo_tpch::DeviceColumn s_nation_by_key, s_nationkey_device, s_row_by_name, ps_availqty;
+  int32_t s_max_suppkey = -1;
+  // Q2: balances (x100), nation index by supplier row (the nation key when below
+  // the nation row count, else -1) with its name, and each row's position in
+  // (acctbal desc, nation name, s_name, row) order.
+  std::vector<int32_t> s_acctbal, s_nation_idx;
+  std::vector<std::string> nation_name_by_idx;
+  bo_tpch::DeviceColumn s_nation_idx_device, s_rank, p_mfgr;
+  bo_tpch::Dictionary mfgr;
   std::unordered_map<std::string, int32_t> region_key_by_name;
   // Result record of the last scan-agg / Q6 query.  Queries on one Database
   // run one at a time (as the reference's single-threaded query()).
@@ -255,6 +272,29 @@ struct Q13ResultRow {
   int64_t custdist = 0;
 };
 
+struct Q20ResultRow {
+  std::string_view s_name;
+  std::string_view s_address;
+};
+
+struct Q2ResultRow {
+  int32_t s_acctbal_raw = 0;
+  std::string_view s_name;
+  std::string_view n_name;
+  int32_t p_partkey = 0;
+  std::string_view p_mfgr;
+  std::string_view s_address;
+  std::string_view s_phone;
+  std::string_view s_comment;
+};
+
+struct Q16ResultRow {
+  std::string_view p_brand;
+  std::string_view p_type;
+  int32_t p_size = 0;
+  int64_t supplier_cnt = 0;
+};
+
 // Allocator that leaves elements default-constructed as nothing: for result
 // rows every field of which the query writes in parallel right after the
 // allocation (a value-initialising std::vector would first write the whole
@@ -327,6 +367,8 @@ std::vector<Q12ResultRow> run_q12(const Database& db, const std::string& shipmod
                                   const std::string& date);
 std::vector<Q13ResultRow> run_q13(const Database& db, const std::string& word1, const std::string& word2);
 std::vector<Q18ResultRow> run_q18(const Database& db, const std::string& quantity);
+std::vector<Q16ResultRow> run_q16(const Database& db, const std::string& brand, const std::string& type,
+                                  const std::string sizes[8]);
 
 void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& rows);
 void write_q3_csv(const Database& db, const std::string& filename, const std::vector<Q3ResultRow>& rows);
@@ -347,5 +389,12 @@ void write_q14_csv(const std::string& filename, const std::vector<Q14ResultRow>&
 void write_q12_csv(const std::string& filename, const std::vector<Q12ResultRow>& rows);
 void write_q13_csv(const std::string& filename, const std::vector<Q13ResultRow>& rows);
 void write_q18_csv(const Database& db, const std::string& filename, const std::vector<Q18ResultRow>& rows);
+void write_q16_csv(const std::string& filename, const std::vector<Q16ResultRow>& rows);
+std::vector<Q20ResultRow> run_q20(const Database& db, const std::string& color, const std::string& date,
+                                  const std::string& nation);
+void write_q20_csv(const std::string& filename, const std::vector<Q20ResultRow>& rows);
+std::vector<Q2ResultRow> run_q2(const Database& db, const std::string& size, const std::string& type,
+                                const std::string& region);
+void write_q2_csv(const std::string& filename, const std::vector<Q2ResultRow>& rows);
 
 }  // namespace bo_tpch

@@ -418,6 +418,51 @@ class TpchQ12Tables(C.Structure):
                 ("n_orders", C.c_int64)]
 
 
+class TpchQ16Tables(C.Structure):
+    """``bo_tpch_q16_tables``: part keys, brand / type codes, sizes; partsupp (by partkey); supplier flags."""
+    _fields_ = [("p_partkey", C.c_void_p), ("p_brand", C.c_void_p), ("p_type", C.c_void_p), ("p_size", C.c_void_p),
+                ("n_part", C.c_int64), ("ps_partkey", C.c_void_p), ("ps_suppkey", C.c_void_p),
+                ("n_partsupp", C.c_int64), ("s_banned", C.c_void_p), ("n_banned", C.c_int64)]
+
+
+class TpchQ16Params(C.Structure):
+    """``bo_tpch_q16_params``: size mask, banned brand, rows per part, dictionary ranks (host arrays)."""
+    _fields_ = [("size_mask", C.c_uint64), ("banned_brand", C.c_int32), ("rows_per_part", C.c_int32),
+                ("n_brand", C.c_int32), ("n_type", C.c_int32), ("brand_rank", C.c_void_p),
+                ("type_rank", C.c_void_p), ("type_banned", C.c_void_p)]
+
+
+class TpchQ16Row(C.Structure):
+    _fields_ = [("brand_code", C.c_int32), ("type_code", C.c_int32), ("size", C.c_int32), ("pad", C.c_int32),
+                ("supplier_cnt", C.c_int64)]
+
+
+class TpchQ20Tables(C.Structure):
+    """``bo_tpch_q20_tables``: part keys and names; lineitem ship dates, keys, supplier nations, quantities;
+    partsupp (by partkey) with availqty and per-partkey offsets; supplier nations by key, rows in name order."""
+    _fields_ = [("p_partkey", C.c_void_p), ("p_name", C.c_void_p), ("p_name_offsets", C.c_void_p),
+                ("n_part", C.c_int64), ("max_partkey", C.c_int32), ("max_suppkey", C.c_int32),
+                ("l_shipdate", C.c_void_p), ("l_partkey", C.c_void_p), ("l_suppkey", C.c_void_p),
+                ("l_supp_nation", C.c_void_p), ("l_quantity", C.c_void_p), ("n_lineitem", C.c_int64),
+                ("ps_partkey", C.c_void_p), ("ps_suppkey", C.c_void_p), ("ps_availqty", C.c_void_p),
+                ("n_partsupp", C.c_int64), ("ps_part_begin", C.c_void_p), ("n_ps_part_keys", C.c_int64),
+                ("s_nation_by_key", C.c_void_p), ("s_suppkey", C.c_void_p), ("s_nationkey", C.c_void_p),
+                ("s_row_by_name", C.c_void_p), ("n_supplier", C.c_int64)]
+
+
+class TpchQ2Tables(C.Structure):
+    """``bo_tpch_q2_tables``: part sizes, type and manufacturer codes; partsupp suppkeys and costs with
+    per-partkey offsets; supplier nation indexes and order ranks."""
+    _fields_ = [("p_size", C.c_void_p), ("p_type", C.c_void_p), ("p_mfgr", C.c_void_p), ("n_part", C.c_int64),
+                ("ps_suppkey", C.c_void_p), ("ps_supplycost", C.c_void_p), ("n_partsupp", C.c_int64),
+                ("ps_part_begin", C.c_void_p), ("n_ps_part_keys", C.c_int64), ("s_nation_idx", C.c_void_p),
+                ("s_rank", C.c_void_p), ("n_supplier", C.c_int64)]
+
+
+class TpchQ2Row(C.Structure):
+    _fields_ = [("partkey", C.c_int32), ("supplier_row", C.c_int32), ("mfgr_code", C.c_int32), ("pad", C.c_int32)]
+
+
 class TpchQ13Tables(C.Structure):
     """``bo_tpch_q13_tables``: order comments (bytes + offsets), custkeys, customer keys."""
     _fields_ = [("o_comment", C.c_void_p), ("o_comment_offsets", C.c_void_p), ("o_custkey", C.c_void_p),
@@ -552,6 +597,13 @@ _SIGNATURES = {
     "bo_tpch_q14": (C.c_int, [_P, C.POINTER(TpchQ14Tables), C.c_int16, C.c_int16, C.POINTER(C.c_int64)]),
     "bo_tpch_q12": (C.c_int, [_P, C.POINTER(TpchQ12Tables), C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int16,
                               C.c_int16, C.POINTER(C.c_int64)]),
+    "bo_tpch_supplier_complaints": (C.c_int, [_P, _P, _P, _P, C.c_int64, _P, C.c_int64]),
+    "bo_tpch_q16": (C.c_int, [_P, C.POINTER(TpchQ16Tables), C.POINTER(TpchQ16Params), C.POINTER(TpchQ16Row),
+                              C.c_int64, C.POINTER(C.c_int64)]),
+    "bo_tpch_q20": (C.c_int, [_P, C.POINTER(TpchQ20Tables), C.c_char_p, C.c_int32, C.c_int32, C.c_int16,
+                              C.c_int16, _P, C.c_int64, C.POINTER(C.c_int64)]),
+    "bo_tpch_q2": (C.c_int, [_P, C.POINTER(TpchQ2Tables), C.c_int32, _P, C.c_int32, _P, C.c_int32,
+                             C.POINTER(TpchQ2Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q13": (C.c_int, [_P, C.POINTER(TpchQ13Tables), C.c_char_p, C.c_int64, C.c_char_p, C.c_int64,
                               C.POINTER(TpchQ13Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q18": (C.c_int, [_P, C.POINTER(TpchQ18Tables), C.c_int32, C.POINTER(TpchQ18Row), C.c_int64,

@@ -36,6 +36,15 @@ Key layouts (they select the reference's code paths):
                     The reference's Q17 reads its part bitmap at each
                     lineitem's partkey unchecked (query_q17.cpp:205-259), so
                     its parity data covers every lineitem partkey.
+  lineitem_keys     "narrow": lineitems name parts 1..199 and suppliers 1..9;
+                    "partsupp": each lineitem names one of the four
+                    (partkey, suppkey) pairs of a random part 1..n_part, as in
+                    TPC-H (a stream of its own).
+  repeat_part       a last part row repeating key 3 with another type (the
+                    later row wins); without it the part table has n_part
+                    rows and partsupp four per part, the case the
+                    reference's Q16 walks by row position
+                    (query_q16.cpp:391-414).
 Regions REGION0..REGION4 (keys 0..4; nations' regionkey = nationkey % 5) and
 a later row repeating REGION1 with key 9.
 Part names are three words of COLORS.  Ship modes MODE_A..MODE_G, AIR and AIR REG, ship
@@ -46,6 +55,10 @@ without the PROMO prefix Q14 looks for.  Commit dates 30..90 days
 after the order, receipts 1..30 days after shipping.  These columns come from
 a second seeded stream, so the other columns do not depend on them.
 The nation table has keys 0..24 except 7; customers' nationkeys run 0..26.
+Supplier comments are one to four words of SUPPLIER_WORDS (some contain
+"Customer" before "Complaints", which Q16 bans, some the two the other way
+round), supplier balances vary and manufacturers are MFGRS; these come from
+streams of their own too.
 """
 from __future__ import annotations
 
@@ -71,6 +84,11 @@ BRANDS = ["BRAND_A", "BRAND_B", "BRAND_C", "BRAND_D", "BRAND_E"]
 COLORS = ["amber", "azure", "cobalt", "coral", "crimson", "ivory", "jade", "khaki", "lilac", "maroon", "ochre",
           "olive", "pearl", "plum", "rust", "sage", "sand", "slate", "teal", "umber"]
 CONTAINERS = ["CONT_A", "CONT_B", "CONT_C", "CONT_D"] + Q19_CONTAINERS
+# supplier-comment words: run_q16 bans suppliers whose comment has "Customer"
+# and, after it, "Complaints" (bespoke_tpch/query_q16.cpp:58-67)
+SUPPLIER_WORDS = ["ironic", "Customer", "Complaints", "Customer Complaints", "requests", "Complaints Customer",
+                  "CustomerComplaints", "carefully", "Customer Complaint", "say \"hi\""]
+MFGRS = ["Manufacturer#1", "Manufacturer#2", "Manufacturer#3", "Manufacturer#4", "Manufacturer#5"]
 D1992 = 8035  # 1992-01-01 in days since 1970-01-01
 
 
@@ -105,7 +123,8 @@ def _ragged_text(rng, n: int, max_words: int) -> list[str]:
 def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: int = 0,
                decimal: bool = False, order_keys: str = "sparse", customer_keys: str = "dense",
                shuffle_lineitem: bool = False, late_receipts: bool = False, customer_nations: str = "wide",
-               n_supplier: int = 1, n_part: int = 150, orderless_customers: bool = False) -> Path:
+               n_supplier: int = 1, n_part: int = 150, orderless_customers: bool = False,
+               repeat_part: bool = True, lineitem_keys: str = "narrow") -> Path:
     rng = np.random.default_rng(seed)
     rng2 = np.random.default_rng([seed, 12])
     out.mkdir(parents=True, exist_ok=True)
@@ -170,9 +189,19 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
         perm = rng.permutation(n)
         lk, ld, qty, price, ship, rf, ls, commit, receipt, mode = (
             a[perm] for a in (lk, ld, qty, price, ship, rf, ls, commit, receipt, mode))
+    l_part = rng.integers(1, 200, n).astype(np.int32)
+    l_supp = rng.integers(1, 10, n).astype(np.int32)
+    ns_ = max(n_supplier, 1)
+    if lineitem_keys == "partsupp":  # a partsupp pair of a random part (the four below)
+        rng7 = np.random.default_rng([seed, 21])
+        l_part = rng7.integers(1, n_part + 1, n).astype(np.int32)
+        j = rng7.integers(0, 4, n)
+        l_supp = ((l_part - 1 + j * (ns_ // 4 + 1)) % ns_ + 1).astype(np.int32)
+    elif lineitem_keys != "narrow":
+        raise ValueError(lineitem_keys)
     pq.write_table(pa.table({
-        "l_orderkey": lk, "l_partkey": rng.integers(1, 200, n).astype(np.int32),
-        "l_suppkey": rng.integers(1, 10, n).astype(np.int32), "l_linenumber": np.ones(n, np.int32),
+        "l_orderkey": lk, "l_partkey": l_part,
+        "l_suppkey": l_supp, "l_linenumber": np.ones(n, np.int32),
         "l_quantity": _dec(qty.astype(np.float64), decimal), "l_extendedprice": _dec(price, decimal),
         "l_discount": _dec(rng.integers(0, 11, n) / 100.0, decimal), "l_tax": _dec(rng.integers(0, 9, n) / 100.0, decimal),
         "l_returnflag": rf.tolist(), "l_linestatus": ls.tolist(),
@@ -187,10 +216,11 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
     # parts 1..n_part (lineitems name 1..199, so by default some have no part)
     # and a last row repeating key 3 with another type (the later row wins)
     rng3 = np.random.default_rng([seed, 14])
-    pkey = np.concatenate([np.arange(1, n_part + 1), [3]]).astype(np.int32)
+    pkey = np.concatenate([np.arange(1, n_part + 1), [3] if repeat_part else []]).astype(np.int32)
     rows_p = len(pkey)
     ptype = [PART_TYPES[i] for i in rng3.integers(0, len(PART_TYPES), rows_p)]
-    ptype[-1] = "STD_A" if ptype[2].startswith("PROMO") else "PROMO_B"
+    if repeat_part:
+        ptype[-1] = "STD_A" if ptype[2].startswith("PROMO") else "PROMO_B"
     psize = rng3.integers(1, 51, rows_p).astype(np.int32)
     pbrand = [BRANDS[i] for i in rng3.integers(0, len(BRANDS), rows_p)]
     pcont = [CONTAINERS[i] for i in rng3.integers(0, len(CONTAINERS), rows_p)]
@@ -198,7 +228,8 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
     # part columns do not depend on them)
     rng5 = np.random.default_rng([seed, 15])
     pname = [" ".join(COLORS[i] for i in row) for row in rng5.integers(0, len(COLORS), (rows_p, 3))]
-    pq.write_table(pa.table({"p_partkey": pkey, "p_name": pname, "p_mfgr": ["m"] * rows_p,
+    pmfgr = [MFGRS[i] for i in np.random.default_rng([seed, 20]).integers(0, len(MFGRS), rows_p)]
+    pq.write_table(pa.table({"p_partkey": pkey, "p_name": pname, "p_mfgr": pmfgr,
                              "p_brand": pbrand, "p_type": ptype, "p_size": psize, "p_container": pcont,
                              "p_retailprice": _dec(np.ones(rows_p), decimal), "p_comment": [""] * rows_p}),
                    out / "part.parquet")
@@ -208,10 +239,14 @@ def write_tpch(out: Path, n_customer: int = 1500, n_orders: int = 15000, seed: i
         skey = np.arange(1, n_supplier + 1, dtype=np.int32)
         snation = np.random.default_rng([seed, 5]).integers(0, 25, n_supplier).astype(np.int32)
     ns = len(skey)
+    rng6 = np.random.default_rng([seed, 18])
+    s_comment = [" ".join(SUPPLIER_WORDS[i] for i in rng6.integers(0, len(SUPPLIER_WORDS), c))
+                 for c in rng6.integers(1, 5, ns)]
+    s_acctbal = np.random.default_rng([seed, 19]).integers(-99999, 999999, ns) / 100.0
     pq.write_table(pa.table({"s_suppkey": skey, "s_name": [f"Supplier#{k:09d}" for k in skey],
                              "s_address": [f"addr {k}, \"{k % 7}\"" for k in skey], "s_nationkey": snation,
                              "s_phone": [f"{10 + k % 25}-{k:03d}-000-0000" for k in skey],
-                             "s_acctbal": _dec(np.ones(ns), decimal), "s_comment": [""] * ns}),
+                             "s_acctbal": _dec(s_acctbal, decimal), "s_comment": s_comment}),
                    out / "supplier.parquet")
     # four suppliers per part (key 1..n_part), rows in random order
     rng4 = np.random.default_rng([seed, 11])

@@ -1197,6 +1197,146 @@ int bo_tpch_q12(bo_ctx* ctx, const bo_tpch_q12_tables* tables, int32_t mode_code
                 int32_t high_code1, int32_t high_code2, int16_t start_offset, int16_t end_offset,
                 int64_t counts_out[4]);
 
+/* Supplier complaint flags, the supplier scan of run_q16
+ * (bespoke_tpch/query_q16.cpp:357-368, the search of :58-67): for each
+ * supplier row whose comment (bytes [offsets[r], offsets[r + 1]) of
+ * comments) holds "Customer" and, after it, "Complaints",
+ * banned_out[suppkeys[r]] = 1.  banned_out (device, n_banned bytes) is
+ * cleared first; suppkeys outside [0, n_banned) set nothing.  The flags do not
+ * depend on a query's parameters, so a database computes them once. */
+int bo_tpch_supplier_complaints(bo_ctx* ctx, const char* comments_device, const uint32_t* offsets_device,
+                                const int32_t* suppkeys_device, int64_t n_supplier, uint8_t* banned_out,
+                                int64_t n_banned);
+
+/* TPC-H Q16 over the storage-plan layout: run_q16 of
+ * bespoke_tpch/query_q16.cpp:167-541.  A part row qualifies when its brand
+ * code is not banned_brand, its size s (0 <= s <= 50) has bit s of size_mask
+ * set and its type code's type_banned byte is 0; a partkey k in
+ * [0, n_part] takes the group (brand, type, size) of its LAST qualifying
+ * row (:276-342).  A partsupp row's partkey is ps_partkey[r], or
+ * r / rows_per_part + 1 when rows_per_part > 0 (the reference's walk by row
+ * position when the partsupp rows are a multiple of the part rows,
+ * :391-414); rows whose partkey has a group and whose suppkey is not flagged
+ * in s_banned count that suppkey once per group (distinct, :449-476).  Rows
+ * out: one per group with a count, by count descending, then brand, type
+ * (by their ranks in string order) and size ascending (:489-521).
+ * rows_out holds max_rows rows; *n_rows is the number of groups (rows past
+ * max_rows are not written).  Groups: n_brand * n_type * 64 <= 2^28. */
+typedef struct bo_tpch_q16_tables {
+  const int32_t* p_partkey;
+  const uint16_t* p_brand;             /* dictionary codes */
+  const uint16_t* p_type;              /* dictionary codes */
+  const int32_t* p_size;
+  int64_t n_part;
+  const int32_t* ps_partkey;           /* partsupp rows (stably) sorted by partkey */
+  const int32_t* ps_suppkey;
+  int64_t n_partsupp;
+  const uint8_t* s_banned;             /* by suppkey (bo_tpch_supplier_complaints) */
+  int64_t n_banned;
+} bo_tpch_q16_tables;
+
+typedef struct bo_tpch_q16_params {
+  uint64_t size_mask;                  /* bit s: size s qualifies (s <= 50) */
+  int32_t banned_brand;                /* brand code; -1: none */
+  int32_t rows_per_part;               /* > 0: partkey of partsupp row r is r / rows_per_part + 1 */
+  int32_t n_brand;                     /* brand dictionary entries */
+  int32_t n_type;                      /* type dictionary entries */
+  const uint16_t* brand_rank;          /* host, n_brand: rank of each code in string order */
+  const uint16_t* type_rank;           /* host, n_type */
+  const uint8_t* type_banned;          /* host, n_type: 1 = the type starts with the query's TYPE */
+} bo_tpch_q16_params;
+
+typedef struct bo_tpch_q16_row {
+  int32_t brand_code;
+  int32_t type_code;
+  int32_t size;
+  int32_t pad;
+  int64_t supplier_cnt;
+} bo_tpch_q16_row;
+
+int bo_tpch_q16(bo_ctx* ctx, const bo_tpch_q16_tables* tables, const bo_tpch_q16_params* params,
+                bo_tpch_q16_row* rows_out, int64_t max_rows, int64_t* n_rows);
+
+/* TPC-H Q20 over the storage-plan layout: run_q20 of
+ * bespoke_tpch/query_q20.cpp:338-676.  Partkeys in [0, max_partkey] whose
+ * part name starts with `color` (:375-392); the quantities of lineitems
+ * shipped in [start_offset, end_offset) (as (uint32)(ship - start) <
+ * (uint32)(end - start), :412-421) by a supplier of nation_key with such a
+ * partkey, summed per (partkey, suppkey) (:405-560 -- the builder's month
+ * shards select the same rows); a partsupp row with such a partkey, a
+ * supplier of nation_key and a sum with 2 * 100 * availqty > sum qualifies
+ * its suppkey (:568-615).  Rows out: the supplier rows of nation_key whose
+ * suppkey qualified, in s_name order (s_row_by_name: the supplier rows
+ * sorted by name), :618-644.  A lineitem's (partkey, suppkey) is summed into
+ * its first partsupp row of that pair (ps_part_begin: each partkey's rows);
+ * pairs without a partsupp row are never looked up, as in the reference. */
+typedef struct bo_tpch_q20_tables {
+  const int32_t* p_partkey;
+  const char* p_name;
+  const uint32_t* p_name_offsets;      /* n_part + 1 */
+  int64_t n_part;
+  int32_t max_partkey;                 /* largest part key; < 0: none */
+  int32_t max_suppkey;                 /* largest supplier key; < 0: none */
+  const int16_t* l_shipdate;
+  const int32_t* l_partkey;
+  const int32_t* l_suppkey;
+  const int16_t* l_supp_nation;        /* -1: no supplier row */
+  const int16_t* l_quantity;           /* x100 */
+  int64_t n_lineitem;
+  const int32_t* ps_partkey;           /* partsupp rows sorted by partkey */
+  const int32_t* ps_suppkey;
+  const int32_t* ps_availqty;
+  int64_t n_partsupp;
+  const int32_t* ps_part_begin;        /* n_ps_part_keys + 1 row offsets */
+  int64_t n_ps_part_keys;
+  const int16_t* s_nation_by_key;      /* max_suppkey + 1 entries; -1: none */
+  const int32_t* s_suppkey;
+  const int32_t* s_nationkey;
+  const int32_t* s_row_by_name;        /* n_supplier */
+  int64_t n_supplier;
+} bo_tpch_q20_tables;
+
+int bo_tpch_q20(bo_ctx* ctx, const bo_tpch_q20_tables* tables, const char* color, int32_t color_len,
+                int32_t nation_key, int16_t start_offset, int16_t end_offset, int32_t* supplier_rows_out,
+                int64_t max_rows, int64_t* n_rows);
+
+/* TPC-H Q2 over the storage-plan layout: run_q2 of
+ * bespoke_tpch/query_q2.cpp:146-430.  Part rows p with size target_size and
+ * a type code whose type_ok byte is set (:214-265) take partkey p + 1 (the
+ * reference's assumption) and its partsupp rows (ps_part_begin); a row's
+ * supplier is row suppkey - 1 (again the reference's) when below n_supplier
+ * and its s_nation_idx has a set nation_ok byte (:186-212).  Of those rows,
+ * the ones with the least supplycost (below INT32_MAX) each give a result
+ * row (:300-381).  Rows out by s_rank[supplier row] (the row's position in
+ * (acctbal desc, nation name, s_name, row) order, unique) then partkey
+ * (:386-401).
+ * *n_rows counts all rows; rows past max_rows are not written. */
+typedef struct bo_tpch_q2_tables {
+  const int32_t* p_size;
+  const uint16_t* p_type;              /* dictionary codes */
+  const uint16_t* p_mfgr;              /* dictionary codes */
+  int64_t n_part;
+  const int32_t* ps_suppkey;           /* partsupp rows sorted by partkey */
+  const int32_t* ps_supplycost;        /* x100 */
+  int64_t n_partsupp;
+  const int32_t* ps_part_begin;        /* n_ps_part_keys + 1 row offsets */
+  int64_t n_ps_part_keys;
+  const int32_t* s_nation_idx;         /* nation key when below the nation row count, else -1 */
+  const uint32_t* s_rank;               /* a permutation of 0 .. n_supplier - 1 */
+  int64_t n_supplier;
+} bo_tpch_q2_tables;
+
+typedef struct bo_tpch_q2_row {
+  int32_t partkey;
+  int32_t supplier_row;
+  int32_t mfgr_code;
+  int32_t pad;
+} bo_tpch_q2_row;
+
+int bo_tpch_q2(bo_ctx* ctx, const bo_tpch_q2_tables* tables, int32_t target_size, const uint8_t* type_ok_host,
+               int32_t n_type, const uint8_t* nation_ok_host, int32_t n_nation, bo_tpch_q2_row* rows_out,
+               int64_t max_rows, int64_t* n_rows);
+
 /* ================================================================= BATCH ==
  * Many pipelines of uneven sizes in ONE persistent kernel fed by a device work
  * queue of (instance, stage, tile) items, captured in a CUDA graph.  Stages of

@@ -2,7 +2,7 @@
 query (bespokeolap_artifacts_b200/host) and the reference's own load / build /
 query (compiled unchanged into oracle/_ref/ref_tpch_driver) read the same
 Parquet files and the same stdin requests; their result<idx>.csv files must
-agree: Q1, Q4, Q6, Q10, Q11, Q12, Q13, Q14 and Q18 byte for byte, Q3 row for row (the reference's
+agree: Q1, Q4, Q6, Q10, Q11, Q12, Q13, Q14, Q16 and Q18 byte for byte, Q3 row for row (the reference's
 std::sort leaves rows equal in revenue and orderdate in unspecified order;
 the GPU emits them in orderkey order).  The key layouts select each of the
 reference's paths: dense and sparse orderkeys (Q18's two scans), dense,
@@ -41,6 +41,10 @@ REQUESTS = [
     '19 "2.5" "2.5" "2.5" "BRAND_E" "BRAND_E" "BRAND_E"', '19 "<<NULL>>" "1" "1" "BRAND_A" "<<NULL>>" "<<NULL>>"',
     '19 "1" "1" "1" "NOSUCH" "BRAND_A" "BRAND_A"', '19 "45" "40" "45" "BRAND_B" "BRAND_C" "BRAND_B"',
     '21 "NATION_00"', '21 "NATION_04"', '21 "NOSUCH"', '21 "<<NULL>>"',
+    '16 "BRAND_A" "PROMO" "1" "5" "9" "14" "23" "36" "45" "49"',
+    '16 "BRAND_C" "STD" "<<NULL>>" "" "7" "x" "51" "49" "2" "3"',
+    '16 "NOSUCH" "" "1" "2" "3" "4" "5" "6" "7" "8"',
+    '16 "BRAND_E" "NOSUCH" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>" "<<NULL>>"',
 ]
 
 LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem, late_receipts)
@@ -107,7 +111,13 @@ Q5_REQUESTS = ['5 "REGION0" "1994-01-01"', '5 "REGION1" "1995-02-28"', '5 "REGIO
                '17 "BRAND_B" "CONT_C"', '17 "BRAND_E" "CONT_A"', '17 "NOSUCH" "CONT_A"', '17 "<<NULL>>" "CONT_A"',
                '17 "BRAND_A" "<<NULL>>"',
                '9 "co"', '9 "slate"', '9 "e p"', '9 ""', '9 "nosuchcolor"', '9 "umber umber"',
-               '21 "NATION_04"', '21 "NATION_10"', '21 "NATION_19"', '21 "NATION_07"']
+               '21 "NATION_04"', '21 "NATION_10"', '21 "NATION_19"', '21 "NATION_07"',
+               '16 "BRAND_B" "ECO_A" "10" "15" "20" "25" "30" "35" "40" "45"',
+               '16 "BRAND_D" "PROMO_A" "3" "6" "9" "12" "18" "27" "33" "50"',
+               '16 "NOSUCH" "NOSUCH" "1" "2" "3" "4" "5" "6" "7" "8"',
+               '16 "BRAND_A" "S" "40" "41" "42" "43" "44" "46" "47" "48"',
+               '2 "15" "_A" "REGION0"', '2 "7" "" "REGION4"', '2 "3" "A" "REGION1"',
+               '20 "" "1993-06-30" "NATION_19"', '20 "ivory" "1994-01-01" "NATION_03"']
 
 Q5_LAYOUTS = [  # (seed, decimal, order_keys, customer_keys, shuffle_lineitem): known nations, 25 suppliers
     (11, False, "sparse", "dense", False),
@@ -149,11 +159,67 @@ def test_dropin_q5_matches_reference_driver(tmp_path, layout):
             assert g.read_bytes() == r.read_bytes(), req
 
 
-def test_dropin_stub_for_queries_off_the_gpu_path(tmp_path):
+Q2_Q20_REQUESTS = ['2 "15" "_A" "REGION0"', '2 "3" "A" "REGION1"', '2 "40" "PROMOTION" "REGION3"', '2 "7" "" "REGION4"',
+                   '2 "22" "_B" "NOSUCH"', '2 "1" "ECO_A" "REGION2"',
+                   '20 "ivory" "1994-01-01" "NATION_03"', '20 "c" "1995-03-01" "NATION_10"',
+                   '20 "" "1993-06-30" "NATION_19"', '20 "nosuch" "1994-01-01" "NATION_03"',
+                   '20 "<<NULL>>" "1994-01-01" "NATION_03"', '20 "s" "1996-02-29" "NOSUCH"']
+
+
+def test_dropin_wide_keys_matches_reference_driver(tmp_path):
+    """Every query on TPC-H-like keys (each lineitem names a partsupp pair;
+    100 suppliers, about four per nation; 400 parts), with Q2 and Q20
+    parameters chosen from the data so that their answers have many rows."""
+    if not REF_DRIVER.exists() or not GPU_DRIVER.exists():
+        pytest.skip("drivers not built")
+    data = write_tpch(tmp_path / "data", n_customer=2000, n_orders=30000, seed=21, customer_nations="known",
+                      n_supplier=100, n_part=400, lineitem_keys="partsupp")
+    import pyarrow.parquet as pq
+    s, n, pt = (pq.read_table(data / f"{x}.parquet") for x in ("supplier", "nation", "part"))
+    nations = s["s_nationkey"].to_pylist()
+    top = dict(zip(n["n_nationkey"].to_pylist(), n["n_name"].to_pylist()))[max(set(nations), key=nations.count)]
+    sizes = pt["p_size"].to_pylist()
+    size = max(set(sizes), key=sizes.count)
+    requests = (Q5_REQUESTS + Q2_Q20_REQUESTS +
+                [f'20 "" "1994-01-01" "{top}"', f'20 "a" "1995-06-30" "{top}"', f'20 "s" "1997-02-28" "{top}"'] +
+                [f'2 "{size}" "" "REGION{r}"' for r in range(5)] + [f'2 "{size}" "_A" "REGION1"'])
+    run(GPU_DRIVER, data, tmp_path / "gpu", requests)
+    run(REF_DRIVER, data, tmp_path / "ref", requests)
+    for i, req in enumerate(requests, start=1):
+        g, r = tmp_path / "gpu" / f"result{i}.csv", tmp_path / "ref" / f"result{i}.csv"
+        assert g.read_bytes() == r.read_bytes(), req
+    lines = [len((tmp_path / "gpu" / f"result{i}.csv").read_text().splitlines()) for i in range(1, len(requests) + 1)]
+    assert max(lines[-9:-6]) > 2 and max(lines[-6:]) > 5  # Q20 and Q2 answers of several rows
+
+
+@pytest.mark.parametrize("n_part,repeat", [(40, False), (3, True)], ids=["by_position", "misattributed"])
+def test_dropin_q16_partsupp_walked_by_position(tmp_path, n_part, repeat):
+    """run_q16 walks partsupp by row position when its row count is a
+    multiple of the part rows (bespoke_tpch/query_q16.cpp:383-414): four rows
+    per part over 40 parts (the position is the key), three per part over
+    four part rows with a repeated key (it is not).  CSVs byte-equal."""
+    if not REF_DRIVER.exists() or not GPU_DRIVER.exists():
+        pytest.skip("drivers not built")
+    data = write_tpch(tmp_path / "data", n_customer=300, n_orders=2000, seed=13, n_supplier=25, n_part=n_part,
+                      repeat_part=repeat)
+    import pyarrow.parquet as pq
+    sizes = list(dict.fromkeys(pq.read_table(data / "part.parquet")["p_size"].to_pylist()))[:8]
+    sizes += ["<<NULL>>"] * (8 - len(sizes))
+    requests = ['16 "NOSUCH" "NOSUCH" ' + " ".join(f'"{x}"' for x in sizes),
+                '16 "BRAND_A" "PROMO" "1" "5" "9" "14" "23" "36" "45" "49"', '1 "90"']
+    run(GPU_DRIVER, data, tmp_path / "gpu", requests)
+    run(REF_DRIVER, data, tmp_path / "ref", requests)
+    for i in range(1, len(requests) + 1):
+        g, r = tmp_path / "gpu" / f"result{i}.csv", tmp_path / "ref" / f"result{i}.csv"
+        assert g.read_bytes() == r.read_bytes(), requests[i - 1]
+    assert len((tmp_path / "gpu" / "result1.csv").read_text().splitlines()) > 1
+
+
+def test_dropin_stub_for_unknown_query_ids(tmp_path):
     if not GPU_DRIVER.exists():
         pytest.skip("driver not built")
     data = write_tpch(tmp_path / "data", n_customer=50, n_orders=200, seed=5)
-    run(GPU_DRIVER, data, tmp_path / "gpu", ['2 "15" "PART_T" "REGION0"', '1 "90"'])
+    run(GPU_DRIVER, data, tmp_path / "gpu", ['23 "15" "PART_T" "REGION0"', '1 "90"'])
     assert (tmp_path / "gpu" / "result1.csv").read_text() == \
-        'query_id,params\n"2","2 \\"15\\" \\"PART_T\\" \\"REGION0\\""\n'
+        'query_id,params\n"23","23 \\"15\\" \\"PART_T\\" \\"REGION0\\""\n'
     assert (tmp_path / "gpu" / "result2.csv").read_text().startswith("l_returnflag,")

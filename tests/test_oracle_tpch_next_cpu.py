@@ -475,3 +475,212 @@ def test_q5_q7_q8_q9_q17_q19_q21_q22_restatements_match_the_reference(known, tmp
     for q in ("5 ", "7 ", "8 ", "9 ", "11 ", "15 ", "17 ", "19 ", "21 ", "22 "):
         assert any(len(g) > 1 and any(x != "0.00" for row in g[1:] for x in (row[1:] if len(row) > 1 else row))
                    for (req, _), g in zip(cases, got) if req.startswith(q)), q
+
+
+# ---- Q16 (bespoke_tpch/query_q16.cpp:167-541): parts by brand / type prefix /
+# size, suppliers whose comment has "Customer" and then "Complaints" banned,
+# distinct suppliers per (brand, type, size).
+
+def q16(t, brand, ptype, sizes, by_key=False):
+    P, PS, S = t["part"], t["partsupp"], t["supplier"]
+    listed = [0 if v == "" else int(v) for v in sizes if v != "<<NULL>>" and all("0" <= c <= "9" for c in v)]
+    if not listed or P.num_rows == 0:
+        return []
+    mask = {s for s in listed if 0 <= s <= 50}
+    group = {}  # partkey -> (brand, type, size) of its last qualifying row
+    for k, b, ty, sz in zip(*(P[c].to_pylist() for c in ("p_partkey", "p_brand", "p_type", "p_size"))):
+        if b != brand and sz in mask and not ty.startswith(ptype):
+            group[k] = (b, ty, sz)
+    if S.num_rows == 0:
+        return []
+    banned = set()
+    for k, c in zip(S["s_suppkey"].to_pylist(), S["s_comment"].to_pylist()):
+        i = c.find("Customer")
+        if i >= 0 and c.find("Complaints", i + 8) >= 0:
+            banned.add(k)
+    pk, sk = PS["ps_partkey"].to_numpy(), PS["ps_suppkey"].to_numpy()
+    order = np.argsort(pk, kind="stable")  # the builder's partsupp order
+    pk, sk = pk[order], sk[order]
+    if len(pk) and len(pk) % P.num_rows == 0 and not by_key:  # walked by position (:383-414)
+        pk = np.arange(len(pk)) // (len(pk) // P.num_rows) + 1
+    sets = {}
+    for k, s in zip(pk.tolist(), sk.tolist()):
+        if k in group and s not in banned:
+            sets.setdefault(group[k], set()).add(s)
+    rows = sorted(((g, len(v)) for g, v in sets.items()), key=lambda x: (-x[1], x[0]))
+    return [[b, ty, str(sz), str(c)] for (b, ty, sz), c in rows]
+
+
+Q16_CASES = [("BRAND_A", "PROMO", ["1", "5", "9", "14", "23", "36", "45", "49"]),
+             ("BRAND_C", "STD", ["<<NULL>>", "", "7", "x", "51", "49", "2", "3"]),
+             ("NOSUCH", "", ["1", "2", "3", "4", "5", "6", "7", "8"]),
+             ("BRAND_B", "ECO_A", [str(s) for s in range(10, 50, 5)]),
+             ("BRAND_E", "NOSUCH", ["<<NULL>>"] * 8)]
+
+
+def q16_request(brand, ptype, sizes):
+    return " ".join(["16", f'"{brand}"', f'"{ptype}"'] + [f'"{s}"' for s in sizes])
+
+
+@pytest.mark.parametrize("layout", ["known", "by_position", "misattributed"])
+def test_q16_restatement_matches_the_reference(known, tmp_path, layout):
+    """The general path on the known data (200 part rows, 796 partsupp rows);
+    the walk by position with four partsupp rows per part, where it agrees
+    with the keys, and with three per part over four part rows (a repeated
+    key), where it does not."""
+    if layout == "known":
+        data, t = known
+    else:
+        data = write_tpch(tmp_path / "d", n_customer=300, n_orders=2000, seed=13, n_supplier=25,
+                          n_part=40 if layout == "by_position" else 3, repeat_part=layout != "by_position")
+        t = {n: pq.read_table(data / f"{n}.parquet") for n in ("part", "partsupp", "supplier")}
+    # and one case that lists the sizes of the first part rows, so that most of them qualify
+    sizes = list(dict.fromkeys(t["part"]["p_size"].to_pylist()))[:8]
+    cases = Q16_CASES + [("NOSUCH", "NOSUCH", [str(s) for s in sizes] + ["<<NULL>>"] * (8 - len(sizes)))]
+    got = reference(data, tmp_path / "ref", [q16_request(*c) for c in cases])
+    for c, g in zip(cases, got):
+        assert g[0] == ["p_brand", "p_type", "p_size", "supplier_cnt"]
+        assert g[1:] == q16(t, *c), c
+    assert len(got[-1]) > 1
+    if layout == "misattributed":  # the walk by position answers differently from one by key here
+        assert got[-1][1:] != q16(t, *cases[-1], by_key=True)
+    if layout == "by_position":
+        assert all(g[1:] == q16(t, *c, by_key=True) for c, g in zip(cases, got))
+    if layout == "known":  # some suppliers are banned and some groups count several suppliers
+        banned = [c for c in t["supplier"]["s_comment"].to_pylist()
+                  if c.find("Customer") >= 0 and c.find("Complaints", c.find("Customer") + 8) >= 0]
+        assert 0 < len(banned) < t["supplier"].num_rows
+        assert any(int(r[3]) > 1 for g in got for r in g[1:])
+
+
+# ---- Q20 (bespoke_tpch/query_q20.cpp:338-676) and Q2 (query_q2.cpp:146-430).
+
+def esc(x: str) -> str:
+    """The reference's CSV field: quoted, inner quotes as \\" (parsed as its file is)."""
+    return '"' + x.replace('"', '\\"') + '"'
+
+
+def q20(t, color, date, nation):
+    if "<<NULL>>" in (color, date, nation):
+        return []
+    N, P, L, PS, S = t["nation"], t["part"], t["lineitem"], t["partsupp"], t["supplier"]
+    key = first_wins(N["n_name"].to_pylist(), N["n_nationkey"].to_pylist()).get(nation)
+    if key is None:
+        return []
+    start, end = offset(date), offset(date, 12)
+    pkeys = P["p_partkey"].to_pylist()
+    top = max(pkeys)
+    colored = {k for k, nm in zip(pkeys, P["p_name"].to_pylist()) if 0 <= k <= top and nm.startswith(color)}
+    snation = last_wins(S["s_suppkey"].to_pylist(), S["s_nationkey"].to_pylist())
+    ship, qty = days(L["l_shipdate"]), scaled(L["l_quantity"])
+    sums = {}
+    for s, pk, sk, q in zip(ship.tolist(), L["l_partkey"].to_pylist(), L["l_suppkey"].to_pylist(), qty.tolist()):
+        if start <= s < end and snation.get(sk, -1) == key and pk in colored:
+            sums[(pk, sk)] = sums.get((pk, sk), 0) + q
+    qualified = set()
+    for pk, sk, a in zip(PS["ps_partkey"].to_pylist(), PS["ps_suppkey"].to_pylist(), PS["ps_availqty"].to_pylist()):
+        if pk in colored and snation.get(sk, -1) == key and (pk, sk) in sums and a * 2 * 100 > sums[(pk, sk)]:
+            qualified.add(sk)
+    rows = [(nm, ad) for sk, nk, nm, ad in zip(*(S[c].to_pylist() for c in
+                                                  ("s_suppkey", "s_nationkey", "s_name", "s_address")))
+            if sk in qualified and nk == key]
+    return list(csv.reader([",".join(map(esc, r)) for r in sorted(rows)]))
+
+
+def q2(t, size, ptype, region):
+    N, P, PS, S, R = t["nation"], t["part"], t["partsupp"], t["supplier"], t["region"]
+    target = int(size)
+    rkey = first_wins(R["r_name"].to_pylist(), R["r_regionkey"].to_pylist()).get(region)
+    if rkey is None:
+        return []
+    n = N.num_rows
+    name_by_idx, in_region = [""] * n, [False] * n
+    for k, r, nm in zip(N["n_nationkey"].to_pylist(), N["n_regionkey"].to_pylist(), N["n_name"].to_pylist()):
+        if 0 <= k < n:
+            name_by_idx[k] = nm
+            in_region[k] = in_region[k] or r == rkey
+    snk = S["s_nationkey"].to_pylist()
+    s_ok = [0 <= k < n and in_region[k] for k in snk]
+    s_nname = [name_by_idx[k] if 0 <= k < n else "" for k in snk]
+    s_acct = scaled(S["s_acctbal"]).tolist()
+    s_cols = [S[c].to_pylist() for c in ("s_name", "s_address", "s_phone", "s_comment")]
+    pk, sk = PS["ps_partkey"].to_numpy(), PS["ps_suppkey"].to_numpy()
+    order = np.argsort(pk, kind="stable")
+    pk, sk, cost = pk[order], sk[order], scaled(PS["ps_supplycost"])[order]
+    rows_of = {}
+    for i, k in enumerate(pk.tolist()):
+        rows_of.setdefault(k, []).append(i)
+    out = []
+    for p, (sz, ty, mf) in enumerate(zip(*(P[c].to_pylist() for c in ("p_size", "p_type", "p_mfgr")))):
+        if sz != target or not ty.endswith(ptype):
+            continue
+        cand = [(int(cost[i]), int(sk[i]) - 1) for i in rows_of.get(p + 1, [])
+                if 0 <= int(sk[i]) - 1 < S.num_rows and s_ok[int(sk[i]) - 1] and cost[i] < 2**31 - 1]
+        if not cand:
+            continue
+        best = min(c for c, _ in cand)
+        for c, r in cand:
+            if c == best:
+                out.append((s_acct[r], s_nname[r], s_cols[0][r], p + 1, mf, r))
+    out.sort(key=lambda x: (-x[0], x[1], x[2], x[3]))
+    lines = [",".join([f"{a / 100:.2f}", esc(nm), esc(nn), str(k), esc(mf), esc(s_cols[1][r]), esc(s_cols[2][r]),
+                       esc(s_cols[3][r])]) for a, nn, nm, k, mf, r in out]
+    return list(csv.reader(lines))
+
+
+Q20_CASES = [("ivory", "1994-01-01", "NATION_03"), ("c", "1995-03-01", "NATION_10"), ("", "1993-06-30", "NATION_19"),
+             ("nosuch", "1994-01-01", "NATION_03"), ("<<NULL>>", "1994-01-01", "NATION_03"),
+             ("s", "1996-02-29", "NOSUCH")]
+Q2_CASES = [("15", "_A", "REGION0"), ("3", "A", "REGION1"), ("40", "PROMOTION", "REGION3"), ("7", "", "REGION4"),
+            ("22", "_B", "NOSUCH"), ("1", "ECO_A", "REGION2")]
+
+
+@pytest.fixture(scope="module")
+def wide(tmp_path_factory):
+    """TPC-H-like keys: each lineitem names a partsupp pair; 100 suppliers
+    (about four per nation), 400 parts."""
+    if not REF_DRIVER.exists():
+        pytest.skip("reference driver not built")
+    d = write_tpch(tmp_path_factory.mktemp("tpch_wide") / "d", n_customer=2000, n_orders=30000, seed=21,
+                   customer_nations="known", n_supplier=100, n_part=400, lineitem_keys="partsupp")
+    t = {n: pq.read_table(d / f"{n}.parquet")
+         for n in ("lineitem", "orders", "part", "supplier", "customer", "nation", "region", "partsupp")}
+    return d, t
+
+
+def data_cases(t):
+    """Parameters with answers of many rows on this data: Q20 for the nation of
+    the most suppliers, Q2 for the commonest part size."""
+    nations = t["supplier"]["s_nationkey"].to_pylist()
+    top_nation = max(set(nations), key=nations.count)
+    name = dict(zip(t["nation"]["n_nationkey"].to_pylist(), t["nation"]["n_name"].to_pylist()))[top_nation]
+    sizes = t["part"]["p_size"].to_pylist()
+    size = max(set(sizes), key=sizes.count)
+    return ([("", "1994-01-01", name), ("a", "1995-06-30", name), ("s", "1997-02-28", name)],
+            [(str(size), "", f"REGION{r}") for r in range(5)] + [(str(size), "_A", "REGION1")])
+
+
+@pytest.mark.parametrize("fixture", ["known", "wide"])
+def test_q20_q2_restatements_match_the_reference(request, tmp_path, fixture):
+    data, t = request.getfixturevalue(fixture)
+    extra20, extra2 = data_cases(t)
+    c20, c2 = Q20_CASES + extra20, Q2_CASES + extra2
+    reqs = ([" ".join(["20"] + [f'"{x}"' for x in c]) for c in c20] +
+            [" ".join(["2"] + [f'"{x}"' for x in c]) for c in c2])
+    got = reference(data, tmp_path / "ref", reqs)
+    for c, g in zip(c20, got[:len(c20)]):
+        assert g[0] == ["s_name", "s_address"]
+        assert g[1:] == q20(t, *c), c
+    for c, g in zip(c2, got[len(c20):]):
+        assert g[0] == ["s_acctbal", "s_name", "n_name", "p_partkey", "p_mfgr", "s_address", "s_phone", "s_comment"]
+        assert g[1:] == q2(t, *c), c
+    if fixture == "wide":
+        assert any(len(g) > 2 for g in got[:len(c20)]) and any(len(g) > 5 for g in got[len(c20):])
+
+
+def test_q16_restatement_on_wide_keys(wide, tmp_path):
+    data, t = wide
+    got = reference(data, tmp_path / "ref", [q16_request(*c) for c in Q16_CASES])
+    for c, g in zip(Q16_CASES, got):
+        assert g[1:] == q16(t, *c), c
+    assert any(len(g) > 10 for g in got) and any(int(r[3]) > 2 for g in got for r in g[1:])
