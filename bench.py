@@ -1137,6 +1137,8 @@ TPCH_REQUESTS = [  # synthetic parameters: segments, ship modes and comment word
     ("14", '14 "1995-09-01"'), ("15", '15 "1996-01-01" "1"'), ("17", '17 "BRAND_B" "CONT_C"'), ("18", '18 "250"'),
     ("22", '22 "13" "31" "23" "29" "30" "18" "17"'), ("9", '9 "co"'),
     ("19", '19 "1" "10" "20" "BRAND_A" "BRAND_B" "BRAND_C"'), ("21", '21 "NATION_04"'),
+    ("2", '2 "15" "_A" "REGION0"'), ("16", '16 "BRAND_A" "PROMO" "49" "14" "23" "45" "19" "3" "36" "9"'),
+    ("20", '20 "ivory" "1994-01-01" "NATION_03"'),
 ]
 
 
@@ -1159,11 +1161,13 @@ def _driver_times(driver: Path, data: Path, workdir: Path, requests: list[str], 
     return build_ms, t
 
 
-def tpch_section(reps: int = 10, n_customer: int = 150_000, n_orders: int = 1_500_000) -> dict:
+def tpch_section(reps: int = 10, n_customer: int = 150_000, n_orders: int = 1_500_000, n_part: int = 200_000,
+                 n_supplier: int = 10_000) -> dict:
     """The drop-in end to end: the GPU host library's driver and the reference's
     own load / build / query (compiled unchanged, single-threaded queries) read
     the same seeded Parquet files of TPC-H shape (150,000 customers, 1,500,000
-    orders, ~6M lineitems) and answer the same requests, each repeated `reps`
+    orders, ~6M lineitems each naming one of the 800,000 partsupp pairs of
+    200,000 parts and 10,000 suppliers) and answer the same requests, each repeated `reps`
     times; per query the median execution time of each, and whether the
     result<idx>.csv files of the first repetition agree (Q3 up to the order of
     rows tied on revenue and orderdate)."""
@@ -1181,12 +1185,13 @@ def tpch_section(reps: int = 10, n_customer: int = 150_000, n_orders: int = 1_50
     try:
         t0 = time.perf_counter()
         data = write_tpch(tmp / "data", n_customer=n_customer, n_orders=n_orders, seed=11, customer_nations="known",
-                          n_supplier=25, n_part=199, orderless_customers=True)
+                          n_supplier=n_supplier, n_part=n_part, orderless_customers=True, lineitem_keys="partsupp")
         gen_s = time.perf_counter() - t0
         reqs = [r for _, r in TPCH_REQUESTS for _ in range(reps)]
         g_build, g_t = _driver_times(gpu, data, tmp / "gpu", reqs, "us")
         out = {"data": f"seeded synthetic Parquet: {n_customer} customers, {n_orders} orders, "
-                       f"~{4 * n_orders} lineitems (generated in {gen_s:.0f} s)",
+                       f"~{4 * n_orders} lineitems, {n_part} parts, {n_supplier} suppliers, {4 * n_part} partsupp "
+                       f"rows (generated in {gen_s:.0f} s)",
                "reps": reps, "gpu_build_ms": g_build, "queries": {}}
         have_ref = ref.exists()
         if have_ref:

@@ -136,4 +136,69 @@ int ordered_compact(bo_ctx* ctx, const Pred& pred, int64_t n, uint32_t* tile_cou
   return after_launch(ctx, "ordered_emit_kernel");
 }
 
+// Order-preserving compaction of a bitmap: the positions of the set bits of
+// words[0 .. n_words), ascending, into out; their number into *n_out.  Same
+// three launches, a thread owning kBitmapWordsPerThread consecutive words
+// (a tile covers kCompactBlockT * kBitmapWordsPerThread * 32 positions), so
+// the passes read the bitmap, not a per-position predicate's inputs.
+constexpr int kBitmapWordsPerThread = 4;
+constexpr int64_t kBitmapTileWords = (int64_t)kCompactBlockT * kBitmapWordsPerThread;
+
+static __global__ void __launch_bounds__(kCompactBlockT) bitmap_count_kernel(const uint32_t* __restrict__ words,
+                                                                            int64_t n_words,
+                                                                            uint32_t* __restrict__ tile_counts) {
+  const int64_t w0 = (int64_t)blockIdx.x * kBitmapTileWords + (int64_t)threadIdx.x * kBitmapWordsPerThread;
+  uint32_t c = 0;
+#pragma unroll
+  for (int k = 0; k < kBitmapWordsPerThread; ++k)
+    if (w0 + k < n_words) c += __popc(__ldg(words + w0 + k));
+  uint32_t total;
+  compact_block_scan(c, &total);
+  if (threadIdx.x == 0) tile_counts[blockIdx.x] = total;
+}
+
+static __global__ void __launch_bounds__(kCompactBlockT) bitmap_emit_kernel(const uint32_t* __restrict__ words,
+                                                                           int64_t n_words,
+                                                                           const uint32_t* __restrict__ tile_offsets,
+                                                                           uint32_t* __restrict__ out) {
+  const int64_t w0 = (int64_t)blockIdx.x * kBitmapTileWords + (int64_t)threadIdx.x * kBitmapWordsPerThread;
+  uint32_t w[kBitmapWordsPerThread];
+  uint32_t c = 0;
+#pragma unroll
+  for (int k = 0; k < kBitmapWordsPerThread; ++k) {
+    w[k] = w0 + k < n_words ? __ldg(words + w0 + k) : 0u;
+    c += __popc(w[k]);
+  }
+  uint32_t total;
+  uint32_t pos = tile_offsets[blockIdx.x] + compact_block_scan(c, &total);
+#pragma unroll
+  for (int k = 0; k < kBitmapWordsPerThread; ++k) {
+    uint32_t x = w[k];
+    while (x) {
+      const int b = __ffs(x) - 1;
+      out[pos++] = (uint32_t)((w0 + k) * 32 + b);
+      x &= x - 1u;
+    }
+  }
+}
+
+// tile_counts holds ceil(n_words / kBitmapTileWords) words; positions must
+// be below 2^32.
+inline int bitmap_compact(bo_ctx* ctx, const uint32_t* words, int64_t n_words, uint32_t* tile_counts, uint32_t* out,
+                          unsigned long long* n_out) {
+  const int64_t tiles = (n_words + kBitmapTileWords - 1) / kBitmapTileWords;
+  if (tiles == 0) {
+    BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, sizeof(unsigned long long), ctx->stream));
+    return BO_OK;
+  }
+  if (n_words > (int64_t)(0xffffffffll / 32)) return set_error(ctx, BO_ERR_INVALID, "bitmap_compact: %lld words", (long long)n_words);
+  bitmap_count_kernel<<<(unsigned)tiles, kCompactBlockT, 0, ctx->stream>>>(words, n_words, tile_counts);
+  int rc = after_launch(ctx, "bitmap_count_kernel");
+  if (rc) return rc;
+  ordered_scan_kernel<<<1, kCompactScanBlock, 0, ctx->stream>>>(tile_counts, tiles, n_out);
+  if ((rc = after_launch(ctx, "ordered_scan_kernel"))) return rc;
+  bitmap_emit_kernel<<<(unsigned)tiles, kCompactBlockT, 0, ctx->stream>>>(words, n_words, tile_counts, out);
+  return after_launch(ctx, "bitmap_emit_kernel");
+}
+
 }  // namespace bo

@@ -97,6 +97,8 @@ __global__ void q10_orders_kernel(const int32_t* __restrict__ o_orderkey, const 
                                   const int32_t* __restrict__ l_orderkey, const uint8_t* __restrict__ l_code,
                                   const int32_t* __restrict__ l_dprice, int64_t n_lineitem, int16_t start,
                                   int16_t end, uint32_t group_lo, uint32_t group_count, int64_t n_map,
+                                  const int32_t* __restrict__ key_to_row, const int32_t* __restrict__ c_nationkey,
+                                  int64_t n_customer, int32_t nation_bound,
                                   unsigned long long* __restrict__ cust_rev, uint32_t* __restrict__ cust_hit,
                                   uint32_t* err) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_orders;
@@ -119,31 +121,18 @@ __global__ void q10_orders_kernel(const int32_t* __restrict__ o_orderkey, const 
       if ((uint32_t)l_code[j] - group_lo >= group_count) continue;
       rev += (unsigned long long)(int64_t)l_dprice[j];
     }
-    if (rev != 0ull) {
-      atomicAdd(cust_rev + c, rev);
-      atomicOr(cust_hit + (c >> 5), 1u << (c & 31));
-    }
+    if (rev == 0ull) continue;
+    // Only customers with a row and a known nation give rows (query_q10.cpp:
+    // 556-563); their bits are the result's custkeys.
+    const int32_t row = __ldg(key_to_row + c);
+    if (row < 0 || (int64_t)row >= n_customer) continue;
+    const int32_t nk = __ldg(c_nationkey + row);
+    if (nk < 0 || nk >= nation_bound) continue;
+    atomicAdd(cust_rev + c, rev);
+    const uint32_t bit = 1u << (c & 31);
+    if (!(__ldg(cust_hit + (c >> 5)) & bit)) atomicOr(cust_hit + (c >> 5), bit);
   }
 }
-
-// Customers with revenue in the window, in ascending custkey order (the value
-// is the custkey): the order the reference's first LSD sort by custkey gives
-// (query_q10.cpp:318-345), so only the revenue sort remains.
-struct Q10Kept {
-  const uint32_t* hit;
-  const int32_t* key_to_row;
-  const int32_t* c_nationkey;
-  int64_t n_customer;
-  int32_t nation_bound;
-  __device__ __forceinline__ bool operator()(int64_t c, uint32_t& v) const {
-    if (!((__ldg(hit + (c >> 5)) >> (c & 31)) & 1u)) return false;
-    const int32_t row = __ldg(key_to_row + c);
-    if (row < 0 || (int64_t)row >= n_customer) return false;
-    const int32_t nk = __ldg(c_nationkey + row);
-    v = (uint32_t)c;
-    return nk >= 0 && nk < nation_bound;
-  }
-};
 
 // Revenue descending as an unsigned 64-bit value: the reference's ~revenue key.
 __global__ void q10_key2_kernel(const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ cust_rev,
@@ -359,6 +348,22 @@ int finish_rows(bo_ctx* ctx, const char* op, const unsigned long long* n_out, co
   return BO_OK;
 }
 
+// The same with the row count already on the host: the rows are copied
+// before the one synchronisation.
+template <class Row>
+int finish_known_rows(bo_ctx* ctx, const char* op, int64_t n, const Row* rows, Row* out_host, int64_t max_rows,
+                      int64_t* n_rows) {
+  const int64_t m = std::min<int64_t>(n, max_rows);
+  if (m > 0)
+    BO_CUDA(ctx, cudaMemcpyAsync(out_host, rows, sizeof(Row) * (size_t)m, cudaMemcpyDeviceToHost, ctx->stream));
+  uint32_t bits = 0;
+  int rc = consume_device_errors(ctx, &bits);  // synchronises the stream
+  if (rc) return rc;
+  if ((rc = device_error_status(ctx, bits, op))) return rc;
+  *n_rows = n;
+  return BO_OK;
+}
+
 }  // namespace
 }  // namespace bo
 
@@ -416,8 +421,8 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
   add(8 * (size_t)nm);  // tmp keys
   add(4 * (size_t)nm);  // tmp vals
   add(sizeof(bo_tpch_q10_row) * (size_t)nm);
-  const int64_t tiles = (nm + kCompactTile - 1) / kCompactTile;
-  add(4 * (size_t)std::max<int64_t>(tiles, 1));  // ordered compaction's tile counts
+  const int64_t tiles = (hit_words + kBitmapTileWords - 1) / kBitmapTileWords;
+  add(4 * (size_t)std::max<int64_t>(tiles, 1));  // bitmap compaction's tile counts
   add(64);
   void* basep = nullptr;
   int rc = region(ctx, "q10_ws", total, &basep);
@@ -440,22 +445,24 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
     q10_orders_kernel<true><<<og, kTpBlock, 0, ctx->stream>>>(
         t->o_orderkey, t->o_custkey, t->o_orderdate, t->o_li_begin, t->o_li_end, t->n_orders, t->l_orderkey,
         t->l_returnflag_linestatus, t->l_discounted_price, t->n_lineitem, start_offset, end_offset,
-        (uint32_t)group_lo, (uint32_t)group_count, nm, rev, hit, ctx->d_err);
+        (uint32_t)group_lo, (uint32_t)group_count, nm, t->custkey_to_row, t->c_nationkey, t->n_customer,
+        t->nation_bound, rev, hit, ctx->d_err);
   else
     q10_orders_kernel<false><<<og, kTpBlock, 0, ctx->stream>>>(
         t->o_orderkey, t->o_custkey, t->o_orderdate, t->o_li_begin, t->o_li_end, t->n_orders, t->l_orderkey,
         t->l_returnflag_linestatus, t->l_discounted_price, t->n_lineitem, start_offset, end_offset,
-        (uint32_t)group_lo, (uint32_t)group_count, nm, rev, hit, ctx->d_err);
+        (uint32_t)group_lo, (uint32_t)group_count, nm, t->custkey_to_row, t->c_nationkey, t->n_customer,
+        t->nation_bound, rev, hit, ctx->d_err);
   if ((rc = after_launch(ctx, "q10_orders_kernel"))) return rc;
-  // Customers with revenue, in ascending custkey order (no sort by custkey needed).
-  if ((rc = ordered_compact(ctx, Q10Kept{hit, t->custkey_to_row, t->c_nationkey, t->n_customer, t->nation_bound}, nm,
-                            tile_counts, vals, n_out)))
-    return rc;
+  // Customers with revenue in the window, in ascending custkey order (the set
+  // bits of the hit bitmap): the order the reference's first LSD sort by
+  // custkey gives (query_q10.cpp:318-345), so only the revenue sort remains.
+  if ((rc = bitmap_compact(ctx, hit, hit_words, tile_counts, vals, n_out))) return rc;
   // The result's size, read back once: up to 128K rows sort in one cluster
   // launch instead of a pass sequence sized for every customer.
   int64_t ns = 0;
   if ((rc = read_device_count(ctx, n_out, nm, &ns))) return rc;
-  q10_key2_kernel<<<grid_for(ctx, nm), kTpBlock, 0, ctx->stream>>>(vals, rev, n_out, keys);
+  q10_key2_kernel<<<grid_for(ctx, std::max<int64_t>(ns, 1)), kTpBlock, 0, ctx->stream>>>(vals, rev, n_out, keys);
   if ((rc = after_launch(ctx, "q10_key2_kernel"))) return rc;
   if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
   const Q10CustStrings cs{{t->c_name_offsets, t->c_address_offsets, t->c_phone_offsets, t->c_comment_offsets},
@@ -463,7 +470,7 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
   q10_gather_kernel<<<grid_for(ctx, std::max<int64_t>(ns, 1)), kTpBlock, 0, ctx->stream>>>(
       vals, rev, t->custkey_to_row, t->c_nationkey, cs, n_out, rows);
   if ((rc = after_launch(ctx, "q10_gather_kernel"))) return rc;
-  return finish_rows(ctx, "q10", n_out, rows, out_host, max_rows, n_rows);
+  return finish_known_rows(ctx, "q10", ns, rows, out_host, max_rows, n_rows);
 }
 
 extern "C" int bo_tpch_q18(bo_ctx* ctx, const bo_tpch_q18_tables* t, int32_t quantity_threshold,
@@ -540,5 +547,5 @@ extern "C" int bo_tpch_q18(bo_ctx* ctx, const bo_tpch_q18_tables* t, int32_t qua
                                                                        t->o_orderdate, t->o_totalprice,
                                                                        dense ? 1 : 0, sum, cust, n_out, rows);
   if ((rc = after_launch(ctx, "q18_gather_kernel"))) return rc;
-  return finish_rows(ctx, "q18", n_out, rows, out_host, max_rows, n_rows);
+  return finish_known_rows(ctx, "q18", ns, rows, out_host, max_rows, n_rows);
 }

@@ -7,11 +7,14 @@
 // Here one thread per partsupp row adds its value to its partkey's sum
 // (each partkey is one run of the sorted rows, so per-key sums are the run
 // sums) and to a per-block total; the threshold, the filter and the order
-// are applied on the host to the per-key sums.
+// are applied on the host to the per-key sums (bo_tpch_q11), or on the
+// device (bo_tpch_q11_rows): an ordered compaction of the keys above the
+// threshold (ascending partkey) and one stable sort by value descending.
 #include <algorithm>
 #include <cstring>
 
 #include "common.cuh"
+#include "compact.cuh"
 #include "context.cuh"
 
 namespace bo {
@@ -41,10 +44,117 @@ __global__ void __launch_bounds__(kQ11Block) q11_kernel(bo_tpch_q11_tables t, co
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(total, (unsigned long long)acc);
 }
 
+// :186-195: a non-zero sum above total * FRACTION (compared as doubles).
+struct Q11Kept {
+  const unsigned long long* sums;
+  const unsigned long long* total;
+  double fraction;
+  __device__ __forceinline__ bool operator()(int64_t i, uint32_t& v) const {
+    const long long s = (long long)__ldg(sums + i);
+    if (s == 0) return false;
+    const double threshold = (double)(long long)__ldg(total) * fraction;
+    if (!((double)s > threshold)) return false;
+    v = (uint32_t)i;
+    return true;
+  }
+};
+
+// Descending signed values as ascending unsigned keys.
+__global__ void __launch_bounds__(kQ11Block) q11_keys_kernel(const uint32_t* __restrict__ idx,
+                                                             const unsigned long long* __restrict__ sums, int64_t n,
+                                                             unsigned long long* __restrict__ keys) {
+  for (int64_t i = (int64_t)blockIdx.x * kQ11Block + threadIdx.x; i < n; i += (int64_t)gridDim.x * kQ11Block)
+    keys[i] = ~(sums[idx[i]] ^ (1ull << 63));
+}
+
+__global__ void __launch_bounds__(kQ11Block) q11_rows_kernel(const uint32_t* __restrict__ idx,
+                                                             const unsigned long long* __restrict__ sums, int64_t n,
+                                                             int32_t min_partkey, bo_tpch_q11_row* __restrict__ rows) {
+  for (int64_t i = (int64_t)blockIdx.x * kQ11Block + threadIdx.x; i < n; i += (int64_t)gridDim.x * kQ11Block) {
+    bo_tpch_q11_row r;
+    r.ps_partkey = (int32_t)((int64_t)min_partkey + idx[i]);
+    r.pad = 0;
+    r.value_raw = (int64_t)sums[idx[i]];
+    rows[i] = r;
+  }
+}
+
+int q11_grid(bo_ctx* ctx, int64_t items) {
+  const int64_t need = (items + kQ11Block - 1) / kQ11Block;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)ctx->num_sms * 8));
+}
+
 }  // namespace
 }  // namespace bo
 
 using namespace bo;
+
+extern "C" int bo_tpch_q11_rows(bo_ctx* ctx, const bo_tpch_q11_tables* t, const uint8_t* supp_in_nation_host,
+                                int64_t n_supp, double fraction, bo_tpch_q11_row* rows_out, int64_t max_rows,
+                                int64_t* n_rows) {
+  BO_CHECK_CTX(ctx);
+  if (!t || !n_rows || (n_supp > 0 && !supp_in_nation_host) || max_rows < 0 || (max_rows > 0 && !rows_out))
+    return set_error(ctx, BO_ERR_INVALID, "q11: null argument");
+  if (t->n_partsupp < 0 || n_supp < 0) return set_error(ctx, BO_ERR_INVALID, "q11: negative size");
+  *n_rows = 0;
+  if (t->n_partsupp == 0 || n_supp == 0) return BO_OK;
+  if (t->max_partkey < t->min_partkey) return set_error(ctx, BO_ERR_INVALID, "q11: empty partkey range");
+  if (!t->ps_partkey || !t->ps_suppkey || !t->ps_value) return set_error(ctx, BO_ERR_INVALID, "q11: null column");
+  const int64_t range = (int64_t)t->max_partkey - t->min_partkey + 1;
+  const int64_t tiles = (range + kCompactTile - 1) / kCompactTile;
+  size_t total_bytes = 0;
+  auto add = [&](size_t b) { total_bytes += (b + 255) & ~size_t(255); };
+  add(256);                        // total, then the compacted count
+  add(8 * (size_t)range);          // sums
+  add((size_t)n_supp);
+  add(4 * (size_t)tiles);
+  add(4 * (size_t)range);          // compacted indexes
+  add(8 * (size_t)range);          // keys
+  add(8 * (size_t)range);          // sort scratch
+  add(4 * (size_t)range);
+  add(sizeof(bo_tpch_q11_row) * (size_t)range);
+  void* base = nullptr;
+  int rc = region(ctx, "q11_rows_ws", total_bytes, &base);
+  if (rc) return rc;
+  char* p = static_cast<char*>(base);
+  unsigned long long* total = carve<unsigned long long>(p, 32);
+  unsigned long long* sums = carve<unsigned long long>(p, (size_t)range);
+  uint8_t* in_nation = carve<uint8_t>(p, (size_t)n_supp);
+  uint32_t* tile_counts = carve<uint32_t>(p, (size_t)tiles);
+  uint32_t* idx = carve<uint32_t>(p, (size_t)range);
+  unsigned long long* keys = carve<unsigned long long>(p, (size_t)range);
+  unsigned long long* tkeys = carve<unsigned long long>(p, (size_t)range);
+  uint32_t* tvals = carve<uint32_t>(p, (size_t)range);
+  bo_tpch_q11_row* rows = carve<bo_tpch_q11_row>(p, (size_t)range);
+  void* h = nullptr;
+  if ((rc = host_stage(ctx, (size_t)n_supp, &h))) return rc;
+  std::memcpy(h, supp_in_nation_host, (size_t)n_supp);
+  BO_CUDA(ctx, cudaMemcpyAsync(in_nation, h, (size_t)n_supp, cudaMemcpyHostToDevice, ctx->stream));
+  BO_CUDA(ctx, cudaMemsetAsync(base, 0, 256 + 8 * (size_t)range, ctx->stream));
+  q11_kernel<<<q11_grid(ctx, t->n_partsupp), kQ11Block, 0, ctx->stream>>>(*t, in_nation, n_supp, sums, total,
+                                                                           ctx->d_err);
+  if ((rc = after_launch(ctx, "q11_kernel"))) return rc;
+  unsigned long long* n_out = total + 1;
+  if ((rc = ordered_compact(ctx, Q11Kept{sums, total, fraction}, range, tile_counts, idx, n_out))) return rc;
+  int64_t ns = 0;
+  if ((rc = read_device_count(ctx, n_out, range, &ns))) return rc;
+  if (ns > 0) {
+    q11_keys_kernel<<<q11_grid(ctx, ns), kQ11Block, 0, ctx->stream>>>(idx, sums, ns, keys);
+    if ((rc = after_launch(ctx, "q11_keys_kernel"))) return rc;
+    if ((rc = radix_sort_pairs(ctx, keys, idx, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
+    q11_rows_kernel<<<q11_grid(ctx, ns), kQ11Block, 0, ctx->stream>>>(idx, sums, ns, t->min_partkey, rows);
+    if ((rc = after_launch(ctx, "q11_rows_kernel"))) return rc;
+  }
+  const int64_t m = std::min<int64_t>(ns, max_rows);
+  if (m > 0)
+    BO_CUDA(ctx, cudaMemcpyAsync(rows_out, rows, sizeof(bo_tpch_q11_row) * (size_t)m, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+  uint32_t bits = 0;
+  if ((rc = consume_device_errors(ctx, &bits))) return rc;  // synchronises the stream
+  if ((rc = device_error_status(ctx, bits, "q11"))) return rc;
+  *n_rows = ns;
+  return BO_OK;
+}
 
 extern "C" int bo_tpch_q11(bo_ctx* ctx, const bo_tpch_q11_tables* t, const uint8_t* supp_in_nation_host,
                            int64_t n_supp, int64_t* sums_out, int64_t* total_out) {

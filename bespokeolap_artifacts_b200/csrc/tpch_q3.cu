@@ -13,9 +13,10 @@
 //          bespoke_tpch/builder_impl.cpp:930-990) and, if that order
 //          qualifies, adds its discounted price and a count with 64-bit
 //          atomics (only the ~2% of lineitems that pass both filters do);
-//   compact orders with at least one such lineitem (`has_lineitem`, :248),
-//          visited through the orderkey map so they come out in ascending
-//          orderkey order (order-preserving compaction, compact.cuh);
+//   compact orders with at least one such lineitem (`has_lineitem`, :248):
+//          the lineitem pass sets the orderkey's bit when it counts an
+//          order's first lineitem, and the set bits come out in ascending
+//          orderkey order (bitmap compaction, compact.cuh);
 //   sort   one stable radix sort by (revenue desc, orderdate asc) -- one
 //          cluster launch up to 128K result rows.  The reference's std::sort
 //          leaves rows equal in both keys in unspecified order; here they keep
@@ -63,7 +64,7 @@ __global__ void q3_lineitem_kernel(const int32_t* __restrict__ l_orderkey, const
                                    const int32_t* __restrict__ l_dprice, int64_t n, int16_t date_offset,
                                    const int32_t* __restrict__ key_to_row, int64_t n_map, int64_t n_orders,
                                    const uint32_t* __restrict__ qual, unsigned long long* __restrict__ rev,
-                                   uint32_t* __restrict__ cnt) {
+                                   uint32_t* __restrict__ cnt, uint32_t* __restrict__ kept) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     if (l_shipdate[i] <= date_offset) continue;
     const int32_t key = l_orderkey[i];
@@ -72,18 +73,20 @@ __global__ void q3_lineitem_kernel(const int32_t* __restrict__ l_orderkey, const
     if (row < 0 || (int64_t)row >= n_orders) continue;
     if (!((qual[row >> 5] >> (row & 31)) & 1u)) continue;
     atomicAdd(rev + row, (unsigned long long)(int64_t)l_dprice[i]);
-    atomicAdd(cnt + row, 1u);
+    if (atomicAdd(cnt + row, 1u) == 0u) atomicOr(kept + (key >> 5), 1u << (key & 31));
   }
 }
 
 // Orders with a counted lineitem -> (orderkey, row) pairs; one reservation per block.
-__global__ void q3_key2_kernel(const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ rev,
-                               const int16_t* __restrict__ o_orderdate, const unsigned long long* n_out,
-                               unsigned long long* __restrict__ keys, uint32_t* err) {
+// vals[i] holds a kept orderkey on entry and its order row on return.
+__global__ void q3_key2_kernel(uint32_t* __restrict__ vals, const int32_t* __restrict__ key_to_row,
+                               const unsigned long long* __restrict__ rev, const int16_t* __restrict__ o_orderdate,
+                               const unsigned long long* n_out, unsigned long long* __restrict__ keys, uint32_t* err) {
   const unsigned long long n = *n_out;
   for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (unsigned long long)gridDim.x * blockDim.x) {
-    const uint32_t row = vals[i];
+    const uint32_t row = (uint32_t)__ldg(key_to_row + vals[i]);  // valid: the lineitem pass marked it
+    vals[i] = row;
     const unsigned long long r = rev[row];
     if (r >> kRevBits) raise_error(err, kErrValueRange);
     const unsigned long long inv = ((1ull << kRevBits) - 1ull) - (r & ((1ull << kRevBits) - 1ull));
@@ -120,7 +123,7 @@ __global__ void __launch_bounds__(kQ3Block) q3_lineitem_v8_kernel(
     const int32_t* __restrict__ l_orderkey, const int16_t* __restrict__ l_shipdate,
     const int32_t* __restrict__ l_dprice, int64_t n, int16_t date_offset, const int32_t* __restrict__ key_to_row,
     int64_t n_map, int64_t n_orders, const uint32_t* __restrict__ qual, unsigned long long* __restrict__ rev,
-    uint32_t* __restrict__ cnt) {
+    uint32_t* __restrict__ cnt, uint32_t* __restrict__ kept) {
   const int64_t chunks = n >> 3;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -154,7 +157,7 @@ __global__ void __launch_bounds__(kQ3Block) q3_lineitem_v8_kernel(
     for (int k = 0; k < 8; ++k) {
       if (row[k] < 0 || !((word[k] >> (row[k] & 31)) & 1u)) continue;
       atomicAdd(rev + row[k], (unsigned long long)(int64_t)__ldg(l_dprice + r0 + k));
-      atomicAdd(cnt + row[k], 1u);
+      if (atomicAdd(cnt + row[k], 1u) == 0u) atomicOr(kept + (key[k] >> 5), 1u << (key[k] & 31));
     }
   }
   for (int64_t i = (chunks << 3) + tid; i < n; i += stride) {
@@ -165,25 +168,9 @@ __global__ void __launch_bounds__(kQ3Block) q3_lineitem_v8_kernel(
     if (row < 0 || (int64_t)row >= n_orders) continue;
     if (!((qual[row >> 5] >> (row & 31)) & 1u)) continue;
     atomicAdd(rev + row, (unsigned long long)(int64_t)l_dprice[i]);
-    atomicAdd(cnt + row, 1u);
+    if (atomicAdd(cnt + row, 1u) == 0u) atomicOr(kept + (key >> 5), 1u << (key & 31));
   }
 }
-
-// Orders that got revenue, visited in ascending orderkey order through the
-// orderkey -> row map (the value is the order's row): the result rows then
-// need one sort only, whose ties keep this order (query_q3.cpp:348-355 breaks
-// them by orderkey).
-struct Q3Kept {
-  const int32_t* map;
-  int64_t n_orders;
-  const uint32_t* cnt;
-  __device__ __forceinline__ bool operator()(int64_t key, uint32_t& row) const {
-    const int32_t r = __ldg(map + key);
-    if (r < 0 || (int64_t)r >= n_orders) return false;
-    row = (uint32_t)r;
-    return __ldg(cnt + r) > 0u;
-  }
-};
 
 int grid_of(bo_ctx* ctx, int64_t items) {
   const int64_t need = (items + kQ3Block - 1) / kQ3Block;
@@ -224,8 +211,10 @@ extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_
   add(8 * (size_t)no);  // tmp keys
   add(4 * (size_t)no);  // tmp vals
   add(sizeof(bo_tpch_q3_row) * (size_t)no);
-  const int64_t tiles = (t->n_orderkey_map + kCompactTile - 1) / kCompactTile;
-  add(4 * (size_t)std::max<int64_t>(tiles, 1));  // ordered compaction's tile counts
+  const int64_t kept_words = t->n_orderkey_map / 32 + 1;
+  const int64_t tiles = (kept_words + kBitmapTileWords - 1) / kBitmapTileWords;
+  add(4 * (size_t)kept_words);                   // orderkeys with a counted lineitem
+  add(4 * (size_t)std::max<int64_t>(tiles, 1));  // bitmap compaction's tile counts
   add(64);
   void* base = nullptr;
   int rc = region(ctx, "q3_ws", total, &base);
@@ -240,12 +229,14 @@ extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_
   unsigned long long* tkeys = carve<unsigned long long>(p, (size_t)no);
   uint32_t* tvals = carve<uint32_t>(p, (size_t)no);
   bo_tpch_q3_row* rows = carve<bo_tpch_q3_row>(p, (size_t)no);
+  uint32_t* kept = carve<uint32_t>(p, (size_t)kept_words);
   uint32_t* tile_counts = carve<uint32_t>(p, (size_t)std::max<int64_t>(tiles, 1));
   unsigned long long* n_out = carve<unsigned long long>(p, 8);
   // Scratch that accumulates starts at zero (the bitmaps are written whole or by atomicOr).
   BO_CUDA(ctx, cudaMemsetAsync(mask, 0, 4 * (size_t)mask_words, ctx->stream));
   BO_CUDA(ctx, cudaMemsetAsync(rev, 0, 8 * (size_t)no, ctx->stream));
   BO_CUDA(ctx, cudaMemsetAsync(cnt, 0, 4 * (size_t)no, ctx->stream));
+  BO_CUDA(ctx, cudaMemsetAsync(kept, 0, 4 * (size_t)kept_words, ctx->stream));
   BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, 8, ctx->stream));
   if (t->n_customer > 0) {
     q3_cust_kernel<<<grid_of(ctx, t->n_customer), kQ3Block, 0, ctx->stream>>>(
@@ -259,40 +250,37 @@ extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_
     if (aligned16(t->l_orderkey) && aligned16(t->l_shipdate)) {
       q3_lineitem_v8_kernel<<<grid_of(ctx, (t->n_lineitem + 7) / 8), kQ3Block, 0, ctx->stream>>>(
           t->l_orderkey, t->l_shipdate, t->l_discounted_price, t->n_lineitem, date_offset, t->orderkey_to_row,
-          t->n_orderkey_map, no, qual, rev, cnt);
+          t->n_orderkey_map, no, qual, rev, cnt, kept);
       if ((rc = after_launch(ctx, "q3_lineitem_v8_kernel"))) return rc;
     } else {
       q3_lineitem_kernel<<<grid_of(ctx, t->n_lineitem), kQ3Block, 0, ctx->stream>>>(
           t->l_orderkey, t->l_shipdate, t->l_discounted_price, t->n_lineitem, date_offset, t->orderkey_to_row,
-          t->n_orderkey_map, no, qual, rev, cnt);
+          t->n_orderkey_map, no, qual, rev, cnt, kept);
       if ((rc = after_launch(ctx, "q3_lineitem_kernel"))) return rc;
     }
   }
-  // Qualifying orders in ascending orderkey order (no sort by orderkey needed).
-  if ((rc = ordered_compact(ctx, Q3Kept{t->orderkey_to_row, no, cnt}, t->n_orderkey_map, tile_counts, vals, n_out)))
-    return rc;
+  // Qualifying orders in ascending orderkey order (no sort by orderkey
+  // needed): the set bits of the kept bitmap (query_q3.cpp:348-355 breaks
+  // ties by orderkey).
+  if ((rc = bitmap_compact(ctx, kept, kept_words, tile_counts, vals, n_out))) return rc;
   // The result's size, read back once: up to 128K rows sort in one cluster
   // launch instead of a pass sequence sized for every order.
   int64_t ns = 0;
   if ((rc = read_device_count(ctx, n_out, no, &ns))) return rc;
-  q3_key2_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(vals, rev, t->o_orderdate, n_out, keys,
-                                                                   ctx->d_err);
+  q3_key2_kernel<<<grid_of(ctx, std::max<int64_t>(ns, 1)), kQ3Block, 0, ctx->stream>>>(
+      vals, t->orderkey_to_row, rev, t->o_orderdate, n_out, keys, ctx->d_err);
   if ((rc = after_launch(ctx, "q3_key2_kernel"))) return rc;
   if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
-  q3_gather_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(vals, rev, t->o_orderkey, t->o_orderdate,
+  q3_gather_kernel<<<grid_of(ctx, std::max<int64_t>(ns, 1)), kQ3Block, 0, ctx->stream>>>(vals, rev, t->o_orderkey, t->o_orderdate,
                                                                      t->o_shippriority, n_out, rows);
   if ((rc = after_launch(ctx, "q3_gather_kernel"))) return rc;
-  unsigned long long n = 0;
-  BO_CUDA(ctx, cudaMemcpyAsync(&n, n_out, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  const int64_t m = std::min<int64_t>(ns, max_rows);
+  if (m > 0)
+    BO_CUDA(ctx, cudaMemcpyAsync(out_host, rows, sizeof(bo_tpch_q3_row) * (size_t)m, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
   uint32_t bits = 0;
   if ((rc = consume_device_errors(ctx, &bits))) return rc;  // synchronises the stream
   if ((rc = device_error_status(ctx, bits, "q3"))) return rc;
-  *n_rows = (int64_t)n;
-  const int64_t m = std::min<int64_t>((int64_t)n, max_rows);
-  if (m > 0) {
-    BO_CUDA(ctx, cudaMemcpyAsync(out_host, rows, sizeof(bo_tpch_q3_row) * (size_t)m, cudaMemcpyDeviceToHost,
-                                 ctx->stream));
-    BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  }
+  *n_rows = ns;
   return BO_OK;
 }

@@ -842,9 +842,9 @@ std::vector<Q16ResultRow> run_q16(const Database& db, const std::string& brand, 
   prm.brand_rank = db.brand_rank.data();
   prm.type_rank = db.type_rank.data();
   prm.type_banned = type_banned.data();
-  std::vector<bo_tpch_q16_row> out(static_cast<size_t>(db.n_part));
+  bo_tpch_q16_row* out = result_rows<bo_tpch_q16_row>(db, db.n_part);
   int64_t n = 0;
-  check(db.ctx, bo_tpch_q16(db.ctx, &t, &prm, out.data(), static_cast<int64_t>(out.size()), &n), "q16");
+  check(db.ctx, bo_tpch_q16(db.ctx, &t, &prm, out, db.n_part, &n), "q16");
   std::vector<Q16ResultRow> rows(static_cast<size_t>(n));
   for (int64_t i = 0; i < n; ++i) {
     const auto& r = out[static_cast<size_t>(i)];
@@ -894,11 +894,11 @@ std::vector<Q20ResultRow> run_q20(const Database& db, const std::string& color, 
   t.s_nationkey = col<int32_t>(db.s_nationkey_device);
   t.s_row_by_name = col<int32_t>(db.s_row_by_name);
   t.n_supplier = static_cast<int64_t>(db.s_suppkey.size());
-  std::vector<int32_t> out(db.s_suppkey.size());
+  int32_t* out = result_rows<int32_t>(db, t.n_supplier);
   int64_t n = 0;
   check(db.ctx,
-        bo_tpch_q20(db.ctx, &t, color.data(), static_cast<int32_t>(color.size()), key, start, end, out.data(),
-                    static_cast<int64_t>(out.size()), &n),
+        bo_tpch_q20(db.ctx, &t, color.data(), static_cast<int32_t>(color.size()), key, start, end, out, t.n_supplier,
+                    &n),
         "q20");
   std::vector<Q20ResultRow> rows(static_cast<size_t>(n));
   for (int64_t i = 0; i < n; ++i) {
@@ -942,11 +942,12 @@ std::vector<Q2ResultRow> run_q2(const Database& db, const std::string& size, con
   t.s_nation_idx = col<int32_t>(db.s_nation_idx_device);
   t.s_rank = col<uint32_t>(db.s_rank);
   t.n_supplier = static_cast<int64_t>(db.s_suppkey.size());
-  std::vector<bo_tpch_q2_row> out(static_cast<size_t>(std::max<int64_t>(db.n_partsupp, 0)));
+  const int64_t cap = std::max<int64_t>(db.n_partsupp, 0);
+  bo_tpch_q2_row* out = result_rows<bo_tpch_q2_row>(db, cap);
   int64_t n = 0;
   check(db.ctx,
         bo_tpch_q2(db.ctx, &t, target_size, type_ok.data(), static_cast<int32_t>(type_ok.size()), nation_ok.data(),
-                   static_cast<int32_t>(n_nation), out.data(), static_cast<int64_t>(out.size()), &n),
+                   static_cast<int32_t>(n_nation), out, cap, &n),
         "q2");
   std::vector<Q2ResultRow> rows(static_cast<size_t>(n));
   for (int64_t i = 0; i < n; ++i) {
@@ -992,20 +993,15 @@ std::vector<Q11ResultRow> run_q11(const Database& db, const std::string& nation,
   t.min_partkey = db.ps_min_partkey;
   t.max_partkey = db.ps_max_partkey;
   const int64_t range = static_cast<int64_t>(db.ps_max_partkey) - db.ps_min_partkey + 1;
-  std::vector<int64_t> sums(static_cast<size_t>(range), 0);
-  int64_t total = 0;
+  // :180-215 on the device: non-zero part sums above total * FRACTION, by
+  // value desc then partkey.
+  bo_tpch_q11_row* out = result_rows<bo_tpch_q11_row>(db, range);
+  int64_t n = 0;
   check(db.ctx,
-        bo_tpch_q11(db.ctx, &t, in_nation.data(), static_cast<int64_t>(in_nation.size()), sums.data(), &total),
+        bo_tpch_q11_rows(db.ctx, &t, in_nation.data(), static_cast<int64_t>(in_nation.size()), frac, out, range, &n),
         "q11");
-  // :180-215: non-zero part sums above total * FRACTION, by value desc then partkey.
-  const double threshold = static_cast<double>(total) * frac;
-  std::vector<Q11ResultRow> rows;
-  for (int64_t i = 0; i < range; ++i)
-    if (sums[static_cast<size_t>(i)] != 0 && static_cast<double>(sums[static_cast<size_t>(i)]) > threshold)
-      rows.push_back(Q11ResultRow{static_cast<int32_t>(db.ps_min_partkey + i), sums[static_cast<size_t>(i)]});
-  std::sort(rows.begin(), rows.end(), [](const Q11ResultRow& a, const Q11ResultRow& b) {
-    return a.value_raw != b.value_raw ? a.value_raw > b.value_raw : a.ps_partkey < b.ps_partkey;
-  });
+  std::vector<Q11ResultRow> rows(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) rows[static_cast<size_t>(i)] = Q11ResultRow{out[i].ps_partkey, out[i].value_raw};
   return rows;
 }
 

@@ -463,6 +463,10 @@ class TpchQ2Row(C.Structure):
     _fields_ = [("partkey", C.c_int32), ("supplier_row", C.c_int32), ("mfgr_code", C.c_int32), ("pad", C.c_int32)]
 
 
+class TpchQ11Row(C.Structure):
+    _fields_ = [("ps_partkey", C.c_int32), ("pad", C.c_int32), ("value_raw", C.c_int64)]
+
+
 class TpchQ13Tables(C.Structure):
     """``bo_tpch_q13_tables``: order comments (bytes + offsets), custkeys, customer keys."""
     _fields_ = [("o_comment", C.c_void_p), ("o_comment_offsets", C.c_void_p), ("o_custkey", C.c_void_p),
@@ -604,6 +608,8 @@ _SIGNATURES = {
                               C.c_int16, _P, C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q2": (C.c_int, [_P, C.POINTER(TpchQ2Tables), C.c_int32, _P, C.c_int32, _P, C.c_int32,
                              C.POINTER(TpchQ2Row), C.c_int64, C.POINTER(C.c_int64)]),
+    "bo_tpch_q11_rows": (C.c_int, [_P, C.POINTER(TpchQ11Tables), C.c_char_p, C.c_int64, C.c_double,
+                                   C.POINTER(TpchQ11Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q13": (C.c_int, [_P, C.POINTER(TpchQ13Tables), C.c_char_p, C.c_int64, C.c_char_p, C.c_int64,
                               C.POINTER(TpchQ13Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q18": (C.c_int, [_P, C.POINTER(TpchQ18Tables), C.c_int32, C.POINTER(TpchQ18Row), C.c_int64,

@@ -815,6 +815,18 @@ typedef struct bo_tpch_q11_tables {
 int bo_tpch_q11(bo_ctx* ctx, const bo_tpch_q11_tables* tables, const uint8_t* supp_in_nation_host, int64_t n_supp,
                 int64_t* sums_out, int64_t* total_out);
 
+/* Q11's result rows on the device (query_q11.cpp:186-210): partkeys whose
+ * non-zero sum exceeds (double)total * fraction, by value descending then
+ * partkey.  *n_rows counts them; rows past max_rows are not written. */
+typedef struct bo_tpch_q11_row {
+  int32_t ps_partkey;
+  int32_t pad;
+  int64_t value_raw;
+} bo_tpch_q11_row;
+
+int bo_tpch_q11_rows(bo_ctx* ctx, const bo_tpch_q11_tables* tables, const uint8_t* supp_in_nation_host,
+                     int64_t n_supp, double fraction, bo_tpch_q11_row* rows_out, int64_t max_rows, int64_t* n_rows);
+
 /* TPC-H Q15 over the storage-plan layout: run_q15 of
  * bespoke_tpch/query_q15.cpp:215-534.  The discounted prices of lineitems
  * shipped in [start_offset, end_offset), summed per suppkey into

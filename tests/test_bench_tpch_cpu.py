@@ -19,7 +19,7 @@ REF_DRIVER = ROOT / "oracle" / "_ref" / "ref_tpch_driver"
 @pytest.mark.skipif(not REF_DRIVER.exists(), reason="reference driver not built")
 def test_section_requests_run_on_the_reference_driver(tmp_path):
     data = write_tpch(tmp_path / "d", n_customer=3000, n_orders=30000, seed=11, customer_nations="known",
-                      n_supplier=25, n_part=199, orderless_customers=True)
+                      n_supplier=200, n_part=4000, orderless_customers=True, lineitem_keys="partsupp")
     reqs = [r for _, r in bench.TPCH_REQUESTS]
     build_ms, times = bench._driver_times(REF_DRIVER, data, tmp_path / "ref", reqs, "ms")
     assert build_ms >= 0 and len(times) == len(reqs)
