@@ -15,11 +15,13 @@
 //   cfilter  C rows -> exact pass bitmap (one 32-row word per thread, no
 //            atomics) and the passing ids into a 64 KB blocked Bloom filter;
 //   amask    A ids -> bitmap over [0, a_id_max];
-//   scan     B streamed 16 rows per lane (256-bit c_id loads, L2 evict-first);
-//            the Bloom filter (read through L1) rejects ~97% of rows without
-//            leaving the SM; hits are compacted per warp, checked against the
-//            exact bitmap and the A mask, and only survivors load their a_id
-//            and the C year (late materialisation).  Survivors aggregate first
+//   scan     B streamed 8 rows per lane (one 256-bit c_id load and one
+//            256-bit a_id load, both L2 evict-first and prefetched a step
+//            ahead, so no survivor waits on a scattered a_id read); the Bloom
+//            filter (read through L1) rejects ~97% of rows without leaving
+//            the SM; hits are compacted per warp with their a_id, checked
+//            against the exact bitmap and the A mask, and only survivors load
+//            the C year (late materialisation).  Survivors aggregate first
 //            into a per-block shared-memory table (count, min year) so Zipf
 //            heavy hitters cost one global update per block, then the block
 //            flushes into a global open-addressing table (key << 32 | count
@@ -47,7 +49,7 @@ constexpr uint32_t kGbBloomWords = kBloomWords;
 constexpr uint32_t kGbBloomBytes = kBloomBytes;
 constexpr int kGbBlock = 256;
 constexpr int kGbWarps = kGbBlock / 32;
-constexpr int kGbRowsPerLane = 16;
+constexpr int kGbRowsPerLane = 8;
 constexpr int kGbRowsPerWarpStep = 32 * kGbRowsPerLane;
 constexpr int kGbQueue = 384;        // per-warp candidate queue (entries)
 constexpr int kGbFlushAt = 128;      // resolve once this many candidates are queued
@@ -265,24 +267,27 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
   const int64_t nwarps = (int64_t)gridDim.x * kGbWarps;
   // One step of software prefetch: the next step's c_ids are in flight while
   // the current step is tested and resolved.
-  auto load_step = [&](int64_t st, int32_t (&out)[kGbRowsPerLane], uint32_t& vmask) {
+  auto load_step = [&](int64_t st, int32_t (&out)[kGbRowsPerLane], int32_t (&out_a)[kGbRowsPerLane], uint32_t& vmask) {
     const int64_t r0 = st * kGbRowsPerWarpStep + lane * kGbRowsPerLane;
     vmask = 0;
     if (st >= steps) return;
     if (r0 + kGbRowsPerLane <= n) {
-      const int8v c0 = ld_first_v8(b.c_id + r0), c1 = ld_first_v8(b.c_id + r0 + 8);
+      const int8v c0 = ld_first_v8(b.c_id + r0);
+      const int8v a0 = ld_first_v8(b.a_id + r0);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         out[k] = c0.v[k];
-        out[8 + k] = c1.v[k];
+        out_a[k] = a0.v[k];
       }
-      vmask = 0xffffu;
+      vmask = 0xffu;
     } else {
 #pragma unroll
       for (int k = 0; k < kGbRowsPerLane; ++k) {
         out[k] = -1;
+        out_a[k] = -1;
         if (r0 + k < n) {
           out[k] = b.c_id[r0 + k];
+          out_a[k] = b.a_id[r0 + k];
           vmask |= 1u << k;
         }
       }
@@ -290,8 +295,9 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
   };
   // Resolves the warp's queued candidates: lanes take up to kGbResolveR
   // entries each and every round issues its loads for all of them at once
-  // (exact C bitmap; then a_id and the C year of the passing ones; then the A
-  // mask), so a warp has many independent memory chains in flight.
+  // (exact C bitmap; then the C year of the passing ones; then the A mask),
+  // so a warp has many independent memory chains in flight.  The queue holds
+  // each candidate's c_id and a_id.
   auto resolve = [&](uint32_t cnt) {
     __syncwarp();
     for (uint32_t i0 = 0; i0 < cnt; i0 += 32 * kGbResolveR) {
@@ -302,14 +308,14 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
       for (int r = 0; r < kGbResolveR; ++r) {
         const uint32_t i = i0 + r * 32 + lane;
         c[r] = i < cnt ? qc[i] : -1;
-        row[r] = i < cnt ? qr[i] : 0u;
+        row[r] = i < cnt ? qr[i] : 0u;  // the candidate's a_id
         const bool in = (uint32_t)c[r] < (uint32_t)n_c;  // negative or past C: no partner
         w[r] = in ? __ldg(cbits + (c[r] >> 5)) : 0u;
       }
 #pragma unroll
       for (int r = 0; r < kGbResolveR; ++r) {
         const bool pass = (w[r] >> (c[r] & 31)) & 1u;
-        a[r] = pass ? __ldg(b.a_id + row[r]) : -1;
+        a[r] = pass ? (int32_t)row[r] : -1;
         y[r] = (pass && kMode >= 1) ? __ldg(c_year + c[r]) : 0;
       }
       // Survivors: A-mask test, then the heavy-hitter table in shared memory;
@@ -381,18 +387,21 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
     }
     __syncwarp();
   };
-  int32_t nxt[kGbRowsPerLane];
+  int32_t nxt[kGbRowsPerLane], nxt_a[kGbRowsPerLane];
   uint32_t nxt_valid;
   int64_t st = (int64_t)blockIdx.x * kGbWarps + warp;
-  load_step(st, nxt, nxt_valid);
+  load_step(st, nxt, nxt_a, nxt_valid);
   for (; st < steps; st += nwarps) {
     const int64_t base = st * kGbRowsPerWarpStep;
-    int32_t cid[kGbRowsPerLane];
+    int32_t cid[kGbRowsPerLane], aid[kGbRowsPerLane];
 #pragma unroll
-    for (int k = 0; k < kGbRowsPerLane; ++k) cid[k] = nxt[k];
+    for (int k = 0; k < kGbRowsPerLane; ++k) {
+      cid[k] = nxt[k];
+      aid[k] = nxt_a[k];
+    }
     const uint32_t valid = nxt_valid;
-    load_step(st + nwarps, nxt, nxt_valid);
-    // Branch-free Bloom test of all 16 rows (every lookup is issued; without
+    load_step(st + nwarps, nxt, nxt_a, nxt_valid);
+    // Branch-free Bloom test of all 8 rows (every lookup is issued; without
     // the filter every word reads as all ones).
     // (The c_id range check happens in the rare resolve path below.)
     uint32_t hit = 0;
@@ -404,7 +413,7 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
     }
     hit &= valid;
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
+    for (int half = 0; half < 1; ++half) {
       const uint32_t hm = (hit >> (8 * half)) & 0xffu;
       uint32_t total;
       uint32_t pos = warp_exclusive_scan(__popc(hm), total);
@@ -418,7 +427,7 @@ __global__ void __launch_bounds__(kGbBlock) gb_scan_kernel(bo_gb_b_cols b, int64
       for (int k = 0; k < 8; ++k) {
         if ((hm >> k) & 1u) {
           qc[pos] = cid[8 * half + k];
-          qr[pos] = (uint32_t)(base + lane * kGbRowsPerLane + 8 * half + k);
+          qr[pos] = (uint32_t)aid[8 * half + k];
           ++pos;
         }
       }
