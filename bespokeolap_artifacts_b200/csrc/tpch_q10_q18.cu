@@ -29,6 +29,7 @@
 //   sort     stable by orderkey, then by (totalprice desc, orderdate asc):
 //            the reference's comparator (:438-449).
 #include <algorithm>
+#include <cstring>
 
 #include "common.cuh"
 #include "compact.cuh"
@@ -182,6 +183,57 @@ __global__ void q10_gather_kernel(const uint32_t* __restrict__ vals, const unsig
     r.comment_begin = b[3];
     r.comment_len = l[3];
     out[i] = r;
+  }
+}
+
+// The customer strings on the host and the nation names (device table of
+// host pointers), for rows the host reads in place.
+struct Q10HostStrings {
+  const char* data[4];     // name, address, phone, comment bytes (host)
+  const uint32_t* off[4];  // their offsets per customer row (device)
+  const int32_t* acctbal;
+  const bo_host_str* nation_names;
+};
+
+// The result rows in their final host form, written straight into mapped
+// pinned host memory.  Each thread builds one 96-byte row in shared memory;
+// the block then stores its rows as consecutive 16-byte words (one warp
+// instruction covers 512 contiguous bytes), so they cross PCIe as full
+// writes rather than as many partial ones.  out is 16-byte aligned.
+constexpr int kQ10RowsBlock = 128;
+
+__global__ void __launch_bounds__(kQ10RowsBlock) q10_host_rows_kernel(
+    const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ cust_rev,
+    const int32_t* __restrict__ key_to_row, const int32_t* __restrict__ c_nationkey, Q10HostStrings hs, int64_t n,
+    bo_tpch_q10_host_row* __restrict__ out) {
+  __shared__ bo_tpch_q10_host_row stage[kQ10RowsBlock];
+  constexpr int kWords = (int)(sizeof(bo_tpch_q10_host_row) / 16);
+  static_assert(sizeof(bo_tpch_q10_host_row) % 16 == 0, "rows are whole 16-byte words");
+  for (int64_t base = (int64_t)blockIdx.x * kQ10RowsBlock; base < n; base += (int64_t)gridDim.x * kQ10RowsBlock) {
+    const int64_t i = base + threadIdx.x;
+    if (i < n) {
+      const uint32_t c = vals[i];
+      const int32_t row = key_to_row[c];
+      bo_tpch_q10_host_row r;
+      r.custkey = (int32_t)c;
+      r.acctbal_raw = __ldg(hs.acctbal + row);
+      r.revenue_raw = (int64_t)cust_rev[c];
+      bo_host_str* f[4] = {&r.name, &r.address, &r.phone, &r.comment};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t b = __ldg(hs.off[k] + row);
+        f[k]->ptr = hs.data[k] + b;
+        f[k]->len = __ldg(hs.off[k] + row + 1) - b;
+      }
+      r.nation_name = hs.nation_names[c_nationkey[row]];
+      stage[threadIdx.x] = r;
+    }
+    __syncthreads();
+    const int rows = (int)(n - base < kQ10RowsBlock ? n - base : kQ10RowsBlock);
+    const uint4* src = reinterpret_cast<const uint4*>(stage);
+    uint4* dst = reinterpret_cast<uint4*>(out + base);
+    for (int w = threadIdx.x; w < rows * kWords; w += kQ10RowsBlock) dst[w] = src[w];
+    __syncthreads();
   }
 }
 
@@ -389,12 +441,21 @@ extern "C" int bo_tpch_order_ranges(bo_ctx* ctx, const int32_t* l_orderkey, int6
   return after_launch(ctx, "order_range_kernel");
 }
 
-extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t start_offset, int16_t end_offset,
-                           int32_t group_lo, int32_t group_count, bo_tpch_q10_row* out_host, int64_t max_rows,
-                           int64_t* n_rows) {
-  BO_CHECK_CTX(ctx);
-  if (!t || !n_rows || max_rows < 0 || (max_rows > 0 && !out_host))
-    return set_error(ctx, BO_ERR_INVALID, "q10: null argument");
+namespace {
+// Q10 up to its sorted result: r->vals holds the result custkeys in row order,
+// r->rev the revenue per custkey, r->n the row count (0: no rows; then the
+// other fields are unset).
+struct Q10Sorted {
+  const uint32_t* vals;
+  const unsigned long long* rev;
+  const unsigned long long* n_out;
+  bo_tpch_q10_row* rows;  // workspace for the rows of bo_tpch_q10
+  int64_t n;
+};
+
+int q10_run(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t start_offset, int16_t end_offset, int32_t group_lo,
+            int32_t group_count, Q10Sorted* r) {
+  r->n = 0;
   if (t->n_orders < 0 || t->n_lineitem < 0 || t->n_custkey_map < 0 || t->n_customer < 0 || t->nation_bound < 0 ||
       group_count < 0)
     return set_error(ctx, BO_ERR_INVALID, "q10: negative size");
@@ -408,7 +469,6 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
     const bool all = t->c_name_offsets && t->c_address_offsets && t->c_phone_offsets && t->c_comment_offsets;
     if (any && !all) return set_error(ctx, BO_ERR_INVALID, "q10: give all four string offset columns or none");
   }
-  *n_rows = 0;
   const int64_t nm = t->n_custkey_map;
   if (group_lo < 0 || t->n_orders == 0 || nm == 0 || t->n_lineitem == 0) return BO_OK;
   const int64_t hit_words = (nm + 31) / 32;
@@ -465,12 +525,89 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
   q10_key2_kernel<<<grid_for(ctx, std::max<int64_t>(ns, 1)), kTpBlock, 0, ctx->stream>>>(vals, rev, n_out, keys);
   if ((rc = after_launch(ctx, "q10_key2_kernel"))) return rc;
   if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
+  *r = Q10Sorted{vals, rev, n_out, rows, ns};
+  return BO_OK;
+}
+}  // namespace
+
+extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t start_offset, int16_t end_offset,
+                           int32_t group_lo, int32_t group_count, bo_tpch_q10_row* out_host, int64_t max_rows,
+                           int64_t* n_rows) {
+  BO_CHECK_CTX(ctx);
+  if (!t || !n_rows || max_rows < 0 || (max_rows > 0 && !out_host))
+    return set_error(ctx, BO_ERR_INVALID, "q10: null argument");
+  *n_rows = 0;
+  Q10Sorted r{};
+  int rc = q10_run(ctx, t, start_offset, end_offset, group_lo, group_count, &r);
+  if (rc) return rc;
+  if (r.n == 0) return finish_known_rows<bo_tpch_q10_row>(ctx, "q10", 0, nullptr, out_host, max_rows, n_rows);
   const Q10CustStrings cs{{t->c_name_offsets, t->c_address_offsets, t->c_phone_offsets, t->c_comment_offsets},
                           t->c_acctbal};
-  q10_gather_kernel<<<grid_for(ctx, std::max<int64_t>(ns, 1)), kTpBlock, 0, ctx->stream>>>(
-      vals, rev, t->custkey_to_row, t->c_nationkey, cs, n_out, rows);
+  q10_gather_kernel<<<grid_for(ctx, r.n), kTpBlock, 0, ctx->stream>>>(r.vals, r.rev, t->custkey_to_row,
+                                                                      t->c_nationkey, cs, r.n_out, r.rows);
   if ((rc = after_launch(ctx, "q10_gather_kernel"))) return rc;
-  return finish_known_rows(ctx, "q10", ns, rows, out_host, max_rows, n_rows);
+  return finish_known_rows(ctx, "q10", r.n, r.rows, out_host, max_rows, n_rows);
+}
+
+extern "C" int bo_tpch_q10_host_rows(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t start_offset,
+                                     int16_t end_offset, int32_t group_lo, int32_t group_count,
+                                     const bo_tpch_q10_host_strings* hs, bo_tpch_q10_host_row* rows_mapped,
+                                     int64_t max_rows, int64_t* n_rows) {
+  BO_CHECK_CTX(ctx);
+  if (!t || !hs || !n_rows || max_rows < 0 || (max_rows > 0 && !rows_mapped))
+    return set_error(ctx, BO_ERR_INVALID, "q10: null argument");
+  *n_rows = 0;
+  if (!t->c_name_offsets || !t->c_address_offsets || !t->c_phone_offsets || !t->c_comment_offsets || !t->c_acctbal ||
+      !hs->name_data || !hs->address_data || !hs->phone_data || !hs->comment_data ||
+      (hs->n_nation > 0 && !hs->nation_names))
+    return set_error(ctx, BO_ERR_INVALID, "q10: host rows need the string offsets, balances and host strings");
+  if (hs->n_nation < 0 || hs->n_nation < t->nation_bound)
+    return set_error(ctx, BO_ERR_INVALID, "q10: %d nation names for nation keys below %d", (int)hs->n_nation,
+                     (int)t->nation_bound);
+  bo_tpch_q10_host_row* dev_rows = nullptr;
+  if (max_rows > 0) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, rows_mapped) != cudaSuccess || attr.type != cudaMemoryTypeHost ||
+        !attr.devicePointer) {
+      cudaGetLastError();
+      return set_error(ctx, BO_ERR_INVALID, "q10: rows_mapped is not mapped pinned host memory");
+    }
+    dev_rows = static_cast<bo_tpch_q10_host_row*>(attr.devicePointer);
+    if (!aligned16(dev_rows)) return set_error(ctx, BO_ERR_INVALID, "q10: rows_mapped is not 16-byte aligned");
+  }
+  Q10Sorted r{};
+  int rc = q10_run(ctx, t, start_offset, end_offset, group_lo, group_count, &r);
+  if (rc) return rc;
+  uint32_t bits = 0;
+  if (r.n == 0) {
+    if ((rc = consume_device_errors(ctx, &bits))) return rc;
+    return device_error_status(ctx, bits, "q10");
+  }
+  // The nation names, as a small device table.
+  const size_t nb = sizeof(bo_host_str) * (size_t)hs->n_nation;
+  void* dn = nullptr;
+  void* h = nullptr;
+  if ((rc = region(ctx, "q10_nation_names", std::max<size_t>(nb, 16), &dn))) return rc;
+  if ((rc = host_stage(ctx, std::max<size_t>(nb, 16), &h))) return rc;
+  if (nb) {
+    std::memcpy(h, hs->nation_names, nb);
+    BO_CUDA(ctx, cudaMemcpyAsync(dn, h, nb, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  const Q10HostStrings hsd{{hs->name_data, hs->address_data, hs->phone_data, hs->comment_data},
+                           {t->c_name_offsets, t->c_address_offsets, t->c_phone_offsets, t->c_comment_offsets},
+                           t->c_acctbal, static_cast<const bo_host_str*>(dn)};
+  const int64_t m = std::min<int64_t>(r.n, max_rows);
+  if (m > 0) {
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((m + kQ10RowsBlock - 1) / kQ10RowsBlock,
+                                                                  (int64_t)ctx->num_sms * 8));
+    q10_host_rows_kernel<<<grid, kQ10RowsBlock, 0, ctx->stream>>>(r.vals, r.rev, t->custkey_to_row, t->c_nationkey,
+                                                                   hsd, m, dev_rows);
+    if ((rc = after_launch(ctx, "q10_host_rows_kernel"))) return rc;
+  }
+  if ((rc = consume_device_errors(ctx, &bits))) return rc;  // synchronises the stream: the rows have landed
+  if ((rc = device_error_status(ctx, bits, "q10"))) return rc;
+  *n_rows = r.n;
+  return BO_OK;
 }
 
 extern "C" int bo_tpch_q18(bo_ctx* ctx, const bo_tpch_q18_tables* t, int32_t quantity_threshold,

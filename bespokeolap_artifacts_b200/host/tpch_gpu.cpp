@@ -427,7 +427,7 @@ T* result_rows(const Database& db, int64_t count) {
 }
 }  // namespace
 
-std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, const std::string& date) {
+RowView<Q3ResultRow> run_q3(const Database& db, const std::string& segment, const std::string& date) {
   const int16_t d = date_offset_of(date, db.base_date_days);
   int32_t code = -1;
   for (size_t i = 0; i < db.mktsegment.values.size(); ++i)
@@ -456,15 +456,7 @@ std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, 
   int64_t n = 0;
   check(db.ctx, bo_tpch_q3(db.ctx, &t, d, code, out, db.n_orders, &n), "q3");
   trace.mark("gpu");
-  std::vector<Q3ResultRow> rows(static_cast<size_t>(n));
-  for (int64_t i = 0; i < n; ++i) {
-    rows[i].orderkey = out[i].orderkey;
-    rows[i].revenue_raw = out[i].revenue_raw;
-    rows[i].orderdate_offset = out[i].orderdate_offset;
-    rows[i].shippriority = out[i].shippriority;
-  }
-  trace.mark("rows");
-  return rows;
+  return RowView<Q3ResultRow>(out, static_cast<size_t>(n));
 }
 
 Q10Rows run_q10(const Database& db, const std::string& date) {
@@ -501,35 +493,19 @@ Q10Rows run_q10(const Database& db, const std::string& date) {
   t.c_comment_offsets = col<uint32_t>(db.c_comment_offsets);
   t.c_acctbal = col<int32_t>(db.c_acctbal_device);
   QueryTrace trace("q10");
-  bo_tpch_q10_row* out = result_rows<bo_tpch_q10_row>(db, db.n_custkey_map);
+  // The rows are finished on the device: its last kernel writes them, strings
+  // resolved to these host columns, straight into the mapped result buffer.
+  const bo_tpch_q10_host_strings hs{db.c_name.data.data(),    db.c_address.data.data(),
+                                    db.c_phone.data.data(),   db.c_comment.data.data(),
+                                    db.nation_name_str.data(), static_cast<int32_t>(db.nation_name_str.size()),
+                                    0};
+  Q10ResultRow* out = result_rows<Q10ResultRow>(db, db.n_custkey_map);
   int64_t n = 0;
-  check(db.ctx, bo_tpch_q10(db.ctx, &t, start, end, rf * ls_count, ls_count, out, db.n_custkey_map, &n),
+  check(db.ctx,
+        bo_tpch_q10_host_rows(db.ctx, &t, start, end, rf * ls_count, ls_count, &hs, out, db.n_custkey_map, &n),
         "q10");
   trace.mark("gpu");
-  // Every field of every row is written below (RowAlloc leaves them unset);
-  // the GPU gathered each customer's string ranges and balance, so this loop
-  // reads the records in order and touches no customer data of its own.
-  Q10Rows rows(static_cast<size_t>(n));
-  const char* name = db.c_name.data.data();
-  const char* address = db.c_address.data.data();
-  const char* phone = db.c_phone.data.data();
-  const char* comment = db.c_comment.data.data();
-  for_row_ranges(n, [&](int64_t lo, int64_t hi) {
-    for (int64_t i = lo; i < hi; ++i) {
-      const auto& g = out[i];
-      auto& row = rows[i];
-      row.custkey = g.custkey;
-      row.name = std::string_view(name + g.name_begin, g.name_len);
-      row.revenue_raw = g.revenue_raw;
-      row.acctbal_raw = g.acctbal_raw;
-      row.nation_name = db.nation_name[static_cast<size_t>(g.nationkey)];
-      row.address = std::string_view(address + g.address_begin, g.address_len);
-      row.phone = std::string_view(phone + g.phone_begin, g.phone_len);
-      row.comment = std::string_view(comment + g.comment_begin, g.comment_len);
-    }
-  });
-  trace.mark("rows");
-  return rows;
+  return Q10Rows(out, static_cast<size_t>(n));
 }
 
 std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date) {
@@ -1432,7 +1408,7 @@ void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& r
   }
 }
 
-void write_q3_csv(const Database& db, const std::string& filename, const std::vector<Q3ResultRow>& rows) {
+void write_q3_csv(const Database& db, const std::string& filename, const RowView<Q3ResultRow>& rows) {
   std::ofstream out(filename);
   out << "l_orderkey,revenue,o_orderdate,o_shippriority\n";
   out.setf(std::ios::fixed);
@@ -1454,19 +1430,19 @@ void write_q10_csv(const std::string& filename, const Q10Rows& rows) {
     const auto res = std::to_chars(std::begin(ib), std::end(ib), r.custkey);
     buf.append(ib, res.ptr);
     buf.push_back(',');
-    append_csv_field(buf, r.name);
+    append_csv_field(buf, view_of(r.name));
     buf.push_back(',');
     append_fixed_2(buf, r.revenue_raw);
     buf.push_back(',');
     append_fixed_2(buf, r.acctbal_raw);
     buf.push_back(',');
-    append_csv_field(buf, r.nation_name);
+    append_csv_field(buf, view_of(r.nation_name));
     buf.push_back(',');
-    append_csv_field(buf, r.address);
+    append_csv_field(buf, view_of(r.address));
     buf.push_back(',');
-    append_csv_field(buf, r.phone);
+    append_csv_field(buf, view_of(r.phone));
     buf.push_back(',');
-    append_csv_field(buf, r.comment);
+    append_csv_field(buf, view_of(r.comment));
     buf.push_back('\n');
     if (buf.size() >= (1u << 20)) {
       out.write(buf.data(), static_cast<std::streamsize>(buf.size()));
@@ -2173,6 +2149,7 @@ Database* build(ParquetTables* tables) {
       db->nation_name.assign(static_cast<size_t>(db->nation_bound), std::string());
       for (size_t i = 0; i < key.size(); ++i)
         if (key[i] >= 0) db->nation_name[static_cast<size_t>(key[i])] = std::string(name.view(i));
+      for (const auto& nm : db->nation_name) db->nation_name_str.push_back(bo_host_str{nm.data(), nm.size()});
       db->nation_key = key;
       db->nation_regionkey = int_values(column(N, "n_regionkey"));
       for (size_t i = 0; i < key.size(); ++i) db->nation_row_name.emplace_back(name.view(i));

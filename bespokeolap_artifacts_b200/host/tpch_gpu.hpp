@@ -121,6 +121,7 @@ struct Database {
   // nation names by nationkey in [0, nation_bound) (last row of each key)
   int32_t nation_bound = 1;
   std::vector<std::string> nation_name;
+  std::vector<bo_host_str> nation_name_str;  // the same names as host strings (Q10's rows point at them)
   // nation rows' keys, region keys and names; region name -> key (first row of a name)
   std::vector<int32_t> nation_key, nation_regionkey;
   std::vector<std::string> nation_row_name;
@@ -188,12 +189,8 @@ struct Q1ResultRow {
   int64_t count_order = 0;
 };
 
-struct Q3ResultRow {
-  int32_t orderkey = 0;
-  int64_t revenue_raw = 0;
-  int16_t orderdate_offset = 0;
-  int32_t shippriority = 0;
-};
+// Q3ResultRow (bespoke_tpch/query_q3.hpp:10-15) as the GPU writes it.
+using Q3ResultRow = bo_tpch_q3_row;
 
 struct Q6ResultRow {
   int64_t revenue_raw = 0;
@@ -295,37 +292,30 @@ struct Q16ResultRow {
   int64_t supplier_cnt = 0;
 };
 
-// Allocator that leaves elements default-constructed as nothing: for result
-// rows every field of which the query writes in parallel right after the
-// allocation (a value-initialising std::vector would first write the whole
-// buffer on one thread).  For implicit-lifetime row types only.
-template <class T>
-struct RowAlloc : std::allocator<T> {
-  template <class U>
-  struct rebind {
-    using other = RowAlloc<U>;
-  };
-  RowAlloc() = default;
-  template <class U>
-  RowAlloc(const RowAlloc<U>&) noexcept {}
-  template <class U>
-  void construct(U*) noexcept {}
-  template <class U, class... A>
-  void construct(U* p, A&&... a) {
-    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
-  }
-};
+// Q10ResultRow (bespoke_tpch/query_q10.hpp:10-19) as the GPU writes it into
+// the Database's mapped pinned result buffer: the strings are host pointers
+// into the Database's customer columns and nation names.
+using Q10ResultRow = bo_tpch_q10_host_row;
+inline std::string_view view_of(const bo_host_str& s) { return std::string_view(s.ptr, s.len); }
 
-struct Q10ResultRow {
-  int32_t custkey = 0;
-  std::string_view name;
-  int64_t revenue_raw = 0;
-  int32_t acctbal_raw = 0;
-  std::string_view nation_name;
-  std::string_view address;
-  std::string_view phone;
-  std::string_view comment;
+// The rows of one request as the GPU left them in the Database's pinned
+// result buffer: a view, valid until the Database answers its next query.
+template <class Row>
+class RowView {
+ public:
+  RowView() = default;
+  RowView(const Row* rows, size_t n) : rows_(rows), n_(n) {}
+  const Row* begin() const { return rows_; }
+  const Row* end() const { return rows_ + n_; }
+  size_t size() const { return n_; }
+  bool empty() const { return n_ == 0; }
+  const Row& operator[](size_t i) const { return rows_[i]; }
+
+ private:
+  const Row* rows_ = nullptr;
+  size_t n_ = 0;
 };
+using Q10Rows = RowView<Q10ResultRow>;
 
 struct Q18ResultRow {
   std::string_view c_name;
@@ -345,10 +335,9 @@ void civil_from_days(int64_t z, int& y, unsigned& m, unsigned& d);
 // DATE; DATE, DISCOUNT, QUANTITY; DATE; WORD1, WORD2; QUANTITY), parsed as the
 // reference parses them.
 std::vector<Q1ResultRow> run_q1(const Database& db, const std::string& delta);
-std::vector<Q3ResultRow> run_q3(const Database& db, const std::string& segment, const std::string& date);
+RowView<Q3ResultRow> run_q3(const Database& db, const std::string& segment, const std::string& date);
 std::vector<Q6ResultRow> run_q6(const Database& db, const std::string& date, const std::string& discount,
                                 const std::string& quantity);
-using Q10Rows = std::vector<Q10ResultRow, RowAlloc<Q10ResultRow>>;
 Q10Rows run_q10(const Database& db, const std::string& date);
 std::vector<Q4ResultRow> run_q4(const Database& db, const std::string& date);
 std::vector<Q5ResultRow> run_q5(const Database& db, const std::string& region, const std::string& date);
@@ -371,7 +360,7 @@ std::vector<Q16ResultRow> run_q16(const Database& db, const std::string& brand, 
                                   const std::string sizes[8]);
 
 void write_q1_csv(const std::string& filename, const std::vector<Q1ResultRow>& rows);
-void write_q3_csv(const Database& db, const std::string& filename, const std::vector<Q3ResultRow>& rows);
+void write_q3_csv(const Database& db, const std::string& filename, const RowView<Q3ResultRow>& rows);
 void write_q6_csv(const std::string& filename, const std::vector<Q6ResultRow>& rows);
 void write_q10_csv(const std::string& filename, const Q10Rows& rows);
 void write_q4_csv(const std::string& filename, const std::vector<Q4ResultRow>& rows);

@@ -467,6 +467,24 @@ class TpchQ11Row(C.Structure):
     _fields_ = [("ps_partkey", C.c_int32), ("pad", C.c_int32), ("value_raw", C.c_int64)]
 
 
+class HostStr(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("len", C.c_uint64)]
+
+
+class TpchQ10HostStrings(C.Structure):
+    """``bo_tpch_q10_host_strings``: host bytes of the customer name / address / phone / comment columns and the
+    nation names by key."""
+    _fields_ = [("name_data", C.c_void_p), ("address_data", C.c_void_p), ("phone_data", C.c_void_p),
+                ("comment_data", C.c_void_p), ("nation_names", C.c_void_p), ("n_nation", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+class TpchQ10HostRow(C.Structure):
+    _fields_ = [("custkey", C.c_int32), ("acctbal_raw", C.c_int32), ("revenue_raw", C.c_int64),
+                ("name", HostStr), ("nation_name", HostStr), ("address", HostStr), ("phone", HostStr),
+                ("comment", HostStr)]
+
+
 class TpchQ13Tables(C.Structure):
     """``bo_tpch_q13_tables``: order comments (bytes + offsets), custkeys, customer keys."""
     _fields_ = [("o_comment", C.c_void_p), ("o_comment_offsets", C.c_void_p), ("o_custkey", C.c_void_p),
@@ -610,6 +628,8 @@ _SIGNATURES = {
                              C.POINTER(TpchQ2Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q11_rows": (C.c_int, [_P, C.POINTER(TpchQ11Tables), C.c_char_p, C.c_int64, C.c_double,
                                    C.POINTER(TpchQ11Row), C.c_int64, C.POINTER(C.c_int64)]),
+    "bo_tpch_q10_host_rows": (C.c_int, [_P, C.POINTER(TpchQ10Tables), C.c_int16, C.c_int16, C.c_int32, C.c_int32,
+                                        C.POINTER(TpchQ10HostStrings), _P, C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q13": (C.c_int, [_P, C.POINTER(TpchQ13Tables), C.c_char_p, C.c_int64, C.c_char_p, C.c_int64,
                               C.POINTER(TpchQ13Row), C.c_int64, C.POINTER(C.c_int64)]),
     "bo_tpch_q18": (C.c_int, [_P, C.POINTER(TpchQ18Tables), C.c_int32, C.POINTER(TpchQ18Row), C.c_int64,

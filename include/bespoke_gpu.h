@@ -559,6 +559,43 @@ int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* tables, int16_t start_off
                 int32_t group_lo, int32_t group_count, bo_tpch_q10_row* out_host, int64_t max_rows,
                 int64_t* n_rows);
 
+/* A host string: bytes [ptr, ptr + len) in host memory. */
+typedef struct bo_host_str {
+  const char* ptr;
+  uint64_t len;
+} bo_host_str;
+
+/* The host's copies of the strings a Q10 result row shows: the customer
+ * columns' bytes (the offset columns of the tables index them) and the name
+ * of each nation key 0 .. n_nation - 1 (n_nation >= the tables' nation_bound). */
+typedef struct bo_tpch_q10_host_strings {
+  const char* name_data;
+  const char* address_data;
+  const char* phone_data;
+  const char* comment_data;
+  const bo_host_str* nation_names;     /* host array */
+  int32_t n_nation;
+  int32_t pad;
+} bo_tpch_q10_host_strings;
+
+/* Q10ResultRow (bespoke_tpch/query_q10.hpp:10-19) with its strings as host
+ * pointers. */
+typedef struct bo_tpch_q10_host_row {
+  int32_t custkey;
+  int32_t acctbal_raw;                 /* x100 */
+  int64_t revenue_raw;                 /* x100 */
+  bo_host_str name, nation_name, address, phone, comment;
+} bo_tpch_q10_host_row;
+
+/* bo_tpch_q10 with the rows finished on the device: the last kernel writes
+ * each row, its strings resolved to host pointers, straight into rows_mapped,
+ * which must be mapped pinned host memory (bo_host_alloc_pinned); no copy
+ * and no host pass follow, so the rows are complete when the call returns.
+ * The tables must carry the four offset columns and c_acctbal. */
+int bo_tpch_q10_host_rows(bo_ctx* ctx, const bo_tpch_q10_tables* tables, int16_t start_offset, int16_t end_offset,
+                          int32_t group_lo, int32_t group_count, const bo_tpch_q10_host_strings* strings,
+                          bo_tpch_q10_host_row* rows_mapped, int64_t max_rows, int64_t* n_rows);
+
 /* =============================================================== TPC-H Q18 ==
  * run_q18 over the storage-plan layout (bespoke_tpch/query_q18.cpp:183-455):
  * sum_qty[k] = sum of l_quantity over the lineitems of orderkey k; orders

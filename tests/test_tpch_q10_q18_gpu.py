@@ -186,6 +186,70 @@ def test_q10_matches_numpy(engine, torch_cuda, shuffle):
     assert n.value == 0
 
 
+def test_q10_host_rows_match_the_device_rows(engine, torch_cuda):
+    """bo_tpch_q10_host_rows writes each row, strings resolved to host
+    pointers, into mapped pinned memory: the same rows as bo_tpch_q10 with
+    every string pointing at base + begin of its column and every nation name
+    at the given table's entry; pageable memory for the rows is refused."""
+    torch = torch_cuda
+    t = tables(1_500_000, 4, False)
+    g = dev(torch, t)
+    no = len(t["okey"])
+    begin, end = ranges(engine, torch, g, no)
+    nc = len(t["cnation"])
+    rng = np.random.default_rng(6)
+    offs = [np.concatenate([[0], np.cumsum(rng.integers(0, 90, size=nc))]).astype(np.uint32) for _ in range(4)]
+    acct = rng.integers(-99_999, 999_999, size=nc).astype(np.int32)
+    offs_d = [torch.from_numpy(o).cuda() for o in offs]
+    acct_d = torch.from_numpy(acct).cuda()
+    tb = N.TpchQ10Tables()
+    tb.o_orderkey, tb.o_custkey, tb.o_orderdate = g["okey"].data_ptr(), g["ocust"].data_ptr(), g["odate"].data_ptr()
+    tb.o_li_begin, tb.o_li_end, tb.n_orders = begin.data_ptr(), end.data_ptr(), no
+    tb.l_orderkey, tb.l_returnflag_linestatus = g["lkey"].data_ptr(), g["lcode"].data_ptr()
+    tb.l_discounted_price, tb.n_lineitem = g["ldp"].data_ptr(), len(t["lkey"])
+    tb.lineitem_orderkey_sorted = 1
+    tb.nation_bound = 25
+    tb.custkey_to_row, tb.n_custkey_map = g["cmap"].data_ptr(), len(t["cmap"])
+    tb.c_nationkey, tb.n_customer = g["cnation"].data_ptr(), nc
+    tb.c_name_offsets, tb.c_address_offsets, tb.c_phone_offsets, tb.c_comment_offsets = [o.data_ptr() for o in offs_d]
+    tb.c_acctbal = acct_d.data_ptr()
+    data = [C.create_string_buffer(int(o[-1]) + 1) for o in offs]  # host bytes the offsets index
+    names = [C.create_string_buffer(f"NATION_{k:02d}".encode()) for k in range(25)]
+    ntab = (N.HostStr * 25)(*[N.HostStr(C.addressof(b), 9) for b in names])
+    hs = N.TpchQ10HostStrings(*[C.addressof(b) for b in data], C.addressof(ntab), 25, 0)
+    cap = len(t["cmap"])
+    nbytes = C.sizeof(N.TpchQ10HostRow) * cap
+    assert C.sizeof(N.TpchQ10HostRow) == 96
+    mapped = C.c_void_p()
+    engine.ctx.call("bo_host_alloc_pinned", nbytes, C.byref(mapped))
+    try:
+        for start, end_ in [(640, 730), (0, 2405), (100, 100)]:
+            ref = (N.TpchQ10Row * cap)()
+            n_ref, n = C.c_int64(), C.c_int64(-1)
+            engine.ctx.call("bo_tpch_q10", C.byref(tb), start, end_, 2, 2, ref, cap, C.byref(n_ref))
+            engine.ctx.call("bo_tpch_q10_host_rows", C.byref(tb), start, end_, 2, 2, C.byref(hs), mapped, cap,
+                            C.byref(n))
+            assert n.value == n_ref.value
+            rows = (N.TpchQ10HostRow * cap).from_address(mapped.value)
+            for i in range(n.value):
+                a, b = rows[i], ref[i]
+                assert (a.custkey, a.revenue_raw, a.acctbal_raw) == (b.custkey, b.revenue_raw, b.acctbal_raw), i
+                for k, (f, bg, ln) in enumerate((("name", b.name_begin, b.name_len),
+                                                 ("address", b.address_begin, b.address_len),
+                                                 ("phone", b.phone_begin, b.phone_len),
+                                                 ("comment", b.comment_begin, b.comment_len))):
+                    hsv = getattr(a, f)
+                    assert (hsv.ptr, hsv.len) == (C.addressof(data[k]) + bg, ln), (i, f)
+                assert (a.nation_name.ptr, a.nation_name.len) == (C.addressof(names[b.nationkey]), 9), i
+        pageable = (N.TpchQ10HostRow * 4)()
+        with pytest.raises(N.BoError) as e:
+            engine.ctx.call("bo_tpch_q10_host_rows", C.byref(tb), 0, 2405, 2, 2, C.byref(hs), pageable, 4,
+                            C.byref(n))
+        assert e.value.status == -1
+    finally:
+        engine.ctx.call("bo_host_free_pinned", mapped)
+
+
 def test_q18_error_contract(engine, torch_cuda):
     torch = torch_cuda
     okey = torch.arange(1, 1001, dtype=torch.int32, device="cuda")
