@@ -102,6 +102,13 @@ T* carve(char*& p, size_t count) {
 int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsigned long long* tmp_keys,
                      uint32_t* tmp_vals, int64_t n, int begin_bit, int end_bit, const unsigned long long* n_dev);
 
+// The one-launch cluster sort of min(*n_dev, n_max) pairs without the count on
+// the host: if the count exceeds what the largest cluster holds (kCsCap per
+// CTA), *overflow is set and nothing moves (the caller then reads the count
+// and sorts with radix_sort_pairs).
+int cluster_sort_pairs_counted(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, const unsigned long long* n_dev,
+                               int64_t n_max, int begin_bit, int end_bit, uint32_t* overflow);
+
 // Copies the device count *n_dev (clamped to n_max) to the host; synchronises
 // the stream.  Lets a caller sort an exact number of pairs.
 int read_device_count(bo_ctx* ctx, const unsigned long long* n_dev, int64_t n_max, int64_t* n);

@@ -427,12 +427,25 @@ constexpr int64_t kCsTargetPerCta = 1024;       // spread: about this many pairs
 constexpr int64_t kClusterSortMax = (int64_t)kCsCap * kCsMaxCluster;
 constexpr size_t kCsDynSmem = (size_t)2 * kCsCap * (sizeof(unsigned long long) + sizeof(uint32_t));
 
+// n_dev (optional): the count is min(*n_dev, n), read on the device; a count
+// beyond the cluster's capacity sets *overflow and sorts nothing (every CTA
+// reads the same count, so all return before the first cluster barrier).
 __global__ void __launch_bounds__(kCsBlock, 1) cluster_sort_kernel(unsigned long long* __restrict__ keys,
                                                                   uint32_t* __restrict__ vals, int64_t n,
-                                                                  int begin_bit, int end_bit) {
+                                                                  int begin_bit, int end_bit,
+                                                                  const unsigned long long* __restrict__ n_dev,
+                                                                  uint32_t* __restrict__ overflow) {
   cg::cluster_group cl = cg::this_cluster();
   const uint32_t cs = cl.num_blocks();
   const uint32_t me = cl.block_rank();
+  if (n_dev) {
+    const unsigned long long nd = *n_dev;
+    if (nd < (unsigned long long)n) n = (int64_t)nd;
+    if (n > (int64_t)kCsCap * cs) {
+      if (me == 0 && threadIdx.x == 0) atomicOr(overflow, 1u);
+      return;
+    }
+  }
   extern __shared__ __align__(16) unsigned char cs_smem[];
   // [2][S] keys then [2][S] values: the launch sizes the dynamic shared
   // memory to the pairs per CTA (S <= kCsCap), not to the capacity.
@@ -621,7 +634,38 @@ int cluster_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, in
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  BO_CUDA(ctx, cudaLaunchKernelEx(&cfg, cluster_sort_kernel, keys, vals, n, begin_bit, end_bit));
+  BO_CUDA(ctx, cudaLaunchKernelEx(&cfg, cluster_sort_kernel, keys, vals, n, begin_bit, end_bit,
+                                  static_cast<const unsigned long long*>(nullptr), static_cast<uint32_t*>(nullptr)));
+  return after_launch(ctx, "cluster_sort_kernel");
+}
+
+int cluster_sort_pairs_counted(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, const unsigned long long* n_dev,
+                               int64_t n_max, int begin_bit, int end_bit, uint32_t* overflow) {
+  if (n_max <= 1 || end_bit <= begin_bit) return BO_OK;
+  const int max_cs = cluster_sort_max(ctx);
+  static bool ready = false;
+  if (!ready) {
+    BO_CUDA(ctx, cudaFuncSetAttribute(cluster_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kCsDynSmem));
+    ready = true;
+  }
+  // The count is unknown here: the largest cluster, each CTA with room for
+  // its capacity, so any count up to kCsCap * max_cs fits.
+  unsigned cs = 1;
+  while ((int)cs < max_cs && (int64_t)cs * kCsTargetPerCta < n_max) cs <<= 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cs);
+  cfg.blockDim = dim3(kCsBlock);
+  cfg.dynamicSmemBytes = kCsDynSmem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BO_CUDA(ctx, cudaLaunchKernelEx(&cfg, cluster_sort_kernel, keys, vals, n_max, begin_bit, end_bit, n_dev, overflow));
   return after_launch(ctx, "cluster_sort_kernel");
 }
 

@@ -18,7 +18,11 @@
 //          order's first lineitem, and the set bits come out in ascending
 //          orderkey order (bitmap compaction, compact.cuh);
 //   sort   one stable radix sort by (revenue desc, orderdate asc) -- one
-//          cluster launch up to 128K result rows.  The reference's std::sort
+//          cluster launch that reads the result's size on the device, up to
+//          128K result rows (more: the pass sequence, sized after a read-back);
+//   rows   staged in shared memory and stored straight into the caller's
+//          mapped pinned memory where it is that, so the query synchronises
+//          once.  The reference's std::sort
 //          leaves rows equal in both keys in unspecified order; here they keep
 //          orderkey order, a canonical form of the same result.
 #include <algorithm>
@@ -94,22 +98,47 @@ __global__ void q3_key2_kernel(uint32_t* __restrict__ vals, const int32_t* __res
   }
 }
 
-__global__ void q3_gather_kernel(const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ rev,
-                                 const int32_t* __restrict__ o_orderkey, const int16_t* __restrict__ o_orderdate,
-                                 const int32_t* __restrict__ o_shippriority, const unsigned long long* n_out,
-                                 bo_tpch_q3_row* __restrict__ out) {
-  const unsigned long long n = *n_out;
-  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (unsigned long long)gridDim.x * blockDim.x) {
-    const uint32_t row = vals[i];
-    bo_tpch_q3_row r;
-    r.revenue_raw = (int64_t)rev[row];
-    r.orderkey = o_orderkey[row];
-    r.shippriority = o_shippriority ? o_shippriority[row] : 0;
-    r.orderdate_offset = o_orderdate[row];
-    r.pad0 = 0;
-    r.pad1 = 0;
-    out[i] = r;
+// The result rows (the first min(*n_out, limit)), one per thread, staged in
+// shared memory and stored as consecutive 16-byte words: out may be mapped
+// pinned host memory (the rows then cross PCIe as whole writes) or device
+// memory.  out is 16-byte aligned.
+constexpr int kQ3RowsBlock = 128;
+
+__global__ void __launch_bounds__(kQ3RowsBlock) q3_gather_kernel(
+    const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ rev,
+    const int32_t* __restrict__ o_orderkey, const int16_t* __restrict__ o_orderdate,
+    const int32_t* __restrict__ o_shippriority, const unsigned long long* n_out, int64_t limit,
+    bo_tpch_q3_row* __restrict__ out) {
+  __shared__ bo_tpch_q3_row stage[kQ3RowsBlock];
+  static_assert((sizeof(bo_tpch_q3_row) * kQ3RowsBlock) % 16 == 0, "a block's rows are whole 16-byte words");
+  const unsigned long long nd = *n_out;
+  const int64_t n = nd < (unsigned long long)limit ? (int64_t)nd : limit;
+  for (int64_t base = (int64_t)blockIdx.x * kQ3RowsBlock; base < n; base += (int64_t)gridDim.x * kQ3RowsBlock) {
+    const int64_t i = base + threadIdx.x;
+    if (i < n) {
+      const uint32_t row = vals[i];
+      bo_tpch_q3_row r;
+      r.revenue_raw = (int64_t)rev[row];
+      r.orderkey = o_orderkey[row];
+      r.shippriority = o_shippriority ? o_shippriority[row] : 0;
+      r.orderdate_offset = o_orderdate[row];
+      r.pad0 = 0;
+      r.pad1 = 0;
+      stage[threadIdx.x] = r;
+    }
+    __syncthreads();
+    const int rows = (int)(n - base < kQ3RowsBlock ? n - base : kQ3RowsBlock);
+    const int words = (int)((sizeof(bo_tpch_q3_row) * rows + 15) / 16);  // the tail word may carry pad bytes
+    const uint4* src = reinterpret_cast<const uint4*>(stage);
+    uint4* dst = reinterpret_cast<uint4*>(out + base);
+    if (rows == kQ3RowsBlock || (sizeof(bo_tpch_q3_row) * rows) % 16 == 0) {
+      for (int w = threadIdx.x; w < words; w += kQ3RowsBlock) dst[w] = src[w];
+    } else {  // a ragged last block: 8-byte words, so nothing past row n - 1 is written
+      const uint2* s2 = reinterpret_cast<const uint2*>(stage);
+      uint2* d2 = reinterpret_cast<uint2*>(out + base);
+      for (int w = threadIdx.x; w < (int)(sizeof(bo_tpch_q3_row) / 8) * rows; w += kQ3RowsBlock) d2[w] = s2[w];
+    }
+    __syncthreads();
   }
 }
 
@@ -237,7 +266,7 @@ extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_
   BO_CUDA(ctx, cudaMemsetAsync(rev, 0, 8 * (size_t)no, ctx->stream));
   BO_CUDA(ctx, cudaMemsetAsync(cnt, 0, 4 * (size_t)no, ctx->stream));
   BO_CUDA(ctx, cudaMemsetAsync(kept, 0, 4 * (size_t)kept_words, ctx->stream));
-  BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, 8, ctx->stream));
+  BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, 16, ctx->stream));  // the count and the sort's overflow word
   if (t->n_customer > 0) {
     q3_cust_kernel<<<grid_of(ctx, t->n_customer), kQ3Block, 0, ctx->stream>>>(
         t->c_custkey, t->c_mktsegment, t->n_customer, segment_code, t->custkey_bound, mask);
@@ -263,24 +292,54 @@ extern "C" int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* t, int16_t date_
   // needed): the set bits of the kept bitmap (query_q3.cpp:348-355 breaks
   // ties by orderkey).
   if ((rc = bitmap_compact(ctx, kept, kept_words, tile_counts, vals, n_out))) return rc;
-  // The result's size, read back once: up to 128K rows sort in one cluster
-  // launch instead of a pass sequence sized for every order.
-  int64_t ns = 0;
-  if ((rc = read_device_count(ctx, n_out, no, &ns))) return rc;
-  q3_key2_kernel<<<grid_of(ctx, std::max<int64_t>(ns, 1)), kQ3Block, 0, ctx->stream>>>(
-      vals, t->orderkey_to_row, rev, t->o_orderdate, n_out, keys, ctx->d_err);
+  // Sort keys and the sort itself without the result's size on the host: one
+  // cluster launch reads the count on the device (up to 128K rows).  Rows go
+  // straight into out_host when it is mapped pinned memory, so the query
+  // synchronises once; a count beyond the cluster sets the overflow word and
+  // the rows are sorted again with the count read back.
+  uint32_t* overflow = reinterpret_cast<uint32_t*>(n_out + 1);
+  q3_key2_kernel<<<grid_of(ctx, no), kQ3Block, 0, ctx->stream>>>(vals, t->orderkey_to_row, rev, t->o_orderdate, n_out,
+                                                                  keys, ctx->d_err);
   if ((rc = after_launch(ctx, "q3_key2_kernel"))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
-  q3_gather_kernel<<<grid_of(ctx, std::max<int64_t>(ns, 1)), kQ3Block, 0, ctx->stream>>>(vals, rev, t->o_orderkey, t->o_orderdate,
-                                                                     t->o_shippriority, n_out, rows);
-  if ((rc = after_launch(ctx, "q3_gather_kernel"))) return rc;
-  const int64_t m = std::min<int64_t>(ns, max_rows);
-  if (m > 0)
-    BO_CUDA(ctx, cudaMemcpyAsync(out_host, rows, sizeof(bo_tpch_q3_row) * (size_t)m, cudaMemcpyDeviceToHost,
-                                 ctx->stream));
+  if ((rc = cluster_sort_pairs_counted(ctx, keys, vals, n_out, no, 0, 64, overflow))) return rc;
+  bo_tpch_q3_row* direct = nullptr;
+  if (max_rows > 0) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, out_host) == cudaSuccess && attr.type == cudaMemoryTypeHost &&
+        attr.devicePointer && aligned16(attr.devicePointer))
+      direct = static_cast<bo_tpch_q3_row*>(attr.devicePointer);
+    cudaGetLastError();  // pageable memory: not an error
+  }
+  auto gather = [&]() {
+    const int64_t lim = direct ? std::min<int64_t>(max_rows, no) : no;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((lim + kQ3RowsBlock - 1) / kQ3RowsBlock,
+                                                                 (int64_t)ctx->num_sms * 8));
+    q3_gather_kernel<<<grid, kQ3RowsBlock, 0, ctx->stream>>>(vals, rev, t->o_orderkey, t->o_orderdate,
+                                                             t->o_shippriority, n_out, lim, direct ? direct : rows);
+    return after_launch(ctx, "q3_gather_kernel");
+  };
+  if ((rc = gather())) return rc;
+  void* hs = nullptr;
+  if ((rc = host_stage(ctx, 16, &hs))) return rc;
+  BO_CUDA(ctx, cudaMemcpyAsync(hs, n_out, 16, cudaMemcpyDeviceToHost, ctx->stream));
   uint32_t bits = 0;
   if ((rc = consume_device_errors(ctx, &bits))) return rc;  // synchronises the stream
   if ((rc = device_error_status(ctx, bits, "q3"))) return rc;
+  const unsigned long long nd = *static_cast<const unsigned long long*>(hs);
+  const bool over = (*reinterpret_cast<const uint32_t*>(static_cast<const char*>(hs) + 8)) != 0u;
+  const int64_t ns = (int64_t)std::min<unsigned long long>(nd, (unsigned long long)no);
+  if (over) {  // more rows than one cluster sorts: the pass sequence, sized by the count now known
+    if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
+    if ((rc = gather())) return rc;
+  }
+  const int64_t m = std::min<int64_t>(ns, max_rows);
+  if (!direct && m > 0)
+    BO_CUDA(ctx, cudaMemcpyAsync(out_host, rows, sizeof(bo_tpch_q3_row) * (size_t)m, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+  if (over || (!direct && m > 0)) {
+    if ((rc = consume_device_errors(ctx, &bits))) return rc;
+    if ((rc = device_error_status(ctx, bits, "q3"))) return rc;
+  }
   *n_rows = ns;
   return BO_OK;
 }
