@@ -204,11 +204,13 @@ constexpr int kQ10RowsBlock = 128;
 
 __global__ void __launch_bounds__(kQ10RowsBlock) q10_host_rows_kernel(
     const uint32_t* __restrict__ vals, const unsigned long long* __restrict__ cust_rev,
-    const int32_t* __restrict__ key_to_row, const int32_t* __restrict__ c_nationkey, Q10HostStrings hs, int64_t n,
-    bo_tpch_q10_host_row* __restrict__ out) {
+    const int32_t* __restrict__ key_to_row, const int32_t* __restrict__ c_nationkey, Q10HostStrings hs,
+    const unsigned long long* n_out, int64_t limit, bo_tpch_q10_host_row* __restrict__ out) {
   __shared__ bo_tpch_q10_host_row stage[kQ10RowsBlock];
   constexpr int kWords = (int)(sizeof(bo_tpch_q10_host_row) / 16);
   static_assert(sizeof(bo_tpch_q10_host_row) % 16 == 0, "rows are whole 16-byte words");
+  const unsigned long long nd = *n_out;
+  const int64_t n = nd < (unsigned long long)limit ? (int64_t)nd : limit;  // the first min(count, limit) rows
   for (int64_t base = (int64_t)blockIdx.x * kQ10RowsBlock; base < n; base += (int64_t)gridDim.x * kQ10RowsBlock) {
     const int64_t i = base + threadIdx.x;
     if (i < n) {
@@ -445,17 +447,22 @@ namespace {
 // Q10 up to its sorted result: r->vals holds the result custkeys in row order,
 // r->rev the revenue per custkey, r->n the row count (0: no rows; then the
 // other fields are unset).
+// counted: the sort reads the count on the device (one cluster launch); n is
+// then -1 and a count beyond the cluster sets *overflow (see q10_resort).
 struct Q10Sorted {
-  const uint32_t* vals;
+  uint32_t* vals;
   const unsigned long long* rev;
   const unsigned long long* n_out;
   bo_tpch_q10_row* rows;  // workspace for the rows of bo_tpch_q10
   int64_t n;
+  unsigned long long *keys, *tkeys;
+  uint32_t* tvals;
+  uint32_t* overflow;
 };
 
 int q10_run(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t start_offset, int16_t end_offset, int32_t group_lo,
-            int32_t group_count, Q10Sorted* r) {
-  r->n = 0;
+            int32_t group_count, bool counted, Q10Sorted* r) {
+  *r = Q10Sorted{};
   if (t->n_orders < 0 || t->n_lineitem < 0 || t->n_custkey_map < 0 || t->n_customer < 0 || t->nation_bound < 0 ||
       group_count < 0)
     return set_error(ctx, BO_ERR_INVALID, "q10: negative size");
@@ -499,7 +506,7 @@ int q10_run(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t start_offset, int1
   auto* n_out = carve<unsigned long long>(p, 8);
   BO_CUDA(ctx, cudaMemsetAsync(rev, 0, 8 * (size_t)nm, ctx->stream));
   BO_CUDA(ctx, cudaMemsetAsync(hit, 0, 4 * (size_t)hit_words, ctx->stream));
-  BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, 8, ctx->stream));
+  BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, 16, ctx->stream));  // the count and the sort's overflow word
   const int og = grid_for(ctx, t->n_orders);
   if (t->lineitem_orderkey_sorted)
     q10_orders_kernel<true><<<og, kTpBlock, 0, ctx->stream>>>(
@@ -520,12 +527,20 @@ int q10_run(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t start_offset, int1
   if ((rc = bitmap_compact(ctx, hit, hit_words, tile_counts, vals, n_out))) return rc;
   // The result's size, read back once: up to 128K rows sort in one cluster
   // launch instead of a pass sequence sized for every customer.
+  uint32_t* overflow = reinterpret_cast<uint32_t*>(n_out + 1);
+  if (counted) {
+    q10_key2_kernel<<<grid_for(ctx, nm), kTpBlock, 0, ctx->stream>>>(vals, rev, n_out, keys);
+    if ((rc = after_launch(ctx, "q10_key2_kernel"))) return rc;
+    if ((rc = cluster_sort_pairs_counted(ctx, keys, vals, n_out, nm, 0, 64, overflow))) return rc;
+    *r = Q10Sorted{vals, rev, n_out, rows, -1, keys, tkeys, tvals, overflow};
+    return BO_OK;
+  }
   int64_t ns = 0;
   if ((rc = read_device_count(ctx, n_out, nm, &ns))) return rc;
   q10_key2_kernel<<<grid_for(ctx, std::max<int64_t>(ns, 1)), kTpBlock, 0, ctx->stream>>>(vals, rev, n_out, keys);
   if ((rc = after_launch(ctx, "q10_key2_kernel"))) return rc;
   if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
-  *r = Q10Sorted{vals, rev, n_out, rows, ns};
+  *r = Q10Sorted{vals, rev, n_out, rows, ns, keys, tkeys, tvals, overflow};
   return BO_OK;
 }
 }  // namespace
@@ -538,7 +553,7 @@ extern "C" int bo_tpch_q10(bo_ctx* ctx, const bo_tpch_q10_tables* t, int16_t sta
     return set_error(ctx, BO_ERR_INVALID, "q10: null argument");
   *n_rows = 0;
   Q10Sorted r{};
-  int rc = q10_run(ctx, t, start_offset, end_offset, group_lo, group_count, &r);
+  int rc = q10_run(ctx, t, start_offset, end_offset, group_lo, group_count, false, &r);
   if (rc) return rc;
   if (r.n == 0) return finish_known_rows<bo_tpch_q10_row>(ctx, "q10", 0, nullptr, out_host, max_rows, n_rows);
   const Q10CustStrings cs{{t->c_name_offsets, t->c_address_offsets, t->c_phone_offsets, t->c_comment_offsets},
@@ -576,10 +591,10 @@ extern "C" int bo_tpch_q10_host_rows(bo_ctx* ctx, const bo_tpch_q10_tables* t, i
     if (!aligned16(dev_rows)) return set_error(ctx, BO_ERR_INVALID, "q10: rows_mapped is not 16-byte aligned");
   }
   Q10Sorted r{};
-  int rc = q10_run(ctx, t, start_offset, end_offset, group_lo, group_count, &r);
+  int rc = q10_run(ctx, t, start_offset, end_offset, group_lo, group_count, true, &r);
   if (rc) return rc;
   uint32_t bits = 0;
-  if (r.n == 0) {
+  if (!r.vals) {  // nothing ran: no rows
     if ((rc = consume_device_errors(ctx, &bits))) return rc;
     return device_error_status(ctx, bits, "q10");
   }
@@ -588,7 +603,7 @@ extern "C" int bo_tpch_q10_host_rows(bo_ctx* ctx, const bo_tpch_q10_tables* t, i
   void* dn = nullptr;
   void* h = nullptr;
   if ((rc = region(ctx, "q10_nation_names", std::max<size_t>(nb, 16), &dn))) return rc;
-  if ((rc = host_stage(ctx, std::max<size_t>(nb, 16), &h))) return rc;
+  if ((rc = host_stage(ctx, std::max<size_t>(nb, 16) + 16, &h))) return rc;
   if (nb) {
     std::memcpy(h, hs->nation_names, nb);
     BO_CUDA(ctx, cudaMemcpyAsync(dn, h, nb, cudaMemcpyHostToDevice, ctx->stream));
@@ -596,17 +611,32 @@ extern "C" int bo_tpch_q10_host_rows(bo_ctx* ctx, const bo_tpch_q10_tables* t, i
   const Q10HostStrings hsd{{hs->name_data, hs->address_data, hs->phone_data, hs->comment_data},
                            {t->c_name_offsets, t->c_address_offsets, t->c_phone_offsets, t->c_comment_offsets},
                            t->c_acctbal, static_cast<const bo_host_str*>(dn)};
-  const int64_t m = std::min<int64_t>(r.n, max_rows);
-  if (m > 0) {
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((m + kQ10RowsBlock - 1) / kQ10RowsBlock,
+  const int64_t lim = std::min<int64_t>(max_rows, t->n_custkey_map);
+  auto rows_out = [&]() {
+    if (lim <= 0) return (int)BO_OK;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((lim + kQ10RowsBlock - 1) / kQ10RowsBlock,
                                                                   (int64_t)ctx->num_sms * 8));
     q10_host_rows_kernel<<<grid, kQ10RowsBlock, 0, ctx->stream>>>(r.vals, r.rev, t->custkey_to_row, t->c_nationkey,
-                                                                   hsd, m, dev_rows);
-    if ((rc = after_launch(ctx, "q10_host_rows_kernel"))) return rc;
-  }
+                                                                   hsd, r.n_out, lim, dev_rows);
+    return after_launch(ctx, "q10_host_rows_kernel");
+  };
+  if ((rc = rows_out())) return rc;
+  // One synchronisation: the count and the sort's overflow word come back
+  // with the error word.
+  char* cnt_h = static_cast<char*>(h) + ((std::max<size_t>(nb, 16) + 15) & ~size_t(15));
+  BO_CUDA(ctx, cudaMemcpyAsync(cnt_h, r.n_out, 16, cudaMemcpyDeviceToHost, ctx->stream));
   if ((rc = consume_device_errors(ctx, &bits))) return rc;  // synchronises the stream: the rows have landed
   if ((rc = device_error_status(ctx, bits, "q10"))) return rc;
-  *n_rows = r.n;
+  const int64_t ns = (int64_t)std::min<unsigned long long>(*reinterpret_cast<const unsigned long long*>(cnt_h),
+                                                           (unsigned long long)t->n_custkey_map);
+  if (*reinterpret_cast<const uint32_t*>(cnt_h + 8) != 0u) {
+    // More rows than one cluster sorts: the pass sequence with the count now known, then the rows again.
+    if ((rc = radix_sort_pairs(ctx, r.keys, r.vals, r.tkeys, r.tvals, ns, 0, 64, nullptr))) return rc;
+    if ((rc = rows_out())) return rc;
+    if ((rc = consume_device_errors(ctx, &bits))) return rc;
+    if ((rc = device_error_status(ctx, bits, "q10"))) return rc;
+  }
+  *n_rows = ns;
   return BO_OK;
 }
 
