@@ -154,7 +154,7 @@ int bo_create(bo_ctx** out, int device) {
   if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamDefault) != cudaSuccess ||
       cudaMalloc(&ctx->d_err, sizeof(uint32_t)) != cudaSuccess ||
       cudaHostAlloc(&ctx->h_err, sizeof(uint32_t), cudaHostAllocDefault) != cudaSuccess ||
-      cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_word), sizeof(unsigned long long), cudaHostAllocDefault) !=
+      cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_word), 2 * sizeof(unsigned long long), cudaHostAllocDefault) !=
           cudaSuccess ||
       cudaMemset(ctx->d_err, 0, sizeof(uint32_t)) != cudaSuccess) {
     bo_destroy(ctx);

@@ -30,7 +30,7 @@ struct bo_ctx {
   // grown on demand; kernels that accumulate into them leave them zeroed.
   uint32_t* d_err = nullptr;
   uint32_t* h_err = nullptr;  // pinned mirror for the single end-of-call read
-  unsigned long long* h_word = nullptr;  // pinned word for a device count read back mid-call
+  unsigned long long* h_word = nullptr;  // two pinned words: a device count (and its overflow word) read back
   struct Region {
     void* ptr = nullptr;
     size_t bytes = 0;
@@ -108,6 +108,16 @@ int radix_sort_pairs(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, unsi
 // and sorts with radix_sort_pairs).
 int cluster_sort_pairs_counted(bo_ctx* ctx, unsigned long long* keys, uint32_t* vals, const unsigned long long* n_dev,
                                int64_t n_max, int begin_bit, int end_bit, uint32_t* overflow);
+
+// The device pointer of mapped pinned host memory (16-byte aligned), or null
+// for any other pointer (pageable memory, device memory).
+void* mapped_device_ptr(const void* host);
+
+// After a pipeline whose sort read its count on the device: the count at
+// n_out (clamped to n_max) and the overflow word after it (the 16 bytes at
+// n_out) come back with the error word, in one synchronisation.
+int read_counted(bo_ctx* ctx, const char* op, const unsigned long long* n_out, int64_t n_max, int64_t* n,
+                 bool* overflow);
 
 // Copies the device count *n_dev (clamped to n_max) to the host; synchronises
 // the stream.  Lets a caller sort an exact number of pairs.

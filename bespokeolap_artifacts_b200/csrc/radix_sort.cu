@@ -669,6 +669,30 @@ int cluster_sort_pairs_counted(bo_ctx* ctx, unsigned long long* keys, uint32_t* 
   return after_launch(ctx, "cluster_sort_kernel");
 }
 
+void* mapped_device_ptr(const void* host) {
+  if (!host) return nullptr;
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, host) != cudaSuccess) {
+    cudaGetLastError();  // not a pointer CUDA knows: pageable memory
+    return nullptr;
+  }
+  if (attr.type != cudaMemoryTypeHost || !attr.devicePointer || !aligned16(attr.devicePointer)) return nullptr;
+  return attr.devicePointer;
+}
+
+int read_counted(bo_ctx* ctx, const char* op, const unsigned long long* n_out, int64_t n_max, int64_t* n,
+                 bool* overflow) {
+  BO_CUDA(ctx, cudaMemcpyAsync(ctx->h_word, n_out, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  uint32_t bits = 0;
+  int rc = consume_device_errors(ctx, &bits);  // synchronises the stream
+  if (rc) return rc;
+  if ((rc = device_error_status(ctx, bits, op))) return rc;
+  *n = (int64_t)std::min<unsigned long long>(ctx->h_word[0], (unsigned long long)std::max<int64_t>(n_max, 0));
+  *overflow = (uint32_t)ctx->h_word[1] != 0u;
+  return BO_OK;
+}
+
 int read_device_count(bo_ctx* ctx, const unsigned long long* n_dev, int64_t n_max, int64_t* n) {
   BO_CUDA(ctx, cudaMemcpyAsync(ctx->h_word, n_dev, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
   BO_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -59,17 +59,27 @@ struct Q11Kept {
   }
 };
 
+// The first min(*n_dev, limit) entries.
+__device__ __forceinline__ int64_t q11_count(const unsigned long long* n_dev, int64_t limit) {
+  const unsigned long long nd = *n_dev;
+  return nd < (unsigned long long)limit ? (int64_t)nd : limit;
+}
+
 // Descending signed values as ascending unsigned keys.
 __global__ void __launch_bounds__(kQ11Block) q11_keys_kernel(const uint32_t* __restrict__ idx,
-                                                             const unsigned long long* __restrict__ sums, int64_t n,
+                                                             const unsigned long long* __restrict__ sums,
+                                                             const unsigned long long* n_dev, int64_t limit,
                                                              unsigned long long* __restrict__ keys) {
+  const int64_t n = q11_count(n_dev, limit);
   for (int64_t i = (int64_t)blockIdx.x * kQ11Block + threadIdx.x; i < n; i += (int64_t)gridDim.x * kQ11Block)
     keys[i] = ~(sums[idx[i]] ^ (1ull << 63));
 }
 
 __global__ void __launch_bounds__(kQ11Block) q11_rows_kernel(const uint32_t* __restrict__ idx,
-                                                             const unsigned long long* __restrict__ sums, int64_t n,
+                                                             const unsigned long long* __restrict__ sums,
+                                                             const unsigned long long* n_dev, int64_t limit,
                                                              int32_t min_partkey, bo_tpch_q11_row* __restrict__ rows) {
+  const int64_t n = q11_count(n_dev, limit);
   for (int64_t i = (int64_t)blockIdx.x * kQ11Block + threadIdx.x; i < n; i += (int64_t)gridDim.x * kQ11Block) {
     bo_tpch_q11_row r;
     r.ps_partkey = (int32_t)((int64_t)min_partkey + idx[i]);
@@ -136,22 +146,37 @@ extern "C" int bo_tpch_q11_rows(bo_ctx* ctx, const bo_tpch_q11_tables* t, const 
   if ((rc = after_launch(ctx, "q11_kernel"))) return rc;
   unsigned long long* n_out = total + 1;
   if ((rc = ordered_compact(ctx, Q11Kept{sums, total, fraction}, range, tile_counts, idx, n_out))) return rc;
+  // Sort and rows read the count on the device; rows into mapped rows_out
+  // directly: one synchronisation (a count beyond one cluster sort is sorted
+  // again after the read-back).  The overflow word follows the count.
+  uint32_t* overflow = reinterpret_cast<uint32_t*>(n_out + 1);
+  q11_keys_kernel<<<q11_grid(ctx, range), kQ11Block, 0, ctx->stream>>>(idx, sums, n_out, range, keys);
+  if ((rc = after_launch(ctx, "q11_keys_kernel"))) return rc;
+  if ((rc = cluster_sort_pairs_counted(ctx, keys, idx, n_out, range, 0, 64, overflow))) return rc;
+  bo_tpch_q11_row* direct = max_rows > 0 ? static_cast<bo_tpch_q11_row*>(mapped_device_ptr(rows_out)) : nullptr;
+  const int64_t lim = direct ? std::min<int64_t>(max_rows, range) : range;
+  auto emit_rows = [&]() {
+    q11_rows_kernel<<<q11_grid(ctx, lim), kQ11Block, 0, ctx->stream>>>(idx, sums, n_out, lim, t->min_partkey,
+                                                                        direct ? direct : rows);
+    return after_launch(ctx, "q11_rows_kernel");
+  };
+  if ((rc = emit_rows())) return rc;
   int64_t ns = 0;
-  if ((rc = read_device_count(ctx, n_out, range, &ns))) return rc;
-  if (ns > 0) {
-    q11_keys_kernel<<<q11_grid(ctx, ns), kQ11Block, 0, ctx->stream>>>(idx, sums, ns, keys);
-    if ((rc = after_launch(ctx, "q11_keys_kernel"))) return rc;
+  bool over = false;
+  if ((rc = read_counted(ctx, "q11", n_out, range, &ns, &over))) return rc;
+  if (over) {
     if ((rc = radix_sort_pairs(ctx, keys, idx, tkeys, tvals, ns, 0, 64, nullptr))) return rc;
-    q11_rows_kernel<<<q11_grid(ctx, ns), kQ11Block, 0, ctx->stream>>>(idx, sums, ns, t->min_partkey, rows);
-    if ((rc = after_launch(ctx, "q11_rows_kernel"))) return rc;
+    if ((rc = emit_rows())) return rc;
   }
   const int64_t m = std::min<int64_t>(ns, max_rows);
-  if (m > 0)
+  if (!direct && m > 0)
     BO_CUDA(ctx, cudaMemcpyAsync(rows_out, rows, sizeof(bo_tpch_q11_row) * (size_t)m, cudaMemcpyDeviceToHost,
                                  ctx->stream));
-  uint32_t bits = 0;
-  if ((rc = consume_device_errors(ctx, &bits))) return rc;  // synchronises the stream
-  if ((rc = device_error_status(ctx, bits, "q11"))) return rc;
+  if (over || (!direct && m > 0)) {
+    uint32_t bits = 0;
+    if ((rc = consume_device_errors(ctx, &bits))) return rc;
+    if ((rc = device_error_status(ctx, bits, "q11"))) return rc;
+  }
   *n_rows = ns;
   return BO_OK;
 }

@@ -14,7 +14,8 @@
 //                        supplier insert (g, suppkey) into a hash set; a new
 //                        entry adds one to the group's count
 //   ordered compaction   groups with a count, in g order
-//   q16_keys_kernel      count-descending keys; one stable sort
+//   q16_keys_kernel      count-descending keys; one stable sort that reads
+//                        the group count on the device
 //   q16_rows_kernel      the rows, decoded from g
 #include <algorithm>
 #include <cstring>
@@ -117,17 +118,27 @@ struct Q16Kept {
   }
 };
 
+// The first min(*n_dev, limit) entries.
+__device__ __forceinline__ int64_t q16_count(const unsigned long long* n_dev, int64_t limit) {
+  const unsigned long long nd = *n_dev;
+  return nd < (unsigned long long)limit ? (int64_t)nd : limit;
+}
+
 // keys[i] = max_count - count of group vals[i]: ascending keys are counts descending.
 __global__ void __launch_bounds__(kQ16Block) q16_keys_kernel(const uint32_t* __restrict__ groups,
-                                                             const uint32_t* __restrict__ cnt, int64_t n,
+                                                             const uint32_t* __restrict__ cnt,
+                                                             const unsigned long long* n_dev, int64_t limit,
                                                              uint32_t max_count, unsigned long long* __restrict__ keys) {
+  const int64_t n = q16_count(n_dev, limit);
   for (int64_t i = (int64_t)blockIdx.x * kQ16Block + threadIdx.x; i < n; i += (int64_t)gridDim.x * kQ16Block)
     keys[i] = (unsigned long long)(max_count - cnt[groups[i]]);
 }
 
 __global__ void __launch_bounds__(kQ16Block) q16_rows_kernel(const uint32_t* __restrict__ groups,
-                                                             const uint32_t* __restrict__ cnt, int64_t n,
+                                                             const uint32_t* __restrict__ cnt,
+                                                             const unsigned long long* n_dev, int64_t limit,
                                                              int32_t n_type, Q16Dev d, bo_tpch_q16_row* __restrict__ rows) {
+  const int64_t n = q16_count(n_dev, limit);
   for (int64_t i = (int64_t)blockIdx.x * kQ16Block + threadIdx.x; i < n; i += (int64_t)gridDim.x * kQ16Block) {
     const uint32_t g = groups[i];
     const uint32_t bt = g >> kQ16SizeBits;
@@ -288,25 +299,43 @@ extern "C" int bo_tpch_q16(bo_ctx* ctx, const bo_tpch_q16_tables* t, const bo_tp
       *t, prm->rows_per_part, best, set, (unsigned long long)(cap - 1), cnt, ctx->d_err);
   if ((rc = after_launch(ctx, "q16_partsupp_kernel"))) return rc;
   if ((rc = ordered_compact(ctx, Q16Kept{cnt}, n_groups, tile_counts, groups, n_out))) return rc;
+  // The sort and the rows read the group count on the device; the rows go
+  // straight into rows_out where it is mapped pinned memory, so the query
+  // synchronises once (a count beyond one cluster sort: sorted again after
+  // the read-back).
+  uint32_t* overflow = reinterpret_cast<uint32_t*>(n_out + 1);
+  BO_CUDA(ctx, cudaMemsetAsync(overflow, 0, 8, ctx->stream));
+  const uint32_t max_count = (uint32_t)t->n_partsupp;
+  int bits = 1;
+  while (bits < 32 && (max_count >> bits) != 0u) ++bits;
+  q16_keys_kernel<<<q16_grid(ctx, max_out), kQ16Block, 0, ctx->stream>>>(groups, cnt, n_out, max_out, max_count,
+                                                                          keys);
+  if ((rc = after_launch(ctx, "q16_keys_kernel"))) return rc;
+  if ((rc = cluster_sort_pairs_counted(ctx, keys, groups, n_out, max_out, 0, bits, overflow))) return rc;
+  bo_tpch_q16_row* direct = max_rows > 0 ? static_cast<bo_tpch_q16_row*>(mapped_device_ptr(rows_out)) : nullptr;
+  const int64_t lim = direct ? std::min<int64_t>(max_rows, max_out) : max_out;
+  auto emit_rows = [&]() {
+    q16_rows_kernel<<<q16_grid(ctx, lim), kQ16Block, 0, ctx->stream>>>(groups, cnt, n_out, lim, (int32_t)nt, d,
+                                                                        direct ? direct : rows);
+    return after_launch(ctx, "q16_rows_kernel");
+  };
+  if ((rc = emit_rows())) return rc;
   int64_t ns = 0;
-  if ((rc = read_device_count(ctx, n_out, max_out, &ns))) return rc;
-  if (ns > 0) {
-    const uint32_t max_count = (uint32_t)t->n_partsupp;
-    int bits = 1;
-    while (bits < 32 && (max_count >> bits) != 0u) ++bits;
-    q16_keys_kernel<<<q16_grid(ctx, ns), kQ16Block, 0, ctx->stream>>>(groups, cnt, ns, max_count, keys);
-    if ((rc = after_launch(ctx, "q16_keys_kernel"))) return rc;
+  bool over = false;
+  if ((rc = read_counted(ctx, "q16", n_out, max_out, &ns, &over))) return rc;
+  if (over) {
     if ((rc = radix_sort_pairs(ctx, keys, groups, tkeys, tvals, ns, 0, bits, nullptr))) return rc;
-    q16_rows_kernel<<<q16_grid(ctx, ns), kQ16Block, 0, ctx->stream>>>(groups, cnt, ns, (int32_t)nt, d, rows);
-    if ((rc = after_launch(ctx, "q16_rows_kernel"))) return rc;
+    if ((rc = emit_rows())) return rc;
   }
   const int64_t m = std::min<int64_t>(ns, max_rows);
-  if (m > 0)
+  if (!direct && m > 0)
     BO_CUDA(ctx, cudaMemcpyAsync(rows_out, rows, sizeof(bo_tpch_q16_row) * (size_t)m, cudaMemcpyDeviceToHost,
                                  ctx->stream));
-  uint32_t bits = 0;
-  if ((rc = consume_device_errors(ctx, &bits))) return rc;  // synchronises the stream
-  if ((rc = device_error_status(ctx, bits, "q16"))) return rc;
+  if (over || (!direct && m > 0)) {
+    uint32_t ebits = 0;
+    if ((rc = consume_device_errors(ctx, &ebits))) return rc;
+    if ((rc = device_error_status(ctx, ebits, "q16"))) return rc;
+  }
   *n_rows = ns;
   return BO_OK;
 }

@@ -179,10 +179,14 @@ __global__ void __launch_bounds__(kQ2Block) q2_part_kernel(bo_tpch_q2_tables t, 
   }
 }
 
+// The first min(*n_dev, limit) sorted pairs as rows.
 __global__ void __launch_bounds__(kQ2Block) q2_rows_kernel(const unsigned long long* __restrict__ keys,
-                                                           const uint32_t* __restrict__ vals, int64_t n,
+                                                           const uint32_t* __restrict__ vals,
+                                                           const unsigned long long* n_dev, int64_t limit,
                                                            const uint16_t* __restrict__ p_mfgr,
                                                            bo_tpch_q2_row* __restrict__ rows) {
+  const unsigned long long nd = *n_dev;
+  const int64_t n = nd < (unsigned long long)limit ? (int64_t)nd : limit;
   for (int64_t i = (int64_t)blockIdx.x * kQ2Block + threadIdx.x; i < n; i += (int64_t)gridDim.x * kQ2Block) {
     const int32_t pk = (int32_t)(uint32_t)keys[i];
     bo_tpch_q2_row r;
@@ -323,28 +327,43 @@ extern "C" int bo_tpch_q2(bo_ctx* ctx, const bo_tpch_q2_tables* t, int32_t targe
   std::memcpy(h, type_ok_host, (size_t)n_type);
   std::memcpy(static_cast<char*>(h) + n_type, nation_ok_host, (size_t)n_nation);
   BO_CUDA(ctx, cudaMemcpyAsync(masks, h, (size_t)n_type + (size_t)n_nation, cudaMemcpyHostToDevice, ctx->stream));
-  BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, 8, ctx->stream));
+  BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, 16, ctx->stream));  // the count and the sort's overflow word
   q2_part_kernel<<<q20_grid(ctx, t->n_part), kQ2Block, 0, ctx->stream>>>(*t, target_size, masks, n_type,
                                                                           masks + n_type, n_nation, cap, n_out, keys,
                                                                           vals, ctx->d_err);
   if ((rc = after_launch(ctx, "q2_part_kernel"))) return rc;
+  // Sort and rows read the count on the device; rows into mapped rows_out
+  // directly: one synchronisation (a count beyond one cluster sort is sorted
+  // again after the read-back).
+  uint32_t* overflow = reinterpret_cast<uint32_t*>(n_out + 1);
+  int rank_bits = 1;
+  while (rank_bits < 32 && ((uint64_t)(t->n_supplier - 1) >> rank_bits) != 0) ++rank_bits;
+  // Keys are rank << 32 | partkey: the low word and the rank's bits.
+  if ((rc = cluster_sort_pairs_counted(ctx, keys, vals, n_out, cap, 0, 32 + rank_bits, overflow))) return rc;
+  bo_tpch_q2_row* direct = max_rows > 0 ? static_cast<bo_tpch_q2_row*>(mapped_device_ptr(rows_out)) : nullptr;
+  const int64_t lim = direct ? std::min<int64_t>(max_rows, cap) : cap;
+  auto emit_rows = [&]() {
+    q2_rows_kernel<<<q20_grid(ctx, lim), kQ2Block, 0, ctx->stream>>>(keys, vals, n_out, lim, t->p_mfgr,
+                                                                      direct ? direct : rows);
+    return after_launch(ctx, "q2_rows_kernel");
+  };
+  if ((rc = emit_rows())) return rc;
   int64_t ns = 0;
-  if ((rc = read_device_count(ctx, n_out, cap, &ns))) return rc;
-  if (ns > 0) {
-    int rank_bits = 1;
-    while (rank_bits < 32 && ((uint64_t)(t->n_supplier - 1) >> rank_bits) != 0) ++rank_bits;
-    // Keys are rank << 32 | partkey: the low word and the rank's bits.
+  bool over = false;
+  if ((rc = read_counted(ctx, "q2", n_out, cap, &ns, &over))) return rc;
+  if (over) {
     if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 32 + rank_bits, nullptr))) return rc;
-    q2_rows_kernel<<<q20_grid(ctx, ns), kQ2Block, 0, ctx->stream>>>(keys, vals, ns, t->p_mfgr, rows);
-    if ((rc = after_launch(ctx, "q2_rows_kernel"))) return rc;
+    if ((rc = emit_rows())) return rc;
   }
   const int64_t m = std::min<int64_t>(ns, max_rows);
-  if (m > 0)
+  if (!direct && m > 0)
     BO_CUDA(ctx, cudaMemcpyAsync(rows_out, rows, sizeof(bo_tpch_q2_row) * (size_t)m, cudaMemcpyDeviceToHost,
                                  ctx->stream));
-  uint32_t ebits = 0;
-  if ((rc = consume_device_errors(ctx, &ebits))) return rc;  // synchronises the stream
-  if ((rc = device_error_status(ctx, ebits, "q2"))) return rc;
+  if (over || (!direct && m > 0)) {
+    uint32_t ebits = 0;
+    if ((rc = consume_device_errors(ctx, &ebits))) return rc;
+    if ((rc = device_error_status(ctx, ebits, "q2"))) return rc;
+  }
   *n_rows = ns;
   return BO_OK;
 }
