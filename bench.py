@@ -1110,7 +1110,9 @@ def serving_section(eng, stream, join_sizer=None, gb_sizer=None, rates=(50, 500,
                            "answers_identical": f"{sum(B.same_answer(a.result, b.result) for a, b in zip(cb, cp))}"
                                                 f"/{len(cb)}"}
     for rate in rates:
-        n = int(min(2000, max(100, rate)))
+        # about 4 s of arrivals (at most 2000 requests): a p99 over a few hundred
+        # requests is its few worst, too few to compare two servers by
+        n = int(min(2000, max(100, 4 * rate)))
         rb = S.poisson_requests(float(rate), n, seed=rate)
         rp = S.poisson_requests(float(rate), n, seed=rate)
         l0 = srv.launches
