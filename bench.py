@@ -1084,7 +1084,8 @@ def serving_section(eng, stream, join_sizer=None, gb_sizer=None, rates=(50, 500,
     load_s = time.perf_counter() - t_load
     tile = B.load_tile_table()
     srv = S.BatchedServer(tables, n_slots=2, max_batch=16, pool_bytes=2 << 30, max_items=65536, workers_per_sm=1,
-                          join_sizer=join_sizer, gb_sizer=gb_sizer, tile_table=tile, policy="short_first")
+                          join_sizer=join_sizer, gb_sizer=gb_sizer, tile_table=tile, policy="short_first",
+                          batch_from=3)
     # warm-up of both servers: every pipeline shape, plans, graphs, workspaces
     srv.serve(S.poisson_requests(1000.0, 48, seed=1))
     S.serve_one_per_launch(eng, tables, S.poisson_requests(1000.0, 30, seed=2))

@@ -254,7 +254,7 @@ class BatchedServer:
                  pool_bytes: int = 2 << 30, max_items: int = 65536, workers_per_sm: int = 1,
                  join_sizer=None, gb_sizer=None, tile_table: B.TileTable | None = None, shared: bool = True,
                  policy: str = "fifo", max_wait_ms: float = 4.0, spill_queue: int = 1,
-                 spill_wait_ms: float = 1.0):
+                 spill_wait_ms: float = 1.0, batch_from: int = 1):
         import torch
 
         from .engine import Engine
@@ -273,6 +273,11 @@ class BatchedServer:
         # the GPU with it (two pipelines that each stream 1-2 GB slow each
         # other down by more than the wait).  spill_queue=1: start at once.
         self.spill_queue, self.spill_wait_ms = max(1, int(spill_queue)), spill_wait_ms
+        # While fewer than batch_from requests wait, a free slot takes one (run
+        # alone, as one pipeline per launch would): a batch of two or three
+        # makes its first request wait for all of them, which only pays once
+        # the queue is long.  batch_from=1: always batch what is waiting.
+        self.batch_from = max(1, int(batch_from))
         self.slots = []
         for _ in range(n_slots):
             e = Engine(0)
@@ -453,7 +458,8 @@ class BatchedServer:
                         break  # the running slot keeps the GPU a little longer
                     running += 1
                     kind = next_kind(pending, self.policy, waited, self.max_wait_ms)
-                    reqs = admit(pending, foot, self.max_batch, self.pool_bytes, self.max_items, kind)
+                    mb = 1 if len(pending) < self.batch_from else self.max_batch
+                    reqs = admit(pending, foot, mb, self.pool_bytes, self.max_items, kind)
                     tb = sum(foot[r.rid][0] for r in reqs)
                     if tb > self.pool_bytes:  # a single request above the pool: upper-bound tables do not fit
                         raise RuntimeError(f"request {reqs[0].rid} needs {tb} bytes of tables, slot holds "

@@ -75,15 +75,17 @@ def test_served_without_sharing(engine, tables):
     srv.close()
 
 
-@pytest.mark.parametrize("policy,slots,spill", [("short_first", 2, 1), ("short_first", 3, 1), ("short_first", 2, 3),
-                                                ("fifo", 2, 2)])
-def test_served_short_first_equals_solo(engine, tables, policy, slots, spill):
+@pytest.mark.parametrize("policy,slots,spill,batch_from", [("short_first", 2, 1, 1), ("short_first", 3, 1, 1),
+                                                           ("short_first", 2, 3, 1), ("fifo", 2, 2, 1),
+                                                           ("short_first", 2, 1, 3), ("fifo", 1, 1, 4)])
+def test_served_short_first_equals_solo(engine, tables, policy, slots, spill, batch_from):
     """Short-first admission (one kind per launch, shortest kind first, no
-    starvation) and the spill rule (a second slot starts only once requests
-    queue): answers unchanged, every request served."""
+    starvation), the spill rule (a second slot starts only once requests
+    queue) and the batch threshold (one request per launch while fewer than
+    batch_from wait): answers unchanged, every request served."""
     reqs = S.poisson_requests(20000.0, 60, seed=12)
     srv = S.BatchedServer(tables, n_slots=slots, max_batch=8, pool_bytes=512 << 20, max_items=32768,
-                          policy=policy, max_wait_ms=1.0, spill_queue=spill)
+                          policy=policy, max_wait_ms=1.0, spill_queue=spill, batch_from=batch_from)
     srv.serve(reqs)
     assert all(r.result is not None and r.done >= r.arrival for r in reqs)
     check(engine, tables, reqs)
