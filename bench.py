@@ -178,15 +178,29 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
 
     res_sz = C.sizeof(N.JoinResult)
     K, W = args.steps, args.warmup
-    results = torch.zeros((K + W) * res_sz, dtype=torch.uint8, device="cuda")
-    preds = torch.zeros(K + W, dtype=torch.float32, device="cuda")
+    results = torch.zeros(max(K + W, 6) * res_sz, dtype=torch.uint8, device="cuda")
+    preds = torch.zeros(max(K + W, 6), dtype=torch.float32, device="cuda")
 
-    def learned_step(i, slot):
+    # Queries in flight: with 2, consecutive queries alternate between two
+    # contexts (each owns its join workspace) on two streams, so one query's
+    # init and build can run on SMs the other's probe has left.  The second
+    # context's sizer is the same network (parameters copied, margin included).
+    lanes = [(eng, stream, sizer)]
+    if args.inflight > 1:
+        eng2 = Engine(local_rank)
+        stream2 = torch.cuda.Stream()
+        eng2.set_stream(stream2.cuda_stream)
+        sizer2 = L.JoinSizer(eng2, seed=5)
+        sizer2.mlp.set_params(sizer.mlp.get_params())
+        sizer2.margin = sizer.margin
+        lanes.append((eng2, stream2, sizer2))
+
+    def learned_step(i, slot, sz=sizer):
         # MLP prediction folded into the table's init kernel (bo_join_learned_device)
         c = copies[i % 3]
         j = c["j"]
-        sizer.join_device(feats[i % 3], c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq,
-                          results[slot * res_sz:(slot + 1) * res_sz], preds[slot:slot + 1])
+        sz.join_device(feats[i % 3], c["b"], c["p"], N_BUILD, N_PROBE, j.date_lt, j.seg_eq,
+                       results[slot * res_sz:(slot + 1) * res_sz], preds[slot:slot + 1])
 
     def check(slots):
         host = results.cpu().numpy().tobytes()
@@ -198,23 +212,35 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
 
     # ---- the step as the product runs it: one learned query (MLP prediction +
     # init + build + probe, no host round trip) is one CUDA graph; one graph
-    # per input copy, each writing its own result record.
-    for i in range(3):
-        learned_step(i, i)
+    # per input copy and context, each writing its own result record (context
+    # l, copy k: record 3 l + k).
+    for li, (le, ls, lz) in enumerate(lanes):  # eager first: workspaces exist before capture
+        for i in range(3):
+            learned_step(i, 3 * li + i, lz)
     torch.cuda.synchronize()
-    step_graphs = []
+    lane_graphs = []
     kernels_per_step = 0
-    for k in range(3):
-        g = torch.cuda.CUDAGraph()
-        n0 = eng.launches
-        with torch.cuda.graph(g, stream=stream):
-            learned_step(k, k)
-        kernels_per_step = eng.launches - n0
-        step_graphs.append(g)
+    for li, (le, ls, lz) in enumerate(lanes):
+        gs = []
+        for k in range(3):
+            g = torch.cuda.CUDAGraph()
+            n0 = le.launches
+            with torch.cuda.graph(g, stream=ls):
+                learned_step(k, 3 * li + k, lz)
+            kernels_per_step = le.launches - n0
+            gs.append(g)
+        lane_graphs.append(gs)
+    step_graphs = lane_graphs[0]
+
+    def replay_step(i):
+        # query i: context i % inflight, copy i % 3, on that context's stream
+        li = i % len(lanes)
+        with torch.cuda.stream(lanes[li][1]):
+            lane_graphs[li][i % 3].replay()
 
     # ---- warm-up
     for i in range(W):
-        step_graphs[i % 3].replay()
+        replay_step(i)
     torch.cuda.synchronize()
 
     # ---- timed: K learned-sized queries (graph replays, copies rotated),
@@ -230,15 +256,21 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     t_win = time.perf_counter()
     while time.perf_counter() - t_win < 0.6:
         for i in range(64):
-            step_graphs[i % 3].replay()
+            replay_step(i)
         torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
+    for _, ls, _ in lanes[1:]:
+        ls.wait_event(ev0)  # every context starts after the opening event
     torch.cuda.nvtx.range_push("timed")  # lets a profiler select exactly the timed launches
     for i in range(K):
-        step_graphs[i % 3].replay()
+        replay_step(i)
     torch.cuda.nvtx.range_pop()
+    for _, ls, _ in lanes[1:]:
+        e_l = torch.cuda.Event()
+        e_l.record(ls)
+        stream.wait_event(e_l)  # the closing event follows every context's last query
     ev1.record(stream)
     torch.cuda.synchronize()
     launches = K * kernels_per_step
@@ -248,9 +280,9 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     # exactly, and the rerun is counted in the time.
     reruns = 0
     t_fix = time.perf_counter()
-    rs_last = check(range(3))
+    rs_last = check(range(3 * len(lanes)))
     for k in range(K):
-        if rs_last[k % 3]["overflowed"]:
+        if rs_last[3 * (k % len(lanes)) + k % 3]["overflowed"]:
             c = copies[k % 3]
             eng.join_plain(c["b"], c["p"], N_BUILD, N_PROBE, c["j"].date_lt, c["j"].seg_eq)
             reruns += 1
@@ -260,11 +292,13 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
     torch.cuda.synchronize()
     clocks = sampler.stop()
     clocks["window"] = "0.6 s of the same step replays, then the timed region"
-    rs = [rs_last[k % 3] for k in range(K)]
-    for k in range(3):  # graph replays agree with the eager runs of the same copy
+    rs = [rs_last[3 * (k % len(lanes)) + k % 3] for k in range(K)]
+    for k in range(3):  # every context's graph replays agree with the plain form on the same copy
         c = copies[k]
         ref = eng.join_plain(c["b"], c["p"], N_BUILD, N_PROBE, c["j"].date_lt, c["j"].seg_eq)
-        assert (rs_last[k]["match_count"], rs_last[k]["sum_exact"]) == (ref["match_count"], ref["sum_exact"])
+        for li in range(len(lanes)):
+            got = rs_last[3 * li + k]
+            assert (got["match_count"], got["sum_exact"]) == (ref["match_count"], ref["sum_exact"])
     ms = max_over_ranks(ms, dist)
 
     # ---- per-query latency: learned vs plain (results on the host each time)
@@ -514,6 +548,7 @@ def run_engine(args, rank: int, world: int, local_rank: int, dist) -> dict | Non
             "config": {
                 "workload": WORKLOAD,
                 "form": "learned-sized (MLP prediction on device, no host round trip), exact rerun on overflow",
+                "queries_in_flight": args.inflight,
                 "build_rows": N_BUILD, "probe_rows": N_PROBE, "global_batch": ROWS_PER_STEP,
                 "l2": "3 input copies rotated between steps (3 x 133.5 MB > 126 MB L2)",
                 "parallelism": f"replicas x{world}",
@@ -1405,6 +1440,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--inflight", type=int, choices=[1, 2], default=1,
+                    help="headline queries in flight: 2 alternates them between two contexts and streams")
     ap.add_argument("--sections", default="all",
                     help="other configurations reported beside the headline: all, none, or a comma list of "
                          "scan_agg,groupby,join_large,batch,serving,tpch,ceb")
