@@ -484,8 +484,11 @@ typedef struct bo_tpch_q3_row {   /* Q3ResultRow fields (bespoke_tpch/query_q3.h
 } bo_tpch_q3_row;
 
 /* Device columns in, rows on the host: the first min(n, max_rows) rows are
- * copied to out_host and *n_rows = n.  segment_code < 0 (segment not in the
- * dictionary) gives no rows. */
+ * written to out_host and *n_rows = n.  segment_code < 0 (segment not in the
+ * dictionary) gives no rows.  Where out_host is mapped pinned host memory
+ * (bo_host_alloc_pinned; 16-byte aligned) the last kernel writes the rows
+ * into it directly and the call synchronises once; other memory receives a
+ * copy.  The same holds for bo_tpch_q11_rows, bo_tpch_q16 and bo_tpch_q2. */
 int bo_tpch_q3(bo_ctx* ctx, const bo_tpch_q3_tables* tables, int16_t date_offset, int32_t segment_code,
                bo_tpch_q3_row* out_host, int64_t max_rows, int64_t* n_rows);
 
