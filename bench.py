@@ -1440,7 +1440,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--inflight", type=int, choices=[1, 2], default=1,
+    ap.add_argument("--inflight", type=int, choices=[1, 2], default=2,
                     help="headline queries in flight: 2 alternates them between two contexts and streams")
     ap.add_argument("--sections", default="all",
                     help="other configurations reported beside the headline: all, none, or a comma list of "
