@@ -56,3 +56,33 @@ def test_options_leave_the_other_columns_unchanged(tmp_path):
         ta, tb = pq.read_table(a / f"{t}.parquet"), pq.read_table(b / f"{t}.parquet")
         for col in cols:
             assert ta[col].equals(tb[col]), (t, col)
+
+
+def test_partsupp_lineitem_keys_and_part_layouts(tmp_path):
+    """lineitem_keys="partsupp": every lineitem names one of its part's four
+    partsupp pairs; repeat_part=False: n_part part rows and four partsupp rows
+    per part (the layout run_q16 walks by row position); supplier comments
+    with and without "Customer" before "Complaints", balances that vary."""
+    d = write_tpch(tmp_path / "d", n_customer=300, n_orders=2000, seed=4, n_supplier=40, n_part=120,
+                   repeat_part=False, lineitem_keys="partsupp")
+    li, ps = pq.read_table(d / "lineitem.parquet"), pq.read_table(d / "partsupp.parquet")
+    pairs = set(zip(ps["ps_partkey"].to_pylist(), ps["ps_suppkey"].to_pylist()))
+    assert len(pairs) == ps.num_rows == 4 * 120
+    assert all((p, s) in pairs for p, s in zip(li["l_partkey"].to_pylist(), li["l_suppkey"].to_pylist()))
+    assert li["l_partkey"].to_numpy().max() <= 120 and len(set(li["l_partkey"].to_pylist())) > 100
+    p = pq.read_table(d / "part.parquet")["p_partkey"].to_pylist()
+    assert p == list(range(1, 121))
+    s = pq.read_table(d / "supplier.parquet")
+    comments = s["s_comment"].to_pylist()
+
+    def banned(c):
+        i = c.find("Customer")
+        return i >= 0 and c.find("Complaints", i + 8) >= 0
+
+    assert 0 < sum(map(banned, comments)) < len(comments)
+    assert len(set(s["s_acctbal"].to_pylist())) > 30
+    # the other columns do not move with these options
+    base = write_tpch(tmp_path / "b", n_customer=300, n_orders=2000, seed=4, n_supplier=40, n_part=120)
+    lb = pq.read_table(base / "lineitem.parquet")
+    for col in ("l_orderkey", "l_quantity", "l_extendedprice", "l_discount", "l_shipdate"):
+        assert li[col].equals(lb[col]), col
