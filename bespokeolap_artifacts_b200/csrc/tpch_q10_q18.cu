@@ -364,8 +364,8 @@ __global__ void q18_gather_kernel(const uint32_t* __restrict__ vals, const int32
                                   const int32_t* __restrict__ o_custkey, const int16_t* __restrict__ o_orderdate,
                                   const int32_t* __restrict__ o_totalprice, int dense,
                                   const int32_t* __restrict__ sum, Q18Cust cust, const unsigned long long* n_out,
-                                  bo_tpch_q18_row* __restrict__ out) {
-  const unsigned long long n = *n_out;
+                                  unsigned long long limit, bo_tpch_q18_row* __restrict__ out) {
+  const unsigned long long n = *n_out < limit ? *n_out : limit;  // the first min(count, limit) rows
   for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (unsigned long long)gridDim.x * blockDim.x) {
     const uint32_t row = vals[i];
@@ -640,9 +640,14 @@ extern "C" int bo_tpch_q10_host_rows(bo_ctx* ctx, const bo_tpch_q10_tables* t, i
   return BO_OK;
 }
 
-extern "C" int bo_tpch_q18(bo_ctx* ctx, const bo_tpch_q18_tables* t, int32_t quantity_threshold,
-                           bo_tpch_q18_row* out_host, int64_t max_rows, int64_t* n_rows) {
-  BO_CHECK_CTX(ctx);
+namespace {
+// counted: both sorts read the result count on the device and the rows go
+// straight into out_host where it is mapped pinned memory (one
+// synchronisation); a count beyond one cluster sort reruns the whole query
+// with the count read back before the sorts (the second sort's keys replace
+// the first's, so the rerun starts over).
+int q18_run(bo_ctx* ctx, const bo_tpch_q18_tables* t, int32_t quantity_threshold, bo_tpch_q18_row* out_host,
+            int64_t max_rows, int64_t* n_rows, bool counted) {
   if (!t || !n_rows || max_rows < 0 || (max_rows > 0 && !out_host))
     return set_error(ctx, BO_ERR_INVALID, "q18: null argument");
   if (t->n_orders < 0 || t->n_lineitem < 0 || t->n_custkey_map < 0 || t->n_customer < 0 || t->orderkey_bound < 0)
@@ -689,7 +694,7 @@ extern "C" int bo_tpch_q18(bo_ctx* ctx, const bo_tpch_q18_tables* t, int32_t qua
   auto* n_out = carve<unsigned long long>(p, 8);
   BO_CUDA(ctx, cudaMemsetAsync(sum, 0, 4 * (size_t)bound, ctx->stream));
   if (use_mark) BO_CUDA(ctx, cudaMemsetAsync(mark, 0, 4 * (size_t)mark_words, ctx->stream));
-  BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, 8, ctx->stream));
+  BO_CUDA(ctx, cudaMemsetAsync(n_out, 0, 16, ctx->stream));  // the count and the sorts' overflow word
   if (t->n_lineitem > 0) {
     const int64_t threads = t->n_lineitem / kQ18RowsPerThread + kQ18RowsPerThread;
     q18_sum_kernel<<<grid_for(ctx, threads), kTpBlock, 0, ctx->stream>>>(
@@ -703,16 +708,44 @@ extern "C" int bo_tpch_q18(bo_ctx* ctx, const bo_tpch_q18_tables* t, int32_t qua
       t->o_orderkey, t->o_custkey, no, dense ? 1 : 0, bound, sum, use_mark ? mark : nullptr, quantity_threshold,
       cust, keys, vals, n_out, ctx->d_err);
   if ((rc = after_launch(ctx, "q18_qualify_kernel"))) return rc;
-  int64_t ns = 0;  // the result's size, read back once (see bo_tpch_q10)
-  if ((rc = read_device_count(ctx, n_out, cap, &ns))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 32, nullptr))) return rc;
+  uint32_t* overflow = reinterpret_cast<uint32_t*>(n_out + 1);
+  int64_t ns = 0;
+  if (!counted) {  // the result's size, read back once before the sorts
+    if ((rc = read_device_count(ctx, n_out, cap, &ns))) return rc;
+    if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 32, nullptr))) return rc;
+  } else if ((rc = cluster_sort_pairs_counted(ctx, keys, vals, n_out, cap, 0, 32, overflow))) {
+    return rc;
+  }
   q18_key2_kernel<<<grid_for(ctx, no), kTpBlock, 0, ctx->stream>>>(vals, t->o_totalprice, t->o_orderdate, n_out,
                                                                      keys);
   if ((rc = after_launch(ctx, "q18_key2_kernel"))) return rc;
-  if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 48, nullptr))) return rc;
+  if (!counted) {
+    if ((rc = radix_sort_pairs(ctx, keys, vals, tkeys, tvals, ns, 0, 48, nullptr))) return rc;
+  } else if ((rc = cluster_sort_pairs_counted(ctx, keys, vals, n_out, cap, 0, 48, overflow))) {
+    return rc;
+  }
+  bo_tpch_q18_row* direct =
+      (counted && max_rows > 0) ? static_cast<bo_tpch_q18_row*>(mapped_device_ptr(out_host)) : nullptr;
+  const int64_t lim = direct ? std::min<int64_t>(max_rows, cap) : cap;
   q18_gather_kernel<<<grid_for(ctx, no), kTpBlock, 0, ctx->stream>>>(vals, t->o_orderkey, t->o_custkey,
                                                                        t->o_orderdate, t->o_totalprice,
-                                                                       dense ? 1 : 0, sum, cust, n_out, rows);
+                                                                       dense ? 1 : 0, sum, cust, n_out,
+                                                                       (unsigned long long)lim, direct ? direct : rows);
   if ((rc = after_launch(ctx, "q18_gather_kernel"))) return rc;
+  if (!counted) return finish_known_rows(ctx, "q18", ns, rows, out_host, max_rows, n_rows);
+  bool over = false;
+  if ((rc = read_counted(ctx, "q18", n_out, cap, &ns, &over))) return rc;
+  if (over) return q18_run(ctx, t, quantity_threshold, out_host, max_rows, n_rows, false);
+  if (direct) {
+    *n_rows = ns;
+    return BO_OK;
+  }
   return finish_known_rows(ctx, "q18", ns, rows, out_host, max_rows, n_rows);
+}
+}  // namespace
+
+extern "C" int bo_tpch_q18(bo_ctx* ctx, const bo_tpch_q18_tables* t, int32_t quantity_threshold,
+                           bo_tpch_q18_row* out_host, int64_t max_rows, int64_t* n_rows) {
+  BO_CHECK_CTX(ctx);
+  return q18_run(ctx, t, quantity_threshold, out_host, max_rows, n_rows, true);
 }

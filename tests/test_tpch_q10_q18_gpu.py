@@ -87,7 +87,11 @@ def q18_oracle(t, thr):
 
 
 @pytest.mark.parametrize("thr", [25_000, 30_000, 0])
-def test_q18_matches_numpy(engine, torch_cuda, thr):
+@pytest.mark.parametrize("mapped", [False, True])
+def test_q18_matches_numpy(engine, torch_cuda, thr, mapped):
+    """Rows into pageable memory (copied) and into mapped pinned memory
+    (written by the gather kernel); threshold 0 keeps more orders than one
+    cluster sort holds (the query reruns with the count read back)."""
     torch = torch_cuda
     t = tables(1_500_000, 2)
     g = dev(torch, t)
@@ -99,13 +103,28 @@ def test_q18_matches_numpy(engine, torch_cuda, thr):
     tb.custkey_to_row, tb.n_custkey_map = g["cmap"].data_ptr(), len(t["cmap"])
     tb.n_customer = 150_000
     tb.orderkey_bound = max(int(t["okey"].max()), int(t["lkey"].max())) + 1
-    out = (N.TpchQ18Row * len(t["okey"]))()
+    cap = len(t["okey"])
     n = C.c_int64()
-    engine.ctx.call("bo_tpch_q18", C.byref(tb), thr, out, len(t["okey"]), C.byref(n))
+    row_t = np.dtype([("sum", "<i8"), ("cust", "<i4"), ("crow", "<i4"), ("okey", "<i4"), ("total", "<i4"),
+                      ("date", "<i2"), ("p0", "<i2"), ("p1", "<i4")])
+    if mapped:
+        buf = C.c_void_p()
+        engine.ctx.call("bo_host_alloc_pinned", C.sizeof(N.TpchQ18Row) * cap, C.byref(buf))
+        try:
+            engine.ctx.call("bo_tpch_q18", C.byref(tb), thr, C.cast(buf, C.POINTER(N.TpchQ18Row)), cap, C.byref(n))
+            got = np.frombuffer((C.c_char * (C.sizeof(N.TpchQ18Row) * cap)).from_address(buf.value),
+                                dtype=row_t).copy()
+        finally:
+            engine.ctx.call("bo_host_free_pinned", buf)
+    else:
+        out = (N.TpchQ18Row * cap)()
+        engine.ctx.call("bo_tpch_q18", C.byref(tb), thr, out, cap, C.byref(n))
+        got = np.frombuffer(out, dtype=row_t)
     want = q18_oracle(t, thr)
     assert n.value == len(want[0]) and n.value > 0
-    got = np.frombuffer(out, dtype=np.dtype([("sum", "<i8"), ("cust", "<i4"), ("crow", "<i4"), ("okey", "<i4"),
-                                            ("total", "<i4"), ("date", "<i2"), ("p0", "<i2"), ("p1", "<i4")]))[: n.value]
+    if thr == 0:
+        assert n.value > 131_072
+    got = got[: n.value]
     for name, w in zip(("sum", "cust", "crow", "okey", "total", "date"), want):
         assert np.array_equal(got[name], w), name
 
