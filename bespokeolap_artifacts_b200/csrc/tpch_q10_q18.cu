@@ -360,27 +360,44 @@ __global__ void q18_key2_kernel(const uint32_t* __restrict__ vals, const int32_t
   }
 }
 
-__global__ void q18_gather_kernel(const uint32_t* __restrict__ vals, const int32_t* __restrict__ o_orderkey,
-                                  const int32_t* __restrict__ o_custkey, const int16_t* __restrict__ o_orderdate,
-                                  const int32_t* __restrict__ o_totalprice, int dense,
-                                  const int32_t* __restrict__ sum, Q18Cust cust, const unsigned long long* n_out,
-                                  unsigned long long limit, bo_tpch_q18_row* __restrict__ out) {
+// The result rows (the first min(*n_out, limit)), built one per thread in
+// shared memory and stored as consecutive 16-byte words: out may be mapped
+// pinned host memory (whole PCIe writes) or device memory; 16-byte aligned.
+constexpr int kQ18RowsBlock = 128;
+
+__global__ void __launch_bounds__(kQ18RowsBlock) q18_gather_kernel(
+    const uint32_t* __restrict__ vals, const int32_t* __restrict__ o_orderkey, const int32_t* __restrict__ o_custkey,
+    const int16_t* __restrict__ o_orderdate, const int32_t* __restrict__ o_totalprice, int dense,
+    const int32_t* __restrict__ sum, Q18Cust cust, const unsigned long long* n_out, unsigned long long limit,
+    bo_tpch_q18_row* __restrict__ out) {
+  __shared__ bo_tpch_q18_row stage[kQ18RowsBlock];
+  constexpr int kWords = (int)(sizeof(bo_tpch_q18_row) / 16);
+  static_assert(sizeof(bo_tpch_q18_row) % 16 == 0, "rows are whole 16-byte words");
   const unsigned long long n = *n_out < limit ? *n_out : limit;  // the first min(count, limit) rows
-  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (unsigned long long)gridDim.x * blockDim.x) {
-    const uint32_t row = vals[i];
-    const int32_t key = dense ? (int32_t)(row + 1) : o_orderkey[row];
-    const int32_t c = o_custkey[row];
-    bo_tpch_q18_row r;
-    r.sum_qty_raw = (int64_t)sum[key];
-    r.custkey = c;
-    r.cust_row = cust.row_of(c);
-    r.orderkey = key;
-    r.totalprice_raw = o_totalprice[row];
-    r.orderdate_offset = o_orderdate[row];
-    r.pad0 = 0;
-    r.pad1 = 0;
-    out[i] = r;
+  for (unsigned long long base = (unsigned long long)blockIdx.x * kQ18RowsBlock; base < n;
+       base += (unsigned long long)gridDim.x * kQ18RowsBlock) {
+    const unsigned long long i = base + threadIdx.x;
+    if (i < n) {
+      const uint32_t row = vals[i];
+      const int32_t key = dense ? (int32_t)(row + 1) : o_orderkey[row];
+      const int32_t c = o_custkey[row];
+      bo_tpch_q18_row r;
+      r.sum_qty_raw = (int64_t)sum[key];
+      r.custkey = c;
+      r.cust_row = cust.row_of(c);
+      r.orderkey = key;
+      r.totalprice_raw = o_totalprice[row];
+      r.orderdate_offset = o_orderdate[row];
+      r.pad0 = 0;
+      r.pad1 = 0;
+      stage[threadIdx.x] = r;
+    }
+    __syncthreads();
+    const int rows = (int)(n - base < kQ18RowsBlock ? n - base : kQ18RowsBlock);
+    const uint4* src = reinterpret_cast<const uint4*>(stage);
+    uint4* dst = reinterpret_cast<uint4*>(out + base);
+    for (int w = threadIdx.x; w < rows * kWords; w += kQ18RowsBlock) dst[w] = src[w];
+    __syncthreads();
   }
 }
 
@@ -727,10 +744,11 @@ int q18_run(bo_ctx* ctx, const bo_tpch_q18_tables* t, int32_t quantity_threshold
   bo_tpch_q18_row* direct =
       (counted && max_rows > 0) ? static_cast<bo_tpch_q18_row*>(mapped_device_ptr(out_host)) : nullptr;
   const int64_t lim = direct ? std::min<int64_t>(max_rows, cap) : cap;
-  q18_gather_kernel<<<grid_for(ctx, no), kTpBlock, 0, ctx->stream>>>(vals, t->o_orderkey, t->o_custkey,
-                                                                       t->o_orderdate, t->o_totalprice,
-                                                                       dense ? 1 : 0, sum, cust, n_out,
-                                                                       (unsigned long long)lim, direct ? direct : rows);
+  const int ggrid = (int)std::max<int64_t>(1, std::min<int64_t>((lim + kQ18RowsBlock - 1) / kQ18RowsBlock,
+                                                                  (int64_t)ctx->num_sms * 8));
+  q18_gather_kernel<<<ggrid, kQ18RowsBlock, 0, ctx->stream>>>(vals, t->o_orderkey, t->o_custkey, t->o_orderdate,
+                                                              t->o_totalprice, dense ? 1 : 0, sum, cust, n_out,
+                                                              (unsigned long long)lim, direct ? direct : rows);
   if ((rc = after_launch(ctx, "q18_gather_kernel"))) return rc;
   if (!counted) return finish_known_rows(ctx, "q18", ns, rows, out_host, max_rows, n_rows);
   bool over = false;
